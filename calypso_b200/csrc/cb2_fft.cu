@@ -1,0 +1,319 @@
+// cb2_fft.cu -- longitudinal transform fused with the grid-space products.
+//
+// One thread block per (theta, r) row: the Fourier coefficients of the 13
+// backward components (u, w, B, J vectors and T) are turned into grid values
+// in shared memory, the nonlinear products are formed pointwise, and the 12
+// product components are transformed back -- the grid never goes to HBM.
+// This replaces back_MHD_FFT_sel_from_recv, s_cal_nonlinear_sph_MHD and
+// fwd_MHD_FFT_sel_from_recv of the reference (MHD_src/sph_MHD/
+// MHD_FFT_selector.F90:185-249, cal_nonlinear_sph_MHD.f90:35-84) and the
+// rtm <-> rtp transposes around them.
+//
+// Normalisation (t_MHD_multi_FFTW.F90:220-355):
+//   f(phi_p) = a_0 + sum_{m=1..L} (a_m cos m phi_p + b_m sin m phi_p),
+//   a_0 = (1/N) sum f, a_m = (2/N) sum f cos, b_m = (2/N) sum f sin.
+// Two real rows share one complex FFT (x + i y).  The complex FFT is a
+// shared-memory Stockham autosort transform with radix 3, 4 and 2 stages,
+// N = 3^a 2^b.
+#include <cmath>
+
+#include "cb2_internal.cuh"
+
+namespace cb2 {
+
+template <typename T> struct C2;
+template <> struct C2<double> { using t = double2; };
+template <> struct C2<float> { using t = float2; };
+
+template <typename T2>
+__device__ inline T2 cmul(T2 a, T2 b) {
+  T2 r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+
+struct FFTPlan {
+  int n, nst;
+  int rad[24];
+};
+
+// one Stockham stage set; returns the buffer that holds the result
+template <typename T, typename T2>
+__device__ T2 *block_fft(T2 *x, T2 *y, const FFTPlan &pl, const T2 *tw, int sign) {
+  const int N = pl.n;
+  int Ns = 1;
+  const T s32 = (T)(0.5 * sqrt(3.0));
+  for (int st = 0; st < pl.nst; st++) {
+    const int R = pl.rad[st];
+    const int nb = N / R;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+      int k = j % Ns;
+      T2 v[4];
+      for (int r = 0; r < R; r++) {
+        T2 a = x[j + r * nb];
+        if (r > 0 && k > 0) {
+          int e = (r * k * (N / (Ns * R))) % N;
+          T2 w = tw[e];
+          if (sign > 0) w.y = -w.y;
+          a = cmul(a, w);
+        }
+        v[r] = a;
+      }
+      T2 o[4];
+      if (R == 2) {
+        o[0].x = v[0].x + v[1].x; o[0].y = v[0].y + v[1].y;
+        o[1].x = v[0].x - v[1].x; o[1].y = v[0].y - v[1].y;
+      } else if (R == 4) {
+        T2 a0, a1, a2, a3;
+        a0.x = v[0].x + v[2].x; a0.y = v[0].y + v[2].y;
+        a1.x = v[0].x - v[2].x; a1.y = v[0].y - v[2].y;
+        a2.x = v[1].x + v[3].x; a2.y = v[1].y + v[3].y;
+        T dx = v[1].x - v[3].x, dy = v[1].y - v[3].y;
+        // forward (sign < 0): (v1 - v3) * (-i); inverse: * (+i)
+        if (sign < 0) { a3.x = dy; a3.y = -dx; } else { a3.x = -dy; a3.y = dx; }
+        o[0].x = a0.x + a2.x; o[0].y = a0.y + a2.y;
+        o[1].x = a1.x + a3.x; o[1].y = a1.y + a3.y;
+        o[2].x = a0.x - a2.x; o[2].y = a0.y - a2.y;
+        o[3].x = a1.x - a3.x; o[3].y = a1.y - a3.y;
+      } else {  // R == 3
+        T2 t1, t2, t3;
+        t1.x = v[1].x + v[2].x; t1.y = v[1].y + v[2].y;
+        t2.x = v[0].x - (T)0.5 * t1.x; t2.y = v[0].y - (T)0.5 * t1.y;
+        T dx = v[1].x - v[2].x, dy = v[1].y - v[2].y;
+        // forward: (v1 - v2) * (-i sqrt3/2); inverse: * (+i sqrt3/2)
+        if (sign < 0) { t3.x = s32 * dy; t3.y = -s32 * dx; } else { t3.x = -s32 * dy; t3.y = s32 * dx; }
+        o[0].x = v[0].x + t1.x; o[0].y = v[0].y + t1.y;
+        o[1].x = t2.x + t3.x; o[1].y = t2.y + t3.y;
+        o[2].x = t2.x - t3.x; o[2].y = t2.y - t3.y;
+      }
+      int d = (j / Ns) * Ns * R + k;
+      for (int r = 0; r < R; r++) y[d + r * Ns] = o[r];
+    }
+    __syncthreads();
+    T2 *t = x; x = y; y = t;
+    Ns *= R;
+  }
+  return x;
+}
+
+// spectrum of two real rows -> z = x + i y (Z = X + i Y, X Hermitian)
+template <typename T, typename T2>
+__device__ void load_pair(T2 *Z, int N, int L, const T *f0, const T *f1) {
+  for (int q = threadIdx.x; q < N; q += blockDim.x) Z[q] = T2{0, 0};
+  __syncthreads();
+  int mmax = min(L, (N + 1) / 2 - 1);
+  for (int m = threadIdx.x; m <= mmax; m += blockDim.x) {
+    T a0 = f0[2 * m], b0 = (m > 0) ? f0[2 * m + 1] : (T)0;
+    T a1 = f1 ? f1[2 * m] : (T)0, b1 = (f1 && m > 0) ? f1[2 * m + 1] : (T)0;
+    if (m == 0) {
+      Z[0] = T2{a0, a1};
+    } else {
+      T xr = (T)0.5 * a0, xi = (T)-0.5 * b0, yr = (T)0.5 * a1, yi = (T)-0.5 * b1;
+      Z[m] = T2{xr - yi, xi + yr};
+      Z[N - m] = T2{xr + yi, -xi + yr};
+    }
+  }
+  __syncthreads();
+}
+
+// FFT of z = x + i y -> (a_m, b_m) of both rows, m = 0..L
+template <typename T, typename T2>
+__device__ void store_pair(const T2 *Z, int N, int L, T *f0, T *f1) {
+  T an = (T)(1.0 / (double)N);
+  for (int m = threadIdx.x; m <= L; m += blockDim.x) {
+    if (m == 0) {
+      f0[0] = an * Z[0].x; f0[1] = 0;
+      if (f1) { f1[0] = an * Z[0].y; f1[1] = 0; }
+    } else if (m < N) {
+      T2 zk = Z[m % N], zn = Z[(N - m) % N];
+      T xr = (T)0.5 * (zk.x + zn.x), xi = (T)0.5 * (zk.y - zn.y);
+      T yr = (T)0.5 * (zk.y + zn.y), yi = (T)-0.5 * (zk.x - zn.x);
+      f0[2 * m] = (T)2 * an * xr; f0[2 * m + 1] = (T)-2 * an * xi;
+      if (f1) { f1[2 * m] = (T)2 * an * yr; f1[2 * m + 1] = (T)-2 * an * yi; }
+    }
+  }
+}
+
+struct ProdCoef {
+  double cv, cl, ci, ct;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_fft_products(FFTPlan pl, int L, int NS, const T *four, T *four2, const typename C2<T>::t *tw,
+               ProdCoef pc) {
+  using T2 = typename C2<T>::t;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int N = pl.n;
+  T2 *Z0 = reinterpret_cast<T2 *>(smraw);
+  T2 *Z1 = Z0 + N;
+  T *g = reinterpret_cast<T *>(Z1 + N);   // [13][N]
+  const size_t row = blockIdx.x;
+  const T *fin = four + row * 13 * NS;
+  T *fout = four2 + row * 12 * NS;
+  for (int c = 0; c < 13; c += 2) {
+    load_pair<T, T2>(Z0, N, L, fin + (size_t)c * NS, (c + 1 < 13) ? fin + (size_t)(c + 1) * NS : nullptr);
+    T2 *z = block_fft<T, T2>(Z0, Z1, pl, tw, +1);
+    for (int q = threadIdx.x; q < N; q += blockDim.x) {
+      g[c * N + q] = z[q].x;
+      if (c + 1 < 13) g[(c + 1) * N + q] = z[q].y;
+    }
+    __syncthreads();
+  }
+  const T cv = (T)pc.cv, cl = (T)pc.cl, ci = (T)pc.ci, ct = (T)pc.ct;
+  for (int q = threadIdx.x; q < N; q += blockDim.x) {
+    T ur = g[0 * N + q], ut = g[1 * N + q], up = g[2 * N + q];
+    T wr = g[3 * N + q], wt = g[4 * N + q], wp = g[5 * N + q];
+    T br = g[6 * N + q], bt = g[7 * N + q], bp = g[8 * N + q];
+    T jr = g[9 * N + q], jt = g[10 * N + q], jp = g[11 * N + q];
+    T tt = g[12 * N + q];
+    g[0 * N + q] = (wt * up - wp * ut) * cv;
+    g[1 * N + q] = (wp * ur - wr * up) * cv;
+    g[2 * N + q] = (wr * ut - wt * ur) * cv;
+    g[3 * N + q] = (jt * bp - jp * bt) * cl;
+    g[4 * N + q] = (jp * br - jr * bp) * cl;
+    g[5 * N + q] = (jr * bt - jt * br) * cl;
+    g[6 * N + q] = (ut * bp - up * bt) * ci;
+    g[7 * N + q] = (up * br - ur * bp) * ci;
+    g[8 * N + q] = (ur * bt - ut * br) * ci;
+    g[9 * N + q] = ur * tt * ct;
+    g[10 * N + q] = ut * tt * ct;
+    g[11 * N + q] = up * tt * ct;
+  }
+  __syncthreads();
+  for (int c = 0; c < 12; c += 2) {
+    for (int q = threadIdx.x; q < N; q += blockDim.x) Z0[q] = T2{g[c * N + q], g[(c + 1) * N + q]};
+    __syncthreads();
+    T2 *z = block_fft<T, T2>(Z0, Z1, pl, tw, -1);
+    store_pair<T, T2>(z, N, L, fout + (size_t)c * NS, fout + (size_t)(c + 1) * NS);
+    __syncthreads();
+  }
+}
+
+// Fourier rows -> grid (float64), for the standalone transform API
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_fft_to_grid(FFTPlan pl, int L, int NS, int nc, int nr, int nth, const T *four, double *grid,
+              const typename C2<T>::t *tw) {
+  using T2 = typename C2<T>::t;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int N = pl.n;
+  T2 *Z0 = reinterpret_cast<T2 *>(smraw), *Z1 = Z0 + N;
+  const size_t row = blockIdx.x;
+  const int th = (int)(row / nr), k = (int)(row % nr);
+  const T *fin = four + row * nc * NS;
+  for (int c = 0; c < nc; c += 2) {
+    load_pair<T, T2>(Z0, N, L, fin + (size_t)c * NS, (c + 1 < nc) ? fin + (size_t)(c + 1) * NS : nullptr);
+    T2 *z = block_fft<T, T2>(Z0, Z1, pl, tw, +1);
+    for (int q = threadIdx.x; q < N; q += blockDim.x) {
+      grid[(((size_t)c * nr + k) * nth + th) * N + q] = (double)z[q].x;
+      if (c + 1 < nc) grid[(((size_t)(c + 1) * nr + k) * nth + th) * N + q] = (double)z[q].y;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_grid_to_fft(FFTPlan pl, int L, int NS, int nc, int nr, int nth, const double *grid, T *four,
+              const typename C2<T>::t *tw) {
+  using T2 = typename C2<T>::t;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int N = pl.n;
+  T2 *Z0 = reinterpret_cast<T2 *>(smraw), *Z1 = Z0 + N;
+  const size_t row = blockIdx.x;
+  const int th = (int)(row / nr), k = (int)(row % nr);
+  T *fout = four + row * nc * NS;
+  for (int c = 0; c < nc; c += 2) {
+    for (int q = threadIdx.x; q < N; q += blockDim.x) {
+      T x = (T)grid[(((size_t)c * nr + k) * nth + th) * N + q];
+      T y = (c + 1 < nc) ? (T)grid[(((size_t)(c + 1) * nr + k) * nth + th) * N + q] : (T)0;
+      Z0[q] = T2{x, y};
+    }
+    __syncthreads();
+    T2 *z = block_fft<T, T2>(Z0, Z1, pl, tw, -1);
+    store_pair<T, T2>(z, N, L, fout + (size_t)c * NS, (c + 1 < nc) ? fout + (size_t)(c + 1) * NS : nullptr);
+    __syncthreads();
+  }
+}
+
+__global__ void k_twiddles(int n, double2 *tw, float2 *tw32) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  double s, c;
+  sincospi(2.0 * (double)e / (double)n, &s, &c);
+  tw[e] = make_double2(c, -s);
+  tw32[e] = make_float2((float)c, (float)-s);
+}
+
+static FFTPlan make_plan(int n) {
+  FFTPlan p{};
+  p.n = n;
+  int m = n;
+  while (m % 3 == 0) { p.rad[p.nst++] = 3; m /= 3; }
+  while (m % 4 == 0) { p.rad[p.nst++] = 4; m /= 4; }
+  while (m % 2 == 0) { p.rad[p.nst++] = 2; m /= 2; }
+  if (m != 1) p.nst = -1;
+  return p;
+}
+
+int fft_setup(Ctx &c) {
+  FFTPlan p = make_plan(c.nph);
+  if (p.nst < 0) {
+    set_error("ngrid_zonal_ctl must be of the form 3^a 2^b");
+    return CB2_ERR_ARG;
+  }
+  CB2_CUDA(cudaMalloc(&c.d_tw_fft, (size_t)c.nph * sizeof(double2)));
+  CB2_CUDA(cudaMalloc(&c.d_tw_fft32, (size_t)c.nph * sizeof(float2)));
+  k_twiddles<<<cdiv(c.nph, 256), 256, 0, c.stream>>>(c.nph, (double2 *)c.d_tw_fft,
+                                                     (float2 *)c.d_tw_fft32);
+  CB2_CUDA(cudaGetLastError());
+  size_t big = 2 * (size_t)c.nph * sizeof(double2) + 13 * (size_t)c.nph * sizeof(double);
+  CB2_CUDA(cudaFuncSetAttribute(k_fft_products<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
+  CB2_CUDA(cudaFuncSetAttribute(k_fft_products<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
+  return 0;
+}
+
+template <typename T>
+static const typename C2<T>::t *twid(Ctx &c) {
+  if (sizeof(T) == 8) return (const typename C2<T>::t *)c.d_tw_fft;
+  return (const typename C2<T>::t *)c.d_tw_fft32;
+}
+
+template <typename T>
+void fft_products(Ctx &c, const T *four, T *four2) {
+  using T2 = typename C2<T>::t;
+  FFTPlan p = make_plan(c.nph);
+  size_t sm = 2 * (size_t)c.nph * sizeof(T2) + 13 * (size_t)c.nph * sizeof(T);
+  ProdCoef pc{c.p.coef_velo, c.p.coef_lor, c.p.coef_induct, c.p.coef_temp};
+  k_fft_products<T><<<(unsigned)(c.nth * c.nr), 256, sm, c.stream>>>(p, c.L, c.NS, four, four2,
+                                                                     twid<T>(c), pc);
+}
+
+template <typename T>
+void fft_backward_grid(Ctx &c, int ncomp, const T *four, double *grid) {
+  using T2 = typename C2<T>::t;
+  FFTPlan p = make_plan(c.nph);
+  size_t sm = 2 * (size_t)c.nph * sizeof(T2);
+  k_fft_to_grid<T><<<(unsigned)(c.nth * c.nr), 256, sm, c.stream>>>(p, c.L, c.NS, ncomp, c.nr, c.nth,
+                                                                    four, grid, twid<T>(c));
+}
+
+template <typename T>
+void fft_forward_grid(Ctx &c, int ncomp, const double *grid, T *four) {
+  using T2 = typename C2<T>::t;
+  FFTPlan p = make_plan(c.nph);
+  size_t sm = 2 * (size_t)c.nph * sizeof(T2);
+  k_grid_to_fft<T><<<(unsigned)(c.nth * c.nr), 256, sm, c.stream>>>(p, c.L, c.NS, ncomp, c.nr, c.nth,
+                                                                    grid, four, twid<T>(c));
+}
+
+template void fft_products<double>(Ctx &, const double *, double *);
+template void fft_products<float>(Ctx &, const float *, float *);
+template void fft_backward_grid<double>(Ctx &, int, const double *, double *);
+template void fft_backward_grid<float>(Ctx &, int, const float *, double *);
+template void fft_forward_grid<double>(Ctx &, int, const double *, double *);
+template void fft_forward_grid<float>(Ctx &, int, const double *, float *);
+
+}  // namespace cb2

@@ -1,0 +1,153 @@
+// cb2_internal.cuh -- private state and helpers of libcalypso_b200.
+//
+// Device layouts (HBM):
+//   spectral field  f[slot][k][jj]   float64, jj = "m-major" index: for
+//                   m = 0..L the block of l = m..L of order +m, then (m>0)
+//                   the block of l = m..L of order -m.  All rj operators
+//                   are elementwise in jj and 3-point stencils in k.
+//   Fourier data    F[theta][k][c][s] with s = 2m (cos, order +m) and
+//                   s = 2m+1 (sin, order -m), NS = 2(L+1) slots per row:
+//                   one (theta, k) row of all components is contiguous for
+//                   the fused FFT + product kernel.
+//   Legendre tables per order m:  P_lt[m][l-m][i], i over the nh = nth/2
+//                   Gauss nodes nearest the south pole (the other half
+//                   follows from the parity of P_l^m), and P_tl[m][i][l-m].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/calypso_b200.h"
+
+namespace cb2 {
+
+// field slots: the same numbering as the reference-side diagnostics use
+enum Slot {
+  VELO = 0, VORT = 3, MAGNE = 6, CURRENT = 9, TEMP = 12, WDIFF = 13,
+  BDIFF = 16, TDIFF = 19, MADV = 20, LOR = 23, VPIND = 26, HFLUX = 29,
+  ROTINERT = 32, ROTLOR = 35, INDUCT = 38, HADV = 41, ROTCOR = 42,
+  ROTBUO = 45, FORCES = 48, PREMOM = 51, PREUXB = 54, PREHEAT = 57,
+  NSLOT = 58
+};
+
+// one-sided boundary weights (see host set-up in cb2_tables.cu)
+struct BCW {
+  double fix_fld_icb[3][4], fix_fld_cmb[3][4];
+  double fix_dr_icb[3][4], fix_dr_cmb[3][4];
+  double r_icb[3], r_cmb[3];
+};
+
+// everything the rj kernels read by value
+struct RJArgs {
+  int nr, jmax, L, kin, kout;
+  double dt, cev, cet, ceb;           // explicit (1 - implicit) fractions
+  double coef_d_velo, coef_d_magne, coef_d_temp, coef_buo, coef_cor;
+  double coef_temp;
+  int use_ref_temp;
+  double temp_icb_fld, temp_cmb_fld;  // l = 0 perturbation wall values
+  BCW bc;
+  // per-jj tables
+  const int *jl, *jm;
+  const double *g3, *g3rlm, *gl;
+  // radial tables
+  const double *r, *ar1, *ar2, *d1, *d2, *reft0, *reft1, *om;  // d1/d2: [3][nr]
+};
+
+struct Ctx {
+  cb2_params p;
+  int prec = 0;
+  int device = 0;
+  int L = 0, nth = 0, nph = 0, nr = 0, jmax = 0, nh = 0, NS = 0, kin = 0, kout = 0;
+  cudaStream_t stream = nullptr;
+  // host tables
+  std::vector<int> h_jl, h_jm;          // per jj
+  std::vector<int> h_perm;              // jj -> j = l(l+1)+m
+  std::vector<int> h_moff;              // offset of block (m, +) for m = 0..L
+  std::vector<size_t> h_poff;           // offset of order m in the P tables
+  std::vector<double> h_r, h_colat, h_wgt;
+  BCW bc{};
+  double cev = 0, cet = 0, ceb = 0, temp_icb_fld = 0, temp_cmb_fld = 0;
+  // device tables
+  int *d_jl = nullptr, *d_jm = nullptr, *d_perm = nullptr, *d_moff = nullptr;
+  double *d_g3 = nullptr, *d_g3rlm = nullptr, *d_gl = nullptr, *d_g6 = nullptr;
+  double *d_g7 = nullptr, *d_g11 = nullptr, *d_g12 = nullptr;
+  double *d_r = nullptr, *d_ar1 = nullptr, *d_ar2 = nullptr, *d_d1 = nullptr, *d_d2 = nullptr;
+  double *d_reft0 = nullptr, *d_reft1 = nullptr, *d_om = nullptr;
+  double *d_colat = nullptr, *d_wgt = nullptr, *d_asin = nullptr;
+  size_t *d_poff = nullptr;
+  double *d_Plt = nullptr, *d_dPlt = nullptr, *d_Ptl = nullptr, *d_dPtl = nullptr;
+  int *d_jgi1 = nullptr, *d_jgi2 = nullptr, *d_jei1 = nullptr;
+  double *d_sw = nullptr, *d_tw = nullptr;       // [6][jmax], [8][jmax]
+  double *d_lu_vp = nullptr, *d_lu_vt = nullptr, *d_lu_bs = nullptr, *d_lu_bt = nullptr, *d_lu_t = nullptr;
+  int *d_pv_vp = nullptr, *d_pv_vt = nullptr, *d_pv_bs = nullptr, *d_pv_bt = nullptr, *d_pv_t = nullptr;
+  int *d_status = nullptr;               // device error word
+  double *d_tw_fft = nullptr;            // exp(-2 pi i e / nph), e = 0..nph-1
+  float *d_tw_fft32 = nullptr;
+  // state
+  double *d_f = nullptr;                 // NSLOT * nr * jmax
+  void *d_four = nullptr;                // F: nth*nr*13*NS (double or float)
+  void *d_four2 = nullptr;               // G: nth*nr*12*NS
+  double *d_ene = nullptr;               // energy partial sums
+  double *h_stage = nullptr;             // pinned staging buffer
+  size_t h_stage_bytes = 0;
+  double *d_tmp = nullptr;               // nr*jmax scratch for host transfers
+  double *d_host_state = nullptr;        // 20 slots for cb2_step_host_state
+  // mixed-precision Legendre operands (split fp16) -- owned by cb2_legendre_mixed.cu
+  void *mixed = nullptr;
+  int istep = 0;
+  bool started = false;
+  bool timers = false;
+  cudaEvent_t ev[64];
+  double stage_ms[32] = {0};
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_nsteps = 0;
+
+  size_t fsize() const { return (size_t)nr * jmax; }
+  double *fld(int slot) { return d_f + (size_t)slot * fsize(); }
+  RJArgs rj_args() const;
+};
+
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define CB2_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t _e = (call);                             \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call);  \
+  } while (0)
+
+// set-up (cb2_tables.cu)
+int setup_tables(Ctx &c);
+void free_tables(Ctx &c);
+// Legendre fp64 (cb2_legendre_f64.cu)
+void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four);
+void leg_fwd_f64(Ctx &c, int nvec, int nscal, const double *four, const int *slots);
+// FFT and grid products (cb2_fft.cu)
+int fft_setup(Ctx &c);
+template <typename T> void fft_products(Ctx &c, const T *four, T *four2);
+template <typename T> void fft_backward_grid(Ctx &c, int ncomp, const T *four, double *grid);
+template <typename T> void fft_forward_grid(Ctx &c, int ncomp, const double *grid, T *four);
+// rj operators and solves (cb2_rj.cu)
+void rj_explicit(Ctx &c, bool euler);
+void rj_implicit(Ctx &c);
+void rj_coriolis(Ctx &c);
+void rj_after_transform(Ctx &c);
+void rj_start_derived(Ctx &c);
+void rj_temp_total(Ctx &c, double sign);
+int rj_energies(Ctx &c, double out[7]);
+int rj_lu_factorise(Ctx &c);
+// mixed-precision Legendre (cb2_legendre_mixed.cu)
+int mixed_setup(Ctx &c);
+void mixed_free(Ctx &c);
+void leg_bwd_mixed(Ctx &c, int nvec, int nscal, const int *slots, float *four);
+void leg_fwd_mixed(Ctx &c, int nvec, int nscal, const float *four, const int *slots);
+
+constexpr int kThreads = 256;
+inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace cb2
+
+struct cb2_ctx : public cb2::Ctx {};

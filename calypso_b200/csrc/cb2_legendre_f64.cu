@@ -1,0 +1,331 @@
+// cb2_legendre_f64.cu -- float64 Legendre transforms (the plain path).
+//
+// Definition: PARALLEL_src/SPH_SHELL_src/legendre_bwd_trans_org.f90:45-209 and
+// legendre_fwd_trans_org.f90:45-169 of the reference, evaluated with the
+// equatorial symmetry that its SYMMETRIC_MATMUL variant uses
+// (cal_vr_rtm_by_matmul.f90, cal_sp_rlm_by_matmul.f90):
+//   P_l^m(pi - theta) = (-1)^(l-m) P_l^m(theta),
+//   dP_l^m/dtheta (pi - theta) = -(-1)^(l-m) dP_l^m/dtheta (theta).
+// Each term is accumulated by its reflection parity sigma, so the south node
+// i gets acc[0] + acc[1] and the mirror node nth-1-i gets acc[0] - acc[1].
+//
+// Backward: one block per (order m, radial tile, colatitude tile); one warp
+// per field group (a vector: S, dS/dr, T of orders +m and -m; or a scalar),
+// one lane per Gauss node of the south half.  The spectral coefficients of a
+// chunk of degrees are staged in shared memory, pre-scaled by l(l+1)/r^2,
+// 1/r and 1/r as legendre_b_trans_vector_org does.
+// Forward: one block per (order m, radial tile); one lane per degree l, the
+// Gauss-weighted symmetric / antisymmetric grid values staged in shared
+// memory.
+#include <algorithm>
+#include <type_traits>
+
+#include "cb2_internal.cuh"
+
+namespace cb2 {
+
+constexpr int BWD_KT = 4;   // radial levels per backward block
+constexpr int BWD_LC = 32;  // degrees per staged chunk
+constexpr int FWD_KT = 2;   // radial levels per forward block
+constexpr int FWD_TC = 16;  // Gauss node pairs per staged chunk
+constexpr int MAXG = 6;     // field groups (vectors + scalars) per launch
+
+struct LegArgs {
+  int L, nr, nth, nh, jmax, NS, nvec, nscal, ncomp, cbase;
+  int slot[MAXG];           // first rj slot of each group of this launch
+  const int *moff;
+  const size_t *poff;
+  const double *Plt, *dPlt, *Ptl, *dPtl, *asin_t, *wgt;
+  const double *g3rlm, *g6, *g7, *r, *ar1;
+  double *f;                // rj fields
+  size_t fs;                // slot stride
+};
+
+__device__ inline int jj_of(const LegArgs &a, int l, int m, int s) {
+  return a.moff[m] + s * (a.L + 1 - m) + (l - m);
+}
+
+// F[theta][k][c][slot], slot 2m = order +m, 2m+1 = order -m
+__device__ inline size_t four_at(const LegArgs &a, int th, int k, int c) {
+  return (((size_t)th * a.nr + k) * a.ncomp + c) * a.NS;
+}
+
+__global__ void __launch_bounds__(32 * MAXG)
+k_leg_bwd_f64(LegArgs a, double *four) {
+  const int m = blockIdx.z, k0 = blockIdx.y * BWD_KT, i0 = blockIdx.x * 32;
+  const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int ngrp = a.nvec + a.nscal;
+  const int nl = a.L + 1 - m;
+  const int i = i0 + lane;
+  const bool act = (g < ngrp) && (i < a.nh);
+  const bool isvec = g < a.nvec;
+  __shared__ double sc[MAXG][BWD_LC][6][BWD_KT];
+  double acc[BWD_KT][6][2];
+#pragma unroll
+  for (int q = 0; q < BWD_KT; q++)
+#pragma unroll
+    for (int c = 0; c < 6; c++) acc[q][c][0] = acc[q][c][1] = 0.0;
+  const double am = (i < a.nh) ? (double)m * a.asin_t[i] : 0.0;
+  const size_t po = a.poff[m];
+  for (int lc0 = 0; lc0 < nl; lc0 += BWD_LC) {
+    __syncthreads();
+    int tot = ngrp * BWD_LC * 6 * BWD_KT;
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      int lc = e % BWD_LC, t = e / BWD_LC;
+      int q = t % BWD_KT; t /= BWD_KT;
+      int v = t % 6, gg = t / 6;
+      int l = m + lc0 + lc, k = k0 + q;
+      int s = v & 1, comp = v >> 1;  // v: 0 S+ 1 S- 2 D+ 3 D- 4 T+ 5 T-
+      double val = 0.0;
+      if (l <= a.L && k < a.nr && !(m == 0 && s == 1)) {
+        int jj = jj_of(a, l, m, s);
+        if (gg < a.nvec) {
+          double x = a.f[(size_t)(a.slot[gg] + comp) * a.fs + (size_t)k * a.jmax + jj];
+          double ar = a.ar1[k];
+          val = (comp == 0) ? x * ar * ar * a.g3rlm[jj] : x * ar;
+        } else if (comp == 0) {
+          val = a.f[(size_t)a.slot[gg] * a.fs + (size_t)k * a.jmax + jj];
+        }
+      }
+      sc[gg][lc][v][q] = val;
+    }
+    __syncthreads();
+    if (act) {
+      int lcn = min(BWD_LC, nl - lc0);
+      // lc0 is even, so degree t = lc0 + lc has parity lc & 1: unrolling by
+      // two keeps the parity index a compile-time constant (registers)
+      auto body = [&](int lc, auto SPc) {
+        constexpr int sp = decltype(SPc)::value, sd = sp ^ 1;
+        int t = lc0 + lc;
+        double P = a.Plt[po + (size_t)t * a.nh + i];
+        double dP = a.dPlt[po + (size_t)t * a.nh + i];
+        double mP = P * am;
+        if (isvec) {
+#pragma unroll
+          for (int q = 0; q < BWD_KT; q++) {
+            double Sp = sc[g][lc][0][q], Sm = sc[g][lc][1][q];
+            double Dp = sc[g][lc][2][q], Dm = sc[g][lc][3][q];
+            double Tp = sc[g][lc][4][q], Tm = sc[g][lc][5][q];
+            acc[q][0][sp] += Sp * P;        // v_r(+m)
+            acc[q][1][sp] += Sm * P;        // v_r(-m)
+            acc[q][2][sd] += Dp * dP;       // v_theta(+m)
+            acc[q][2][sp] += Tm * mP;
+            acc[q][3][sd] += Dm * dP;       // v_theta(-m)
+            acc[q][3][sp] -= Tp * mP;
+            acc[q][4][sd] -= Tp * dP;       // v_phi(+m)
+            acc[q][4][sp] += Dm * mP;
+            acc[q][5][sd] -= Tm * dP;       // v_phi(-m)
+            acc[q][5][sp] -= Dp * mP;
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < BWD_KT; q++) {
+            acc[q][0][sp] += sc[g][lc][0][q] * P;
+            acc[q][1][sp] += sc[g][lc][1][q] * P;
+          }
+        }
+      };
+      int lc = 0;
+      for (; lc + 1 < lcn; lc += 2) {
+        body(lc, std::integral_constant<int, 0>());
+        body(lc + 1, std::integral_constant<int, 1>());
+      }
+      if (lc < lcn) body(lc, std::integral_constant<int, 0>());
+    }
+  }
+  if (!act) return;
+  const int ii = a.nth - 1 - i;
+  const int ncw = isvec ? 3 : 1;
+  const int c0 = a.cbase + (isvec ? 3 * g : 3 * a.nvec + (g - a.nvec));
+#pragma unroll
+  for (int q = 0; q < BWD_KT; q++) {
+    int k = k0 + q;
+    if (k >= a.nr) break;
+    for (int c = 0; c < ncw; c++) {
+      double e0 = acc[q][2 * c][0], o0 = acc[q][2 * c][1];
+      double e1 = acc[q][2 * c + 1][0], o1 = acc[q][2 * c + 1][1];
+      double2 south = make_double2(e0 + o0, m == 0 ? 0.0 : e1 + o1);
+      double2 north = make_double2(e0 - o0, m == 0 ? 0.0 : e1 - o1);
+      *reinterpret_cast<double2 *>(four + four_at(a, i, k, c0 + c) + 2 * m) = south;
+      if (ii != i)
+        *reinterpret_cast<double2 *>(four + four_at(a, ii, k, c0 + c) + 2 * m) = north;
+    }
+  }
+}
+
+// forward: block = (order m, radial tile); lane = degree l - m.  NV vectors
+// and NSC scalars starting at component c0 of the Fourier buffer (which
+// holds a.ncomp components) and at group g0 of a.slot.
+template <int NV, int NSC>
+__global__ void __launch_bounds__(256)
+k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
+  const int m = blockIdx.z, k0 = blockIdx.y * FWD_KT;
+  const int nl = a.L + 1 - m;
+  constexpr int C = 3 * NV + NSC;
+  extern __shared__ double hs[];   // [pair][k][c][s][sym/anti]
+  auto H = [&](int ip, int q, int c, int s, int par) -> double & {
+    return hs[((((size_t)ip * FWD_KT + q) * C + c) * 2 + s) * 2 + par];
+  };
+  const size_t po = a.poff[m];
+  for (int lt0 = 0; lt0 < nl; lt0 += blockDim.x) {
+    const int t = lt0 + threadIdx.x;   // l - m
+    const bool act = t < nl;
+    const int par = t & 1;
+    double accv[NV > 0 ? NV : 1][FWD_KT][6];
+    double accs[NSC > 0 ? NSC : 1][FWD_KT][2];
+#pragma unroll
+    for (int q = 0; q < FWD_KT; q++) {
+#pragma unroll
+      for (int v = 0; v < (NV > 0 ? NV : 1); v++)
+#pragma unroll
+        for (int c = 0; c < 6; c++) accv[v][q][c] = 0.0;
+#pragma unroll
+      for (int v = 0; v < (NSC > 0 ? NSC : 1); v++) accs[v][q][0] = accs[v][q][1] = 0.0;
+    }
+    for (int ib = 0; ib < a.nh; ib += FWD_TC) {
+      __syncthreads();
+      int npair = min(FWD_TC, a.nh - ib);
+      int tot = npair * FWD_KT * C * 2;
+      for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+        int s = e & 1, tt = e >> 1;
+        int c = tt % C; tt /= C;
+        int q = tt % FWD_KT, ip = tt / FWD_KT;
+        int k = k0 + q, i = ib + ip, ii = a.nth - 1 - i;
+        double fa = 0.0, fb = 0.0;
+        if (k < a.nr && !(m == 0 && s == 1)) {
+          fa = four[four_at(a, i, k, c0 + c) + 2 * m + s] * a.wgt[i];
+          fb = four[four_at(a, ii, k, c0 + c) + 2 * m + s] * a.wgt[ii];
+        }
+        H(ip, q, c, s, 0) = fa + fb;
+        H(ip, q, c, s, 1) = fa - fb;
+      }
+      __syncthreads();
+      if (act) {
+        for (int ip = 0; ip < npair; ip++) {
+          int i = ib + ip;
+          double P = a.Ptl[po + (size_t)i * nl + t];
+          double dP = a.dPtl[po + (size_t)i * nl + t];
+          double pg = P * (double)m * a.asin_t[i];   // P m / sin(theta), order +m
+#pragma unroll
+          for (int v = 0; v < NV; v++) {
+#pragma unroll
+            for (int q = 0; q < FWD_KT; q++) {
+              // order +m: ip slot 0, in slot 1 ; order -m: ip slot 1, in slot 0
+              double r0 = H(ip, q, 3 * v, 0, par), r1 = H(ip, q, 3 * v, 1, par);
+              double tp0 = H(ip, q, 3 * v + 1, 0, par ^ 1), tp1 = H(ip, q, 3 * v + 1, 1, par ^ 1);
+              double tn0 = H(ip, q, 3 * v + 1, 0, par), tn1 = H(ip, q, 3 * v + 1, 1, par);
+              double pp0 = H(ip, q, 3 * v + 2, 0, par ^ 1), pp1 = H(ip, q, 3 * v + 2, 1, par ^ 1);
+              double pn0 = H(ip, q, 3 * v + 2, 0, par), pn1 = H(ip, q, 3 * v + 2, 1, par);
+              accv[v][q][0] += r0 * P;
+              accv[v][q][1] += r1 * P;
+              accv[v][q][2] += tp0 * dP - pn1 * pg;
+              accv[v][q][3] += tp1 * dP + pn0 * pg;
+              accv[v][q][4] -= tn1 * pg + pp0 * dP;
+              accv[v][q][5] -= -tn0 * pg + pp1 * dP;
+            }
+          }
+#pragma unroll
+          for (int sc = 0; sc < NSC; sc++) {
+#pragma unroll
+            for (int q = 0; q < FWD_KT; q++) {
+              accs[sc][q][0] += H(ip, q, 3 * NV + sc, 0, par) * P;
+              accs[sc][q][1] += H(ip, q, 3 * NV + sc, 1, par) * P;
+            }
+          }
+        }
+      }
+    }
+    if (act) {
+      int l = m + t;
+      for (int s = 0; s < (m == 0 ? 1 : 2); s++) {
+        int jj = jj_of(a, l, m, s);
+        double g7 = a.g7[jj], g6 = a.g6[jj];
+#pragma unroll
+        for (int q = 0; q < FWD_KT; q++) {
+          int k = k0 + q;
+          if (k >= a.nr) break;
+          double r = a.r[k];
+          size_t at = (size_t)k * a.jmax + jj;
+#pragma unroll
+          for (int v = 0; v < NV; v++) {
+            double *f0 = a.f + (size_t)a.slot[g0 + v] * a.fs;
+            f0[at] = accv[v][q][0 + s] * g7 * r * r;
+            f0[a.fs + at] = accv[v][q][2 + s] * g7 * r;
+            f0[2 * a.fs + at] = accv[v][q][4 + s] * g7 * r;
+          }
+#pragma unroll
+          for (int sc = 0; sc < NSC; sc++)
+            a.f[(size_t)a.slot[g0 + NV + sc] * a.fs + at] = accs[sc][q][s] * g6;
+        }
+      }
+    }
+  }
+}
+
+static LegArgs leg_args(Ctx &c, int nvec, int nscal, const int *slots) {
+  LegArgs a;
+  a.L = c.L; a.nr = c.nr; a.nth = c.nth; a.nh = c.nh; a.jmax = c.jmax; a.NS = c.NS;
+  a.nvec = nvec; a.nscal = nscal; a.ncomp = 3 * nvec + nscal; a.cbase = 0;
+  for (int g = 0; g < MAXG; g++) a.slot[g] = 0;
+  a.moff = c.d_moff; a.poff = c.d_poff;
+  a.Plt = c.d_Plt; a.dPlt = c.d_dPlt; a.Ptl = c.d_Ptl; a.dPtl = c.d_dPtl;
+  a.asin_t = c.d_asin; a.wgt = c.d_wgt;
+  a.g3rlm = c.d_g3rlm; a.g6 = c.d_g6; a.g7 = c.d_g7; a.r = c.d_r; a.ar1 = c.d_ar1;
+  a.f = c.d_f; a.fs = c.fsize();
+  return a;
+}
+
+void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four) {
+  LegArgs a = leg_args(c, nvec, nscal, slots);
+  // launches of at most MAXG groups: vectors first, then scalars
+  int g = 0, comp = 0, ngrp = nvec + nscal;
+  while (g < ngrp) {
+    int nb = std::min(MAXG, ngrp - g);
+    LegArgs b = a;
+    b.nvec = std::max(0, std::min(nvec - g, nb));
+    b.nscal = nb - b.nvec;
+    b.cbase = comp;
+    for (int q = 0; q < nb; q++) b.slot[q] = slots[g + q];
+    dim3 grid(cdiv(c.nh, 32), cdiv(c.nr, BWD_KT), c.L + 1);
+    k_leg_bwd_f64<<<grid, 32 * nb, 0, c.stream>>>(b, four);
+    comp += 3 * b.nvec + b.nscal;
+    g += nb;
+  }
+}
+
+template <int NV, int NSC>
+static void launch_fwd(Ctx &c, LegArgs a, const double *four, int c0, const int *slots) {
+  for (int q = 0; q < NV + NSC; q++) a.slot[q] = slots[q];
+  int nthr = 32 * cdiv(std::min(c.L + 1, 256), 32);
+  size_t sm = (size_t)FWD_TC * FWD_KT * (3 * NV + NSC) * 2 * 2 * sizeof(double);
+  dim3 grid(1, cdiv(c.nr, FWD_KT), c.L + 1);
+  k_leg_fwd_f64<NV, NSC><<<grid, nthr, sm, c.stream>>>(a, four, c0, 0);
+}
+
+void leg_fwd_f64(Ctx &c, int nvec, int nscal, const double *four, const int *slots) {
+  LegArgs a = leg_args(c, nvec, nscal, slots);
+  int g = 0, comp = 0;
+  // vectors in batches of up to 4, scalars in batches of up to 4
+  while (g < nvec) {
+    int nb = std::min(4, nvec - g);
+    if (nb == 4) launch_fwd<4, 0>(c, a, four, comp, slots + g);
+    else if (nb == 3) launch_fwd<3, 0>(c, a, four, comp, slots + g);
+    else if (nb == 2) launch_fwd<2, 0>(c, a, four, comp, slots + g);
+    else launch_fwd<1, 0>(c, a, four, comp, slots + g);
+    g += nb;
+    comp += 3 * nb;
+  }
+  int s = 0;
+  while (s < nscal) {
+    int nb = std::min(4, nscal - s);
+    if (nb == 4) launch_fwd<0, 4>(c, a, four, comp, slots + g);
+    else if (nb == 3) launch_fwd<0, 3>(c, a, four, comp, slots + g);
+    else if (nb == 2) launch_fwd<0, 2>(c, a, four, comp, slots + g);
+    else launch_fwd<0, 1>(c, a, four, comp, slots + g);
+    g += nb;
+    s += nb;
+    comp += nb;
+  }
+}
+
+}  // namespace cb2

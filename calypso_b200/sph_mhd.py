@@ -1,0 +1,240 @@
+"""Host side of the B200 time-step hot path (ctypes over libcalypso_b200.so).
+
+The class names and methods mirror the reference's module procedures so a
+caller of the reference finds the same operations:
+
+=============================  ==============================================
+this module                    reference (src/Fortran_libraries/...)
+=============================  ==============================================
+``SphMHD(params)``             ``SPH_initialize_MHD`` set-up part
+                               (programs/SPH_MHD/SPH_analyzer_MHD.f90:21-110)
+``init_fields(kind, seed)``    ``sph_initial_data_control`` + ``set_sph_field_to_start``
+                               + first ``nonlinear``
+``SPH_analyze_MHD(n)``         ``SPH_analyze_MHD`` (SPH_analyzer_MHD.f90:115-202)
+``energies()``                 ``cal_rms_sph_outer_core`` -> sph_pwr_volume_s.dat row
+``sel_backward_legendre_trans``  the backward SHT (legendre_transform_select.f90:309,
+                               MHD_FFT_selector.F90:219) from spectra to grid
+``sel_forward_legendre_trans``   the forward SHT (legendre_transform_select.f90:375,
+                               MHD_FFT_selector.F90:185) from grid to spectra
+=============================  ==============================================
+
+Errors come back as :class:`CalypsoError` (the reference aborts through
+``calypso_MPI_abort``; the library never aborts the process).  There is no
+CPU fallback: without the CUDA library this module raises on import of the
+library, and every call runs on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcalypso_b200.so")
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+# d_rj slots of the evolved fields
+VELO, VORT, MAGNE, CURRENT, TEMP = 0, 3, 6, 9, 12
+
+
+class CalypsoError(RuntimeError):
+    pass
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("ltr", ctypes.c_int), ("nth", ctypes.c_int), ("nph", ctypes.c_int),
+        ("nr", ctypes.c_int), ("radial_grid_type", ctypes.c_int),
+        ("r_icb", ctypes.c_double), ("r_cmb", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("coef_imp_v", ctypes.c_double), ("coef_imp_t", ctypes.c_double),
+        ("coef_imp_b", ctypes.c_double),
+        ("coef_velo", ctypes.c_double), ("coef_d_velo", ctypes.c_double),
+        ("coef_buo", ctypes.c_double), ("coef_cor", ctypes.c_double),
+        ("coef_lor", ctypes.c_double),
+        ("coef_temp", ctypes.c_double), ("coef_d_temp", ctypes.c_double),
+        ("coef_magne", ctypes.c_double), ("coef_d_magne", ctypes.c_double),
+        ("coef_induct", ctypes.c_double),
+        ("use_ref_temp", ctypes.c_int),
+        ("depth_high_t", ctypes.c_double), ("depth_low_t", ctypes.c_double),
+        ("high_temp", ctypes.c_double), ("low_temp", ctypes.c_double),
+        ("temp_icb", ctypes.c_double), ("temp_cmb", ctypes.c_double),
+        ("nthreads", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+EXPORTS = [
+    "cb2_last_error", "cb2_create", "cb2_destroy", "cb2_init_fields", "cb2_start",
+    "cb2_step", "cb2_step_graph", "cb2_sync", "cb2_istep", "cb2_energies",
+    "cb2_get_field", "cb2_set_field", "cb2_get_field_device", "cb2_set_field_device",
+    "cb2_step_host_state", "cb2_sht_backward", "cb2_sht_forward", "cb2_get_gauss",
+    "cb2_get_plm", "cb2_stage_times",
+]
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libcalypso_b200.so and declare its C ABI; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise CalypsoError(
+            f"{path} is missing: build it with `python -m calypso_b200.build` "
+            "(there is no CPU fallback)")
+    L = ctypes.CDLL(path)
+    P, d, vp, i = ctypes.POINTER, ctypes.c_double, ctypes.c_void_p, ctypes.c_int
+    pd = P(d)
+    sig = {
+        "cb2_last_error": ([], ctypes.c_char_p),
+        "cb2_create": ([P(Params), i, i, P(vp)], i),
+        "cb2_destroy": ([vp], i),
+        "cb2_init_fields": ([vp, i, ctypes.c_uint], i),
+        "cb2_start": ([vp], i),
+        "cb2_step": ([vp, i], i),
+        "cb2_step_graph": ([vp, i], i),
+        "cb2_sync": ([vp], i),
+        "cb2_istep": ([vp], i),
+        "cb2_energies": ([vp, pd], i),
+        "cb2_get_field": ([vp, i, pd], i),
+        "cb2_set_field": ([vp, i, pd], i),
+        "cb2_get_field_device": ([vp, i, vp], i),
+        "cb2_set_field_device": ([vp, i, vp], i),
+        "cb2_step_host_state": ([vp, pd, pd], i),
+        "cb2_sht_backward": ([vp, i, i, pd, pd], i),
+        "cb2_sht_forward": ([vp, i, i, pd, pd], i),
+        "cb2_get_gauss": ([vp, pd, pd], i),
+        "cb2_get_plm": ([vp, i, i, pd, pd], i),
+        "cb2_stage_times": ([vp, pd], i),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _ptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise CalypsoError("arrays passed to the library must be C-contiguous float64")
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        msg = load_library().cb2_last_error().decode(errors="replace")
+        raise CalypsoError(f"{what} failed ({rc}): {msg}")
+
+
+class SphMHD:
+    """One spherical shell advanced on the GPU (device-resident state)."""
+
+    def __init__(self, params: dict, precision: int = PREC_FP64, device: int = -1):
+        lib = load_library()
+        p = Params()
+        for k, v in params.items():
+            setattr(p, k, v)
+        h = ctypes.c_void_p()
+        _check(lib.cb2_create(ctypes.byref(p), precision, device, ctypes.byref(h)), "cb2_create")
+        self._h = h
+        self.params = dict(params)
+        self.precision = precision
+        self.L, self.nr, self.nth, self.nph = p.ltr, p.nr, p.nth, p.nph
+        self.jmax = (self.L + 1) ** 2
+
+    # --- lifetime -----------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            load_library().cb2_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- time stepping ------------------------------------------------
+    def init_fields(self, kind: int = 1, seed: int = 0):
+        _check(load_library().cb2_init_fields(self._h, kind, seed), "cb2_init_fields")
+
+    def start(self):
+        _check(load_library().cb2_start(self._h), "cb2_start")
+
+    def SPH_analyze_MHD(self, nsteps: int = 1, graph: bool = False):
+        f = load_library().cb2_step_graph if graph else load_library().cb2_step
+        _check(f(self._h, nsteps), "cb2_step")
+
+    step = SPH_analyze_MHD
+
+    def sync(self):
+        _check(load_library().cb2_sync(self._h), "cb2_sync")
+
+    @property
+    def istep(self) -> int:
+        return load_library().cb2_istep(self._h)
+
+    def energies(self) -> np.ndarray:
+        out = np.zeros(7)
+        _check(load_library().cb2_energies(self._h, _ptr(out)), "cb2_energies")
+        return out
+
+    def stage_times(self) -> np.ndarray:
+        out = np.zeros(32)
+        _check(load_library().cb2_stage_times(self._h, _ptr(out)), "cb2_stage_times")
+        return out
+
+    # --- fields -------------------------------------------------------
+    def get_field(self, slot: int) -> np.ndarray:
+        out = np.zeros((self.nr, self.jmax))
+        _check(load_library().cb2_get_field(self._h, slot, _ptr(out)), "cb2_get_field")
+        return out
+
+    def set_field(self, slot: int, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(self.nr, self.jmax)
+        _check(load_library().cb2_set_field(self._h, slot, _ptr(a)), "cb2_set_field")
+
+    def step_host_state(self, state: np.ndarray, with_energies: bool = True):
+        """One step with the 20-field host-resident state (cb2_step_host_state)."""
+        ene = np.zeros(7)
+        _check(load_library().cb2_step_host_state(
+            self._h, _ptr(state), _ptr(ene) if with_energies else None), "cb2_step_host_state")
+        return ene
+
+    # --- transforms -----------------------------------------------------
+    def sel_backward_legendre_trans(self, nvec: int, nscal: int, spec: np.ndarray) -> np.ndarray:
+        nc = 3 * nvec + nscal
+        spec = np.ascontiguousarray(spec, dtype=np.float64).reshape(nc, self.nr, self.jmax)
+        grid = np.zeros((nc, self.nr, self.nth, self.nph))
+        _check(load_library().cb2_sht_backward(self._h, nvec, nscal, _ptr(spec), _ptr(grid)),
+               "cb2_sht_backward")
+        return grid
+
+    def sel_forward_legendre_trans(self, nvec: int, nscal: int, grid: np.ndarray) -> np.ndarray:
+        nc = 3 * nvec + nscal
+        grid = np.ascontiguousarray(grid, dtype=np.float64).reshape(nc, self.nr, self.nth, self.nph)
+        spec = np.zeros((nc, self.nr, self.jmax))
+        _check(load_library().cb2_sht_forward(self._h, nvec, nscal, _ptr(grid), _ptr(spec)),
+               "cb2_sht_forward")
+        return spec
+
+    def gauss(self):
+        c, w = np.zeros(self.nth), np.zeros(self.nth)
+        _check(load_library().cb2_get_gauss(self._h, _ptr(c), _ptr(w)), "cb2_get_gauss")
+        return c, w
+
+    def plm(self, l: int, m: int):
+        p, dp = np.zeros(self.nth), np.zeros(self.nth)
+        _check(load_library().cb2_get_plm(self._h, l, m, _ptr(p), _ptr(dp)), "cb2_get_plm")
+        return p, dp

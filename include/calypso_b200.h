@@ -1,0 +1,148 @@
+/*
+ * calypso_b200.h -- C ABI of the B200 (sm_100a) time-step hot path of the
+ * Calypso spherical-shell MHD dynamo code.
+ *
+ * The reference (hlokavarapu/calypso) is Fortran 90; its hot path is reached
+ * through module procedures with module-global state.  Each entry point
+ * below names the reference routine it replaces (paths relative to the
+ * reference's src/Fortran_libraries).  A Fortran host binds these with
+ * bind(C) interfaces (INTEGRATION.md shows the iso_c_binding module);
+ * the Python host (calypso_b200/) binds them with ctypes.
+ *
+ * Conventions
+ *   - every call returns 0 on success or a negative CB2_ERR_* code;
+ *     cb2_last_error() gives a message.  Nothing aborts the process.
+ *   - spectral (rj) arrays are float64 [nr][jmax] with j = l*(l+1)+m,
+ *     m < 0 holding the sin(|m| phi) part (the reference's d_rj(inod, field)
+ *     with inod = j + (k-1)*jmax when its j table is ordered by l*(l+1)+m).
+ *   - vector fields are three slots (poloidal S, dS/dr, toroidal T).
+ *   - grid arrays are float64 [comp][nr][nth][nph], theta index 0 nearest
+ *     the south pole (reference Gauss ordering), phi_p = 2 pi p / nph.
+ *   - host pointers are plain host memory; the library copies through its
+ *     own pinned staging buffers.  Calls on one context are not thread safe.
+ */
+#ifndef CALYPSO_B200_H
+#define CALYPSO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CB2_OK 0
+#define CB2_ERR_ARG -1        /* bad argument / unsupported configuration   */
+#define CB2_ERR_CUDA -2       /* a CUDA call failed (message has the name)  */
+#define CB2_ERR_SINGULAR -3   /* zero pivot in a radial LU factorisation    */
+#define CB2_ERR_NAN -4        /* NaN/Inf found in the energy diagnostics    */
+#define CB2_ERR_STATE -5      /* call out of order (e.g. step before start) */
+
+#define CB2_PREC_FP64 0       /* plain path: every stage in float64          */
+#define CB2_PREC_MIXED 1      /* Legendre split-fp16 tcgen05, fp32 FFT and
+                                 products, fp64 radial solves / diagnostics */
+
+/* Shell and equation parameters: the values the reference reads from
+ * control_sph_shell (num_grid_sph) and control_MHD (model, control) and
+ * turns into coefficients in F/MHD_src/sph_MHD/material_property.f90. */
+typedef struct cb2_params {
+  int ltr;              /* truncation_level_ctl                          */
+  int nth;              /* ngrid_meridonal_ctl                           */
+  int nph;              /* ngrid_zonal_ctl                               */
+  int nr;               /* radial points = num_fluid_grid_ctl + 1        */
+  int radial_grid_type; /* 0 equidistance, 1 Chebyshev                   */
+  double r_icb, r_cmb;
+  double dt;
+  double coef_imp_v, coef_imp_t, coef_imp_b;
+  double coef_velo, coef_d_velo, coef_buo, coef_cor, coef_lor;
+  double coef_temp, coef_d_temp;
+  double coef_magne, coef_d_magne, coef_induct;
+  int use_ref_temp;     /* ref_temp_ctl spherical_shell                  */
+  double depth_high_t, depth_low_t, high_temp, low_temp;
+  double temp_icb, temp_cmb;   /* fixed total temperature at the walls   */
+  int nthreads;         /* unused by the GPU library (layout compatible) */
+} cb2_params;
+
+typedef struct cb2_ctx cb2_ctx;
+
+const char *cb2_last_error(void);
+
+/* SPH_initialize_MHD set-up part (programs/SPH_MHD/SPH_analyzer_MHD.f90:21-110):
+ * radial grid and FDM weights (set_radius_func.f90), boundary weights
+ * (MHD_src/sph_MHD/set_bc_sph_mhd.f90), Gauss nodes and Schmidt P_l^m on the
+ * GPU (PARALLEL_src/SPH_SHELL_src/init_sph_trans.f90:64-92), Coriolis
+ * couplings (MHD_src/sph_MHD/const_coriolis_sph_rlm.f90:34-67) and the
+ * banded LU factors of the implicit operators on the GPU
+ * (MHD_src/sph_MHD/const_radial_mat_4_sph.f90:33-114).  device < 0 keeps
+ * the current device. */
+int cb2_create(const cb2_params *p, int precision, int device, cb2_ctx **out);
+/* sel_finalize_legendre_trans + deallocation of the module globals */
+int cb2_destroy(cb2_ctx *ctx);
+
+/* Initial state on the device: kind 1 = dynamo benchmark case 1
+ * (MHD_src/sph_MHD/set_initial_sph_dynamo.f90 sph_initial_data_control with
+ * rst_ctl dynamo_benchmark_1); kind 2 = seeded thermal perturbation on
+ * random l <= 8 modes plus a weak dipole-dominated seed field.  Ends with
+ * cb2_start(). */
+int cb2_init_fields(cb2_ctx *ctx, int kind, unsigned seed);
+/* set_sph_field_to_start + first nonlinear (SPH_analyzer_MHD.f90:92-101):
+ * recompute gradients, vorticity, current, diffusion terms and the
+ * nonlinear terms of the state loaded with cb2_set_field. */
+int cb2_start(cb2_ctx *ctx);
+/* SPH_analyze_MHD (SPH_analyzer_MHD.f90:115-202) repeated nsteps times on
+ * the context's stream (asynchronous): Euler first step, Adams-Bashforth 2
+ * after, Crank-Nicolson radial solves, nonlinear terms through the SHT. */
+int cb2_step(cb2_ctx *ctx, int nsteps);
+/* the same nsteps, captured once as a CUDA graph and replayed */
+int cb2_step_graph(cb2_ctx *ctx, int nsteps);
+int cb2_sync(cb2_ctx *ctx);
+int cb2_istep(const cb2_ctx *ctx);
+/* volume mean squares of sph_pwr_volume_s.dat after the last step
+ * (PARALLEL_src/SPH_SHELL_src/cal_rms_fields_by_sph.f90 cal_rms_sph_outer_core):
+ * out = K_pol, K_tor, K, <T^2> (total temperature), M_pol, M_tor, M.
+ * Synchronises.  Returns CB2_ERR_NAN if any value is not finite
+ * (MHD_src/sph_MHD/cal_sol_sph_fluid_crank.f90 check_NaN_temperature). */
+int cb2_energies(cb2_ctx *ctx, double out[7]);
+
+/* d_rj field slot access (host buffers of nr*jmax float64).  Slot numbers:
+ * 0 velocity, 3 vorticity, 6 magnetic field, 9 current density,
+ * 12 (perturbation) temperature; other slots are work fields. */
+int cb2_get_field(cb2_ctx *ctx, int slot, double *host);
+int cb2_set_field(cb2_ctx *ctx, int slot, const double *host);
+/* the same with device buffers on the context's device (no copy to host) */
+int cb2_get_field_device(cb2_ctx *ctx, int slot, double *dev);
+int cb2_set_field_device(cb2_ctx *ctx, int slot, const double *dev);
+
+/* Drop-in for a host that keeps d_rj in its own memory (the reference's
+ * Fortran host): copies in the 20 fields one step reads, advances one
+ * Adams-Bashforth step (call cb2_step for the first, Euler step) and copies
+ * the same 20 fields back.  state = 20 x nr*jmax float64 in this order:
+ * vorticity S,T; vorticity diffusion S,T; curl of forces S,T; its previous
+ * value S,T; magnetic field S,T; magnetic diffusion S,T; induction S,T; its
+ * previous value S,T; temperature; thermal diffusion; heat advection; its
+ * previous value (negated).  out_energies may be NULL. */
+int cb2_step_host_state(cb2_ctx *ctx, double *state, double out_energies[7]);
+
+/* Spherical transform of nvec vectors + nscal scalars at every radius
+ * (PARALLEL_src/SPH_SHELL_src/legendre_transform_select.f90:309-439
+ *  sel_backward_legendre_trans / sel_forward_legendre_trans, plus
+ *  MHD_src/sph_MHD/MHD_FFT_selector.F90:185-249 back/fwd_MHD_FFT_sel_from_recv).
+ * spec: (3*nvec+nscal) x nr x jmax float64; grid: (3*nvec+nscal) x nr x nth x
+ * nph float64, vector components (r, theta, phi).  Host buffers.  The
+ * context's precision selects the Legendre / FFT arithmetic. */
+int cb2_sht_backward(cb2_ctx *ctx, int nvec, int nscal, const double *spec, double *grid);
+int cb2_sht_forward(cb2_ctx *ctx, int nvec, int nscal, const double *grid, double *spec);
+
+/* Tables computed on the device, for checking: Gauss colatitudes/weights
+ * (nth), Schmidt P_l^m and dP/dtheta at the nth nodes for one (l, m>=0). */
+int cb2_get_gauss(cb2_ctx *ctx, double *colat, double *weight);
+int cb2_get_plm(cb2_ctx *ctx, int l, int m, double *p, double *dp);
+
+/* CUDA-event time of the last cb2_step/cb2_step_graph call, per stage
+ * (stage ids follow the reference's elapsed-time labels of
+ * MHD_src/IO/init_sph_MHD_elapsed_label.f90: 6 explicit, 7 implicit,
+ * 22 Legendre backward, 23 Legendre forward, 24 FFT+products, 13 Coriolis,
+ * 17 rj operators).  ms[0..31]; only filled when CB2_TIMERS=1 in the env. */
+int cb2_stage_times(cb2_ctx *ctx, double ms[32]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
