@@ -373,6 +373,25 @@ int cb2_step_graph(cb2_ctx *c, int nsteps) {
   return 0;
 }
 
+int cb2_time_steps(cb2_ctx *c, int nsteps, int use_graph, double *ms) {
+  if (!c || !ms) return CB2_ERR_ARG;
+  if (!c->started) { set_error("cb2_time_steps before cb2_start"); return CB2_ERR_STATE; }
+  cudaEvent_t e0, e1;
+  CB2_CUDA(cudaEventCreate(&e0));
+  CB2_CUDA(cudaEventCreate(&e1));
+  CB2_CUDA(cudaStreamSynchronize(c->stream));
+  CB2_CUDA(cudaEventRecord(e0, c->stream));
+  int rc = use_graph ? cb2_step_graph(c, nsteps) : cb2_step(c, nsteps);
+  CB2_CUDA(cudaEventRecord(e1, c->stream));
+  CB2_CUDA(cudaEventSynchronize(e1));
+  float t = 0.0f;
+  CB2_CUDA(cudaEventElapsedTime(&t, e0, e1));
+  *ms = t;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
 int cb2_sync(cb2_ctx *c) {
   if (!c) return CB2_ERR_ARG;
   CB2_CUDA(cudaStreamSynchronize(c->stream));
@@ -437,11 +456,18 @@ int cb2_step_host_state(cb2_ctx *c, double *state, double out_energies[7]) {
   if (!c || !state) return CB2_ERR_ARG;
   if (!c->started) { set_error("cb2_step_host_state before cb2_start"); return CB2_ERR_STATE; }
   size_t n = c->fsize(), bytes = 20 * n * sizeof(double);
-  int rc = host_stage(*c, bytes);
-  if (rc) return rc;
   if (!c->d_host_state) CB2_CUDA(cudaMalloc(&c->d_host_state, bytes));
-  memcpy(c->h_stage, state, bytes);
-  CB2_CUDA(cudaMemcpyAsync(c->d_host_state, c->h_stage, bytes, cudaMemcpyHostToDevice, c->stream));
+  // pinned caller buffers are copied directly, pageable ones through staging
+  cudaPointerAttributes pa;
+  bool pinned = cudaPointerGetAttributes(&pa, state) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  if (!pinned) {
+    int rc = host_stage(*c, bytes);
+    if (rc) return rc;
+  }
+  double *src = pinned ? state : c->h_stage;
+  if (!pinned) memcpy(c->h_stage, state, bytes);
+  CB2_CUDA(cudaMemcpyAsync(c->d_host_state, src, bytes, cudaMemcpyHostToDevice, c->stream));
   for (int q = 0; q < 20; q++)
     k_to_device_order<<<cdiv(n, 256), 256, 0, c->stream>>>(c->nr, c->jmax, c->d_perm,
                                                              c->d_host_state + q * n, c->fld(kHostStateSlots[q]));
@@ -450,9 +476,9 @@ int cb2_step_host_state(cb2_ctx *c, double *state, double out_energies[7]) {
   for (int q = 0; q < 20; q++)
     k_to_host_order<<<cdiv(n, 256), 256, 0, c->stream>>>(c->nr, c->jmax, c->d_perm,
                                                          c->fld(kHostStateSlots[q]), c->d_host_state + q * n);
-  CB2_CUDA(cudaMemcpyAsync(c->h_stage, c->d_host_state, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CB2_CUDA(cudaMemcpyAsync(src, c->d_host_state, bytes, cudaMemcpyDeviceToHost, c->stream));
   CB2_CUDA(cudaStreamSynchronize(c->stream));
-  memcpy(state, c->h_stage, bytes);
+  if (!pinned) memcpy(state, c->h_stage, bytes);
   if (out_energies) return cb2_energies(c, out_energies);
   return 0;
 }
@@ -539,6 +565,17 @@ int cb2_get_plm(cb2_ctx *c, int l, int m, double *p, double *dp) {
     p[c->nth - 1 - i] = sg * a[i];
     dp[c->nth - 1 - i] = -sg * b[i];
   }
+  return 0;
+}
+
+int cb2_alloc_pinned(size_t bytes, void **out) {
+  if (!out) return CB2_ERR_ARG;
+  CB2_CUDA(cudaMallocHost(out, bytes));
+  return 0;
+}
+
+int cb2_free_pinned(void *p) {
+  if (p) CB2_CUDA(cudaFreeHost(p));
   return 0;
 }
 

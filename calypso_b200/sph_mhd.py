@@ -73,7 +73,7 @@ EXPORTS = [
     "cb2_step", "cb2_step_graph", "cb2_sync", "cb2_istep", "cb2_energies",
     "cb2_get_field", "cb2_set_field", "cb2_get_field_device", "cb2_set_field_device",
     "cb2_step_host_state", "cb2_sht_backward", "cb2_sht_forward", "cb2_get_gauss",
-    "cb2_get_plm", "cb2_stage_times",
+    "cb2_get_plm", "cb2_stage_times", "cb2_time_steps", "cb2_alloc_pinned", "cb2_free_pinned",
 ]
 
 
@@ -110,6 +110,9 @@ def load_library(path: str = LIB_PATH):
         "cb2_get_gauss": ([vp, pd, pd], i),
         "cb2_get_plm": ([vp, i, i, pd, pd], i),
         "cb2_stage_times": ([vp, pd], i),
+        "cb2_time_steps": ([vp, i, i, pd], i),
+        "cb2_alloc_pinned": ([ctypes.c_size_t, P(vp)], i),
+        "cb2_free_pinned": ([vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -178,6 +181,13 @@ class SphMHD:
 
     step = SPH_analyze_MHD
 
+    def time_steps(self, nsteps: int, graph: bool = True) -> float:
+        """Device time (ms) of nsteps, CUDA events on the library's stream."""
+        ms = ctypes.c_double()
+        _check(load_library().cb2_time_steps(self._h, nsteps, 1 if graph else 0, ctypes.byref(ms)),
+               "cb2_time_steps")
+        return ms.value
+
     def sync(self):
         _check(load_library().cb2_sync(self._h), "cb2_sync")
 
@@ -238,3 +248,22 @@ class SphMHD:
         p, dp = np.zeros(self.nth), np.zeros(self.nth)
         _check(load_library().cb2_get_plm(self._h, l, m, _ptr(p), _ptr(dp)), "cb2_get_plm")
         return p, dp
+
+
+class PinnedArray:
+    """Page-locked float64 array from cb2_alloc_pinned (freed with the object)."""
+
+    def __init__(self, shape):
+        n = int(np.prod(shape))
+        p = ctypes.c_void_p()
+        _check(load_library().cb2_alloc_pinned(n * 8, ctypes.byref(p)), "cb2_alloc_pinned")
+        self._p = p
+        buf = (ctypes.c_double * n).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=np.float64).reshape(shape)
+
+    def __del__(self):
+        try:
+            if self._p.value:
+                load_library().cb2_free_pinned(self._p)
+        except Exception:
+            pass

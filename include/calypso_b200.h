@@ -24,6 +24,8 @@
 #ifndef CALYPSO_B200_H
 #define CALYPSO_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -93,6 +95,9 @@ int cb2_step(cb2_ctx *ctx, int nsteps);
 /* the same nsteps, captured once as a CUDA graph and replayed */
 int cb2_step_graph(cb2_ctx *ctx, int nsteps);
 int cb2_sync(cb2_ctx *ctx);
+/* nsteps of cb2_step (use_graph = 0) or cb2_step_graph (1) bracketed by CUDA
+ * events on the context's stream; ms = device time.  Synchronises. */
+int cb2_time_steps(cb2_ctx *ctx, int nsteps, int use_graph, double *ms);
 int cb2_istep(const cb2_ctx *ctx);
 /* volume mean squares of sph_pwr_volume_s.dat after the last step
  * (PARALLEL_src/SPH_SHELL_src/cal_rms_fields_by_sph.f90 cal_rms_sph_outer_core):
@@ -134,6 +139,11 @@ int cb2_sht_forward(cb2_ctx *ctx, int nvec, int nscal, const double *grid, doubl
  * (nth), Schmidt P_l^m and dP/dtheta at the nth nodes for one (l, m>=0). */
 int cb2_get_gauss(cb2_ctx *ctx, double *colat, double *weight);
 int cb2_get_plm(cb2_ctx *ctx, int l, int m, double *p, double *dp);
+
+/* pinned host memory for cb2_step_host_state callers without an allocator
+ * of their own (the library copies pinned buffers without staging) */
+int cb2_alloc_pinned(size_t bytes, void **out);
+int cb2_free_pinned(void *p);
 
 /* CUDA-event time of the last cb2_step/cb2_step_graph call, per stage
  * (stage ids follow the reference's elapsed-time labels of

@@ -96,7 +96,7 @@ def test_case1_fields_match_oracle(oracle_lib, case1):
     o = oracle_lib.Oracle(case1)
     g.init_fields(1)
     o.init_fields(1)
-    _compare_fields(g, o, 1e-12)
+    _compare_fields(g, o, 1e-10)
     g.step(20)
     o.step(20)
     _compare_fields(g, o, 1e-10)
@@ -109,7 +109,7 @@ def test_small_shell_seeded_matches_oracle(oracle_lib):
     o = oracle_lib.Oracle(p)
     g.init_fields(2, seed=3)
     o.init_fields(2, 3)
-    _compare_fields(g, o, 1e-12)
+    _compare_fields(g, o, 1e-10)
     g.step(400)
     o.step(400)
     _compare_fields(g, o, 1e-10)
