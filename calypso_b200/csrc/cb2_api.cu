@@ -180,6 +180,17 @@ static void accumulate_timers(Ctx &c) {
   c.stage_ms[0] += el(0, 3);
 }
 
+int check_status(Ctx &c) {
+  int st = 0;
+  CB2_CUDA(cudaMemcpyAsync(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  CB2_CUDA(cudaStreamSynchronize(c.stream));
+  if (st & CB2_STATUS_PIPE_TIMEOUT) {
+    set_error("a tensor-core Legendre pipeline wait ran out of time; the state is void");
+    return CB2_ERR_TIMEOUT;
+  }
+  return 0;
+}
+
 static int host_stage(Ctx &c, size_t bytes) {
   if (c.h_stage_bytes >= bytes) return 0;
   if (c.h_stage) cudaFreeHost(c.h_stage);
@@ -389,20 +400,21 @@ int cb2_time_steps(cb2_ctx *c, int nsteps, int use_graph, double *ms) {
   *ms = t;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  return rc;
+  return rc ? rc : check_status(*c);
 }
 
 int cb2_sync(cb2_ctx *c) {
   if (!c) return CB2_ERR_ARG;
   CB2_CUDA(cudaStreamSynchronize(c->stream));
-  return 0;
+  return check_status(*c);
 }
 
 int cb2_istep(const cb2_ctx *c) { return c ? c->istep : -1; }
 
 int cb2_energies(cb2_ctx *c, double out[7]) {
   if (!c || !out) return CB2_ERR_ARG;
-  return rj_energies(*c, out);
+  int rc = check_status(*c);
+  return rc ? rc : rj_energies(*c, out);
 }
 
 int cb2_get_field_device(cb2_ctx *c, int slot, double *dev) {
@@ -488,6 +500,10 @@ static int sht_common(cb2_ctx *c, int nvec, int nscal) {
     set_error("sht: need 1..13 components");
     return CB2_ERR_ARG;
   }
+  if (c->prec == CB2_PREC_MIXED && nvec + nscal > 8) {
+    set_error("sht: the mixed precision path takes at most 8 vectors + scalars");
+    return CB2_ERR_ARG;
+  }
   return 0;
 }
 
@@ -515,7 +531,7 @@ int cb2_sht_backward(cb2_ctx *c, int nvec, int nscal, const double *spec, double
   CB2_CUDA(cudaMemcpyAsync(grid, dgrid, gsz * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CB2_CUDA(cudaStreamSynchronize(c->stream));
   cudaFree(dgrid);
-  return 0;
+  return check_status(*c);
 }
 
 int cb2_sht_forward(cb2_ctx *c, int nvec, int nscal, const double *grid, double *spec) {
@@ -539,6 +555,7 @@ int cb2_sht_forward(cb2_ctx *c, int nvec, int nscal, const double *grid, double 
   CB2_CUDA(cudaGetLastError());
   CB2_CUDA(cudaStreamSynchronize(c->stream));
   cudaFree(dgrid);
+  if ((rc = check_status(*c))) return rc;
   for (int q = 0; q < nc; q++)
     if ((rc = cb2_get_field(c, MADV + q, spec + q * n))) return rc;
   return 0;

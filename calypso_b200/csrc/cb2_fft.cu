@@ -139,55 +139,137 @@ struct ProdCoef {
   double cv, cl, ci, ct;
 };
 
+// Stockham stages over nf independent FFTs held in x[f*N + n]; all FFTs of
+// the row advance together so each stage costs one barrier
+template <typename T, typename T2>
+__device__ T2 *batch_fft(T2 *x, T2 *y, int nf, const FFTPlan &pl, const T2 *__restrict__ tw, int sign) {
+  const int N = pl.n;
+  int Ns = 1;
+  const T s32 = (T)(0.5 * sqrt(3.0));
+  for (int st = 0; st < pl.nst; st++) {
+    const int R = pl.rad[st];
+    const int nb = N / R, tstride = N / (Ns * R);
+    for (int idx = threadIdx.x; idx < nf * nb; idx += blockDim.x) {
+      int f = idx / nb, j = idx - f * nb;
+      int k = j % Ns;
+      const T2 *xf = x + f * N;
+      T2 v[4];
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        if (r < R) {
+          T2 a = xf[j + r * nb];
+          if (r > 0 && k > 0) {
+            T2 w = tw[r * k * tstride];
+            if (sign > 0) w.y = -w.y;
+            a = cmul(a, w);
+          }
+          v[r] = a;
+        }
+      }
+      T2 o[4];
+      if (R == 4) {
+        T2 a0, a1, a2, a3;
+        a0.x = v[0].x + v[2].x; a0.y = v[0].y + v[2].y;
+        a1.x = v[0].x - v[2].x; a1.y = v[0].y - v[2].y;
+        a2.x = v[1].x + v[3].x; a2.y = v[1].y + v[3].y;
+        T dx = v[1].x - v[3].x, dy = v[1].y - v[3].y;
+        if (sign < 0) { a3.x = dy; a3.y = -dx; } else { a3.x = -dy; a3.y = dx; }
+        o[0].x = a0.x + a2.x; o[0].y = a0.y + a2.y;
+        o[1].x = a1.x + a3.x; o[1].y = a1.y + a3.y;
+        o[2].x = a0.x - a2.x; o[2].y = a0.y - a2.y;
+        o[3].x = a1.x - a3.x; o[3].y = a1.y - a3.y;
+      } else if (R == 2) {
+        o[0].x = v[0].x + v[1].x; o[0].y = v[0].y + v[1].y;
+        o[1].x = v[0].x - v[1].x; o[1].y = v[0].y - v[1].y;
+      } else {
+        T2 t1, t2, t3;
+        t1.x = v[1].x + v[2].x; t1.y = v[1].y + v[2].y;
+        t2.x = v[0].x - (T)0.5 * t1.x; t2.y = v[0].y - (T)0.5 * t1.y;
+        T dx = v[1].x - v[2].x, dy = v[1].y - v[2].y;
+        if (sign < 0) { t3.x = s32 * dy; t3.y = -s32 * dx; } else { t3.x = -s32 * dy; t3.y = s32 * dx; }
+        o[0].x = v[0].x + t1.x; o[0].y = v[0].y + t1.y;
+        o[1].x = t2.x + t3.x; o[1].y = t2.y + t3.y;
+        o[2].x = t2.x - t3.x; o[2].y = t2.y - t3.y;
+      }
+      T2 *yf = y + f * N;
+      int d = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+        if (r < R) yf[d + r * Ns] = o[r];
+    }
+    __syncthreads();
+    T2 *t = x; x = y; y = t;
+    Ns *= R;
+  }
+  return x;
+}
+
+// one block per (theta, r) row: 13 components -> grid -> 12 products -> spectra
 template <typename T>
-__global__ void __launch_bounds__(256)
-k_fft_products(FFTPlan pl, int L, int NS, const T *four, T *four2, const typename C2<T>::t *tw,
-               ProdCoef pc) {
+__global__ void __launch_bounds__(512)
+k_fft_products(FFTPlan pl, int L, int NS, const T *__restrict__ four, T *__restrict__ four2,
+               const typename C2<T>::t *__restrict__ tw, ProdCoef pc) {
   using T2 = typename C2<T>::t;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int N = pl.n;
-  T2 *Z0 = reinterpret_cast<T2 *>(smraw);
-  T2 *Z1 = Z0 + N;
-  T *g = reinterpret_cast<T *>(Z1 + N);   // [13][N]
+  T2 *A = reinterpret_cast<T2 *>(smraw);    // 7 x N
+  T2 *B = A + 7 * N;                         // 7 x N
   const size_t row = blockIdx.x;
   const T *fin = four + row * 13 * NS;
   T *fout = four2 + row * 12 * NS;
-  for (int c = 0; c < 13; c += 2) {
-    load_pair<T, T2>(Z0, N, L, fin + (size_t)c * NS, (c + 1 < 13) ? fin + (size_t)(c + 1) * NS : nullptr);
-    T2 *z = block_fft<T, T2>(Z0, Z1, pl, tw, +1);
-    for (int q = threadIdx.x; q < N; q += blockDim.x) {
-      g[c * N + q] = z[q].x;
-      if (c + 1 < 13) g[(c + 1) * N + q] = z[q].y;
+  const int mmax = min(L, (N + 1) / 2 - 1);
+  // Hermitian spectra of the 7 pairs (z = x + i y)
+  for (int idx = threadIdx.x; idx < 7 * N; idx += blockDim.x) {
+    int p = idx / N, n = idx - p * N;
+    const T *f0 = fin + (size_t)(2 * p) * NS;
+    const T *f1 = (2 * p + 1 < 13) ? fin + (size_t)(2 * p + 1) * NS : nullptr;
+    T2 z = T2{0, 0};
+    if (n == 0) {
+      z = T2{f0[0], f1 ? f1[0] : (T)0};
+    } else {
+      int m = (n <= mmax) ? n : ((N - n <= mmax) ? N - n : -1);
+      if (m > 0) {
+        T a0 = f0[2 * m], b0 = f0[2 * m + 1];
+        T a1 = f1 ? f1[2 * m] : (T)0, b1 = f1 ? f1[2 * m + 1] : (T)0;
+        T xr = (T)0.5 * a0, xi = (T)-0.5 * b0, yr = (T)0.5 * a1, yi = (T)-0.5 * b1;
+        z = (m == n) ? T2{xr - yi, xi + yr} : T2{xr + yi, -xi + yr};
+      }
     }
-    __syncthreads();
-  }
-  const T cv = (T)pc.cv, cl = (T)pc.cl, ci = (T)pc.ci, ct = (T)pc.ct;
-  for (int q = threadIdx.x; q < N; q += blockDim.x) {
-    T ur = g[0 * N + q], ut = g[1 * N + q], up = g[2 * N + q];
-    T wr = g[3 * N + q], wt = g[4 * N + q], wp = g[5 * N + q];
-    T br = g[6 * N + q], bt = g[7 * N + q], bp = g[8 * N + q];
-    T jr = g[9 * N + q], jt = g[10 * N + q], jp = g[11 * N + q];
-    T tt = g[12 * N + q];
-    g[0 * N + q] = (wt * up - wp * ut) * cv;
-    g[1 * N + q] = (wp * ur - wr * up) * cv;
-    g[2 * N + q] = (wr * ut - wt * ur) * cv;
-    g[3 * N + q] = (jt * bp - jp * bt) * cl;
-    g[4 * N + q] = (jp * br - jr * bp) * cl;
-    g[5 * N + q] = (jr * bt - jt * br) * cl;
-    g[6 * N + q] = (ut * bp - up * bt) * ci;
-    g[7 * N + q] = (up * br - ur * bp) * ci;
-    g[8 * N + q] = (ur * bt - ut * br) * ci;
-    g[9 * N + q] = ur * tt * ct;
-    g[10 * N + q] = ut * tt * ct;
-    g[11 * N + q] = up * tt * ct;
+    A[idx] = z;
   }
   __syncthreads();
-  for (int c = 0; c < 12; c += 2) {
-    for (int q = threadIdx.x; q < N; q += blockDim.x) Z0[q] = T2{g[c * N + q], g[(c + 1) * N + q]};
-    __syncthreads();
-    T2 *z = block_fft<T, T2>(Z0, Z1, pl, tw, -1);
-    store_pair<T, T2>(z, N, L, fout + (size_t)c * NS, fout + (size_t)(c + 1) * NS);
-    __syncthreads();
+  T2 *g = batch_fft<T, T2>(A, B, 7, pl, tw, +1);
+  T2 *h = (g == A) ? B : A;
+  const T cv = (T)pc.cv, cl = (T)pc.cl, ci = (T)pc.ci, ct = (T)pc.ct;
+  for (int q = threadIdx.x; q < N; q += blockDim.x) {
+    T2 p0 = g[0 * N + q], p1 = g[1 * N + q], p2 = g[2 * N + q], p3 = g[3 * N + q];
+    T2 p4 = g[4 * N + q], p5 = g[5 * N + q], p6 = g[6 * N + q];
+    T ur = p0.x, ut = p0.y, up = p1.x, wr = p1.y, wt = p2.x, wp = p2.y;
+    T br = p3.x, bt = p3.y, bp = p4.x, jr = p4.y, jt = p5.x, jp = p5.y, tt = p6.x;
+    h[0 * N + q] = T2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv};
+    h[1 * N + q] = T2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl};
+    h[2 * N + q] = T2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl};
+    h[3 * N + q] = T2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci};
+    h[4 * N + q] = T2{(ur * bt - ut * br) * ci, ur * tt * ct};
+    h[5 * N + q] = T2{ut * tt * ct, up * tt * ct};
+  }
+  __syncthreads();
+  T2 *zf = batch_fft<T, T2>(h, g, 6, pl, tw, -1);
+  const T an = (T)(1.0 / (double)N);
+  for (int idx = threadIdx.x; idx < 6 * (L + 1); idx += blockDim.x) {
+    int p = idx / (L + 1), m = idx - p * (L + 1);
+    T *f0 = fout + (size_t)(2 * p) * NS, *f1 = fout + (size_t)(2 * p + 1) * NS;
+    const T2 *Z = zf + p * N;
+    if (m == 0) {
+      f0[0] = an * Z[0].x; f0[1] = 0;
+      f1[0] = an * Z[0].y; f1[1] = 0;
+    } else {
+      T2 zk = Z[m % N], zn = Z[(N - m) % N];
+      T xr = (T)0.5 * (zk.x + zn.x), xi = (T)0.5 * (zk.y - zn.y);
+      T yr = (T)0.5 * (zk.y + zn.y), yi = (T)-0.5 * (zk.x - zn.x);
+      f0[2 * m] = (T)2 * an * xr; f0[2 * m + 1] = (T)-2 * an * xi;
+      f1[2 * m] = (T)2 * an * yr; f1[2 * m + 1] = (T)-2 * an * yi;
+    }
   }
 }
 
@@ -269,7 +351,11 @@ int fft_setup(Ctx &c) {
   k_twiddles<<<cdiv(c.nph, 256), 256, 0, c.stream>>>(c.nph, (double2 *)c.d_tw_fft,
                                                      (float2 *)c.d_tw_fft32);
   CB2_CUDA(cudaGetLastError());
-  size_t big = 2 * (size_t)c.nph * sizeof(double2) + 13 * (size_t)c.nph * sizeof(double);
+  size_t big = 14 * (size_t)c.nph * sizeof(double2);
+  if (big > 227 * 1024) {
+    set_error("ngrid_zonal_ctl too large for the fused FFT kernel");
+    return CB2_ERR_ARG;
+  }
   CB2_CUDA(cudaFuncSetAttribute(k_fft_products<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
   CB2_CUDA(cudaFuncSetAttribute(k_fft_products<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
   return 0;
@@ -285,9 +371,9 @@ template <typename T>
 void fft_products(Ctx &c, const T *four, T *four2) {
   using T2 = typename C2<T>::t;
   FFTPlan p = make_plan(c.nph);
-  size_t sm = 2 * (size_t)c.nph * sizeof(T2) + 13 * (size_t)c.nph * sizeof(T);
+  size_t sm = 14 * (size_t)c.nph * sizeof(T2);
   ProdCoef pc{c.p.coef_velo, c.p.coef_lor, c.p.coef_induct, c.p.coef_temp};
-  k_fft_products<T><<<(unsigned)(c.nth * c.nr), 256, sm, c.stream>>>(p, c.L, c.NS, four, four2,
+  k_fft_products<T><<<(unsigned)(c.nth * c.nr), 512, sm, c.stream>>>(p, c.L, c.NS, four, four2,
                                                                      twid<T>(c), pc);
 }
 

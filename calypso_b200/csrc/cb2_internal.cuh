@@ -145,6 +145,12 @@ void mixed_free(Ctx &c);
 void leg_bwd_mixed(Ctx &c, int nvec, int nscal, const int *slots, float *four);
 void leg_fwd_mixed(Ctx &c, int nvec, int nscal, const float *four, const int *slots);
 
+// bits of the device status word d_status
+constexpr int CB2_STATUS_SINGULAR = 1;        // zero pivot in an LU factorisation
+constexpr int CB2_STATUS_PIPE_TIMEOUT = 2;    // a tensor-core pipeline wait ran out
+// reads d_status (synchronises the stream); CB2_ERR_TIMEOUT after a pipeline timeout
+int check_status(Ctx &c);
+
 constexpr int kThreads = 256;
 inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
 

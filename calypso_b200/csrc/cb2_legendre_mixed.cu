@@ -1,16 +1,843 @@
-// cb2_legendre_mixed.cu -- mixed-precision Legendre transforms (placeholder
-// until the tcgen05 kernels land: the mixed context refuses to be created).
+// cb2_legendre_mixed.cu -- Legendre transforms on the tcgen05 tensor cores.
+//
+// Arithmetic: every operand x is scaled by a power of two s (per GEMM row or
+// column, so the largest |x s| lies in [2^13, 2^14)) and split into two
+// float16 halves
+//     x s = hi + lo,  hi = fp16(x s),  lo = fp16(x s - hi),
+// and a product is accumulated in float32 as hi*hi' + hi*lo' + lo*hi'
+// (three tcgen05.mma kind::f16 into one TMEM accumulator), unscaled in the
+// epilogue.  Scaling to 2^14 rather than 1 keeps lo a normal fp16 number for
+// every value within 2^17 of the row (column) maximum, so those values carry
+// 22 significant bits; smaller ones keep an absolute error of ~2^-38 of the
+// maximum.  The float32 accumulator adds ~2^-24 of the running sum per term.
+//
+// Mathematics: the per-order contractions of legendre_bwd_trans_org.f90 /
+// legendre_fwd_trans_org.f90 of the reference (the float64 version is
+// cb2_legendre_f64.cu), written as GEMMs per order m with the equatorial
+// symmetry P_l^m(pi - t) = (-1)^(l-m) P_l^m(t):
+//
+// backward, D[row][theta] = sum_K A[row][K] B[K][theta] over the nh south
+//   nodes; two TMEM accumulators, one per reflection parity of the basis
+//   function, give the south (acc0 + acc1) and north (acc0 - acc1) nodes.
+//   gemm P   rows (k, group, +-m): A = S l(l+1)/r^2 (vectors) or the scalar,
+//            B = P_l^m; K runs over the degrees of one parity of l-m.
+//   gemm DM  rows (k, vector, {theta +m, theta -m, phi +m, phi -m}):
+//            K = [dP part | mP part], B = [dP_l^m/dtheta ; m P_l^m/sin theta]
+//            grouped as {dP of odd l-m, mP of even l-m} (parity 0) and the
+//            converse (parity 1); A = dP part {D+, D-, -T+, -T-}, mP part
+//            {T-, -T+, D-, -D+} with D = (dS/dr)/r, T = T/r.
+// forward, D[row][l] = sum_theta A[row][theta] B[theta][l] with the Gauss
+//   weights and the north/south fold in A (sym = f(i)w_i + f(i')w_i',
+//   anti = f(i)w_i - f(i')w_i'); one accumulator per parity of l-m.
+//   gemm P   rows (k, group, +-m): A = sym/anti of the r component (vectors)
+//            or the scalar, B = P_l^m.
+//   gemm DM  rows (k, vector, {dS +m, dS -m, T +m, T -m}), K = [dP | mP].
+//
+// One CTA = (order m, gemm, tile of 128 rows), 4 warps.  The warps build the
+// A tile (scaled fp16 hi/lo, 128-byte swizzled, K-major) in shared memory
+// while one thread issues the TMA loads of the B tiles (hi/lo) and the MMAs;
+// two pipeline stages overlap the three.  The accumulators live in TMEM (two
+// x up to 256 fp32 columns) and the 4 warps read them back with tcgen05.ld
+// (warp w owns TMEM lanes 32w..32w+31 = tile rows).  Every mbarrier wait is
+// bounded in time: a wait that runs out sets bit 2 of the context's status
+// word, the CTA drains its own TMA loads and MMAs (bounded again), releases
+// TMEM and returns without writing results; the host reports the status.
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
 #include "cb2_internal.cuh"
 
 namespace cb2 {
 
-int mixed_setup(Ctx &c) {
-  (void)c;
-  set_error("mixed precision path is not available in this build");
-  return CB2_ERR_ARG;
+namespace {
+
+constexpr int TM = 128;          // GEMM rows per CTA (= TMEM lanes)
+constexpr int KB = 64;           // K per pipeline stage: one 128-byte swizzle row of fp16
+constexpr int NSTAGE = 2;
+constexpr int NTHR = 128;
+constexpr int ACC1 = 256;        // TMEM column of the parity-1 accumulator
+constexpr uint32_t TMEM_COLS = 512;
+constexpr unsigned long long kWaitNs = 200ull * 1000 * 1000;   // 200 ms per wait
+
+__device__ inline uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-void mixed_free(Ctx &c) { (void)c; }
-void leg_bwd_mixed(Ctx &, int, int, const int *, float *) {}
-void leg_fwd_mixed(Ctx &, int, int, const float *, const int *) {}
+
+__device__ inline unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ inline void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ inline void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// wait for the phase with the given parity to complete; false after kWaitNs
+__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  unsigned long long t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (it == 64) t0 = globaltimer();
+    if (it > 64) {
+      if (globaltimer() - t0 > kWaitNs) return false;
+      __nanosleep(32);
+    }
+  }
+}
+
+__device__ inline void tma_load_2d(void *dst, const CUtensorMap *tm, uint64_t *bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(tm)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+      : "memory");
+}
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (tile base 1024-byte aligned)
+__device__ inline uint64_t smem_desc_sw128(const void *p) {
+  uint64_t d = (uint64_t)((smem_u32(p) & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset
+  d |= (uint64_t)1 << 46;                 // descriptor version of tcgen05
+  d |= (uint64_t)2 << 61;                 // 128-byte swizzle
+  return d;
+}
+
+// instruction descriptor: D f32, A and B f16, both K-major, M x N
+__device__ inline uint32_t idesc_f16_f32(int M, int N) {
+  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ inline void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+
+__device__ inline void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ inline void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ inline void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ inline void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 8 consecutive fp32 columns of this thread's TMEM lane
+__device__ inline void tmem_ld8(uint32_t taddr, float v[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                 "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// byte offset of the 16-byte chunk holding elements (row, 8c .. 8c+7) in a
+// 128-byte-swizzled K-major tile (the layout TMA SWIZZLE_128B writes)
+__device__ inline uint32_t sw128_chunk(int row, int c) {
+  return (uint32_t)row * 128u + ((uint32_t)(c ^ (row & 7)) << 4);
+}
+
+// largest scaled magnitude: 2^13 <= mx s < 2^14 (fp16 holds up to 65504)
+constexpr int kScaleExp = 14;
+
+// power-of-two scale for a row (column) whose largest |x| is mx; the exponent
+// is clamped so neither s nor 1/s leaves the float range (1 for an all-zero row)
+__host__ __device__ inline float pow2_scale(double mx) {
+  if (!(mx > 0.0) || !(mx < 1e300)) return 1.0f;
+  int e;
+  frexp(mx, &e);
+  int sh = kScaleExp - e;
+  sh = sh < -120 ? -120 : (sh > 120 ? 120 : sh);
+  return ldexpf(1.0f, sh);
+}
+
+__device__ inline uint32_t pack_half2(__half a, __half b) {
+  return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
+}
+
+struct Smem {
+  uint64_t full[NSTAGE], empty[NSTAGE], done;
+  uint32_t tmem_base;
+  int mma_any;
+  float rowscale[TM];
+};
+
+// ---------------------------------------------------------------------------
+// The pipelined GEMM of one CTA, shared by the backward and forward kernels.
+// Prob supplies nkb(p) (K blocks of parity p), kvalid(p) (K extent with
+// non-zero A), kpad(p) (K extent the MMAs read), a(p, r, kk) (unscaled A of
+// tile row r), tma_xy(p, kb, x, y) (B box origin) and n(p) (MMA N).
+template <class Prob>
+__device__ bool gemm_tile(const Prob &pr, Smem *sh, unsigned char *base, uint32_t b_rows,
+                          const CUtensorMap *thi, const CUtensorMap *tlo, int *status) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t A_BYTES = TM * 128, B_BYTES = b_rows * 128;
+  const uint32_t STAGE = 2 * A_BYTES + 2 * B_BYTES;
+  const int nkb0 = pr.nkb(0), total = nkb0 + pr.nkb(1);
+  auto blk = [&](int kbi, int &p, int &kb) {
+    p = (kbi < nkb0) ? 0 : 1;
+    kb = p ? kbi - nkb0 : kbi;
+  };
+  if (tid == 0) {
+    for (int s = 0; s < NSTAGE; s++) { mbar_init(&sh->full[s], 1); mbar_init(&sh->empty[s], 1); }
+    mbar_init(&sh->done, 1);
+    sh->mma_any = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem_base)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // per-row power-of-two scale over every K value of the row (both parities)
+  for (int r = warp; r < TM; r += NTHR / 32) {
+    float mx = 0.0f;
+    for (int p = 0; p < 2; p++)
+      for (int kk = lane; kk < pr.kvalid(p); kk += 32) mx = fmaxf(mx, fabsf(pr.a(p, r, kk)));
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) sh->rowscale[r] = pow2_scale(mx);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh->tmem_base;
+
+  uint32_t ph_full = 0, ph_empty = 0;   // phase parity of each stage's barrier, one bit per stage
+  int n_tma = 0, n_full = 0;   // thread 0: B stages requested / consumed
+  // fail fast once a wait has run out anywhere in this launch
+  int failed = __syncthreads_or((*(volatile int *)status & CB2_STATUS_PIPE_TIMEOUT) != 0);
+  auto issue_tma = [&](int kbi) {
+    int p, kb, x, y;
+    blk(kbi, p, kb);
+    pr.tma_xy(p, kb, x, y);
+    const int s = kbi % NSTAGE;
+    unsigned char *st = base + s * STAGE;
+    mbar_expect_tx(&sh->full[s], 2 * B_BYTES);
+    tma_load_2d(st + 2 * A_BYTES, thi, &sh->full[s], x, y);
+    tma_load_2d(st + 2 * A_BYTES + B_BYTES, tlo, &sh->full[s], x, y);
+  };
+  if (tid == 0 && total > 0 && !failed) { issue_tma(0); n_tma = 1; }
+  for (int kbi = 0; kbi < total && !failed; kbi++) {
+    int p, kb;
+    blk(kbi, p, kb);
+    const int s = kbi % NSTAGE;
+    unsigned char *st = base + s * STAGE;
+    int f = 0;
+    // the A buffers of stage s were last read by the MMAs of block kbi - NSTAGE
+    if (kbi >= NSTAGE) {
+      if (!mbar_wait(&sh->empty[s], (ph_empty >> s) & 1)) f = 1;
+      ph_empty ^= 1u << s;
+    }
+    // the B tiles of the next block go into the stage the MMAs of block kbi-1 read
+    if (tid == 0 && !f && kbi + 1 < total) {
+      const int s1 = (kbi + 1) % NSTAGE;
+      if (kbi + 1 >= NSTAGE && !mbar_wait(&sh->empty[s1], (ph_empty >> s1) & 1)) f = 1;
+      if (!f) { issue_tma(kbi + 1); n_tma++; }
+    }
+    if (__syncthreads_or(f)) { failed = 1; break; }
+    // A tile of this block: 128 rows x 64 K, hi and lo, in 16-byte chunks
+    unsigned char *ahi = st, *alo = st + A_BYTES;
+    const int kv = pr.kvalid(p);
+    for (int c = tid; c < TM * (KB / 8); c += NTHR) {
+      const int r = c >> 3, ch = c & 7;
+      const float sc = sh->rowscale[r];
+      uint32_t h[4], l[4];
+#pragma unroll
+      for (int e = 0; e < 8; e += 2) {
+        const int kk = kb * KB + ch * 8 + e;
+        const float x0 = (kk < kv) ? pr.a(p, r, kk) * sc : 0.0f;
+        const float x1 = (kk + 1 < kv) ? pr.a(p, r, kk + 1) * sc : 0.0f;
+        const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
+        const __half l0 = __float2half_rn(x0 - __half2float(h0)), l1 = __float2half_rn(x1 - __half2float(h1));
+        h[e >> 1] = pack_half2(h0, h1);
+        l[e >> 1] = pack_half2(l0, l1);
+      }
+      const uint32_t off = sw128_chunk(r, ch);
+      *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4 *>(alo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      if (!mbar_wait(&sh->full[s], (ph_full >> s) & 1)) {
+        f = 1;
+      } else {
+        n_full++;
+        tc_fence_after();
+        const unsigned char *bhi = st + 2 * A_BYTES, *blo = st + 2 * A_BYTES + B_BYTES;
+        const uint32_t acc = tmem + (uint32_t)(p * ACC1);
+        const uint32_t idesc = idesc_f16_f32(TM, pr.n(p));
+        const int nks = (min(KB, pr.kpad(p) - kb * KB) + 15) / 16;
+        const uint64_t dah = smem_desc_sw128(ahi), dal = smem_desc_sw128(alo);
+        const uint64_t dbh = smem_desc_sw128(bhi), dbl = smem_desc_sw128(blo);
+        for (int ks = 0; ks < nks; ks++) {
+          const uint64_t o = (uint64_t)(ks * 2);   // +32 bytes along K
+          mma_f16(acc, dah + o, dbh + o, idesc, (kb == 0 && ks == 0) ? 0u : 1u);
+          mma_f16(acc, dah + o, dbl + o, idesc, 1u);
+          mma_f16(acc, dal + o, dbh + o, idesc, 1u);
+        }
+        mma_commit(&sh->empty[s]);
+        sh->mma_any = 1;
+      }
+      ph_full ^= 1u << s;
+    }
+    if (__syncthreads_or(f)) { failed = 1; break; }
+  }
+  // drain: B loads still in flight, then every MMA this CTA issued
+  if (tid == 0) {
+    for (; n_full < n_tma; n_full++) {
+      const int s = n_full % NSTAGE;
+      if (!mbar_wait(&sh->full[s], (ph_full >> s) & 1)) failed = 1;
+      ph_full ^= 1u << s;
+    }
+    if (sh->mma_any) mma_commit(&sh->done);
+  }
+  __syncthreads();
+  int f = failed;
+  if (sh->mma_any && !mbar_wait(&sh->done, 0)) f = 1;
+  f = __syncthreads_or(f);
+  tc_fence_after();
+  if (f && tid == 0) atomicOr(status, CB2_STATUS_PIPE_TIMEOUT);
+  return !f && total > 0;
+}
+
+__device__ inline void tmem_release(Smem *sh) {
+  tc_fence_before();
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sh->tmem_base), "r"(TMEM_COLS));
+}
+
+__device__ inline unsigned char *smem_base_1024(unsigned char *raw) {
+  return (unsigned char *)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
+}
+
+// ---------------------------------------------------------------------------
+// backward
+struct BwdArgs {
+  int L, nr, jmax, nh, nhp, NS, ncomp, nvec, nscal, nth;
+  int slot[8];
+  const int *moff;
+  const double *g3rlm, *ar1;
+  const double *f;
+  size_t fs;
+  const float *bunscale;          // [gemm][m][nhp] 1 / column scale of B
+  const int *koff, *klen, *n1;    // per (m, group) K offset / length; dP part length
+  float *four;
+  int *status;
+};
+
+struct BwdProb {
+  const BwdArgs *A;
+  int m, g, nrows, row0;
+  int kl[2], ko[2], n1[2];
+  __device__ int nkb(int p) const { return (kl[p] + KB - 1) / KB; }
+  __device__ int kvalid(int p) const { return kl[p]; }
+  __device__ int kpad(int p) const { return ((kl[p] + 15) / 16) * 16; }
+  __device__ int n(int) const { return A->nhp; }
+  __device__ void tma_xy(int p, int kb, int &x, int &y) const { x = ko[p] + kb * KB; y = 0; }
+  __device__ float a(int p, int r, int kk) const {
+    const BwdArgs &b = *A;
+    const int row = row0 + r;
+    if (row >= nrows) return 0.0f;
+    if (g == 0) {
+      const int ng = b.nvec + b.nscal, s = row & 1, v = (row >> 1) % ng, k = (row >> 1) / ng;
+      if (m == 0 && s == 1) return 0.0f;
+      const int l = m + p + 2 * kk;
+      const int jj = b.moff[m] + s * (b.L + 1 - m) + (l - m);
+      const size_t at = (size_t)k * b.jmax + jj;
+      if (v < b.nvec) {
+        const double ar = b.ar1[k];
+        return (float)(b.f[(size_t)b.slot[v] * b.fs + at] * ar * ar * b.g3rlm[jj]);
+      }
+      return (float)b.f[(size_t)b.slot[v] * b.fs + at];
+    }
+    const int q = row & 3, v = (row >> 2) % b.nvec, k = (row >> 2) / b.nvec;
+    const bool dpart = kk < n1[p];
+    const int l = dpart ? m + (1 - p) + 2 * kk : m + p + 2 * (kk - n1[p]);
+    // dP part {D+, D-, -T+, -T-}; mP part {T-, -T+, D-, -D+}; comp 1 = dS/dr, 2 = T
+    int comp, s;
+    float sg;
+    if (dpart) {
+      comp = (q < 2) ? 1 : 2; s = q & 1; sg = (q < 2) ? 1.0f : -1.0f;
+    } else {
+      comp = (q < 2) ? 2 : 1; s = (q & 1) ^ 1; sg = (q & 1) ? -1.0f : 1.0f;
+    }
+    if (m == 0 && s == 1) return 0.0f;
+    const int jj = b.moff[m] + s * (b.L + 1 - m) + (l - m);
+    const size_t at = (size_t)k * b.jmax + jj;
+    return sg * (float)(b.f[(size_t)(b.slot[v] + comp) * b.fs + at] * b.ar1[k]);
+  }
+};
+
+__global__ void __launch_bounds__(NTHR, 1)
+k_leg_bwd_mixed(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int tiles_g0,
+                const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char *base = smem_base_1024(smem_raw);
+  const uint32_t BR = (uint32_t)a.nhp;
+  Smem *sh = reinterpret_cast<Smem *>(base + NSTAGE * (2 * TM * 128 + 2 * BR * 128));
+  BwdProb pr;
+  pr.A = &a;
+  pr.m = blockIdx.y;
+  pr.g = (blockIdx.x < (unsigned)tiles_g0) ? 0 : 1;
+  pr.nrows = pr.g ? rows_g1 : rows_g0;
+  pr.row0 = (pr.g ? blockIdx.x - tiles_g0 : blockIdx.x) * TM;
+  const int m = pr.m;
+  for (int p = 0; p < 2; p++) {
+    pr.kl[p] = a.klen[m * 4 + 2 * pr.g + p];
+    pr.ko[p] = a.koff[m * 4 + 2 * pr.g + p];
+    pr.n1[p] = pr.g ? a.n1[m * 2 + p] : 0;
+  }
+  const bool ok = gemm_tile(pr, sh, base, BR, &tm_hi, &tm_lo, a.status);
+  if (ok) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = warp * 32 + lane, row = pr.row0 + r;
+    int k, c, s;
+    if (pr.g == 0) {
+      const int ng = a.nvec + a.nscal, v = (row >> 1) % ng;
+      s = row & 1; k = (row >> 1) / ng;
+      c = (v < a.nvec) ? 3 * v : 3 * a.nvec + (v - a.nvec);
+    } else {
+      const int q = row & 3, v = (row >> 2) % a.nvec;
+      k = (row >> 2) / a.nvec; s = q & 1; c = 3 * v + 1 + (q >> 1);
+    }
+    const bool valid = row < pr.nrows;
+    const float ua = 1.0f / sh->rowscale[r];
+    const uint32_t tl = sh->tmem_base + ((uint32_t)(warp * 32) << 16);
+    const bool has1 = pr.kl[1] > 0;
+    for (int t0 = 0; t0 < (int)BR; t0 += 8) {
+      float e[8], o[8];
+      tmem_ld8(tl + (uint32_t)t0, e);
+      if (has1) {
+        tmem_ld8(tl + (uint32_t)(ACC1 + t0), o);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; q++) o[q] = 0.0f;
+      }
+      if (!valid) continue;
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const int i = t0 + q;
+        if (i < a.nh) {
+          const float us = ua * a.bunscale[((size_t)pr.g * (a.L + 1) + m) * a.nhp + i];
+          a.four[(((size_t)i * a.nr + k) * a.ncomp + c) * a.NS + 2 * m + s] = (e[q] + o[q]) * us;
+          a.four[(((size_t)(a.nth - 1 - i) * a.nr + k) * a.ncomp + c) * a.NS + 2 * m + s] = (e[q] - o[q]) * us;
+        }
+      }
+    }
+  }
+  tmem_release(sh);
+}
+
+// ---------------------------------------------------------------------------
+// forward
+struct FwdArgs {
+  int L, nr, jmax, nh, nhp, NS, ncomp, nvec, nscal, nth, NFmax;
+  int slot[8];
+  const int *moff;
+  const double *g6, *g7, *r, *wgt;
+  const float *four;
+  double *f;
+  size_t fs;
+  const float *bunscale; // [gemm][(m, parity)][NFmax] 1 / column scale of B
+  const int *roff, *nlp; // B row offset and number of degrees of (m, parity)
+  int *status;
+};
+
+struct FwdProb {
+  const FwdArgs *A;
+  int m, g, nrows, row0, K;
+  int np[2], ro[2];
+  __device__ int nkb(int p) const { return np[p] > 0 ? (K + KB - 1) / KB : 0; }
+  __device__ int kvalid(int) const { return K; }
+  __device__ int kpad(int) const { return K; }
+  __device__ int n(int p) const { return ((np[p] + 15) / 16) * 16; }
+  __device__ void tma_xy(int p, int kb, int &x, int &y) const { x = kb * KB; y = ro[p]; }
+  // f(theta_i) w_i of grid component c, order sign s
+  __device__ float fw(int i, int k, int c, int s) const {
+    const FwdArgs &b = *A;
+    return b.four[(((size_t)i * b.nr + k) * b.ncomp + c) * b.NS + 2 * m + s] * (float)b.wgt[i];
+  }
+  __device__ float a(int p, int r, int kk) const {
+    const FwdArgs &b = *A;
+    const int row = row0 + r;
+    if (row >= nrows) return 0.0f;
+    if (g == 0) {
+      const int ng = b.nvec + b.nscal, s = row & 1, v = (row >> 1) % ng, k = (row >> 1) / ng;
+      if (kk >= b.nh || (m == 0 && s == 1)) return 0.0f;
+      const int c = (v < b.nvec) ? 3 * v : 3 * b.nvec + (v - b.nvec);
+      const float fa = fw(kk, k, c, s), fb = fw(b.nth - 1 - kk, k, c, s);
+      return p ? fa - fb : fa + fb;
+    }
+    const int q = row & 3, v = (row >> 2) % b.nvec, k = (row >> 2) / b.nvec;
+    const bool dpart = kk < b.nhp;
+    const int i = dpart ? kk : kk - b.nhp;
+    if (i >= b.nh) return 0.0f;
+    // dS+ = [theta+ (fold 1-p) | -phi- (fold p)], dS- = [theta- | +phi+],
+    // T+  = [-phi+ (fold 1-p) | -theta- (fold p)], T- = [-phi- | +theta+]
+    int comp, s, sigma;
+    float sg;
+    if (dpart) {
+      comp = (q < 2) ? 1 : 2; s = q & 1; sg = (q < 2) ? 1.0f : -1.0f; sigma = 1 - p;
+    } else {
+      comp = (q < 2) ? 2 : 1; s = (q & 1) ^ 1; sg = (q & 1) ? 1.0f : -1.0f; sigma = p;
+    }
+    if (m == 0 && s == 1) return 0.0f;
+    const int c = 3 * v + comp;
+    const float fa = fw(i, k, c, s), fb = fw(b.nth - 1 - i, k, c, s);
+    return sg * (sigma ? fa - fb : fa + fb);
+  }
+};
+
+__global__ void __launch_bounds__(NTHR, 1)
+k_leg_fwd_mixed(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int tiles_g0,
+                const __grid_constant__ CUtensorMap tmp_hi, const __grid_constant__ CUtensorMap tmp_lo,
+                const __grid_constant__ CUtensorMap tmd_hi, const __grid_constant__ CUtensorMap tmd_lo) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char *base = smem_base_1024(smem_raw);
+  const uint32_t BR = (uint32_t)a.NFmax;
+  Smem *sh = reinterpret_cast<Smem *>(base + NSTAGE * (2 * TM * 128 + 2 * BR * 128));
+  FwdProb pr;
+  pr.A = &a;
+  pr.m = blockIdx.y;
+  pr.g = (blockIdx.x < (unsigned)tiles_g0) ? 0 : 1;
+  pr.nrows = pr.g ? rows_g1 : rows_g0;
+  pr.row0 = (pr.g ? blockIdx.x - tiles_g0 : blockIdx.x) * TM;
+  pr.K = pr.g ? 2 * a.nhp : a.nhp;
+  const int m = pr.m;
+  for (int p = 0; p < 2; p++) {
+    pr.np[p] = a.nlp[m * 2 + p];
+    pr.ro[p] = a.roff[m * 2 + p];
+  }
+  const bool ok = gemm_tile(pr, sh, base, BR, pr.g ? &tmd_hi : &tmp_hi, pr.g ? &tmd_lo : &tmp_lo, a.status);
+  if (ok) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = warp * 32 + lane, row = pr.row0 + r;
+    int k, slot, kind, s;   // kind 0: S (g7 r^2), 1: dS or T (g7 r), 2: scalar (g6)
+    if (pr.g == 0) {
+      const int ng = a.nvec + a.nscal, v = (row >> 1) % ng;
+      s = row & 1; k = (row >> 1) / ng;
+      slot = a.slot[v]; kind = (v < a.nvec) ? 0 : 2;
+    } else {
+      const int q = row & 3, v = (row >> 2) % a.nvec;
+      k = (row >> 2) / a.nvec; s = q & 1;
+      slot = a.slot[v] + 1 + (q >> 1); kind = 1;
+    }
+    const bool valid = row < pr.nrows && !(m == 0 && s == 1);
+    const double ua = 1.0 / (double)sh->rowscale[r];
+    const uint32_t tl = sh->tmem_base + ((uint32_t)(warp * 32) << 16);
+    const double rk = valid ? a.r[k] : 0.0;
+    for (int p = 0; p < 2; p++) {
+      for (int c0 = 0; c0 < pr.np[p]; c0 += 8) {
+        float v8[8];
+        tmem_ld8(tl + (uint32_t)(p * ACC1 + c0), v8);
+        if (!valid) continue;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const int t = c0 + q;
+          if (t < pr.np[p]) {
+            const int l = m + p + 2 * t;
+            const int jj = a.moff[m] + s * (a.L + 1 - m) + (l - m);
+            const double us = ua * (double)a.bunscale[((size_t)pr.g * (a.L + 1) * 2 + m * 2 + p) * a.NFmax + t];
+            const double fac = (kind == 0) ? a.g7[jj] * rk * rk : (kind == 2) ? a.g6[jj] : a.g7[jj] * rk;
+            a.f[(size_t)slot * a.fs + (size_t)k * a.jmax + jj] = (double)v8[q] * us * fac;
+          }
+        }
+      }
+    }
+  }
+  tmem_release(sh);
+}
+
+// ---------------------------------------------------------------------------
+// B operands: scaled fp16 hi/lo copies of the float64 P tables
+__device__ inline void split_store(__half *hi, __half *lo, size_t at, double v, float s) {
+  const double x = v * (double)s;
+  const __half h = __float2half_rn((float)x);
+  hi[at] = h;
+  lo[at] = __float2half_rn((float)(x - (double)__half2float(h)));
+}
+
+// backward B[theta][K]: one thread per (m, south node i)
+__global__ void k_build_bwd_b(int L, int nh, int nhp, const size_t *poff, const double *Plt, const double *dPlt,
+                              const double *asin_t, const int *koff, const int *klen, const int *n1, int Kb_all,
+                              float *bunscale, __half *bhi, __half *blo) {
+  const int m = blockIdx.y, i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m > L || i >= nh) return;
+  const int nl = L + 1 - m;
+  const size_t po = poff[m];
+  const double am = (double)m * asin_t[i];
+  double mxp = 0.0, mxd = 0.0;
+  for (int t = 0; t < nl; t++) {
+    const double P = Plt[po + (size_t)t * nh + i], dP = dPlt[po + (size_t)t * nh + i];
+    mxp = fmax(mxp, fabs(P));
+    mxd = fmax(mxd, fmax(fabs(dP), fabs(P * am)));
+  }
+  const float sp = pow2_scale(mxp), sd = pow2_scale(mxd);
+  bunscale[(size_t)m * nhp + i] = 1.0f / sp;                     // gemm P
+  bunscale[((size_t)(L + 1) + m) * nhp + i] = 1.0f / sd;         // gemm DM
+  for (int gi = 0; gi < 4; gi++) {
+    const int ko = koff[m * 4 + gi], kl = klen[m * 4 + gi];
+    const float s = (gi < 2) ? sp : sd;
+    for (int kk = 0; kk < kl; kk++) {
+      double v;
+      if (gi < 2) {
+        const int l = m + gi + 2 * kk;
+        v = Plt[po + (size_t)(l - m) * nh + i];
+      } else {
+        const int p = gi - 2, nn = n1[m * 2 + p];
+        if (kk < nn) {
+          const int l = m + (1 - p) + 2 * kk;
+          v = dPlt[po + (size_t)(l - m) * nh + i];
+        } else {
+          const int l = m + p + 2 * (kk - nn);
+          v = Plt[po + (size_t)(l - m) * nh + i] * am;
+        }
+      }
+      split_store(bhi, blo, (size_t)i * Kb_all + ko + kk, v, s);
+    }
+  }
+}
+
+// forward B[l][theta] (P) and B[l][dP theta | mP theta] (DM): one thread per (m, degree)
+__global__ void k_build_fwd_b(int L, int nh, int nhp, int NFmax, const size_t *poff, const double *Plt,
+                              const double *dPlt, const double *asin_t, const int *roff, const int *nlp,
+                              float *bunscale, __half *php, __half *plp, __half *dhp, __half *dlp) {
+  const int m = blockIdx.y, t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m > L) return;
+  const size_t po = poff[m];
+  for (int p = 0; p < 2; p++) {
+    if (t >= nlp[m * 2 + p]) continue;
+    const int l = m + p + 2 * t;
+    const size_t row = (size_t)roff[m * 2 + p] + t;
+    double mxp = 0.0, mxd = 0.0;
+    for (int i = 0; i < nh; i++) {
+      const double P = Plt[po + (size_t)(l - m) * nh + i], dP = dPlt[po + (size_t)(l - m) * nh + i];
+      mxp = fmax(mxp, fabs(P));
+      mxd = fmax(mxd, fmax(fabs(dP), fabs(P * (double)m * asin_t[i])));
+    }
+    const float sp = pow2_scale(mxp), sd = pow2_scale(mxd);
+    bunscale[(size_t)(m * 2 + p) * NFmax + t] = 1.0f / sp;                        // gemm P
+    bunscale[((size_t)(L + 1) * 2 + m * 2 + p) * NFmax + t] = 1.0f / sd;          // gemm DM
+    for (int i = 0; i < nh; i++) {
+      const double P = Plt[po + (size_t)(l - m) * nh + i];
+      split_store(php, plp, row * nhp + i, P, sp);
+      split_store(dhp, dlp, row * 2 * nhp + i, dPlt[po + (size_t)(l - m) * nh + i], sd);
+      split_store(dhp, dlp, row * 2 * nhp + nhp + i, P * (double)m * asin_t[i], sd);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+struct MixedTables {
+  __half *bb_hi = nullptr, *bb_lo = nullptr;      // backward B [nhp][Kb_all]
+  float *bb_unscale = nullptr;                    // [gemm][m][nhp]
+  int *bb_koff = nullptr, *bb_klen = nullptr, *bb_n1 = nullptr;
+  __half *bfp_hi = nullptr, *bfp_lo = nullptr;    // forward B (P) [rows_all][nhp]
+  __half *bfd_hi = nullptr, *bfd_lo = nullptr;    // forward B (DM) [rows_all][2 nhp]
+  float *bf_unscale = nullptr;                    // [gemm][(m, parity)][NFmax]
+  int *bf_roff = nullptr, *bf_nl = nullptr;
+  int Kb_all = 0, rows_all = 0, nhp = 0, NFmax = 0;
+  size_t smem_bwd = 0, smem_fwd = 0;
+  CUtensorMap tm_bb_hi, tm_bb_lo, tm_bfp_hi, tm_bfp_lo, tm_bfd_hi, tm_bfd_lo;
+};
+
+using EncodeFn = PFN_cuTensorMapEncodeTiled_v12000;
+
+EncodeFn get_encode() {
+  static EncodeFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeFn)p;
+  }
+  return fn;
+}
+
+// fp16 [rows][cols] (cols contiguous, cols * 2 bytes a multiple of 16), box 64 x box_rows, 128B swizzle
+int make_map(CUtensorMap *tm, const void *ptr, uint64_t cols, uint64_t rows, uint32_t box_rows) {
+  EncodeFn enc = get_encode();
+  if (!enc) { set_error("cuTensorMapEncodeTiled is not available"); return CB2_ERR_CUDA; }
+  if ((cols * sizeof(__half)) % 16 != 0 || box_rows == 0 || box_rows > 256 || rows < box_rows) {
+    set_error("tensor map shape");
+    return CB2_ERR_ARG;
+  }
+  cuuint64_t dims[2] = {cols, rows};
+  cuuint64_t strides[1] = {cols * sizeof(__half)};
+  cuuint32_t box[2] = {(cuuint32_t)KB, box_rows};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled failed"); return CB2_ERR_CUDA; }
+  return 0;
+}
+
+// 1024 alignment slack + stages + control block; at least 120 KB so a CTA
+// holding 512 TMEM columns has the SM to itself
+size_t smem_bytes(int b_rows) {
+  size_t s = 1024 + (size_t)NSTAGE * (2 * TM * 128 + 2 * (size_t)b_rows * 128) + sizeof(Smem);
+  return std::max(s, (size_t)120 * 1024);
+}
+
+}  // namespace
+
+int mixed_setup(Ctx &c) {
+  MixedTables *t = new MixedTables();
+  c.mixed = t;
+  const int L = c.L, nh = c.nh;
+  t->nhp = ((nh + 15) / 16) * 16;
+  if (t->nhp > 256) { set_error("mixed precision path needs nth <= 512"); return CB2_ERR_ARG; }
+  // backward K groups per m: P0, P1 (l-m even / odd), D0 = {dP odd | mP even}, D1 = {dP even | mP odd}
+  std::vector<int> koff((L + 1) * 4), klen((L + 1) * 4), n1((L + 1) * 2);
+  int K = 0;
+  for (int m = 0; m <= L; m++) {
+    const int nl = L + 1 - m, ne = (nl + 1) / 2, no = nl / 2;
+    const int lens[4] = {ne, no, no + ne, ne + no};
+    n1[m * 2 + 0] = no;
+    n1[m * 2 + 1] = ne;
+    for (int gi = 0; gi < 4; gi++) {
+      koff[m * 4 + gi] = K;
+      klen[m * 4 + gi] = lens[gi];
+      K += ((lens[gi] + 15) / 16) * 16;
+    }
+  }
+  t->Kb_all = K + KB;   // every 64-wide box starting at a group stays in the array
+  // forward B rows: per (m, parity) the degrees l = m + p + 2t
+  std::vector<int> roff((L + 1) * 2), nlp((L + 1) * 2);
+  int R = 0, nfmax = 16;
+  for (int m = 0; m <= L; m++) {
+    const int nl = L + 1 - m, cnt[2] = {(nl + 1) / 2, nl / 2};
+    for (int p = 0; p < 2; p++) {
+      roff[m * 2 + p] = R;
+      nlp[m * 2 + p] = cnt[p];
+      const int padded = ((cnt[p] + 15) / 16) * 16;
+      R += padded;
+      nfmax = std::max(nfmax, padded);
+    }
+  }
+  t->NFmax = nfmax;
+  if (t->NFmax > 256) { set_error("mixed precision path needs L <= 511"); return CB2_ERR_ARG; }
+  t->rows_all = R + t->NFmax;   // every NFmax-row box stays in the array
+  auto up = [&](int **d, const std::vector<int> &v) -> int {
+    CB2_CUDA(cudaMalloc(d, v.size() * sizeof(int)));
+    CB2_CUDA(cudaMemcpy(*d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+    return 0;
+  };
+  int rc;
+  if ((rc = up(&t->bb_koff, koff)) || (rc = up(&t->bb_klen, klen)) || (rc = up(&t->bb_n1, n1)) ||
+      (rc = up(&t->bf_roff, roff)) || (rc = up(&t->bf_nl, nlp)))
+    return rc;
+  const size_t nb = (size_t)t->nhp * t->Kb_all;
+  const size_t nfp = (size_t)t->rows_all * t->nhp, nfd = 2 * nfp;
+  __half **bufs[6] = {&t->bb_hi, &t->bb_lo, &t->bfp_hi, &t->bfp_lo, &t->bfd_hi, &t->bfd_lo};
+  const size_t lens[6] = {nb, nb, nfp, nfp, nfd, nfd};
+  for (int q = 0; q < 6; q++) {
+    CB2_CUDA(cudaMalloc(bufs[q], lens[q] * sizeof(__half)));
+    CB2_CUDA(cudaMemsetAsync(*bufs[q], 0, lens[q] * sizeof(__half), c.stream));
+  }
+  const size_t nbs = 2 * (size_t)(L + 1) * t->nhp, nfs = 2 * (size_t)(L + 1) * 2 * t->NFmax;
+  CB2_CUDA(cudaMalloc(&t->bb_unscale, nbs * sizeof(float)));
+  CB2_CUDA(cudaMemsetAsync(t->bb_unscale, 0, nbs * sizeof(float), c.stream));
+  CB2_CUDA(cudaMalloc(&t->bf_unscale, nfs * sizeof(float)));
+  CB2_CUDA(cudaMemsetAsync(t->bf_unscale, 0, nfs * sizeof(float), c.stream));
+  k_build_bwd_b<<<dim3(cdiv(nh, 64), L + 1), 64, 0, c.stream>>>(L, nh, t->nhp, c.d_poff, c.d_Plt, c.d_dPlt,
+                                                                c.d_asin, t->bb_koff, t->bb_klen, t->bb_n1,
+                                                                t->Kb_all, t->bb_unscale, t->bb_hi, t->bb_lo);
+  CB2_CUDA(cudaGetLastError());
+  k_build_fwd_b<<<dim3(cdiv(t->NFmax, 64), L + 1), 64, 0, c.stream>>>(
+      L, nh, t->nhp, t->NFmax, c.d_poff, c.d_Plt, c.d_dPlt, c.d_asin, t->bf_roff, t->bf_nl, t->bf_unscale,
+      t->bfp_hi, t->bfp_lo, t->bfd_hi, t->bfd_lo);
+  CB2_CUDA(cudaGetLastError());
+  CB2_CUDA(cudaStreamSynchronize(c.stream));
+  if ((rc = make_map(&t->tm_bb_hi, t->bb_hi, t->Kb_all, t->nhp, t->nhp)) ||
+      (rc = make_map(&t->tm_bb_lo, t->bb_lo, t->Kb_all, t->nhp, t->nhp)) ||
+      (rc = make_map(&t->tm_bfp_hi, t->bfp_hi, t->nhp, t->rows_all, t->NFmax)) ||
+      (rc = make_map(&t->tm_bfp_lo, t->bfp_lo, t->nhp, t->rows_all, t->NFmax)) ||
+      (rc = make_map(&t->tm_bfd_hi, t->bfd_hi, 2 * t->nhp, t->rows_all, t->NFmax)) ||
+      (rc = make_map(&t->tm_bfd_lo, t->bfd_lo, 2 * t->nhp, t->rows_all, t->NFmax)))
+    return rc;
+  t->smem_bwd = smem_bytes(t->nhp);
+  t->smem_fwd = smem_bytes(t->NFmax);
+  if (t->smem_bwd > 227 * 1024 || t->smem_fwd > 227 * 1024) {
+    set_error("mixed precision tiles exceed shared memory");
+    return CB2_ERR_ARG;
+  }
+  CB2_CUDA(cudaFuncSetAttribute(k_leg_bwd_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_bwd));
+  CB2_CUDA(cudaFuncSetAttribute(k_leg_fwd_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_fwd));
+  return 0;
+}
+
+void mixed_free(Ctx &c) {
+  MixedTables *t = (MixedTables *)c.mixed;
+  if (!t) return;
+  void *ptrs[] = {t->bb_hi, t->bb_lo, t->bb_unscale, t->bb_koff, t->bb_klen, t->bb_n1, t->bfp_hi,
+                  t->bfp_lo, t->bfd_hi, t->bfd_lo, t->bf_unscale, t->bf_roff, t->bf_nl};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  delete t;
+  c.mixed = nullptr;
+}
+
+void leg_bwd_mixed(Ctx &c, int nvec, int nscal, const int *slots, float *four) {
+  MixedTables *t = (MixedTables *)c.mixed;
+  BwdArgs a{};
+  a.L = c.L; a.nr = c.nr; a.jmax = c.jmax; a.nh = c.nh; a.nhp = t->nhp; a.NS = c.NS;
+  a.ncomp = 3 * nvec + nscal; a.nvec = nvec; a.nscal = nscal; a.nth = c.nth;
+  for (int q = 0; q < nvec + nscal && q < 8; q++) a.slot[q] = slots[q];
+  a.moff = c.d_moff; a.g3rlm = c.d_g3rlm; a.ar1 = c.d_ar1; a.f = c.d_f; a.fs = c.fsize();
+  a.bunscale = t->bb_unscale; a.koff = t->bb_koff; a.klen = t->bb_klen; a.n1 = t->bb_n1;
+  a.four = four; a.status = c.d_status;
+  const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
+  const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
+  k_leg_bwd_mixed<<<dim3(tiles0 + tiles1, c.L + 1), NTHR, t->smem_bwd, c.stream>>>(a, rows0, rows1, tiles0,
+                                                                                  t->tm_bb_hi, t->tm_bb_lo);
+}
+
+void leg_fwd_mixed(Ctx &c, int nvec, int nscal, const float *four, const int *slots) {
+  MixedTables *t = (MixedTables *)c.mixed;
+  FwdArgs a{};
+  a.L = c.L; a.nr = c.nr; a.jmax = c.jmax; a.nh = c.nh; a.nhp = t->nhp; a.NS = c.NS;
+  a.ncomp = 3 * nvec + nscal; a.nvec = nvec; a.nscal = nscal; a.nth = c.nth; a.NFmax = t->NFmax;
+  for (int q = 0; q < nvec + nscal && q < 8; q++) a.slot[q] = slots[q];
+  a.moff = c.d_moff; a.g6 = c.d_g6; a.g7 = c.d_g7; a.r = c.d_r; a.wgt = c.d_wgt;
+  a.four = four; a.f = c.d_f; a.fs = c.fsize();
+  a.bunscale = t->bf_unscale; a.roff = t->bf_roff; a.nlp = t->bf_nl;
+  a.status = c.d_status;
+  const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
+  const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
+  k_leg_fwd_mixed<<<dim3(tiles0 + tiles1, c.L + 1), NTHR, t->smem_fwd, c.stream>>>(
+      a, rows0, rows1, tiles0, t->tm_bfp_hi, t->tm_bfp_lo, t->tm_bfd_hi, t->tm_bfd_lo);
+}
 
 }  // namespace cb2

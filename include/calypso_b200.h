@@ -36,6 +36,8 @@ extern "C" {
 #define CB2_ERR_SINGULAR -3   /* zero pivot in a radial LU factorisation    */
 #define CB2_ERR_NAN -4        /* NaN/Inf found in the energy diagnostics    */
 #define CB2_ERR_STATE -5      /* call out of order (e.g. step before start) */
+#define CB2_ERR_TIMEOUT -6    /* a bounded wait inside a tensor-core kernel
+                                 ran out; the results of that step are void */
 
 #define CB2_PREC_FP64 0       /* plain path: every stage in float64          */
 #define CB2_PREC_MIXED 1      /* Legendre split-fp16 tcgen05, fp32 FFT and

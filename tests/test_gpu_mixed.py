@@ -1,0 +1,113 @@
+"""GPU checks of the mixed-precision path (split-fp16 tcgen05 Legendre
+transforms, float32 FFT and grid products, float64 radial solves).
+
+Tolerances, stated per check:
+  - one SHT (backward or forward) against the float64 oracle: 5e-6
+    relative L2 per component (split fp16 products carry ~2^-22 of the row
+    and column scales, float32 accumulation and FFT ~1e-7);
+  - volume energies of a time-stepped run against the float64 plain path:
+    1e-6 relative from the dynamo benchmark state (every energy of order
+    one); 2e-6 from the seeded start, whose toroidal magnetic field starts
+    at zero, so its relative error is that of the float32 induction term
+    measured against |u||B| rather than against the field itself;
+  - CUDA-graph replay against eager stepping: bitwise (no atomics).
+"""
+import numpy as np
+import pytest
+
+from calypso_b200 import PREC_FP64, PREC_MIXED, SphMHD, configs
+from calypso_b200.sph_mhd import MAGNE, TEMP, VELO
+
+pytestmark = pytest.mark.gpu
+
+SHT_TOL = 5e-6
+ENERGY_TOL = 1e-6
+ENERGY_TOL_SEEDED = 2e-6
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def random_spec(L, nr, nc, seed, zero_l0=()):
+    """Spectra with a decaying l-spectrum (amplitude ~ 1/(l sqrt(2l+1)))."""
+    rng = np.random.default_rng(seed)
+    jmax = (L + 1) ** 2
+    ls = np.array([l for l in range(L + 1) for _ in range(2 * l + 1)])
+    amp = 1.0 / np.sqrt(2 * ls + 1.0) / np.maximum(ls, 1)
+    spec = rng.standard_normal((nc, nr, jmax)) * amp[None, None, :]
+    for c in zero_l0:
+        spec[c, :, 0] = 0.0
+    return spec
+
+
+SHAPES = {
+    "L31_nth48": configs.dynamobench_case1(),
+    # nth/2 = 48 south nodes: a forward K block only partly inside the tables
+    "L63_nth96": configs.shell_params(63, 9, 96, 192, E=1e-4, Ra=300.0, dt=5e-6),
+    # nth/2 = 96 south nodes: B tiles of 96 rows, 2 K blocks per order; near
+    # the poles P_l^m of high m is far below the float range (sin^m theta)
+    "L127_nth192": configs.shell_params(127, 9, 192, 384, E=1e-4, Ra=300.0, dt=5e-6),
+}
+
+
+@pytest.mark.parametrize("shape", sorted(SHAPES))
+@pytest.mark.parametrize("nvec,nscal", [(4, 1), (1, 0), (0, 1), (3, 2)])
+def test_sht_mixed_matches_oracle(oracle_lib, shape, nvec, nscal):
+    p = SHAPES[shape]
+    g = SphMHD(p, PREC_MIXED)
+    o = oracle_lib.Oracle(p)
+    nc = 3 * nvec + nscal
+    zl0 = [3 * v + 1 for v in range(nvec)] + [3 * v + 2 for v in range(nvec)]
+    spec = random_spec(g.L, g.nr, nc, 11 + nc, zero_l0=zl0)
+    grid_g = g.sel_backward_legendre_trans(nvec, nscal, spec)
+    grid_o = o.sht_backward(nvec, nscal, spec)
+    assert np.isfinite(grid_g).all()
+    for c in range(nc):
+        assert rel_l2(grid_g[c], grid_o[c]) < SHT_TOL, (c, rel_l2(grid_g[c], grid_o[c]))
+    back_g = g.sel_forward_legendre_trans(nvec, nscal, grid_o)
+    back_o = o.sht_forward(nvec, nscal, grid_o)
+    assert np.isfinite(back_g).all()
+    for c in range(nc):
+        assert rel_l2(back_g[c], back_o[c]) < SHT_TOL, (c, rel_l2(back_g[c], back_o[c]))
+    g.sync()
+
+
+def _run(p, prec, kind, seed, nsteps):
+    g = SphMHD(p, prec)
+    g.init_fields(kind, seed)
+    g.step(nsteps)
+    return g
+
+
+def test_case1_mixed_energies_track_fp64():
+    p = configs.dynamobench_case1()
+    a = _run(p, PREC_FP64, 1, 0, 200)
+    b = _run(p, PREC_MIXED, 1, 0, 200)
+    ea, eb = a.energies(), b.energies()
+    rel = np.abs(eb - ea) / np.abs(ea)
+    assert rel.max() < ENERGY_TOL, rel
+    for slot in (VELO, MAGNE, TEMP):
+        assert rel_l2(b.get_field(slot), a.get_field(slot)) < 1e-4, slot
+
+
+def test_small_shell_mixed_energies_track_fp64():
+    p = configs.small_shell()
+    a = _run(p, PREC_FP64, 2, 5, 300)
+    b = _run(p, PREC_MIXED, 2, 5, 300)
+    ea, eb = a.energies(), b.energies()
+    rel = np.abs(eb - ea) / np.abs(ea)
+    assert rel.max() < ENERGY_TOL_SEEDED, rel
+
+
+def test_mixed_graph_replay_is_bitwise_eager():
+    p = configs.dynamobench_case1()
+    a = SphMHD(p, PREC_MIXED)
+    b = SphMHD(p, PREC_MIXED)
+    a.init_fields(1)
+    b.init_fields(1)
+    a.step(10)
+    b.step(10, graph=True)
+    for slot in (VELO, MAGNE + 2, TEMP):
+        assert np.array_equal(a.get_field(slot), b.get_field(slot)), slot
+    b.sync()
