@@ -138,6 +138,7 @@ void rj_after_transform(Ctx &c);
 void rj_start_derived(Ctx &c);
 void rj_temp_total(Ctx &c, double sign);
 int rj_energies(Ctx &c, double out[7]);
+int rj_energies_scratch(Ctx &c, double *scratch, double out[7]);
 int rj_lu_factorise(Ctx &c);
 // mixed-precision Legendre (cb2_legendre_mixed.cu)
 int mixed_setup(Ctx &c);

@@ -776,4 +776,27 @@ int rj_energies(Ctx &c, double out[7]) {
   return 0;
 }
 
+// The same diagnostics with caller-provided device scratch of at least
+// 7 * jmax + 7 doubles (per-(l,m) partial sums, then the 7 totals).  Every
+// element the kernels read is written first in the same call, so the
+// scratch needs no clearing.
+int rj_energies_scratch(Ctx &c, double *scratch, double out[7]) {
+  double *sums = scratch + 7 * (size_t)c.jmax;
+  k_energy_j<<<cdiv(c.jmax, 128), 128, 0, c.stream>>>(c.rj_args(), fields(c), c.d_g11, c.d_g12, scratch);
+  k_energy_reduce<<<7, 256, 0, c.stream>>>(c.jmax, scratch, sums);
+  CB2_CUDA(cudaGetLastError());
+  double s[7];
+  CB2_CUDA(cudaMemcpyAsync(s, sums, 7 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  CB2_CUDA(cudaStreamSynchronize(c.stream));
+  double ri = c.h_r[c.kin], ro = c.h_r[c.kout];
+  double avol = 3.0 / (ro * ro * ro - ri * ri * ri);
+  for (int q = 0; q < 7; q++) out[q] = avol * s[q];
+  for (int q = 0; q < 7; q++)
+    if (!std::isfinite(out[q])) {
+      set_error("non-finite value in the energy diagnostics");
+      return CB2_ERR_NAN;
+    }
+  return 0;
+}
+
 }  // namespace cb2

@@ -107,6 +107,18 @@ int cb2_istep(const cb2_ctx *ctx);
  * Synchronises.  Returns CB2_ERR_NAN if any value is not finite
  * (MHD_src/sph_MHD/cal_sol_sph_fluid_crank.f90 check_NaN_temperature). */
 int cb2_energies(cb2_ctx *ctx, double out[7]);
+/* The same seven values as cb2_energies, computed without allocating any
+ * device memory: the partial sums go to a static array in the library (one
+ * per device, 3.5 MiB) instead of a buffer of the context.  This entry point
+ * has no counterpart in the reference; it is for hosts that must not call
+ * the CUDA allocator during a run (device memory owned and budgeted by
+ * another component, or a monitoring loop that must not add allocations).
+ * Limits: jmax = (L+1)^2 <= 65536 (L <= 255), else CB2_ERR_ARG.  Every call
+ * on a device shares the array (it keeps the last call's contents; nothing
+ * in it needs to start at zero), so calls that overlap on one device race:
+ * serialise them.  The first call on a device looks the array up; make it
+ * before any stream capture starts on that device.  Synchronises. */
+int cb2_energies_static(cb2_ctx *ctx, double out[7]);
 
 /* d_rj field slot access (host buffers of nr*jmax float64).  Slot numbers:
  * 0 velocity, 3 vorticity, 6 magnetic field, 9 current density,
