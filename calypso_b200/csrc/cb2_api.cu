@@ -132,11 +132,12 @@ static int nonlinear(Ctx &c) {
     if (c.timers) cudaEventRecord(c.ev[13], c.stream);
     leg_fwd_f64(c, 4, 0, (const double *)c.d_four2, fslots);
   } else {
-    leg_bwd_mixed(c, 4, 1, bslots, (float *)c.d_four);
+    const MLayout fin = mlayout(c, c.d_four, 4, 1), fout = mlayout(c, c.d_four2, 4, 0);
+    leg_bwd_mixed(c, bslots, fin);
     if (c.timers) cudaEventRecord(c.ev[12], c.stream);
-    fft_products<float>(c, (const float *)c.d_four, (float *)c.d_four2);
+    fft_products_m(c, fin, fout);
     if (c.timers) cudaEventRecord(c.ev[13], c.stream);
-    leg_fwd_mixed(c, 4, 0, (const float *)c.d_four2, fslots);
+    leg_fwd_mixed(c, fout, fslots);
   }
   if (c.timers) cudaEventRecord(c.ev[14], c.stream);
   rj_after_transform(c);
@@ -524,8 +525,9 @@ int cb2_sht_backward(cb2_ctx *c, int nvec, int nscal, const double *spec, double
     leg_bwd_f64(*c, nvec, nscal, slots, (double *)c->d_four);
     fft_backward_grid<double>(*c, nc, (const double *)c->d_four, dgrid);
   } else {
-    leg_bwd_mixed(*c, nvec, nscal, slots, (float *)c->d_four);
-    fft_backward_grid<float>(*c, nc, (const float *)c->d_four, dgrid);
+    const MLayout l = mlayout(*c, c->d_four, nvec, nscal);
+    leg_bwd_mixed(*c, slots, l);
+    fft_backward_grid_m(*c, l, dgrid);
   }
   CB2_CUDA(cudaGetLastError());
   CB2_CUDA(cudaMemcpyAsync(grid, dgrid, gsz * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -549,8 +551,9 @@ int cb2_sht_forward(cb2_ctx *c, int nvec, int nscal, const double *grid, double 
     fft_forward_grid<double>(*c, nc, dgrid, (double *)c->d_four);
     leg_fwd_f64(*c, nvec, nscal, (const double *)c->d_four, slots);
   } else {
-    fft_forward_grid<float>(*c, nc, dgrid, (float *)c->d_four);
-    leg_fwd_mixed(*c, nvec, nscal, (const float *)c->d_four, slots);
+    const MLayout l = mlayout(*c, c->d_four, nvec, nscal);
+    fft_forward_grid_m(*c, dgrid, l);
+    leg_fwd_mixed(*c, l, slots);
   }
   CB2_CUDA(cudaGetLastError());
   CB2_CUDA(cudaStreamSynchronize(c->stream));

@@ -320,6 +320,181 @@ k_grid_to_fft(FFTPlan pl, int L, int NS, int nc, int nr, int nth, const double *
   }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed-precision path: the same fused transform over the order-major
+// Fourier layout (MLayout).  Input 4 vectors (u, w, B, J) + 1 scalar (T),
+// output 4 vectors (w x u, J x B, u x B, u T).  At one (theta, k) the 26
+// input floats of an order m are one run of 10 (P block) and one of 16
+// (D block); threads take consecutive elements of a run, the values are
+// staged in shared memory [component][s][m], and the Hermitian rows are
+// built from there.  Output is written the same way, one run per m.
+__device__ inline void m_comp_of_in(int j, int &c, int &s) {
+  // P block (k, field, s): fields 0..3 = r of u, w, B, J; 4 = T
+  if (j < 10) { const int f = j >> 1; s = j & 1; c = (f < 4) ? 3 * f : 12; return; }
+  // D block (k, vector, {theta s0, theta s1, phi s0, phi s1})
+  const int jd = j - 10, v = jd >> 2, q = jd & 3;
+  c = 3 * v + 1 + (q >> 1); s = q & 1;
+}
+
+__device__ inline void m_comp_of_out(int j, int &c, int &s) {
+  if (j < 8) { s = j & 1; c = 3 * (j >> 1); return; }
+  const int jd = j - 8, v = jd >> 2, q = jd & 3;
+  c = 3 * v + 1 + (q >> 1); s = q & 1;
+}
+
+__global__ void __launch_bounds__(512)
+k_fft_products_m(FFTPlan pl, int L, MLayout fin, MLayout fout, const float2 *__restrict__ tw, ProdCoef pc) {
+  using T = float;
+  using T2 = float2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int N = pl.n;
+  T2 *A = reinterpret_cast<T2 *>(smraw);    // 7 x N
+  T2 *B = A + 7 * N;                         // 7 x N (first used as the staging buffer)
+  T *S = reinterpret_cast<T *>(B);           // [c * 2 + s][m], 26 x (L+1)
+  const int th = blockIdx.x / fin.nr, k = blockIdx.x % fin.nr;
+  const int M1 = L + 1;
+  const float *Pin = fin.P + (size_t)th * fin.sP() + (size_t)k * 10;
+  const float *Din = fin.D + (size_t)th * fin.sD() + (size_t)k * 16;
+  const size_t mstP = (size_t)fin.nth * fin.sP(), mstD = (size_t)fin.nth * fin.sD();
+  for (int idx = threadIdx.x; idx < 26 * M1; idx += blockDim.x) {
+    const int m = idx / 26, j = idx - 26 * m;
+    int c, s;
+    m_comp_of_in(j, c, s);
+    S[(c * 2 + s) * M1 + m] = (j < 10) ? Pin[m * mstP + j] : Din[m * mstD + (j - 10)];
+  }
+  __syncthreads();
+  const int mmax = min(L, (N + 1) / 2 - 1);
+  for (int idx = threadIdx.x; idx < 7 * N; idx += blockDim.x) {
+    const int p = idx / N, n = idx - p * N;
+    const int c0 = 2 * p, c1 = 2 * p + 1;
+    const bool has1 = c1 < 13;
+    T2 z = T2{0, 0};
+    if (n == 0) {
+      z = T2{S[(c0 * 2) * M1], has1 ? S[(c1 * 2) * M1] : (T)0};
+    } else {
+      const int m = (n <= mmax) ? n : ((N - n <= mmax) ? N - n : -1);
+      if (m > 0) {
+        const T a0 = S[(c0 * 2) * M1 + m], b0 = S[(c0 * 2 + 1) * M1 + m];
+        const T a1 = has1 ? S[(c1 * 2) * M1 + m] : (T)0, b1 = has1 ? S[(c1 * 2 + 1) * M1 + m] : (T)0;
+        const T xr = (T)0.5 * a0, xi = (T)-0.5 * b0, yr = (T)0.5 * a1, yi = (T)-0.5 * b1;
+        z = (m == n) ? T2{xr - yi, xi + yr} : T2{xr + yi, -xi + yr};
+      }
+    }
+    A[idx] = z;
+  }
+  __syncthreads();
+  T2 *g = batch_fft<T, T2>(A, B, 7, pl, tw, +1);
+  T2 *hb = (g == A) ? B : A;
+  const T cv = (T)pc.cv, cl = (T)pc.cl, ci = (T)pc.ci, ct = (T)pc.ct;
+  for (int q = threadIdx.x; q < N; q += blockDim.x) {
+    T2 p0 = g[0 * N + q], p1 = g[1 * N + q], p2 = g[2 * N + q], p3 = g[3 * N + q];
+    T2 p4 = g[4 * N + q], p5 = g[5 * N + q], p6 = g[6 * N + q];
+    T ur = p0.x, ut = p0.y, up = p1.x, wr = p1.y, wt = p2.x, wp = p2.y;
+    T br = p3.x, bt = p3.y, bp = p4.x, jr = p4.y, jt = p5.x, jp = p5.y, tt = p6.x;
+    hb[0 * N + q] = T2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv};
+    hb[1 * N + q] = T2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl};
+    hb[2 * N + q] = T2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl};
+    hb[3 * N + q] = T2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci};
+    hb[4 * N + q] = T2{(ur * bt - ut * br) * ci, ur * tt * ct};
+    hb[5 * N + q] = T2{ut * tt * ct, up * tt * ct};
+  }
+  __syncthreads();
+  const T2 *zf = batch_fft<T, T2>(hb, g, 6, pl, tw, -1);
+  const T an = (T)(1.0 / (double)N);
+  float *Pout = fout.P + (size_t)th * fout.sP() + (size_t)k * 8;
+  float *Dout = fout.D + (size_t)th * fout.sD() + (size_t)k * 16;
+  const size_t oP = (size_t)fout.nth * fout.sP(), oD = (size_t)fout.nth * fout.sD();
+  for (int idx = threadIdx.x; idx < 24 * M1; idx += blockDim.x) {
+    const int m = idx / 24, j = idx - 24 * m;
+    int c, s;
+    m_comp_of_out(j, c, s);
+    const T2 *Z = zf + (c >> 1) * N;
+    const bool isy = c & 1;
+    T v;
+    if (m == 0) {
+      v = (s == 0) ? an * (isy ? Z[0].y : Z[0].x) : (T)0;
+    } else {
+      const T2 zk = Z[m % N], zn = Z[(N - m) % N];
+      if (!isy) v = (s == 0) ? (T)2 * an * (T)0.5 * (zk.x + zn.x) : (T)-2 * an * (T)0.5 * (zk.y - zn.y);
+      else v = (s == 0) ? (T)2 * an * (T)0.5 * (zk.y + zn.y) : (T)2 * an * (T)0.5 * (zk.x - zn.x);
+    }
+    if (j < 8) Pout[m * oP + j] = v;
+    else Dout[m * oD + (j - 8)] = v;
+  }
+}
+
+// order-major Fourier rows -> grid (float64), for the standalone transform API
+__global__ void __launch_bounds__(256)
+k_fft_to_grid_m(FFTPlan pl, int L, MLayout fin, double *grid, const float2 *tw) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int N = pl.n, nc = 3 * fin.nvec + fin.nscal, nr = fin.nr, nth = fin.nth;
+  float2 *Z0 = reinterpret_cast<float2 *>(smraw), *Z1 = Z0 + N;
+  const int th = blockIdx.x / nr, k = blockIdx.x % nr;
+  const int mmax = min(L, (N + 1) / 2 - 1);
+  for (int c = 0; c < nc; c += 2) {
+    const bool has1 = c + 1 < nc;
+    for (int q = threadIdx.x; q < N; q += blockDim.x) Z0[q] = float2{0, 0};
+    __syncthreads();
+    for (int m = threadIdx.x; m <= mmax; m += blockDim.x) {
+      const float a0 = *fin.at(m, th, k, c, 0), b0 = (m > 0) ? *fin.at(m, th, k, c, 1) : 0.0f;
+      const float a1 = has1 ? *fin.at(m, th, k, c + 1, 0) : 0.0f;
+      const float b1 = (has1 && m > 0) ? *fin.at(m, th, k, c + 1, 1) : 0.0f;
+      if (m == 0) {
+        Z0[0] = float2{a0, a1};
+      } else {
+        const float xr = 0.5f * a0, xi = -0.5f * b0, yr = 0.5f * a1, yi = -0.5f * b1;
+        Z0[m] = float2{xr - yi, xi + yr};
+        Z0[N - m] = float2{xr + yi, -xi + yr};
+      }
+    }
+    __syncthreads();
+    float2 *z = block_fft<float, float2>(Z0, Z1, pl, tw, +1);
+    for (int q = threadIdx.x; q < N; q += blockDim.x) {
+      grid[(((size_t)c * nr + k) * nth + th) * N + q] = (double)z[q].x;
+      if (has1) grid[(((size_t)(c + 1) * nr + k) * nth + th) * N + q] = (double)z[q].y;
+    }
+    __syncthreads();
+  }
+}
+
+// grid (float64) -> order-major Fourier rows
+__global__ void __launch_bounds__(256)
+k_grid_to_fft_m(FFTPlan pl, int L, const double *grid, MLayout fout, const float2 *tw) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int N = pl.n, nc = 3 * fout.nvec + fout.nscal, nr = fout.nr, nth = fout.nth;
+  float2 *Z0 = reinterpret_cast<float2 *>(smraw), *Z1 = Z0 + N;
+  const int th = blockIdx.x / nr, k = blockIdx.x % nr;
+  const float an = (float)(1.0 / (double)N);
+  for (int c = 0; c < nc; c += 2) {
+    const bool has1 = c + 1 < nc;
+    for (int q = threadIdx.x; q < N; q += blockDim.x) {
+      const float x = (float)grid[(((size_t)c * nr + k) * nth + th) * N + q];
+      const float y = has1 ? (float)grid[(((size_t)(c + 1) * nr + k) * nth + th) * N + q] : 0.0f;
+      Z0[q] = float2{x, y};
+    }
+    __syncthreads();
+    const float2 *z = block_fft<float, float2>(Z0, Z1, pl, tw, -1);
+    for (int m = threadIdx.x; m <= L; m += blockDim.x) {
+      float a0, b0, a1, b1;
+      if (m == 0) {
+        a0 = an * z[0].x; b0 = 0.0f; a1 = an * z[0].y; b1 = 0.0f;
+      } else {
+        const float2 zk = z[m % N], zn = z[(N - m) % N];
+        const float xr = 0.5f * (zk.x + zn.x), xi = 0.5f * (zk.y - zn.y);
+        const float yr = 0.5f * (zk.y + zn.y), yi = -0.5f * (zk.x - zn.x);
+        a0 = 2.0f * an * xr; b0 = -2.0f * an * xi; a1 = 2.0f * an * yr; b1 = -2.0f * an * yi;
+      }
+      *fout.at(m, th, k, c, 0) = a0;
+      *fout.at(m, th, k, c, 1) = b0;
+      if (has1) {
+        *fout.at(m, th, k, c + 1, 0) = a1;
+        *fout.at(m, th, k, c + 1, 1) = b1;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void k_twiddles(int n, double2 *tw, float2 *tw32) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
@@ -358,6 +533,12 @@ int fft_setup(Ctx &c) {
   }
   CB2_CUDA(cudaFuncSetAttribute(k_fft_products<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
   CB2_CUDA(cudaFuncSetAttribute(k_fft_products<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
+  CB2_CUDA(cudaFuncSetAttribute(k_fft_products_m, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(14 * (size_t)c.nph * sizeof(float2))));
+  if (26 * (size_t)(c.L + 1) * sizeof(float) > 7 * (size_t)c.nph * sizeof(float2)) {
+    set_error("ngrid_zonal_ctl too small for the staging of the fused FFT kernel");
+    return CB2_ERR_ARG;
+  }
   return 0;
 }
 
@@ -393,6 +574,26 @@ void fft_forward_grid(Ctx &c, int ncomp, const double *grid, T *four) {
   size_t sm = 2 * (size_t)c.nph * sizeof(T2);
   k_grid_to_fft<T><<<(unsigned)(c.nth * c.nr), 256, sm, c.stream>>>(p, c.L, c.NS, ncomp, c.nr, c.nth,
                                                                     grid, four, twid<T>(c));
+}
+
+void fft_products_m(Ctx &c, const MLayout &in, const MLayout &out) {
+  FFTPlan p = make_plan(c.nph);
+  size_t sm = 14 * (size_t)c.nph * sizeof(float2);
+  ProdCoef pc{c.p.coef_velo, c.p.coef_lor, c.p.coef_induct, c.p.coef_temp};
+  k_fft_products_m<<<(unsigned)(c.nth * c.nr), 512, sm, c.stream>>>(p, c.L, in, out, (const float2 *)c.d_tw_fft32,
+                                                                   pc);
+}
+
+void fft_backward_grid_m(Ctx &c, const MLayout &in, double *grid) {
+  FFTPlan p = make_plan(c.nph);
+  size_t sm = 2 * (size_t)c.nph * sizeof(float2);
+  k_fft_to_grid_m<<<(unsigned)(c.nth * c.nr), 256, sm, c.stream>>>(p, c.L, in, grid, (const float2 *)c.d_tw_fft32);
+}
+
+void fft_forward_grid_m(Ctx &c, const double *grid, const MLayout &out) {
+  FFTPlan p = make_plan(c.nph);
+  size_t sm = 2 * (size_t)c.nph * sizeof(float2);
+  k_grid_to_fft_m<<<(unsigned)(c.nth * c.nr), 256, sm, c.stream>>>(p, c.L, grid, out, (const float2 *)c.d_tw_fft32);
 }
 
 template void fft_products<double>(Ctx &, const double *, double *);

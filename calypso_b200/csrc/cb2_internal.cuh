@@ -140,11 +140,46 @@ void rj_temp_total(Ctx &c, double sign);
 int rj_energies(Ctx &c, double out[7]);
 int rj_energies_scratch(Ctx &c, double *scratch, double out[7]);
 int rj_lu_factorise(Ctx &c);
+// Fourier coefficients of the mixed-precision path, order-major so that one
+// Legendre GEMM row is one contiguous element.  For nvec vectors + nscal
+// scalars, at each (m, theta):
+//   P block: nr * 2 (nvec + nscal) floats ordered (k, field, s): the r
+//            component of each vector, then each scalar;
+//   D block: nr * 4 nvec floats ordered (k, vector, {theta s=0, theta s=1,
+//            phi s=0, phi s=1});
+// s = 0 is the cos (order +m) coefficient, s = 1 the sin (order -m) one.
+// P[m][theta][...] sits at `P`, D[m][theta][...] at `D`.
+struct MLayout {
+  float *P = nullptr, *D = nullptr;
+  int nvec = 0, nscal = 0, nr = 0, nth = 0;
+  __host__ __device__ int rpP() const { return 2 * (nvec + nscal); }
+  __host__ __device__ int rpD() const { return 4 * nvec; }
+  __host__ __device__ size_t sP() const { return (size_t)nr * rpP(); }
+  __host__ __device__ size_t sD() const { return (size_t)nr * rpD(); }
+  // element of component c (vector v: 3v r, 3v+1 theta, 3v+2 phi; scalars
+  // after the vectors) at (m, theta, k), order sign s
+  __host__ __device__ float *at(int m, int th, int k, int c, int s) const {
+    if (c < 3 * nvec) {
+      const int v = c / 3, cc = c - 3 * v;
+      if (cc == 0) return P + ((size_t)m * nth + th) * sP() + (size_t)k * rpP() + 2 * v + s;
+      return D + ((size_t)m * nth + th) * sD() + (size_t)k * rpD() + 4 * v + 2 * (cc - 1) + s;
+    }
+    return P + ((size_t)m * nth + th) * sP() + (size_t)k * rpP() + 2 * (nvec + (c - 3 * nvec)) + s;
+  }
+};
+// layout over a float buffer of (L+1) * nth * nr * 2 * (3 nvec + nscal) floats
+MLayout mlayout(const Ctx &c, void *buf, int nvec, int nscal);
+
 // mixed-precision Legendre (cb2_legendre_mixed.cu)
 int mixed_setup(Ctx &c);
 void mixed_free(Ctx &c);
-void leg_bwd_mixed(Ctx &c, int nvec, int nscal, const int *slots, float *four);
-void leg_fwd_mixed(Ctx &c, int nvec, int nscal, const float *four, const int *slots);
+// slots: first rj slot of each vector, then of each scalar (out.nvec + out.nscal)
+void leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out);
+void leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots);
+// FFT and products of the mixed path (cb2_fft.cu), float32, order-major layouts
+void fft_products_m(Ctx &c, const MLayout &in, const MLayout &out);
+void fft_backward_grid_m(Ctx &c, const MLayout &in, double *grid);
+void fft_forward_grid_m(Ctx &c, const double *grid, const MLayout &out);
 
 // bits of the device status word d_status
 constexpr int CB2_STATUS_SINGULAR = 1;        // zero pivot in an LU factorisation

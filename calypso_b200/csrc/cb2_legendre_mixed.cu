@@ -59,7 +59,7 @@ namespace {
 constexpr int TM = 128;          // GEMM rows per CTA (= TMEM lanes)
 constexpr int KB = 64;           // K per pipeline stage: one 128-byte swizzle row of fp16
 constexpr int NSTAGE = 2;
-constexpr int NTHR = 128;
+constexpr int NTHR = 256;          // two threads per GEMM row
 constexpr int ACC1 = 256;        // TMEM column of the parity-1 accumulator
 constexpr uint32_t TMEM_COLS = 512;
 constexpr unsigned long long kWaitNs = 200ull * 1000 * 1000;   // 200 ms per wait
@@ -185,25 +185,38 @@ struct Smem {
   uint64_t full[NSTAGE], empty[NSTAGE], done;
   uint32_t tmem_base;
   int mma_any;
+  float rowmax[2][TM];
   float rowscale[TM];
 };
 
+// Order of the K blocks: both parities of block kb back to back (they read
+// the same operand rows), then the blocks only parity 0 has.  Needs
+// nkb0 >= nkb1, true for every gemm here.
+__device__ inline void block_of(int kbi, int nkb1, int &p, int &kb) {
+  if (kbi < 2 * nkb1) { p = kbi & 1; kb = kbi >> 1; }
+  else { p = 0; kb = nkb1 + (kbi - 2 * nkb1); }
+}
+
 // ---------------------------------------------------------------------------
 // The pipelined GEMM of one CTA, shared by the backward and forward kernels.
-// Prob supplies nkb(p) (K blocks of parity p), kvalid(p) (K extent with
-// non-zero A), kpad(p) (K extent the MMAs read), a(p, r, kk) (unscaled A of
-// tile row r), tma_xy(p, kb, x, y) (B box origin) and n(p) (MMA N).
+// Thread t works on tile row r = t % 128 and K half h = t / 128 (warps w and
+// w + 4 share TMEM lanes 32 (w % 4) ..).  Prob supplies
+//   nkb(p)                K blocks of parity p;
+//   kpad(p)               K extent the MMAs read (multiple of 16);
+//   n(p)                  MMA N (multiple of 16, <= 256);
+//   tma_xy(p, kb, x, y)   origin of the B box;
+//   absmax(r, h)          max |A| over half h of row r's values (both parities);
+//   fill(p, kb, r, h, s, hi, lo)  row r's K values 32 h .. 32 h + 31 of block
+//                         (p, kb), scaled by s, split and stored as four
+//                         16-byte chunks into the swizzled hi / lo tiles.
 template <class Prob>
 __device__ bool gemm_tile(const Prob &pr, Smem *sh, unsigned char *base, uint32_t b_rows,
                           const CUtensorMap *thi, const CUtensorMap *tlo, int *status) {
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int r = tid & (TM - 1), h = tid >> 7;
   const uint32_t A_BYTES = TM * 128, B_BYTES = b_rows * 128;
   const uint32_t STAGE = 2 * A_BYTES + 2 * B_BYTES;
-  const int nkb0 = pr.nkb(0), total = nkb0 + pr.nkb(1);
-  auto blk = [&](int kbi, int &p, int &kb) {
-    p = (kbi < nkb0) ? 0 : 1;
-    kb = p ? kbi - nkb0 : kbi;
-  };
+  const int nkb1 = pr.nkb(1), total = pr.nkb(0) + nkb1;
   if (tid == 0) {
     for (int s = 0; s < NSTAGE; s++) { mbar_init(&sh->full[s], 1); mbar_init(&sh->empty[s], 1); }
     mbar_init(&sh->done, 1);
@@ -216,25 +229,22 @@ __device__ bool gemm_tile(const Prob &pr, Smem *sh, unsigned char *base, uint32_
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   // per-row power-of-two scale over every K value of the row (both parities)
-  for (int r = warp; r < TM; r += NTHR / 32) {
-    float mx = 0.0f;
-    for (int p = 0; p < 2; p++)
-      for (int kk = lane; kk < pr.kvalid(p); kk += 32) mx = fmaxf(mx, fabsf(pr.a(p, r, kk)));
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) sh->rowscale[r] = pow2_scale(mx);
-  }
+  sh->rowmax[h][r] = pr.absmax(r, h);
+  __syncthreads();
+  if (h == 0) sh->rowscale[r] = pow2_scale(fmaxf(sh->rowmax[0][r], sh->rowmax[1][r]));
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sh->tmem_base;
+  const float sc = sh->rowscale[r];
 
-  uint32_t ph_full = 0, ph_empty = 0;   // phase parity of each stage's barrier, one bit per stage
-  int n_tma = 0, n_full = 0;   // thread 0: B stages requested / consumed
+  uint32_t ph_full = 0, ph_empty = 0;   // phase parity of each stage's barriers, one bit per stage
+  int n_tma = 0, n_full = 0;            // thread 0: B stages requested / consumed
   // fail fast once a wait has run out anywhere in this launch
   int failed = __syncthreads_or((*(volatile int *)status & CB2_STATUS_PIPE_TIMEOUT) != 0);
   auto issue_tma = [&](int kbi) {
     int p, kb, x, y;
-    blk(kbi, p, kb);
+    block_of(kbi, nkb1, p, kb);
     pr.tma_xy(p, kb, x, y);
     const int s = kbi % NSTAGE;
     unsigned char *st = base + s * STAGE;
@@ -245,7 +255,7 @@ __device__ bool gemm_tile(const Prob &pr, Smem *sh, unsigned char *base, uint32_
   if (tid == 0 && total > 0 && !failed) { issue_tma(0); n_tma = 1; }
   for (int kbi = 0; kbi < total && !failed; kbi++) {
     int p, kb;
-    blk(kbi, p, kb);
+    block_of(kbi, nkb1, p, kb);
     const int s = kbi % NSTAGE;
     unsigned char *st = base + s * STAGE;
     int f = 0;
@@ -261,27 +271,7 @@ __device__ bool gemm_tile(const Prob &pr, Smem *sh, unsigned char *base, uint32_
       if (!f) { issue_tma(kbi + 1); n_tma++; }
     }
     if (__syncthreads_or(f)) { failed = 1; break; }
-    // A tile of this block: 128 rows x 64 K, hi and lo, in 16-byte chunks
-    unsigned char *ahi = st, *alo = st + A_BYTES;
-    const int kv = pr.kvalid(p);
-    for (int c = tid; c < TM * (KB / 8); c += NTHR) {
-      const int r = c >> 3, ch = c & 7;
-      const float sc = sh->rowscale[r];
-      uint32_t h[4], l[4];
-#pragma unroll
-      for (int e = 0; e < 8; e += 2) {
-        const int kk = kb * KB + ch * 8 + e;
-        const float x0 = (kk < kv) ? pr.a(p, r, kk) * sc : 0.0f;
-        const float x1 = (kk + 1 < kv) ? pr.a(p, r, kk + 1) * sc : 0.0f;
-        const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
-        const __half l0 = __float2half_rn(x0 - __half2float(h0)), l1 = __float2half_rn(x1 - __half2float(h1));
-        h[e >> 1] = pack_half2(h0, h1);
-        l[e >> 1] = pack_half2(l0, l1);
-      }
-      const uint32_t off = sw128_chunk(r, ch);
-      *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-      *reinterpret_cast<uint4 *>(alo + off) = make_uint4(l[0], l[1], l[2], l[3]);
-    }
+    pr.fill(p, kb, r, h, sc, st, st + A_BYTES);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
@@ -294,7 +284,7 @@ __device__ bool gemm_tile(const Prob &pr, Smem *sh, unsigned char *base, uint32_
         const uint32_t acc = tmem + (uint32_t)(p * ACC1);
         const uint32_t idesc = idesc_f16_f32(TM, pr.n(p));
         const int nks = (min(KB, pr.kpad(p) - kb * KB) + 15) / 16;
-        const uint64_t dah = smem_desc_sw128(ahi), dal = smem_desc_sw128(alo);
+        const uint64_t dah = smem_desc_sw128(st), dal = smem_desc_sw128(st + A_BYTES);
         const uint64_t dbh = smem_desc_sw128(bhi), dbl = smem_desc_sw128(blo);
         for (int ks = 0; ks < nks; ks++) {
           const uint64_t o = (uint64_t)(ks * 2);   // +32 bytes along K
@@ -338,10 +328,24 @@ __device__ inline unsigned char *smem_base_1024(unsigned char *raw) {
   return (unsigned char *)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
 }
 
+// split 8 scaled values into fp16 hi / lo and store them as one 16-byte chunk each
+__device__ inline void store_chunk(unsigned char *hi, unsigned char *lo, int r, int ch, const float x[8]) {
+  uint32_t hh[4], ll[4];
+#pragma unroll
+  for (int e = 0; e < 8; e += 2) {
+    const __half h0 = __float2half_rn(x[e]), h1 = __float2half_rn(x[e + 1]);
+    hh[e >> 1] = pack_half2(h0, h1);
+    ll[e >> 1] = pack_half2(__float2half_rn(x[e] - __half2float(h0)), __float2half_rn(x[e + 1] - __half2float(h1)));
+  }
+  const uint32_t off = sw128_chunk(r, ch);
+  *reinterpret_cast<uint4 *>(hi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+  *reinterpret_cast<uint4 *>(lo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+}
+
 // ---------------------------------------------------------------------------
-// backward
+// backward: spectra f[slot][k][jj] -> order-major Fourier rows
 struct BwdArgs {
-  int L, nr, jmax, nh, nhp, NS, ncomp, nvec, nscal, nth;
+  int L, nr, jmax, nh, nhp, nth, nvec, nscal;
   int slot[8];
   const int *moff;
   const double *g3rlm, *ar1;
@@ -349,50 +353,105 @@ struct BwdArgs {
   size_t fs;
   const float *bunscale;          // [gemm][m][nhp] 1 / column scale of B
   const int *koff, *klen, *n1;    // per (m, group) K offset / length; dP part length
-  float *four;
+  MLayout out;
   int *status;
+};
+
+// One tile row of the backward gemms.  gemm P: row (k, field, s), value at
+// K index kk of parity p is f(l = m + p + 2 kk) (times l(l+1)/r^2 for a
+// vector).  gemm DM: row (k, vector, q); K = [dP part | mP part]:
+// dP part, l = m + (1-p) + 2 kk, value sd * X_d(l); mP part, l = m + p +
+// 2 (kk - n1), value sm * X_m(l), with X = (dS/dr)/r or T/r per q.
+struct BwdRow {
+  const double *xa = nullptr, *xb = nullptr;   // spectra at l = m (nullptr: zero)
+  const double *g3 = nullptr;                  // l(l+1) table at l = m (gemm P vectors)
+  double fa = 0.0, fb = 0.0;                   // factors incl. sign
 };
 
 struct BwdProb {
   const BwdArgs *A;
-  int m, g, nrows, row0;
+  int m, g, nrows, row0, nl;
   int kl[2], ko[2], n1[2];
   __device__ int nkb(int p) const { return (kl[p] + KB - 1) / KB; }
-  __device__ int kvalid(int p) const { return kl[p]; }
   __device__ int kpad(int p) const { return ((kl[p] + 15) / 16) * 16; }
   __device__ int n(int) const { return A->nhp; }
   __device__ void tma_xy(int p, int kb, int &x, int &y) const { x = ko[p] + kb * KB; y = 0; }
-  __device__ float a(int p, int r, int kk) const {
+
+  __device__ BwdRow row_src(int r) const {
     const BwdArgs &b = *A;
+    BwdRow w;
     const int row = row0 + r;
-    if (row >= nrows) return 0.0f;
+    if (row >= nrows) return w;
     if (g == 0) {
       const int ng = b.nvec + b.nscal, s = row & 1, v = (row >> 1) % ng, k = (row >> 1) / ng;
-      if (m == 0 && s == 1) return 0.0f;
-      const int l = m + p + 2 * kk;
-      const int jj = b.moff[m] + s * (b.L + 1 - m) + (l - m);
-      const size_t at = (size_t)k * b.jmax + jj;
+      if (m == 0 && s == 1) return w;
+      const int jjb = b.moff[m] + s * (b.L + 1 - m);
+      w.xa = b.f + (size_t)b.slot[v] * b.fs + (size_t)k * b.jmax + jjb;
       if (v < b.nvec) {
         const double ar = b.ar1[k];
-        return (float)(b.f[(size_t)b.slot[v] * b.fs + at] * ar * ar * b.g3rlm[jj]);
+        w.fa = ar * ar;
+        w.g3 = b.g3rlm + jjb;
+      } else {
+        w.fa = 1.0;
       }
-      return (float)b.f[(size_t)b.slot[v] * b.fs + at];
+      return w;
     }
-    const int q = row & 3, v = (row >> 2) % b.nvec, k = (row >> 2) / b.nvec;
-    const bool dpart = kk < n1[p];
-    const int l = dpart ? m + (1 - p) + 2 * kk : m + p + 2 * (kk - n1[p]);
     // dP part {D+, D-, -T+, -T-}; mP part {T-, -T+, D-, -D+}; comp 1 = dS/dr, 2 = T
-    int comp, s;
-    float sg;
-    if (dpart) {
-      comp = (q < 2) ? 1 : 2; s = q & 1; sg = (q < 2) ? 1.0f : -1.0f;
-    } else {
-      comp = (q < 2) ? 2 : 1; s = (q & 1) ^ 1; sg = (q & 1) ? -1.0f : 1.0f;
+    const int q = row & 3, v = (row >> 2) % b.nvec, k = (row >> 2) / b.nvec;
+    const double ar = b.ar1[k];
+    const int cd = (q < 2) ? 1 : 2, sd = q & 1, cm = (q < 2) ? 2 : 1, smm = (q & 1) ^ 1;
+    if (!(m == 0 && sd == 1)) {
+      w.xa = b.f + (size_t)(b.slot[v] + cd) * b.fs + (size_t)k * b.jmax + b.moff[m] + sd * (b.L + 1 - m);
+      w.fa = (q < 2) ? ar : -ar;
     }
-    if (m == 0 && s == 1) return 0.0f;
-    const int jj = b.moff[m] + s * (b.L + 1 - m) + (l - m);
-    const size_t at = (size_t)k * b.jmax + jj;
-    return sg * (float)(b.f[(size_t)(b.slot[v] + comp) * b.fs + at] * b.ar1[k]);
+    if (!(m == 0 && smm == 1)) {
+      w.xb = b.f + (size_t)(b.slot[v] + cm) * b.fs + (size_t)k * b.jmax + b.moff[m] + smm * (b.L + 1 - m);
+      w.fb = (q & 1) ? -ar : ar;
+    }
+    return w;
+  }
+
+  __device__ float absmax(int r, int h) const {
+    const BwdRow w = row_src(r);
+    const int half = (nl + 1) / 2, t0 = h * half, t1 = min(nl, t0 + half);
+    double mx = 0.0;
+    if (g == 0) {
+      if (w.xa)
+        for (int t = t0; t < t1; t++) mx = fmax(mx, fabs(w.xa[t] * (w.g3 ? w.g3[t] : 1.0)));
+      return (float)(mx * w.fa);
+    }
+    for (int t = t0; t < t1; t++) {
+      if (w.xa) mx = fmax(mx, fabs(w.xa[t] * w.fa));
+      if (w.xb) mx = fmax(mx, fabs(w.xb[t] * w.fb));
+    }
+    return (float)mx;
+  }
+
+  __device__ void fill(int p, int kb, int r, int h, float sc, unsigned char *hi, unsigned char *lo) const {
+    const BwdRow w = row_src(r);
+    const int kk0 = kb * KB + h * 32;
+    for (int c = 0; c < 4; c++) {
+      float x[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int kk = kk0 + c * 8 + e;
+        double v = 0.0;
+        if (kk < kl[p]) {
+          if (g == 0) {
+            if (w.xa) {
+              const int t = p + 2 * kk;
+              v = w.xa[t] * w.fa * (w.g3 ? w.g3[t] : 1.0);
+            }
+          } else if (kk < n1[p]) {
+            if (w.xa) v = w.xa[(1 - p) + 2 * kk] * w.fa;
+          } else {
+            if (w.xb) v = w.xb[p + 2 * (kk - n1[p])] * w.fb;
+          }
+        }
+        x[e] = (float)v * sc;
+      }
+      store_chunk(hi, lo, r, h * 4 + c, x);
+    }
   }
 };
 
@@ -409,6 +468,7 @@ k_leg_bwd_mixed(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int
   pr.g = (blockIdx.x < (unsigned)tiles_g0) ? 0 : 1;
   pr.nrows = pr.g ? rows_g1 : rows_g0;
   pr.row0 = (pr.g ? blockIdx.x - tiles_g0 : blockIdx.x) * TM;
+  pr.nl = a.L + 1 - pr.m;
   const int m = pr.m;
   for (int p = 0; p < 2; p++) {
     pr.kl[p] = a.klen[m * 4 + 2 * pr.g + p];
@@ -417,22 +477,18 @@ k_leg_bwd_mixed(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int
   }
   const bool ok = gemm_tile(pr, sh, base, BR, &tm_hi, &tm_lo, a.status);
   if (ok) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = warp * 32 + lane, row = pr.row0 + r;
-    int k, c, s;
-    if (pr.g == 0) {
-      const int ng = a.nvec + a.nscal, v = (row >> 1) % ng;
-      s = row & 1; k = (row >> 1) / ng;
-      c = (v < a.nvec) ? 3 * v : 3 * a.nvec + (v - a.nvec);
-    } else {
-      const int q = row & 3, v = (row >> 2) % a.nvec;
-      k = (row >> 2) / a.nvec; s = q & 1; c = 3 * v + 1 + (q >> 1);
-    }
+    // thread: tile row r (TMEM lane), columns (theta) of half h
+    const int warp = threadIdx.x >> 5;
+    const int r = threadIdx.x & (TM - 1), h = threadIdx.x >> 7, row = pr.row0 + r;
     const bool valid = row < pr.nrows;
     const float ua = 1.0f / sh->rowscale[r];
-    const uint32_t tl = sh->tmem_base + ((uint32_t)(warp * 32) << 16);
+    const uint32_t tl = sh->tmem_base + ((uint32_t)((warp & 3) * 32) << 16);
     const bool has1 = pr.kl[1] > 0;
-    for (int t0 = 0; t0 < (int)BR; t0 += 8) {
+    float *outb = pr.g ? a.out.D : a.out.P;
+    const size_t so = pr.g ? a.out.sD() : a.out.sP();
+    const float *bun = a.bunscale + ((size_t)pr.g * (a.L + 1) + m) * a.nhp;
+    const int half = (int)BR / 2;
+    for (int t0 = h * half; t0 < (h + 1) * half; t0 += 8) {
       float e[8], o[8];
       tmem_ld8(tl + (uint32_t)t0, e);
       if (has1) {
@@ -446,9 +502,9 @@ k_leg_bwd_mixed(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int
       for (int q = 0; q < 8; q++) {
         const int i = t0 + q;
         if (i < a.nh) {
-          const float us = ua * a.bunscale[((size_t)pr.g * (a.L + 1) + m) * a.nhp + i];
-          a.four[(((size_t)i * a.nr + k) * a.ncomp + c) * a.NS + 2 * m + s] = (e[q] + o[q]) * us;
-          a.four[(((size_t)(a.nth - 1 - i) * a.nr + k) * a.ncomp + c) * a.NS + 2 * m + s] = (e[q] - o[q]) * us;
+          const float us = ua * bun[i];
+          outb[((size_t)m * a.nth + i) * so + row] = (e[q] + o[q]) * us;
+          outb[((size_t)m * a.nth + (a.nth - 1 - i)) * so + row] = (e[q] - o[q]) * us;
         }
       }
     }
@@ -457,13 +513,14 @@ k_leg_bwd_mixed(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int
 }
 
 // ---------------------------------------------------------------------------
-// forward
+// forward: order-major Fourier rows -> spectra f[slot][k][jj]
 struct FwdArgs {
-  int L, nr, jmax, nh, nhp, NS, ncomp, nvec, nscal, nth, NFmax;
+  int L, nr, jmax, nh, nhp, nth, nvec, nscal, NFmax;
   int slot[8];
   const int *moff;
-  const double *g6, *g7, *r, *wgt;
-  const float *four;
+  const double *g6, *g7, *r;
+  const float *wgt;      // Gauss weights (float)
+  MLayout in;
   double *f;
   size_t fs;
   const float *bunscale; // [gemm][(m, parity)][NFmax] 1 / column scale of B
@@ -471,48 +528,79 @@ struct FwdArgs {
   int *status;
 };
 
+// One tile row of the forward gemms.  gemm P: row (k, field, s) = element
+// `row` of the P block at every theta; value at south node i =
+// sym (p = 0) or anti (p = 1) of f w.  gemm DM: row (k, vector, q) with
+// K = [dP part (theta i) | mP part (theta i)]; dP part reads element `row`
+// of the D block with sign sd and fold 1-p, mP part element row - q + 3 - q
+// with sign sm and fold p:
+//   dS+ = [theta+ | -phi-], dS- = [theta- | +phi+],
+//   T+  = [-phi+ | -theta-], T- = [-phi- | +theta+].
 struct FwdProb {
   const FwdArgs *A;
   int m, g, nrows, row0, K;
   int np[2], ro[2];
   __device__ int nkb(int p) const { return np[p] > 0 ? (K + KB - 1) / KB : 0; }
-  __device__ int kvalid(int) const { return K; }
   __device__ int kpad(int) const { return K; }
   __device__ int n(int p) const { return ((np[p] + 15) / 16) * 16; }
   __device__ void tma_xy(int p, int kb, int &x, int &y) const { x = kb * KB; y = ro[p]; }
-  // f(theta_i) w_i of grid component c, order sign s
-  __device__ float fw(int i, int k, int c, int s) const {
-    const FwdArgs &b = *A;
-    return b.four[(((size_t)i * b.nr + k) * b.ncomp + c) * b.NS + 2 * m + s] * (float)b.wgt[i];
-  }
-  __device__ float a(int p, int r, int kk) const {
+
+  // pointers to the element of this row at theta = 0 (nullptr: row outside the gemm)
+  __device__ const float *src(int r, int part) const {
     const FwdArgs &b = *A;
     const int row = row0 + r;
-    if (row >= nrows) return 0.0f;
-    if (g == 0) {
-      const int ng = b.nvec + b.nscal, s = row & 1, v = (row >> 1) % ng, k = (row >> 1) / ng;
-      if (kk >= b.nh || (m == 0 && s == 1)) return 0.0f;
-      const int c = (v < b.nvec) ? 3 * v : 3 * b.nvec + (v - b.nvec);
-      const float fa = fw(kk, k, c, s), fb = fw(b.nth - 1 - kk, k, c, s);
-      return p ? fa - fb : fa + fb;
+    if (row >= nrows) return nullptr;
+    if (g == 0) return b.in.P + (size_t)m * b.nth * b.in.sP() + row;
+    const int q = row & 3;
+    return b.in.D + (size_t)m * b.nth * b.in.sD() + (part ? row - q + 3 - q : row);
+  }
+  __device__ size_t stride() const { return g ? A->in.sD() : A->in.sP(); }
+
+  __device__ float absmax(int r, int h) const {
+    const FwdArgs &b = *A;
+    const size_t st = stride();
+    const int half = (b.nh + 1) / 2, i0 = h * half, i1 = min(b.nh, i0 + half);
+    float mx = 0.0f;
+    for (int part = 0; part < (g ? 2 : 1); part++) {
+      const float *s0 = src(r, part);
+      if (!s0) continue;
+      for (int i = i0; i < i1; i++) {
+        const float fa = s0[(size_t)i * st] * b.wgt[i];
+        const float fb = s0[(size_t)(b.nth - 1 - i) * st] * b.wgt[b.nth - 1 - i];
+        mx = fmaxf(mx, fabsf(fa) + fabsf(fb));
+      }
     }
-    const int q = row & 3, v = (row >> 2) % b.nvec, k = (row >> 2) / b.nvec;
-    const bool dpart = kk < b.nhp;
-    const int i = dpart ? kk : kk - b.nhp;
-    if (i >= b.nh) return 0.0f;
-    // dS+ = [theta+ (fold 1-p) | -phi- (fold p)], dS- = [theta- | +phi+],
-    // T+  = [-phi+ (fold 1-p) | -theta- (fold p)], T- = [-phi- | +theta+]
-    int comp, s, sigma;
-    float sg;
-    if (dpart) {
-      comp = (q < 2) ? 1 : 2; s = q & 1; sg = (q < 2) ? 1.0f : -1.0f; sigma = 1 - p;
-    } else {
-      comp = (q < 2) ? 2 : 1; s = (q & 1) ^ 1; sg = (q & 1) ? 1.0f : -1.0f; sigma = p;
+    return mx;
+  }
+
+  __device__ void fill(int p, int kb, int r, int h, float sc, unsigned char *hi, unsigned char *lo) const {
+    const FwdArgs &b = *A;
+    const size_t st = stride();
+    const int row = row0 + r;
+    const int q = row & 3;
+    const float *s0 = src(r, 0), *s1 = g ? src(r, 1) : nullptr;
+    const float sd = (g == 0 || q < 2) ? sc : -sc;
+    const float sm = (q & 1) ? sc : -sc;
+    const int kk0 = kb * KB + h * 32;
+    for (int c = 0; c < 4; c++) {
+      float x[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int kk = kk0 + c * 8 + e;
+        float v = 0.0f;
+        const bool dpart = (g == 0) || kk < b.nhp;
+        const int i = dpart ? kk : kk - b.nhp;
+        const float *s = dpart ? s0 : s1;
+        if (s && i < b.nh) {
+          const int ii = b.nth - 1 - i;
+          const float fa = s[(size_t)i * st] * b.wgt[i], fb = s[(size_t)ii * st] * b.wgt[ii];
+          const int sigma = (g == 0) ? p : (dpart ? 1 - p : p);
+          v = (sigma ? fa - fb : fa + fb) * (dpart ? sd : sm);
+        }
+        x[e] = v;
+      }
+      store_chunk(hi, lo, r, h * 4 + c, x);
     }
-    if (m == 0 && s == 1) return 0.0f;
-    const int c = 3 * v + comp;
-    const float fa = fw(i, k, c, s), fb = fw(b.nth - 1 - i, k, c, s);
-    return sg * (sigma ? fa - fb : fa + fb);
   }
 };
 
@@ -538,8 +626,8 @@ k_leg_fwd_mixed(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int
   }
   const bool ok = gemm_tile(pr, sh, base, BR, pr.g ? &tmd_hi : &tmp_hi, pr.g ? &tmd_lo : &tmp_lo, a.status);
   if (ok) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = warp * 32 + lane, row = pr.row0 + r;
+    const int warp = threadIdx.x >> 5;
+    const int r = threadIdx.x & (TM - 1), h = threadIdx.x >> 7, row = pr.row0 + r;
     int k, slot, kind, s;   // kind 0: S (g7 r^2), 1: dS or T (g7 r), 2: scalar (g6)
     if (pr.g == 0) {
       const int ng = a.nvec + a.nscal, v = (row >> 1) % ng;
@@ -552,22 +640,25 @@ k_leg_fwd_mixed(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int
     }
     const bool valid = row < pr.nrows && !(m == 0 && s == 1);
     const double ua = 1.0 / (double)sh->rowscale[r];
-    const uint32_t tl = sh->tmem_base + ((uint32_t)(warp * 32) << 16);
+    const uint32_t tl = sh->tmem_base + ((uint32_t)((warp & 3) * 32) << 16);
     const double rk = valid ? a.r[k] : 0.0;
+    const int jjb = a.moff[m] + s * (a.L + 1 - m);
+    double *dst = a.f + (size_t)slot * a.fs + (size_t)k * a.jmax + jjb;
     for (int p = 0; p < 2; p++) {
-      for (int c0 = 0; c0 < pr.np[p]; c0 += 8) {
+      const float *bun = a.bunscale + ((size_t)pr.g * (a.L + 1) * 2 + m * 2 + p) * a.NFmax;
+      const int nch = (pr.np[p] + 7) / 8;
+      for (int c8 = h; c8 < nch; c8 += 2) {
         float v8[8];
-        tmem_ld8(tl + (uint32_t)(p * ACC1 + c0), v8);
+        tmem_ld8(tl + (uint32_t)(p * ACC1 + c8 * 8), v8);
         if (!valid) continue;
 #pragma unroll
         for (int q = 0; q < 8; q++) {
-          const int t = c0 + q;
+          const int t = c8 * 8 + q;
           if (t < pr.np[p]) {
-            const int l = m + p + 2 * t;
-            const int jj = a.moff[m] + s * (a.L + 1 - m) + (l - m);
-            const double us = ua * (double)a.bunscale[((size_t)pr.g * (a.L + 1) * 2 + m * 2 + p) * a.NFmax + t];
-            const double fac = (kind == 0) ? a.g7[jj] * rk * rk : (kind == 2) ? a.g6[jj] : a.g7[jj] * rk;
-            a.f[(size_t)slot * a.fs + (size_t)k * a.jmax + jj] = (double)v8[q] * us * fac;
+            const int lm = p + 2 * t;   // l - m
+            const double fac = (kind == 0) ? a.g7[jjb + lm] * rk * rk
+                             : (kind == 2) ? a.g6[jjb + lm] : a.g7[jjb + lm] * rk;
+            dst[lm] = (double)v8[q] * (ua * (double)bun[t]) * fac;
           }
         }
       }
@@ -665,6 +756,7 @@ struct MixedTables {
   __half *bfd_hi = nullptr, *bfd_lo = nullptr;    // forward B (DM) [rows_all][2 nhp]
   float *bf_unscale = nullptr;                    // [gemm][(m, parity)][NFmax]
   int *bf_roff = nullptr, *bf_nl = nullptr;
+  float *wgt32 = nullptr;                         // Gauss weights in float
   int Kb_all = 0, rows_all = 0, nhp = 0, NFmax = 0;
   size_t smem_bwd = 0, smem_fwd = 0;
   CUtensorMap tm_bb_hi, tm_bb_lo, tm_bfp_hi, tm_bfp_lo, tm_bfd_hi, tm_bfd_lo;
@@ -771,6 +863,11 @@ int mixed_setup(Ctx &c) {
   CB2_CUDA(cudaMemsetAsync(t->bb_unscale, 0, nbs * sizeof(float), c.stream));
   CB2_CUDA(cudaMalloc(&t->bf_unscale, nfs * sizeof(float)));
   CB2_CUDA(cudaMemsetAsync(t->bf_unscale, 0, nfs * sizeof(float), c.stream));
+  {
+    std::vector<float> w(c.h_wgt.begin(), c.h_wgt.end());
+    CB2_CUDA(cudaMalloc(&t->wgt32, w.size() * sizeof(float)));
+    CB2_CUDA(cudaMemcpy(t->wgt32, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
   k_build_bwd_b<<<dim3(cdiv(nh, 64), L + 1), 64, 0, c.stream>>>(L, nh, t->nhp, c.d_poff, c.d_Plt, c.d_dPlt,
                                                                 c.d_asin, t->bb_koff, t->bb_klen, t->bb_n1,
                                                                 t->Kb_all, t->bb_unscale, t->bb_hi, t->bb_lo);
@@ -802,36 +899,46 @@ void mixed_free(Ctx &c) {
   MixedTables *t = (MixedTables *)c.mixed;
   if (!t) return;
   void *ptrs[] = {t->bb_hi, t->bb_lo, t->bb_unscale, t->bb_koff, t->bb_klen, t->bb_n1, t->bfp_hi,
-                  t->bfp_lo, t->bfd_hi, t->bfd_lo, t->bf_unscale, t->bf_roff, t->bf_nl};
+                  t->bfp_lo, t->bfd_hi, t->bfd_lo, t->bf_unscale, t->bf_roff, t->bf_nl, t->wgt32};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete t;
   c.mixed = nullptr;
 }
 
-void leg_bwd_mixed(Ctx &c, int nvec, int nscal, const int *slots, float *four) {
+MLayout mlayout(const Ctx &c, void *buf, int nvec, int nscal) {
+  MLayout l;
+  l.nvec = nvec; l.nscal = nscal; l.nr = c.nr; l.nth = c.nth;
+  l.P = static_cast<float *>(buf);
+  l.D = l.P + (size_t)(c.L + 1) * c.nth * l.sP();
+  return l;
+}
+
+void leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   MixedTables *t = (MixedTables *)c.mixed;
+  const int nvec = out.nvec, nscal = out.nscal;
   BwdArgs a{};
-  a.L = c.L; a.nr = c.nr; a.jmax = c.jmax; a.nh = c.nh; a.nhp = t->nhp; a.NS = c.NS;
-  a.ncomp = 3 * nvec + nscal; a.nvec = nvec; a.nscal = nscal; a.nth = c.nth;
+  a.L = c.L; a.nr = c.nr; a.jmax = c.jmax; a.nh = c.nh; a.nhp = t->nhp; a.nth = c.nth;
+  a.nvec = nvec; a.nscal = nscal;
   for (int q = 0; q < nvec + nscal && q < 8; q++) a.slot[q] = slots[q];
   a.moff = c.d_moff; a.g3rlm = c.d_g3rlm; a.ar1 = c.d_ar1; a.f = c.d_f; a.fs = c.fsize();
   a.bunscale = t->bb_unscale; a.koff = t->bb_koff; a.klen = t->bb_klen; a.n1 = t->bb_n1;
-  a.four = four; a.status = c.d_status;
+  a.out = out; a.status = c.d_status;
   const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
   k_leg_bwd_mixed<<<dim3(tiles0 + tiles1, c.L + 1), NTHR, t->smem_bwd, c.stream>>>(a, rows0, rows1, tiles0,
                                                                                   t->tm_bb_hi, t->tm_bb_lo);
 }
 
-void leg_fwd_mixed(Ctx &c, int nvec, int nscal, const float *four, const int *slots) {
+void leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots) {
   MixedTables *t = (MixedTables *)c.mixed;
+  const int nvec = in.nvec, nscal = in.nscal;
   FwdArgs a{};
-  a.L = c.L; a.nr = c.nr; a.jmax = c.jmax; a.nh = c.nh; a.nhp = t->nhp; a.NS = c.NS;
-  a.ncomp = 3 * nvec + nscal; a.nvec = nvec; a.nscal = nscal; a.nth = c.nth; a.NFmax = t->NFmax;
+  a.L = c.L; a.nr = c.nr; a.jmax = c.jmax; a.nh = c.nh; a.nhp = t->nhp; a.nth = c.nth; a.NFmax = t->NFmax;
+  a.nvec = nvec; a.nscal = nscal;
   for (int q = 0; q < nvec + nscal && q < 8; q++) a.slot[q] = slots[q];
-  a.moff = c.d_moff; a.g6 = c.d_g6; a.g7 = c.d_g7; a.r = c.d_r; a.wgt = c.d_wgt;
-  a.four = four; a.f = c.d_f; a.fs = c.fsize();
+  a.moff = c.d_moff; a.g6 = c.d_g6; a.g7 = c.d_g7; a.r = c.d_r; a.wgt = t->wgt32;
+  a.in = in; a.f = c.d_f; a.fs = c.fsize();
   a.bunscale = t->bf_unscale; a.roff = t->bf_roff; a.nlp = t->bf_nl;
   a.status = c.d_status;
   const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
