@@ -133,11 +133,12 @@ static int nonlinear(Ctx &c) {
     leg_fwd_f64(c, 4, 0, (const double *)c.d_four2, fslots);
   } else {
     const MLayout fin = mlayout(c, c.d_four, 4, 1), fout = mlayout(c, c.d_four2, 4, 0);
-    leg_bwd_mixed(c, bslots, fin);
+    int rc = leg_bwd_mixed(c, bslots, fin);
+    if (rc) return rc;
     if (c.timers) cudaEventRecord(c.ev[12], c.stream);
     fft_products_m(c, fin, fout);
     if (c.timers) cudaEventRecord(c.ev[13], c.stream);
-    leg_fwd_mixed(c, fout, fslots);
+    if ((rc = leg_fwd_mixed(c, fout, fslots))) return rc;
   }
   if (c.timers) cudaEventRecord(c.ev[14], c.stream);
   rj_after_transform(c);
@@ -157,10 +158,10 @@ static int one_step(Ctx &c) {
   if (c.timers) cudaEventRecord(c.ev[1], c.stream);
   rj_implicit(c);
   if (c.timers) cudaEventRecord(c.ev[2], c.stream);
-  nonlinear(c);
+  int rc = nonlinear(c);
   temp_roundtrip(c);
   if (c.timers) cudaEventRecord(c.ev[3], c.stream);
-  return 0;
+  return rc;
 }
 
 static void accumulate_timers(Ctx &c) {
@@ -251,10 +252,13 @@ int cb2_create(const cb2_params *p, int precision, int device, cb2_ctx **out) {
   if (cudaMalloc(&c->d_f, (size_t)NSLOT * fs * sizeof(double)) != cudaSuccess)
     return fail(cuda_fail(cudaGetLastError(), "cudaMalloc(fields)"));
   cudaMemsetAsync(c->d_f, 0, (size_t)NSLOT * fs * sizeof(double), c->stream);
-  size_t es = (precision == CB2_PREC_FP64) ? sizeof(double) : sizeof(float);
   size_t rows = (size_t)c->nth * c->nr * c->NS;
-  if (cudaMalloc(&c->d_four, rows * 13 * es) != cudaSuccess ||
-      cudaMalloc(&c->d_four2, rows * 12 * es) != cudaSuccess ||
+  // float64 rows [theta][k][c][s] (13 and 12 components), or the padded
+  // order-major float32 layout of the mixed path
+  const size_t b1 = (precision == CB2_PREC_FP64) ? rows * 13 * sizeof(double) : mlayout_floats(*c) * sizeof(float);
+  const size_t b2 = (precision == CB2_PREC_FP64) ? rows * 12 * sizeof(double) : mlayout_floats(*c) * sizeof(float);
+  if (cudaMalloc(&c->d_four, b1) != cudaSuccess ||
+      cudaMalloc(&c->d_four2, b2) != cudaSuccess ||
       cudaMalloc(&c->d_ene, (7 * (size_t)c->jmax + 16) * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->d_tmp, fs * sizeof(double)) != cudaSuccess)
     return fail(cuda_fail(cudaGetLastError(), "cudaMalloc(work)"));
@@ -335,7 +339,8 @@ int cb2_init_fields(cb2_ctx *c, int kind, unsigned seed) {
 int cb2_start(cb2_ctx *c) {
   if (!c) return CB2_ERR_ARG;
   rj_start_derived(*c);
-  nonlinear(*c);
+  int rc = nonlinear(*c);
+  if (rc) return rc;
   CB2_CUDA(cudaGetLastError());
   CB2_CUDA(cudaStreamSynchronize(c->stream));
   c->istep = 0;
@@ -348,7 +353,8 @@ int cb2_step(cb2_ctx *c, int nsteps) {
   if (!c->started) { set_error("cb2_step before cb2_start / cb2_init_fields"); return CB2_ERR_STATE; }
   if (c->timers) for (int i = 0; i < 32; i++) c->stage_ms[i] = 0.0;
   for (int s = 0; s < nsteps; s++) {
-    one_step(*c);
+    int rc = one_step(*c);
+    if (rc) return rc;
     if (c->timers) accumulate_timers(*c);
   }
   CB2_CUDA(cudaGetLastError());
@@ -361,7 +367,8 @@ int cb2_step_graph(cb2_ctx *c, int nsteps) {
   // the first step is an Euler step and not captured
   int done = 0;
   if (c->istep == 0 && nsteps > 0) {
-    one_step(*c);
+    int rc = one_step(*c);
+    if (rc) return rc;
     done = 1;
   }
   if (done == nsteps) return 0;
@@ -371,9 +378,15 @@ int cb2_step_graph(cb2_ctx *c, int nsteps) {
     cudaGraph_t g;
     CB2_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int save = c->istep;
-    one_step(*c);
+    int rc = one_step(*c);
     c->istep = save;
-    CB2_CUDA(cudaStreamEndCapture(c->stream, &g));
+    cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    if (rc) {
+      if (ec == cudaSuccess) cudaGraphDestroy(g);
+      c->timers = tm;
+      return rc;
+    }
+    if (ec != cudaSuccess) return cuda_fail(ec, "cudaStreamEndCapture");
     CB2_CUDA(cudaGraphInstantiate(&c->graph_exec, g, 0));
     cudaGraphDestroy(g);
     c->timers = tm;
@@ -485,7 +498,7 @@ int cb2_step_host_state(cb2_ctx *c, double *state, double out_energies[7]) {
     k_to_device_order<<<cdiv(n, 256), 256, 0, c->stream>>>(c->nr, c->jmax, c->d_perm,
                                                              c->d_host_state + q * n, c->fld(kHostStateSlots[q]));
   if (c->istep == 0) c->istep = 1;   // the loaded history makes this an Adams-Bashforth step
-  one_step(*c);
+  if (int rc = one_step(*c)) return rc;
   for (int q = 0; q < 20; q++)
     k_to_host_order<<<cdiv(n, 256), 256, 0, c->stream>>>(c->nr, c->jmax, c->d_perm,
                                                          c->fld(kHostStateSlots[q]), c->d_host_state + q * n);
@@ -526,7 +539,7 @@ int cb2_sht_backward(cb2_ctx *c, int nvec, int nscal, const double *spec, double
     fft_backward_grid<double>(*c, nc, (const double *)c->d_four, dgrid);
   } else {
     const MLayout l = mlayout(*c, c->d_four, nvec, nscal);
-    leg_bwd_mixed(*c, slots, l);
+    if ((rc = leg_bwd_mixed(*c, slots, l))) { cudaFree(dgrid); return rc; }
     fft_backward_grid_m(*c, l, dgrid);
   }
   CB2_CUDA(cudaGetLastError());
@@ -553,7 +566,7 @@ int cb2_sht_forward(cb2_ctx *c, int nvec, int nscal, const double *grid, double 
   } else {
     const MLayout l = mlayout(*c, c->d_four, nvec, nscal);
     fft_forward_grid_m(*c, dgrid, l);
-    leg_fwd_mixed(*c, l, slots);
+    if ((rc = leg_fwd_mixed(*c, l, slots))) { cudaFree(dgrid); return rc; }
   }
   CB2_CUDA(cudaGetLastError());
   CB2_CUDA(cudaStreamSynchronize(c->stream));

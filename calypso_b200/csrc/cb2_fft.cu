@@ -423,6 +423,202 @@ k_fft_products_m(FFTPlan pl, int L, MLayout fin, MLayout fout, const float2 *__r
   }
 }
 
+// ---------------------------------------------------------------------------
+// Compile-time FFT passes for N = 3 * 2^b (the zonal grids 96 .. 768 that
+// the shells use): radix 3 first, then radix 4, a final radix 2 when b is
+// odd.  With N and the radices known at compile time every index division
+// is by a constant, and the twiddle table sits in shared memory.
+template <int N>
+struct Plan3x2 {
+  static constexpr int nst() {
+    int n = N / 3, s = 1;
+    while (n % 4 == 0) { n /= 4; s++; }
+    if (n == 2) s++;
+    return s;
+  }
+  static constexpr int radix(int st) {
+    if (st == 0) return 3;
+    int n = N / 3;
+    for (int q = 1; q < st; q++) n /= 4;
+    return (n % 4 == 0) ? 4 : 2;
+  }
+  static constexpr int ns(int st) {   // product of the radices before stage st
+    int p = 1;
+    for (int q = 0; q < st; q++) p *= radix(q);
+    return p;
+  }
+  // stage st reads its twiddles w^(r k), r = 1..R-1, k = 0..NS-1, from
+  // entries off(st) + (r-1) NS + k of one table (contiguous in k, so a
+  // warp's reads never collide in a bank)
+  static constexpr int off(int st) {
+    int o = 0;
+    for (int q = 0; q < st; q++) o += (radix(q) - 1) * ns(q);
+    return o;
+  }
+  static constexpr int ntw() { return off(nst()); }
+};
+
+template <int N, int R, int NS, int NF, int SIGN>
+__device__ __forceinline__ void fft_pass(const float2 *__restrict__ x, float2 *__restrict__ y,
+                                         const float2 *__restrict__ tw) {
+  constexpr int NB = N / R;
+  const float s32 = 0.86602540378443864676f;   // sin(pi/3) = sqrt(3)/2
+  for (int idx = threadIdx.x; idx < NF * NB; idx += blockDim.x) {
+    const int f = idx / NB, j = idx - f * NB;
+    const int k = j % NS;
+    const float2 *xf = x + f * N;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      float2 a = xf[j + r * NB];
+      if (NS > 1 && r > 0) {
+        float2 w = tw[(r - 1) * NS + k];
+        if (SIGN > 0) w.y = -w.y;
+        a = float2{a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x};
+      }
+      v[r] = a;
+    }
+    float2 o[R];
+    if constexpr (R == 4) {
+      const float2 a0{v[0].x + v[2].x, v[0].y + v[2].y}, a1{v[0].x - v[2].x, v[0].y - v[2].y};
+      const float2 a2{v[1].x + v[3].x, v[1].y + v[3].y};
+      const float dx = v[1].x - v[3].x, dy = v[1].y - v[3].y;
+      const float2 a3 = (SIGN < 0) ? float2{dy, -dx} : float2{-dy, dx};
+      o[0] = float2{a0.x + a2.x, a0.y + a2.y};
+      o[1] = float2{a1.x + a3.x, a1.y + a3.y};
+      o[2] = float2{a0.x - a2.x, a0.y - a2.y};
+      o[3] = float2{a1.x - a3.x, a1.y - a3.y};
+    } else if constexpr (R == 2) {
+      o[0] = float2{v[0].x + v[1].x, v[0].y + v[1].y};
+      o[1] = float2{v[0].x - v[1].x, v[0].y - v[1].y};
+    } else {
+      const float2 t1{v[1].x + v[2].x, v[1].y + v[2].y};
+      const float2 t2{v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y};
+      const float dx = v[1].x - v[2].x, dy = v[1].y - v[2].y;
+      const float2 t3 = (SIGN < 0) ? float2{s32 * dy, -s32 * dx} : float2{-s32 * dy, s32 * dx};
+      o[0] = float2{v[0].x + t1.x, v[0].y + t1.y};
+      o[1] = float2{t2.x + t3.x, t2.y + t3.y};
+      o[2] = float2{t2.x - t3.x, t2.y - t3.y};
+    }
+    float2 *yf = y + f * N;
+    const int d = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) yf[d + r * NS] = o[r];
+  }
+  __syncthreads();
+}
+
+// all stages from `st` on; the result ends in x when the remaining stage
+// count is even, in y otherwise (returned)
+template <int N, int NF, int SIGN, int ST>
+__device__ __forceinline__ float2 *fft_passes(float2 *x, float2 *y, const float2 *tw) {
+  using P = Plan3x2<N>;
+  if constexpr (ST >= P::nst()) {
+    return x;
+  } else {
+    fft_pass<N, P::radix(ST), P::ns(ST), NF, SIGN>(x, y, tw + P::off(ST));
+    return fft_passes<N, NF, SIGN, ST + 1>(y, x, tw);
+  }
+}
+
+// The fused row kernel for N = 3 * 2^b (see k_fft_products_m for the data
+// flow).  Staging rows are padded to an odd stride so the transposes between
+// the (m, element) order of HBM and the (element, m) order of the FFT rows
+// are free of bank conflicts.
+template <int N>
+__global__ void __launch_bounds__(512, 2)
+k_fft_products_t(int L, MLayout fin, MLayout fout, const float2 *__restrict__ twg, ProdCoef pc) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *A = reinterpret_cast<float2 *>(smraw);   // 7 x N
+  float2 *B = A + 7 * N;                            // 7 x N
+  float2 *TW = B + 7 * N;                           // N
+  const int M1 = L + 1, MP = M1 | 1;                // padded (odd) staging stride
+  float *S = reinterpret_cast<float *>(B);          // [c * 2 + s][MP]
+  const int th = blockIdx.x / fin.nr, k = blockIdx.x % fin.nr;
+  using P = Plan3x2<N>;
+  static_assert(P::ntw() <= N, "twiddle table");
+  for (int e = threadIdx.x; e < P::ntw(); e += blockDim.x) {
+    int st = 0;
+    while (st + 1 < P::nst() && e >= P::off(st + 1)) st++;
+    const int NS = P::ns(st), loc = e - P::off(st), r = 1 + loc / NS, kk = loc - (r - 1) * NS;
+    TW[e] = twg[r * kk * (N / (NS * P::radix(st)))];
+  }
+  const float *Pin = fin.P + (size_t)th * fin.sP() + (size_t)k * 10;
+  const float *Din = fin.D + (size_t)th * fin.sD() + (size_t)k * 16;
+  const size_t mstP = (size_t)fin.nth * fin.sP(), mstD = (size_t)fin.nth * fin.sD();
+  for (int idx = threadIdx.x; idx < 26 * M1; idx += blockDim.x) {
+    const int m = idx / 26, j = idx - 26 * m;
+    int c, s;
+    m_comp_of_in(j, c, s);
+    S[(c * 2 + s) * MP + m] = (j < 10) ? __ldg(Pin + m * mstP + j) : __ldg(Din + m * mstD + (j - 10));
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < 7 * N; idx += blockDim.x) {
+    const int p = idx / N, n = idx - p * N;
+    const int c0 = 2 * p, c1 = 2 * p + 1;
+    const bool has1 = c1 < 13;
+    float2 z{0.0f, 0.0f};
+    const int m = (n <= L) ? n : ((N - n <= L) ? N - n : -1);
+    if (n == 0) {
+      z = float2{S[(c0 * 2) * MP], has1 ? S[(c1 * 2) * MP] : 0.0f};
+    } else if (m > 0) {
+      const float a0 = S[(c0 * 2) * MP + m], b0 = S[(c0 * 2 + 1) * MP + m];
+      const float a1 = has1 ? S[(c1 * 2) * MP + m] : 0.0f, b1 = has1 ? S[(c1 * 2 + 1) * MP + m] : 0.0f;
+      const float xr = 0.5f * a0, xi = -0.5f * b0, yr = 0.5f * a1, yi = -0.5f * b1;
+      z = (m == n) ? float2{xr - yi, xi + yr} : float2{xr + yi, -xi + yr};
+    }
+    A[idx] = z;
+  }
+  __syncthreads();
+  float2 *g = fft_passes<N, 7, +1, 0>(A, B, TW);
+  float2 *hb = (g == A) ? B : A;
+  const float cv = (float)pc.cv, cl = (float)pc.cl, ci = (float)pc.ci, ct = (float)pc.ct;
+  for (int q = threadIdx.x; q < N; q += blockDim.x) {
+    const float2 p0 = g[0 * N + q], p1 = g[1 * N + q], p2 = g[2 * N + q], p3 = g[3 * N + q];
+    const float2 p4 = g[4 * N + q], p5 = g[5 * N + q], p6 = g[6 * N + q];
+    const float ur = p0.x, ut = p0.y, up = p1.x, wr = p1.y, wt = p2.x, wp = p2.y;
+    const float br = p3.x, bt = p3.y, bp = p4.x, jr = p4.y, jt = p5.x, jp = p5.y, tt = p6.x;
+    hb[0 * N + q] = float2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv};
+    hb[1 * N + q] = float2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl};
+    hb[2 * N + q] = float2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl};
+    hb[3 * N + q] = float2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci};
+    hb[4 * N + q] = float2{(ur * bt - ut * br) * ci, ur * tt * ct};
+    hb[5 * N + q] = float2{ut * tt * ct, up * tt * ct};
+  }
+  __syncthreads();
+  float2 *zf = fft_passes<N, 6, -1, 0>(hb, g, TW);
+  // (a_m, b_m) of the 12 outputs into the staging rows O[j][MP] (lanes over m),
+  // then one contiguous run per m to HBM (lanes over j)
+  float *O = reinterpret_cast<float *>((zf == A) ? B : A);
+  const float an = 1.0f / (float)N;
+  for (int idx = threadIdx.x; idx < 24 * M1; idx += blockDim.x) {
+    const int j = idx / M1, m = idx - j * M1;
+    int c, s;
+    m_comp_of_out(j, c, s);
+    const float2 *Z = zf + (c >> 1) * N;
+    const bool isy = c & 1;
+    float v;
+    if (m == 0) {
+      v = (s == 0) ? an * (isy ? Z[0].y : Z[0].x) : 0.0f;
+    } else {
+      const float2 zk = Z[m], zn = Z[N - m];
+      if (!isy) v = (s == 0) ? an * (zk.x + zn.x) : -an * (zk.y - zn.y);
+      else v = (s == 0) ? an * (zk.y + zn.y) : an * (zk.x - zn.x);
+    }
+    O[j * MP + m] = v;
+  }
+  __syncthreads();
+  float *Pout = fout.P + (size_t)th * fout.sP() + (size_t)k * 8;
+  float *Dout = fout.D + (size_t)th * fout.sD() + (size_t)k * 16;
+  const size_t oP = (size_t)fout.nth * fout.sP(), oD = (size_t)fout.nth * fout.sD();
+  for (int idx = threadIdx.x; idx < 24 * M1; idx += blockDim.x) {
+    const int m = idx / 24, j = idx - 24 * m;
+    const float v = O[j * MP + m];
+    if (j < 8) Pout[m * oP + j] = v;
+    else Dout[m * oD + (j - 8)] = v;
+  }
+}
+
 // order-major Fourier rows -> grid (float64), for the standalone transform API
 __global__ void __launch_bounds__(256)
 k_fft_to_grid_m(FFTPlan pl, int L, MLayout fin, double *grid, const float2 *tw) {
@@ -515,6 +711,13 @@ static FFTPlan make_plan(int n) {
   return p;
 }
 
+template <int N>
+static int attr_fft_t() {
+  CB2_CUDA(cudaFuncSetAttribute(k_fft_products_t<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(15 * (size_t)N * sizeof(float2))));
+  return 0;
+}
+
 int fft_setup(Ctx &c) {
   FFTPlan p = make_plan(c.nph);
   if (p.nst < 0) {
@@ -535,6 +738,17 @@ int fft_setup(Ctx &c) {
   CB2_CUDA(cudaFuncSetAttribute(k_fft_products<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
   CB2_CUDA(cudaFuncSetAttribute(k_fft_products_m, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(14 * (size_t)c.nph * sizeof(float2))));
+  {
+    int rc = 0;
+    switch (c.nph) {
+      case 768: rc = attr_fft_t<768>(); break;
+      case 384: rc = attr_fft_t<384>(); break;
+      case 192: rc = attr_fft_t<192>(); break;
+      case 96: rc = attr_fft_t<96>(); break;
+      default: break;
+    }
+    if (rc) return rc;
+  }
   if (26 * (size_t)(c.L + 1) * sizeof(float) > 7 * (size_t)c.nph * sizeof(float2)) {
     set_error("ngrid_zonal_ctl too small for the staging of the fused FFT kernel");
     return CB2_ERR_ARG;
@@ -576,10 +790,24 @@ void fft_forward_grid(Ctx &c, int ncomp, const double *grid, T *four) {
                                                                     grid, four, twid<T>(c));
 }
 
+template <int N>
+static void launch_fft_t(Ctx &c, const MLayout &in, const MLayout &out, const ProdCoef &pc) {
+  const size_t sm = 15 * (size_t)N * sizeof(float2);
+  k_fft_products_t<N><<<(unsigned)(c.nth * c.nr), 512, sm, c.stream>>>(c.L, in, out, (const float2 *)c.d_tw_fft32,
+                                                                      pc);
+}
+
 void fft_products_m(Ctx &c, const MLayout &in, const MLayout &out) {
+  ProdCoef pc{c.p.coef_velo, c.p.coef_lor, c.p.coef_induct, c.p.coef_temp};
+  switch (c.nph) {
+    case 768: launch_fft_t<768>(c, in, out, pc); return;
+    case 384: launch_fft_t<384>(c, in, out, pc); return;
+    case 192: launch_fft_t<192>(c, in, out, pc); return;
+    case 96: launch_fft_t<96>(c, in, out, pc); return;
+    default: break;
+  }
   FFTPlan p = make_plan(c.nph);
   size_t sm = 14 * (size_t)c.nph * sizeof(float2);
-  ProdCoef pc{c.p.coef_velo, c.p.coef_lor, c.p.coef_induct, c.p.coef_temp};
   k_fft_products_m<<<(unsigned)(c.nth * c.nr), 512, sm, c.stream>>>(p, c.L, in, out, (const float2 *)c.d_tw_fft32,
                                                                    pc);
 }

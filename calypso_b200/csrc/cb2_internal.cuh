@@ -154,8 +154,10 @@ struct MLayout {
   int nvec = 0, nscal = 0, nr = 0, nth = 0;
   __host__ __device__ int rpP() const { return 2 * (nvec + nscal); }
   __host__ __device__ int rpD() const { return 4 * nvec; }
-  __host__ __device__ size_t sP() const { return (size_t)nr * rpP(); }
-  __host__ __device__ size_t sD() const { return (size_t)nr * rpD(); }
+  // per-(m, theta) block strides, rounded up to 4 floats (16 bytes) so TMA
+  // boxes can start on any block
+  __host__ __device__ size_t sP() const { return (((size_t)nr * rpP() + 3) / 4) * 4; }
+  __host__ __device__ size_t sD() const { return (((size_t)nr * rpD() + 3) / 4) * 4; }
   // element of component c (vector v: 3v r, 3v+1 theta, 3v+2 phi; scalars
   // after the vectors) at (m, theta, k), order sign s
   __host__ __device__ float *at(int m, int th, int k, int c, int s) const {
@@ -167,15 +169,17 @@ struct MLayout {
     return P + ((size_t)m * nth + th) * sP() + (size_t)k * rpP() + 2 * (nvec + (c - 3 * nvec)) + s;
   }
 };
-// layout over a float buffer of (L+1) * nth * nr * 2 * (3 nvec + nscal) floats
+// layout over a float buffer of at least mlayout_floats(c) floats (any
+// nvec, nscal with 3 nvec + nscal <= 13)
 MLayout mlayout(const Ctx &c, void *buf, int nvec, int nscal);
+size_t mlayout_floats(const Ctx &c);
 
 // mixed-precision Legendre (cb2_legendre_mixed.cu)
 int mixed_setup(Ctx &c);
 void mixed_free(Ctx &c);
 // slots: first rj slot of each vector, then of each scalar (out.nvec + out.nscal)
-void leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out);
-void leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots);
+int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out);
+int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots);
 // FFT and products of the mixed path (cb2_fft.cu), float32, order-major layouts
 void fft_products_m(Ctx &c, const MLayout &in, const MLayout &out);
 void fft_backward_grid_m(Ctx &c, const MLayout &in, double *grid);

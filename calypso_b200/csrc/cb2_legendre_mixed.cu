@@ -185,7 +185,6 @@ struct Smem {
   uint64_t full[NSTAGE], empty[NSTAGE], done;
   uint32_t tmem_base;
   int mma_any;
-  float rowmax[2][TM];
   float rowscale[TM];
 };
 
@@ -205,7 +204,8 @@ __device__ inline void block_of(int kbi, int nkb1, int &p, int &kb) {
 //   kpad(p)               K extent the MMAs read (multiple of 16);
 //   n(p)                  MMA N (multiple of 16, <= 256);
 //   tma_xy(p, kb, x, y)   origin of the B box;
-//   absmax(r, h)          max |A| over half h of row r's values (both parities);
+//   rowmax(r)             an upper bound of |A| over row r (both parities),
+//                         from the row-maximum tables;
 //   fill(p, kb, r, h, s, hi, lo)  row r's K values 32 h .. 32 h + 31 of block
 //                         (p, kb), scaled by s, split and stored as four
 //                         16-byte chunks into the swizzled hi / lo tiles.
@@ -229,9 +229,7 @@ __device__ bool gemm_tile(const Prob &pr, Smem *sh, unsigned char *base, uint32_
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   // per-row power-of-two scale over every K value of the row (both parities)
-  sh->rowmax[h][r] = pr.absmax(r, h);
-  __syncthreads();
-  if (h == 0) sh->rowscale[r] = pow2_scale(fmaxf(sh->rowmax[0][r], sh->rowmax[1][r]));
+  if (h == 0) sh->rowscale[r] = pow2_scale(pr.rowmax(r));
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -353,6 +351,7 @@ struct BwdArgs {
   size_t fs;
   const float *bunscale;          // [gemm][m][nhp] 1 / column scale of B
   const int *koff, *klen, *n1;    // per (m, group) K offset / length; dP part length
+  const float *rowmax;            // [field][comp][k][m][s], k_rowmax_spec
   MLayout out;
   int *status;
 };
@@ -411,47 +410,53 @@ struct BwdProb {
     return w;
   }
 
-  __device__ float absmax(int r, int h) const {
-    const BwdRow w = row_src(r);
-    const int half = (nl + 1) / 2, t0 = h * half, t1 = min(nl, t0 + half);
-    double mx = 0.0;
+  // from the table M[field][comp][k][m][s] = max over l of |S l(l+1)| (comp 0,
+  // vectors), |S| (comp 0, scalars), |dS/dr| (comp 1), |T| (comp 2)
+  __device__ float rowmax(int r) const {
+    const BwdArgs &b = *A;
+    const int row = row0 + r;
+    if (row >= nrows) return 0.0f;
+    const int M1 = b.L + 1;
+    auto M = [&](int v, int c, int k, int s) { return b.rowmax[(((size_t)v * 3 + c) * b.nr + k) * 2 * M1 + 2 * m + s]; };
     if (g == 0) {
-      if (w.xa)
-        for (int t = t0; t < t1; t++) mx = fmax(mx, fabs(w.xa[t] * (w.g3 ? w.g3[t] : 1.0)));
-      return (float)(mx * w.fa);
+      const int ng = b.nvec + b.nscal, s = row & 1, v = (row >> 1) % ng, k = (row >> 1) / ng;
+      const double ar = b.ar1[k];
+      return (float)((double)M(v, 0, k, s) * ((v < b.nvec) ? ar * ar : 1.0));
     }
-    for (int t = t0; t < t1; t++) {
-      if (w.xa) mx = fmax(mx, fabs(w.xa[t] * w.fa));
-      if (w.xb) mx = fmax(mx, fabs(w.xb[t] * w.fb));
-    }
-    return (float)mx;
+    const int q = row & 3, v = (row >> 2) % b.nvec, k = (row >> 2) / b.nvec;
+    const int cd = (q < 2) ? 1 : 2, sd = q & 1, cm = (q < 2) ? 2 : 1, smm = (q & 1) ^ 1;
+    return (float)((double)fmaxf(M(v, cd, k, sd), M(v, cm, k, smm)) * b.ar1[k]);
   }
 
   __device__ void fill(int p, int kb, int r, int h, float sc, unsigned char *hi, unsigned char *lo) const {
     const BwdRow w = row_src(r);
-    const int kk0 = kb * KB + h * 32;
-    for (int c = 0; c < 4; c++) {
-      float x[8];
+    const int kk0 = kb * KB + h * 32, klp = kl[p], n1p = n1[p];
+    float x[32];
+    if (g == 0) {
+      const double fa = w.fa * (double)sc;
 #pragma unroll
-      for (int e = 0; e < 8; e++) {
-        const int kk = kk0 + c * 8 + e;
+      for (int e = 0; e < 32; e++) {
+        const int kk = kk0 + e, t = p + 2 * kk;
         double v = 0.0;
-        if (kk < kl[p]) {
-          if (g == 0) {
-            if (w.xa) {
-              const int t = p + 2 * kk;
-              v = w.xa[t] * w.fa * (w.g3 ? w.g3[t] : 1.0);
-            }
-          } else if (kk < n1[p]) {
-            if (w.xa) v = w.xa[(1 - p) + 2 * kk] * w.fa;
-          } else {
-            if (w.xb) v = w.xb[p + 2 * (kk - n1[p])] * w.fb;
-          }
-        }
-        x[e] = (float)v * sc;
+        if (w.xa && kk < klp) v = __ldg(w.xa + t) * (w.g3 ? __ldg(w.g3 + t) : 1.0);
+        x[e] = (float)(v * fa);
       }
-      store_chunk(hi, lo, r, h * 4 + c, x);
+    } else {
+      const double fa = w.fa * (double)sc, fb = w.fb * (double)sc;
+#pragma unroll
+      for (int e = 0; e < 32; e++) {
+        const int kk = kk0 + e;
+        double v = 0.0;
+        if (kk < n1p) {
+          if (w.xa) v = __ldg(w.xa + (1 - p) + 2 * kk) * fa;
+        } else if (kk < klp) {
+          if (w.xb) v = __ldg(w.xb + p + 2 * (kk - n1p)) * fb;
+        }
+        x[e] = (float)v;
+      }
     }
+#pragma unroll
+    for (int c = 0; c < 4; c++) store_chunk(hi, lo, r, h * 4 + c, x + 8 * c);
   }
 };
 
@@ -514,157 +519,337 @@ k_leg_bwd_mixed(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int
 
 // ---------------------------------------------------------------------------
 // forward: order-major Fourier rows -> spectra f[slot][k][jj]
+//
+// One CTA = (order m, parity p of l-m, gemm, tile of 128 rows).  For each
+// block of 32 south nodes tb, TMA brings the raw float32 rows of the tile at
+// those 32 colatitudes and at their 32 mirror nodes ([theta][row], 16 KB
+// each); converter threads form the folded, weighted operand
+//   A[row][i] = sg * s_row * (f(i) w_i +- f(i') w_i')     (i' = nth-1-i)
+// split into fp16 hi / lo (64-byte swizzled, K = 32) while TMA brings the
+// B tiles (P_l^m rows of this parity, 64-byte swizzled).  gemm P takes one
+// K block per tb; gemm DM two (dP part: element `row`, fold 1-p; mP part:
+// element row - q + 3 - q, fold p).  Three raw stages, three A/B stages, loads
+// two blocks ahead.  One accumulator (N = degrees of this parity).
+constexpr int FKB = 32;            // K per block (64-byte rows)
+constexpr int FST = 3;             // stages (raw and A/B)
+constexpr uint32_t RAW_BYTES = 2 * FKB * TM * 4;    // south + north, float32
+constexpr uint32_t FA_BYTES = TM * FKB * 2;         // one of hi / lo
+
 struct FwdArgs {
-  int L, nr, jmax, nh, nhp, nth, nvec, nscal, NFmax;
+  int L, nr, jmax, nh, nhp, nth, nvec, nscal, NFmax, boxr, nfb;   // nfb: B rows in smem
   int slot[8];
   const int *moff;
   const double *g6, *g7, *r;
-  const float *wgt;      // Gauss weights (float)
-  MLayout in;
+  const float *wgt;      // Gauss weights (float), nth
   double *f;
   size_t fs;
+  size_t sP, sD;         // block strides of the input layout
   const float *bunscale; // [gemm][(m, parity)][NFmax] 1 / column scale of B
   const int *roff, *nlp; // B row offset and number of degrees of (m, parity)
+  const float *rowmax;   // [m][element], k_rowmax_four
   int *status;
 };
 
-// One tile row of the forward gemms.  gemm P: row (k, field, s) = element
-// `row` of the P block at every theta; value at south node i =
-// sym (p = 0) or anti (p = 1) of f w.  gemm DM: row (k, vector, q) with
-// K = [dP part (theta i) | mP part (theta i)]; dP part reads element `row`
-// of the D block with sign sd and fold 1-p, mP part element row - q + 3 - q
-// with sign sm and fold p:
-//   dS+ = [theta+ | -phi-], dS- = [theta- | +phi+],
-//   T+  = [-phi+ | -theta-], T- = [-phi- | +theta+].
-struct FwdProb {
-  const FwdArgs *A;
-  int m, g, nrows, row0, K;
-  int np[2], ro[2];
-  __device__ int nkb(int p) const { return np[p] > 0 ? (K + KB - 1) / KB : 0; }
-  __device__ int kpad(int) const { return K; }
-  __device__ int n(int p) const { return ((np[p] + 15) / 16) * 16; }
-  __device__ void tma_xy(int p, int kb, int &x, int &y) const { x = kb * KB; y = ro[p]; }
+struct FwdSmem {
+  uint64_t rawfull[FST], bfull[FST], mmadone[FST], done;
+  uint32_t tmem_base;
+  int mma_any;
+  float rowscale[TM];
+  float w[1024];         // Gauss weights (nth <= 1024)
+};
 
-  // pointers to the element of this row at theta = 0 (nullptr: row outside the gemm)
-  __device__ const float *src(int r, int part) const {
-    const FwdArgs &b = *A;
-    const int row = row0 + r;
-    if (row >= nrows) return nullptr;
-    if (g == 0) return b.in.P + (size_t)m * b.nth * b.in.sP() + row;
-    const int q = row & 3;
-    return b.in.D + (size_t)m * b.nth * b.in.sD() + (part ? row - q + 3 - q : row);
-  }
-  __device__ size_t stride() const { return g ? A->in.sD() : A->in.sP(); }
+// shared-memory descriptor, K-major, 64-byte swizzle (8-row groups 512 bytes apart)
+__device__ inline uint64_t smem_desc_sw64(const void *p) {
+  uint64_t d = (uint64_t)((smem_u32(p) & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(512 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)4 << 61;                 // 64-byte swizzle
+  return d;
+}
 
-  __device__ float absmax(int r, int h) const {
-    const FwdArgs &b = *A;
-    const size_t st = stride();
-    const int half = (b.nh + 1) / 2, i0 = h * half, i1 = min(b.nh, i0 + half);
-    float mx = 0.0f;
-    for (int part = 0; part < (g ? 2 : 1); part++) {
-      const float *s0 = src(r, part);
-      if (!s0) continue;
-      for (int i = i0; i < i1; i++) {
-        const float fa = s0[(size_t)i * st] * b.wgt[i];
-        const float fb = s0[(size_t)(b.nth - 1 - i) * st] * b.wgt[b.nth - 1 - i];
-        mx = fmaxf(mx, fabsf(fa) + fabsf(fb));
-      }
+__device__ inline uint32_t sw64_chunk(int row, int c) {
+  return (uint32_t)row * 64u + ((uint32_t)(c ^ ((row >> 1) & 3)) << 4);
+}
+
+__global__ void __launch_bounds__(NTHR, 1)
+k_leg_fwd_tma(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int tiles_g0,
+              const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
+              const __grid_constant__ CUtensorMap tmp_hi, const __grid_constant__ CUtensorMap tmp_lo,
+              const __grid_constant__ CUtensorMap tmd_hi, const __grid_constant__ CUtensorMap tmd_lo,
+              uint32_t tmem_cols) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char *base = smem_base_1024(smem_raw);
+  const uint32_t B_BYTES = (uint32_t)a.nfb * FKB * 2;       // one of hi / lo
+  const uint32_t AB_BYTES = 2 * FA_BYTES + 2 * B_BYTES;
+  unsigned char *raw0 = base;                                // FST x RAW_BYTES
+  unsigned char *ab0 = base + FST * RAW_BYTES;               // FST x AB_BYTES
+  FwdSmem *sh = reinterpret_cast<FwdSmem *>(ab0 + FST * AB_BYTES);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int r = tid & (TM - 1), h = tid >> 7;
+  const int m = blockIdx.y, p = blockIdx.z;
+  const int g = (blockIdx.x < (unsigned)tiles_g0) ? 0 : 1;
+  const int nrows = g ? rows_g1 : rows_g0;
+  const int row0 = (g ? blockIdx.x - tiles_g0 : blockIdx.x) * TM;
+  const int np = a.nlp[m * 2 + p];
+  const int npad = ((np + 15) / 16) * 16;
+  const int nbox = (npad + a.boxr - 1) / a.boxr;
+  const int NT = (a.nh + FKB - 1) / FKB;                    // theta blocks
+  const int NB = g ? 2 * NT : NT;                           // K blocks
+  const CUtensorMap *traw = g ? &tm_rawD : &tm_rawP;
+  const CUtensorMap *tbh = g ? &tmd_hi : &tmp_hi, *tbl = g ? &tmd_lo : &tmp_lo;
+  const int brow = a.roff[m * 2 + p];
+
+  if (tid == 0) {
+    for (int q = 0; q < FST; q++) {
+      mbar_init(&sh->rawfull[q], 1); mbar_init(&sh->bfull[q], 1); mbar_init(&sh->mmadone[q], 1);
     }
-    return mx;
+    mbar_init(&sh->done, 1);
+    sh->mma_any = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-
-  __device__ void fill(int p, int kb, int r, int h, float sc, unsigned char *hi, unsigned char *lo) const {
-    const FwdArgs &b = *A;
-    const size_t st = stride();
+  for (int q = tid; q < a.nth; q += NTHR) sh->w[q] = a.wgt[q];
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem_base)),
+                 "r"(tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // row scale from the row-maximum table (a bound of both folds)
+  if (h == 0) {
     const int row = row0 + r;
-    const int q = row & 3;
-    const float *s0 = src(r, 0), *s1 = g ? src(r, 1) : nullptr;
-    const float sd = (g == 0 || q < 2) ? sc : -sc;
-    const float sm = (q & 1) ? sc : -sc;
-    const int kk0 = kb * KB + h * 32;
-    for (int c = 0; c < 4; c++) {
-      float x[8];
+    float mx = 0.0f;
+    if (row < nrows && np > 0) {
+      const float *Mf = a.rowmax + (size_t)m * (a.sP + a.sD);
+      if (g == 0) mx = Mf[row];
+      else { const int q = row & 3; mx = fmaxf(Mf[a.sP + row], Mf[a.sP + row - q + 3 - q]); }
+    }
+    sh->rowscale[r] = pow2_scale(mx);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh->tmem_base;
+
+  // block b -> (theta block, part)
+  auto tb_of = [&](int b) { return g ? (b >> 1) : b; };
+  auto part_of = [&](int b) { return g ? (b & 1) : 0; };
+  auto issue_raw = [&](int tb) {
+    const int q = tb % FST;
+    unsigned char *dst = raw0 + q * RAW_BYTES;
+    mbar_expect_tx(&sh->rawfull[q], RAW_BYTES);
+    tma_load_2d(dst, traw, &sh->rawfull[q], row0, m * a.nth + tb * FKB);
+    tma_load_2d(dst + RAW_BYTES / 2, traw, &sh->rawfull[q], row0, m * a.nth + a.nth - tb * FKB - FKB);
+  };
+  auto issue_b = [&](int b) {
+    const int q = b % FST, tb = tb_of(b), part = part_of(b);
+    unsigned char *bh = ab0 + q * AB_BYTES + 2 * FA_BYTES, *bl = bh + B_BYTES;
+    const uint32_t bytes = (uint32_t)nbox * a.boxr * FKB * 2;
+    mbar_expect_tx(&sh->bfull[q], 2 * bytes);
+    const int x = part * a.nhp + tb * FKB;
+    for (int j = 0; j < nbox; j++) {
+      tma_load_2d(bh + j * a.boxr * FKB * 2, tbh, &sh->bfull[q], x, brow + j * a.boxr);
+      tma_load_2d(bl + j * a.boxr * FKB * 2, tbl, &sh->bfull[q], x, brow + j * a.boxr);
+    }
+  };
+
+  int n_raw = 0, n_b = 0, n_rawdone = 0, n_bdone = 0;     // thread 0 bookkeeping
+  int failed = __syncthreads_or((*(volatile int *)a.status & CB2_STATUS_PIPE_TIMEOUT) != 0 || np == 0);
+  if (tid == 0 && !failed) {
+    for (int tb = 0; tb < min(NT, FST); tb++) { issue_raw(tb); n_raw++; }
+    for (int b = 0; b < min(NB, FST - 1); b++) { issue_b(b); n_b++; }
+  }
+  const int row = row0 + r, q4 = row & 3;
+  const float sc = sh->rowscale[r];
+  for (int b = 0; b < NB && !failed; b++) {
+    const int s = b % FST, tb = tb_of(b), part = part_of(b), rs = tb % FST;
+    int f = 0;
+    // raw tile of this theta block (all threads observe the phase)
+    if (!mbar_wait(&sh->rawfull[rs], (uint32_t)((tb / FST) & 1))) f = 1;
+    // A/B stage s was last read by the MMAs of block b - FST
+    if (b >= FST && !mbar_wait(&sh->mmadone[s], (uint32_t)(((b - FST) / FST) & 1))) f = 1;
+    if (__syncthreads_or(f)) { failed = 1; break; }
+    // convert: thread (r, h) builds K values 16 h .. 16 h + 15 of row r
+    {
+      const float *rs_s = reinterpret_cast<const float *>(raw0 + rs * RAW_BYTES);
+      const float *rs_n = rs_s + FKB * TM;
+      int src = r, sigma = p;
+      float sg = 1.0f;
+      if (g) {
+        if (part == 0) { sigma = 1 - p; sg = (q4 < 2) ? 1.0f : -1.0f; }
+        else { src = r - q4 + 3 - q4; sigma = p; sg = (q4 & 1) ? 1.0f : -1.0f; }
+      }
+      sg *= sc;
+      float x[16];
 #pragma unroll
-      for (int e = 0; e < 8; e++) {
-        const int kk = kk0 + c * 8 + e;
+      for (int e = 0; e < 16; e++) {
+        const int kk = h * 16 + e, i = tb * FKB + kk;
         float v = 0.0f;
-        const bool dpart = (g == 0) || kk < b.nhp;
-        const int i = dpart ? kk : kk - b.nhp;
-        const float *s = dpart ? s0 : s1;
-        if (s && i < b.nh) {
-          const int ii = b.nth - 1 - i;
-          const float fa = s[(size_t)i * st] * b.wgt[i], fb = s[(size_t)ii * st] * b.wgt[ii];
-          const int sigma = (g == 0) ? p : (dpart ? 1 - p : p);
-          v = (sigma ? fa - fb : fa + fb) * (dpart ? sd : sm);
+        if (i < a.nh) {
+          const float fa = rs_s[kk * TM + src] * sh->w[i];
+          const float fb = rs_n[(FKB - 1 - kk) * TM + src] * sh->w[a.nth - 1 - i];
+          v = (sigma ? fa - fb : fa + fb) * sg;
         }
         x[e] = v;
       }
-      store_chunk(hi, lo, r, h * 4 + c, x);
+      unsigned char *ahi = ab0 + s * AB_BYTES, *alo = ahi + FA_BYTES;
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        uint32_t hh[4], ll[4];
+#pragma unroll
+        for (int e = 0; e < 8; e += 2) {
+          const float x0 = x[c * 8 + e], x1 = x[c * 8 + e + 1];
+          const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
+          hh[e >> 1] = pack_half2(h0, h1);
+          ll[e >> 1] = pack_half2(__float2half_rn(x0 - __half2float(h0)), __float2half_rn(x1 - __half2float(h1)));
+        }
+        const uint32_t off = sw64_chunk(r, 2 * h + c);
+        *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+        *reinterpret_cast<uint4 *>(alo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+      }
     }
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      // the raw stage of tb is free once its last block is converted
+      const bool last_of_tb = (!g) || part == 1;
+      if (last_of_tb && tb + FST < NT) { issue_raw(tb + FST); n_raw++; }
+      n_rawdone = last_of_tb ? tb + 1 : n_rawdone;
+      if (!mbar_wait(&sh->bfull[s], (uint32_t)((b / FST) & 1))) {
+        f = 1;
+      } else {
+        n_bdone = b + 1;
+        tc_fence_after();
+        unsigned char *ahi = ab0 + s * AB_BYTES, *alo = ahi + FA_BYTES;
+        unsigned char *bh = ahi + 2 * FA_BYTES, *bl = bh + B_BYTES;
+        const uint32_t idesc = idesc_f16_f32(TM, npad);
+        const uint64_t dah = smem_desc_sw64(ahi), dal = smem_desc_sw64(alo);
+        const uint64_t dbh = smem_desc_sw64(bh), dbl = smem_desc_sw64(bl);
+#pragma unroll
+        for (int ks = 0; ks < FKB / 16; ks++) {
+          const uint64_t o = (uint64_t)(ks * 2);   // +32 bytes along K
+          mma_f16(tmem, dah + o, dbh + o, idesc, (b == 0 && ks == 0) ? 0u : 1u);
+          mma_f16(tmem, dah + o, dbl + o, idesc, 1u);
+          mma_f16(tmem, dal + o, dbh + o, idesc, 1u);
+        }
+        mma_commit(&sh->mmadone[s]);
+        sh->mma_any = 1;
+        // the B tiles of block b + FST - 1 go to the stage the MMAs of block b - 1 used
+        const int bn = b + FST - 1;
+        if (bn < NB) {
+          if (bn >= FST && !mbar_wait(&sh->mmadone[bn % FST], (uint32_t)(((bn - FST) / FST) & 1))) f = 1;
+          else { issue_b(bn); n_b++; }
+        }
+      }
+    }
+    if (__syncthreads_or(f)) { failed = 1; break; }
   }
-};
-
-__global__ void __launch_bounds__(NTHR, 1)
-k_leg_fwd_mixed(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int tiles_g0,
-                const __grid_constant__ CUtensorMap tmp_hi, const __grid_constant__ CUtensorMap tmp_lo,
-                const __grid_constant__ CUtensorMap tmd_hi, const __grid_constant__ CUtensorMap tmd_lo) {
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char *base = smem_base_1024(smem_raw);
-  const uint32_t BR = (uint32_t)a.NFmax;
-  Smem *sh = reinterpret_cast<Smem *>(base + NSTAGE * (2 * TM * 128 + 2 * BR * 128));
-  FwdProb pr;
-  pr.A = &a;
-  pr.m = blockIdx.y;
-  pr.g = (blockIdx.x < (unsigned)tiles_g0) ? 0 : 1;
-  pr.nrows = pr.g ? rows_g1 : rows_g0;
-  pr.row0 = (pr.g ? blockIdx.x - tiles_g0 : blockIdx.x) * TM;
-  pr.K = pr.g ? 2 * a.nhp : a.nhp;
-  const int m = pr.m;
-  for (int p = 0; p < 2; p++) {
-    pr.np[p] = a.nlp[m * 2 + p];
-    pr.ro[p] = a.roff[m * 2 + p];
+  // drain: loads still in flight (raw and B), then every MMA
+  if (tid == 0) {
+    for (int tb = n_rawdone; tb < n_raw; tb++)
+      if (!mbar_wait(&sh->rawfull[tb % FST], (uint32_t)((tb / FST) & 1))) failed = 1;
+    for (int b = n_bdone; b < n_b; b++)
+      if (!mbar_wait(&sh->bfull[b % FST], (uint32_t)((b / FST) & 1))) failed = 1;
+    if (sh->mma_any) mma_commit(&sh->done);
   }
-  const bool ok = gemm_tile(pr, sh, base, BR, pr.g ? &tmd_hi : &tmp_hi, pr.g ? &tmd_lo : &tmp_lo, a.status);
-  if (ok) {
-    const int warp = threadIdx.x >> 5;
-    const int r = threadIdx.x & (TM - 1), h = threadIdx.x >> 7, row = pr.row0 + r;
+  __syncthreads();
+  int f = failed && np > 0;
+  if (sh->mma_any && !mbar_wait(&sh->done, 0)) f = 1;
+  f = __syncthreads_or(f);
+  tc_fence_after();
+  if (f && tid == 0) atomicOr(a.status, CB2_STATUS_PIPE_TIMEOUT);
+  if (!f && np > 0) {
     int k, slot, kind, s;   // kind 0: S (g7 r^2), 1: dS or T (g7 r), 2: scalar (g6)
-    if (pr.g == 0) {
+    if (g == 0) {
       const int ng = a.nvec + a.nscal, v = (row >> 1) % ng;
       s = row & 1; k = (row >> 1) / ng;
       slot = a.slot[v]; kind = (v < a.nvec) ? 0 : 2;
     } else {
-      const int q = row & 3, v = (row >> 2) % a.nvec;
-      k = (row >> 2) / a.nvec; s = q & 1;
-      slot = a.slot[v] + 1 + (q >> 1); kind = 1;
+      const int v = (row >> 2) % a.nvec;
+      k = (row >> 2) / a.nvec; s = q4 & 1;
+      slot = a.slot[v] + 1 + (q4 >> 1); kind = 1;
     }
-    const bool valid = row < pr.nrows && !(m == 0 && s == 1);
-    const double ua = 1.0 / (double)sh->rowscale[r];
-    const uint32_t tl = sh->tmem_base + ((uint32_t)((warp & 3) * 32) << 16);
+    const bool valid = row < nrows && !(m == 0 && s == 1);
+    const double ua = 1.0 / (double)sc;
+    const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
     const double rk = valid ? a.r[k] : 0.0;
     const int jjb = a.moff[m] + s * (a.L + 1 - m);
     double *dst = a.f + (size_t)slot * a.fs + (size_t)k * a.jmax + jjb;
-    for (int p = 0; p < 2; p++) {
-      const float *bun = a.bunscale + ((size_t)pr.g * (a.L + 1) * 2 + m * 2 + p) * a.NFmax;
-      const int nch = (pr.np[p] + 7) / 8;
-      for (int c8 = h; c8 < nch; c8 += 2) {
-        float v8[8];
-        tmem_ld8(tl + (uint32_t)(p * ACC1 + c8 * 8), v8);
-        if (!valid) continue;
+    const float *bun = a.bunscale + ((size_t)g * (a.L + 1) * 2 + m * 2 + p) * a.NFmax;
+    const int nch = (np + 7) / 8;
+    for (int c8 = h; c8 < nch; c8 += 2) {
+      float v8[8];
+      tmem_ld8(tl + (uint32_t)(c8 * 8), v8);
+      if (!valid) continue;
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-          const int t = c8 * 8 + q;
-          if (t < pr.np[p]) {
-            const int lm = p + 2 * t;   // l - m
-            const double fac = (kind == 0) ? a.g7[jjb + lm] * rk * rk
-                             : (kind == 2) ? a.g6[jjb + lm] : a.g7[jjb + lm] * rk;
-            dst[lm] = (double)v8[q] * (ua * (double)bun[t]) * fac;
-          }
+      for (int qq = 0; qq < 8; qq++) {
+        const int t = c8 * 8 + qq;
+        if (t < np) {
+          const int lm = p + 2 * t;   // l - m
+          const double fac = (kind == 0) ? a.g7[jjb + lm] * rk * rk
+                           : (kind == 2) ? a.g6[jjb + lm] : a.g7[jjb + lm] * rk;
+          dst[lm] = (double)v8[qq] * (ua * (double)bun[t]) * fac;
         }
       }
     }
   }
-  tmem_release(sh);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+}
+
+// ---------------------------------------------------------------------------
+// Row maxima for the operand scales, one streaming pass each.
+//
+// spectra: M[field][comp][k][m][s] = max over l = m..L of |X(l, m, s)|, X =
+// S l(l+1) (vector comp 0; l(l+1) from g3rlm), S (scalar), dS/dr, T; one
+// warp per (m, s) block of one (field, comp, k) row, lanes over l.
+struct Slots8 {
+  int s[8];
+};
+
+__global__ void __launch_bounds__(256)
+k_rowmax_spec(int L, int nr, int jmax, int nvec, Slots8 slot, const int *moff, const double *g3rlm,
+              const double *f, size_t fs, float *M) {
+  const int k = blockIdx.x, v = blockIdx.y, c = blockIdx.z;
+  const bool isvec = v < nvec;
+  if (!isvec && c > 0) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, M1 = L + 1;
+  const double *x = f + (size_t)(slot.s[v] + c) * fs + (size_t)k * jmax;
+  float *out = M + (((size_t)v * 3 + c) * nr + k) * 2 * M1;
+  for (int seg = warp; seg < 2 * M1; seg += blockDim.x >> 5) {
+    const int m = seg >> 1, s = seg & 1;
+    if (m == 0 && s == 1) {
+      if (lane == 0) out[1] = 0.0f;
+      continue;
+    }
+    const int nl = L + 1 - m, jjb = moff[m] + s * (L + 1 - m);
+    double mx = 0.0;
+    for (int t = lane; t < nl; t += 32) {
+      double a = fabs(x[jjb + t]);
+      if (isvec && c == 0) a *= g3rlm[jjb + t];
+      mx = fmax(mx, a);
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) out[seg] = (float)mx;
+  }
+}
+
+// Fourier rows: Mf[m][e] = 2 max over theta of |F(m, theta, e) w(theta)|
+// for every element e of the P block and then the D block; one thread per
+// (m, e), consecutive threads on consecutive elements.
+__global__ void __launch_bounds__(256)
+k_rowmax_four(MLayout in, const float *wgt, float *Mf) {
+  const int m = blockIdx.y;
+  const size_t sP = in.sP(), sD = in.sD();
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= sP + sD) return;
+  const float *x = (e < sP) ? in.P + (size_t)m * in.nth * sP + e : in.D + (size_t)m * in.nth * sD + (e - sP);
+  const size_t st = (e < sP) ? sP : sD;
+  float mx = 0.0f;
+#pragma unroll 8
+  for (int th = 0; th < in.nth; th++) mx = fmaxf(mx, fabsf(__ldg(x + (size_t)th * st)) * __ldg(wgt + th));
+  Mf[(size_t)m * (sP + sD) + e] = 2.0f * mx;
 }
 
 // ---------------------------------------------------------------------------
@@ -757,9 +942,13 @@ struct MixedTables {
   float *bf_unscale = nullptr;                    // [gemm][(m, parity)][NFmax]
   int *bf_roff = nullptr, *bf_nl = nullptr;
   float *wgt32 = nullptr;                         // Gauss weights in float
+  float *rowmax_spec = nullptr;                   // [8 fields][3][nr][2 (L+1)]
+  float *rowmax_four = nullptr;                   // [(L+1)][26 nr + 8]
   int Kb_all = 0, rows_all = 0, nhp = 0, NFmax = 0;
   size_t smem_bwd = 0, smem_fwd = 0;
   CUtensorMap tm_bb_hi, tm_bb_lo, tm_bfp_hi, tm_bfp_lo, tm_bfd_hi, tm_bfd_lo;
+  int boxr = 0, nfb = 0;
+  uint32_t tmem_fwd = 0;
 };
 
 using EncodeFn = PFN_cuTensorMapEncodeTiled_v12000;
@@ -776,23 +965,38 @@ EncodeFn get_encode() {
   return fn;
 }
 
-// fp16 [rows][cols] (cols contiguous, cols * 2 bytes a multiple of 16), box 64 x box_rows, 128B swizzle
-int make_map(CUtensorMap *tm, const void *ptr, uint64_t cols, uint64_t rows, uint32_t box_rows) {
+// 2-D map over [rows][cols] (cols contiguous, a row a multiple of 16 bytes),
+// box = box_cols x box_rows (box_cols * element size <= the swizzle span)
+int make_map_any(CUtensorMap *tm, CUtensorMapDataType dt, size_t es, const void *ptr, uint64_t cols, uint64_t rows,
+                 uint32_t box_cols, uint32_t box_rows, CUtensorMapSwizzle sw) {
   EncodeFn enc = get_encode();
   if (!enc) { set_error("cuTensorMapEncodeTiled is not available"); return CB2_ERR_CUDA; }
-  if ((cols * sizeof(__half)) % 16 != 0 || box_rows == 0 || box_rows > 256 || rows < box_rows) {
+  if ((cols * es) % 16 != 0 || (box_cols * es) % 16 != 0 || box_rows == 0 || box_rows > 256 || box_cols > 256 ||
+      (reinterpret_cast<uintptr_t>(ptr) & 15) != 0) {
     set_error("tensor map shape");
     return CB2_ERR_ARG;
   }
   cuuint64_t dims[2] = {cols, rows};
-  cuuint64_t strides[1] = {cols * sizeof(__half)};
-  cuuint32_t box[2] = {(cuuint32_t)KB, box_rows};
-  cuuint32_t es[2] = {1, 1};
-  CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, es,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  cuuint64_t strides[1] = {cols * es};
+  cuuint32_t box[2] = {box_cols, box_rows};
+  cuuint32_t ests[2] = {1, 1};
+  CUresult r = enc(tm, dt, 2, const_cast<void *>(ptr), dims, strides, box, ests, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled failed"); return CB2_ERR_CUDA; }
   return 0;
+}
+
+// fp16 [rows][cols], box 64 x box_rows, 128-byte swizzle (backward B tiles)
+int make_map(CUtensorMap *tm, const void *ptr, uint64_t cols, uint64_t rows, uint32_t box_rows) {
+  if (rows < box_rows) { set_error("tensor map shape"); return CB2_ERR_ARG; }
+  return make_map_any(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, ptr, cols, rows, KB, box_rows,
+                      CU_TENSOR_MAP_SWIZZLE_128B);
+}
+
+// fp16 [rows][cols], box 32 x box_rows, 64-byte swizzle (forward B tiles)
+int make_map64(CUtensorMap *tm, const void *ptr, uint64_t cols, uint64_t rows, uint32_t box_rows) {
+  return make_map_any(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, ptr, cols, rows, FKB, box_rows,
+                      CU_TENSOR_MAP_SWIZZLE_64B);
 }
 
 // 1024 alignment slack + stages + control block; at least 120 KB so a CTA
@@ -840,6 +1044,11 @@ int mixed_setup(Ctx &c) {
   }
   t->NFmax = nfmax;
   if (t->NFmax > 256) { set_error("mixed precision path needs L <= 511"); return CB2_ERR_ARG; }
+  if (c.nth % 8 != 0) { set_error("mixed precision path needs nth divisible by 8"); return CB2_ERR_ARG; }
+  t->boxr = std::min(64, t->NFmax);
+  t->nfb = ((t->NFmax + t->boxr - 1) / t->boxr) * t->boxr;
+  t->tmem_fwd = 32;
+  while ((int)t->tmem_fwd < t->NFmax) t->tmem_fwd *= 2;
   t->rows_all = R + t->NFmax;   // every NFmax-row box stays in the array
   auto up = [&](int **d, const std::vector<int> &v) -> int {
     CB2_CUDA(cudaMalloc(d, v.size() * sizeof(int)));
@@ -868,6 +1077,8 @@ int mixed_setup(Ctx &c) {
     CB2_CUDA(cudaMalloc(&t->wgt32, w.size() * sizeof(float)));
     CB2_CUDA(cudaMemcpy(t->wgt32, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
+  CB2_CUDA(cudaMalloc(&t->rowmax_spec, (size_t)8 * 3 * c.nr * 2 * (L + 1) * sizeof(float)));
+  CB2_CUDA(cudaMalloc(&t->rowmax_four, (size_t)(L + 1) * (26 * (size_t)c.nr + 8) * sizeof(float)));
   k_build_bwd_b<<<dim3(cdiv(nh, 64), L + 1), 64, 0, c.stream>>>(L, nh, t->nhp, c.d_poff, c.d_Plt, c.d_dPlt,
                                                                 c.d_asin, t->bb_koff, t->bb_klen, t->bb_n1,
                                                                 t->Kb_all, t->bb_unscale, t->bb_hi, t->bb_lo);
@@ -879,19 +1090,20 @@ int mixed_setup(Ctx &c) {
   CB2_CUDA(cudaStreamSynchronize(c.stream));
   if ((rc = make_map(&t->tm_bb_hi, t->bb_hi, t->Kb_all, t->nhp, t->nhp)) ||
       (rc = make_map(&t->tm_bb_lo, t->bb_lo, t->Kb_all, t->nhp, t->nhp)) ||
-      (rc = make_map(&t->tm_bfp_hi, t->bfp_hi, t->nhp, t->rows_all, t->NFmax)) ||
-      (rc = make_map(&t->tm_bfp_lo, t->bfp_lo, t->nhp, t->rows_all, t->NFmax)) ||
-      (rc = make_map(&t->tm_bfd_hi, t->bfd_hi, 2 * t->nhp, t->rows_all, t->NFmax)) ||
-      (rc = make_map(&t->tm_bfd_lo, t->bfd_lo, 2 * t->nhp, t->rows_all, t->NFmax)))
+      (rc = make_map64(&t->tm_bfp_hi, t->bfp_hi, t->nhp, t->rows_all, t->boxr)) ||
+      (rc = make_map64(&t->tm_bfp_lo, t->bfp_lo, t->nhp, t->rows_all, t->boxr)) ||
+      (rc = make_map64(&t->tm_bfd_hi, t->bfd_hi, 2 * t->nhp, t->rows_all, t->boxr)) ||
+      (rc = make_map64(&t->tm_bfd_lo, t->bfd_lo, 2 * t->nhp, t->rows_all, t->boxr)))
     return rc;
   t->smem_bwd = smem_bytes(t->nhp);
-  t->smem_fwd = smem_bytes(t->NFmax);
+  t->smem_fwd = 1024 + FST * (size_t)RAW_BYTES + FST * (2 * (size_t)FA_BYTES + 2 * (size_t)t->nfb * FKB * 2) +
+                sizeof(FwdSmem);
   if (t->smem_bwd > 227 * 1024 || t->smem_fwd > 227 * 1024) {
     set_error("mixed precision tiles exceed shared memory");
     return CB2_ERR_ARG;
   }
   CB2_CUDA(cudaFuncSetAttribute(k_leg_bwd_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_bwd));
-  CB2_CUDA(cudaFuncSetAttribute(k_leg_fwd_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_fwd));
+  CB2_CUDA(cudaFuncSetAttribute(k_leg_fwd_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_fwd));
   return 0;
 }
 
@@ -899,12 +1111,15 @@ void mixed_free(Ctx &c) {
   MixedTables *t = (MixedTables *)c.mixed;
   if (!t) return;
   void *ptrs[] = {t->bb_hi, t->bb_lo, t->bb_unscale, t->bb_koff, t->bb_klen, t->bb_n1, t->bfp_hi,
-                  t->bfp_lo, t->bfd_hi, t->bfd_lo, t->bf_unscale, t->bf_roff, t->bf_nl, t->wgt32};
+                  t->bfp_lo, t->bfd_hi, t->bfd_lo, t->bf_unscale, t->bf_roff, t->bf_nl, t->wgt32,
+                  t->rowmax_spec, t->rowmax_four};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete t;
   c.mixed = nullptr;
 }
+
+size_t mlayout_floats(const Ctx &c) { return (size_t)(c.L + 1) * c.nth * (26 * (size_t)c.nr + 8); }
 
 MLayout mlayout(const Ctx &c, void *buf, int nvec, int nscal) {
   MLayout l;
@@ -914,7 +1129,7 @@ MLayout mlayout(const Ctx &c, void *buf, int nvec, int nscal) {
   return l;
 }
 
-void leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
+int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   MixedTables *t = (MixedTables *)c.mixed;
   const int nvec = out.nvec, nscal = out.nscal;
   BwdArgs a{};
@@ -923,28 +1138,50 @@ void leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   for (int q = 0; q < nvec + nscal && q < 8; q++) a.slot[q] = slots[q];
   a.moff = c.d_moff; a.g3rlm = c.d_g3rlm; a.ar1 = c.d_ar1; a.f = c.d_f; a.fs = c.fsize();
   a.bunscale = t->bb_unscale; a.koff = t->bb_koff; a.klen = t->bb_klen; a.n1 = t->bb_n1;
+  a.rowmax = t->rowmax_spec;
   a.out = out; a.status = c.d_status;
+  Slots8 sl{};
+  for (int q = 0; q < nvec + nscal && q < 8; q++) sl.s[q] = slots[q];
+  k_rowmax_spec<<<dim3(c.nr, nvec + nscal, 3), 256, 0, c.stream>>>(c.L, c.nr, c.jmax, nvec, sl, c.d_moff, c.d_g3rlm,
+                                                                  c.d_f, c.fsize(), t->rowmax_spec);
   const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
   k_leg_bwd_mixed<<<dim3(tiles0 + tiles1, c.L + 1), NTHR, t->smem_bwd, c.stream>>>(a, rows0, rows1, tiles0,
                                                                                   t->tm_bb_hi, t->tm_bb_lo);
+  return 0;
 }
 
-void leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots) {
+int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots) {
   MixedTables *t = (MixedTables *)c.mixed;
   const int nvec = in.nvec, nscal = in.nscal;
   FwdArgs a{};
   a.L = c.L; a.nr = c.nr; a.jmax = c.jmax; a.nh = c.nh; a.nhp = t->nhp; a.nth = c.nth; a.NFmax = t->NFmax;
+  a.boxr = t->boxr; a.nfb = t->nfb;
   a.nvec = nvec; a.nscal = nscal;
   for (int q = 0; q < nvec + nscal && q < 8; q++) a.slot[q] = slots[q];
   a.moff = c.d_moff; a.g6 = c.d_g6; a.g7 = c.d_g7; a.r = c.d_r; a.wgt = t->wgt32;
-  a.in = in; a.f = c.d_f; a.fs = c.fsize();
+  a.f = c.d_f; a.fs = c.fsize();
+  a.sP = in.sP(); a.sD = in.sD();
   a.bunscale = t->bf_unscale; a.roff = t->bf_roff; a.nlp = t->bf_nl;
+  a.rowmax = t->rowmax_four;
   a.status = c.d_status;
+  // raw Fourier rows: float32 [(m, theta)][element], boxes of 128 elements x 32 colatitudes
+  CUtensorMap rawP{}, rawD{};
+  const uint64_t nthr = (uint64_t)(c.L + 1) * c.nth;
+  if (make_map_any(&rawP, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, in.P, in.sP(), nthr, TM, FKB,
+                   CU_TENSOR_MAP_SWIZZLE_NONE) ||
+      (nvec > 0 && make_map_any(&rawD, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, in.D, in.sD(), nthr, TM, FKB,
+                                CU_TENSOR_MAP_SWIZZLE_NONE))) {
+    return CB2_ERR_ARG;
+  }
+  if (nvec == 0) rawD = rawP;
+  k_rowmax_four<<<dim3(cdiv((long)(in.sP() + in.sD()), 256), c.L + 1), 256, 0, c.stream>>>(in, t->wgt32,
+                                                                                       t->rowmax_four);
   const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
-  k_leg_fwd_mixed<<<dim3(tiles0 + tiles1, c.L + 1), NTHR, t->smem_fwd, c.stream>>>(
-      a, rows0, rows1, tiles0, t->tm_bfp_hi, t->tm_bfp_lo, t->tm_bfd_hi, t->tm_bfd_lo);
+  k_leg_fwd_tma<<<dim3(tiles0 + tiles1, c.L + 1, 2), NTHR, t->smem_fwd, c.stream>>>(
+      a, rows0, rows1, tiles0, rawP, rawD, t->tm_bfp_hi, t->tm_bfp_lo, t->tm_bfd_hi, t->tm_bfd_lo, t->tmem_fwd);
+  return 0;
 }
 
 }  // namespace cb2
