@@ -16,6 +16,7 @@
 // shared-memory Stockham autosort transform with radix 3, 4 and 2 stages,
 // N = 3^a 2^b.
 #include <cmath>
+#include <vector>
 
 #include "cb2_internal.cuh"
 
@@ -425,91 +426,149 @@ k_fft_products_m(FFTPlan pl, int L, MLayout fin, MLayout fout, const float2 *__r
 
 // ---------------------------------------------------------------------------
 // Compile-time FFT passes for N = 3 * 2^b (the zonal grids 96 .. 768 that
-// the shells use): radix 3 first, then radix 4, a final radix 2 when b is
-// odd.  With N and the radices known at compile time every index division
-// is by a constant, and the twiddle table sits in shared memory.
+// the shells use): radix 3 first, then radix 16 while it divides, then the
+// remaining 8, 4 or 2 (768 = 3 16 16: three passes).  Every butterfly is a
+// register DFT; with N and the radices known at compile time every index
+// division is by a constant.  The twiddles of stage st are one table
+// w^(r k), r = 1..R-1, k = 0..NS-1, contiguous in k.  Rows in shared memory
+// carry one pad element per 16 (index i -> i + i/16), which keeps the
+// stride-NS writes of the radix-16 stages free of bank conflicts.
 template <int N>
 struct Plan3x2 {
-  static constexpr int nst() {
-    int n = N / 3, s = 1;
-    while (n % 4 == 0) { n /= 4; s++; }
-    if (n == 2) s++;
-    return s;
-  }
   static constexpr int radix(int st) {
     if (st == 0) return 3;
     int n = N / 3;
-    for (int q = 1; q < st; q++) n /= 4;
-    return (n % 4 == 0) ? 4 : 2;
+    for (int q = 1; q < st; q++) n /= (n % 16 == 0) ? 16 : n;
+    return (n % 16 == 0) ? 16 : n;
+  }
+  static constexpr int nst() {
+    int n = N / 3, s = 1;
+    while (n > 1) { n /= (n % 16 == 0) ? 16 : n; s++; }
+    return s;
   }
   static constexpr int ns(int st) {   // product of the radices before stage st
     int p = 1;
     for (int q = 0; q < st; q++) p *= radix(q);
     return p;
   }
-  // stage st reads its twiddles w^(r k), r = 1..R-1, k = 0..NS-1, from
-  // entries off(st) + (r-1) NS + k of one table (contiguous in k, so a
-  // warp's reads never collide in a bank)
   static constexpr int off(int st) {
     int o = 0;
     for (int q = 0; q < st; q++) o += (radix(q) - 1) * ns(q);
     return o;
   }
   static constexpr int ntw() { return off(nst()); }
+  static constexpr int NP = N + N / 16;   // padded row length
 };
+
+__host__ __device__ __forceinline__ int fpad(int i) { return i + (i >> 4); }
+
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return float2{a.x + b.x, a.y + b.y}; }
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return float2{a.x - b.x, a.y - b.y}; }
+__host__ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return float2{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+// multiply by -i (forward) or +i (inverse)
+template <int SIGN>
+__host__ __device__ __forceinline__ float2 rot90(float2 a) {
+  return (SIGN < 0) ? float2{a.y, -a.x} : float2{-a.y, a.x};
+}
+
+// exp(SIGN 2 pi i q / 16) from exact values of the cosine at multiples of
+// pi/8: cos(pi/8) = sqrt(2 + sqrt 2)/2, cos(pi/4) = sqrt(2)/2, sin(pi/8) =
+// sqrt(2 - sqrt 2)/2
+template <int SIGN>
+__host__ __device__ __forceinline__ float2 w16(int q) {
+  constexpr float c1 = 0.92387953251128675613f, c2 = 0.70710678118654752440f, c3 = 0.38268343236508977173f;
+  const float cs[16] = {1.f, c1, c2, c3, 0.f, -c3, -c2, -c1, -1.f, -c1, -c2, -c3, 0.f, c3, c2, c1};
+  const float sn[16] = {0.f, c3, c2, c1, 1.f, c1, c2, c3, 0.f, -c3, -c2, -c1, -1.f, -c1, -c2, -c3};
+  return float2{cs[q & 15], (SIGN < 0) ? -sn[q & 15] : sn[q & 15]};
+}
+
+template <int SIGN>
+__host__ __device__ __forceinline__ void dft4(float2 &v0, float2 &v1, float2 &v2, float2 &v3) {
+  const float2 a0 = cadd(v0, v2), a1 = csub(v0, v2), a2 = cadd(v1, v3), a3 = rot90<SIGN>(csub(v1, v3));
+  v0 = cadd(a0, a2); v1 = cadd(a1, a3); v2 = csub(a0, a2); v3 = csub(a1, a3);
+}
+
+// in-register DFT of R points, natural order in and out
+template <int R, int SIGN>
+__host__ __device__ __forceinline__ void dftr(float2 (&v)[R]) {
+  if constexpr (R == 2) {
+    const float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b); v[1] = csub(a, b);
+  } else if constexpr (R == 3) {
+    const float s32 = 0.86602540378443864676f;   // sin(pi/3) = sqrt(3)/2
+    const float2 t1 = cadd(v[1], v[2]);
+    const float2 t2 = float2{v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y};
+    const float dx = v[1].x - v[2].x, dy = v[1].y - v[2].y;
+    const float2 t3 = (SIGN < 0) ? float2{s32 * dy, -s32 * dx} : float2{-s32 * dy, s32 * dx};
+    v[0] = cadd(v[0], t1); v[1] = cadd(t2, t3); v[2] = csub(t2, t3);
+  } else if constexpr (R == 4) {
+    dft4<SIGN>(v[0], v[1], v[2], v[3]);
+  } else if constexpr (R == 8) {
+    // 2 x 4: even / odd halves, then W8^k twiddles
+    float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<SIGN>(e0, e1, e2, e3);
+    dft4<SIGN>(o0, o1, o2, o3);
+    o1 = cmulf(o1, w16<SIGN>(2));
+    o2 = rot90<SIGN>(o2);
+    o3 = cmulf(o3, w16<SIGN>(6));
+    v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+  } else {
+    static_assert(R == 16, "radix");
+    // 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2
+    float2 a[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) {
+      a[n2][0] = v[n2]; a[n2][1] = v[4 + n2]; a[n2][2] = v[8 + n2]; a[n2][3] = v[12 + n2];
+      dft4<SIGN>(a[n2][0], a[n2][1], a[n2][2], a[n2][3]);   // over n1 -> k1
+    }
+#pragma unroll
+    for (int n2 = 1; n2 < 4; n2++)
+#pragma unroll
+      for (int k1 = 1; k1 < 4; k1++) a[n2][k1] = cmulf(a[n2][k1], w16<SIGN>(n2 * k1));
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+      float2 b0 = a[0][k1], b1 = a[1][k1], b2 = a[2][k1], b3 = a[3][k1];
+      dft4<SIGN>(b0, b1, b2, b3);                              // over n2 -> k2
+      v[k1] = b0; v[k1 + 4] = b1; v[k1 + 8] = b2; v[k1 + 12] = b3;
+    }
+  }
+}
 
 template <int N, int R, int NS, int NF, int SIGN>
 __device__ __forceinline__ void fft_pass(const float2 *__restrict__ x, float2 *__restrict__ y,
                                          const float2 *__restrict__ tw) {
-  constexpr int NB = N / R;
-  const float s32 = 0.86602540378443864676f;   // sin(pi/3) = sqrt(3)/2
+  constexpr int NB = N / R, NP = Plan3x2<N>::NP;
   for (int idx = threadIdx.x; idx < NF * NB; idx += blockDim.x) {
     const int f = idx / NB, j = idx - f * NB;
     const int k = j % NS;
-    const float2 *xf = x + f * N;
+    const float2 *xf = x + f * NP;
     float2 v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) {
-      float2 a = xf[j + r * NB];
+      float2 a = xf[fpad(j + r * NB)];
       if (NS > 1 && r > 0) {
         float2 w = tw[(r - 1) * NS + k];
         if (SIGN > 0) w.y = -w.y;
-        a = float2{a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x};
+        a = cmulf(a, w);
       }
       v[r] = a;
     }
-    float2 o[R];
-    if constexpr (R == 4) {
-      const float2 a0{v[0].x + v[2].x, v[0].y + v[2].y}, a1{v[0].x - v[2].x, v[0].y - v[2].y};
-      const float2 a2{v[1].x + v[3].x, v[1].y + v[3].y};
-      const float dx = v[1].x - v[3].x, dy = v[1].y - v[3].y;
-      const float2 a3 = (SIGN < 0) ? float2{dy, -dx} : float2{-dy, dx};
-      o[0] = float2{a0.x + a2.x, a0.y + a2.y};
-      o[1] = float2{a1.x + a3.x, a1.y + a3.y};
-      o[2] = float2{a0.x - a2.x, a0.y - a2.y};
-      o[3] = float2{a1.x - a3.x, a1.y - a3.y};
-    } else if constexpr (R == 2) {
-      o[0] = float2{v[0].x + v[1].x, v[0].y + v[1].y};
-      o[1] = float2{v[0].x - v[1].x, v[0].y - v[1].y};
-    } else {
-      const float2 t1{v[1].x + v[2].x, v[1].y + v[2].y};
-      const float2 t2{v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y};
-      const float dx = v[1].x - v[2].x, dy = v[1].y - v[2].y;
-      const float2 t3 = (SIGN < 0) ? float2{s32 * dy, -s32 * dx} : float2{-s32 * dy, s32 * dx};
-      o[0] = float2{v[0].x + t1.x, v[0].y + t1.y};
-      o[1] = float2{t2.x + t3.x, t2.y + t3.y};
-      o[2] = float2{t2.x - t3.x, t2.y - t3.y};
-    }
-    float2 *yf = y + f * N;
+    dftr<R, SIGN>(v);
+    float2 *yf = y + f * NP;
     const int d = (j / NS) * NS * R + k;
 #pragma unroll
-    for (int r = 0; r < R; r++) yf[d + r * NS] = o[r];
+    for (int r = 0; r < R; r++) yf[fpad(d + r * NS)] = v[r];
   }
   __syncthreads();
 }
 
-// all stages from `st` on; the result ends in x when the remaining stage
-// count is even, in y otherwise (returned)
+// all stages from `st` on; returns the buffer holding the result
 template <int N, int NF, int SIGN, int ST>
 __device__ __forceinline__ float2 *fft_passes(float2 *x, float2 *y, const float2 *tw) {
   using P = Plan3x2<N>;
@@ -527,95 +586,96 @@ __device__ __forceinline__ float2 *fft_passes(float2 *x, float2 *y, const float2
 // are free of bank conflicts.
 template <int N>
 __global__ void __launch_bounds__(512, 2)
-k_fft_products_t(int L, MLayout fin, MLayout fout, const float2 *__restrict__ twg, ProdCoef pc) {
+k_fft_products_t(int L, MLayout fin, MLayout fout, const float2 *__restrict__ twp, ProdCoef pc) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  float2 *A = reinterpret_cast<float2 *>(smraw);   // 7 x N
-  float2 *B = A + 7 * N;                            // 7 x N
-  float2 *TW = B + 7 * N;                           // N
+  using P = Plan3x2<N>;
+  constexpr int NP = P::NP;
+  static_assert(P::ntw() <= N, "twiddle table");
+  float2 *A = reinterpret_cast<float2 *>(smraw);   // 7 x NP
+  float2 *B = A + 7 * NP;                           // 7 x NP
+  float2 *TW = B + 7 * NP;                          // per-stage twiddles (ntw)
   const int M1 = L + 1, MP = M1 | 1;                // padded (odd) staging stride
   float *S = reinterpret_cast<float *>(B);          // [c * 2 + s][MP]
   const int th = blockIdx.x / fin.nr, k = blockIdx.x % fin.nr;
-  using P = Plan3x2<N>;
-  static_assert(P::ntw() <= N, "twiddle table");
-  for (int e = threadIdx.x; e < P::ntw(); e += blockDim.x) {
-    int st = 0;
-    while (st + 1 < P::nst() && e >= P::off(st + 1)) st++;
-    const int NS = P::ns(st), loc = e - P::off(st), r = 1 + loc / NS, kk = loc - (r - 1) * NS;
-    TW[e] = twg[r * kk * (N / (NS * P::radix(st)))];
-  }
-  const float *Pin = fin.P + (size_t)th * fin.sP() + (size_t)k * 10;
-  const float *Din = fin.D + (size_t)th * fin.sD() + (size_t)k * 16;
-  const size_t mstP = (size_t)fin.nth * fin.sP(), mstD = (size_t)fin.nth * fin.sD();
-  for (int idx = threadIdx.x; idx < 26 * M1; idx += blockDim.x) {
-    const int m = idx / 26, j = idx - 26 * m;
-    int c, s;
-    m_comp_of_in(j, c, s);
-    S[(c * 2 + s) * MP + m] = (j < 10) ? __ldg(Pin + m * mstP + j) : __ldg(Din + m * mstD + (j - 10));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  for (int e = tid; e < P::ntw(); e += blockDim.x) TW[e] = twp[e];
+  // input: one warp per order m, lane j < 26 reads element j of the 10 + 16 run
+  {
+    int cs = 0;
+    if (lane < 26) { int c, sg; m_comp_of_in(lane, c, sg); cs = c * 2 + sg; }
+    const float *src = (lane < 10) ? fin.P + (size_t)th * fin.sP() + (size_t)k * 10 + lane
+                                   : fin.D + (size_t)th * fin.sD() + (size_t)k * 16 + (lane - 10);
+    const size_t mst = (size_t)fin.nth * ((lane < 10) ? fin.sP() : fin.sD());
+    if (lane < 26)
+      for (int m = warp; m <= L; m += nwarp) S[cs * MP + m] = __ldg(src + m * mst);
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < 7 * N; idx += blockDim.x) {
-    const int p = idx / N, n = idx - p * N;
+  // Hermitian rows z = x + i y of the 7 pairs: one thread per (pair, m) fills
+  // n = m and n = N - m; the orders above L are zero
+  for (int p = 0; p < 7; p++) {
     const int c0 = 2 * p, c1 = 2 * p + 1;
     const bool has1 = c1 < 13;
-    float2 z{0.0f, 0.0f};
-    const int m = (n <= L) ? n : ((N - n <= L) ? N - n : -1);
-    if (n == 0) {
-      z = float2{S[(c0 * 2) * MP], has1 ? S[(c1 * 2) * MP] : 0.0f};
-    } else if (m > 0) {
-      const float a0 = S[(c0 * 2) * MP + m], b0 = S[(c0 * 2 + 1) * MP + m];
-      const float a1 = has1 ? S[(c1 * 2) * MP + m] : 0.0f, b1 = has1 ? S[(c1 * 2 + 1) * MP + m] : 0.0f;
-      const float xr = 0.5f * a0, xi = -0.5f * b0, yr = 0.5f * a1, yi = -0.5f * b1;
-      z = (m == n) ? float2{xr - yi, xi + yr} : float2{xr + yi, -xi + yr};
+    float2 *Z = A + p * NP;
+    for (int m = tid; m <= L; m += blockDim.x) {
+      const float a0 = S[(c0 * 2) * MP + m], a1 = has1 ? S[(c1 * 2) * MP + m] : 0.0f;
+      if (m == 0) {
+        Z[0] = float2{a0, a1};
+      } else {
+        const float b0 = S[(c0 * 2 + 1) * MP + m], b1 = has1 ? S[(c1 * 2 + 1) * MP + m] : 0.0f;
+        const float xr = 0.5f * a0, xi = -0.5f * b0, yr = 0.5f * a1, yi = -0.5f * b1;
+        Z[fpad(m)] = float2{xr - yi, xi + yr};
+        Z[fpad(N - m)] = float2{xr + yi, -xi + yr};
+      }
     }
-    A[idx] = z;
+    for (int n = L + 1 + tid; n < N - L; n += blockDim.x) Z[fpad(n)] = float2{0.0f, 0.0f};
   }
   __syncthreads();
   float2 *g = fft_passes<N, 7, +1, 0>(A, B, TW);
   float2 *hb = (g == A) ? B : A;
   const float cv = (float)pc.cv, cl = (float)pc.cl, ci = (float)pc.ci, ct = (float)pc.ct;
-  for (int q = threadIdx.x; q < N; q += blockDim.x) {
-    const float2 p0 = g[0 * N + q], p1 = g[1 * N + q], p2 = g[2 * N + q], p3 = g[3 * N + q];
-    const float2 p4 = g[4 * N + q], p5 = g[5 * N + q], p6 = g[6 * N + q];
+  for (int qq = tid; qq < N; qq += blockDim.x) {
+    const int q = fpad(qq);
+    const float2 p0 = g[0 * NP + q], p1 = g[1 * NP + q], p2 = g[2 * NP + q], p3 = g[3 * NP + q];
+    const float2 p4 = g[4 * NP + q], p5 = g[5 * NP + q], p6 = g[6 * NP + q];
     const float ur = p0.x, ut = p0.y, up = p1.x, wr = p1.y, wt = p2.x, wp = p2.y;
     const float br = p3.x, bt = p3.y, bp = p4.x, jr = p4.y, jt = p5.x, jp = p5.y, tt = p6.x;
-    hb[0 * N + q] = float2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv};
-    hb[1 * N + q] = float2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl};
-    hb[2 * N + q] = float2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl};
-    hb[3 * N + q] = float2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci};
-    hb[4 * N + q] = float2{(ur * bt - ut * br) * ci, ur * tt * ct};
-    hb[5 * N + q] = float2{ut * tt * ct, up * tt * ct};
+    hb[0 * NP + q] = float2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv};
+    hb[1 * NP + q] = float2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl};
+    hb[2 * NP + q] = float2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl};
+    hb[3 * NP + q] = float2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci};
+    hb[4 * NP + q] = float2{(ur * bt - ut * br) * ci, ur * tt * ct};
+    hb[5 * NP + q] = float2{ut * tt * ct, up * tt * ct};
   }
   __syncthreads();
   float2 *zf = fft_passes<N, 6, -1, 0>(hb, g, TW);
-  // (a_m, b_m) of the 12 outputs into the staging rows O[j][MP] (lanes over m),
-  // then one contiguous run per m to HBM (lanes over j)
+  // (a_m, b_m) of both components of a pair from Z[m], Z[N - m]: one thread
+  // per (pair, m), into the staging rows O[c * 2 + s][MP]
   float *O = reinterpret_cast<float *>((zf == A) ? B : A);
   const float an = 1.0f / (float)N;
-  for (int idx = threadIdx.x; idx < 24 * M1; idx += blockDim.x) {
-    const int j = idx / M1, m = idx - j * M1;
-    int c, s;
-    m_comp_of_out(j, c, s);
-    const float2 *Z = zf + (c >> 1) * N;
-    const bool isy = c & 1;
-    float v;
-    if (m == 0) {
-      v = (s == 0) ? an * (isy ? Z[0].y : Z[0].x) : 0.0f;
-    } else {
-      const float2 zk = Z[m], zn = Z[N - m];
-      if (!isy) v = (s == 0) ? an * (zk.x + zn.x) : -an * (zk.y - zn.y);
-      else v = (s == 0) ? an * (zk.y + zn.y) : an * (zk.x - zn.x);
+  for (int p = 0; p < 6; p++) {
+    const float2 *Z = zf + p * NP;
+    float *o0 = O + (2 * p) * 2 * MP, *o1 = O + (2 * p + 1) * 2 * MP;
+    for (int m = tid; m <= L; m += blockDim.x) {
+      if (m == 0) {
+        const float2 z0 = Z[0];
+        o0[0] = an * z0.x; o0[MP] = 0.0f; o1[0] = an * z0.y; o1[MP] = 0.0f;
+      } else {
+        const float2 zk = Z[fpad(m)], zn = Z[fpad(N - m)];
+        o0[m] = an * (zk.x + zn.x); o0[MP + m] = -an * (zk.y - zn.y);
+        o1[m] = an * (zk.y + zn.y); o1[MP + m] = an * (zk.x - zn.x);
+      }
     }
-    O[j * MP + m] = v;
   }
   __syncthreads();
-  float *Pout = fout.P + (size_t)th * fout.sP() + (size_t)k * 8;
-  float *Dout = fout.D + (size_t)th * fout.sD() + (size_t)k * 16;
-  const size_t oP = (size_t)fout.nth * fout.sP(), oD = (size_t)fout.nth * fout.sD();
-  for (int idx = threadIdx.x; idx < 24 * M1; idx += blockDim.x) {
-    const int m = idx / 24, j = idx - 24 * m;
-    const float v = O[j * MP + m];
-    if (j < 8) Pout[m * oP + j] = v;
-    else Dout[m * oD + (j - 8)] = v;
+  // output: one warp per m, lane j < 24 writes element j of the 8 + 16 run
+  {
+    int cs = 0;
+    if (lane < 24) { int c, sg; m_comp_of_out(lane, c, sg); cs = c * 2 + sg; }
+    float *dst = (lane < 8) ? fout.P + (size_t)th * fout.sP() + (size_t)k * 8 + lane
+                            : fout.D + (size_t)th * fout.sD() + (size_t)k * 16 + (lane - 8);
+    const size_t mst = (size_t)fout.nth * ((lane < 8) ? fout.sP() : fout.sD());
+    if (lane < 24)
+      for (int m = warp; m <= L; m += nwarp) dst[m * mst] = O[cs * MP + m];
   }
 }
 
@@ -712,9 +772,26 @@ static FFTPlan make_plan(int n) {
 }
 
 template <int N>
-static int attr_fft_t() {
+static size_t smem_fft_t() { return (14 * (size_t)Plan3x2<N>::NP + N) * sizeof(float2); }
+
+// smem attribute and the per-stage twiddle table w^(r k) of Plan3x2<N>
+template <int N>
+static int attr_fft_t(Ctx &c) {
+  using P = Plan3x2<N>;
   CB2_CUDA(cudaFuncSetAttribute(k_fft_products_t<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(15 * (size_t)N * sizeof(float2))));
+                                (int)smem_fft_t<N>()));
+  std::vector<float2> t(P::ntw());
+  const double pi = 3.14159265358979323846;
+  for (int st = 0; st < P::nst(); st++) {
+    const int R = P::radix(st), NS = P::ns(st), tstr = N / (NS * R);
+    for (int r = 1; r < R; r++)
+      for (int k = 0; k < NS; k++) {
+        const double ang = -2.0 * pi * (double)(r * k * tstr) / (double)N;
+        t[P::off(st) + (r - 1) * NS + k] = float2{(float)std::cos(ang), (float)std::sin(ang)};
+      }
+  }
+  CB2_CUDA(cudaMalloc(&c.d_twp32, t.size() * sizeof(float2)));
+  CB2_CUDA(cudaMemcpy(c.d_twp32, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
   return 0;
 }
 
@@ -741,10 +818,10 @@ int fft_setup(Ctx &c) {
   {
     int rc = 0;
     switch (c.nph) {
-      case 768: rc = attr_fft_t<768>(); break;
-      case 384: rc = attr_fft_t<384>(); break;
-      case 192: rc = attr_fft_t<192>(); break;
-      case 96: rc = attr_fft_t<96>(); break;
+      case 768: rc = attr_fft_t<768>(c); break;
+      case 384: rc = attr_fft_t<384>(c); break;
+      case 192: rc = attr_fft_t<192>(c); break;
+      case 96: rc = attr_fft_t<96>(c); break;
       default: break;
     }
     if (rc) return rc;
@@ -792,9 +869,8 @@ void fft_forward_grid(Ctx &c, int ncomp, const double *grid, T *four) {
 
 template <int N>
 static void launch_fft_t(Ctx &c, const MLayout &in, const MLayout &out, const ProdCoef &pc) {
-  const size_t sm = 15 * (size_t)N * sizeof(float2);
-  k_fft_products_t<N><<<(unsigned)(c.nth * c.nr), 512, sm, c.stream>>>(c.L, in, out, (const float2 *)c.d_tw_fft32,
-                                                                      pc);
+  const size_t sm = smem_fft_t<N>();
+  k_fft_products_t<N><<<(unsigned)(c.nth * c.nr), 512, sm, c.stream>>>(c.L, in, out, (const float2 *)c.d_twp32, pc);
 }
 
 void fft_products_m(Ctx &c, const MLayout &in, const MLayout &out) {

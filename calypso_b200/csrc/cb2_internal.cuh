@@ -86,6 +86,7 @@ struct Ctx {
   int *d_status = nullptr;               // device error word
   double *d_tw_fft = nullptr;            // exp(-2 pi i e / nph), e = 0..nph-1
   float *d_tw_fft32 = nullptr;
+  void *d_twp32 = nullptr;               // per-stage float2 twiddles of the compile-time FFT plans
   // state
   double *d_f = nullptr;                 // NSLOT * nr * jmax
   void *d_four = nullptr;                // F: nth*nr*13*NS (double or float)
