@@ -9,7 +9,11 @@ feeds the CPU oracle).  One "step" is one SPH_analyze_MHD call.
 
 Arms
   (default)          this library on N GPUs (one replica shell per GPU, no
-                     collective in the data path; launched by torchrun for N>1)
+                     collective in the data path; launched by torchrun for N>1),
+                     mixed precision unless --precision fp64.  The FP64 plain
+                     path is timed beside it on the same GPU, and both paths
+                     run --compare-steps steps (500) from the same seeded start
+                     to report the relative energy error of the mixed path.
   --impl reference   the reference's algorithm restated on the CPU (the
                      oracle; the reference's Fortran build is unavailable in
                      this image), timed on the host cores, rank 0 only.
@@ -161,10 +165,12 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--compare-steps", type=int, default=500,
+                    help="steps of the mixed and FP64 runs whose energies are compared")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -210,7 +216,6 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * args.steps / (ms / 1000.0)
-    ene_mixed = g.energies()
 
     # stage breakdown (eager steps with per-stage CUDA events, not the timed run)
     os.environ["CB2_TIMERS"] = "1"
@@ -223,46 +228,66 @@ def main():
     gt.close()
     os.environ.pop("CB2_TIMERS", None)
 
-    L, nr, nth = params["ltr"], params["nr"], params["nth"]
+    L, nr, nth, nph = params["ltr"], params["nr"], params["nth"], params["nph"]
     fb, ff = legendre_flops(L, nr, nth)
     peaks, peak_kind = load_peaks()
     stages = {"explicit": st[6], "implicit+rj_derived": st[7], "coriolis": st[13],
               "legendre_bwd": st[22], "fft_products": st[24], "legendre_fwd": st[23],
               "rj_after_transform": st[17], "step": st[0]}
-    # dominant kernel and its roofline
-    if prec == PREC_MIXED:
-        bound, unit, peak = "tensor", "TFLOP/s", peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"])
-    else:
-        bound, unit, peak = "fp64", "TFLOP/s", 37.0
-    top = max(("legendre_bwd", "legendre_fwd", "fft_products"), key=lambda k: stages[k])
-    if top in ("legendre_bwd", "legendre_fwd"):
-        fl = fb if top == "legendre_bwd" else ff
-        achieved = fl / (stages[top] * 1e-3) / 1e12
-        roof = {"kernel": top, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-                "frac": achieved / peak, "traffic": None,
-                "peak_source": (peak_kind if bound == "tensor" else "nominal B200 FP64 37 TFLOP/s"),
-                "algorithmic_per_launch": fl}
-    else:
-        es = 4 if prec == PREC_MIXED else 8
-        nrow = nth * nr
-        bytes_ = nrow * (13 + 12) * 2 * (L + 1) * es
-        achieved = bytes_ / (stages[top] * 1e-3) / 1e9
-        roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-                "peak_source": peak_kind, "algorithmic_per_launch": bytes_}
+    # dominant transform stage and its roofline.  Algorithmic bytes: one read
+    # of each input and one write of each output (13 spectral slots and 13
+    # Fourier components backward, 12 each forward); algorithmic flops:
+    # legendre_flops.  The mixed Legendre stages execute 3x their flops on
+    # the tensor pipe (split products).
+    es = 4 if prec == PREC_MIXED else 8
+    spec_b = 13 * nr * (L + 1) ** 2 * 8
+    spec_f = 12 * nr * (L + 1) ** 2 * 8
+    four_b = (L + 1) * nth * nr * 26 * es
+    four_f = (L + 1) * nth * nr * 24 * es
+    traffic = {"legendre_bwd": spec_b + four_b, "fft_products": four_b + four_f,
+               "legendre_fwd": four_f + spec_f}
+    flops = {"legendre_bwd": fb, "legendre_fwd": ff}
+    top = max(traffic, key=lambda k: stages[k])
+    t_s = stages[top] * 1e-3
+    achieved = traffic[top] / t_s / 1e9
+    roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                           else "fallback 6650 GB/s",
+            "algorithmic_bytes_per_launch": traffic[top],
+            "per_stage": {}}
+    for k in ("legendre_bwd", "fft_products", "legendre_fwd"):
+        t = stages[k] * 1e-3
+        ent = {"ms": stages[k], "bytes": traffic[k], "hbm_frac": traffic[k] / t / 1e9 / peaks["hbm_gbs"]}
+        if k in flops:
+            ent["flops"] = flops[k]
+            if prec == PREC_MIXED:
+                tp = peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"])
+                ent["tensor_tflops_executed"] = 3 * flops[k] / t / 1e12
+                ent["tensor_frac_of_measured_sustained"] = 3 * flops[k] / t / 1e12 / tp
+            else:
+                ent["fp64_tflops"] = flops[k] / t / 1e12
+        roof["per_stage"][k] = ent
 
-    # FP64 plain path on the same GPU, same steps (speed-up and energy error)
+    # FP64 plain path on the same GPU: speed, and the energies of both paths
+    # after the same number of steps from the same seeded start (the mixed
+    # run continues the timed context)
     fp64 = None
     if prec == PREC_MIXED and not args.no_fp64_compare:
+        ncmp = max(args.compare_steps, 1 + args.warmup + args.steps)
+        g.step(ncmp - g.istep, graph=True)
+        ene_mixed = g.energies()
         g64 = SphMHD(params, PREC_FP64, device=local_rank)
         g64.init_fields(2, seed=1 + rank)
         g64.step(1)
         g64.step(args.warmup, graph=True)
         ms64 = g64.time_steps(args.steps, graph=True)
+        g64.step(ncmp - g64.istep, graph=True)
         e64 = g64.energies()
         rel = np.abs(ene_mixed - e64) / np.abs(e64)
         fp64 = {"steps_per_s": args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
                 "speedup_mixed_over_fp64": (args.steps / (ms / 1000.0)) / (args.steps / (ms64 / 1000.0)),
+                "compare_steps": ncmp,
                 "energy_rel_err_max": float(rel.max()),
                 "energy_rel_err": dict(zip(["K_pol", "K_tor", "K", "T2", "M_pol", "M_tor", "M"],
                                            [float(x) for x in rel]))}
@@ -312,7 +337,7 @@ def main():
                        "l2": "state 3.9 GB > 126 MB L2, no flush needed", "graph": True},
             "roofline": roof, "stages_ms": stages, "cpu_baseline": cpu, "e2e": e2e,
             "fp64_plain": fp64,
-            "gpu_launches": 10 * args.steps, "clocks": clocks,
+            "gpu_launches": (12 if prec == PREC_MIXED else 10) * args.steps, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

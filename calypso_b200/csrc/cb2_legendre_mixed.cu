@@ -57,8 +57,7 @@ namespace cb2 {
 namespace {
 
 constexpr int TM = 128;          // GEMM rows per CTA (= TMEM lanes)
-constexpr int KB = 64;           // K per pipeline stage: one 128-byte swizzle row of fp16
-constexpr int NSTAGE = 2;
+
 constexpr int NTHR = 256;          // two threads per GEMM row
 constexpr int ACC1 = 256;        // TMEM column of the parity-1 accumulator
 constexpr uint32_t TMEM_COLS = 512;
@@ -112,16 +111,6 @@ __device__ inline void tma_load_2d(void *dst, const CUtensorMap *tm, uint64_t *b
       : "memory");
 }
 
-// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
-// 1024 bytes apart (tile base 1024-byte aligned)
-__device__ inline uint64_t smem_desc_sw128(const void *p) {
-  uint64_t d = (uint64_t)((smem_u32(p) & 0x3FFFF) >> 4);
-  d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset
-  d |= (uint64_t)1 << 46;                 // descriptor version of tcgen05
-  d |= (uint64_t)2 << 61;                 // 128-byte swizzle
-  return d;
-}
 
 // instruction descriptor: D f32, A and B f16, both K-major, M x N
 __device__ inline uint32_t idesc_f16_f32(int M, int N) {
@@ -157,11 +146,6 @@ __device__ inline void tmem_ld8(uint32_t taddr, float v[8]) {
   for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// byte offset of the 16-byte chunk holding elements (row, 8c .. 8c+7) in a
-// 128-byte-swizzled K-major tile (the layout TMA SWIZZLE_128B writes)
-__device__ inline uint32_t sw128_chunk(int row, int c) {
-  return (uint32_t)row * 128u + ((uint32_t)(c ^ (row & 7)) << 4);
-}
 
 // largest scaled magnitude: 2^13 <= mx s < 2^14 (fp16 holds up to 65504)
 constexpr int kScaleExp = 14;
@@ -181,340 +165,8 @@ __device__ inline uint32_t pack_half2(__half a, __half b) {
   return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
 }
 
-struct Smem {
-  uint64_t full[NSTAGE], empty[NSTAGE], done;
-  uint32_t tmem_base;
-  int mma_any;
-  float rowscale[TM];
-};
-
-// Order of the K blocks: both parities of block kb back to back (they read
-// the same operand rows), then the blocks only parity 0 has.  Needs
-// nkb0 >= nkb1, true for every gemm here.
-__device__ inline void block_of(int kbi, int nkb1, int &p, int &kb) {
-  if (kbi < 2 * nkb1) { p = kbi & 1; kb = kbi >> 1; }
-  else { p = 0; kb = nkb1 + (kbi - 2 * nkb1); }
-}
-
-// ---------------------------------------------------------------------------
-// The pipelined GEMM of one CTA, shared by the backward and forward kernels.
-// Thread t works on tile row r = t % 128 and K half h = t / 128 (warps w and
-// w + 4 share TMEM lanes 32 (w % 4) ..).  Prob supplies
-//   nkb(p)                K blocks of parity p;
-//   kpad(p)               K extent the MMAs read (multiple of 16);
-//   n(p)                  MMA N (multiple of 16, <= 256);
-//   tma_xy(p, kb, x, y)   origin of the B box;
-//   rowmax(r)             an upper bound of |A| over row r (both parities),
-//                         from the row-maximum tables;
-//   fill(p, kb, r, h, s, hi, lo)  row r's K values 32 h .. 32 h + 31 of block
-//                         (p, kb), scaled by s, split and stored as four
-//                         16-byte chunks into the swizzled hi / lo tiles.
-template <class Prob>
-__device__ bool gemm_tile(const Prob &pr, Smem *sh, unsigned char *base, uint32_t b_rows,
-                          const CUtensorMap *thi, const CUtensorMap *tlo, int *status) {
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int r = tid & (TM - 1), h = tid >> 7;
-  const uint32_t A_BYTES = TM * 128, B_BYTES = b_rows * 128;
-  const uint32_t STAGE = 2 * A_BYTES + 2 * B_BYTES;
-  const int nkb1 = pr.nkb(1), total = pr.nkb(0) + nkb1;
-  if (tid == 0) {
-    for (int s = 0; s < NSTAGE; s++) { mbar_init(&sh->full[s], 1); mbar_init(&sh->empty[s], 1); }
-    mbar_init(&sh->done, 1);
-    sh->mma_any = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem_base)),
-                 "r"(TMEM_COLS));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
-  // per-row power-of-two scale over every K value of the row (both parities)
-  if (h == 0) sh->rowscale[r] = pow2_scale(pr.rowmax(r));
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = sh->tmem_base;
-  const float sc = sh->rowscale[r];
-
-  uint32_t ph_full = 0, ph_empty = 0;   // phase parity of each stage's barriers, one bit per stage
-  int n_tma = 0, n_full = 0;            // thread 0: B stages requested / consumed
-  // fail fast once a wait has run out anywhere in this launch
-  int failed = __syncthreads_or((*(volatile int *)status & CB2_STATUS_PIPE_TIMEOUT) != 0);
-  auto issue_tma = [&](int kbi) {
-    int p, kb, x, y;
-    block_of(kbi, nkb1, p, kb);
-    pr.tma_xy(p, kb, x, y);
-    const int s = kbi % NSTAGE;
-    unsigned char *st = base + s * STAGE;
-    mbar_expect_tx(&sh->full[s], 2 * B_BYTES);
-    tma_load_2d(st + 2 * A_BYTES, thi, &sh->full[s], x, y);
-    tma_load_2d(st + 2 * A_BYTES + B_BYTES, tlo, &sh->full[s], x, y);
-  };
-  if (tid == 0 && total > 0 && !failed) { issue_tma(0); n_tma = 1; }
-  for (int kbi = 0; kbi < total && !failed; kbi++) {
-    int p, kb;
-    block_of(kbi, nkb1, p, kb);
-    const int s = kbi % NSTAGE;
-    unsigned char *st = base + s * STAGE;
-    int f = 0;
-    // the A buffers of stage s were last read by the MMAs of block kbi - NSTAGE
-    if (kbi >= NSTAGE) {
-      if (!mbar_wait(&sh->empty[s], (ph_empty >> s) & 1)) f = 1;
-      ph_empty ^= 1u << s;
-    }
-    // the B tiles of the next block go into the stage the MMAs of block kbi-1 read
-    if (tid == 0 && !f && kbi + 1 < total) {
-      const int s1 = (kbi + 1) % NSTAGE;
-      if (kbi + 1 >= NSTAGE && !mbar_wait(&sh->empty[s1], (ph_empty >> s1) & 1)) f = 1;
-      if (!f) { issue_tma(kbi + 1); n_tma++; }
-    }
-    if (__syncthreads_or(f)) { failed = 1; break; }
-    pr.fill(p, kb, r, h, sc, st, st + A_BYTES);
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      if (!mbar_wait(&sh->full[s], (ph_full >> s) & 1)) {
-        f = 1;
-      } else {
-        n_full++;
-        tc_fence_after();
-        const unsigned char *bhi = st + 2 * A_BYTES, *blo = st + 2 * A_BYTES + B_BYTES;
-        const uint32_t acc = tmem + (uint32_t)(p * ACC1);
-        const uint32_t idesc = idesc_f16_f32(TM, pr.n(p));
-        const int nks = (min(KB, pr.kpad(p) - kb * KB) + 15) / 16;
-        const uint64_t dah = smem_desc_sw128(st), dal = smem_desc_sw128(st + A_BYTES);
-        const uint64_t dbh = smem_desc_sw128(bhi), dbl = smem_desc_sw128(blo);
-        for (int ks = 0; ks < nks; ks++) {
-          const uint64_t o = (uint64_t)(ks * 2);   // +32 bytes along K
-          mma_f16(acc, dah + o, dbh + o, idesc, (kb == 0 && ks == 0) ? 0u : 1u);
-          mma_f16(acc, dah + o, dbl + o, idesc, 1u);
-          mma_f16(acc, dal + o, dbh + o, idesc, 1u);
-        }
-        mma_commit(&sh->empty[s]);
-        sh->mma_any = 1;
-      }
-      ph_full ^= 1u << s;
-    }
-    if (__syncthreads_or(f)) { failed = 1; break; }
-  }
-  // drain: B loads still in flight, then every MMA this CTA issued
-  if (tid == 0) {
-    for (; n_full < n_tma; n_full++) {
-      const int s = n_full % NSTAGE;
-      if (!mbar_wait(&sh->full[s], (ph_full >> s) & 1)) failed = 1;
-      ph_full ^= 1u << s;
-    }
-    if (sh->mma_any) mma_commit(&sh->done);
-  }
-  __syncthreads();
-  int f = failed;
-  if (sh->mma_any && !mbar_wait(&sh->done, 0)) f = 1;
-  f = __syncthreads_or(f);
-  tc_fence_after();
-  if (f && tid == 0) atomicOr(status, CB2_STATUS_PIPE_TIMEOUT);
-  return !f && total > 0;
-}
-
-__device__ inline void tmem_release(Smem *sh) {
-  tc_fence_before();
-  __syncthreads();
-  if ((threadIdx.x >> 5) == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sh->tmem_base), "r"(TMEM_COLS));
-}
-
 __device__ inline unsigned char *smem_base_1024(unsigned char *raw) {
   return (unsigned char *)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
-}
-
-// split 8 scaled values into fp16 hi / lo and store them as one 16-byte chunk each
-__device__ inline void store_chunk(unsigned char *hi, unsigned char *lo, int r, int ch, const float x[8]) {
-  uint32_t hh[4], ll[4];
-#pragma unroll
-  for (int e = 0; e < 8; e += 2) {
-    const __half h0 = __float2half_rn(x[e]), h1 = __float2half_rn(x[e + 1]);
-    hh[e >> 1] = pack_half2(h0, h1);
-    ll[e >> 1] = pack_half2(__float2half_rn(x[e] - __half2float(h0)), __float2half_rn(x[e + 1] - __half2float(h1)));
-  }
-  const uint32_t off = sw128_chunk(r, ch);
-  *reinterpret_cast<uint4 *>(hi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
-  *reinterpret_cast<uint4 *>(lo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
-}
-
-// ---------------------------------------------------------------------------
-// backward: spectra f[slot][k][jj] -> order-major Fourier rows
-struct BwdArgs {
-  int L, nr, jmax, nh, nhp, nth, nvec, nscal;
-  int slot[8];
-  const int *moff;
-  const double *g3rlm, *ar1;
-  const double *f;
-  size_t fs;
-  const float *bunscale;          // [gemm][m][nhp] 1 / column scale of B
-  const int *koff, *klen, *n1;    // per (m, group) K offset / length; dP part length
-  const float *rowmax;            // [field][comp][k][m][s], k_rowmax_spec
-  MLayout out;
-  int *status;
-};
-
-// One tile row of the backward gemms.  gemm P: row (k, field, s), value at
-// K index kk of parity p is f(l = m + p + 2 kk) (times l(l+1)/r^2 for a
-// vector).  gemm DM: row (k, vector, q); K = [dP part | mP part]:
-// dP part, l = m + (1-p) + 2 kk, value sd * X_d(l); mP part, l = m + p +
-// 2 (kk - n1), value sm * X_m(l), with X = (dS/dr)/r or T/r per q.
-struct BwdRow {
-  const double *xa = nullptr, *xb = nullptr;   // spectra at l = m (nullptr: zero)
-  const double *g3 = nullptr;                  // l(l+1) table at l = m (gemm P vectors)
-  double fa = 0.0, fb = 0.0;                   // factors incl. sign
-};
-
-struct BwdProb {
-  const BwdArgs *A;
-  int m, g, nrows, row0, nl;
-  int kl[2], ko[2], n1[2];
-  __device__ int nkb(int p) const { return (kl[p] + KB - 1) / KB; }
-  __device__ int kpad(int p) const { return ((kl[p] + 15) / 16) * 16; }
-  __device__ int n(int) const { return A->nhp; }
-  __device__ void tma_xy(int p, int kb, int &x, int &y) const { x = ko[p] + kb * KB; y = 0; }
-
-  __device__ BwdRow row_src(int r) const {
-    const BwdArgs &b = *A;
-    BwdRow w;
-    const int row = row0 + r;
-    if (row >= nrows) return w;
-    if (g == 0) {
-      const int ng = b.nvec + b.nscal, s = row & 1, v = (row >> 1) % ng, k = (row >> 1) / ng;
-      if (m == 0 && s == 1) return w;
-      const int jjb = b.moff[m] + s * (b.L + 1 - m);
-      w.xa = b.f + (size_t)b.slot[v] * b.fs + (size_t)k * b.jmax + jjb;
-      if (v < b.nvec) {
-        const double ar = b.ar1[k];
-        w.fa = ar * ar;
-        w.g3 = b.g3rlm + jjb;
-      } else {
-        w.fa = 1.0;
-      }
-      return w;
-    }
-    // dP part {D+, D-, -T+, -T-}; mP part {T-, -T+, D-, -D+}; comp 1 = dS/dr, 2 = T
-    const int q = row & 3, v = (row >> 2) % b.nvec, k = (row >> 2) / b.nvec;
-    const double ar = b.ar1[k];
-    const int cd = (q < 2) ? 1 : 2, sd = q & 1, cm = (q < 2) ? 2 : 1, smm = (q & 1) ^ 1;
-    if (!(m == 0 && sd == 1)) {
-      w.xa = b.f + (size_t)(b.slot[v] + cd) * b.fs + (size_t)k * b.jmax + b.moff[m] + sd * (b.L + 1 - m);
-      w.fa = (q < 2) ? ar : -ar;
-    }
-    if (!(m == 0 && smm == 1)) {
-      w.xb = b.f + (size_t)(b.slot[v] + cm) * b.fs + (size_t)k * b.jmax + b.moff[m] + smm * (b.L + 1 - m);
-      w.fb = (q & 1) ? -ar : ar;
-    }
-    return w;
-  }
-
-  // from the table M[field][comp][k][m][s] = max over l of |S l(l+1)| (comp 0,
-  // vectors), |S| (comp 0, scalars), |dS/dr| (comp 1), |T| (comp 2)
-  __device__ float rowmax(int r) const {
-    const BwdArgs &b = *A;
-    const int row = row0 + r;
-    if (row >= nrows) return 0.0f;
-    const int M1 = b.L + 1;
-    auto M = [&](int v, int c, int k, int s) { return b.rowmax[(((size_t)v * 3 + c) * b.nr + k) * 2 * M1 + 2 * m + s]; };
-    if (g == 0) {
-      const int ng = b.nvec + b.nscal, s = row & 1, v = (row >> 1) % ng, k = (row >> 1) / ng;
-      const double ar = b.ar1[k];
-      return (float)((double)M(v, 0, k, s) * ((v < b.nvec) ? ar * ar : 1.0));
-    }
-    const int q = row & 3, v = (row >> 2) % b.nvec, k = (row >> 2) / b.nvec;
-    const int cd = (q < 2) ? 1 : 2, sd = q & 1, cm = (q < 2) ? 2 : 1, smm = (q & 1) ^ 1;
-    return (float)((double)fmaxf(M(v, cd, k, sd), M(v, cm, k, smm)) * b.ar1[k]);
-  }
-
-  __device__ void fill(int p, int kb, int r, int h, float sc, unsigned char *hi, unsigned char *lo) const {
-    const BwdRow w = row_src(r);
-    const int kk0 = kb * KB + h * 32, klp = kl[p], n1p = n1[p];
-    float x[32];
-    if (g == 0) {
-      const double fa = w.fa * (double)sc;
-#pragma unroll
-      for (int e = 0; e < 32; e++) {
-        const int kk = kk0 + e, t = p + 2 * kk;
-        double v = 0.0;
-        if (w.xa && kk < klp) v = __ldg(w.xa + t) * (w.g3 ? __ldg(w.g3 + t) : 1.0);
-        x[e] = (float)(v * fa);
-      }
-    } else {
-      const double fa = w.fa * (double)sc, fb = w.fb * (double)sc;
-#pragma unroll
-      for (int e = 0; e < 32; e++) {
-        const int kk = kk0 + e;
-        double v = 0.0;
-        if (kk < n1p) {
-          if (w.xa) v = __ldg(w.xa + (1 - p) + 2 * kk) * fa;
-        } else if (kk < klp) {
-          if (w.xb) v = __ldg(w.xb + p + 2 * (kk - n1p)) * fb;
-        }
-        x[e] = (float)v;
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < 4; c++) store_chunk(hi, lo, r, h * 4 + c, x + 8 * c);
-  }
-};
-
-__global__ void __launch_bounds__(NTHR, 1)
-k_leg_bwd_mixed(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int tiles_g0,
-                const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo) {
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char *base = smem_base_1024(smem_raw);
-  const uint32_t BR = (uint32_t)a.nhp;
-  Smem *sh = reinterpret_cast<Smem *>(base + NSTAGE * (2 * TM * 128 + 2 * BR * 128));
-  BwdProb pr;
-  pr.A = &a;
-  pr.m = blockIdx.y;
-  pr.g = (blockIdx.x < (unsigned)tiles_g0) ? 0 : 1;
-  pr.nrows = pr.g ? rows_g1 : rows_g0;
-  pr.row0 = (pr.g ? blockIdx.x - tiles_g0 : blockIdx.x) * TM;
-  pr.nl = a.L + 1 - pr.m;
-  const int m = pr.m;
-  for (int p = 0; p < 2; p++) {
-    pr.kl[p] = a.klen[m * 4 + 2 * pr.g + p];
-    pr.ko[p] = a.koff[m * 4 + 2 * pr.g + p];
-    pr.n1[p] = pr.g ? a.n1[m * 2 + p] : 0;
-  }
-  const bool ok = gemm_tile(pr, sh, base, BR, &tm_hi, &tm_lo, a.status);
-  if (ok) {
-    // thread: tile row r (TMEM lane), columns (theta) of half h
-    const int warp = threadIdx.x >> 5;
-    const int r = threadIdx.x & (TM - 1), h = threadIdx.x >> 7, row = pr.row0 + r;
-    const bool valid = row < pr.nrows;
-    const float ua = 1.0f / sh->rowscale[r];
-    const uint32_t tl = sh->tmem_base + ((uint32_t)((warp & 3) * 32) << 16);
-    const bool has1 = pr.kl[1] > 0;
-    float *outb = pr.g ? a.out.D : a.out.P;
-    const size_t so = pr.g ? a.out.sD() : a.out.sP();
-    const float *bun = a.bunscale + ((size_t)pr.g * (a.L + 1) + m) * a.nhp;
-    const int half = (int)BR / 2;
-    for (int t0 = h * half; t0 < (h + 1) * half; t0 += 8) {
-      float e[8], o[8];
-      tmem_ld8(tl + (uint32_t)t0, e);
-      if (has1) {
-        tmem_ld8(tl + (uint32_t)(ACC1 + t0), o);
-      } else {
-#pragma unroll
-        for (int q = 0; q < 8; q++) o[q] = 0.0f;
-      }
-      if (!valid) continue;
-#pragma unroll
-      for (int q = 0; q < 8; q++) {
-        const int i = t0 + q;
-        if (i < a.nh) {
-          const float us = ua * bun[i];
-          outb[((size_t)m * a.nth + i) * so + row] = (e[q] + o[q]) * us;
-          outb[((size_t)m * a.nth + (a.nth - 1 - i)) * so + row] = (e[q] - o[q]) * us;
-        }
-      }
-    }
-  }
-  tmem_release(sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -799,42 +451,315 @@ k_leg_fwd_tma(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int t
 }
 
 // ---------------------------------------------------------------------------
-// Row maxima for the operand scales, one streaming pass each.
+// backward: spectra f[slot][k][jj] -> order-major Fourier rows
 //
-// spectra: M[field][comp][k][m][s] = max over l = m..L of |X(l, m, s)|, X =
-// S l(l+1) (vector comp 0; l(l+1) from g3rlm), S (scalar), dS/dr, T; one
-// warp per (m, s) block of one (field, comp, k) row, lanes over l.
-struct Slots8 {
-  int s[8];
+// Step 1, k_pack_bwd (the reference's rj -> rlm transpose, on the device):
+// the spectra of one order m are rewritten as float32 rows, one row per GEMM
+// row and one contiguous run of rows per (m, parity of l-m, K index):
+//   P block  rlmP[Kbase(m, par) + kk][(k, field, s)]  = S l(l+1)/r^2 (vector)
+//                                                        or the scalar,
+//   D block  rlmD[Kbase(m, par) + kk][(k, vector, q')] = X/r, q' = 2 c + s,
+//            c = 0 dS/dr, 1 T,
+// at l = m + par + 2 kk, with the row maxima over all l (for the scales).
+// Step 2, k_leg_bwd_tma: one CTA = (m, gemm, tile of 128 rows).  For each K
+// block TMA brings the raw rows [32 K][128 rows] and the B tile
+// [nhp theta][32 K]; converter threads scale, sign and split into fp16 hi/lo
+// (64-byte swizzled); two TMEM accumulators (parity of the basis function)
+// give the south (acc0 + acc1) and north (acc0 - acc1) nodes.  gemm DM,
+// accumulator p: dP part from D rows q at parity 1-p with sign {+,+,-,-},
+// then mP part from rows 3-q at parity p with sign {+,-,+,-}.
+struct PackArgs {
+  int L, nr, jmax, nvec, ng, kc;
+  int slot[8];
+  const int *moff;
+  const double *g3rlm, *ar1, *f;
+  size_t fs;
+  float *rlmP, *rlmD;
+  int pitchP, pitchD;      // row pitch (floats) of the two blocks
+  const int *kbase;        // [(L+1) * 2] first K row of (m, parity)
+  float *maxP, *maxD;      // [m][pitch] row maxima
 };
 
 __global__ void __launch_bounds__(256)
-k_rowmax_spec(int L, int nr, int jmax, int nvec, Slots8 slot, const int *moff, const double *g3rlm,
-              const double *f, size_t fs, float *M) {
-  const int k = blockIdx.x, v = blockIdx.y, c = blockIdx.z;
-  const bool isvec = v < nvec;
-  if (!isvec && c > 0) return;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, M1 = L + 1;
-  const double *x = f + (size_t)(slot.s[v] + c) * fs + (size_t)k * jmax;
-  float *out = M + (((size_t)v * 3 + c) * nr + k) * 2 * M1;
-  for (int seg = warp; seg < 2 * M1; seg += blockDim.x >> 5) {
-    const int m = seg >> 1, s = seg & 1;
-    if (m == 0 && s == 1) {
-      if (lane == 0) out[1] = 0.0f;
-      continue;
+k_pack_bwd(const __grid_constant__ PackArgs a) {
+  extern __shared__ float T[];   // [kc * RK][NLP]
+  const int m = blockIdx.x, k0 = blockIdx.y * a.kc, nk = min(a.kc, a.nr - k0);
+  const int nl = a.L + 1 - m, NLP = nl | 1;
+  const int RP = 2 * a.ng, RD = 4 * a.nvec, RK = RP + RD;
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < nk * RK * nl; idx += blockDim.x) {
+    const int rl = idx / nl, lm = idx - rl * nl, kq = rl / RK, j = rl - kq * RK, k = k0 + kq;
+    float v = 0.0f;
+    if (j < RP) {
+      const int fl = j >> 1, s = j & 1;
+      if (!(m == 0 && s == 1)) {
+        const int jj = a.moff[m] + s * (a.L + 1 - m) + lm;
+        double x = __ldg(a.f + (size_t)a.slot[fl] * a.fs + (size_t)k * a.jmax + jj);
+        if (fl < a.nvec) { const double ar = a.ar1[k]; x *= ar * ar * __ldg(a.g3rlm + jj); }
+        v = (float)x;
+      }
+    } else {
+      const int jd = j - RP, vv = jd >> 2, qd = jd & 3, comp = qd >> 1, s = qd & 1;
+      if (!(m == 0 && s == 1)) {
+        const int jj = a.moff[m] + s * (a.L + 1 - m) + lm;
+        v = (float)(__ldg(a.f + (size_t)(a.slot[vv] + 1 + comp) * a.fs + (size_t)k * a.jmax + jj) * a.ar1[k]);
+      }
     }
-    const int nl = L + 1 - m, jjb = moff[m] + s * (L + 1 - m);
-    double mx = 0.0;
-    for (int t = lane; t < nl; t += 32) {
-      double a = fabs(x[jjb + t]);
-      if (isvec && c == 0) a *= g3rlm[jjb + t];
-      mx = fmax(mx, a);
+    T[rl * NLP + lm] = v;
+  }
+  __syncthreads();
+  // row maxima: one warp per row
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int rl = warp; rl < nk * RK; rl += blockDim.x >> 5) {
+    float mx = 0.0f;
+    for (int lm = lane; lm < nl; lm += 32) mx = fmaxf(mx, fabsf(T[rl * NLP + lm]));
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) {
+      const int kq = rl / RK, j = rl - kq * RK, k = k0 + kq;
+      if (j < RP) a.maxP[(size_t)m * a.pitchP + k * RP + j] = mx;
+      else a.maxD[(size_t)m * a.pitchD + k * RD + (j - RP)] = mx;
     }
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) out[seg] = (float)mx;
+  }
+  // rows out, contiguous in (k, row) for each (parity, kk)
+  for (int par = 0; par < 2; par++) {
+    const int cnt = par ? nl / 2 : (nl + 1) / 2;
+    const size_t base = a.kbase[m * 2 + par];
+    const int wP = nk * RP, wD = nk * RD;
+    for (int idx = tid; idx < cnt * wP; idx += blockDim.x) {
+      const int kk = idx / wP, rr = idx - kk * wP, kq = rr / RP, j = rr - kq * RP;
+      a.rlmP[(base + kk) * a.pitchP + (size_t)k0 * RP + rr] = T[(kq * RK + j) * NLP + par + 2 * kk];
+    }
+    for (int idx = tid; idx < cnt * wD; idx += blockDim.x) {
+      const int kk = idx / wD, rr = idx - kk * wD, kq = rr / RD, j = rr - kq * RD;
+      a.rlmD[(base + kk) * a.pitchD + (size_t)k0 * RD + rr] = T[(kq * RK + RP + j) * NLP + par + 2 * kk];
+    }
   }
 }
 
+struct BwdArgs {
+  int L, nr, nh, nhp, nth, nvec, nscal;
+  int pitchP, pitchD;
+  const int *kbase;        // as in PackArgs
+  const int *ko;           // [(m * 4 + group) * 2 + part] B column offset (multiples of 32)
+  const float *maxP, *maxD;
+  const float *bunscale;   // [gemm][m][nhp] 1 / column scale of B
+  MLayout out;
+  int *status;
+};
+
+struct BwdSmem {
+  uint64_t full[FST], mmadone[FST], done;
+  uint32_t tmem_base;
+  int mma_any;
+  float rowscale[TM];
+};
+
+constexpr uint32_t BRAW_BYTES = FKB * TM * 4;   // raw rows of one K block
+
+__global__ void __launch_bounds__(NTHR, 1)
+k_leg_bwd_tma(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int tiles_g0,
+              const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
+              const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char *base = smem_base_1024(smem_raw);
+  const uint32_t B_BYTES = (uint32_t)a.nhp * FKB * 2;       // one of hi / lo
+  const uint32_t ST_BYTES = BRAW_BYTES + 2 * FA_BYTES + 2 * B_BYTES;
+  BwdSmem *sh = reinterpret_cast<BwdSmem *>(base + FST * ST_BYTES);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int r = tid & (TM - 1), h = tid >> 7;
+  const int m = blockIdx.y;
+  const int g = (blockIdx.x < (unsigned)tiles_g0) ? 0 : 1;
+  const int nrows = g ? rows_g1 : rows_g0;
+  const int row0 = (g ? blockIdx.x - tiles_g0 : blockIdx.x) * TM;
+  const int nl = a.L + 1 - m, cnt0 = (nl + 1) / 2, cnt1 = nl / 2;
+  // K parts per accumulator p: gemm P one part (parity p); gemm DM dP part
+  // (parity 1-p) then mP part (parity p)
+  int plen[2][2], pblk[2][2], nkb[2];
+  for (int p = 0; p < 2; p++) {
+    const int cp = p ? cnt1 : cnt0, cq = p ? cnt0 : cnt1;
+    plen[p][0] = g ? cq : cp;
+    plen[p][1] = g ? cp : 0;
+    pblk[p][0] = (plen[p][0] + FKB - 1) / FKB;
+    pblk[p][1] = (plen[p][1] + FKB - 1) / FKB;
+    nkb[p] = pblk[p][0] + pblk[p][1];
+  }
+  const int nmin = min(nkb[0], nkb[1]), total = nkb[0] + nkb[1];
+  const int pmore = (nkb[0] >= nkb[1]) ? 0 : 1;
+  // block b -> accumulator p, part, block index within the part
+  auto blk = [&](int b, int &p, int &part, int &ib) {
+    int i;
+    if (b < 2 * nmin) { p = b & 1; i = b >> 1; } else { p = pmore; i = nmin + (b - 2 * nmin); }
+    part = (i < pblk[p][0]) ? 0 : 1;
+    ib = part ? i - pblk[p][0] : i;
+  };
+  const CUtensorMap *traw = g ? &tm_rawD : &tm_rawP;
+
+  if (tid == 0) {
+    for (int q = 0; q < FST; q++) { mbar_init(&sh->full[q], 1); mbar_init(&sh->mmadone[q], 1); }
+    mbar_init(&sh->done, 1);
+    sh->mma_any = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem_base)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  const int row = row0 + r, q4 = row & 3;
+  if (h == 0) {
+    float mx = 0.0f;
+    if (row < nrows) {
+      if (g == 0) mx = a.maxP[(size_t)m * a.pitchP + row];
+      else mx = fmaxf(a.maxD[(size_t)m * a.pitchD + row], a.maxD[(size_t)m * a.pitchD + row - q4 + 3 - q4]);
+    }
+    sh->rowscale[r] = pow2_scale(mx);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh->tmem_base;
+
+  auto issue = [&](int b) {
+    int p, part, ib;
+    blk(b, p, part, ib);
+    const int q = b % FST;
+    unsigned char *st = base + q * ST_BYTES;
+    // raw rows: parity of l-m of this part
+    const int par = (g == 0) ? p : (part == 0 ? 1 - p : p);
+    const int ky = a.kbase[m * 2 + par] + ib * FKB;
+    const int gi = g * 2 + p;
+    const int bx = a.ko[(m * 4 + gi) * 2 + part] + ib * FKB;
+    mbar_expect_tx(&sh->full[q], BRAW_BYTES + 2 * B_BYTES);
+    tma_load_2d(st, traw, &sh->full[q], row0, ky);
+    tma_load_2d(st + BRAW_BYTES + 2 * FA_BYTES, &tb_hi, &sh->full[q], bx, 0);
+    tma_load_2d(st + BRAW_BYTES + 2 * FA_BYTES + B_BYTES, &tb_lo, &sh->full[q], bx, 0);
+  };
+
+  int n_iss = 0, n_done = 0;   // thread 0 bookkeeping
+  int failed = __syncthreads_or((*(volatile int *)a.status & CB2_STATUS_PIPE_TIMEOUT) != 0);
+  if (tid == 0 && !failed)
+    for (int b = 0; b < min(total, FST - 1); b++) { issue(b); n_iss++; }
+  const float sc = sh->rowscale[r];
+  for (int b = 0; b < total && !failed; b++) {
+    int p, part, ib;
+    blk(b, p, part, ib);
+    const int s = b % FST;
+    unsigned char *st = base + s * ST_BYTES;
+    int f = 0;
+    if (!mbar_wait(&sh->full[s], (uint32_t)((b / FST) & 1))) f = 1;
+    if (__syncthreads_or(f)) { failed = 1; break; }
+    // convert: thread (r, h) builds K values 16 h .. 16 h + 15 of row r
+    {
+      const float *raw = reinterpret_cast<const float *>(st);
+      int src = r;
+      float sg = sc;
+      if (g) {
+        if (part == 0) sg = (q4 < 2) ? sc : -sc;
+        else { src = r - q4 + 3 - q4; sg = (q4 & 1) ? -sc : sc; }
+      }
+      const int kv = plen[p][part] - ib * FKB;   // valid K entries of this block
+      float x[16];
+#pragma unroll
+      for (int e = 0; e < 16; e++) {
+        const int kk = h * 16 + e;
+        x[e] = (kk < kv) ? raw[kk * TM + src] * sg : 0.0f;
+      }
+      unsigned char *ahi = st + BRAW_BYTES, *alo = ahi + FA_BYTES;
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        uint32_t hh[4], ll[4];
+#pragma unroll
+        for (int e = 0; e < 8; e += 2) {
+          const float x0 = x[c * 8 + e], x1 = x[c * 8 + e + 1];
+          const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
+          hh[e >> 1] = pack_half2(h0, h1);
+          ll[e >> 1] = pack_half2(__float2half_rn(x0 - __half2float(h0)), __float2half_rn(x1 - __half2float(h1)));
+        }
+        const uint32_t off = sw64_chunk(r, 2 * h + c);
+        *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+        *reinterpret_cast<uint4 *>(alo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+      }
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      n_done = b + 1;
+      tc_fence_after();
+      unsigned char *ahi = st + BRAW_BYTES, *alo = ahi + FA_BYTES;
+      unsigned char *bh = alo + FA_BYTES, *bl = bh + B_BYTES;
+      const uint32_t idesc = idesc_f16_f32(TM, a.nhp);
+      const uint64_t dah = smem_desc_sw64(ahi), dal = smem_desc_sw64(alo);
+      const uint64_t dbh = smem_desc_sw64(bh), dbl = smem_desc_sw64(bl);
+      const uint32_t acc = tmem + (uint32_t)(p * ACC1);
+      const bool first = (ib == 0) && (part == 0 || pblk[p][0] == 0);   // first block of accumulator p
+#pragma unroll
+      for (int ks = 0; ks < FKB / 16; ks++) {
+        const uint64_t o = (uint64_t)(ks * 2);
+        mma_f16(acc, dah + o, dbh + o, idesc, (first && ks == 0) ? 0u : 1u);
+        mma_f16(acc, dah + o, dbl + o, idesc, 1u);
+        mma_f16(acc, dal + o, dbh + o, idesc, 1u);
+      }
+      mma_commit(&sh->mmadone[s]);
+      sh->mma_any = 1;
+      // block b + FST - 1 goes to the stage of block b - 1, free once its MMAs are done
+      const int bn = b + FST - 1;
+      if (bn < total) {
+        if (bn >= FST && !mbar_wait(&sh->mmadone[bn % FST], (uint32_t)(((bn - FST) / FST) & 1))) f = 1;
+        else { issue(bn); n_iss++; }
+      }
+    }
+    if (__syncthreads_or(f)) { failed = 1; break; }
+  }
+  if (tid == 0) {
+    for (int b = n_done; b < n_iss; b++)
+      if (!mbar_wait(&sh->full[b % FST], (uint32_t)((b / FST) & 1))) failed = 1;
+    if (sh->mma_any) mma_commit(&sh->done);
+  }
+  __syncthreads();
+  int f = failed;
+  if (sh->mma_any && !mbar_wait(&sh->done, 0)) f = 1;
+  f = __syncthreads_or(f);
+  tc_fence_after();
+  if (f && tid == 0) atomicOr(a.status, CB2_STATUS_PIPE_TIMEOUT);
+  if (!f && total > 0) {
+    const bool valid = row < nrows;
+    const float ua = 1.0f / sc;
+    const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const bool has1 = nkb[1] > 0;
+    float *outb = g ? a.out.D : a.out.P;
+    const size_t so = g ? a.out.sD() : a.out.sP();
+    const float *bun = a.bunscale + ((size_t)g * (a.L + 1) + m) * a.nhp;
+    const int half = a.nhp / 2;
+    for (int t0 = h * half; t0 < (h + 1) * half; t0 += 8) {
+      float e[8], o[8];
+      tmem_ld8(tl + (uint32_t)t0, e);
+      if (has1) {
+        tmem_ld8(tl + (uint32_t)(ACC1 + t0), o);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; q++) o[q] = 0.0f;
+      }
+      if (!valid) continue;
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const int i = t0 + q;
+        if (i < a.nh) {
+          const float us = ua * bun[i];
+          outb[((size_t)m * a.nth + i) * so + row] = (e[q] + o[q]) * us;
+          outb[((size_t)m * a.nth + (a.nth - 1 - i)) * so + row] = (e[q] - o[q]) * us;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+}
+
+// ---------------------------------------------------------------------------
+// Row maxima for the operand scales, one streaming pass each.
+//
 // Fourier rows: Mf[m][e] = 2 max over theta of |F(m, theta, e) w(theta)|
 // for every element e of the P block and then the D block; one thread per
 // (m, e), consecutive threads on consecutive elements.
@@ -861,13 +786,16 @@ __device__ inline void split_store(__half *hi, __half *lo, size_t at, double v, 
   lo[at] = __float2half_rn((float)(x - (double)__half2float(h)));
 }
 
-// backward B[theta][K]: one thread per (m, south node i)
+// backward B[theta][K]: one thread per (m, south node i).  Column groups per
+// m: P0, P1 (P_l^m, l - m even / odd), D0 = {dP of odd l-m | mP of even l-m},
+// D1 = {dP of even | mP of odd}; each part starts at ko[(m * 4 + group) * 2 +
+// part], a multiple of 32, so no K block of 32 mixes two parts.
 __global__ void k_build_bwd_b(int L, int nh, int nhp, const size_t *poff, const double *Plt, const double *dPlt,
-                              const double *asin_t, const int *koff, const int *klen, const int *n1, int Kb_all,
-                              float *bunscale, __half *bhi, __half *blo) {
+                              const double *asin_t, const int *ko, int Kc, float *bunscale, __half *bhi,
+                              __half *blo) {
   const int m = blockIdx.y, i = blockIdx.x * blockDim.x + threadIdx.x;
   if (m > L || i >= nh) return;
-  const int nl = L + 1 - m;
+  const int nl = L + 1 - m, cnt[2] = {(nl + 1) / 2, nl / 2};
   const size_t po = poff[m];
   const double am = (double)m * asin_t[i];
   double mxp = 0.0, mxd = 0.0;
@@ -879,26 +807,18 @@ __global__ void k_build_bwd_b(int L, int nh, int nhp, const size_t *poff, const 
   const float sp = pow2_scale(mxp), sd = pow2_scale(mxd);
   bunscale[(size_t)m * nhp + i] = 1.0f / sp;                     // gemm P
   bunscale[((size_t)(L + 1) + m) * nhp + i] = 1.0f / sd;         // gemm DM
-  for (int gi = 0; gi < 4; gi++) {
-    const int ko = koff[m * 4 + gi], kl = klen[m * 4 + gi];
-    const float s = (gi < 2) ? sp : sd;
-    for (int kk = 0; kk < kl; kk++) {
-      double v;
-      if (gi < 2) {
-        const int l = m + gi + 2 * kk;
-        v = Plt[po + (size_t)(l - m) * nh + i];
-      } else {
-        const int p = gi - 2, nn = n1[m * 2 + p];
-        if (kk < nn) {
-          const int l = m + (1 - p) + 2 * kk;
-          v = dPlt[po + (size_t)(l - m) * nh + i];
-        } else {
-          const int l = m + p + 2 * (kk - nn);
-          v = Plt[po + (size_t)(l - m) * nh + i] * am;
-        }
-      }
-      split_store(bhi, blo, (size_t)i * Kb_all + ko + kk, v, s);
-    }
+  __half *hrow = bhi + (size_t)i * Kc, *lrow = blo + (size_t)i * Kc;
+  for (int p = 0; p < 2; p++) {
+    // P_p: P at l = m + p + 2 kk
+    const int oP = ko[(m * 4 + p) * 2];
+    for (int kk = 0; kk < cnt[p]; kk++)
+      split_store(hrow, lrow, oP + kk, Plt[po + (size_t)(p + 2 * kk) * nh + i], sp);
+    // D_p: dP at l = m + (1-p) + 2 kk, then P m / sin(theta) at l = m + p + 2 kk
+    const int oA = ko[(m * 4 + 2 + p) * 2], oB = ko[(m * 4 + 2 + p) * 2 + 1];
+    for (int kk = 0; kk < cnt[1 - p]; kk++)
+      split_store(hrow, lrow, oA + kk, dPlt[po + (size_t)((1 - p) + 2 * kk) * nh + i], sd);
+    for (int kk = 0; kk < cnt[p]; kk++)
+      split_store(hrow, lrow, oB + kk, Plt[po + (size_t)(p + 2 * kk) * nh + i] * am, sd);
   }
 }
 
@@ -936,16 +856,19 @@ __global__ void k_build_fwd_b(int L, int nh, int nhp, int NFmax, const size_t *p
 struct MixedTables {
   __half *bb_hi = nullptr, *bb_lo = nullptr;      // backward B [nhp][Kb_all]
   float *bb_unscale = nullptr;                    // [gemm][m][nhp]
-  int *bb_koff = nullptr, *bb_klen = nullptr, *bb_n1 = nullptr;
+  int *bb_ko = nullptr;                           // [(m * 4 + group) * 2 + part]
+  int *kbase = nullptr;                           // [(L+1) * 2] first rlm row of (m, parity)
+  float *rlmP = nullptr, *rlmD = nullptr;         // [Ktot][pitch] order-major spectra
+  float *maxP = nullptr, *maxD = nullptr;         // [(L+1)][pitch] their row maxima
+  int Ktot = 0, pitch_max = 0;
   __half *bfp_hi = nullptr, *bfp_lo = nullptr;    // forward B (P) [rows_all][nhp]
   __half *bfd_hi = nullptr, *bfd_lo = nullptr;    // forward B (DM) [rows_all][2 nhp]
   float *bf_unscale = nullptr;                    // [gemm][(m, parity)][NFmax]
   int *bf_roff = nullptr, *bf_nl = nullptr;
   float *wgt32 = nullptr;                         // Gauss weights in float
-  float *rowmax_spec = nullptr;                   // [8 fields][3][nr][2 (L+1)]
   float *rowmax_four = nullptr;                   // [(L+1)][26 nr + 8]
   int Kb_all = 0, rows_all = 0, nhp = 0, NFmax = 0;
-  size_t smem_bwd = 0, smem_fwd = 0;
+  size_t smem_bwd = 0, smem_fwd = 0, smem_pack = 0;
   CUtensorMap tm_bb_hi, tm_bb_lo, tm_bfp_hi, tm_bfp_lo, tm_bfd_hi, tm_bfd_lo;
   int boxr = 0, nfb = 0;
   uint32_t tmem_fwd = 0;
@@ -986,12 +909,6 @@ int make_map_any(CUtensorMap *tm, CUtensorMapDataType dt, size_t es, const void 
   return 0;
 }
 
-// fp16 [rows][cols], box 64 x box_rows, 128-byte swizzle (backward B tiles)
-int make_map(CUtensorMap *tm, const void *ptr, uint64_t cols, uint64_t rows, uint32_t box_rows) {
-  if (rows < box_rows) { set_error("tensor map shape"); return CB2_ERR_ARG; }
-  return make_map_any(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, ptr, cols, rows, KB, box_rows,
-                      CU_TENSOR_MAP_SWIZZLE_128B);
-}
 
 // fp16 [rows][cols], box 32 x box_rows, 64-byte swizzle (forward B tiles)
 int make_map64(CUtensorMap *tm, const void *ptr, uint64_t cols, uint64_t rows, uint32_t box_rows) {
@@ -999,12 +916,6 @@ int make_map64(CUtensorMap *tm, const void *ptr, uint64_t cols, uint64_t rows, u
                       CU_TENSOR_MAP_SWIZZLE_64B);
 }
 
-// 1024 alignment slack + stages + control block; at least 120 KB so a CTA
-// holding 512 TMEM columns has the SM to itself
-size_t smem_bytes(int b_rows) {
-  size_t s = 1024 + (size_t)NSTAGE * (2 * TM * 128 + 2 * (size_t)b_rows * 128) + sizeof(Smem);
-  return std::max(s, (size_t)120 * 1024);
-}
 
 }  // namespace
 
@@ -1014,21 +925,26 @@ int mixed_setup(Ctx &c) {
   const int L = c.L, nh = c.nh;
   t->nhp = ((nh + 15) / 16) * 16;
   if (t->nhp > 256) { set_error("mixed precision path needs nth <= 512"); return CB2_ERR_ARG; }
-  // backward K groups per m: P0, P1 (l-m even / odd), D0 = {dP odd | mP even}, D1 = {dP even | mP odd}
-  std::vector<int> koff((L + 1) * 4), klen((L + 1) * 4), n1((L + 1) * 2);
-  int K = 0;
+  // backward B column parts per m (each padded to 32): P0 {P, l-m even},
+  // P1 {P, odd}, D0 {dP odd | mP even}, D1 {dP even | mP odd}; and the first
+  // order-major spectral row of each (m, parity)
+  std::vector<int> ko((L + 1) * 8, 0), kbase((L + 1) * 2);
+  int K = 0, Kr = 0;
   for (int m = 0; m <= L; m++) {
-    const int nl = L + 1 - m, ne = (nl + 1) / 2, no = nl / 2;
-    const int lens[4] = {ne, no, no + ne, ne + no};
-    n1[m * 2 + 0] = no;
-    n1[m * 2 + 1] = ne;
-    for (int gi = 0; gi < 4; gi++) {
-      koff[m * 4 + gi] = K;
-      klen[m * 4 + gi] = lens[gi];
-      K += ((lens[gi] + 15) / 16) * 16;
-    }
+    const int nl = L + 1 - m, cnt[2] = {(nl + 1) / 2, nl / 2};
+    const int lens[4][2] = {{cnt[0], 0}, {cnt[1], 0}, {cnt[1], cnt[0]}, {cnt[0], cnt[1]}};
+    for (int gi = 0; gi < 4; gi++)
+      for (int part = 0; part < 2; part++) {
+        ko[(m * 4 + gi) * 2 + part] = K;
+        K += ((lens[gi][part] + FKB - 1) / FKB) * FKB;
+      }
+    kbase[m * 2] = Kr;
+    kbase[m * 2 + 1] = Kr + cnt[0];
+    Kr += nl;
   }
-  t->Kb_all = K + KB;   // every 64-wide box starting at a group stays in the array
+  t->Kb_all = K + FKB;
+  t->Ktot = Kr;
+  t->pitch_max = ((16 * c.nr + 3) / 4) * 4;   // up to 8 fields (P) or 4 vectors (D)
   // forward B rows: per (m, parity) the degrees l = m + p + 2t
   std::vector<int> roff((L + 1) * 2), nlp((L + 1) * 2);
   int R = 0, nfmax = 16;
@@ -1056,9 +972,13 @@ int mixed_setup(Ctx &c) {
     return 0;
   };
   int rc;
-  if ((rc = up(&t->bb_koff, koff)) || (rc = up(&t->bb_klen, klen)) || (rc = up(&t->bb_n1, n1)) ||
-      (rc = up(&t->bf_roff, roff)) || (rc = up(&t->bf_nl, nlp)))
+  if ((rc = up(&t->bb_ko, ko)) || (rc = up(&t->kbase, kbase)) || (rc = up(&t->bf_roff, roff)) ||
+      (rc = up(&t->bf_nl, nlp)))
     return rc;
+  CB2_CUDA(cudaMalloc(&t->rlmP, (size_t)t->Ktot * t->pitch_max * sizeof(float)));
+  CB2_CUDA(cudaMalloc(&t->rlmD, (size_t)t->Ktot * t->pitch_max * sizeof(float)));
+  CB2_CUDA(cudaMalloc(&t->maxP, (size_t)(L + 1) * t->pitch_max * sizeof(float)));
+  CB2_CUDA(cudaMalloc(&t->maxD, (size_t)(L + 1) * t->pitch_max * sizeof(float)));
   const size_t nb = (size_t)t->nhp * t->Kb_all;
   const size_t nfp = (size_t)t->rows_all * t->nhp, nfd = 2 * nfp;
   __half **bufs[6] = {&t->bb_hi, &t->bb_lo, &t->bfp_hi, &t->bfp_lo, &t->bfd_hi, &t->bfd_lo};
@@ -1077,32 +997,34 @@ int mixed_setup(Ctx &c) {
     CB2_CUDA(cudaMalloc(&t->wgt32, w.size() * sizeof(float)));
     CB2_CUDA(cudaMemcpy(t->wgt32, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
-  CB2_CUDA(cudaMalloc(&t->rowmax_spec, (size_t)8 * 3 * c.nr * 2 * (L + 1) * sizeof(float)));
   CB2_CUDA(cudaMalloc(&t->rowmax_four, (size_t)(L + 1) * (26 * (size_t)c.nr + 8) * sizeof(float)));
   k_build_bwd_b<<<dim3(cdiv(nh, 64), L + 1), 64, 0, c.stream>>>(L, nh, t->nhp, c.d_poff, c.d_Plt, c.d_dPlt,
-                                                                c.d_asin, t->bb_koff, t->bb_klen, t->bb_n1,
-                                                                t->Kb_all, t->bb_unscale, t->bb_hi, t->bb_lo);
+                                                                c.d_asin, t->bb_ko, t->Kb_all, t->bb_unscale,
+                                                                t->bb_hi, t->bb_lo);
   CB2_CUDA(cudaGetLastError());
   k_build_fwd_b<<<dim3(cdiv(t->NFmax, 64), L + 1), 64, 0, c.stream>>>(
       L, nh, t->nhp, t->NFmax, c.d_poff, c.d_Plt, c.d_dPlt, c.d_asin, t->bf_roff, t->bf_nl, t->bf_unscale,
       t->bfp_hi, t->bfp_lo, t->bfd_hi, t->bfd_lo);
   CB2_CUDA(cudaGetLastError());
   CB2_CUDA(cudaStreamSynchronize(c.stream));
-  if ((rc = make_map(&t->tm_bb_hi, t->bb_hi, t->Kb_all, t->nhp, t->nhp)) ||
-      (rc = make_map(&t->tm_bb_lo, t->bb_lo, t->Kb_all, t->nhp, t->nhp)) ||
+  if ((rc = make_map64(&t->tm_bb_hi, t->bb_hi, t->Kb_all, t->nhp, t->nhp)) ||
+      (rc = make_map64(&t->tm_bb_lo, t->bb_lo, t->Kb_all, t->nhp, t->nhp)) ||
       (rc = make_map64(&t->tm_bfp_hi, t->bfp_hi, t->nhp, t->rows_all, t->boxr)) ||
       (rc = make_map64(&t->tm_bfp_lo, t->bfp_lo, t->nhp, t->rows_all, t->boxr)) ||
       (rc = make_map64(&t->tm_bfd_hi, t->bfd_hi, 2 * t->nhp, t->rows_all, t->boxr)) ||
       (rc = make_map64(&t->tm_bfd_lo, t->bfd_lo, 2 * t->nhp, t->rows_all, t->boxr)))
     return rc;
-  t->smem_bwd = smem_bytes(t->nhp);
+  t->smem_bwd = 1024 + FST * ((size_t)BRAW_BYTES + 2 * (size_t)FA_BYTES + 2 * (size_t)t->nhp * FKB * 2) +
+                sizeof(BwdSmem);
+  t->smem_pack = (size_t)2 * 26 * ((L + 1) | 1) * sizeof(float);
   t->smem_fwd = 1024 + FST * (size_t)RAW_BYTES + FST * (2 * (size_t)FA_BYTES + 2 * (size_t)t->nfb * FKB * 2) +
                 sizeof(FwdSmem);
   if (t->smem_bwd > 227 * 1024 || t->smem_fwd > 227 * 1024) {
     set_error("mixed precision tiles exceed shared memory");
     return CB2_ERR_ARG;
   }
-  CB2_CUDA(cudaFuncSetAttribute(k_leg_bwd_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_bwd));
+  CB2_CUDA(cudaFuncSetAttribute(k_leg_bwd_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_bwd));
+  CB2_CUDA(cudaFuncSetAttribute(k_pack_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_pack));
   CB2_CUDA(cudaFuncSetAttribute(k_leg_fwd_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_fwd));
   return 0;
 }
@@ -1110,9 +1032,9 @@ int mixed_setup(Ctx &c) {
 void mixed_free(Ctx &c) {
   MixedTables *t = (MixedTables *)c.mixed;
   if (!t) return;
-  void *ptrs[] = {t->bb_hi, t->bb_lo, t->bb_unscale, t->bb_koff, t->bb_klen, t->bb_n1, t->bfp_hi,
-                  t->bfp_lo, t->bfd_hi, t->bfd_lo, t->bf_unscale, t->bf_roff, t->bf_nl, t->wgt32,
-                  t->rowmax_spec, t->rowmax_four};
+  void *ptrs[] = {t->bb_hi, t->bb_lo, t->bb_unscale, t->bb_ko, t->kbase, t->rlmP, t->rlmD, t->maxP, t->maxD,
+                  t->bfp_hi, t->bfp_lo, t->bfd_hi, t->bfd_lo, t->bf_unscale, t->bf_roff, t->bf_nl, t->wgt32,
+                  t->rowmax_four};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete t;
@@ -1131,23 +1053,41 @@ MLayout mlayout(const Ctx &c, void *buf, int nvec, int nscal) {
 
 int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   MixedTables *t = (MixedTables *)c.mixed;
-  const int nvec = out.nvec, nscal = out.nscal;
+  const int nvec = out.nvec, nscal = out.nscal, ng = nvec + nscal;
+  const int pitchP = ((2 * ng * c.nr + 3) / 4) * 4, pitchD = ((4 * nvec * c.nr + 3) / 4) * 4;
+  if (ng > 8 || nvec > 4 || pitchP > t->pitch_max || pitchD > t->pitch_max) {
+    set_error("mixed backward transform: at most 8 fields and 4 vectors");
+    return CB2_ERR_ARG;
+  }
+  // step 1: order-major float32 spectra and their row maxima
+  PackArgs pk{};
+  pk.L = c.L; pk.nr = c.nr; pk.jmax = c.jmax; pk.nvec = nvec; pk.ng = ng; pk.kc = 2;
+  for (int q = 0; q < ng; q++) pk.slot[q] = slots[q];
+  pk.moff = c.d_moff; pk.g3rlm = c.d_g3rlm; pk.ar1 = c.d_ar1; pk.f = c.d_f; pk.fs = c.fsize();
+  pk.rlmP = t->rlmP; pk.rlmD = t->rlmD; pk.pitchP = pitchP; pk.pitchD = pitchD;
+  pk.kbase = t->kbase; pk.maxP = t->maxP; pk.maxD = t->maxD;
+  k_pack_bwd<<<dim3(c.L + 1, cdiv(c.nr, pk.kc)), 256, t->smem_pack, c.stream>>>(pk);
+  // step 2: the tensor-core transform
+  CUtensorMap rawP{}, rawD{};
+  if (make_map_any(&rawP, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, t->rlmP, pitchP, t->Ktot, TM, FKB,
+                   CU_TENSOR_MAP_SWIZZLE_NONE))
+    return CB2_ERR_ARG;
+  if (nvec > 0) {
+    if (make_map_any(&rawD, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, t->rlmD, pitchD, t->Ktot, TM, FKB,
+                     CU_TENSOR_MAP_SWIZZLE_NONE))
+      return CB2_ERR_ARG;
+  } else {
+    rawD = rawP;
+  }
   BwdArgs a{};
-  a.L = c.L; a.nr = c.nr; a.jmax = c.jmax; a.nh = c.nh; a.nhp = t->nhp; a.nth = c.nth;
-  a.nvec = nvec; a.nscal = nscal;
-  for (int q = 0; q < nvec + nscal && q < 8; q++) a.slot[q] = slots[q];
-  a.moff = c.d_moff; a.g3rlm = c.d_g3rlm; a.ar1 = c.d_ar1; a.f = c.d_f; a.fs = c.fsize();
-  a.bunscale = t->bb_unscale; a.koff = t->bb_koff; a.klen = t->bb_klen; a.n1 = t->bb_n1;
-  a.rowmax = t->rowmax_spec;
-  a.out = out; a.status = c.d_status;
-  Slots8 sl{};
-  for (int q = 0; q < nvec + nscal && q < 8; q++) sl.s[q] = slots[q];
-  k_rowmax_spec<<<dim3(c.nr, nvec + nscal, 3), 256, 0, c.stream>>>(c.L, c.nr, c.jmax, nvec, sl, c.d_moff, c.d_g3rlm,
-                                                                  c.d_f, c.fsize(), t->rowmax_spec);
-  const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
+  a.L = c.L; a.nr = c.nr; a.nh = c.nh; a.nhp = t->nhp; a.nth = c.nth; a.nvec = nvec; a.nscal = nscal;
+  a.pitchP = pitchP; a.pitchD = pitchD;
+  a.kbase = t->kbase; a.ko = t->bb_ko; a.maxP = t->maxP; a.maxD = t->maxD;
+  a.bunscale = t->bb_unscale; a.out = out; a.status = c.d_status;
+  const int rows0 = ng * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
-  k_leg_bwd_mixed<<<dim3(tiles0 + tiles1, c.L + 1), NTHR, t->smem_bwd, c.stream>>>(a, rows0, rows1, tiles0,
-                                                                                  t->tm_bb_hi, t->tm_bb_lo);
+  k_leg_bwd_tma<<<dim3(tiles0 + tiles1, c.L + 1), NTHR, t->smem_bwd, c.stream>>>(a, rows0, rows1, tiles0, rawP, rawD,
+                                                                                t->tm_bb_hi, t->tm_bb_lo);
   return 0;
 }
 
