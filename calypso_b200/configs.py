@@ -65,3 +65,26 @@ CONFIGS = {
     "sht_roundtrip_L255_Nr65": sht_roundtrip,
     "full_step_L255_Nr129": full_step_L255,
 }
+
+
+ENSEMBLE_SHAPES = (
+    # (L, Nr, Ntheta, Nphi, dt): Ntheta = 3(L+1)/2 and Nphi = 2 Ntheta as in the
+    # reference's L31 grid; dt halves with each doubling of L
+    (31, 33, 48, 96, 1e-4),
+    (63, 65, 96, 192, 5e-5),
+    (127, 97, 192, 384, 2.5e-5),
+)
+
+
+def ensemble(n_per_shape: int = 16, seed: int = 0, E: float = 1e-3, ra_range=(80.0, 400.0)) -> list:
+    """Batched ensemble: n_per_shape shells of each of ENSEMBLE_SHAPES, the
+    physics of the small shell with the Rayleigh number of each shell drawn
+    uniformly in ra_range (seeded).  48 shells by default."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for (L, nr, nth, nph, dt) in ENSEMBLE_SHAPES:
+        for _ in range(n_per_shape):
+            ra = float(rng.uniform(*ra_range))
+            out.append(shell_params(L, nr, nth, nph, E=E, Ra=ra, dt=dt))
+    return out

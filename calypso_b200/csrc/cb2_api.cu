@@ -151,7 +151,7 @@ static void temp_roundtrip(Ctx &c) {
   k_temp_roundtrip<<<cdiv(c.nr, 128), 128, 0, c.stream>>>(c.nr, (size_t)c.jmax, c.d_reft0, c.fld(TEMP));
 }
 
-static int one_step(Ctx &c) {
+int step_once(Ctx &c) {
   c.istep += 1;
   if (c.timers) cudaEventRecord(c.ev[0], c.stream);
   rj_explicit(c, c.istep == 1);
@@ -353,7 +353,7 @@ int cb2_step(cb2_ctx *c, int nsteps) {
   if (!c->started) { set_error("cb2_step before cb2_start / cb2_init_fields"); return CB2_ERR_STATE; }
   if (c->timers) for (int i = 0; i < 32; i++) c->stage_ms[i] = 0.0;
   for (int s = 0; s < nsteps; s++) {
-    int rc = one_step(*c);
+    int rc = step_once(*c);
     if (rc) return rc;
     if (c->timers) accumulate_timers(*c);
   }
@@ -367,7 +367,7 @@ int cb2_step_graph(cb2_ctx *c, int nsteps) {
   // the first step is an Euler step and not captured
   int done = 0;
   if (c->istep == 0 && nsteps > 0) {
-    int rc = one_step(*c);
+    int rc = step_once(*c);
     if (rc) return rc;
     done = 1;
   }
@@ -378,7 +378,7 @@ int cb2_step_graph(cb2_ctx *c, int nsteps) {
     cudaGraph_t g;
     CB2_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int save = c->istep;
-    int rc = one_step(*c);
+    int rc = step_once(*c);
     c->istep = save;
     cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
     if (rc) {
@@ -498,7 +498,7 @@ int cb2_step_host_state(cb2_ctx *c, double *state, double out_energies[7]) {
     k_to_device_order<<<cdiv(n, 256), 256, 0, c->stream>>>(c->nr, c->jmax, c->d_perm,
                                                              c->d_host_state + q * n, c->fld(kHostStateSlots[q]));
   if (c->istep == 0) c->istep = 1;   // the loaded history makes this an Adams-Bashforth step
-  if (int rc = one_step(*c)) return rc;
+  if (int rc = step_once(*c)) return rc;
   for (int q = 0; q < 20; q++)
     k_to_host_order<<<cdiv(n, 256), 256, 0, c->stream>>>(c->nr, c->jmax, c->d_perm,
                                                          c->fld(kHostStateSlots[q]), c->d_host_state + q * n);

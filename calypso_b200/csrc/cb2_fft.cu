@@ -870,7 +870,10 @@ void fft_forward_grid(Ctx &c, int ncomp, const double *grid, T *four) {
 template <int N>
 static void launch_fft_t(Ctx &c, const MLayout &in, const MLayout &out, const ProdCoef &pc) {
   const size_t sm = smem_fft_t<N>();
-  k_fft_products_t<N><<<(unsigned)(c.nth * c.nr), 512, sm, c.stream>>>(c.L, in, out, (const float2 *)c.d_twp32, pc);
+  const int nt = c.tune[TUNE_FFT_THREADS];
+  const int threads = (nt == 128 || nt == 256) ? nt : 512;
+  k_fft_products_t<N><<<(unsigned)(c.nth * c.nr), threads, sm, c.stream>>>(c.L, in, out, (const float2 *)c.d_twp32,
+                                                                          pc);
 }
 
 void fft_products_m(Ctx &c, const MLayout &in, const MLayout &out) {

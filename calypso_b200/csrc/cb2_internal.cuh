@@ -105,6 +105,8 @@ struct Ctx {
   double stage_ms[32] = {0};
   cudaGraphExec_t graph_exec = nullptr;
   int graph_nsteps = 0;
+  // kernel variants chosen by the autotuner (cb2_autotune); defaults until tuned
+  int tune[8] = {4, 2, 2, 512, 0, 0, 0, 0};
 
   size_t fsize() const { return (size_t)nr * jmax; }
   double *fld(int slot) { return d_f + (size_t)slot * fsize(); }
@@ -185,6 +187,17 @@ int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots);
 void fft_products_m(Ctx &c, const MLayout &in, const MLayout &out);
 void fft_backward_grid_m(Ctx &c, const MLayout &in, double *grid);
 void fft_forward_grid_m(Ctx &c, const double *grid, const MLayout &out);
+
+// autotuned kernel variants (Ctx::tune)
+enum Tune {
+  TUNE_BWD_KT = 0,       // float64 backward Legendre: radial levels per block (2, 4)
+  TUNE_FWD_KT = 1,       // float64 forward Legendre: radial levels per block (1, 2, 4)
+  TUNE_PACK_KC = 2,      // mixed backward pack: radial levels per block (1, 2, 4)
+  TUNE_FFT_THREADS = 3,  // mixed FFT + products: threads per row block (128, 256, 512)
+  TUNE_N = 4
+};
+// one time step (explicit, implicit, nonlinear); advances istep (cb2_api.cu)
+int step_once(Ctx &c);
 
 // bits of the device status word d_status
 constexpr int CB2_STATUS_SINGULAR = 1;        // zero pivot in an LU factorisation

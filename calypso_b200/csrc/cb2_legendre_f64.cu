@@ -24,10 +24,10 @@
 
 namespace cb2 {
 
-constexpr int BWD_KT = 4;   // radial levels per backward block
 constexpr int BWD_LC = 32;  // degrees per staged chunk
-constexpr int FWD_KT = 2;   // radial levels per forward block
 constexpr int FWD_TC = 16;  // Gauss node pairs per staged chunk
+// radial levels per block (BWD_KT backward, FWD_KT forward) are template
+// parameters; the autotuner picks them per shell shape (cb2_autotune)
 constexpr int MAXG = 6;     // field groups (vectors + scalars) per launch
 
 struct LegArgs {
@@ -50,6 +50,7 @@ __device__ inline size_t four_at(const LegArgs &a, int th, int k, int c) {
   return (((size_t)th * a.nr + k) * a.ncomp + c) * a.NS;
 }
 
+template <int BWD_KT>
 __global__ void __launch_bounds__(32 * MAXG)
 k_leg_bwd_f64(LegArgs a, double *four) {
   const int m = blockIdx.z, k0 = blockIdx.y * BWD_KT, i0 = blockIdx.x * 32;
@@ -156,7 +157,7 @@ k_leg_bwd_f64(LegArgs a, double *four) {
 // forward: block = (order m, radial tile); lane = degree l - m.  NV vectors
 // and NSC scalars starting at component c0 of the Fourier buffer (which
 // holds a.ncomp components) and at group g0 of a.slot.
-template <int NV, int NSC>
+template <int NV, int NSC, int FWD_KT>
 __global__ void __launch_bounds__(256)
 k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
   const int m = blockIdx.z, k0 = blockIdx.y * FWD_KT;
@@ -286,20 +287,34 @@ void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four) {
     b.nscal = nb - b.nvec;
     b.cbase = comp;
     for (int q = 0; q < nb; q++) b.slot[q] = slots[g + q];
-    dim3 grid(cdiv(c.nh, 32), cdiv(c.nr, BWD_KT), c.L + 1);
-    k_leg_bwd_f64<<<grid, 32 * nb, 0, c.stream>>>(b, four);
+    if (c.tune[TUNE_BWD_KT] == 2) {
+      dim3 grid(cdiv(c.nh, 32), cdiv(c.nr, 2), c.L + 1);
+      k_leg_bwd_f64<2><<<grid, 32 * nb, 0, c.stream>>>(b, four);
+    } else {
+      dim3 grid(cdiv(c.nh, 32), cdiv(c.nr, 4), c.L + 1);
+      k_leg_bwd_f64<4><<<grid, 32 * nb, 0, c.stream>>>(b, four);
+    }
     comp += 3 * b.nvec + b.nscal;
     g += nb;
   }
 }
 
+template <int NV, int NSC, int KT>
+static void launch_fwd_kt(Ctx &c, const LegArgs &a, const double *four, int c0) {
+  int nthr = 32 * cdiv(std::min(c.L + 1, 256), 32);
+  size_t sm = (size_t)FWD_TC * KT * (3 * NV + NSC) * 2 * 2 * sizeof(double);
+  dim3 grid(1, cdiv(c.nr, KT), c.L + 1);
+  k_leg_fwd_f64<NV, NSC, KT><<<grid, nthr, sm, c.stream>>>(a, four, c0, 0);
+}
+
 template <int NV, int NSC>
 static void launch_fwd(Ctx &c, LegArgs a, const double *four, int c0, const int *slots) {
   for (int q = 0; q < NV + NSC; q++) a.slot[q] = slots[q];
-  int nthr = 32 * cdiv(std::min(c.L + 1, 256), 32);
-  size_t sm = (size_t)FWD_TC * FWD_KT * (3 * NV + NSC) * 2 * 2 * sizeof(double);
-  dim3 grid(1, cdiv(c.nr, FWD_KT), c.L + 1);
-  k_leg_fwd_f64<NV, NSC><<<grid, nthr, sm, c.stream>>>(a, four, c0, 0);
+  switch (c.tune[TUNE_FWD_KT]) {
+    case 1: launch_fwd_kt<NV, NSC, 1>(c, a, four, c0); break;
+    case 4: launch_fwd_kt<NV, NSC, 4>(c, a, four, c0); break;
+    default: launch_fwd_kt<NV, NSC, 2>(c, a, four, c0); break;
+  }
 }
 
 void leg_fwd_f64(Ctx &c, int nvec, int nscal, const double *four, const int *slots) {

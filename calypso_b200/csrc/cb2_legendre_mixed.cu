@@ -1016,7 +1016,7 @@ int mixed_setup(Ctx &c) {
     return rc;
   t->smem_bwd = 1024 + FST * ((size_t)BRAW_BYTES + 2 * (size_t)FA_BYTES + 2 * (size_t)t->nhp * FKB * 2) +
                 sizeof(BwdSmem);
-  t->smem_pack = (size_t)2 * 26 * ((L + 1) | 1) * sizeof(float);
+  t->smem_pack = (size_t)4 * 26 * ((L + 1) | 1) * sizeof(float);   // up to 4 radial levels per block
   t->smem_fwd = 1024 + FST * (size_t)RAW_BYTES + FST * (2 * (size_t)FA_BYTES + 2 * (size_t)t->nfb * FKB * 2) +
                 sizeof(FwdSmem);
   if (t->smem_bwd > 227 * 1024 || t->smem_fwd > 227 * 1024) {
@@ -1061,12 +1061,14 @@ int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   }
   // step 1: order-major float32 spectra and their row maxima
   PackArgs pk{};
-  pk.L = c.L; pk.nr = c.nr; pk.jmax = c.jmax; pk.nvec = nvec; pk.ng = ng; pk.kc = 2;
+  pk.L = c.L; pk.nr = c.nr; pk.jmax = c.jmax; pk.nvec = nvec; pk.ng = ng;
+  pk.kc = (c.tune[TUNE_PACK_KC] == 1 || c.tune[TUNE_PACK_KC] == 4) ? c.tune[TUNE_PACK_KC] : 2;
   for (int q = 0; q < ng; q++) pk.slot[q] = slots[q];
   pk.moff = c.d_moff; pk.g3rlm = c.d_g3rlm; pk.ar1 = c.d_ar1; pk.f = c.d_f; pk.fs = c.fsize();
   pk.rlmP = t->rlmP; pk.rlmD = t->rlmD; pk.pitchP = pitchP; pk.pitchD = pitchD;
   pk.kbase = t->kbase; pk.maxP = t->maxP; pk.maxD = t->maxD;
-  k_pack_bwd<<<dim3(c.L + 1, cdiv(c.nr, pk.kc)), 256, t->smem_pack, c.stream>>>(pk);
+  const size_t smp = (size_t)pk.kc * (2 * ng + 4 * nvec) * ((c.L + 1) | 1) * sizeof(float);
+  k_pack_bwd<<<dim3(c.L + 1, cdiv(c.nr, pk.kc)), 256, smp, c.stream>>>(pk);
   // step 2: the tensor-core transform
   CUtensorMap rawP{}, rawD{};
   if (make_map_any(&rawP, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, t->rlmP, pitchP, t->Ktot, TM, FKB,

@@ -1,0 +1,56 @@
+"""Throughput of the batched ensemble (48 shells: 16 x L31/Nr33, 16 x
+L63/Nr65, 16 x L127/Nr97, seeded Rayleigh numbers in [80, 400]).
+
+    python -m calypso_b200.ensemble_bench [--steps K] [--precision mixed|fp64]
+
+prints one JSON line: shell-steps/s of the ensemble (one CUDA graph launch
+per step holding every shell as a parallel branch) and of the same shells
+stepped one after another with their own graphs, both timed with CUDA
+events, and the autotuned kernel variants of each shape."""
+from __future__ import annotations
+
+import argparse
+import json
+
+from . import configs
+from .sph_mhd import PREC_FP64, PREC_MIXED, Ensemble, SphMHD
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--per-shape", type=int, default=16)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    args = ap.parse_args(argv)
+    prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
+    params = configs.ensemble(args.per_shape)
+    ens = Ensemble(params, prec, device=0, autotune=True)
+    ens.init_fields(2, 1)
+    ens.step(1 + args.warmup)
+    ms = ens.time_steps(args.steps)
+    tuning = {f"L{p['ltr']}": s.tuning for p, s in zip(params, ens.shells)}
+    ens.close()
+    # the same shells one after another (each its own captured graph)
+    seq_ms = 0.0
+    for q, p in enumerate(params):
+        g = SphMHD(p, prec, device=0)
+        g.tuning = tuning[f"L{p['ltr']}"]
+        g.init_fields(2, 1 + q)
+        g.step(1)
+        g.step(args.warmup, graph=True)
+        seq_ms += g.time_steps(args.steps, graph=True)
+        g.close()
+    n = len(params)
+    print(json.dumps({
+        "workload": f"ensemble_{n}_shells", "precision": args.precision, "steps": args.steps,
+        "shell_steps_per_s": n * args.steps / (ms / 1000.0),
+        "ms_per_ensemble_step": ms / args.steps,
+        "sequential_shell_steps_per_s": n * args.steps / (seq_ms / 1000.0),
+        "speedup_over_sequential": seq_ms / ms,
+        "tuning": tuning,
+    }), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -74,6 +74,10 @@ EXPORTS = [
     "cb2_get_field", "cb2_set_field", "cb2_get_field_device", "cb2_set_field_device",
     "cb2_step_host_state", "cb2_sht_backward", "cb2_sht_forward", "cb2_get_gauss",
     "cb2_get_plm", "cb2_stage_times", "cb2_time_steps", "cb2_alloc_pinned", "cb2_free_pinned",
+    "cb2_energies_static", "cb2_autotune", "cb2_get_tuning", "cb2_set_tuning",
+    "cb2_ensemble_create", "cb2_ensemble_destroy", "cb2_ensemble_size", "cb2_ensemble_shell",
+    "cb2_ensemble_init_fields", "cb2_ensemble_step", "cb2_ensemble_sync", "cb2_ensemble_time_steps",
+    "cb2_ensemble_energies",
 ]
 
 
@@ -113,6 +117,19 @@ def load_library(path: str = LIB_PATH):
         "cb2_time_steps": ([vp, i, i, pd], i),
         "cb2_alloc_pinned": ([ctypes.c_size_t, P(vp)], i),
         "cb2_free_pinned": ([vp], i),
+        "cb2_energies_static": ([vp, pd], i),
+        "cb2_autotune": ([vp], i),
+        "cb2_get_tuning": ([vp, P(i)], i),
+        "cb2_set_tuning": ([vp, P(i)], i),
+        "cb2_ensemble_create": ([P(Params), i, i, i, i, P(vp)], i),
+        "cb2_ensemble_destroy": ([vp], i),
+        "cb2_ensemble_size": ([vp], i),
+        "cb2_ensemble_shell": ([vp, i], vp),
+        "cb2_ensemble_init_fields": ([vp, i, ctypes.c_uint], i),
+        "cb2_ensemble_step": ([vp, i], i),
+        "cb2_ensemble_sync": ([vp], i),
+        "cb2_ensemble_time_steps": ([vp, i, pd], i),
+        "cb2_ensemble_energies": ([vp, pd], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -150,11 +167,23 @@ class SphMHD:
         self.L, self.nr, self.nth, self.nph = p.ltr, p.nr, p.nth, p.nph
         self.jmax = (self.L + 1) ** 2
 
+    @classmethod
+    def _wrap(cls, handle, params: dict, precision: int):
+        """A non-owning view of a context that belongs to an Ensemble."""
+        self = cls.__new__(cls)
+        self._h = ctypes.c_void_p(handle)
+        self._owned = False
+        self.params = dict(params)
+        self.precision = precision
+        self.L, self.nr, self.nth, self.nph = params["ltr"], params["nr"], params["nth"], params["nph"]
+        self.jmax = (self.L + 1) ** 2
+        return self
+
     # --- lifetime -----------------------------------------------------
     def close(self):
-        if getattr(self, "_h", None) and self._h.value:
+        if getattr(self, "_h", None) and self._h.value and getattr(self, "_owned", True):
             load_library().cb2_destroy(self._h)
-            self._h = ctypes.c_void_p()
+        self._h = ctypes.c_void_p()
 
     def __del__(self):
         try:
@@ -190,6 +219,22 @@ class SphMHD:
 
     def sync(self):
         _check(load_library().cb2_sync(self._h), "cb2_sync")
+
+    # --- kernel-variant autotuning (before init_fields) -----------------
+    def autotune(self) -> list:
+        _check(load_library().cb2_autotune(self._h), "cb2_autotune")
+        return self.tuning
+
+    @property
+    def tuning(self) -> list:
+        out = (ctypes.c_int * 4)()
+        _check(load_library().cb2_get_tuning(self._h, out), "cb2_get_tuning")
+        return list(out)
+
+    @tuning.setter
+    def tuning(self, values):
+        arr = (ctypes.c_int * 4)(*values)
+        _check(load_library().cb2_set_tuning(self._h, arr), "cb2_set_tuning")
 
     @property
     def istep(self) -> int:
@@ -248,6 +293,59 @@ class SphMHD:
         p, dp = np.zeros(self.nth), np.zeros(self.nth)
         _check(load_library().cb2_get_plm(self._h, l, m, _ptr(p), _ptr(dp)), "cb2_get_plm")
         return p, dp
+
+
+class Ensemble:
+    """Independent shells advanced together, one CUDA graph launch per step
+    (cb2_ensemble_*).  `shells[i]` is a view of shell i (do not close it)."""
+
+    def __init__(self, params_list, precision: int = PREC_MIXED, device: int = -1, autotune: bool = True):
+        lib = load_library()
+        n = len(params_list)
+        arr = (Params * n)()
+        for q, prm in enumerate(params_list):
+            for k, v in prm.items():
+                setattr(arr[q], k, v)
+        h = ctypes.c_void_p()
+        _check(lib.cb2_ensemble_create(arr, n, precision, device, 1 if autotune else 0, ctypes.byref(h)),
+               "cb2_ensemble_create")
+        self._h = h
+        self.params = [dict(p) for p in params_list]
+        self.shells = [SphMHD._wrap(lib.cb2_ensemble_shell(h, q), self.params[q], precision) for q in range(n)]
+
+    def __len__(self):
+        return len(self.shells)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            load_library().cb2_ensemble_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            self.shells = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init_fields(self, kind: int = 2, seed0: int = 0):
+        _check(load_library().cb2_ensemble_init_fields(self._h, kind, seed0), "cb2_ensemble_init_fields")
+
+    def step(self, nsteps: int = 1):
+        _check(load_library().cb2_ensemble_step(self._h, nsteps), "cb2_ensemble_step")
+
+    def sync(self):
+        _check(load_library().cb2_ensemble_sync(self._h), "cb2_ensemble_sync")
+
+    def time_steps(self, nsteps: int) -> float:
+        ms = ctypes.c_double()
+        _check(load_library().cb2_ensemble_time_steps(self._h, nsteps, ctypes.byref(ms)), "cb2_ensemble_time_steps")
+        return ms.value
+
+    def energies(self) -> np.ndarray:
+        out = np.zeros((len(self.shells), 7))
+        _check(load_library().cb2_ensemble_energies(self._h, _ptr(out)), "cb2_ensemble_energies")
+        return out
 
 
 class PinnedArray:

@@ -159,6 +159,39 @@ int cb2_get_plm(cb2_ctx *ctx, int l, int m, double *p, double *dp);
 int cb2_alloc_pinned(size_t bytes, void **out);
 int cb2_free_pinned(void *p);
 
+/* Kernel-variant autotuner (the counterpart of the reference's
+ * select_legendre_transform, MHD_src/sph_MHD/sph_transforms_4_MHD.f90:309-426,
+ * which times its Legendre loop variants at start-up): times every
+ * candidate tile / launch shape of the transform kernels on this context
+ * and keeps the fastest.  Only before cb2_init_fields / cb2_start (it
+ * overwrites the work fields).  tuning[4]: float64 backward radial tile,
+ * float64 forward radial tile, mixed pack radial tile, mixed FFT threads. */
+int cb2_autotune(cb2_ctx *ctx);
+int cb2_get_tuning(const cb2_ctx *ctx, int tuning[4]);
+int cb2_set_tuning(cb2_ctx *ctx, const int tuning[4]);
+
+/* Ensemble of independent shells (any mix of truncations and parameters),
+ * advanced together: one CUDA graph holds a time step of every shell as
+ * parallel branches, so one graph launch advances all of them.  No
+ * counterpart in the reference (it runs one shell per job).  Shells of one
+ * shape (ltr, nr, nth, nph) share one autotuning when autotune_shapes != 0.
+ * Shell i is an ordinary context (cb2_ensemble_shell); call
+ * cb2_ensemble_sync before using it directly after cb2_ensemble_step. */
+typedef struct cb2_ensemble cb2_ensemble;
+int cb2_ensemble_create(const cb2_params *params, int n, int precision, int device, int autotune_shapes,
+                        cb2_ensemble **out);
+int cb2_ensemble_destroy(cb2_ensemble *e);
+int cb2_ensemble_size(const cb2_ensemble *e);
+cb2_ctx *cb2_ensemble_shell(cb2_ensemble *e, int i);
+/* shell i gets cb2_init_fields(kind, seed0 + i) */
+int cb2_ensemble_init_fields(cb2_ensemble *e, int kind, unsigned seed0);
+int cb2_ensemble_step(cb2_ensemble *e, int nsteps);
+int cb2_ensemble_sync(cb2_ensemble *e);
+/* nsteps of cb2_ensemble_step bracketed by CUDA events; ms = device time */
+int cb2_ensemble_time_steps(cb2_ensemble *e, int nsteps, double *ms);
+/* out = n x 7 energies (cb2_energies of each shell) */
+int cb2_ensemble_energies(cb2_ensemble *e, double *out);
+
 /* CUDA-event time of the last cb2_step/cb2_step_graph call, per stage
  * (stage ids follow the reference's elapsed-time labels of
  * MHD_src/IO/init_sph_MHD_elapsed_label.f90: 6 explicit, 7 implicit,

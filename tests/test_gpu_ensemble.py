@@ -1,0 +1,75 @@
+"""Batched ensemble and kernel-variant autotuner on the GPU.
+
+  - every shell of an ensemble (mixed truncations, one CUDA graph launch per
+    step) ends bit-for-bit where the same shell stepped alone ends;
+  - the autotuner picks from its candidate sets, refuses to run once the
+    fields exist, and no kernel variant changes a result (bitwise)."""
+import numpy as np
+import pytest
+
+from calypso_b200 import PREC_FP64, PREC_MIXED, CalypsoError, Ensemble, SphMHD, configs
+from calypso_b200.sph_mhd import MAGNE, TEMP, VELO
+
+pytestmark = pytest.mark.gpu
+
+CANDIDATES = [(2, 4), (1, 2), (1, 2, 4), (128, 256, 512)]
+
+
+def small_ensemble():
+    out = []
+    for q, (L, nr, nth, nph, dt) in enumerate([(31, 17, 48, 96, 1e-4), (63, 17, 96, 192, 5e-5)]):
+        for ra in (120.0, 300.0):
+            out.append(configs.shell_params(L, nr, nth, nph, E=1e-3, Ra=ra, dt=dt))
+    return out
+
+
+@pytest.mark.parametrize("prec", [PREC_MIXED, PREC_FP64])
+def test_ensemble_matches_shells_stepped_alone(prec):
+    params = small_ensemble()
+    ens = Ensemble(params, prec, device=0, autotune=True)
+    ens.init_fields(2, 11)
+    ens.step(12)
+    e_ens = ens.energies()
+    fields = [[s.get_field(slot) for slot in (VELO, MAGNE + 2, TEMP)] for s in ens.shells]
+    tunings = [s.tuning for s in ens.shells]
+    ens.close()
+    for q, p in enumerate(params):
+        g = SphMHD(p, prec, device=0)
+        g.tuning = tunings[q]
+        g.init_fields(2, 11 + q)
+        g.step(12, graph=True)
+        assert np.array_equal(g.energies(), e_ens[q]), q
+        for a, slot in zip(fields[q], (VELO, MAGNE + 2, TEMP)):
+            assert np.array_equal(a, g.get_field(slot)), (q, slot)
+        g.close()
+
+
+@pytest.mark.parametrize("prec", [PREC_MIXED, PREC_FP64])
+def test_autotune_candidates_and_state(prec):
+    p = configs.small_shell()
+    g = SphMHD(p, prec, device=0)
+    t = g.autotune()
+    for q, cand in enumerate(CANDIDATES):
+        assert t[q] in cand or q in ((2, 3) if prec == PREC_FP64 else (0, 1)), (q, t)
+    g.init_fields(2, 3)
+    with pytest.raises(CalypsoError):
+        g.autotune()
+    g.close()
+
+
+@pytest.mark.parametrize("prec", [PREC_MIXED, PREC_FP64])
+def test_kernel_variants_give_identical_results(prec):
+    p = configs.small_shell()
+    ref = None
+    variants = [[2, 1, 1, 128], [4, 2, 2, 256], [2, 2, 4, 512]]
+    for v in variants:
+        g = SphMHD(p, prec, device=0)
+        g.tuning = v
+        g.init_fields(2, 5)
+        g.step(6)
+        f = np.stack([g.get_field(s) for s in (VELO, MAGNE, TEMP)])
+        g.close()
+        if ref is None:
+            ref = f
+        else:
+            assert np.array_equal(f, ref), v
