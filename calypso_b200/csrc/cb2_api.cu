@@ -142,6 +142,10 @@ static int nonlinear(Ctx &c) {
   }
   if (c.timers) cudaEventRecord(c.ev[14], c.stream);
   rj_after_transform(c);
+  if (c.closure) {
+    int rc = closure_apply(c);
+    if (rc) return rc;
+  }
   if (c.timers) cudaEventRecord(c.ev[15], c.stream);
   return 0;
 }
@@ -274,6 +278,7 @@ int cb2_destroy(cb2_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->prec == CB2_PREC_MIXED) mixed_free(*c);
+  closure_free(*c);
   free_tables(*c);
   void *ptrs[] = {c->d_lu_vp, c->d_lu_vt, c->d_lu_bs, c->d_lu_bt, c->d_lu_t, c->d_pv_vp, c->d_pv_vt,
                   c->d_pv_bs, c->d_pv_bt, c->d_pv_t, c->d_status, c->d_tw_fft, c->d_tw_fft32, c->d_twp32,

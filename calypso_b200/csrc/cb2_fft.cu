@@ -778,8 +778,7 @@ static size_t smem_fft_t() { return (14 * (size_t)Plan3x2<N>::NP + N) * sizeof(f
 template <int N>
 static int attr_fft_t(Ctx &c) {
   using P = Plan3x2<N>;
-  CB2_CUDA(cudaFuncSetAttribute(k_fft_products_t<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_fft_t<N>()));
+  CB2_CUDA(raise_smem_limit(k_fft_products_t<N>, (int)smem_fft_t<N>()));
   std::vector<float2> t(P::ntw());
   const double pi = 3.14159265358979323846;
   for (int st = 0; st < P::nst(); st++) {
@@ -811,10 +810,9 @@ int fft_setup(Ctx &c) {
     set_error("ngrid_zonal_ctl too large for the fused FFT kernel");
     return CB2_ERR_ARG;
   }
-  CB2_CUDA(cudaFuncSetAttribute(k_fft_products<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
-  CB2_CUDA(cudaFuncSetAttribute(k_fft_products<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big));
-  CB2_CUDA(cudaFuncSetAttribute(k_fft_products_m, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(14 * (size_t)c.nph * sizeof(float2))));
+  CB2_CUDA(raise_smem_limit(k_fft_products<double>, (int)big));
+  CB2_CUDA(raise_smem_limit(k_fft_products<float>, (int)big));
+  CB2_CUDA(raise_smem_limit(k_fft_products_m, (int)(14 * (size_t)c.nph * sizeof(float2))));
   {
     int rc = 0;
     switch (c.nph) {

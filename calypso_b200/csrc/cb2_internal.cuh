@@ -98,6 +98,8 @@ struct Ctx {
   double *d_host_state = nullptr;        // 20 slots for cb2_step_host_state
   // mixed-precision Legendre operands (split fp16) -- owned by cb2_legendre_mixed.cu
   void *mixed = nullptr;
+  // learned subgrid closure attached to the step (cb2_closure.cu), or null
+  void *closure = nullptr;
   int istep = 0;
   bool started = false;
   bool timers = false;
@@ -121,6 +123,19 @@ int cuda_fail(cudaError_t e, const char *what);
     cudaError_t _e = (call);                             \
     if (_e != cudaSuccess) return cuda_fail(_e, #call);  \
   } while (0)
+
+// Raise (never lower) a kernel's dynamic shared-memory limit.  The limit is
+// a property of the kernel in the whole process, shared by every context:
+// lowering it for a small shell would make the launches of a larger shell
+// created earlier fail.
+template <typename K>
+inline cudaError_t raise_smem_limit(K *kernel, size_t bytes) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
 
 // set-up (cb2_tables.cu)
 int setup_tables(Ctx &c);
@@ -198,6 +213,9 @@ enum Tune {
 };
 // one time step (explicit, implicit, nonlinear); advances istep (cb2_api.cu)
 int step_once(Ctx &c);
+// learned closure (cb2_closure.cu): adds its tendency to the nonlinear terms
+int closure_apply(Ctx &c);
+void closure_free(Ctx &c);
 
 // bits of the device status word d_status
 constexpr int CB2_STATUS_SINGULAR = 1;        // zero pivot in an LU factorisation

@@ -1023,9 +1023,9 @@ int mixed_setup(Ctx &c) {
     set_error("mixed precision tiles exceed shared memory");
     return CB2_ERR_ARG;
   }
-  CB2_CUDA(cudaFuncSetAttribute(k_leg_bwd_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_bwd));
-  CB2_CUDA(cudaFuncSetAttribute(k_pack_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_pack));
-  CB2_CUDA(cudaFuncSetAttribute(k_leg_fwd_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t->smem_fwd));
+  CB2_CUDA(raise_smem_limit(k_leg_bwd_tma, (int)t->smem_bwd));
+  CB2_CUDA(raise_smem_limit(k_pack_bwd, (int)t->smem_pack));
+  CB2_CUDA(raise_smem_limit(k_leg_fwd_tma, (int)t->smem_fwd));
   return 0;
 }
 

@@ -192,6 +192,48 @@ int cb2_ensemble_time_steps(cb2_ensemble *e, int nsteps, double *ms);
 /* out = n x 7 energies (cb2_energies of each shell) */
 int cb2_ensemble_energies(cb2_ensemble *e, double *out);
 
+/* Learned spectral subgrid closure.  No counterpart in the reference (its
+ * SGS hooks, MHD_src/sph_MHD/cal_explicit_terms.f90:70-95, are unused on
+ * the spherical-shell path).  A low-resolution shell misses the part of its
+ * nonlinear terms carried by modes it does not resolve; a small MLP
+ * predicts it per radial level and (l, m) from 16 local spectral features
+ * (the 13 coefficients of velocity, vorticity, magnetic field, current and
+ * temperature, l/L, m/L, r) for the 5 explicit nonlinear terms (curl of
+ * the forces S, T; induction S, T; heat advection).  Weights bfloat16,
+ * float32 accumulation; trained on the GPU by these kernels. */
+typedef struct cb2_mlp cb2_mlp;
+/* MLP nin -> nhid -> nhid -> nout, SiLU, seeded initial weights */
+int cb2_mlp_create(int nin, int nhid, int nout, unsigned seed, cb2_mlp **out);
+int cb2_mlp_destroy(cb2_mlp *net);
+int cb2_mlp_num_params(const cb2_mlp *net);
+/* float32 master parameters W1[nhid][nin], b1, W2[nhid][nhid], b2, W3[nout][nhid], b3 */
+int cb2_mlp_get_params(cb2_mlp *net, float *host);
+int cb2_mlp_set_params(cb2_mlp *net, const float *host);
+/* device buffers: x = rows x nin, y = rows x nout (float32) */
+int cb2_mlp_forward(cb2_mlp *net, const float *dev_x, long long rows, float *dev_y);
+/* mean squared error against dev_t and its gradient (kept for
+ * cb2_mlp_adam_step; also copied to host_grad when it is not NULL) */
+int cb2_mlp_loss_grad(cb2_mlp *net, const float *dev_x, const float *dev_t, long long rows, double *loss,
+                      float *host_grad);
+int cb2_mlp_adam_step(cb2_mlp *net, float lr, float beta1, float beta2, float eps);
+int cb2_mlp_sync(cb2_mlp *net);
+/* dst state := src state truncated to dst's L and restricted to dst's
+ * radial points (a subset of src's Chebyshev points), then cb2_start(dst) */
+int cb2_filter_fields(cb2_ctx *src, cb2_ctx *dst);
+/* src's 5 nonlinear terms filtered onto dst's shape: dev_out = 5 x nr x jmax float64 */
+int cb2_filter_terms(cb2_ctx *src, cb2_ctx *dst, double *dev_out);
+/* features (nr*jmax x 16) and targets (nr*jmax x 5: dev_hi minus ctx's own
+ * terms) of ctx's current state, float32 device buffers */
+int cb2_closure_features(cb2_ctx *ctx, float *dev_x);
+int cb2_closure_targets(cb2_ctx *ctx, const double *dev_hi, float *dev_y);
+/* attach (net != NULL) or detach the closure: each step then adds
+ * net((features - mean[k]) / std[k]) * scale[k] to the 5 nonlinear terms at
+ * the interior radial levels k (the walls are left to the boundary
+ * conditions).  norm = nr x 16 means, nr x 16 standard deviations, nr x 5
+ * output scales.  Attach before the step graph is captured; one context
+ * per network at a time. */
+int cb2_closure_attach(cb2_ctx *ctx, cb2_mlp *net, const float *norm);
+
 /* CUDA-event time of the last cb2_step/cb2_step_graph call, per stage
  * (stage ids follow the reference's elapsed-time labels of
  * MHD_src/IO/init_sph_MHD_elapsed_label.f90: 6 explicit, 7 implicit,

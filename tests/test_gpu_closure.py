@@ -1,0 +1,126 @@
+"""Learned subgrid closure on the GPU.
+
+  - the library's MLP forward pass and gradients against the float64 CPU
+    oracle (same bfloat16 weights): relative error 1e-4;
+  - training on solver-generated data lowers the loss, and the network
+    explains part of the held-out subgrid tendency that the plain
+    low-resolution solver misses entirely (explained fraction > 0.05);
+  - with the closure attached the low-resolution step still runs (eager and
+    graph) and detaching restores the plain solver bit for bit."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from calypso_b200 import PREC_MIXED, SphMHD, closure, configs  # noqa: E402
+from oracle import mlp_oracle  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_mlp_gradients_match_oracle():
+    nin, nhid, nout, n = 16, 256, 5, 333
+    net = closure.MLP(nin, nhid, nout, seed=3)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((n, nin)).astype(np.float32)
+    t = rng.standard_normal((n, nout)).astype(np.float32)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    p = net.params()
+    y_gpu = net.forward(xd).cpu().numpy()
+    y_ref, _ = mlp_oracle.forward(p, x, nin, nhid, nout)
+    assert rel(y_gpu, y_ref) < 1e-4
+    loss, g = net.loss_grad(xd, td, want_grad=True)
+    loss_ref, g_ref = mlp_oracle.loss_grad(p, x, t, nin, nhid, nout)
+    assert abs(loss - loss_ref) < 1e-4 * loss_ref
+    sizes = [nhid * nin, nhid, nhid * nhid, nhid, nout * nhid, nout]
+    o = 0
+    for s in sizes:
+        assert rel(g[o:o + s], g_ref[o:o + s]) < 1e-4, (o, s)
+        o += s
+    net.close()
+
+
+def small_pair():
+    hi = configs.shell_params(63, 33, 96, 192, E=1e-4, Ra=300.0, dt=5e-6)
+    lo = configs.shell_params(31, 17, 48, 96, E=1e-4, Ra=300.0, dt=5e-6)
+    return hi, lo
+
+
+def test_closure_trains_and_explains_held_out_tendency():
+    p_hi, p_lo = small_pair()
+    hi = SphMHD(p_hi, PREC_MIXED, device=0)
+    lo = SphMHD(p_lo, PREC_MIXED, device=0)
+    hi.init_fields(2, 2)
+    hi.step(100, graph=True)
+    xs, ys = closure.generate(hi, lo, 24, 4)
+    norm = closure.Normaliser(xs[:20], ys[:20], p_lo["nr"])
+    net = closure.MLP(seed=2)
+    hist = closure.train(net, xs[:20], ys[:20], norm, epochs=6, batch=4096, lr=2e-3)
+    assert hist[-1] < hist[0]
+    r2 = closure.explained(net, norm, xs[20:], ys[20:])
+    assert r2 > 0.05, r2
+    net.close()
+
+
+def test_closure_attach_detach():
+    p_hi, p_lo = small_pair()
+    hi = SphMHD(p_hi, PREC_MIXED, device=0)
+    hi.init_fields(2, 4)
+    hi.step(20, graph=True)
+    a = SphMHD(p_lo, PREC_MIXED, device=0)
+    b = SphMHD(p_lo, PREC_MIXED, device=0)
+    xs, ys = closure.generate(hi, a, 4, 2)
+    norm = closure.Normaliser(xs, ys, p_lo["nr"])
+    net = closure.MLP(seed=5)
+    closure.attach(b, net, norm)
+    closure.attach(b, None)          # detached: plain solver again
+    closure.filter_fields(hi, a)
+    closure.filter_fields(hi, b)
+    a.step(5)
+    b.step(5)
+    assert np.array_equal(a.get_field(0), b.get_field(0))
+    c = SphMHD(p_lo, PREC_MIXED, device=0)
+    closure.attach(c, net, norm)
+    closure.filter_fields(hi, c)
+    c.step(3)
+    c.step(4, graph=True)
+    e = c.energies()
+    assert np.all(np.isfinite(e))
+    assert not np.array_equal(c.get_field(0), a.get_field(0))
+    net.close()
+
+
+def test_closure_beats_plain_low_resolution_rollout():
+    # the plain low-resolution solver is the judge: from a filtered
+    # high-resolution state, 40 steps with the closure (relaxation 0.5) end
+    # with kinetic and magnetic energy spectra closer to the filtered
+    # high-resolution run than 40 plain steps do (deterministic: seeded data,
+    # seeded network, bitwise-reproducible kernels)
+    p_hi, p_lo = small_pair()
+    hi = SphMHD(p_hi, PREC_MIXED, device=0)
+    lo = SphMHD(p_lo, PREC_MIXED, device=0)
+    hi.init_fields(2, 1)
+    hi.step(200, graph=True)
+    xs, ys = closure.generate(hi, lo, 48, 4)
+    norm = closure.Normaliser(xs[:40], ys[:40], p_lo["nr"])
+    net = closure.MLP(seed=1)
+    closure.train(net, xs[:40], ys[:40], norm, epochs=6, batch=16384, lr=1e-3, seed=1)
+    plain = SphMHD(p_lo, PREC_MIXED, device=0)
+    closed = SphMHD(p_lo, PREC_MIXED, device=0)
+    closure.attach(closed, net, norm, alpha=0.5)
+    closure.filter_fields(hi, plain)
+    closure.filter_fields(hi, closed)
+    plain.step(40)
+    closed.step(40)
+    hi.step(40, graph=True)
+    ref = SphMHD(p_lo, PREC_MIXED, device=0)
+    closure.filter_fields(hi, ref)
+    s_ref = closure.energy_spectra(ref)
+    e_plain = closure.spectra_error(closure.energy_spectra(plain), s_ref)
+    e_closed = closure.spectra_error(closure.energy_spectra(closed), s_ref)
+    assert e_closed < e_plain, (e_closed, e_plain)
+    net.close()

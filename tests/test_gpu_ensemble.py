@@ -73,3 +73,20 @@ def test_kernel_variants_give_identical_results(prec):
             ref = f
         else:
             assert np.array_equal(f, ref), v
+
+
+def test_small_shell_created_after_large_one_leaves_it_working():
+    # kernel shared-memory limits are process-wide: a small shell must not
+    # lower them below what a larger shell created earlier launches with
+    big = configs.shell_params(63, 33, 96, 192, E=1e-4, Ra=300.0, dt=5e-6)
+    small = configs.shell_params(31, 17, 48, 96, E=1e-4, Ra=300.0, dt=5e-6)
+    for prec in (PREC_MIXED, PREC_FP64):
+        a = SphMHD(big, prec, device=0)
+        b = SphMHD(small, prec, device=0)
+        a.init_fields(2, 1)
+        b.init_fields(2, 1)
+        a.step(3)
+        b.step(3)
+        assert np.all(np.isfinite(a.energies())) and np.all(np.isfinite(b.energies()))
+        a.close()
+        b.close()
