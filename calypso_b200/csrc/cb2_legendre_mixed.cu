@@ -104,10 +104,25 @@ __device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity) {
   }
 }
 
-__device__ inline void tma_load_2d(void *dst, const CUtensorMap *tm, uint64_t *bar, int c0, int c1) {
+// L2 policies: the B tables are re-read by every CTA of an order (keep
+// them), the raw operand rows are read once (let them go first)
+__device__ inline uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ inline uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ inline void tma_load_2d_hint(void *dst, const CUtensorMap *tm, uint64_t *bar, int c0, int c1,
+                                        uint64_t policy) {
   asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(tm)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%3, %4}], [%2], %5;"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(tm)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "l"(policy)
       : "memory");
 }
 
@@ -202,14 +217,6 @@ struct FwdArgs {
   int *status;
 };
 
-struct FwdSmem {
-  uint64_t rawfull[FST], bfull[FST], mmadone[FST], done;
-  uint32_t tmem_base;
-  int mma_any;
-  float rowscale[TM];
-  float w[1024];         // Gauss weights (nth <= 1024)
-};
-
 // shared-memory descriptor, K-major, 64-byte swizzle (8-row groups 512 bytes apart)
 __device__ inline uint64_t smem_desc_sw64(const void *p) {
   uint64_t d = (uint64_t)((smem_u32(p) & 0x3FFFF) >> 4);
@@ -224,38 +231,57 @@ __device__ inline uint32_t sw64_chunk(int row, int c) {
   return (uint32_t)row * 64u + ((uint32_t)(c ^ ((row >> 1) & 3)) << 4);
 }
 
+// Both parities in one CTA: the raw tiles of a block feed the symmetric and
+// the antisymmetric fold at once (one read of the raw rows instead of two).
+// Stages: two raw (south + north, 32 KB each), two A/B holding the A tiles
+// of both parities (4 x 8 KB) and their B tiles.  Accumulator of parity p at
+// TMEM column p * tmem_cols / 2.
+constexpr int FRS = 2;   // raw stages
+constexpr int FAB = 2;   // A/B stages
+
+struct FwdSmem2 {
+  uint64_t rawfull[FRS], bfull[FAB], mmadone[FAB], done;
+  uint32_t tmem_base;
+  int mma_any;
+  float rowscale[TM];
+  float w[1024];
+};
+
 __global__ void __launch_bounds__(NTHR, 1)
-k_leg_fwd_tma(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int tiles_g0,
-              const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
-              const __grid_constant__ CUtensorMap tmp_hi, const __grid_constant__ CUtensorMap tmp_lo,
-              const __grid_constant__ CUtensorMap tmd_hi, const __grid_constant__ CUtensorMap tmd_lo,
-              uint32_t tmem_cols) {
+k_leg_fwd_tma2(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int tiles_g0,
+               const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
+               const __grid_constant__ CUtensorMap tmp_hi, const __grid_constant__ CUtensorMap tmp_lo,
+               const __grid_constant__ CUtensorMap tmd_hi, const __grid_constant__ CUtensorMap tmd_lo,
+               uint32_t tmem_cols) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char *base = smem_base_1024(smem_raw);
-  const uint32_t B_BYTES = (uint32_t)a.nfb * FKB * 2;       // one of hi / lo
-  const uint32_t AB_BYTES = 2 * FA_BYTES + 2 * B_BYTES;
-  unsigned char *raw0 = base;                                // FST x RAW_BYTES
-  unsigned char *ab0 = base + FST * RAW_BYTES;               // FST x AB_BYTES
-  FwdSmem *sh = reinterpret_cast<FwdSmem *>(ab0 + FST * AB_BYTES);
+  const uint32_t B_BYTES = (uint32_t)a.nfb * FKB * 2;       // one of hi / lo, one parity
+  const uint32_t AB_BYTES = 4 * FA_BYTES + 4 * B_BYTES;     // A hi/lo x 2 parities, B hi/lo x 2 parities
+  unsigned char *raw0 = base;
+  unsigned char *ab0 = base + FRS * RAW_BYTES;
+  FwdSmem2 *sh = reinterpret_cast<FwdSmem2 *>(ab0 + FAB * AB_BYTES);
   const int tid = threadIdx.x, warp = tid >> 5;
   const int r = tid & (TM - 1), h = tid >> 7;
-  const int m = blockIdx.y, p = blockIdx.z;
+  const int m = blockIdx.y;
   const int g = (blockIdx.x < (unsigned)tiles_g0) ? 0 : 1;
   const int nrows = g ? rows_g1 : rows_g0;
   const int row0 = (g ? blockIdx.x - tiles_g0 : blockIdx.x) * TM;
-  const int np = a.nlp[m * 2 + p];
-  const int npad = ((np + 15) / 16) * 16;
-  const int nbox = (npad + a.boxr - 1) / a.boxr;
-  const int NT = (a.nh + FKB - 1) / FKB;                    // theta blocks
-  const int NB = g ? 2 * NT : NT;                           // K blocks
+  int np[2], npad[2], nbox[2], brow[2];
+  for (int p = 0; p < 2; p++) {
+    np[p] = a.nlp[m * 2 + p];
+    npad[p] = ((np[p] + 15) / 16) * 16;
+    nbox[p] = (npad[p] + a.boxr - 1) / a.boxr;
+    brow[p] = a.roff[m * 2 + p];
+  }
+  const int NT = (a.nh + FKB - 1) / FKB;
+  const int NB = g ? 2 * NT : NT;
   const CUtensorMap *traw = g ? &tm_rawD : &tm_rawP;
   const CUtensorMap *tbh = g ? &tmd_hi : &tmp_hi, *tbl = g ? &tmd_lo : &tmp_lo;
-  const int brow = a.roff[m * 2 + p];
+  const uint32_t acc1 = tmem_cols / 2;
 
   if (tid == 0) {
-    for (int q = 0; q < FST; q++) {
-      mbar_init(&sh->rawfull[q], 1); mbar_init(&sh->bfull[q], 1); mbar_init(&sh->mmadone[q], 1);
-    }
+    for (int q = 0; q < FRS; q++) mbar_init(&sh->rawfull[q], 1);
+    for (int q = 0; q < FAB; q++) { mbar_init(&sh->bfull[q], 1); mbar_init(&sh->mmadone[q], 1); }
     mbar_init(&sh->done, 1);
     sh->mma_any = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -266,14 +292,13 @@ k_leg_fwd_tma(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int t
                  "r"(tmem_cols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // row scale from the row-maximum table (a bound of both folds)
+  const int row = row0 + r, q4 = row & 3;
   if (h == 0) {
-    const int row = row0 + r;
     float mx = 0.0f;
-    if (row < nrows && np > 0) {
+    if (row < nrows) {
       const float *Mf = a.rowmax + (size_t)m * (a.sP + a.sD);
       if (g == 0) mx = Mf[row];
-      else { const int q = row & 3; mx = fmaxf(Mf[a.sP + row], Mf[a.sP + row - q + 3 - q]); }
+      else mx = fmaxf(Mf[a.sP + row], Mf[a.sP + row - q4 + 3 - q4]);
     }
     sh->rowscale[r] = pow2_scale(mx);
   }
@@ -282,134 +307,148 @@ k_leg_fwd_tma(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int t
   tc_fence_after();
   const uint32_t tmem = sh->tmem_base;
 
-  // block b -> (theta block, part)
   auto tb_of = [&](int b) { return g ? (b >> 1) : b; };
   auto part_of = [&](int b) { return g ? (b & 1) : 0; };
   auto issue_raw = [&](int tb) {
-    const int q = tb % FST;
+    const int q = tb % FRS;
     unsigned char *dst = raw0 + q * RAW_BYTES;
     mbar_expect_tx(&sh->rawfull[q], RAW_BYTES);
-    tma_load_2d(dst, traw, &sh->rawfull[q], row0, m * a.nth + tb * FKB);
-    tma_load_2d(dst + RAW_BYTES / 2, traw, &sh->rawfull[q], row0, m * a.nth + a.nth - tb * FKB - FKB);
+    const uint64_t pf = policy_evict_first();
+    tma_load_2d_hint(dst, traw, &sh->rawfull[q], row0, m * a.nth + tb * FKB, pf);
+    tma_load_2d_hint(dst + RAW_BYTES / 2, traw, &sh->rawfull[q], row0, m * a.nth + a.nth - tb * FKB - FKB, pf);
   };
   auto issue_b = [&](int b) {
-    const int q = b % FST, tb = tb_of(b), part = part_of(b);
-    unsigned char *bh = ab0 + q * AB_BYTES + 2 * FA_BYTES, *bl = bh + B_BYTES;
-    const uint32_t bytes = (uint32_t)nbox * a.boxr * FKB * 2;
-    mbar_expect_tx(&sh->bfull[q], 2 * bytes);
+    const int q = b % FAB, tb = tb_of(b), part = part_of(b);
+    unsigned char *bb = ab0 + q * AB_BYTES + 4 * FA_BYTES;
+    uint32_t bytes = 0;
+    for (int p = 0; p < 2; p++) bytes += 2u * (uint32_t)nbox[p] * a.boxr * FKB * 2;
+    mbar_expect_tx(&sh->bfull[q], bytes);
     const int x = part * a.nhp + tb * FKB;
-    for (int j = 0; j < nbox; j++) {
-      tma_load_2d(bh + j * a.boxr * FKB * 2, tbh, &sh->bfull[q], x, brow + j * a.boxr);
-      tma_load_2d(bl + j * a.boxr * FKB * 2, tbl, &sh->bfull[q], x, brow + j * a.boxr);
+    const uint64_t pl = policy_evict_last();
+    for (int p = 0; p < 2; p++) {
+      unsigned char *bh = bb + (2 * p) * B_BYTES, *bl = bh + B_BYTES;
+      for (int j = 0; j < nbox[p]; j++) {
+        tma_load_2d_hint(bh + j * a.boxr * FKB * 2, tbh, &sh->bfull[q], x, brow[p] + j * a.boxr, pl);
+        tma_load_2d_hint(bl + j * a.boxr * FKB * 2, tbl, &sh->bfull[q], x, brow[p] + j * a.boxr, pl);
+      }
     }
   };
 
-  int n_raw = 0, n_b = 0, n_rawdone = 0, n_bdone = 0;     // thread 0 bookkeeping
-  int failed = __syncthreads_or((*(volatile int *)a.status & CB2_STATUS_PIPE_TIMEOUT) != 0 || np == 0);
+  int n_raw = 0, n_b = 0, n_rawdone = 0, n_bdone = 0;
+  int failed = __syncthreads_or((*(volatile int *)a.status & CB2_STATUS_PIPE_TIMEOUT) != 0);
   if (tid == 0 && !failed) {
-    for (int tb = 0; tb < min(NT, FST); tb++) { issue_raw(tb); n_raw++; }
-    for (int b = 0; b < min(NB, FST - 1); b++) { issue_b(b); n_b++; }
+    for (int tb = 0; tb < min(NT, FRS); tb++) { issue_raw(tb); n_raw++; }
+    issue_b(0);
+    n_b = 1;
   }
-  const int row = row0 + r, q4 = row & 3;
   const float sc = sh->rowscale[r];
   for (int b = 0; b < NB && !failed; b++) {
-    const int s = b % FST, tb = tb_of(b), part = part_of(b), rs = tb % FST;
+    const int s = b % FAB, tb = tb_of(b), part = part_of(b), rs = tb % FRS;
     int f = 0;
-    // raw tile of this theta block (all threads observe the phase)
-    if (!mbar_wait(&sh->rawfull[rs], (uint32_t)((tb / FST) & 1))) f = 1;
-    // A/B stage s was last read by the MMAs of block b - FST
-    if (b >= FST && !mbar_wait(&sh->mmadone[s], (uint32_t)(((b - FST) / FST) & 1))) f = 1;
+    if (!mbar_wait(&sh->rawfull[rs], (uint32_t)((tb / FRS) & 1))) f = 1;
+    if (b >= FAB && !mbar_wait(&sh->mmadone[s], (uint32_t)(((b - FAB) / FAB) & 1))) f = 1;
     if (__syncthreads_or(f)) { failed = 1; break; }
-    // convert: thread (r, h) builds K values 16 h .. 16 h + 15 of row r
     {
+      // the two folds of this row's 16 K values; parity 0 / 1 take sym or
+      // anti: gemm P and the mP part use fold p, the dP part fold 1 - p
       const float *rs_s = reinterpret_cast<const float *>(raw0 + rs * RAW_BYTES);
       const float *rs_n = rs_s + FKB * TM;
-      int src = r, sigma = p;
-      float sg = 1.0f;
+      int src = r;
+      float sg = sc;
+      bool swap = false;   // parity 0 takes anti
       if (g) {
-        if (part == 0) { sigma = 1 - p; sg = (q4 < 2) ? 1.0f : -1.0f; }
-        else { src = r - q4 + 3 - q4; sigma = p; sg = (q4 & 1) ? 1.0f : -1.0f; }
+        if (part == 0) { sg = (q4 < 2) ? sc : -sc; swap = true; }
+        else { src = r - q4 + 3 - q4; sg = (q4 & 1) ? sc : -sc; }
       }
-      sg *= sc;
-      float x[16];
+      float xs[16], xa[16];
 #pragma unroll
       for (int e = 0; e < 16; e++) {
         const int kk = h * 16 + e, i = tb * FKB + kk;
-        float v = 0.0f;
+        float vs = 0.0f, va = 0.0f;
         if (i < a.nh) {
           const float fa = rs_s[kk * TM + src] * sh->w[i];
           const float fb = rs_n[(FKB - 1 - kk) * TM + src] * sh->w[a.nth - 1 - i];
-          v = (sigma ? fa - fb : fa + fb) * sg;
+          vs = (fa + fb) * sg;
+          va = (fa - fb) * sg;
         }
-        x[e] = v;
+        xs[e] = vs;
+        xa[e] = va;
       }
-      unsigned char *ahi = ab0 + s * AB_BYTES, *alo = ahi + FA_BYTES;
+      unsigned char *at = ab0 + s * AB_BYTES;
 #pragma unroll
-      for (int c = 0; c < 2; c++) {
-        uint32_t hh[4], ll[4];
+      for (int p = 0; p < 2; p++) {
+        const float *x = ((p == 0) != swap) ? xs : xa;
+        unsigned char *ahi = at + (2 * p) * FA_BYTES, *alo = ahi + FA_BYTES;
 #pragma unroll
-        for (int e = 0; e < 8; e += 2) {
-          const float x0 = x[c * 8 + e], x1 = x[c * 8 + e + 1];
-          const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
-          hh[e >> 1] = pack_half2(h0, h1);
-          ll[e >> 1] = pack_half2(__float2half_rn(x0 - __half2float(h0)), __float2half_rn(x1 - __half2float(h1)));
+        for (int c = 0; c < 2; c++) {
+          uint32_t hh[4], ll[4];
+#pragma unroll
+          for (int e = 0; e < 8; e += 2) {
+            const float x0 = x[c * 8 + e], x1 = x[c * 8 + e + 1];
+            const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
+            hh[e >> 1] = pack_half2(h0, h1);
+            ll[e >> 1] = pack_half2(__float2half_rn(x0 - __half2float(h0)), __float2half_rn(x1 - __half2float(h1)));
+          }
+          const uint32_t off = sw64_chunk(r, 2 * h + c);
+          *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+          *reinterpret_cast<uint4 *>(alo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
         }
-        const uint32_t off = sw64_chunk(r, 2 * h + c);
-        *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
-        *reinterpret_cast<uint4 *>(alo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
       }
     }
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      // the raw stage of tb is free once its last block is converted
       const bool last_of_tb = (!g) || part == 1;
-      if (last_of_tb && tb + FST < NT) { issue_raw(tb + FST); n_raw++; }
-      n_rawdone = last_of_tb ? tb + 1 : n_rawdone;
-      if (!mbar_wait(&sh->bfull[s], (uint32_t)((b / FST) & 1))) {
+      if (last_of_tb) {
+        n_rawdone = tb + 1;
+        if (tb + FRS < NT) { issue_raw(tb + FRS); n_raw++; }
+      }
+      if (!mbar_wait(&sh->bfull[s], (uint32_t)((b / FAB) & 1))) {
         f = 1;
       } else {
         n_bdone = b + 1;
         tc_fence_after();
-        unsigned char *ahi = ab0 + s * AB_BYTES, *alo = ahi + FA_BYTES;
-        unsigned char *bh = ahi + 2 * FA_BYTES, *bl = bh + B_BYTES;
-        const uint32_t idesc = idesc_f16_f32(TM, npad);
-        const uint64_t dah = smem_desc_sw64(ahi), dal = smem_desc_sw64(alo);
-        const uint64_t dbh = smem_desc_sw64(bh), dbl = smem_desc_sw64(bl);
+        unsigned char *at = ab0 + s * AB_BYTES, *bb = at + 4 * FA_BYTES;
+        for (int p = 0; p < 2; p++) {
+          if (np[p] == 0) continue;
+          const uint32_t idesc = idesc_f16_f32(TM, npad[p]);
+          const uint64_t dah = smem_desc_sw64(at + (2 * p) * FA_BYTES), dal = smem_desc_sw64(at + (2 * p + 1) * FA_BYTES);
+          const uint64_t dbh = smem_desc_sw64(bb + (2 * p) * B_BYTES), dbl = smem_desc_sw64(bb + (2 * p + 1) * B_BYTES);
+          const uint32_t acc = tmem + (p ? acc1 : 0u);
 #pragma unroll
-        for (int ks = 0; ks < FKB / 16; ks++) {
-          const uint64_t o = (uint64_t)(ks * 2);   // +32 bytes along K
-          mma_f16(tmem, dah + o, dbh + o, idesc, (b == 0 && ks == 0) ? 0u : 1u);
-          mma_f16(tmem, dah + o, dbl + o, idesc, 1u);
-          mma_f16(tmem, dal + o, dbh + o, idesc, 1u);
+          for (int ks = 0; ks < FKB / 16; ks++) {
+            const uint64_t o = (uint64_t)(ks * 2);
+            mma_f16(acc, dah + o, dbh + o, idesc, (b == 0 && ks == 0) ? 0u : 1u);
+            mma_f16(acc, dah + o, dbl + o, idesc, 1u);
+            mma_f16(acc, dal + o, dbh + o, idesc, 1u);
+          }
         }
         mma_commit(&sh->mmadone[s]);
         sh->mma_any = 1;
-        // the B tiles of block b + FST - 1 go to the stage the MMAs of block b - 1 used
-        const int bn = b + FST - 1;
+        // B tiles of block b + 1 go to the other stage, free once block b - 1's MMAs are done
+        const int bn = b + 1;
         if (bn < NB) {
-          if (bn >= FST && !mbar_wait(&sh->mmadone[bn % FST], (uint32_t)(((bn - FST) / FST) & 1))) f = 1;
+          if (bn >= FAB && !mbar_wait(&sh->mmadone[bn % FAB], (uint32_t)(((bn - FAB) / FAB) & 1))) f = 1;
           else { issue_b(bn); n_b++; }
         }
       }
     }
     if (__syncthreads_or(f)) { failed = 1; break; }
   }
-  // drain: loads still in flight (raw and B), then every MMA
   if (tid == 0) {
     for (int tb = n_rawdone; tb < n_raw; tb++)
-      if (!mbar_wait(&sh->rawfull[tb % FST], (uint32_t)((tb / FST) & 1))) failed = 1;
+      if (!mbar_wait(&sh->rawfull[tb % FRS], (uint32_t)((tb / FRS) & 1))) failed = 1;
     for (int b = n_bdone; b < n_b; b++)
-      if (!mbar_wait(&sh->bfull[b % FST], (uint32_t)((b / FST) & 1))) failed = 1;
+      if (!mbar_wait(&sh->bfull[b % FAB], (uint32_t)((b / FAB) & 1))) failed = 1;
     if (sh->mma_any) mma_commit(&sh->done);
   }
   __syncthreads();
-  int f = failed && np > 0;
+  int f = failed;
   if (sh->mma_any && !mbar_wait(&sh->done, 0)) f = 1;
   f = __syncthreads_or(f);
   tc_fence_after();
   if (f && tid == 0) atomicOr(a.status, CB2_STATUS_PIPE_TIMEOUT);
-  if (!f && np > 0) {
+  if (!f) {
     int k, slot, kind, s;   // kind 0: S (g7 r^2), 1: dS or T (g7 r), 2: scalar (g6)
     if (g == 0) {
       const int ng = a.nvec + a.nscal, v = (row >> 1) % ng;
@@ -426,20 +465,22 @@ k_leg_fwd_tma(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int t
     const double rk = valid ? a.r[k] : 0.0;
     const int jjb = a.moff[m] + s * (a.L + 1 - m);
     double *dst = a.f + (size_t)slot * a.fs + (size_t)k * a.jmax + jjb;
-    const float *bun = a.bunscale + ((size_t)g * (a.L + 1) * 2 + m * 2 + p) * a.NFmax;
-    const int nch = (np + 7) / 8;
-    for (int c8 = h; c8 < nch; c8 += 2) {
-      float v8[8];
-      tmem_ld8(tl + (uint32_t)(c8 * 8), v8);
-      if (!valid) continue;
+    for (int p = 0; p < 2; p++) {
+      const float *bun = a.bunscale + ((size_t)g * (a.L + 1) * 2 + m * 2 + p) * a.NFmax;
+      const int nch = (np[p] + 7) / 8;
+      for (int c8 = h; c8 < nch; c8 += 2) {
+        float v8[8];
+        tmem_ld8(tl + (p ? acc1 : 0u) + (uint32_t)(c8 * 8), v8);
+        if (!valid) continue;
 #pragma unroll
-      for (int qq = 0; qq < 8; qq++) {
-        const int t = c8 * 8 + qq;
-        if (t < np) {
-          const int lm = p + 2 * t;   // l - m
-          const double fac = (kind == 0) ? a.g7[jjb + lm] * rk * rk
-                           : (kind == 2) ? a.g6[jjb + lm] : a.g7[jjb + lm] * rk;
-          dst[lm] = (double)v8[qq] * (ua * (double)bun[t]) * fac;
+        for (int qq = 0; qq < 8; qq++) {
+          const int t = c8 * 8 + qq;
+          if (t < np[p]) {
+            const int lm = p + 2 * t;
+            const double fac = (kind == 0) ? a.g7[jjb + lm] * rk * rk
+                             : (kind == 2) ? a.g6[jjb + lm] : a.g7[jjb + lm] * rk;
+            dst[lm] = (double)v8[qq] * (ua * (double)bun[t]) * fac;
+          }
         }
       }
     }
@@ -630,9 +671,10 @@ k_leg_bwd_tma(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int t
     const int gi = g * 2 + p;
     const int bx = a.ko[(m * 4 + gi) * 2 + part] + ib * FKB;
     mbar_expect_tx(&sh->full[q], BRAW_BYTES + 2 * B_BYTES);
-    tma_load_2d(st, traw, &sh->full[q], row0, ky);
-    tma_load_2d(st + BRAW_BYTES + 2 * FA_BYTES, &tb_hi, &sh->full[q], bx, 0);
-    tma_load_2d(st + BRAW_BYTES + 2 * FA_BYTES + B_BYTES, &tb_lo, &sh->full[q], bx, 0);
+    const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+    tma_load_2d_hint(st, traw, &sh->full[q], row0, ky, pf);
+    tma_load_2d_hint(st + BRAW_BYTES + 2 * FA_BYTES, &tb_hi, &sh->full[q], bx, 0, pl);
+    tma_load_2d_hint(st + BRAW_BYTES + 2 * FA_BYTES + B_BYTES, &tb_lo, &sh->full[q], bx, 0, pl);
   };
 
   int n_iss = 0, n_done = 0;   // thread 0 bookkeeping
@@ -964,7 +1006,7 @@ int mixed_setup(Ctx &c) {
   t->boxr = std::min(64, t->NFmax);
   t->nfb = ((t->NFmax + t->boxr - 1) / t->boxr) * t->boxr;
   t->tmem_fwd = 32;
-  while ((int)t->tmem_fwd < t->NFmax) t->tmem_fwd *= 2;
+  while ((int)t->tmem_fwd < 2 * t->NFmax) t->tmem_fwd *= 2;   // two accumulators
   t->rows_all = R + t->NFmax;   // every NFmax-row box stays in the array
   auto up = [&](int **d, const std::vector<int> &v) -> int {
     CB2_CUDA(cudaMalloc(d, v.size() * sizeof(int)));
@@ -1017,15 +1059,15 @@ int mixed_setup(Ctx &c) {
   t->smem_bwd = 1024 + FST * ((size_t)BRAW_BYTES + 2 * (size_t)FA_BYTES + 2 * (size_t)t->nhp * FKB * 2) +
                 sizeof(BwdSmem);
   t->smem_pack = (size_t)4 * 26 * ((L + 1) | 1) * sizeof(float);   // up to 4 radial levels per block
-  t->smem_fwd = 1024 + FST * (size_t)RAW_BYTES + FST * (2 * (size_t)FA_BYTES + 2 * (size_t)t->nfb * FKB * 2) +
-                sizeof(FwdSmem);
+  t->smem_fwd = 1024 + FRS * (size_t)RAW_BYTES + FAB * (4 * (size_t)FA_BYTES + 4 * (size_t)t->nfb * FKB * 2) +
+                sizeof(FwdSmem2);
   if (t->smem_bwd > 227 * 1024 || t->smem_fwd > 227 * 1024) {
     set_error("mixed precision tiles exceed shared memory");
     return CB2_ERR_ARG;
   }
   CB2_CUDA(raise_smem_limit(k_leg_bwd_tma, (int)t->smem_bwd));
   CB2_CUDA(raise_smem_limit(k_pack_bwd, (int)t->smem_pack));
-  CB2_CUDA(raise_smem_limit(k_leg_fwd_tma, (int)t->smem_fwd));
+  CB2_CUDA(raise_smem_limit(k_leg_fwd_tma2, (int)t->smem_fwd));
   return 0;
 }
 
@@ -1121,7 +1163,7 @@ int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots) {
                                                                                        t->rowmax_four);
   const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
-  k_leg_fwd_tma<<<dim3(tiles0 + tiles1, c.L + 1, 2), NTHR, t->smem_fwd, c.stream>>>(
+  k_leg_fwd_tma2<<<dim3(tiles0 + tiles1, c.L + 1), NTHR, t->smem_fwd, c.stream>>>(
       a, rows0, rows1, tiles0, rawP, rawD, t->tm_bfp_hi, t->tm_bfp_lo, t->tm_bfd_hi, t->tm_bfd_lo, t->tmem_fwd);
   return 0;
 }
