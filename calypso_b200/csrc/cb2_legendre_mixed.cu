@@ -149,18 +149,37 @@ __device__ inline void fence_proxy_async() { asm volatile("fence.proxy.async.sha
 __device__ inline void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ inline void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// 8 consecutive fp32 columns of this thread's TMEM lane
-__device__ inline void tmem_ld8(uint32_t taddr, float v[8]) {
-  uint32_t r[8];
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                 "=r"(r[7])
-               : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+// 16 consecutive fp32 columns of this thread's TMEM lane (load and wait in
+// one statement, so no use of the registers can move above the wait)
+__device__ inline void tmem_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
 #pragma unroll
-  for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// two 16-column loads (columns ta.. and tb..) behind one wait
+__device__ inline void tmem_ld16x2(uint32_t ta, uint32_t tb, float va[16], float vb[16]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%32];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%33];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(ta), "r"(tb)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) { va[i] = __uint_as_float(r[i]); vb[i] = __uint_as_float(r[16 + i]); }
+}
 
 // largest scaled magnitude: 2^13 <= mx s < 2^14 (fp16 holds up to 65504)
 constexpr int kScaleExp = 14;
@@ -355,12 +374,12 @@ k_leg_fwd_tma2(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int 
       const float *rs_n = rs_s + FKB * TM;
       int src = r;
       float sg = sc;
-      bool swap = false;   // parity 0 takes anti
+      bool swap = false;   // true: accumulator 0 takes the anti fold
       if (g) {
         if (part == 0) { sg = (q4 < 2) ? sc : -sc; swap = true; }
         else { src = r - q4 + 3 - q4; sg = (q4 & 1) ? sc : -sc; }
       }
-      float xs[16], xa[16];
+      float x2[2][16];   // A rows of accumulator 0 and 1
 #pragma unroll
       for (int e = 0; e < 16; e++) {
         const int kk = h * 16 + e, i = tb * FKB + kk;
@@ -371,13 +390,13 @@ k_leg_fwd_tma2(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int 
           vs = (fa + fb) * sg;
           va = (fa - fb) * sg;
         }
-        xs[e] = vs;
-        xa[e] = va;
+        x2[0][e] = swap ? va : vs;
+        x2[1][e] = swap ? vs : va;
       }
       unsigned char *at = ab0 + s * AB_BYTES;
 #pragma unroll
       for (int p = 0; p < 2; p++) {
-        const float *x = ((p == 0) != swap) ? xs : xa;
+        const float *x = x2[p];
         unsigned char *ahi = at + (2 * p) * FA_BYTES, *alo = ahi + FA_BYTES;
 #pragma unroll
         for (int c = 0; c < 2; c++) {
@@ -449,39 +468,62 @@ k_leg_fwd_tma2(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int 
   tc_fence_after();
   if (f && tid == 0) atomicOr(a.status, CB2_STATUS_PIPE_TIMEOUT);
   if (!f) {
-    int k, slot, kind, s;   // kind 0: S (g7 r^2), 1: dS or T (g7 r), 2: scalar (g6)
-    if (g == 0) {
-      const int ng = a.nvec + a.nscal, v = (row >> 1) % ng;
-      s = row & 1; k = (row >> 1) / ng;
-      slot = a.slot[v]; kind = (v < a.nvec) ? 0 : 2;
-    } else {
-      const int v = (row >> 2) % a.nvec;
-      k = (row >> 2) / a.nvec; s = q4 & 1;
-      slot = a.slot[v] + 1 + (q4 >> 1); kind = 1;
+    // the accumulators go through shared memory (the pipeline buffers are
+    // idle now: every load has landed and every MMA has completed), so that
+    // each warp writes one row's degrees l = m .. L as one contiguous run
+    const int nl = a.L + 1 - m, SP = (a.L + 1) | 1;
+    float *stg = reinterpret_cast<float *>(base);   // [TM][SP], lm = p + 2 t
+    // per-order tables: g7 and g6 at s = 0, 1 and the column unscale by lm
+    double *gt = reinterpret_cast<double *>(base + (((size_t)TM * SP * 4 + 15) & ~(size_t)15));
+    float *bt = reinterpret_cast<float *>(gt + 4 * nl);
+    {
+      const float *bun0 = a.bunscale + ((size_t)g * (a.L + 1) * 2 + m * 2) * a.NFmax, *bun1 = bun0 + a.NFmax;
+      for (int i = tid; i < nl; i += NTHR) {
+        const int j0 = a.moff[m] + i, j1 = j0 + nl;
+        gt[i] = a.g7[j0];
+        gt[nl + i] = (m > 0) ? a.g7[j1] : 0.0;
+        gt[2 * nl + i] = a.g6[j0];
+        gt[3 * nl + i] = (m > 0) ? a.g6[j1] : 0.0;
+        bt[i] = (i & 1) ? bun1[i >> 1] : bun0[i >> 1];
+      }
     }
-    const bool valid = row < nrows && !(m == 0 && s == 1);
-    const double ua = 1.0 / (double)sc;
     const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-    const double rk = valid ? a.r[k] : 0.0;
-    const int jjb = a.moff[m] + s * (a.L + 1 - m);
-    double *dst = a.f + (size_t)slot * a.fs + (size_t)k * a.jmax + jjb;
     for (int p = 0; p < 2; p++) {
-      const float *bun = a.bunscale + ((size_t)g * (a.L + 1) * 2 + m * 2 + p) * a.NFmax;
-      const int nch = (np[p] + 7) / 8;
-      for (int c8 = h; c8 < nch; c8 += 2) {
-        float v8[8];
-        tmem_ld8(tl + (p ? acc1 : 0u) + (uint32_t)(c8 * 8), v8);
-        if (!valid) continue;
+      const int nch = (np[p] + 15) / 16;
+      for (int c = h; c < nch; c += 2) {
+        float v[16];
+        tmem_ld16(tl + (p ? acc1 : 0u) + (uint32_t)(c * 16), v);
 #pragma unroll
-        for (int qq = 0; qq < 8; qq++) {
-          const int t = c8 * 8 + qq;
-          if (t < np[p]) {
-            const int lm = p + 2 * t;
-            const double fac = (kind == 0) ? a.g7[jjb + lm] * rk * rk
-                             : (kind == 2) ? a.g6[jjb + lm] : a.g7[jjb + lm] * rk;
-            dst[lm] = (double)v8[qq] * (ua * (double)bun[t]) * fac;
-          }
+        for (int q = 0; q < 16; q++) {
+          const int t = c * 16 + q;
+          if (t < np[p]) stg[r * SP + p + 2 * t] = v[q];
         }
+      }
+    }
+    __syncthreads();
+    const int lane = tid & 31;
+    for (int rr = warp; rr < TM; rr += NTHR / 32) {
+      const int rw = row0 + rr;
+      if (rw >= nrows) break;
+      int k, slot, kind, s;   // kind 0: S (g7 r^2), 1: dS or T (g7 r), 2: scalar (g6)
+      if (g == 0) {
+        const int ng = a.nvec + a.nscal, v = (rw >> 1) % ng;
+        s = rw & 1; k = (rw >> 1) / ng;
+        slot = a.slot[v]; kind = (v < a.nvec) ? 0 : 2;
+      } else {
+        const int v = (rw >> 2) % a.nvec;
+        k = (rw >> 2) / a.nvec; s = rw & 1;
+        slot = a.slot[v] + 1 + ((rw & 3) >> 1); kind = 1;
+      }
+      if (m == 0 && s == 1) continue;
+      const double ua = 1.0 / (double)sh->rowscale[rr];
+      const double rk = a.r[k];
+      double *dst = a.f + (size_t)slot * a.fs + (size_t)k * a.jmax + a.moff[m] + s * nl;
+      const double *gr = gt + ((kind == 2) ? 2 * nl : 0) + s * nl;
+      for (int lm = lane; lm < nl; lm += 32) {
+        const double gl = gr[lm];
+        const double fac = (kind == 2) ? gl : (kind == 0) ? gl * rk * rk : gl * rk;
+        dst[lm] = (double)stg[rr * SP + lm] * (ua * (double)bt[lm]) * fac;
       }
     }
   }
@@ -593,6 +635,7 @@ struct BwdSmem {
   uint32_t tmem_base;
   int mma_any;
   float rowscale[TM];
+  float bun[256];   // 1 / column scale of this (gemm, m), nhp <= 256
 };
 
 constexpr uint32_t BRAW_BYTES = FKB * TM * 4;   // raw rows of one K block
@@ -615,23 +658,22 @@ k_leg_bwd_tma(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int t
   const int nl = a.L + 1 - m, cnt0 = (nl + 1) / 2, cnt1 = nl / 2;
   // K parts per accumulator p: gemm P one part (parity p); gemm DM dP part
   // (parity 1-p) then mP part (parity p)
-  int plen[2][2], pblk[2][2], nkb[2];
-  for (int p = 0; p < 2; p++) {
-    const int cp = p ? cnt1 : cnt0, cq = p ? cnt0 : cnt1;
-    plen[p][0] = g ? cq : cp;
-    plen[p][1] = g ? cp : 0;
-    pblk[p][0] = (plen[p][0] + FKB - 1) / FKB;
-    pblk[p][1] = (plen[p][1] + FKB - 1) / FKB;
-    nkb[p] = pblk[p][0] + pblk[p][1];
-  }
-  const int nmin = min(nkb[0], nkb[1]), total = nkb[0] + nkb[1];
-  const int pmore = (nkb[0] >= nkb[1]) ? 0 : 1;
-  // block b -> accumulator p, part, block index within the part
-  auto blk = [&](int b, int &p, int &part, int &ib) {
+  // (scalars, not arrays: a runtime index would put them in local memory)
+  const int len00 = g ? cnt1 : cnt0, len01 = g ? cnt0 : 0;   // accumulator 0, parts 0 / 1
+  const int len10 = g ? cnt0 : cnt1, len11 = g ? cnt1 : 0;   // accumulator 1
+  const int blk00 = (len00 + FKB - 1) / FKB, blk01 = (len01 + FKB - 1) / FKB;
+  const int blk10 = (len10 + FKB - 1) / FKB, blk11 = (len11 + FKB - 1) / FKB;
+  const int nkb0 = blk00 + blk01, nkb1 = blk10 + blk11;
+  const int nmin = min(nkb0, nkb1), total = nkb0 + nkb1;
+  const int pmore = (nkb0 >= nkb1) ? 0 : 1;
+  // block b -> accumulator p, part, block index within the part, valid K rows
+  auto blk = [&](int b, int &p, int &part, int &ib, int &len) {
     int i;
     if (b < 2 * nmin) { p = b & 1; i = b >> 1; } else { p = pmore; i = nmin + (b - 2 * nmin); }
-    part = (i < pblk[p][0]) ? 0 : 1;
-    ib = part ? i - pblk[p][0] : i;
+    const int b0 = p ? blk10 : blk00;
+    part = (i < b0) ? 0 : 1;
+    ib = part ? i - b0 : i;
+    len = p ? (part ? len11 : len10) : (part ? len01 : len00);
   };
   const CUtensorMap *traw = g ? &tm_rawD : &tm_rawP;
 
@@ -655,14 +697,15 @@ k_leg_bwd_tma(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int t
     }
     sh->rowscale[r] = pow2_scale(mx);
   }
+  for (int i = tid; i < a.nhp; i += NTHR) sh->bun[i] = a.bunscale[((size_t)g * (a.L + 1) + m) * a.nhp + i];
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sh->tmem_base;
 
   auto issue = [&](int b) {
-    int p, part, ib;
-    blk(b, p, part, ib);
+    int p, part, ib, len;
+    blk(b, p, part, ib, len);
     const int q = b % FST;
     unsigned char *st = base + q * ST_BYTES;
     // raw rows: parity of l-m of this part
@@ -683,8 +726,8 @@ k_leg_bwd_tma(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int t
     for (int b = 0; b < min(total, FST - 1); b++) { issue(b); n_iss++; }
   const float sc = sh->rowscale[r];
   for (int b = 0; b < total && !failed; b++) {
-    int p, part, ib;
-    blk(b, p, part, ib);
+    int p, part, ib, len;
+    blk(b, p, part, ib, len);
     const int s = b % FST;
     unsigned char *st = base + s * ST_BYTES;
     int f = 0;
@@ -699,7 +742,7 @@ k_leg_bwd_tma(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int t
         if (part == 0) sg = (q4 < 2) ? sc : -sc;
         else { src = r - q4 + 3 - q4; sg = (q4 & 1) ? -sc : sc; }
       }
-      const int kv = plen[p][part] - ib * FKB;   // valid K entries of this block
+      const int kv = len - ib * FKB;   // valid K entries of this block
       float x[16];
 #pragma unroll
       for (int e = 0; e < 16; e++) {
@@ -733,7 +776,7 @@ k_leg_bwd_tma(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int t
       const uint64_t dah = smem_desc_sw64(ahi), dal = smem_desc_sw64(alo);
       const uint64_t dbh = smem_desc_sw64(bh), dbl = smem_desc_sw64(bl);
       const uint32_t acc = tmem + (uint32_t)(p * ACC1);
-      const bool first = (ib == 0) && (part == 0 || pblk[p][0] == 0);   // first block of accumulator p
+      const bool first = (ib == 0) && (part == 0 || (p ? blk10 : blk00) == 0);   // first block of accumulator p
 #pragma unroll
       for (int ks = 0; ks < FKB / 16; ks++) {
         const uint64_t o = (uint64_t)(ks * 2);
@@ -767,26 +810,26 @@ k_leg_bwd_tma(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int t
     const bool valid = row < nrows;
     const float ua = 1.0f / sc;
     const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-    const bool has1 = nkb[1] > 0;
+    const bool has1 = nkb1 > 0;
     float *outb = g ? a.out.D : a.out.P;
     const size_t so = g ? a.out.sD() : a.out.sP();
-    const float *bun = a.bunscale + ((size_t)g * (a.L + 1) + m) * a.nhp;
     const int half = a.nhp / 2;
-    for (int t0 = h * half; t0 < (h + 1) * half; t0 += 8) {
-      float e[8], o[8];
-      tmem_ld8(tl + (uint32_t)t0, e);
+    const int iend = min((h + 1) * half, a.nh);
+    for (int t0 = h * half; t0 < (h + 1) * half; t0 += 16) {
+      float e[16], o[16];
       if (has1) {
-        tmem_ld8(tl + (uint32_t)(ACC1 + t0), o);
+        tmem_ld16x2(tl + (uint32_t)t0, tl + (uint32_t)(ACC1 + t0), e, o);
       } else {
+        tmem_ld16(tl + (uint32_t)t0, e);
 #pragma unroll
-        for (int q = 0; q < 8; q++) o[q] = 0.0f;
+        for (int q = 0; q < 16; q++) o[q] = 0.0f;
       }
       if (!valid) continue;
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
+      for (int q = 0; q < 16; q++) {
         const int i = t0 + q;
-        if (i < a.nh) {
-          const float us = ua * bun[i];
+        if (i < iend) {
+          const float us = ua * sh->bun[i];
           outb[((size_t)m * a.nth + i) * so + row] = (e[q] + o[q]) * us;
           outb[((size_t)m * a.nth + (a.nth - 1 - i)) * so + row] = (e[q] - o[q]) * us;
         }
@@ -1061,7 +1104,11 @@ int mixed_setup(Ctx &c) {
   t->smem_pack = (size_t)4 * 26 * ((L + 1) | 1) * sizeof(float);   // up to 4 radial levels per block
   t->smem_fwd = 1024 + FRS * (size_t)RAW_BYTES + FAB * (4 * (size_t)FA_BYTES + 4 * (size_t)t->nfb * FKB * 2) +
                 sizeof(FwdSmem2);
-  if (t->smem_bwd > 227 * 1024 || t->smem_fwd > 227 * 1024) {
+  // the forward epilogue stages [TM][(L+1)|1] floats and its factor tables
+  // (4 (L+1) doubles, L+1 floats) in the pipeline buffers
+  const size_t fwd_pipe = FRS * (size_t)RAW_BYTES + FAB * (4 * (size_t)FA_BYTES + 4 * (size_t)t->nfb * FKB * 2);
+  const size_t fwd_epi = (((size_t)TM * ((L + 1) | 1) * 4 + 15) & ~(size_t)15) + (size_t)(L + 1) * 36;
+  if (t->smem_bwd > 227 * 1024 || t->smem_fwd > 227 * 1024 || fwd_epi > fwd_pipe) {
     set_error("mixed precision tiles exceed shared memory");
     return CB2_ERR_ARG;
   }
