@@ -250,285 +250,392 @@ __device__ inline uint32_t sw64_chunk(int row, int c) {
   return (uint32_t)row * 64u + ((uint32_t)(c ^ ((row >> 1) & 3)) << 4);
 }
 
-// Both parities in one CTA: the raw tiles of a block feed the symmetric and
-// the antisymmetric fold at once (one read of the raw rows instead of two).
-// Stages: two raw (south + north, 32 KB each), two A/B holding the A tiles
-// of both parities (4 x 8 KB) and their B tiles.  Accumulator of parity p at
-// TMEM column p * tmem_cols / 2.
+// Forward stages: both parities come from one raw tile (the symmetric and
+// the antisymmetric fold), so a K block has two raw halves (south + north,
+// 32 KB together), the A tiles of both parities (4 x 8 KB) and their B
+// tiles.
 constexpr int FRS = 2;   // raw stages
 constexpr int FAB = 2;   // A/B stages
 
-struct FwdSmem2 {
-  uint64_t rawfull[FRS], bfull[FAB], mmadone[FAB], done;
-  uint32_t tmem_base;
-  int mma_any;
-  float rowscale[TM];
-  float w[1024];
+// ---------------------------------------------------------------------------
+// forward, warp-specialised and persistent: one CTA per SM walks the tiles
+// (m, gemm, 128 rows) in order-major order, so the CTAs in flight share the
+// basis tables of a few orders in L2.  Roles:
+//   warps 0-7   converters: raw float32 rows (TMA) -> scaled, folded, split
+//               fp16 hi/lo A operands (64-byte swizzle), both parities
+//   warps 8-11  epilogue: TMEM -> per-warp shared transpose -> one row's
+//               degrees l = m .. L per store run, float64, geometric factors
+//   warp 12     TMA producer (raw rows and basis tiles)
+//   warp 13     MMA issuer (tcgen05, one elected thread)
+// Two TMEM accumulator sets (when they fit) let the epilogue of one tile
+// overlap the main loop of the next.
+constexpr int FW_CONV = 256, FW_EPI = 128, FW_THREADS = 448;
+constexpr int FW_PROD_WARP = 12, FW_MMA_WARP = 13;
+constexpr int FW_EPI_PITCH = 33;
+
+struct FwdWsLayout {
+  uint32_t raw, ab, stg, moff, mc, mg, w, bar, total;   // byte offsets from the aligned base
 };
 
-__global__ void __launch_bounds__(NTHR, 1)
-k_leg_fwd_tma2(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int tiles_g0,
-               const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
-               const __grid_constant__ CUtensorMap tmp_hi, const __grid_constant__ CUtensorMap tmp_lo,
-               const __grid_constant__ CUtensorMap tmd_hi, const __grid_constant__ CUtensorMap tmd_lo,
-               uint32_t tmem_cols) {
+__host__ __device__ inline FwdWsLayout fwd_ws_layout(int nfb, int L, int nth) {
+  FwdWsLayout o;
+  uint32_t p = 0;
+  const uint32_t bbytes = (uint32_t)nfb * FKB * 2;
+  o.raw = p; p += FRS * RAW_BYTES;
+  o.ab = p; p += FAB * (4 * FA_BYTES + 4 * bbytes);
+  o.stg = p; p += 4 * 32 * FW_EPI_PITCH * 4;
+  o.moff = p; p += TM * 8;
+  o.mc = p; p += TM * 8;
+  o.mg = p; p += TM * 4;
+  o.w = p; p += ((uint32_t)nth * 4 + 15) & ~15u;
+  o.bar = p; p += 256;
+  o.total = p;
+  return o;
+}
+
+struct FwdWsBars {
+  uint64_t rawfull[FRS], rawempty[FRS], afull[FAB], bfull[FAB], abempty[FAB];
+  uint64_t accfull[2], accempty[2], fin;
+  uint32_t tmem_base;
+  int abort;
+};
+
+struct FwdTile {
+  int m, g, row0, nrows, np0, np1, npad0, npad1, nbox0, nbox1, brow0, brow1, NB;
+};
+
+__device__ inline FwdTile fwd_tile(const FwdArgs &a, int t, int rows_g0, int rows_g1, int tiles_g0, int tiles_g1) {
+  FwdTile q;
+  const int tpm = tiles_g0 + tiles_g1;
+  q.m = t / tpm;
+  const int x = t - q.m * tpm;
+  q.g = (x >= tiles_g0) ? 1 : 0;
+  q.row0 = (q.g ? x - tiles_g0 : x) * TM;
+  q.nrows = q.g ? rows_g1 : rows_g0;
+  q.np0 = a.nlp[q.m * 2];
+  q.np1 = a.nlp[q.m * 2 + 1];
+  q.npad0 = ((q.np0 + 15) / 16) * 16;
+  q.npad1 = ((q.np1 + 15) / 16) * 16;
+  q.nbox0 = (q.npad0 + a.boxr - 1) / a.boxr;
+  q.nbox1 = (q.npad1 + a.boxr - 1) / a.boxr;
+  q.brow0 = a.roff[q.m * 2];
+  q.brow1 = a.roff[q.m * 2 + 1];
+  const int NT = (a.nh + FKB - 1) / FKB;
+  q.NB = q.g ? 2 * NT : NT;
+  return q;
+}
+
+// row scale of tile row `row` (converters and epilogue compute the same value)
+__device__ inline float fwd_row_scale(const FwdArgs &a, const FwdTile &q, int row) {
+  float mx = 0.0f;
+  if (row < q.nrows) {
+    const float *Mf = a.rowmax + (size_t)q.m * (a.sP + a.sD);
+    const int q4 = row & 3;
+    if (q.g == 0) mx = Mf[row];
+    else mx = fmaxf(Mf[a.sP + row], Mf[a.sP + row - q4 + 3 - q4]);
+  }
+  return pow2_scale(mx);
+}
+
+__device__ inline void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ inline bool ws_aborted(const FwdWsBars *sb) { return *(volatile const int *)&sb->abort != 0; }
+
+__global__ void __launch_bounds__(FW_THREADS, 1)
+k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int tiles_g0, int tiles_g1, int ntiles,
+             const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
+             const __grid_constant__ CUtensorMap tmp_hi, const __grid_constant__ CUtensorMap tmp_lo,
+             const __grid_constant__ CUtensorMap tmd_hi, const __grid_constant__ CUtensorMap tmd_lo,
+             uint32_t tmem_cols, int nacc) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char *base = smem_base_1024(smem_raw);
-  const uint32_t B_BYTES = (uint32_t)a.nfb * FKB * 2;       // one of hi / lo, one parity
-  const uint32_t AB_BYTES = 4 * FA_BYTES + 4 * B_BYTES;     // A hi/lo x 2 parities, B hi/lo x 2 parities
-  unsigned char *raw0 = base;
-  unsigned char *ab0 = base + FRS * RAW_BYTES;
-  FwdSmem2 *sh = reinterpret_cast<FwdSmem2 *>(ab0 + FAB * AB_BYTES);
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int r = tid & (TM - 1), h = tid >> 7;
-  const int m = blockIdx.y;
-  const int g = (blockIdx.x < (unsigned)tiles_g0) ? 0 : 1;
-  const int nrows = g ? rows_g1 : rows_g0;
-  const int row0 = (g ? blockIdx.x - tiles_g0 : blockIdx.x) * TM;
-  int np[2], npad[2], nbox[2], brow[2];
-  for (int p = 0; p < 2; p++) {
-    np[p] = a.nlp[m * 2 + p];
-    npad[p] = ((np[p] + 15) / 16) * 16;
-    nbox[p] = (npad[p] + a.boxr - 1) / a.boxr;
-    brow[p] = a.roff[m * 2 + p];
-  }
-  const int NT = (a.nh + FKB - 1) / FKB;
-  const int NB = g ? 2 * NT : NT;
-  const CUtensorMap *traw = g ? &tm_rawD : &tm_rawP;
-  const CUtensorMap *tbh = g ? &tmd_hi : &tmp_hi, *tbl = g ? &tmd_lo : &tmp_lo;
-  const uint32_t acc1 = tmem_cols / 2;
+  const FwdWsLayout lay = fwd_ws_layout(a.nfb, a.L, a.nth);
+  FwdWsBars *sb = reinterpret_cast<FwdWsBars *>(base + lay.bar);
+  float *w = reinterpret_cast<float *>(base + lay.w);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t B_BYTES = (uint32_t)a.nfb * FKB * 2;      // one of hi / lo, one parity
+  const uint32_t AB_BYTES = 4 * FA_BYTES + 4 * B_BYTES;    // A hi/lo x 2 parities, B hi/lo x 2 parities
+  unsigned char *raw0 = base + lay.raw, *ab0 = base + lay.ab;
+  const uint32_t accw = tmem_cols / (uint32_t)nacc;       // columns of one accumulator set
+  const uint32_t acc1 = accw / 2;                          // parity-1 accumulator within a set
 
   if (tid == 0) {
-    for (int q = 0; q < FRS; q++) mbar_init(&sh->rawfull[q], 1);
-    for (int q = 0; q < FAB; q++) { mbar_init(&sh->bfull[q], 1); mbar_init(&sh->mmadone[q], 1); }
-    mbar_init(&sh->done, 1);
-    sh->mma_any = 0;
+    for (int q = 0; q < FRS; q++) { mbar_init(&sb->rawfull[q], 1); mbar_init(&sb->rawempty[q], FW_CONV); }
+    for (int q = 0; q < FAB; q++) {
+      mbar_init(&sb->afull[q], FW_CONV); mbar_init(&sb->bfull[q], 1); mbar_init(&sb->abempty[q], 1);
+    }
+    for (int q = 0; q < 2; q++) { mbar_init(&sb->accfull[q], 1); mbar_init(&sb->accempty[q], FW_EPI); }
+    mbar_init(&sb->fin, 1);
+    sb->abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int q = tid; q < a.nth; q += NTHR) sh->w[q] = a.wgt[q];
+  for (int q = tid; q < a.nth; q += FW_THREADS) w[q] = a.wgt[q];
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem_base)),
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sb->tmem_base)),
                  "r"(tmem_cols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  const int row = row0 + r, q4 = row & 3;
-  if (h == 0) {
-    float mx = 0.0f;
-    if (row < nrows) {
-      const float *Mf = a.rowmax + (size_t)m * (a.sP + a.sD);
-      if (g == 0) mx = Mf[row];
-      else mx = fmaxf(Mf[a.sP + row], Mf[a.sP + row - q4 + 3 - q4]);
-    }
-    sh->rowscale[r] = pow2_scale(mx);
-  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = sh->tmem_base;
+  const uint32_t tmem = sb->tmem_base;
+  const bool skip = (*(volatile int *)a.status & CB2_STATUS_PIPE_TIMEOUT) != 0;
 
-  auto tb_of = [&](int b) { return g ? (b >> 1) : b; };
-  auto part_of = [&](int b) { return g ? (b & 1) : 0; };
-  auto issue_raw = [&](int tb) {
-    const int q = tb % FRS;
-    unsigned char *dst = raw0 + q * RAW_BYTES;
-    mbar_expect_tx(&sh->rawfull[q], RAW_BYTES);
-    const uint64_t pf = policy_evict_first();
-    tma_load_2d_hint(dst, traw, &sh->rawfull[q], row0, m * a.nth + tb * FKB, pf);
-    tma_load_2d_hint(dst + RAW_BYTES / 2, traw, &sh->rawfull[q], row0, m * a.nth + a.nth - tb * FKB - FKB, pf);
-  };
-  auto issue_b = [&](int b) {
-    const int q = b % FAB, tb = tb_of(b), part = part_of(b);
-    unsigned char *bb = ab0 + q * AB_BYTES + 4 * FA_BYTES;
-    uint32_t bytes = 0;
-    for (int p = 0; p < 2; p++) bytes += 2u * (uint32_t)nbox[p] * a.boxr * FKB * 2;
-    mbar_expect_tx(&sh->bfull[q], bytes);
-    const int x = part * a.nhp + tb * FKB;
-    const uint64_t pl = policy_evict_last();
-    for (int p = 0; p < 2; p++) {
-      unsigned char *bh = bb + (2 * p) * B_BYTES, *bl = bh + B_BYTES;
-      for (int j = 0; j < nbox[p]; j++) {
-        tma_load_2d_hint(bh + j * a.boxr * FKB * 2, tbh, &sh->bfull[q], x, brow[p] + j * a.boxr, pl);
-        tma_load_2d_hint(bl + j * a.boxr * FKB * 2, tbl, &sh->bfull[q], x, brow[p] + j * a.boxr, pl);
-      }
-    }
-  };
-
-  int n_raw = 0, n_b = 0, n_rawdone = 0, n_bdone = 0;
-  int failed = __syncthreads_or((*(volatile int *)a.status & CB2_STATUS_PIPE_TIMEOUT) != 0);
-  if (tid == 0 && !failed) {
-    for (int tb = 0; tb < min(NT, FRS); tb++) { issue_raw(tb); n_raw++; }
-    issue_b(0);
-    n_b = 1;
-  }
-  const float sc = sh->rowscale[r];
-  for (int b = 0; b < NB && !failed; b++) {
-    const int s = b % FAB, tb = tb_of(b), part = part_of(b), rs = tb % FRS;
-    int f = 0;
-    if (!mbar_wait(&sh->rawfull[rs], (uint32_t)((tb / FRS) & 1))) f = 1;
-    if (b >= FAB && !mbar_wait(&sh->mmadone[s], (uint32_t)(((b - FAB) / FAB) & 1))) f = 1;
-    if (__syncthreads_or(f)) { failed = 1; break; }
-    {
-      // the two folds of this row's 16 K values; parity 0 / 1 take sym or
-      // anti: gemm P and the mP part use fold p, the dP part fold 1 - p
-      const float *rs_s = reinterpret_cast<const float *>(raw0 + rs * RAW_BYTES);
-      const float *rs_n = rs_s + FKB * TM;
-      int src = r;
-      float sg = sc;
-      bool swap = false;   // true: accumulator 0 takes the anti fold
-      if (g) {
-        if (part == 0) { sg = (q4 < 2) ? sc : -sc; swap = true; }
-        else { src = r - q4 + 3 - q4; sg = (q4 & 1) ? sc : -sc; }
-      }
-      float x2[2][16];   // A rows of accumulator 0 and 1
-#pragma unroll
-      for (int e = 0; e < 16; e++) {
-        const int kk = h * 16 + e, i = tb * FKB + kk;
-        float vs = 0.0f, va = 0.0f;
-        if (i < a.nh) {
-          const float fa = rs_s[kk * TM + src] * sh->w[i];
-          const float fb = rs_n[(FKB - 1 - kk) * TM + src] * sh->w[a.nth - 1 - i];
-          vs = (fa + fb) * sg;
-          va = (fa - fb) * sg;
-        }
-        x2[0][e] = swap ? va : vs;
-        x2[1][e] = swap ? vs : va;
-      }
-      unsigned char *at = ab0 + s * AB_BYTES;
-#pragma unroll
-      for (int p = 0; p < 2; p++) {
-        const float *x = x2[p];
-        unsigned char *ahi = at + (2 * p) * FA_BYTES, *alo = ahi + FA_BYTES;
-#pragma unroll
-        for (int c = 0; c < 2; c++) {
-          uint32_t hh[4], ll[4];
-#pragma unroll
-          for (int e = 0; e < 8; e += 2) {
-            const float x0 = x[c * 8 + e], x1 = x[c * 8 + e + 1];
-            const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
-            hh[e >> 1] = pack_half2(h0, h1);
-            ll[e >> 1] = pack_half2(__float2half_rn(x0 - __half2float(h0)), __float2half_rn(x1 - __half2float(h1)));
+  if (skip) {
+    // an earlier launch timed out: do nothing
+  } else if (warp == FW_PROD_WARP) {
+    if (lane == 0) {
+      uint32_t nraw = 0, nab = 0;
+      bool bad = false;
+      for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x) {
+        if (ws_aborted(sb)) { bad = true; break; }
+        const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+        const CUtensorMap *traw = q.g ? &tm_rawD : &tm_rawP;
+        const CUtensorMap *tbh = q.g ? &tmd_hi : &tmp_hi, *tbl = q.g ? &tmd_lo : &tmp_lo;
+        const uint32_t bbytes = 2u * (uint32_t)(q.nbox0 + q.nbox1) * a.boxr * FKB * 2;
+        for (int b = 0; b < q.NB; b++) {
+          const int tb = q.g ? (b >> 1) : b, part = q.g ? (b & 1) : 0;
+          if (part == 0) {
+            const uint32_t rs = nraw % FRS;
+            if (nraw >= FRS && !mbar_wait(&sb->rawempty[rs], ((nraw / FRS) - 1) & 1)) { bad = true; break; }
+            unsigned char *dst = raw0 + rs * RAW_BYTES;
+            mbar_expect_tx(&sb->rawfull[rs], RAW_BYTES);
+            const uint64_t pf = policy_evict_first();
+            tma_load_2d_hint(dst, traw, &sb->rawfull[rs], q.row0, q.m * a.nth + tb * FKB, pf);
+            tma_load_2d_hint(dst + RAW_BYTES / 2, traw, &sb->rawfull[rs], q.row0,
+                             q.m * a.nth + a.nth - tb * FKB - FKB, pf);
+            nraw++;
           }
-          const uint32_t off = sw64_chunk(r, 2 * h + c);
-          *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
-          *reinterpret_cast<uint4 *>(alo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+          const uint32_t s = nab % FAB;
+          if (nab >= FAB && !mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1)) { bad = true; break; }
+          unsigned char *bb = ab0 + s * AB_BYTES + 4 * FA_BYTES;
+          mbar_expect_tx(&sb->bfull[s], bbytes);
+          const int x = part * a.nhp + tb * FKB;
+          const uint64_t pl = policy_evict_last();
+          for (int p = 0; p < 2; p++) {
+            unsigned char *bh = bb + (2 * p) * B_BYTES, *bl = bh + B_BYTES;
+            const int nbx = p ? q.nbox1 : q.nbox0, br = p ? q.brow1 : q.brow0;
+            for (int j = 0; j < nbx; j++) {
+              tma_load_2d_hint(bh + j * a.boxr * FKB * 2, tbh, &sb->bfull[s], x, br + j * a.boxr, pl);
+              tma_load_2d_hint(bl + j * a.boxr * FKB * 2, tbl, &sb->bfull[s], x, br + j * a.boxr, pl);
+            }
+          }
+          nab++;
+        }
+      }
+      if (bad) {
+        sb->abort = 1;
+        // every copy still in flight lands before the CTA may exit
+        for (uint32_t q = 0; q < FRS && q < nraw; q++) {
+          const uint32_t last = ((nraw - 1 - q) / FRS) * FRS + q;   // last load issued to stage q
+          mbar_wait(&sb->rawfull[q], (last / FRS) & 1);
+        }
+        for (uint32_t q = 0; q < FAB && q < nab; q++) {
+          const uint32_t last = ((nab - 1 - q) / FAB) * FAB + q;
+          mbar_wait(&sb->bfull[q], (last / FAB) & 1);
         }
       }
     }
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      const bool last_of_tb = (!g) || part == 1;
-      if (last_of_tb) {
-        n_rawdone = tb + 1;
-        if (tb + FRS < NT) { issue_raw(tb + FRS); n_raw++; }
-      }
-      if (!mbar_wait(&sh->bfull[s], (uint32_t)((b / FAB) & 1))) {
-        f = 1;
-      } else {
-        n_bdone = b + 1;
+  } else if (warp == FW_MMA_WARP) {
+    if (lane == 0) {
+      uint32_t nab = 0;
+      bool bad = false, any = false;
+      int i = 0;
+      for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x, i++) {
+        if (ws_aborted(sb)) { bad = true; break; }
+        const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+        const int ab = i % nacc;
+        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1)) { bad = true; break; }
         tc_fence_after();
-        unsigned char *at = ab0 + s * AB_BYTES, *bb = at + 4 * FA_BYTES;
-        for (int p = 0; p < 2; p++) {
-          if (np[p] == 0) continue;
-          const uint32_t idesc = idesc_f16_f32(TM, npad[p]);
-          const uint64_t dah = smem_desc_sw64(at + (2 * p) * FA_BYTES), dal = smem_desc_sw64(at + (2 * p + 1) * FA_BYTES);
-          const uint64_t dbh = smem_desc_sw64(bb + (2 * p) * B_BYTES), dbl = smem_desc_sw64(bb + (2 * p + 1) * B_BYTES);
-          const uint32_t acc = tmem + (p ? acc1 : 0u);
+        const uint32_t accb = tmem + (uint32_t)ab * accw;
+        for (int b = 0; b < q.NB; b++) {
+          const uint32_t s = nab % FAB, ph = (nab / FAB) & 1;
+          if (!mbar_wait(&sb->afull[s], ph) || !mbar_wait(&sb->bfull[s], ph)) { bad = true; break; }
+          tc_fence_after();
+          unsigned char *at = ab0 + s * AB_BYTES, *bb = at + 4 * FA_BYTES;
+          for (int p = 0; p < 2; p++) {
+            const int np = p ? q.np1 : q.np0, npad = p ? q.npad1 : q.npad0;
+            if (np == 0) continue;
+            const uint32_t idesc = idesc_f16_f32(TM, npad);
+            const uint64_t dah = smem_desc_sw64(at + (2 * p) * FA_BYTES), dal = smem_desc_sw64(at + (2 * p + 1) * FA_BYTES);
+            const uint64_t dbh = smem_desc_sw64(bb + (2 * p) * B_BYTES), dbl = smem_desc_sw64(bb + (2 * p + 1) * B_BYTES);
+            const uint32_t acc = accb + (p ? acc1 : 0u);
 #pragma unroll
-          for (int ks = 0; ks < FKB / 16; ks++) {
-            const uint64_t o = (uint64_t)(ks * 2);
-            mma_f16(acc, dah + o, dbh + o, idesc, (b == 0 && ks == 0) ? 0u : 1u);
-            mma_f16(acc, dah + o, dbl + o, idesc, 1u);
-            mma_f16(acc, dal + o, dbh + o, idesc, 1u);
+            for (int ks = 0; ks < FKB / 16; ks++) {
+              const uint64_t o = (uint64_t)(ks * 2);
+              mma_f16(acc, dah + o, dbh + o, idesc, (b == 0 && ks == 0) ? 0u : 1u);
+              mma_f16(acc, dah + o, dbl + o, idesc, 1u);
+              mma_f16(acc, dal + o, dbh + o, idesc, 1u);
+            }
+          }
+          mma_commit(&sb->abempty[s]);
+          any = true;
+          nab++;
+        }
+        if (bad) break;
+        mma_commit(&sb->accfull[ab]);
+      }
+      // no MMA may still run when the CTA releases its tensor memory
+      if (any) {
+        mma_commit(&sb->fin);
+        if (!mbar_wait(&sb->fin, 0)) bad = true;
+      }
+      if (bad) sb->abort = 1;
+    }
+  } else if (warp < FW_CONV / 32) {
+    const int r = tid & (TM - 1), h = tid >> 7;
+    uint32_t nraw = 0, nab = 0;
+    bool bad = false;
+    for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x) {
+      if (ws_aborted(sb)) { bad = true; break; }
+      const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+      const int row = q.row0 + r, q4 = row & 3;
+      const float sc = fwd_row_scale(a, q, row);
+      for (int b = 0; b < q.NB; b++) {
+        const int tb = q.g ? (b >> 1) : b, part = q.g ? (b & 1) : 0;
+        const uint32_t rs = nraw % FRS, s = nab % FAB;
+        if (part == 0 && !mbar_wait(&sb->rawfull[rs], (nraw / FRS) & 1)) { bad = true; break; }
+        if (nab >= FAB && !mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1)) { bad = true; break; }
+        // the two folds of this row's 16 K values; gemm P and the mP part
+        // use fold p, the dP part fold 1 - p (with the signs of its rows)
+        const float *rs_s = reinterpret_cast<const float *>(raw0 + rs * RAW_BYTES);
+        const float *rs_n = rs_s + FKB * TM;
+        int src = r;
+        float sg = sc;
+        bool swap = false;   // true: accumulator 0 takes the anti fold
+        if (q.g) {
+          if (part == 0) { sg = (q4 < 2) ? sc : -sc; swap = true; }
+          else { src = r - q4 + 3 - q4; sg = (q4 & 1) ? sc : -sc; }
+        }
+        float x2[2][16];
+#pragma unroll
+        for (int e = 0; e < 16; e++) {
+          const int kk = h * 16 + e, i = tb * FKB + kk;
+          float vs = 0.0f, va = 0.0f;
+          if (i < a.nh) {
+            const float fa = rs_s[kk * TM + src] * w[i];
+            const float fb = rs_n[(FKB - 1 - kk) * TM + src] * w[a.nth - 1 - i];
+            vs = (fa + fb) * sg;
+            va = (fa - fb) * sg;
+          }
+          x2[0][e] = swap ? va : vs;
+          x2[1][e] = swap ? vs : va;
+        }
+        unsigned char *at = ab0 + s * AB_BYTES;
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+          unsigned char *ahi = at + (2 * p) * FA_BYTES, *alo = ahi + FA_BYTES;
+#pragma unroll
+          for (int c = 0; c < 2; c++) {
+            uint32_t hh[4], ll[4];
+#pragma unroll
+            for (int e = 0; e < 8; e += 2) {
+              const float x0 = x2[p][c * 8 + e], x1 = x2[p][c * 8 + e + 1];
+              const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
+              hh[e >> 1] = pack_half2(h0, h1);
+              ll[e >> 1] = pack_half2(__float2half_rn(x0 - __half2float(h0)), __float2half_rn(x1 - __half2float(h1)));
+            }
+            const uint32_t off = sw64_chunk(r, 2 * h + c);
+            *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+            *reinterpret_cast<uint4 *>(alo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
           }
         }
-        mma_commit(&sh->mmadone[s]);
-        sh->mma_any = 1;
-        // B tiles of block b + 1 go to the other stage, free once block b - 1's MMAs are done
-        const int bn = b + 1;
-        if (bn < NB) {
-          if (bn >= FAB && !mbar_wait(&sh->mmadone[bn % FAB], (uint32_t)(((bn - FAB) / FAB) & 1))) f = 1;
-          else { issue_b(bn); n_b++; }
+        fence_proxy_async();
+        mbar_arrive(&sb->afull[s]);
+        nab++;
+        if (!q.g || part == 1) { mbar_arrive(&sb->rawempty[rs]); nraw++; }
+      }
+    }
+    if (bad) sb->abort = 1;
+  } else {
+    // epilogue warps 8-11: TMEM lanes 32 (warp % 4) .. + 31.  Every
+    // decision that guards a warp-collective TMEM load is made warp-uniform.
+    const int ew = warp - FW_CONV / 32, er = ew * 32 + lane;
+    float *stg = reinterpret_cast<float *>(base + lay.stg) + ew * 32 * FW_EPI_PITCH;
+    long long *moff = reinterpret_cast<long long *>(base + lay.moff);
+    double *mc = reinterpret_cast<double *>(base + lay.mc);
+    int *mg = reinterpret_cast<int *>(base + lay.mg);
+    double *__restrict__ fout = a.f;
+    int i = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
+      if (__any_sync(0xffffffffu, ws_aborted(sb))) break;
+      const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+      const int nl = a.L + 1 - q.m;
+      // this thread's row: destination, scale and geometric factor
+      // (sel: 0 g7 at s = 0, 1 g7 at s = 1, 2 g6 at s = 0, 3 g6 at s = 1)
+      {
+        const int rw = q.row0 + er;
+        long long off = -1;
+        double cr = 0.0;
+        int sel = 0;
+        if (rw < q.nrows) {
+          int k, slot, kind, s;   // kind 0: S (g7 r^2), 1: dS or T (g7 r), 2: scalar (g6)
+          if (q.g == 0) {
+            const int ng = a.nvec + a.nscal, v = (rw >> 1) % ng;
+            s = rw & 1; k = (rw >> 1) / ng;
+            slot = a.slot[v]; kind = (v < a.nvec) ? 0 : 2;
+          } else {
+            const int v = (rw >> 2) % a.nvec;
+            k = (rw >> 2) / a.nvec; s = rw & 1;
+            slot = a.slot[v] + 1 + ((rw & 3) >> 1); kind = 1;
+          }
+          if (!(q.m == 0 && s == 1)) {
+            const double ua = 1.0 / (double)fwd_row_scale(a, q, rw), rk = a.r[k];
+            cr = (kind == 0) ? ua * rk * rk : (kind == 1) ? ua * rk : ua;
+            off = (long long)slot * (long long)a.fs + (long long)k * a.jmax + a.moff[q.m] + s * nl;
+            sel = ((kind == 2) ? 2 : 0) + s;
+          }
         }
+        moff[er] = off; mc[er] = cr; mg[er] = sel;
       }
-    }
-    if (__syncthreads_or(f)) { failed = 1; break; }
-  }
-  if (tid == 0) {
-    for (int tb = n_rawdone; tb < n_raw; tb++)
-      if (!mbar_wait(&sh->rawfull[tb % FRS], (uint32_t)((tb / FRS) & 1))) failed = 1;
-    for (int b = n_bdone; b < n_b; b++)
-      if (!mbar_wait(&sh->bfull[b % FAB], (uint32_t)((b / FAB) & 1))) failed = 1;
-    if (sh->mma_any) mma_commit(&sh->done);
-  }
-  __syncthreads();
-  int f = failed;
-  if (sh->mma_any && !mbar_wait(&sh->done, 0)) f = 1;
-  f = __syncthreads_or(f);
-  tc_fence_after();
-  if (f && tid == 0) atomicOr(a.status, CB2_STATUS_PIPE_TIMEOUT);
-  if (!f) {
-    // the accumulators go through shared memory (the pipeline buffers are
-    // idle now: every load has landed and every MMA has completed), so that
-    // each warp writes one row's degrees l = m .. L as one contiguous run
-    const int nl = a.L + 1 - m, SP = (a.L + 1) | 1;
-    float *stg = reinterpret_cast<float *>(base);   // [TM][SP], lm = p + 2 t
-    // per-order tables: g7 and g6 at s = 0, 1 and the column unscale by lm
-    double *gt = reinterpret_cast<double *>(base + (((size_t)TM * SP * 4 + 15) & ~(size_t)15));
-    float *bt = reinterpret_cast<float *>(gt + 4 * nl);
-    {
-      const float *bun0 = a.bunscale + ((size_t)g * (a.L + 1) * 2 + m * 2) * a.NFmax, *bun1 = bun0 + a.NFmax;
-      for (int i = tid; i < nl; i += NTHR) {
-        const int j0 = a.moff[m] + i, j1 = j0 + nl;
-        gt[i] = a.g7[j0];
-        gt[nl + i] = (m > 0) ? a.g7[j1] : 0.0;
-        gt[2 * nl + i] = a.g6[j0];
-        gt[3 * nl + i] = (m > 0) ? a.g6[j1] : 0.0;
-        bt[i] = (i & 1) ? bun1[i >> 1] : bun0[i >> 1];
-      }
-    }
-    const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-    for (int p = 0; p < 2; p++) {
-      const int nch = (np[p] + 15) / 16;
-      for (int c = h; c < nch; c += 2) {
-        float v[16];
-        tmem_ld16(tl + (p ? acc1 : 0u) + (uint32_t)(c * 16), v);
+      __syncwarp();
+      const int ab = i % nacc;
+      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1);
+      if (!__all_sync(0xffffffffu, ok)) { sb->abort = 1; break; }
+      tc_fence_after();
+      const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)(ew * 32) << 16);
+      const int nch = (nl + 31) / 32, j0 = a.moff[q.m];
+      const float *bun0 = a.bunscale + ((size_t)q.g * (a.L + 1) * 2 + q.m * 2) * a.NFmax, *bun1 = bun0 + a.NFmax;
+      for (int c = 0; c < nch; c++) {
+        float v0[16], v1[16];
+        tmem_ld16x2(tl + (uint32_t)(c * 16), tl + acc1 + (uint32_t)(c * 16), v0, v1);
+        if (c == nch - 1) {
+          tc_fence_before();
+          mbar_arrive(&sb->accempty[ab]);
+        }
+        const int lm = c * 32 + lane;
+        double gsel[4] = {0.0, 0.0, 0.0, 0.0};
+        double bu = 0.0;
+        if (lm < nl) {
+          gsel[0] = __ldg(a.g7 + j0 + lm);
+          gsel[2] = __ldg(a.g6 + j0 + lm);
+          if (q.m > 0) { gsel[1] = __ldg(a.g7 + j0 + nl + lm); gsel[3] = __ldg(a.g6 + j0 + nl + lm); }
+          bu = (double)((lm & 1) ? __ldg(bun1 + (lm >> 1)) : __ldg(bun0 + (lm >> 1)));
+        }
 #pragma unroll
-        for (int q = 0; q < 16; q++) {
-          const int t = c * 16 + q;
-          if (t < np[p]) stg[r * SP + p + 2 * t] = v[q];
+        for (int e = 0; e < 16; e++) {
+          stg[lane * FW_EPI_PITCH + 2 * e] = v0[e];
+          stg[lane * FW_EPI_PITCH + 2 * e + 1] = v1[e];
         }
-      }
-    }
-    __syncthreads();
-    const int lane = tid & 31;
-    for (int rr = warp; rr < TM; rr += NTHR / 32) {
-      const int rw = row0 + rr;
-      if (rw >= nrows) break;
-      int k, slot, kind, s;   // kind 0: S (g7 r^2), 1: dS or T (g7 r), 2: scalar (g6)
-      if (g == 0) {
-        const int ng = a.nvec + a.nscal, v = (rw >> 1) % ng;
-        s = rw & 1; k = (rw >> 1) / ng;
-        slot = a.slot[v]; kind = (v < a.nvec) ? 0 : 2;
-      } else {
-        const int v = (rw >> 2) % a.nvec;
-        k = (rw >> 2) / a.nvec; s = rw & 1;
-        slot = a.slot[v] + 1 + ((rw & 3) >> 1); kind = 1;
-      }
-      if (m == 0 && s == 1) continue;
-      const double ua = 1.0 / (double)sh->rowscale[rr];
-      const double rk = a.r[k];
-      double *dst = a.f + (size_t)slot * a.fs + (size_t)k * a.jmax + a.moff[m] + s * nl;
-      const double *gr = gt + ((kind == 2) ? 2 * nl : 0) + s * nl;
-      for (int lm = lane; lm < nl; lm += 32) {
-        const double gl = gr[lm];
-        const double fac = (kind == 2) ? gl : (kind == 0) ? gl * rk * rk : gl * rk;
-        dst[lm] = (double)stg[rr * SP + lm] * (ua * (double)bt[lm]) * fac;
+        __syncwarp();
+        if (lm < nl) {
+#pragma unroll 4
+          for (int rr = 0; rr < 32; rr++) {
+            const long long o = moff[ew * 32 + rr];
+            const int sl = mg[ew * 32 + rr];
+            const double gv = (sl == 0) ? gsel[0] : (sl == 1) ? gsel[1] : (sl == 2) ? gsel[2] : gsel[3];
+            if (o >= 0) fout[o + lm] = (double)stg[rr * FW_EPI_PITCH + lane] * bu * mc[ew * 32 + rr] * gv;
+          }
+        }
+        __syncwarp();
       }
     }
   }
   tc_fence_before();
   __syncthreads();
+  if (tid == 0 && sb->abort) atomicOr(a.status, CB2_STATUS_PIPE_TIMEOUT);
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
 }
@@ -957,6 +1064,7 @@ struct MixedTables {
   CUtensorMap tm_bb_hi, tm_bb_lo, tm_bfp_hi, tm_bfp_lo, tm_bfd_hi, tm_bfd_lo;
   int boxr = 0, nfb = 0;
   uint32_t tmem_fwd = 0;
+  int nacc_fwd = 1, nsm = 148;
 };
 
 using EncodeFn = PFN_cuTensorMapEncodeTiled_v12000;
@@ -1048,8 +1156,10 @@ int mixed_setup(Ctx &c) {
   if (c.nth % 8 != 0) { set_error("mixed precision path needs nth divisible by 8"); return CB2_ERR_ARG; }
   t->boxr = std::min(64, t->NFmax);
   t->nfb = ((t->NFmax + t->boxr - 1) / t->boxr) * t->boxr;
+  // one accumulator set = both parities; two sets when they fit in TMEM
+  t->nacc_fwd = (4 * t->NFmax <= 512) ? 2 : 1;
   t->tmem_fwd = 32;
-  while ((int)t->tmem_fwd < 2 * t->NFmax) t->tmem_fwd *= 2;   // two accumulators
+  while ((int)t->tmem_fwd < 2 * t->nacc_fwd * t->NFmax) t->tmem_fwd *= 2;
   t->rows_all = R + t->NFmax;   // every NFmax-row box stays in the array
   auto up = [&](int **d, const std::vector<int> &v) -> int {
     CB2_CUDA(cudaMalloc(d, v.size() * sizeof(int)));
@@ -1102,19 +1212,21 @@ int mixed_setup(Ctx &c) {
   t->smem_bwd = 1024 + FST * ((size_t)BRAW_BYTES + 2 * (size_t)FA_BYTES + 2 * (size_t)t->nhp * FKB * 2) +
                 sizeof(BwdSmem);
   t->smem_pack = (size_t)4 * 26 * ((L + 1) | 1) * sizeof(float);   // up to 4 radial levels per block
-  t->smem_fwd = 1024 + FRS * (size_t)RAW_BYTES + FAB * (4 * (size_t)FA_BYTES + 4 * (size_t)t->nfb * FKB * 2) +
-                sizeof(FwdSmem2);
-  // the forward epilogue stages [TM][(L+1)|1] floats and its factor tables
-  // (4 (L+1) doubles, L+1 floats) in the pipeline buffers
-  const size_t fwd_pipe = FRS * (size_t)RAW_BYTES + FAB * (4 * (size_t)FA_BYTES + 4 * (size_t)t->nfb * FKB * 2);
-  const size_t fwd_epi = (((size_t)TM * ((L + 1) | 1) * 4 + 15) & ~(size_t)15) + (size_t)(L + 1) * 36;
-  if (t->smem_bwd > 227 * 1024 || t->smem_fwd > 227 * 1024 || fwd_epi > fwd_pipe) {
+  static_assert(sizeof(FwdWsBars) <= 256, "forward barrier block");
+  t->smem_fwd = 1024 + fwd_ws_layout(t->nfb, L, c.nth).total;
+  if (t->smem_bwd > 227 * 1024 || t->smem_fwd > 227 * 1024) {
     set_error("mixed precision tiles exceed shared memory");
     return CB2_ERR_ARG;
   }
   CB2_CUDA(raise_smem_limit(k_leg_bwd_tma, (int)t->smem_bwd));
   CB2_CUDA(raise_smem_limit(k_pack_bwd, (int)t->smem_pack));
-  CB2_CUDA(raise_smem_limit(k_leg_fwd_tma2, (int)t->smem_fwd));
+  CB2_CUDA(raise_smem_limit(k_leg_fwd_ws, (int)t->smem_fwd));
+  {
+    int dev = 0, nsm = 0;
+    CB2_CUDA(cudaGetDevice(&dev));
+    CB2_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    t->nsm = std::max(1, nsm);
+  }
   return 0;
 }
 
@@ -1210,8 +1322,10 @@ int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots) {
                                                                                        t->rowmax_four);
   const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
-  k_leg_fwd_tma2<<<dim3(tiles0 + tiles1, c.L + 1), NTHR, t->smem_fwd, c.stream>>>(
-      a, rows0, rows1, tiles0, rawP, rawD, t->tm_bfp_hi, t->tm_bfp_lo, t->tm_bfd_hi, t->tm_bfd_lo, t->tmem_fwd);
+  const int ntiles = (tiles0 + tiles1) * (c.L + 1);
+  k_leg_fwd_ws<<<std::min(ntiles, t->nsm), FW_THREADS, t->smem_fwd, c.stream>>>(
+      a, rows0, rows1, tiles0, tiles1, ntiles, rawP, rawD, t->tm_bfp_hi, t->tm_bfp_lo, t->tm_bfd_hi, t->tm_bfd_lo,
+      t->tmem_fwd, t->nacc_fwd);
   return 0;
 }
 
