@@ -563,8 +563,8 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
       if (__any_sync(0xffffffffu, ws_aborted(sb))) break;
       const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
       const int nl = a.L + 1 - q.m;
-      // this thread's row: destination, scale and geometric factor
-      // (sel: 0 g7 at s = 0, 1 g7 at s = 1, 2 g6 at s = 0, 3 g6 at s = 1)
+      // this thread's row: destination, scale and which degree factor
+      // (sel 0: g7, 1: g6; both depend on l and m only, not on s)
       {
         const int rw = q.row0 + er;
         long long off = -1;
@@ -585,7 +585,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             const double ua = 1.0 / (double)fwd_row_scale(a, q, rw), rk = a.r[k];
             cr = (kind == 0) ? ua * rk * rk : (kind == 1) ? ua * rk : ua;
             off = (long long)slot * (long long)a.fs + (long long)k * a.jmax + a.moff[q.m] + s * nl;
-            sel = ((kind == 2) ? 2 : 0) + s;
+            sel = (kind == 2) ? 1 : 0;
           }
         }
         moff[er] = off; mc[er] = cr; mg[er] = sel;
@@ -598,6 +598,19 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
       const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)(ew * 32) << 16);
       const int nch = (nl + 31) / 32, j0 = a.moff[q.m];
       const float *bun0 = a.bunscale + ((size_t)q.g * (a.L + 1) * 2 + q.m * 2) * a.NFmax, *bun1 = bun0 + a.NFmax;
+      // degree factors of chunk c (l = m + 32 c + lane), fetched one chunk ahead
+      auto fetch = [&](int c, double &g7v, double &g6v, float &buv) {
+        const int lm = c * 32 + lane;
+        g7v = 0.0; g6v = 0.0; buv = 0.0f;
+        if (c < nch && lm < nl) {
+          g7v = __ldg(a.g7 + j0 + lm);
+          g6v = __ldg(a.g6 + j0 + lm);
+          buv = (lm & 1) ? __ldg(bun1 + (lm >> 1)) : __ldg(bun0 + (lm >> 1));
+        }
+      };
+      double n7, n6;
+      float nbu;
+      fetch(0, n7, n6, nbu);
       for (int c = 0; c < nch; c++) {
         float v0[16], v1[16];
         tmem_ld16x2(tl + (uint32_t)(c * 16), tl + acc1 + (uint32_t)(c * 16), v0, v1);
@@ -605,28 +618,32 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
           tc_fence_before();
           mbar_arrive(&sb->accempty[ab]);
         }
-        const int lm = c * 32 + lane;
-        double gsel[4] = {0.0, 0.0, 0.0, 0.0};
-        double bu = 0.0;
-        if (lm < nl) {
-          gsel[0] = __ldg(a.g7 + j0 + lm);
-          gsel[2] = __ldg(a.g6 + j0 + lm);
-          if (q.m > 0) { gsel[1] = __ldg(a.g7 + j0 + nl + lm); gsel[3] = __ldg(a.g6 + j0 + nl + lm); }
-          bu = (double)((lm & 1) ? __ldg(bun1 + (lm >> 1)) : __ldg(bun0 + (lm >> 1)));
-        }
+        const double c7 = n7 * (double)nbu, c6 = n6 * (double)nbu;
+        fetch(c + 1, n7, n6, nbu);
 #pragma unroll
         for (int e = 0; e < 16; e++) {
           stg[lane * FW_EPI_PITCH + 2 * e] = v0[e];
           stg[lane * FW_EPI_PITCH + 2 * e + 1] = v1[e];
         }
         __syncwarp();
+        const int lm = c * 32 + lane;
         if (lm < nl) {
-#pragma unroll 4
-          for (int rr = 0; rr < 32; rr++) {
-            const long long o = moff[ew * 32 + rr];
-            const int sl = mg[ew * 32 + rr];
-            const double gv = (sl == 0) ? gsel[0] : (sl == 1) ? gsel[1] : (sl == 2) ? gsel[2] : gsel[3];
-            if (o >= 0) fout[o + lm] = (double)stg[rr * FW_EPI_PITCH + lane] * bu * mc[ew * 32 + rr] * gv;
+          // eight rows at a time: all loads, then all stores
+          for (int r0 = 0; r0 < 32; r0 += 8) {
+            float v[8];
+            long long o[8];
+            double cr[8];
+            int sl[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+              v[u] = stg[(r0 + u) * FW_EPI_PITCH + lane];
+              o[u] = moff[ew * 32 + r0 + u];
+              cr[u] = mc[ew * 32 + r0 + u];
+              sl[u] = mg[ew * 32 + r0 + u];
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+              if (o[u] >= 0) fout[o[u] + lm] = (double)v[u] * cr[u] * (sl[u] ? c6 : c7);
           }
         }
         __syncwarp();
