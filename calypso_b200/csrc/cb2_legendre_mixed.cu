@@ -693,52 +693,77 @@ k_pack_bwd(const __grid_constant__ PackArgs a) {
   const int m = blockIdx.x, k0 = blockIdx.y * a.kc, nk = min(a.kc, a.nr - k0);
   const int nl = a.L + 1 - m, NLP = nl | 1;
   const int RP = 2 * a.ng, RD = 4 * a.nvec, RK = RP + RD;
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < nk * RK * nl; idx += blockDim.x) {
-    const int rl = idx / nl, lm = idx - rl * nl, kq = rl / RK, j = rl - kq * RK, k = k0 + kq;
-    float v = 0.0f;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int jm = a.moff[m];
+  // rows in: one warp per (radial level, row), lanes along l (coalesced
+  // float64 reads, 256 degrees per pass with all loads in flight together),
+  // the row maximum on the way
+  for (int rl = warp; rl < nk * RK; rl += nw) {
+    const int kq = rl / RK, j = rl - kq * RK, k = k0 + kq;
+    const double *src;
+    double rowf;
+    bool vec;
+    int s;
     if (j < RP) {
-      const int fl = j >> 1, s = j & 1;
-      if (!(m == 0 && s == 1)) {
-        const int jj = a.moff[m] + s * (a.L + 1 - m) + lm;
-        double x = __ldg(a.f + (size_t)a.slot[fl] * a.fs + (size_t)k * a.jmax + jj);
-        if (fl < a.nvec) { const double ar = a.ar1[k]; x *= ar * ar * __ldg(a.g3rlm + jj); }
-        v = (float)x;
-      }
+      const int fl = j >> 1;
+      s = j & 1;
+      src = a.f + (size_t)a.slot[fl] * a.fs + (size_t)k * a.jmax + jm + s * nl;
+      vec = fl < a.nvec;
+      const double ar = a.ar1[k];
+      rowf = vec ? ar * ar : 1.0;
     } else {
-      const int jd = j - RP, vv = jd >> 2, qd = jd & 3, comp = qd >> 1, s = qd & 1;
-      if (!(m == 0 && s == 1)) {
-        const int jj = a.moff[m] + s * (a.L + 1 - m) + lm;
-        v = (float)(__ldg(a.f + (size_t)(a.slot[vv] + 1 + comp) * a.fs + (size_t)k * a.jmax + jj) * a.ar1[k]);
+      const int jd = j - RP, vv = jd >> 2, comp = (jd & 3) >> 1;
+      s = jd & 1;
+      src = a.f + (size_t)(a.slot[vv] + 1 + comp) * a.fs + (size_t)k * a.jmax + jm + s * nl;
+      vec = false;
+      rowf = a.ar1[k];
+    }
+    const bool zero = (m == 0 && s == 1);
+    const double *g3 = a.g3rlm + jm + s * nl;
+    float mx = 0.0f;
+    for (int l0 = 0; l0 < nl; l0 += 256) {
+      double x[8], gg[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int lm = l0 + u * 32 + lane;
+        const bool ok = !zero && lm < nl;
+        x[u] = ok ? __ldg(src + lm) : 0.0;
+        gg[u] = (ok && vec) ? __ldg(g3 + lm) : 1.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int lm = l0 + u * 32 + lane;
+        if (lm < nl) {
+          const float v = (float)(vec ? x[u] * (rowf * gg[u]) : x[u] * rowf);
+          T[rl * NLP + lm] = v;
+          mx = fmaxf(mx, fabsf(v));
+        }
       }
     }
-    T[rl * NLP + lm] = v;
-  }
-  __syncthreads();
-  // row maxima: one warp per row
-  const int warp = tid >> 5, lane = tid & 31;
-  for (int rl = warp; rl < nk * RK; rl += blockDim.x >> 5) {
-    float mx = 0.0f;
-    for (int lm = lane; lm < nl; lm += 32) mx = fmaxf(mx, fabsf(T[rl * NLP + lm]));
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if (lane == 0) {
-      const int kq = rl / RK, j = rl - kq * RK, k = k0 + kq;
       if (j < RP) a.maxP[(size_t)m * a.pitchP + k * RP + j] = mx;
       else a.maxD[(size_t)m * a.pitchD + k * RD + (j - RP)] = mx;
     }
   }
-  // rows out, contiguous in (k, row) for each (parity, kk)
+  __syncthreads();
+  // rows out: per (parity, kk) one contiguous run of nk RP (P block) and
+  // nk RD (D block) values; a lane keeps its (level, row) for every kk
+  const int wP = nk * RP, wD = nk * RD;
   for (int par = 0; par < 2; par++) {
     const int cnt = par ? nl / 2 : (nl + 1) / 2;
     const size_t base = a.kbase[m * 2 + par];
-    const int wP = nk * RP, wD = nk * RD;
-    for (int idx = tid; idx < cnt * wP; idx += blockDim.x) {
-      const int kk = idx / wP, rr = idx - kk * wP, kq = rr / RP, j = rr - kq * RP;
-      a.rlmP[(base + kk) * a.pitchP + (size_t)k0 * RP + rr] = T[(kq * RK + j) * NLP + par + 2 * kk];
+    for (int rr = lane; rr < wP; rr += 32) {
+      const int kq = rr / RP, j = rr - kq * RP;
+      const float *tr = T + (kq * RK + j) * NLP + par;
+      float *dst = a.rlmP + base * a.pitchP + (size_t)k0 * RP + rr;
+      for (int kk = warp; kk < cnt; kk += nw) dst[(size_t)kk * a.pitchP] = tr[2 * kk];
     }
-    for (int idx = tid; idx < cnt * wD; idx += blockDim.x) {
-      const int kk = idx / wD, rr = idx - kk * wD, kq = rr / RD, j = rr - kq * RD;
-      a.rlmD[(base + kk) * a.pitchD + (size_t)k0 * RD + rr] = T[(kq * RK + RP + j) * NLP + par + 2 * kk];
+    for (int rr = lane; rr < wD; rr += 32) {
+      const int kq = rr / RD, j = rr - kq * RD;
+      const float *tr = T + (kq * RK + RP + j) * NLP + par;
+      float *dst = a.rlmD + base * a.pitchD + (size_t)k0 * RD + rr;
+      for (int kk = warp; kk < cnt; kk += nw) dst[(size_t)kk * a.pitchD] = tr[2 * kk];
     }
   }
 }
