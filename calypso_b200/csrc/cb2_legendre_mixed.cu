@@ -56,11 +56,7 @@ namespace cb2 {
 
 namespace {
 
-constexpr int TM = 128;          // GEMM rows per CTA (= TMEM lanes)
-
-constexpr int NTHR = 256;          // two threads per GEMM row
-constexpr int ACC1 = 256;        // TMEM column of the parity-1 accumulator
-constexpr uint32_t TMEM_COLS = 512;
+constexpr int TM = 128;          // GEMM rows per tile (= TMEM lanes)
 constexpr unsigned long long kWaitNs = 200ull * 1000 * 1000;   // 200 ms per wait
 
 __device__ inline uint32_t smem_u32(const void *p) {
@@ -206,18 +202,17 @@ __device__ inline unsigned char *smem_base_1024(unsigned char *raw) {
 // ---------------------------------------------------------------------------
 // forward: order-major Fourier rows -> spectra f[slot][k][jj]
 //
-// One CTA = (order m, parity p of l-m, gemm, tile of 128 rows).  For each
-// block of 32 south nodes tb, TMA brings the raw float32 rows of the tile at
-// those 32 colatitudes and at their 32 mirror nodes ([theta][row], 16 KB
-// each); converter threads form the folded, weighted operand
+// A tile = (order m, gemm, 128 rows).  For each block of 32 south nodes tb,
+// TMA brings the raw float32 rows of the tile at those 32 colatitudes and at
+// their 32 mirror nodes ([theta][row], 16 KB each); converter threads form
+// the folded, weighted operands of both parities of l-m
 //   A[row][i] = sg * s_row * (f(i) w_i +- f(i') w_i')     (i' = nth-1-i)
 // split into fp16 hi / lo (64-byte swizzled, K = 32) while TMA brings the
-// B tiles (P_l^m rows of this parity, 64-byte swizzled).  gemm P takes one
+// B tiles (P_l^m rows of each parity, 64-byte swizzled).  gemm P takes one
 // K block per tb; gemm DM two (dP part: element `row`, fold 1-p; mP part:
-// element row - q + 3 - q, fold p).  Three raw stages, three A/B stages, loads
-// two blocks ahead.  One accumulator (N = degrees of this parity).
+// element row - q + 3 - q, fold p).  One accumulator per parity
+// (N = degrees of that parity).
 constexpr int FKB = 32;            // K per block (64-byte rows)
-constexpr int FST = 3;             // stages (raw and A/B)
 constexpr uint32_t RAW_BYTES = 2 * FKB * TM * 4;    // south + north, float32
 constexpr uint32_t FA_BYTES = TM * FKB * 2;         // one of hi / lo
 
@@ -341,7 +336,8 @@ __device__ inline void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-__device__ inline bool ws_aborted(const FwdWsBars *sb) { return *(volatile const int *)&sb->abort != 0; }
+template <typename Bars>
+__device__ inline bool ws_aborted(const Bars *sb) { return *(volatile const int *)&sb->abort != 0; }
 
 __global__ void __launch_bounds__(FW_THREADS, 1)
 k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int tiles_g0, int tiles_g1, int ntiles,
@@ -668,7 +664,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
 //   D block  rlmD[Kbase(m, par) + kk][(k, vector, q')] = X/r, q' = 2 c + s,
 //            c = 0 dS/dr, 1 T,
 // at l = m + par + 2 kk, with the row maxima over all l (for the scales).
-// Step 2, k_leg_bwd_tma: one CTA = (m, gemm, tile of 128 rows).  For each K
+// Step 2, k_leg_bwd_ws: a tile = (m, gemm, 128 rows).  For each K
 // block TMA brings the raw rows [32 K][128 rows] and the B tile
 // [nhp theta][32 K]; converter threads scale, sign and split into fp16 hi/lo
 // (64-byte swizzled); two TMEM accumulators (parity of the basis function)
@@ -779,216 +775,312 @@ struct BwdArgs {
   int *status;
 };
 
-struct BwdSmem {
-  uint64_t full[FST], mmadone[FST], done;
-  uint32_t tmem_base;
-  int mma_any;
-  float rowscale[TM];
-  float bun[256];   // 1 / column scale of this (gemm, m), nhp <= 256
-};
-
 constexpr uint32_t BRAW_BYTES = FKB * TM * 4;   // raw rows of one K block
 
-__global__ void __launch_bounds__(NTHR, 1)
-k_leg_bwd_tma(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int tiles_g0,
-              const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
-              const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo) {
+// ---------------------------------------------------------------------------
+// backward, warp-specialised and persistent: the roles of the forward kernel
+// (converters, epilogue warps, TMA producer, MMA issuer), one CTA per SM over
+// the tiles (m, gemm, 128 rows) in order-major order.  A stage holds one K
+// block: the raw rows [32 K][128 rows], the A tiles (hi, lo) and the B
+// tiles (hi, lo) [nhp theta][32 K].  The parity-p accumulator of a set sits
+// at TMEM column p nhp; two sets (epilogue of one tile overlapping the main
+// loop of the next) when 4 nhp columns fit, else one.
+constexpr int BW_ST = 3;
+
+struct BwdWsBars {
+  uint64_t full[BW_ST], afull[BW_ST], empty[BW_ST];
+  uint64_t accfull[2], accempty[2], fin;
+  uint32_t tmem_base;
+  int abort;
+};
+
+struct BwdTile {
+  int m, g, row0, nrows;
+  int len00, len01, len10, len11, blk00, blk10, nkb0, nkb1, nmin, total, pmore;
+};
+
+// K parts per accumulator p: gemm P one part (parity p); gemm DM the dP part
+// (parity 1-p) then the mP part (parity p)
+__device__ inline BwdTile bwd_tile(const BwdArgs &a, int t, int rows_g0, int rows_g1, int tiles_g0, int tiles_g1) {
+  BwdTile q;
+  const int tpm = tiles_g0 + tiles_g1;
+  q.m = t / tpm;
+  const int x = t - q.m * tpm;
+  q.g = (x >= tiles_g0) ? 1 : 0;
+  q.row0 = (q.g ? x - tiles_g0 : x) * TM;
+  q.nrows = q.g ? rows_g1 : rows_g0;
+  const int nl = a.L + 1 - q.m, cnt0 = (nl + 1) / 2, cnt1 = nl / 2;
+  q.len00 = q.g ? cnt1 : cnt0;
+  q.len01 = q.g ? cnt0 : 0;
+  q.len10 = q.g ? cnt0 : cnt1;
+  q.len11 = q.g ? cnt1 : 0;
+  q.blk00 = (q.len00 + FKB - 1) / FKB;
+  q.blk10 = (q.len10 + FKB - 1) / FKB;
+  q.nkb0 = q.blk00 + (q.len01 + FKB - 1) / FKB;
+  q.nkb1 = q.blk10 + (q.len11 + FKB - 1) / FKB;
+  q.nmin = min(q.nkb0, q.nkb1);
+  q.total = q.nkb0 + q.nkb1;
+  q.pmore = (q.nkb0 >= q.nkb1) ? 0 : 1;
+  return q;
+}
+
+// block b of a tile -> accumulator p, part, block index within the part and
+// the valid K rows of that part (the two accumulators alternate)
+__device__ inline void bwd_blk(const BwdTile &q, int b, int &p, int &part, int &ib, int &len) {
+  int i;
+  if (b < 2 * q.nmin) { p = b & 1; i = b >> 1; } else { p = q.pmore; i = q.nmin + (b - 2 * q.nmin); }
+  const int b0 = p ? q.blk10 : q.blk00;
+  part = (i < b0) ? 0 : 1;
+  ib = part ? i - b0 : i;
+  len = p ? (part ? q.len11 : q.len10) : (part ? q.len01 : q.len00);
+}
+
+// largest |value| of tile row `row` (gemm DM: over the row and its partner)
+__device__ inline float bwd_row_max(const BwdArgs &a, const BwdTile &q, int row) {
+  if (row >= q.nrows) return 0.0f;
+  const int q4 = row & 3;
+  if (q.g == 0) return a.maxP[(size_t)q.m * a.pitchP + row];
+  return fmaxf(a.maxD[(size_t)q.m * a.pitchD + row], a.maxD[(size_t)q.m * a.pitchD + row - q4 + 3 - q4]);
+}
+
+__global__ void __launch_bounds__(FW_THREADS, 1)
+k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int tiles_g0, int tiles_g1, int ntiles,
+             const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
+             const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo,
+             uint32_t tmem_cols, int nacc) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char *base = smem_base_1024(smem_raw);
   const uint32_t B_BYTES = (uint32_t)a.nhp * FKB * 2;       // one of hi / lo
   const uint32_t ST_BYTES = BRAW_BYTES + 2 * FA_BYTES + 2 * B_BYTES;
-  BwdSmem *sh = reinterpret_cast<BwdSmem *>(base + FST * ST_BYTES);
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int r = tid & (TM - 1), h = tid >> 7;
-  const int m = blockIdx.y;
-  const int g = (blockIdx.x < (unsigned)tiles_g0) ? 0 : 1;
-  const int nrows = g ? rows_g1 : rows_g0;
-  const int row0 = (g ? blockIdx.x - tiles_g0 : blockIdx.x) * TM;
-  const int nl = a.L + 1 - m, cnt0 = (nl + 1) / 2, cnt1 = nl / 2;
-  // K parts per accumulator p: gemm P one part (parity p); gemm DM dP part
-  // (parity 1-p) then mP part (parity p)
-  // (scalars, not arrays: a runtime index would put them in local memory)
-  const int len00 = g ? cnt1 : cnt0, len01 = g ? cnt0 : 0;   // accumulator 0, parts 0 / 1
-  const int len10 = g ? cnt0 : cnt1, len11 = g ? cnt1 : 0;   // accumulator 1
-  const int blk00 = (len00 + FKB - 1) / FKB, blk01 = (len01 + FKB - 1) / FKB;
-  const int blk10 = (len10 + FKB - 1) / FKB, blk11 = (len11 + FKB - 1) / FKB;
-  const int nkb0 = blk00 + blk01, nkb1 = blk10 + blk11;
-  const int nmin = min(nkb0, nkb1), total = nkb0 + nkb1;
-  const int pmore = (nkb0 >= nkb1) ? 0 : 1;
-  // block b -> accumulator p, part, block index within the part, valid K rows
-  auto blk = [&](int b, int &p, int &part, int &ib, int &len) {
-    int i;
-    if (b < 2 * nmin) { p = b & 1; i = b >> 1; } else { p = pmore; i = nmin + (b - 2 * nmin); }
-    const int b0 = p ? blk10 : blk00;
-    part = (i < b0) ? 0 : 1;
-    ib = part ? i - b0 : i;
-    len = p ? (part ? len11 : len10) : (part ? len01 : len00);
-  };
-  const CUtensorMap *traw = g ? &tm_rawD : &tm_rawP;
+  BwdWsBars *sb = reinterpret_cast<BwdWsBars *>(base + BW_ST * ST_BYTES);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t accw = tmem_cols / (uint32_t)nacc;         // columns of one accumulator set
+  const uint32_t acc1 = (uint32_t)a.nhp;                    // parity-1 accumulator within a set
 
   if (tid == 0) {
-    for (int q = 0; q < FST; q++) { mbar_init(&sh->full[q], 1); mbar_init(&sh->mmadone[q], 1); }
-    mbar_init(&sh->done, 1);
-    sh->mma_any = 0;
+    for (int q = 0; q < BW_ST; q++) {
+      mbar_init(&sb->full[q], 1); mbar_init(&sb->afull[q], FW_CONV); mbar_init(&sb->empty[q], 1);
+    }
+    for (int q = 0; q < 2; q++) { mbar_init(&sb->accfull[q], 1); mbar_init(&sb->accempty[q], FW_EPI); }
+    mbar_init(&sb->fin, 1);
+    sb->abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh->tmem_base)),
-                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sb->tmem_base)),
+                 "r"(tmem_cols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  const int row = row0 + r, q4 = row & 3;
-  if (h == 0) {
-    float mx = 0.0f;
-    if (row < nrows) {
-      if (g == 0) mx = a.maxP[(size_t)m * a.pitchP + row];
-      else mx = fmaxf(a.maxD[(size_t)m * a.pitchD + row], a.maxD[(size_t)m * a.pitchD + row - q4 + 3 - q4]);
-    }
-    sh->rowscale[r] = pow2_scale(mx);
-  }
-  for (int i = tid; i < a.nhp; i += NTHR) sh->bun[i] = a.bunscale[((size_t)g * (a.L + 1) + m) * a.nhp + i];
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = sh->tmem_base;
+  const uint32_t tmem = sb->tmem_base;
+  const bool skip = (*(volatile int *)a.status & CB2_STATUS_PIPE_TIMEOUT) != 0;
 
-  auto issue = [&](int b) {
-    int p, part, ib, len;
-    blk(b, p, part, ib, len);
-    const int q = b % FST;
-    unsigned char *st = base + q * ST_BYTES;
-    // raw rows: parity of l-m of this part
-    const int par = (g == 0) ? p : (part == 0 ? 1 - p : p);
-    const int ky = a.kbase[m * 2 + par] + ib * FKB;
-    const int gi = g * 2 + p;
-    const int bx = a.ko[(m * 4 + gi) * 2 + part] + ib * FKB;
-    mbar_expect_tx(&sh->full[q], BRAW_BYTES + 2 * B_BYTES);
-    const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
-    tma_load_2d_hint(st, traw, &sh->full[q], row0, ky, pf);
-    tma_load_2d_hint(st + BRAW_BYTES + 2 * FA_BYTES, &tb_hi, &sh->full[q], bx, 0, pl);
-    tma_load_2d_hint(st + BRAW_BYTES + 2 * FA_BYTES + B_BYTES, &tb_lo, &sh->full[q], bx, 0, pl);
-  };
-
-  int n_iss = 0, n_done = 0;   // thread 0 bookkeeping
-  int failed = __syncthreads_or((*(volatile int *)a.status & CB2_STATUS_PIPE_TIMEOUT) != 0);
-  if (tid == 0 && !failed)
-    for (int b = 0; b < min(total, FST - 1); b++) { issue(b); n_iss++; }
-  const float sc = sh->rowscale[r];
-  for (int b = 0; b < total && !failed; b++) {
-    int p, part, ib, len;
-    blk(b, p, part, ib, len);
-    const int s = b % FST;
-    unsigned char *st = base + s * ST_BYTES;
-    int f = 0;
-    if (!mbar_wait(&sh->full[s], (uint32_t)((b / FST) & 1))) f = 1;
-    if (__syncthreads_or(f)) { failed = 1; break; }
-    // convert: thread (r, h) builds K values 16 h .. 16 h + 15 of row r
-    {
-      const float *raw = reinterpret_cast<const float *>(st);
-      int src = r;
-      float sg = sc;
-      if (g) {
-        if (part == 0) sg = (q4 < 2) ? sc : -sc;
-        else { src = r - q4 + 3 - q4; sg = (q4 & 1) ? -sc : sc; }
-      }
-      const int kv = len - ib * FKB;   // valid K entries of this block
-      float x[16];
-#pragma unroll
-      for (int e = 0; e < 16; e++) {
-        const int kk = h * 16 + e;
-        x[e] = (kk < kv) ? raw[kk * TM + src] * sg : 0.0f;
-      }
-      unsigned char *ahi = st + BRAW_BYTES, *alo = ahi + FA_BYTES;
-#pragma unroll
-      for (int c = 0; c < 2; c++) {
-        uint32_t hh[4], ll[4];
-#pragma unroll
-        for (int e = 0; e < 8; e += 2) {
-          const float x0 = x[c * 8 + e], x1 = x[c * 8 + e + 1];
-          const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
-          hh[e >> 1] = pack_half2(h0, h1);
-          ll[e >> 1] = pack_half2(__float2half_rn(x0 - __half2float(h0)), __float2half_rn(x1 - __half2float(h1)));
+  if (skip) {
+    // an earlier launch timed out: do nothing
+  } else if (warp == FW_PROD_WARP) {
+    if (lane == 0) {
+      uint32_t n = 0;
+      bool bad = false;
+      for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x) {
+        if (ws_aborted(sb)) { bad = true; break; }
+        const BwdTile q = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+        const CUtensorMap *traw = q.g ? &tm_rawD : &tm_rawP;
+        for (int b = 0; b < q.total; b++) {
+          int p, part, ib, len;
+          bwd_blk(q, b, p, part, ib, len);
+          const uint32_t s = n % BW_ST;
+          if (n >= BW_ST && !mbar_wait(&sb->empty[s], ((n / BW_ST) - 1) & 1)) { bad = true; break; }
+          unsigned char *st = base + s * ST_BYTES;
+          // raw rows: parity of l-m of this part
+          const int par = (q.g == 0) ? p : (part == 0 ? 1 - p : p);
+          const int ky = a.kbase[q.m * 2 + par] + ib * FKB;
+          const int bx = a.ko[(q.m * 4 + q.g * 2 + p) * 2 + part] + ib * FKB;
+          mbar_expect_tx(&sb->full[s], BRAW_BYTES + 2 * B_BYTES);
+          const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
+          tma_load_2d_hint(st, traw, &sb->full[s], q.row0, ky, pf);
+          tma_load_2d_hint(st + BRAW_BYTES + 2 * FA_BYTES, &tb_hi, &sb->full[s], bx, 0, pl);
+          tma_load_2d_hint(st + BRAW_BYTES + 2 * FA_BYTES + B_BYTES, &tb_lo, &sb->full[s], bx, 0, pl);
+          n++;
         }
-        const uint32_t off = sw64_chunk(r, 2 * h + c);
-        *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
-        *reinterpret_cast<uint4 *>(alo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+      }
+      if (bad) {
+        sb->abort = 1;
+        // every copy still in flight lands before the CTA may exit
+        for (uint32_t q = 0; q < BW_ST && q < n; q++) {
+          const uint32_t last = ((n - 1 - q) / BW_ST) * BW_ST + q;   // last load issued to stage q
+          mbar_wait(&sb->full[q], (last / BW_ST) & 1);
+        }
       }
     }
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      n_done = b + 1;
-      tc_fence_after();
-      unsigned char *ahi = st + BRAW_BYTES, *alo = ahi + FA_BYTES;
-      unsigned char *bh = alo + FA_BYTES, *bl = bh + B_BYTES;
+  } else if (warp == FW_MMA_WARP) {
+    if (lane == 0) {
+      uint32_t n = 0;
+      bool bad = false, any = false;
+      int i = 0;
       const uint32_t idesc = idesc_f16_f32(TM, a.nhp);
-      const uint64_t dah = smem_desc_sw64(ahi), dal = smem_desc_sw64(alo);
-      const uint64_t dbh = smem_desc_sw64(bh), dbl = smem_desc_sw64(bl);
-      const uint32_t acc = tmem + (uint32_t)(p * ACC1);
-      const bool first = (ib == 0) && (part == 0 || (p ? blk10 : blk00) == 0);   // first block of accumulator p
+      for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x, i++) {
+        if (ws_aborted(sb)) { bad = true; break; }
+        const BwdTile q = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+        const int ab = i % nacc;
+        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1)) { bad = true; break; }
+        tc_fence_after();
+        const uint32_t accb = tmem + (uint32_t)ab * accw;
+        for (int b = 0; b < q.total; b++) {
+          int p, part, ib, len;
+          bwd_blk(q, b, p, part, ib, len);
+          const uint32_t s = n % BW_ST, ph = (n / BW_ST) & 1;
+          if (!mbar_wait(&sb->afull[s], ph) || !mbar_wait(&sb->full[s], ph)) { bad = true; break; }
+          tc_fence_after();
+          unsigned char *ahi = base + s * ST_BYTES + BRAW_BYTES, *alo = ahi + FA_BYTES;
+          unsigned char *bh = alo + FA_BYTES, *bl = bh + B_BYTES;
+          const uint64_t dah = smem_desc_sw64(ahi), dal = smem_desc_sw64(alo);
+          const uint64_t dbh = smem_desc_sw64(bh), dbl = smem_desc_sw64(bl);
+          const uint32_t acc = accb + (p ? acc1 : 0u);
+          const bool first = (ib == 0) && (part == 0 || (p ? q.blk10 : q.blk00) == 0);   // first block of p
 #pragma unroll
-      for (int ks = 0; ks < FKB / 16; ks++) {
-        const uint64_t o = (uint64_t)(ks * 2);
-        mma_f16(acc, dah + o, dbh + o, idesc, (first && ks == 0) ? 0u : 1u);
-        mma_f16(acc, dah + o, dbl + o, idesc, 1u);
-        mma_f16(acc, dal + o, dbh + o, idesc, 1u);
+          for (int ks = 0; ks < FKB / 16; ks++) {
+            const uint64_t o = (uint64_t)(ks * 2);
+            mma_f16(acc, dah + o, dbh + o, idesc, (first && ks == 0) ? 0u : 1u);
+            mma_f16(acc, dah + o, dbl + o, idesc, 1u);
+            mma_f16(acc, dal + o, dbh + o, idesc, 1u);
+          }
+          mma_commit(&sb->empty[s]);
+          any = true;
+          n++;
+        }
+        if (bad) break;
+        mma_commit(&sb->accfull[ab]);
       }
-      mma_commit(&sh->mmadone[s]);
-      sh->mma_any = 1;
-      // block b + FST - 1 goes to the stage of block b - 1, free once its MMAs are done
-      const int bn = b + FST - 1;
-      if (bn < total) {
-        if (bn >= FST && !mbar_wait(&sh->mmadone[bn % FST], (uint32_t)(((bn - FST) / FST) & 1))) f = 1;
-        else { issue(bn); n_iss++; }
+      // no MMA may still run when the CTA releases its tensor memory
+      if (any) {
+        mma_commit(&sb->fin);
+        if (!mbar_wait(&sb->fin, 0)) bad = true;
+      }
+      if (bad) sb->abort = 1;
+    }
+  } else if (warp < FW_CONV / 32) {
+    // converters: thread (r, h) builds K values 16 h .. 16 h + 15 of row r
+    const int r = tid & (TM - 1), h = tid >> 7;
+    uint32_t n = 0;
+    bool bad = false;
+    int t = blockIdx.x;
+    float mx_next = 0.0f;
+    if (t < ntiles) {
+      const BwdTile q0 = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+      mx_next = bwd_row_max(a, q0, q0.row0 + r);
+    }
+    for (; t < ntiles && !bad; t += gridDim.x) {
+      if (ws_aborted(sb)) { bad = true; break; }
+      const BwdTile q = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+      const int row = q.row0 + r, q4 = row & 3;
+      const float sc = pow2_scale(mx_next);
+      // the next tile's row maximum is fetched now and used a tile later
+      const int tn = t + gridDim.x;
+      if (tn < ntiles) {
+        const BwdTile qn = bwd_tile(a, tn, rows_g0, rows_g1, tiles_g0, tiles_g1);
+        mx_next = bwd_row_max(a, qn, qn.row0 + r);
+      }
+      for (int b = 0; b < q.total; b++) {
+        int p, part, ib, len;
+        bwd_blk(q, b, p, part, ib, len);
+        const uint32_t s = n % BW_ST;
+        if (!mbar_wait(&sb->full[s], (n / BW_ST) & 1)) { bad = true; break; }
+        unsigned char *st = base + s * ST_BYTES;
+        const float *raw = reinterpret_cast<const float *>(st);
+        int src = r;
+        float sg = sc;
+        if (q.g) {
+          if (part == 0) sg = (q4 < 2) ? sc : -sc;
+          else { src = r - q4 + 3 - q4; sg = (q4 & 1) ? -sc : sc; }
+        }
+        const int kv = len - ib * FKB;   // valid K entries of this block
+        float x[16];
+#pragma unroll
+        for (int e = 0; e < 16; e++) {
+          const int kk = h * 16 + e;
+          x[e] = (kk < kv) ? raw[kk * TM + src] * sg : 0.0f;
+        }
+        unsigned char *ahi = st + BRAW_BYTES, *alo = ahi + FA_BYTES;
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          uint32_t hh[4], ll[4];
+#pragma unroll
+          for (int e = 0; e < 8; e += 2) {
+            const float x0 = x[c * 8 + e], x1 = x[c * 8 + e + 1];
+            const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
+            hh[e >> 1] = pack_half2(h0, h1);
+            ll[e >> 1] = pack_half2(__float2half_rn(x0 - __half2float(h0)), __float2half_rn(x1 - __half2float(h1)));
+          }
+          const uint32_t off = sw64_chunk(r, 2 * h + c);
+          *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+          *reinterpret_cast<uint4 *>(alo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+        }
+        fence_proxy_async();
+        mbar_arrive(&sb->afull[s]);
+        n++;
       }
     }
-    if (__syncthreads_or(f)) { failed = 1; break; }
-  }
-  if (tid == 0) {
-    for (int b = n_done; b < n_iss; b++)
-      if (!mbar_wait(&sh->full[b % FST], (uint32_t)((b / FST) & 1))) failed = 1;
-    if (sh->mma_any) mma_commit(&sh->done);
-  }
-  __syncthreads();
-  int f = failed;
-  if (sh->mma_any && !mbar_wait(&sh->done, 0)) f = 1;
-  f = __syncthreads_or(f);
-  tc_fence_after();
-  if (f && tid == 0) atomicOr(a.status, CB2_STATUS_PIPE_TIMEOUT);
-  if (!f && total > 0) {
-    const bool valid = row < nrows;
-    const float ua = 1.0f / sc;
-    const uint32_t tl = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-    const bool has1 = nkb1 > 0;
-    float *outb = g ? a.out.D : a.out.P;
-    const size_t so = g ? a.out.sD() : a.out.sP();
-    const int half = a.nhp / 2;
-    const int iend = min((h + 1) * half, a.nh);
-    for (int t0 = h * half; t0 < (h + 1) * half; t0 += 16) {
-      float e[16], o[16];
-      if (has1) {
-        tmem_ld16x2(tl + (uint32_t)t0, tl + (uint32_t)(ACC1 + t0), e, o);
-      } else {
-        tmem_ld16(tl + (uint32_t)t0, e);
+    if (bad) sb->abort = 1;
+  } else {
+    // epilogue warps 8-11: TMEM lanes 32 (warp % 4) .. + 31, one row per
+    // thread; south (acc0 + acc1) and north (acc0 - acc1) colatitudes, each
+    // store 32 consecutive rows.  Decisions that guard the warp-collective
+    // TMEM loads are warp-uniform.
+    const int ew = warp - FW_CONV / 32, er = ew * 32 + lane;
+    int i = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
+      if (__any_sync(0xffffffffu, ws_aborted(sb))) break;
+      const BwdTile q = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+      const int row = q.row0 + er;
+      const bool valid = row < q.nrows;
+      const float ua = 1.0f / pow2_scale(bwd_row_max(a, q, row));
+      float *outb = q.g ? a.out.D : a.out.P;
+      const size_t so = q.g ? a.out.sD() : a.out.sP();
+      float *ob = outb + (size_t)q.m * a.nth * so + row;
+      const float *bun = a.bunscale + ((size_t)q.g * (a.L + 1) + q.m) * a.nhp;
+      const bool has1 = q.nkb1 > 0;
+      const int ab = i % nacc;
+      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1);
+      if (!__all_sync(0xffffffffu, ok)) { sb->abort = 1; break; }
+      tc_fence_after();
+      const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)(ew * 32) << 16);
+      const int nch = (a.nh + 15) / 16;
+      for (int c = 0; c < nch; c++) {
+        float e[16], o[16], bu[16];
+        if (has1) {
+          tmem_ld16x2(tl + (uint32_t)(c * 16), tl + acc1 + (uint32_t)(c * 16), e, o);
+        } else {
+          tmem_ld16(tl + (uint32_t)(c * 16), e);
 #pragma unroll
-        for (int q = 0; q < 16; q++) o[q] = 0.0f;
-      }
-      if (!valid) continue;
+          for (int u = 0; u < 16; u++) o[u] = 0.0f;
+        }
+        if (c == nch - 1) {
+          tc_fence_before();
+          mbar_arrive(&sb->accempty[ab]);
+        }
 #pragma unroll
-      for (int q = 0; q < 16; q++) {
-        const int i = t0 + q;
-        if (i < iend) {
-          const float us = ua * sh->bun[i];
-          outb[((size_t)m * a.nth + i) * so + row] = (e[q] + o[q]) * us;
-          outb[((size_t)m * a.nth + (a.nth - 1 - i)) * so + row] = (e[q] - o[q]) * us;
+        for (int u = 0; u < 16; u++) bu[u] = (c * 16 + u < a.nh) ? __ldg(bun + c * 16 + u) : 0.0f;
+        if (valid) {
+#pragma unroll
+          for (int u = 0; u < 16; u++) {
+            const int th = c * 16 + u;
+            if (th < a.nh) {
+              const float us = ua * bu[u];
+              ob[(size_t)th * so] = (e[u] + o[u]) * us;
+              ob[(size_t)(a.nth - 1 - th) * so] = (e[u] - o[u]) * us;
+            }
+          }
         }
       }
     }
   }
   tc_fence_before();
   __syncthreads();
+  if (tid == 0 && sb->abort) atomicOr(a.status, CB2_STATUS_PIPE_TIMEOUT);
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
 }
 
 // ---------------------------------------------------------------------------
@@ -1107,6 +1199,8 @@ struct MixedTables {
   int boxr = 0, nfb = 0;
   uint32_t tmem_fwd = 0;
   int nacc_fwd = 1, nsm = 148;
+  uint32_t tmem_bwd = 0;
+  int nacc_bwd = 1;
 };
 
 using EncodeFn = PFN_cuTensorMapEncodeTiled_v12000;
@@ -1251,8 +1345,12 @@ int mixed_setup(Ctx &c) {
       (rc = make_map64(&t->tm_bfd_hi, t->bfd_hi, 2 * t->nhp, t->rows_all, t->boxr)) ||
       (rc = make_map64(&t->tm_bfd_lo, t->bfd_lo, 2 * t->nhp, t->rows_all, t->boxr)))
     return rc;
-  t->smem_bwd = 1024 + FST * ((size_t)BRAW_BYTES + 2 * (size_t)FA_BYTES + 2 * (size_t)t->nhp * FKB * 2) +
-                sizeof(BwdSmem);
+  t->smem_bwd = 1024 + BW_ST * ((size_t)BRAW_BYTES + 2 * (size_t)FA_BYTES + 2 * (size_t)t->nhp * FKB * 2) +
+                sizeof(BwdWsBars);
+  // backward accumulator set = both parities (2 nhp columns); two sets when they fit
+  t->nacc_bwd = (4 * t->nhp <= 512) ? 2 : 1;
+  t->tmem_bwd = 32;
+  while ((int)t->tmem_bwd < 2 * t->nacc_bwd * t->nhp) t->tmem_bwd *= 2;
   t->smem_pack = (size_t)4 * 26 * ((L + 1) | 1) * sizeof(float);   // up to 4 radial levels per block
   static_assert(sizeof(FwdWsBars) <= 256, "forward barrier block");
   t->smem_fwd = 1024 + fwd_ws_layout(t->nfb, L, c.nth).total;
@@ -1260,7 +1358,7 @@ int mixed_setup(Ctx &c) {
     set_error("mixed precision tiles exceed shared memory");
     return CB2_ERR_ARG;
   }
-  CB2_CUDA(raise_smem_limit(k_leg_bwd_tma, (int)t->smem_bwd));
+  CB2_CUDA(raise_smem_limit(k_leg_bwd_ws, (int)t->smem_bwd));
   CB2_CUDA(raise_smem_limit(k_pack_bwd, (int)t->smem_pack));
   CB2_CUDA(raise_smem_limit(k_leg_fwd_ws, (int)t->smem_fwd));
   {
@@ -1331,8 +1429,9 @@ int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   a.bunscale = t->bb_unscale; a.out = out; a.status = c.d_status;
   const int rows0 = ng * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
-  k_leg_bwd_tma<<<dim3(tiles0 + tiles1, c.L + 1), NTHR, t->smem_bwd, c.stream>>>(a, rows0, rows1, tiles0, rawP, rawD,
-                                                                                t->tm_bb_hi, t->tm_bb_lo);
+  const int ntiles = (tiles0 + tiles1) * (c.L + 1);
+  k_leg_bwd_ws<<<std::min(ntiles, t->nsm), FW_THREADS, t->smem_bwd, c.stream>>>(
+      a, rows0, rows1, tiles0, tiles1, ntiles, rawP, rawD, t->tm_bb_hi, t->tm_bb_lo, t->tmem_bwd, t->nacc_bwd);
   return 0;
 }
 
