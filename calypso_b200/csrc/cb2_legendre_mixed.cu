@@ -145,21 +145,6 @@ __device__ inline void fence_proxy_async() { asm volatile("fence.proxy.async.sha
 __device__ inline void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ inline void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// 16 consecutive fp32 columns of this thread's TMEM lane (load and wait in
-// one statement, so no use of the registers can move above the wait)
-__device__ inline void tmem_ld16(uint32_t taddr, float v[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
-      "tcgen05.wait::ld.sync.aligned;"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr)
-      : "memory");
-#pragma unroll
-  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
-}
-
 // two 16-column loads (columns ta.. and tb..) behind one wait
 __device__ inline void tmem_ld16x2(uint32_t ta, uint32_t tb, float va[16], float vb[16]) {
   uint32_t r[32];
@@ -175,6 +160,20 @@ __device__ inline void tmem_ld16x2(uint32_t ta, uint32_t tb, float va[16], float
       : "memory");
 #pragma unroll
   for (int i = 0; i < 16; i++) { va[i] = __uint_as_float(r[i]); vb[i] = __uint_as_float(r[16 + i]); }
+}
+
+// two 32-column loads (columns ta.. and tb..) behind one wait
+__device__ inline void tmem_ld32x2(uint32_t ta, uint32_t tb, float va[32], float vb[32]) {
+  uint32_t r[64];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%64];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%65];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(ta), "r"(tb)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) { va[i] = __uint_as_float(r[i]); vb[i] = __uint_as_float(r[32 + i]); }
 }
 
 // largest scaled magnitude: 2^13 <= mx s < 2^14 (fp16 holds up to 65504)
@@ -786,6 +785,10 @@ constexpr uint32_t BRAW_BYTES = FKB * TM * 4;   // raw rows of one K block
 // at TMEM column p nhp; two sets (epilogue of one tile overlapping the main
 // loop of the next) when 4 nhp columns fit, else one.
 constexpr int BW_ST = 3;
+// roles: converters warps 0-7, epilogue warps 8-15 (two per TMEM lane
+// quarter, one per half of the colatitude columns), producer 16, MMA 17
+constexpr int BW_CONV = 256, BW_EPI = 256, BW_THREADS = 576;
+constexpr int BW_PROD_WARP = 16, BW_MMA_WARP = 17;
 
 struct BwdWsBars {
   uint64_t full[BW_ST], afull[BW_ST], empty[BW_ST];
@@ -843,7 +846,7 @@ __device__ inline float bwd_row_max(const BwdArgs &a, const BwdTile &q, int row)
   return fmaxf(a.maxD[(size_t)q.m * a.pitchD + row], a.maxD[(size_t)q.m * a.pitchD + row - q4 + 3 - q4]);
 }
 
-__global__ void __launch_bounds__(FW_THREADS, 1)
+__global__ void __launch_bounds__(BW_THREADS, 1)
 k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int tiles_g0, int tiles_g1, int ntiles,
              const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
              const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo,
@@ -853,15 +856,16 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
   const uint32_t B_BYTES = (uint32_t)a.nhp * FKB * 2;       // one of hi / lo
   const uint32_t ST_BYTES = BRAW_BYTES + 2 * FA_BYTES + 2 * B_BYTES;
   BwdWsBars *sb = reinterpret_cast<BwdWsBars *>(base + BW_ST * ST_BYTES);
+  float *buntab = reinterpret_cast<float *>(base + BW_ST * ST_BYTES + 256);   // [8 epilogue warps][nhp]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t accw = tmem_cols / (uint32_t)nacc;         // columns of one accumulator set
   const uint32_t acc1 = (uint32_t)a.nhp;                    // parity-1 accumulator within a set
 
   if (tid == 0) {
     for (int q = 0; q < BW_ST; q++) {
-      mbar_init(&sb->full[q], 1); mbar_init(&sb->afull[q], FW_CONV); mbar_init(&sb->empty[q], 1);
+      mbar_init(&sb->full[q], 1); mbar_init(&sb->afull[q], BW_CONV); mbar_init(&sb->empty[q], 1);
     }
-    for (int q = 0; q < 2; q++) { mbar_init(&sb->accfull[q], 1); mbar_init(&sb->accempty[q], FW_EPI); }
+    for (int q = 0; q < 2; q++) { mbar_init(&sb->accfull[q], 1); mbar_init(&sb->accempty[q], BW_EPI); }
     mbar_init(&sb->fin, 1);
     sb->abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -879,7 +883,7 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
 
   if (skip) {
     // an earlier launch timed out: do nothing
-  } else if (warp == FW_PROD_WARP) {
+  } else if (warp == BW_PROD_WARP) {
     if (lane == 0) {
       uint32_t n = 0;
       bool bad = false;
@@ -914,7 +918,7 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
         }
       }
     }
-  } else if (warp == FW_MMA_WARP) {
+  } else if (warp == BW_MMA_WARP) {
     if (lane == 0) {
       uint32_t n = 0;
       bool bad = false, any = false;
@@ -960,7 +964,7 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
       }
       if (bad) sb->abort = 1;
     }
-  } else if (warp < FW_CONV / 32) {
+  } else if (warp < BW_CONV / 32) {
     // converters: thread (r, h) builds K values 16 h .. 16 h + 15 of row r
     const int r = tid & (TM - 1), h = tid >> 7;
     uint32_t n = 0;
@@ -1024,11 +1028,14 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
     }
     if (bad) sb->abort = 1;
   } else {
-    // epilogue warps 8-11: TMEM lanes 32 (warp % 4) .. + 31, one row per
-    // thread; south (acc0 + acc1) and north (acc0 - acc1) colatitudes, each
-    // store 32 consecutive rows.  Decisions that guard the warp-collective
-    // TMEM loads are warp-uniform.
-    const int ew = warp - FW_CONV / 32, er = ew * 32 + lane;
+    // epilogue warps 8-15: TMEM lanes 32 (warp % 4) .. + 31, one row per
+    // thread, warps 8-11 the first half of the 32-column chunks and 12-15
+    // the rest; south (acc0 + acc1) and north (acc0 - acc1) colatitudes,
+    // each store 32 consecutive rows.  Each warp keeps its own copy of the
+    // tile's column unscale (no barrier between the epilogue warps).
+    // Decisions that guard the warp-collective TMEM loads are warp-uniform.
+    const int ew = warp - BW_CONV / 32, er = (ew & 3) * 32 + lane, hc = ew >> 2;
+    float *bw = buntab + ew * a.nhp;
     int i = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
       if (__any_sync(0xffffffffu, ws_aborted(sb))) break;
@@ -1040,34 +1047,40 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
       const size_t so = q.g ? a.out.sD() : a.out.sP();
       float *ob = outb + (size_t)q.m * a.nth * so + row;
       const float *bun = a.bunscale + ((size_t)q.g * (a.L + 1) + q.m) * a.nhp;
+      __syncwarp();
+      for (int u = lane; u < a.nhp; u += 32) bw[u] = __ldg(bun + u);
+      __syncwarp();
       const bool has1 = q.nkb1 > 0;
       const int ab = i % nacc;
       const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1);
       if (!__all_sync(0xffffffffu, ok)) { sb->abort = 1; break; }
       tc_fence_after();
-      const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)(ew * 32) << 16);
-      const int nch = (a.nh + 15) / 16;
-      for (int c = 0; c < nch; c++) {
-        float e[16], o[16], bu[16];
+      const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)((ew & 3) * 32) << 16);
+      const int nch = (a.nh + 31) / 32, ch = (nch + 1) / 2;
+      const int c0 = hc ? ch : 0, c1 = hc ? nch : ch;
+      if (c0 == c1) {
+        tc_fence_before();
+        mbar_arrive(&sb->accempty[ab]);
+      }
+      for (int c = c0; c < c1; c++) {
+        float e[32], o[32];
         if (has1) {
-          tmem_ld16x2(tl + (uint32_t)(c * 16), tl + acc1 + (uint32_t)(c * 16), e, o);
+          tmem_ld32x2(tl + (uint32_t)(c * 32), tl + acc1 + (uint32_t)(c * 32), e, o);
         } else {
-          tmem_ld16(tl + (uint32_t)(c * 16), e);
+          tmem_ld32x2(tl + (uint32_t)(c * 32), tl + (uint32_t)(c * 32), e, o);
 #pragma unroll
-          for (int u = 0; u < 16; u++) o[u] = 0.0f;
+          for (int u = 0; u < 32; u++) o[u] = 0.0f;
         }
-        if (c == nch - 1) {
+        if (c == c1 - 1) {
           tc_fence_before();
           mbar_arrive(&sb->accempty[ab]);
         }
-#pragma unroll
-        for (int u = 0; u < 16; u++) bu[u] = (c * 16 + u < a.nh) ? __ldg(bun + c * 16 + u) : 0.0f;
         if (valid) {
 #pragma unroll
-          for (int u = 0; u < 16; u++) {
-            const int th = c * 16 + u;
+          for (int u = 0; u < 32; u++) {
+            const int th = c * 32 + u;
             if (th < a.nh) {
-              const float us = ua * bu[u];
+              const float us = ua * bw[th];
               ob[(size_t)th * so] = (e[u] + o[u]) * us;
               ob[(size_t)(a.nth - 1 - th) * so] = (e[u] - o[u]) * us;
             }
@@ -1345,12 +1358,15 @@ int mixed_setup(Ctx &c) {
       (rc = make_map64(&t->tm_bfd_hi, t->bfd_hi, 2 * t->nhp, t->rows_all, t->boxr)) ||
       (rc = make_map64(&t->tm_bfd_lo, t->bfd_lo, 2 * t->nhp, t->rows_all, t->boxr)))
     return rc;
-  t->smem_bwd = 1024 + BW_ST * ((size_t)BRAW_BYTES + 2 * (size_t)FA_BYTES + 2 * (size_t)t->nhp * FKB * 2) +
-                sizeof(BwdWsBars);
-  // backward accumulator set = both parities (2 nhp columns); two sets when they fit
-  t->nacc_bwd = (4 * t->nhp <= 512) ? 2 : 1;
+  static_assert(sizeof(BwdWsBars) <= 256, "backward barrier block");
+  t->smem_bwd = 1024 + BW_ST * ((size_t)BRAW_BYTES + 2 * (size_t)FA_BYTES + 2 * (size_t)t->nhp * FKB * 2) + 256 +
+                (BW_EPI / 32) * (size_t)t->nhp * sizeof(float);
+  // backward accumulator set = both parities (parity 1 at column nhp; the
+  // epilogue reads 32-column chunks); two sets when they fit
+  const int setw = t->nhp + ((t->nhp + 31) / 32) * 32;
+  t->nacc_bwd = (2 * setw <= 512) ? 2 : 1;
   t->tmem_bwd = 32;
-  while ((int)t->tmem_bwd < 2 * t->nacc_bwd * t->nhp) t->tmem_bwd *= 2;
+  while ((int)t->tmem_bwd < t->nacc_bwd * setw) t->tmem_bwd *= 2;
   t->smem_pack = (size_t)4 * 26 * ((L + 1) | 1) * sizeof(float);   // up to 4 radial levels per block
   static_assert(sizeof(FwdWsBars) <= 256, "forward barrier block");
   t->smem_fwd = 1024 + fwd_ws_layout(t->nfb, L, c.nth).total;
@@ -1430,7 +1446,7 @@ int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   const int rows0 = ng * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
   const int ntiles = (tiles0 + tiles1) * (c.L + 1);
-  k_leg_bwd_ws<<<std::min(ntiles, t->nsm), FW_THREADS, t->smem_bwd, c.stream>>>(
+  k_leg_bwd_ws<<<std::min(ntiles, t->nsm), BW_THREADS, t->smem_bwd, c.stream>>>(
       a, rows0, rows1, tiles0, tiles1, ntiles, rawP, rawD, t->tm_bb_hi, t->tm_bb_lo, t->tmem_bwd, t->nacc_bwd);
   return 0;
 }
