@@ -679,6 +679,190 @@ k_fft_products_t(int L, MLayout fin, MLayout fout, const float2 *__restrict__ tw
   }
 }
 
+// ---------------------------------------------------------------------------
+// Four-step products kernel for N = 3 M, M = R1 R2 = L + 1 (the standard
+// nphi = 3 (L + 1) grids).  One CTA per (theta, radial level) as above; 24
+// groups of 16 threads, group (pair p, residue r) owns the M-point transform
+// of the colatitude samples phi_j with j = 3 j' + r:
+//   backward (spectrum -> grid, exponent +): the orders above L vanish, so
+//     z(3 j' + r) = sum_{m < M} e^{2 pi i m j'/M} e^{2 pi i m r/N}
+//                   (Z[m] + e^{4 pi i r/3} Z[N - (M - m)])
+//   forward (grid -> spectrum, exponent -): F_r = M-point DFT of h(3 j' + r),
+//     Z[m] = sum_r e^{-2 pi i m r/N} F_r[m],
+//     Z[N - m] = sum_r e^{+2 pi i m r/N} F_r[(M - m) mod M].
+// The M-point DFT is R1 x R2: n = n1 R2 + n2, k = k1 + R1 k2; a thread holds
+// one n2 column (R1 values, DFT over n1 in registers, twiddle
+// e^{+-2 pi i n2 k1/M}), a transpose through shared memory, then one k1 row
+// (R2 values, DFT over n2).  The Hermitian pair rows are built on the fly
+// from the staged (a_m, b_m) without the 1/2 of z = x + i y: the products
+// are bilinear, so their coefficients carry the 1/4 instead (exact).
+constexpr int F4_THREADS = 384;
+
+template <int R1, int R2>
+struct F4Plan {
+  static constexpr int M = R1 * R2, N = 3 * M;
+  static constexpr int TP = R2 + 1;            // transpose row pitch (complex)
+  static constexpr int TG = R1 * TP;           // transpose block of one group
+  static constexpr int X = (21 * TG > 7 * N) ? 21 * TG : 7 * N;   // work buffer (complex)
+  static constexpr int MP2 = M + 1;            // staging row pitch (complex), slot M stays zero
+  static constexpr int WP = R1 + 1;            // twiddle row pitch (complex)
+  static constexpr int NTW = 3 * M + R2 * WP;  // tables: [3][M] e^{2 pi i m r/N}, [R2][WP] e^{2 pi i n2 k1/M}
+  // staging: max(14 rows x MP2 complex in, 24 rows x (M | 1) floats out)
+  static constexpr int SF = (28 * MP2 > 24 * (M | 1)) ? 28 * MP2 : 24 * (M | 1);
+  static constexpr size_t smem() { return (size_t)SF * 4 + ((size_t)X + NTW) * 8; }
+};
+
+__device__ __forceinline__ float2 cmulc(float2 a, float2 w) {   // a * conj(w)
+  return float2{a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y};
+}
+
+template <int R1, int R2>
+__global__ void __launch_bounds__(F4_THREADS, 2)
+k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, ProdCoef pc) {
+  using P = F4Plan<R1, R2>;
+  constexpr int M = P::M, N = P::N, TP = P::TP, TG = P::TG, MP2 = P::MP2, WP = P::WP, MPO = M | 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float *Sf = reinterpret_cast<float *>(smraw);                    // staging
+  float2 *S2 = reinterpret_cast<float2 *>(smraw);                  // [14][MP2] (a_m, b_m), row 13 zero
+  float2 *X = reinterpret_cast<float2 *>(smraw + (size_t)P::SF * 4);   // transposes / grid rows / F_r
+  float2 *TW3 = X + P::X;                                          // [3][M]
+  float2 *TWM = TW3 + 3 * M;                                       // [R2][WP]
+  const int th = blockIdx.x / fin.nr, k = blockIdx.x % fin.nr;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = F4_THREADS / 32;
+  const int grp = tid >> 4, lt = tid & 15;
+  for (int e = tid; e < P::NTW; e += F4_THREADS) TW3[e] = tables[e];
+  for (int e = tid; e < 14; e += F4_THREADS) S2[e * MP2 + M] = float2{0.0f, 0.0f};
+  for (int e = tid; e < M; e += F4_THREADS) S2[13 * MP2 + e] = float2{0.0f, 0.0f};
+  // input: one warp per order m, lane j < 26 reads element j of the 10 + 16 run
+  {
+    int off = 0;
+    if (lane < 26) { int c, sg; m_comp_of_in(lane, c, sg); off = c * 2 * MP2 + sg; }
+    const float *src = (lane < 10) ? fin.P + (size_t)th * fin.sP() + (size_t)k * 10 + lane
+                                   : fin.D + (size_t)th * fin.sD() + (size_t)k * 16 + (lane - 10);
+    const size_t mst = (size_t)fin.nth * ((lane < 10) ? fin.sP() : fin.sD());
+    if (lane < 26)
+      for (int m = warp; m < M; m += nwarp) Sf[off + 2 * m] = __ldg(src + m * mst);
+  }
+  __syncthreads();
+  const int gp = grp / 3, gr = grp - 3 * gp;   // pair, residue of this group
+  // ---- backward, step 1: column n2 = lt, pair rows built from the staging
+  if (grp < 21 && lt < R2) {
+    const float2 *x0 = S2 + (2 * gp) * MP2, *y0 = S2 + (2 * gp + 1) * MP2;
+    const float2 om = (gr == 0) ? float2{1.0f, 0.0f}
+                    : float2{-0.5f, (gr == 1) ? -0.86602540378443864676f : 0.86602540378443864676f};
+    const float2 *tw = TW3 + gr * M;
+    float2 v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; n1++) {
+      const int m = n1 * R2 + lt, mq = M - m;
+      const float2 a = x0[m], b = y0[m], c = x0[mq], d = y0[mq];
+      float2 zm = float2{a.x + b.y, b.x - a.y};           // 2 Z[m]
+      const float2 zp = float2{c.x - d.y, c.y + d.x};     // 2 Z[N - (M - m)] (zero at m = 0)
+      if (n1 == 0 && lt == 0) zm = float2{2.0f * a.x, 2.0f * b.x};   // 2 Z[0] = 2 (a_0, a'_0)
+      v[n1] = cmulf(cadd(zm, cmulf(om, zp)), tw[m]);
+    }
+    dftr<R1, +1>(v);
+    float2 *T = X + grp * TG;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; k1++) T[k1 * TP + lt] = (k1 == 0) ? v[0] : cmulf(v[k1], TWM[lt * WP + k1]);
+  }
+  __syncthreads();
+  // ---- backward, step 2: row k1 = lt -> grid samples j = 3 (k1 + R1 k2) + r
+  float2 w[R2];
+  if (grp < 21 && lt < R1) {
+    const float2 *T = X + grp * TG + lt * TP;
+#pragma unroll
+    for (int n2 = 0; n2 < R2; n2++) w[n2] = T[n2];
+    dftr<R2, +1>(w);
+  }
+  __syncthreads();
+  if (grp < 21 && lt < R1) {
+    float2 *G = X + gp * N + 3 * lt + gr;
+#pragma unroll
+    for (int k2 = 0; k2 < R2; k2++) G[3 * R1 * k2] = w[k2];
+  }
+  __syncthreads();
+  // ---- products at every grid point (in place: 7 pair rows in, 6 out)
+  {
+    const float cv = 0.25f * (float)pc.cv, cl = 0.25f * (float)pc.cl, ci = 0.25f * (float)pc.ci,
+                ct = 0.25f * (float)pc.ct;
+    for (int q = tid; q < N; q += F4_THREADS) {
+      const float2 p0 = X[0 * N + q], p1 = X[1 * N + q], p2 = X[2 * N + q], p3 = X[3 * N + q];
+      const float2 p4 = X[4 * N + q], p5 = X[5 * N + q], p6 = X[6 * N + q];
+      const float ur = p0.x, ut = p0.y, up = p1.x, wr = p1.y, wt = p2.x, wp = p2.y;
+      const float br = p3.x, bt = p3.y, bp = p4.x, jr = p4.y, jt = p5.x, jp = p5.y, tt = p6.x;
+      X[0 * N + q] = float2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv};
+      X[1 * N + q] = float2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl};
+      X[2 * N + q] = float2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl};
+      X[3 * N + q] = float2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci};
+      X[4 * N + q] = float2{(ur * bt - ut * br) * ci, ur * tt * ct};
+      X[5 * N + q] = float2{ut * tt * ct, up * tt * ct};
+    }
+  }
+  __syncthreads();
+  // ---- forward, step 1: column n2 = lt of the samples j = 3 (n1 R2 + n2) + r
+  float2 v[R1];
+  if (grp < 18 && lt < R2) {
+    const float2 *G = X + gp * N + 3 * lt + gr;
+#pragma unroll
+    for (int n1 = 0; n1 < R1; n1++) v[n1] = G[3 * R2 * n1];
+    dftr<R1, -1>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < R1; k1++) v[k1] = cmulc(v[k1], TWM[lt * WP + k1]);
+  }
+  __syncthreads();
+  if (grp < 18 && lt < R2) {
+    float2 *T = X + grp * TG;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; k1++) T[k1 * TP + lt] = v[k1];
+  }
+  __syncthreads();
+  // ---- forward, step 2: row k1 = lt -> F_r[k1 + R1 k2]
+  if (grp < 18 && lt < R1) {
+    const float2 *T = X + grp * TG + lt * TP;
+#pragma unroll
+    for (int n2 = 0; n2 < R2; n2++) w[n2] = T[n2];
+    dftr<R2, -1>(w);
+  }
+  __syncthreads();
+  if (grp < 18 && lt < R1) {
+    float2 *F = X + grp * M + lt;   // [pair][r][M]: grp = 3 p + r
+#pragma unroll
+    for (int k2 = 0; k2 < R2; k2++) F[R1 * k2] = w[k2];
+  }
+  __syncthreads();
+  // ---- combine the residues: Z[m], Z[N - m] -> (a_m, b_m) of both
+  // components of each pair, into the output staging rows [c * 2 + s][M | 1]
+  {
+    const float an = 1.0f / (float)N;
+    for (int idx = tid; idx < 6 * M; idx += F4_THREADS) {
+      const int p = idx / M, m = idx - p * M, mm = (M - m) & (M - 1);
+      const float2 *F = X + p * 3 * M;
+      const float2 t1 = TW3[M + m], t2 = TW3[2 * M + m];
+      const float2 zk = cadd(F[m], cadd(cmulc(F[M + m], t1), cmulc(F[2 * M + m], t2)));
+      const float2 zn = cadd(F[mm], cadd(cmulf(F[M + mm], t1), cmulf(F[2 * M + mm], t2)));
+      float *o0 = Sf + (2 * p) * 2 * MPO, *o1 = Sf + (2 * p + 1) * 2 * MPO;
+      if (m == 0) {
+        o0[0] = an * zk.x; o0[MPO] = 0.0f; o1[0] = an * zk.y; o1[MPO] = 0.0f;
+      } else {
+        o0[m] = an * (zk.x + zn.x); o0[MPO + m] = -an * (zk.y - zn.y);
+        o1[m] = an * (zk.y + zn.y); o1[MPO + m] = an * (zk.x - zn.x);
+      }
+    }
+  }
+  __syncthreads();
+  // output: one warp per m, lane j < 24 writes element j of the 8 + 16 run
+  {
+    int cs = 0;
+    if (lane < 24) { int c, sg; m_comp_of_out(lane, c, sg); cs = c * 2 + sg; }
+    float *dst = (lane < 8) ? fout.P + (size_t)th * fout.sP() + (size_t)k * 8 + lane
+                            : fout.D + (size_t)th * fout.sD() + (size_t)k * 16 + (lane - 8);
+    const size_t mst = (size_t)fout.nth * ((lane < 8) ? fout.sP() : fout.sD());
+    if (lane < 24)
+      for (int m = warp; m < M; m += nwarp) dst[m * mst] = Sf[cs * MPO + m];
+  }
+}
+
 // order-major Fourier rows -> grid (float64), for the standalone transform API
 __global__ void __launch_bounds__(256)
 k_fft_to_grid_m(FFTPlan pl, int L, MLayout fin, double *grid, const float2 *tw) {
@@ -794,6 +978,29 @@ static int attr_fft_t(Ctx &c) {
   return 0;
 }
 
+// smem attribute and the tables of the four-step kernel:
+// [3][M] e^{2 pi i m r/N} (row 0 ones), [R2][R1 + 1] e^{2 pi i n2 k1/M}
+template <int R1, int R2>
+static int attr_fft_4s(Ctx &c) {
+  using P = F4Plan<R1, R2>;
+  CB2_CUDA(raise_smem_limit(k_fft_products_4s<R1, R2>, (int)P::smem()));
+  std::vector<float2> t(P::NTW, float2{0.0f, 0.0f});
+  const double pi = 3.14159265358979323846;
+  for (int r = 0; r < 3; r++)
+    for (int m = 0; m < P::M; m++) {
+      const double ang = 2.0 * pi * (double)(m * r) / (double)P::N;
+      t[r * P::M + m] = float2{(float)std::cos(ang), (float)std::sin(ang)};
+    }
+  for (int n2 = 0; n2 < R2; n2++)
+    for (int k1 = 0; k1 < R1; k1++) {
+      const double ang = 2.0 * pi * (double)(n2 * k1) / (double)P::M;
+      t[3 * P::M + n2 * P::WP + k1] = float2{(float)std::cos(ang), (float)std::sin(ang)};
+    }
+  CB2_CUDA(cudaMalloc(&c.d_twf4, t.size() * sizeof(float2)));
+  CB2_CUDA(cudaMemcpy(c.d_twf4, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  return 0;
+}
+
 int fft_setup(Ctx &c) {
   FFTPlan p = make_plan(c.nph);
   if (p.nst < 0) {
@@ -823,6 +1030,16 @@ int fft_setup(Ctx &c) {
       default: break;
     }
     if (rc) return rc;
+    if (c.nph == 3 * (c.L + 1)) {
+      switch (c.nph) {
+        case 768: rc = attr_fft_4s<16, 16>(c); break;
+        case 384: rc = attr_fft_4s<16, 8>(c); break;
+        case 192: rc = attr_fft_4s<8, 8>(c); break;
+        case 96: rc = attr_fft_4s<8, 4>(c); break;
+        default: break;
+      }
+      if (rc) return rc;
+    }
   }
   if (26 * (size_t)(c.L + 1) * sizeof(float) > 7 * (size_t)c.nph * sizeof(float2)) {
     set_error("ngrid_zonal_ctl too small for the staging of the fused FFT kernel");
@@ -874,8 +1091,24 @@ static void launch_fft_t(Ctx &c, const MLayout &in, const MLayout &out, const Pr
                                                                           pc);
 }
 
+template <int R1, int R2>
+static void launch_fft_4s(Ctx &c, const MLayout &in, const MLayout &out, const ProdCoef &pc) {
+  k_fft_products_4s<R1, R2><<<(unsigned)(c.nth * c.nr), F4_THREADS, F4Plan<R1, R2>::smem(), c.stream>>>(
+      in, out, (const float2 *)c.d_twf4, pc);
+}
+
 void fft_products_m(Ctx &c, const MLayout &in, const MLayout &out) {
   ProdCoef pc{c.p.coef_velo, c.p.coef_lor, c.p.coef_induct, c.p.coef_temp};
+  // tuning value F4_THREADS selects the four-step kernel where it applies
+  if (c.d_twf4 && c.tune[TUNE_FFT_THREADS] == F4_THREADS) {
+    switch (c.nph) {
+      case 768: launch_fft_4s<16, 16>(c, in, out, pc); return;
+      case 384: launch_fft_4s<16, 8>(c, in, out, pc); return;
+      case 192: launch_fft_4s<8, 8>(c, in, out, pc); return;
+      case 96: launch_fft_4s<8, 4>(c, in, out, pc); return;
+      default: break;
+    }
+  }
   switch (c.nph) {
     case 768: launch_fft_t<768>(c, in, out, pc); return;
     case 384: launch_fft_t<384>(c, in, out, pc); return;

@@ -87,6 +87,7 @@ struct Ctx {
   double *d_tw_fft = nullptr;            // exp(-2 pi i e / nph), e = 0..nph-1
   float *d_tw_fft32 = nullptr;
   void *d_twp32 = nullptr;               // per-stage float2 twiddles of the compile-time FFT plans
+  void *d_twf4 = nullptr;                // tables of the four-step products kernel (nphi = 3 (L + 1))
   // state
   double *d_f = nullptr;                 // NSLOT * nr * jmax
   void *d_four = nullptr;                // F: nth*nr*13*NS (double or float)
@@ -108,7 +109,7 @@ struct Ctx {
   cudaGraphExec_t graph_exec = nullptr;
   int graph_nsteps = 0;
   // kernel variants chosen by the autotuner (cb2_autotune); defaults until tuned
-  int tune[8] = {4, 2, 2, 512, 0, 0, 0, 0};
+  int tune[8] = {4, 2, 2, 384, 0, 0, 0, 0};
 
   size_t fsize() const { return (size_t)nr * jmax; }
   double *fld(int slot) { return d_f + (size_t)slot * fsize(); }
@@ -208,7 +209,8 @@ enum Tune {
   TUNE_BWD_KT = 0,       // float64 backward Legendre: radial levels per block (2, 4)
   TUNE_FWD_KT = 1,       // float64 forward Legendre: radial levels per block (1, 2, 4)
   TUNE_PACK_KC = 2,      // mixed backward pack: radial levels per block (1, 2, 4)
-  TUNE_FFT_THREADS = 3,  // mixed FFT + products: threads per row block (128, 256, 512)
+  TUNE_FFT_THREADS = 3,  // mixed FFT + products: threads per row block; 384 = the four-step kernel
+                         // (nphi = 3 (L + 1)), 128 / 256 / 512 = the Stockham kernel
   TUNE_N = 4
 };
 // one time step (explicit, implicit, nonlinear); advances istep (cb2_api.cu)

@@ -81,7 +81,7 @@ int autotune(Ctx &c) {
     items.push_back({TUNE_FWD_KT, {1, 2}, stage_fwd_f64});
   } else {
     items.push_back({TUNE_PACK_KC, {1, 2, 4}, stage_bwd_mixed});
-    items.push_back({TUNE_FFT_THREADS, {128, 256, 512}, stage_fft_mixed});
+    items.push_back({TUNE_FFT_THREADS, {384, 512, 256, 128}, stage_fft_mixed});
   }
   for (const Item &it : items) {
     int best = c.tune[it.which];

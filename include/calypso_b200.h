@@ -165,7 +165,9 @@ int cb2_free_pinned(void *p);
  * candidate tile / launch shape of the transform kernels on this context
  * and keeps the fastest.  Only before cb2_init_fields / cb2_start (it
  * overwrites the work fields).  tuning[4]: float64 backward radial tile,
- * float64 forward radial tile, mixed pack radial tile, mixed FFT threads. */
+ * float64 forward radial tile, mixed pack radial tile, mixed FFT threads
+ * (384: the four-step kernel, used where nphi = 3 (ltr + 1); 128, 256, 512:
+ * the Stockham kernel). */
 int cb2_autotune(cb2_ctx *ctx);
 int cb2_get_tuning(const cb2_ctx *ctx, int tuning[4]);
 int cb2_set_tuning(cb2_ctx *ctx, const int tuning[4]);

@@ -12,7 +12,7 @@ from calypso_b200.sph_mhd import MAGNE, TEMP, VELO
 
 pytestmark = pytest.mark.gpu
 
-CANDIDATES = [(2, 4), (1, 2), (1, 2, 4), (128, 256, 512)]
+CANDIDATES = [(2, 4), (1, 2), (1, 2, 4), (384, 512, 256, 128)]
 
 
 def small_ensemble():
@@ -90,3 +90,22 @@ def test_small_shell_created_after_large_one_leaves_it_working():
         assert np.all(np.isfinite(a.energies())) and np.all(np.isfinite(b.energies()))
         a.close()
         b.close()
+
+
+def test_four_step_and_stockham_fft_agree():
+    # tuning value 384 runs the four-step products kernel (nphi = 3 (L + 1)),
+    # 512 the Stockham kernel: the same float32 transform up to rounding
+    p = configs.small_shell()
+    assert p["nph"] == 3 * (p["ltr"] + 1)
+    out = []
+    for nt in (384, 512):
+        g = SphMHD(p, PREC_MIXED, device=0)
+        t = g.tuning
+        t[3] = nt
+        g.tuning = t
+        g.init_fields(2, 5)
+        g.step(6)
+        out.append(np.stack([g.get_field(s) for s in (VELO, MAGNE, TEMP)]))
+        g.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b)
