@@ -292,40 +292,83 @@ int rj_lu_factorise(Ctx &c) {
 // column access x(k) = base[(k-1)*stride], 1-based k
 #define XC(i) x[(size_t)((i) - 1) * stride]
 
-__device__ static void d_lubksb_3band(int n, const double *lu, const int *piv, double *x,
-                                      size_t stride) {
+// Banded back substitutions of one column (lubksb_3band / lubksb_5band,
+// SOLVER_src/direct_solver/lubksb_357band.f90:69-140, over the pivoted LU of
+// m_ludcmp_3band.f90 / m_ludcmp_band.f90): row interchanges, L y = P b, then
+// U x = y, with the recurrence carried in registers -- each value of the
+// column is read once per sweep (the read of the next row issued before the
+// store of this one) and the band factors come through the read-only path.
+__device__ static void d_pivots(int n, const int *piv, double *x, size_t stride) {
   for (int i = 1; i <= n; i++) {
-    int ll = piv[i - 1];
-    double s = XC(ll); XC(ll) = XC(i); XC(i) = s;
+    const int ll = __ldg(piv + i - 1);
+    if (ll != i) { const double s = XC(ll); XC(ll) = XC(i); XC(i) = s; }
   }
-  XC(2) = XC(2) - M5(lu, 4, 1) * XC(1);
-  for (int i = 3; i <= n; i++) XC(i) = XC(i) - M5(lu, 5, i - 2) * XC(i - 2) - M5(lu, 4, i - 1) * XC(i - 1);
-  XC(n) = XC(n) / M5(lu, 3, n);
-  XC(n - 1) = (XC(n - 1) - M5(lu, 2, n) * XC(n)) / M5(lu, 3, n - 1);
-  for (int i = n - 2; i >= 1; i--)
-    XC(i) = (XC(i) - M5(lu, 2, i + 1) * XC(i + 1) - M5(lu, 1, i + 2) * XC(i + 2)) / M5(lu, 3, i);
 }
 
-__device__ static void d_lubksb_5band(int n, const double *lu, const int *piv, double *x,
-                                      size_t stride) {
-  for (int i = 1; i <= n; i++) {
-    int ll = piv[i - 1];
-    double s = XC(ll); XC(ll) = XC(i); XC(i) = s;
+__device__ static void d_solve_3band(int n, const double *lu, const int *piv, double *x, size_t stride) {
+  d_pivots(n, piv, x, stride);
+  // forward: L y = P b
+  double ym2 = XC(1), ym1 = XC(2) - __ldg(&M5(lu, 4, 1)) * ym2;
+  XC(2) = ym1;
+  double nx = XC(3);
+  for (int i = 3; i <= n; i++) {
+    const double b = nx;
+    if (i < n) nx = XC(i + 1);
+    const double y = b - __ldg(&M5(lu, 5, i - 2)) * ym2 - __ldg(&M5(lu, 4, i - 1)) * ym1;
+    XC(i) = y;
+    ym2 = ym1; ym1 = y;
   }
-  XC(2) = XC(2) - M9(lu, 6, 1) * XC(1);
-  XC(3) = XC(3) - M9(lu, 7, 1) * XC(1) - M9(lu, 6, 2) * XC(2);
-  XC(4) = XC(4) - M9(lu, 8, 1) * XC(1) - M9(lu, 7, 2) * XC(2) - M9(lu, 6, 3) * XC(3);
-  for (int i = 5; i <= n; i++)
-    XC(i) = XC(i) - M9(lu, 9, i - 4) * XC(i - 4) - M9(lu, 8, i - 3) * XC(i - 3)
-          - M9(lu, 7, i - 2) * XC(i - 2) - M9(lu, 6, i - 1) * XC(i - 1);
-  XC(n) = XC(n) / M9(lu, 5, n);
-  XC(n - 1) = (XC(n - 1) - M9(lu, 4, n) * XC(n)) / M9(lu, 5, n - 1);
-  XC(n - 2) = (XC(n - 2) - M9(lu, 4, n - 1) * XC(n - 1) - M9(lu, 3, n) * XC(n)) / M9(lu, 5, n - 2);
-  XC(n - 3) = (XC(n - 3) - M9(lu, 4, n - 2) * XC(n - 2) - M9(lu, 3, n - 1) * XC(n - 1)
-               - M9(lu, 2, n) * XC(n)) / M9(lu, 5, n - 3);
-  for (int i = n - 4; i >= 1; i--)
-    XC(i) = (XC(i) - M9(lu, 4, i + 1) * XC(i + 1) - M9(lu, 3, i + 2) * XC(i + 2)
-             - M9(lu, 2, i + 3) * XC(i + 3) - M9(lu, 1, i + 4) * XC(i + 4)) / M9(lu, 5, i);
+  // backward: U x = y
+  double xp2 = ym1 / __ldg(&M5(lu, 3, n));
+  const double yn1 = XC(n - 1);
+  XC(n) = xp2;
+  double xp1 = (yn1 - __ldg(&M5(lu, 2, n)) * xp2) / __ldg(&M5(lu, 3, n - 1));
+  nx = XC(n - 2);
+  XC(n - 1) = xp1;
+  for (int i = n - 2; i >= 1; i--) {
+    const double b = nx;
+    if (i > 1) nx = XC(i - 1);
+    const double v = (b - __ldg(&M5(lu, 2, i + 1)) * xp1 - __ldg(&M5(lu, 1, i + 2)) * xp2) / __ldg(&M5(lu, 3, i));
+    XC(i) = v;
+    xp2 = xp1; xp1 = v;
+  }
+}
+
+__device__ static void d_solve_5band(int n, const double *lu, const int *piv, double *x, size_t stride) {
+  d_pivots(n, piv, x, stride);
+  // forward: L y = P b
+  double y1 = XC(1);
+  double y2 = XC(2) - __ldg(&M9(lu, 6, 1)) * y1;
+  double y3 = XC(3) - __ldg(&M9(lu, 7, 1)) * y1 - __ldg(&M9(lu, 6, 2)) * y2;
+  double y4 = XC(4) - __ldg(&M9(lu, 8, 1)) * y1 - __ldg(&M9(lu, 7, 2)) * y2 - __ldg(&M9(lu, 6, 3)) * y3;
+  XC(2) = y2; XC(3) = y3; XC(4) = y4;
+  double nx = XC(5);
+  for (int i = 5; i <= n; i++) {
+    const double b = nx;
+    if (i < n) nx = XC(i + 1);
+    const double y = b - __ldg(&M9(lu, 9, i - 4)) * y1 - __ldg(&M9(lu, 8, i - 3)) * y2
+                   - __ldg(&M9(lu, 7, i - 2)) * y3 - __ldg(&M9(lu, 6, i - 1)) * y4;
+    XC(i) = y;
+    y1 = y2; y2 = y3; y3 = y4; y4 = y;
+  }
+  // backward: U x = y (y4 = y(n))
+  const double b1 = XC(n - 1), b2 = XC(n - 2), b3 = XC(n - 3);
+  const double x0 = y4 / __ldg(&M9(lu, 5, n));
+  const double xm1 = (b1 - __ldg(&M9(lu, 4, n)) * x0) / __ldg(&M9(lu, 5, n - 1));
+  const double xm2 = (b2 - __ldg(&M9(lu, 4, n - 1)) * xm1 - __ldg(&M9(lu, 3, n)) * x0) / __ldg(&M9(lu, 5, n - 2));
+  const double xm3 = (b3 - __ldg(&M9(lu, 4, n - 2)) * xm2 - __ldg(&M9(lu, 3, n - 1)) * xm1
+                      - __ldg(&M9(lu, 2, n)) * x0) / __ldg(&M9(lu, 5, n - 3));
+  XC(n) = x0; XC(n - 1) = xm1; XC(n - 2) = xm2; XC(n - 3) = xm3;
+  double p1 = xm3, p2 = xm2, p3 = xm1, p4 = x0;   // x(i+1) .. x(i+4)
+  nx = XC(n - 4);
+  for (int i = n - 4; i >= 1; i--) {
+    const double b = nx;
+    if (i > 1) nx = XC(i - 1);
+    const double v = (b - __ldg(&M9(lu, 4, i + 1)) * p1 - __ldg(&M9(lu, 3, i + 2)) * p2
+                      - __ldg(&M9(lu, 2, i + 3)) * p3 - __ldg(&M9(lu, 1, i + 4)) * p4) / __ldg(&M9(lu, 5, i));
+    XC(i) = v;
+    p4 = p3; p3 = p2; p2 = p1; p1 = v;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -376,43 +419,51 @@ __global__ void k_explicit(RJArgs a, Fields F, int euler) {
 __device__ inline double icb_fld(const RJArgs &a, int jj) { return jj == 0 ? a.temp_icb_fld : 0.0; }
 __device__ inline double cmb_fld(const RJArgs &a, int jj) { return jj == 0 ? a.temp_cmb_fld : 0.0; }
 
-// Crank-Nicolson solves: one thread per (l, m) column
+// Crank-Nicolson solves: one thread per (field, (l, m) column); the five
+// solves of a column are independent (blockIdx.y picks the field)
 __global__ void k_implicit(RJArgs a, Fields F, const double *lu_vp, const int *pv_vp,
                            const double *lu_vt, const int *pv_vt, const double *lu_bs,
                            const int *pv_bs, const double *lu_bt, const int *pv_bt,
                            const double *lu_t, const int *pv_t) {
-  int jj = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x;
   if (jj >= a.jmax) return;
-  int n = a.nr, l = a.jl[jj];
-  size_t st = a.jmax;
-  double *uS = F(VELO) + jj, *udS = F(VELO + 1) + jj, *uT = F(VELO + 2) + jj;
-  const double *wS = F(VORT) + jj, *wT = F(VORT + 2) + jj;
-  // velocity from vorticity: S <- tor(w), T <- pol(w); l = 0 removed; walls zero
-  for (int k = 0; k < n; k++) {
-    bool wall = (k <= a.kin || k == a.kout);
-    double s = wT[k * st], t = wS[k * st];
-    if (jj == 0 || wall) { s = 0.0; t = 0.0; }
-    uS[k * st] = s;
-    uT[k * st] = t;
-    if (wall) udS[k * st] = 0.0;
+  const int n = a.nr, l = a.jl[jj], fld = blockIdx.y;
+  const size_t st = a.jmax;
+  if (fld < 2) {
+    // velocity from vorticity: S <- tor(w), T <- pol(w); l = 0 removed; walls zero
+    double *u = F(VELO + 2 * fld) + jj, *udS = F(VELO + 1) + jj;
+    const double *w = F(VORT + 2 - 2 * fld) + jj;
+    for (int k = 0; k < n; k++) {
+      const bool wall = (k <= a.kin || k == a.kout);
+      const double v = (jj == 0 || wall) ? 0.0 : w[k * st];
+      u[k * st] = v;
+      if (fld == 0 && wall) udS[k * st] = 0.0;
+    }
+    if (fld == 0) d_solve_5band(n, lu_vp + (size_t)l * 9 * n, pv_vp + (size_t)l * n, u, st);
+    else d_solve_3band(n, lu_vt + (size_t)l * 5 * n, pv_vt + (size_t)l * n, u, st);
+  } else if (fld == 2) {
+    // temperature with fixed wall values
+    double *T = F(TEMP) + jj;
+    for (int k = a.kout; k < n; k++) T[k * st] = cmb_fld(a, jj);
+    for (int k = 0; k <= a.kin; k++) T[k * st] = icb_fld(a, jj);
+    d_solve_3band(n, lu_t + (size_t)l * 5 * n, pv_t + (size_t)l * n, T, st);
+  } else if (fld == 3) {
+    // poloidal magnetic field, insulating walls, l = 0 removed
+    double *bS = F(MAGNE) + jj, *bdS = F(MAGNE + 1) + jj;
+    if (jj == 0)
+      for (int k = 0; k < n; k++) bS[k * st] = 0.0;
+    bdS[a.kin * st] = (a.gl[jj] + 1.0) * a.bc.r_icb[1] * bS[a.kin * st];
+    bdS[a.kout * st] = -a.gl[jj] * a.bc.r_cmb[1] * bS[a.kout * st];
+    d_solve_3band(n, lu_bs + (size_t)l * 5 * n, pv_bs + (size_t)l * n, bS, st);
+  } else {
+    // toroidal magnetic field, zero at the walls
+    double *bT = F(MAGNE + 2) + jj;
+    if (jj == 0)
+      for (int k = 0; k < n; k++) bT[k * st] = 0.0;
+    bT[a.kin * st] = 0.0;
+    bT[a.kout * st] = 0.0;
+    d_solve_3band(n, lu_bt + (size_t)l * 5 * n, pv_bt + (size_t)l * n, bT, st);
   }
-  d_lubksb_5band(n, lu_vp + (size_t)l * 9 * n, pv_vp + (size_t)l * n, uS, st);
-  d_lubksb_3band(n, lu_vt + (size_t)l * 5 * n, pv_vt + (size_t)l * n, uT, st);
-  // temperature with fixed wall values
-  double *T = F(TEMP) + jj;
-  for (int k = a.kout; k < n; k++) T[k * st] = cmb_fld(a, jj);
-  for (int k = 0; k <= a.kin; k++) T[k * st] = icb_fld(a, jj);
-  d_lubksb_3band(n, lu_t + (size_t)l * 5 * n, pv_t + (size_t)l * n, T, st);
-  // magnetic field, insulating walls, l = 0 removed
-  double *bS = F(MAGNE) + jj, *bdS = F(MAGNE + 1) + jj, *bT = F(MAGNE + 2) + jj;
-  if (jj == 0)
-    for (int k = 0; k < n; k++) { bS[k * st] = 0.0; bT[k * st] = 0.0; }
-  bdS[a.kin * st] = (a.gl[jj] + 1.0) * a.bc.r_icb[1] * bS[a.kin * st];
-  bT[a.kin * st] = 0.0;
-  bdS[a.kout * st] = -a.gl[jj] * a.bc.r_cmb[1] * bS[a.kout * st];
-  bT[a.kout * st] = 0.0;
-  d_lubksb_3band(n, lu_bs + (size_t)l * 5 * n, pv_bs + (size_t)l * n, bS, st);
-  d_lubksb_3band(n, lu_bt + (size_t)l * 5 * n, pv_bt + (size_t)l * n, bT, st);
 }
 
 __device__ inline double D1(const RJArgs &a, const double *f, int k, int jj) {
@@ -725,7 +776,7 @@ void rj_explicit(Ctx &c, bool euler) {
 
 void rj_implicit(Ctx &c) {
   RJArgs a = c.rj_args();
-  k_implicit<<<cdiv(c.jmax, 128), 128, 0, c.stream>>>(a, fields(c), c.d_lu_vp, c.d_pv_vp, c.d_lu_vt,
+  k_implicit<<<dim3(cdiv(c.jmax, 128), 5), 128, 0, c.stream>>>(a, fields(c), c.d_lu_vp, c.d_pv_vp, c.d_lu_vt,
                                                       c.d_pv_vt, c.d_lu_bs, c.d_pv_bs, c.d_lu_bt,
                                                       c.d_pv_bt, c.d_lu_t, c.d_pv_t);
   size_t n = c.fsize();
