@@ -293,7 +293,7 @@ int rj_lu_factorise(Ctx &c) {
 #define XC(i) x[(size_t)((i) - 1) * stride]
 
 // Banded back substitutions of one column (lubksb_3band / lubksb_5band,
-// SOLVER_src/direct_solver/lubksb_357band.f90:69-140, over the pivoted LU of
+// SOLVER_src/direct_solver/lubksb_357band.f90:69-148, over the pivoted LU of
 // m_ludcmp_3band.f90 / m_ludcmp_band.f90): row interchanges, L y = P b, then
 // U x = y, with the recurrence carried in registers -- each value of the
 // column is read once per sweep (the read of the next row issued before the
