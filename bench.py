@@ -250,8 +250,16 @@ def main():
     top = max(traffic, key=lambda k: stages[k])
     t_s = stages[top] * 1e-3
     achieved = traffic[top] / t_s / 1e9
+    # DRAM bytes (read + write) of the dominant kernel from one ncu capture of
+    # the same kernel at L255 / Nr33 (614.6 MB per launch), scaled by the
+    # (theta, k) rows processed; other shapes have no capture
+    dram_per_row = {("fft_products", 255, 384, 768): 614_629_376 / (384 * 33)}
+    dkey = (top, L, nth, nph)
+    measured = dram_per_row[dkey] * nth * nr if (prec == PREC_MIXED and dkey in dram_per_row) else None
     roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+            "frac": achieved / peaks["hbm_gbs"], "traffic": measured,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at Nr33, scaled by rows"
+                              if measured else None,
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                            else "fallback 6650 GB/s",
             "algorithmic_bytes_per_launch": traffic[top],
