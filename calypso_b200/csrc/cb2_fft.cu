@@ -733,7 +733,8 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
   for (int e = tid; e < P::NTW; e += F4_THREADS) TW3[e] = tables[e];
   for (int e = tid; e < 14; e += F4_THREADS) S2[e * MP2 + M] = float2{0.0f, 0.0f};
   for (int e = tid; e < M; e += F4_THREADS) S2[13 * MP2 + e] = float2{0.0f, 0.0f};
-  // input: one warp per order m, lane j < 26 reads element j of the 10 + 16 run
+  // input: one warp per order m, lane j < 26 copies element j of the 10 + 16
+  // run; asynchronous copies, so every load of the CTA is in flight at once
   {
     int off = 0;
     if (lane < 26) { int c, sg; m_comp_of_in(lane, c, sg); off = c * 2 * MP2 + sg; }
@@ -741,7 +742,11 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
                                    : fin.D + (size_t)th * fin.sD() + (size_t)k * 16 + (lane - 10);
     const size_t mst = (size_t)fin.nth * ((lane < 10) ? fin.sP() : fin.sD());
     if (lane < 26)
-      for (int m = warp; m < M; m += nwarp) Sf[off + 2 * m] = __ldg(src + m * mst);
+      for (int m = warp; m < M; m += nwarp) {
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(Sf + off + 2 * m);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + m * mst) : "memory");
+      }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
   }
   __syncthreads();
   const int gp = grp / 3, gr = grp - 3 * gp;   // pair, residue of this group
