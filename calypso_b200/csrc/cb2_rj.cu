@@ -380,10 +380,9 @@ struct Fields {
 
 // explicit update (Euler on the first step, Adams-Bashforth 2 after)
 __global__ void k_explicit(RJArgs a, Fields F, int euler) {
-  size_t n = (size_t)a.nr * a.jmax;
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n) return;
-  int k = (int)(idx / a.jmax);
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+  if (jj >= a.jmax) return;
+  const size_t idx = (size_t)k * a.jmax + jj;
   bool in_shell = (k >= a.kin && k <= a.kout);
   const double adam_0 = 3.0 / 2.0, adam_1 = -1.0 / 2.0, dt = a.dt;
   double *wS = F(VORT), *wT = F(VORT + 2), *dwS = F(WDIFF), *dwT = F(WDIFF + 2);
@@ -482,10 +481,10 @@ __device__ inline double D2(const RJArgs &a, const double *f, int k, int jj) {
 //  with insulating walls, cal_rot_buoyancy_sph_MHD).  Wall values of u and
 // of the toroidal field are zero by the boundary conditions.
 __global__ void k_derived_a(RJArgs a, Fields F) {
-  size_t n = (size_t)a.nr * a.jmax;
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n) return;
-  int k = (int)(idx / a.jmax), jj = (int)(idx % a.jmax);
+  // grid (jj blocks, radial level k): no division to find k and jj
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+  if (jj >= a.jmax) return;
+  const size_t idx = (size_t)k * a.jmax + jj;
   size_t s = a.jmax;
   const BCW &b = a.bc;
   double g3 = a.g3[jj], gl = a.gl[jj];
@@ -553,10 +552,10 @@ __global__ void k_derived_a(RJArgs a, Fields F) {
 // diffusion terms (const_sph_vorticirty_diffusion, const_sph_scalar_diffusion,
 // const_sph_mag_diffuse_by_j); the wall values of T are the fixed values
 __global__ void k_derived_b(RJArgs a, Fields F) {
-  size_t n = (size_t)a.nr * a.jmax;
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n) return;
-  int k = (int)(idx / a.jmax), jj = (int)(idx % a.jmax);
+  // grid (jj blocks, radial level k): no division to find k and jj
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+  if (jj >= a.jmax) return;
+  const size_t idx = (size_t)k * a.jmax + jj;
   size_t s = a.jmax;
   const BCW &b = a.bc;
   double g3 = a.g3[jj], gl = a.gl[jj];
@@ -619,10 +618,10 @@ __global__ void k_derived_b(RJArgs a, Fields F) {
 // Coriolis term (sum_rot_coriolis_rlm_10): one thread per (k, jj)
 __global__ void k_coriolis(RJArgs a, Fields F, const int *jgi1, const int *jgi2, const int *jei1,
                            const double *sw, const double *tw) {
-  size_t n = (size_t)a.nr * a.jmax;
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n) return;
-  int k = (int)(idx / a.jmax), jj = (int)(idx % a.jmax);
+  // grid (jj blocks, radial level k): no division to find k and jj
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+  if (jj >= a.jmax) return;
+  const size_t idx = (size_t)k * a.jmax + jj;
   size_t base = (size_t)k * a.jmax, J = a.jmax;
   const double *vS = F(VELO), *vdS = F(VELO + 1), *wS = F(VORT), *wdS = F(VORT + 1), *wT = F(VORT + 2);
   size_t i11 = base + jgi1[jj], i21 = base + jgi2[jj], i12 = base + jei1[jj];
@@ -645,10 +644,10 @@ __global__ void k_coriolis(RJArgs a, Fields F, const int *jgi1, const int *jgi2,
 // (const_sph_force_rot2, const_sph_rotation_uxb, const_sph_scalar_advect,
 //  add_reftemp_advect_sph_MHD, set_MHD_terms_to_force)
 __global__ void k_after_transform(RJArgs a, Fields F) {
-  size_t n = (size_t)a.nr * a.jmax;
-  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n) return;
-  int k = (int)(idx / a.jmax), jj = (int)(idx % a.jmax);
+  // grid (jj blocks, radial level k): no division to find k and jj
+  const int jj = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+  if (jj >= a.jmax) return;
+  const size_t idx = (size_t)k * a.jmax + jj;
   size_t s = a.jmax;
   const BCW &b = a.bc;
   double g3 = a.g3[jj], gl = a.gl[jj];
@@ -770,8 +769,7 @@ __global__ void k_energy_reduce(int jmax, const double *ej, double *out) {
 static Fields fields(Ctx &c) { return Fields{c.d_f, c.fsize()}; }
 
 void rj_explicit(Ctx &c, bool euler) {
-  size_t n = c.fsize();
-  k_explicit<<<cdiv(n, kThreads), kThreads, 0, c.stream>>>(c.rj_args(), fields(c), euler ? 1 : 0);
+  k_explicit<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(c.rj_args(), fields(c), euler ? 1 : 0);
 }
 
 void rj_implicit(Ctx &c) {
@@ -779,27 +777,23 @@ void rj_implicit(Ctx &c) {
   k_implicit<<<dim3(cdiv(c.jmax, 128), 5), 128, 0, c.stream>>>(a, fields(c), c.d_lu_vp, c.d_pv_vp, c.d_lu_vt,
                                                       c.d_pv_vt, c.d_lu_bs, c.d_pv_bs, c.d_lu_bt,
                                                       c.d_pv_bt, c.d_lu_t, c.d_pv_t);
-  size_t n = c.fsize();
-  k_derived_a<<<cdiv(n, kThreads), kThreads, 0, c.stream>>>(a, fields(c));
-  k_derived_b<<<cdiv(n, kThreads), kThreads, 0, c.stream>>>(a, fields(c));
+  k_derived_a<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(a, fields(c));
+  k_derived_b<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(a, fields(c));
 }
 
 void rj_start_derived(Ctx &c) {
   RJArgs a = c.rj_args();
-  size_t n = c.fsize();
-  k_derived_a<<<cdiv(n, kThreads), kThreads, 0, c.stream>>>(a, fields(c));
-  k_derived_b<<<cdiv(n, kThreads), kThreads, 0, c.stream>>>(a, fields(c));
+  k_derived_a<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(a, fields(c));
+  k_derived_b<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(a, fields(c));
 }
 
 void rj_coriolis(Ctx &c) {
-  size_t n = c.fsize();
-  k_coriolis<<<cdiv(n, kThreads), kThreads, 0, c.stream>>>(c.rj_args(), fields(c), c.d_jgi1, c.d_jgi2,
+  k_coriolis<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(c.rj_args(), fields(c), c.d_jgi1, c.d_jgi2,
                                                            c.d_jei1, c.d_sw, c.d_tw);
 }
 
 void rj_after_transform(Ctx &c) {
-  size_t n = c.fsize();
-  k_after_transform<<<cdiv(n, kThreads), kThreads, 0, c.stream>>>(c.rj_args(), fields(c));
+  k_after_transform<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(c.rj_args(), fields(c));
 }
 
 void rj_temp_total(Ctx &c, double sign) {
