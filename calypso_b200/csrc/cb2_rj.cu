@@ -295,13 +295,29 @@ int rj_lu_factorise(Ctx &c) {
 // Banded back substitutions of one column (lubksb_3band / lubksb_5band,
 // SOLVER_src/direct_solver/lubksb_357band.f90:69-148, over the pivoted LU of
 // m_ludcmp_3band.f90 / m_ludcmp_band.f90): row interchanges, L y = P b, then
-// U x = y, with the recurrence carried in registers -- each value of the
-// column is read once per sweep (the read of the next row issued before the
-// store of this one) and the band factors come through the read-only path.
+// U x = y.  The recurrence is carried in registers and the column streamed
+// in chunks of PF rows, the loads of the next chunk issued before the stores
+// of this one, so a sweep waits on memory once per chunk rather than once
+// per row; the band factors come through the read-only path and the
+// divisions by the diagonal of U become multiplications by its reciprocal
+// (off the dependency chain).
+constexpr int PF = 8;
+
 __device__ static void d_pivots(int n, const int *piv, double *x, size_t stride) {
   for (int i = 1; i <= n; i++) {
     const int ll = __ldg(piv + i - 1);
     if (ll != i) { const double s = XC(ll); XC(ll) = XC(i); XC(i) = s; }
+  }
+}
+
+// rows i0 .. i0 + PF - 1 (ascending, dir = +1) or i0 .. i0 - PF + 1
+// (descending, dir = -1) that lie in 1 .. n; others read as zero
+template <int DIR>
+__device__ __forceinline__ void d_chunk(const double *x, size_t stride, int n, int i0, double (&v)[PF]) {
+#pragma unroll
+  for (int u = 0; u < PF; u++) {
+    const int q = i0 + DIR * u;
+    v[u] = (q >= 1 && q <= n) ? XC(q) : 0.0;
   }
 }
 
@@ -310,27 +326,43 @@ __device__ static void d_solve_3band(int n, const double *lu, const int *piv, do
   // forward: L y = P b
   double ym2 = XC(1), ym1 = XC(2) - __ldg(&M5(lu, 4, 1)) * ym2;
   XC(2) = ym1;
-  double nx = XC(3);
-  for (int i = 3; i <= n; i++) {
-    const double b = nx;
-    if (i < n) nx = XC(i + 1);
-    const double y = b - __ldg(&M5(lu, 5, i - 2)) * ym2 - __ldg(&M5(lu, 4, i - 1)) * ym1;
-    XC(i) = y;
-    ym2 = ym1; ym1 = y;
+  double buf[PF], nb[PF];
+  d_chunk<1>(x, stride, n, 3, buf);
+  for (int i0 = 3; i0 <= n; i0 += PF) {
+    d_chunk<1>(x, stride, n, i0 + PF, nb);
+#pragma unroll
+    for (int u = 0; u < PF; u++) {
+      const int i = i0 + u;
+      if (i <= n) {
+        const double y = buf[u] - __ldg(&M5(lu, 5, i - 2)) * ym2 - __ldg(&M5(lu, 4, i - 1)) * ym1;
+        XC(i) = y;
+        ym2 = ym1; ym1 = y;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PF; u++) buf[u] = nb[u];
   }
   // backward: U x = y
-  double xp2 = ym1 / __ldg(&M5(lu, 3, n));
+  double xp2 = ym1 * (1.0 / __ldg(&M5(lu, 3, n)));
   const double yn1 = XC(n - 1);
+  double xp1 = (yn1 - __ldg(&M5(lu, 2, n)) * xp2) * (1.0 / __ldg(&M5(lu, 3, n - 1)));
+  d_chunk<-1>(x, stride, n, n - 2, buf);
   XC(n) = xp2;
-  double xp1 = (yn1 - __ldg(&M5(lu, 2, n)) * xp2) / __ldg(&M5(lu, 3, n - 1));
-  nx = XC(n - 2);
   XC(n - 1) = xp1;
-  for (int i = n - 2; i >= 1; i--) {
-    const double b = nx;
-    if (i > 1) nx = XC(i - 1);
-    const double v = (b - __ldg(&M5(lu, 2, i + 1)) * xp1 - __ldg(&M5(lu, 1, i + 2)) * xp2) / __ldg(&M5(lu, 3, i));
-    XC(i) = v;
-    xp2 = xp1; xp1 = v;
+  for (int i0 = n - 2; i0 >= 1; i0 -= PF) {
+    d_chunk<-1>(x, stride, n, i0 - PF, nb);
+#pragma unroll
+    for (int u = 0; u < PF; u++) {
+      const int i = i0 - u;
+      if (i >= 1) {
+        const double v = (buf[u] - __ldg(&M5(lu, 2, i + 1)) * xp1 - __ldg(&M5(lu, 1, i + 2)) * xp2) *
+                         (1.0 / __ldg(&M5(lu, 3, i)));
+        XC(i) = v;
+        xp2 = xp1; xp1 = v;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PF; u++) buf[u] = nb[u];
   }
 }
 
@@ -341,33 +373,50 @@ __device__ static void d_solve_5band(int n, const double *lu, const int *piv, do
   double y2 = XC(2) - __ldg(&M9(lu, 6, 1)) * y1;
   double y3 = XC(3) - __ldg(&M9(lu, 7, 1)) * y1 - __ldg(&M9(lu, 6, 2)) * y2;
   double y4 = XC(4) - __ldg(&M9(lu, 8, 1)) * y1 - __ldg(&M9(lu, 7, 2)) * y2 - __ldg(&M9(lu, 6, 3)) * y3;
+  double buf[PF], nb[PF];
+  d_chunk<1>(x, stride, n, 5, buf);
   XC(2) = y2; XC(3) = y3; XC(4) = y4;
-  double nx = XC(5);
-  for (int i = 5; i <= n; i++) {
-    const double b = nx;
-    if (i < n) nx = XC(i + 1);
-    const double y = b - __ldg(&M9(lu, 9, i - 4)) * y1 - __ldg(&M9(lu, 8, i - 3)) * y2
-                   - __ldg(&M9(lu, 7, i - 2)) * y3 - __ldg(&M9(lu, 6, i - 1)) * y4;
-    XC(i) = y;
-    y1 = y2; y2 = y3; y3 = y4; y4 = y;
+  for (int i0 = 5; i0 <= n; i0 += PF) {
+    d_chunk<1>(x, stride, n, i0 + PF, nb);
+#pragma unroll
+    for (int u = 0; u < PF; u++) {
+      const int i = i0 + u;
+      if (i <= n) {
+        const double y = buf[u] - __ldg(&M9(lu, 9, i - 4)) * y1 - __ldg(&M9(lu, 8, i - 3)) * y2
+                       - __ldg(&M9(lu, 7, i - 2)) * y3 - __ldg(&M9(lu, 6, i - 1)) * y4;
+        XC(i) = y;
+        y1 = y2; y2 = y3; y3 = y4; y4 = y;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PF; u++) buf[u] = nb[u];
   }
   // backward: U x = y (y4 = y(n))
   const double b1 = XC(n - 1), b2 = XC(n - 2), b3 = XC(n - 3);
-  const double x0 = y4 / __ldg(&M9(lu, 5, n));
-  const double xm1 = (b1 - __ldg(&M9(lu, 4, n)) * x0) / __ldg(&M9(lu, 5, n - 1));
-  const double xm2 = (b2 - __ldg(&M9(lu, 4, n - 1)) * xm1 - __ldg(&M9(lu, 3, n)) * x0) / __ldg(&M9(lu, 5, n - 2));
+  const double x0 = y4 * (1.0 / __ldg(&M9(lu, 5, n)));
+  const double xm1 = (b1 - __ldg(&M9(lu, 4, n)) * x0) * (1.0 / __ldg(&M9(lu, 5, n - 1)));
+  const double xm2 = (b2 - __ldg(&M9(lu, 4, n - 1)) * xm1 - __ldg(&M9(lu, 3, n)) * x0) *
+                     (1.0 / __ldg(&M9(lu, 5, n - 2)));
   const double xm3 = (b3 - __ldg(&M9(lu, 4, n - 2)) * xm2 - __ldg(&M9(lu, 3, n - 1)) * xm1
-                      - __ldg(&M9(lu, 2, n)) * x0) / __ldg(&M9(lu, 5, n - 3));
+                      - __ldg(&M9(lu, 2, n)) * x0) * (1.0 / __ldg(&M9(lu, 5, n - 3)));
+  d_chunk<-1>(x, stride, n, n - 4, buf);
   XC(n) = x0; XC(n - 1) = xm1; XC(n - 2) = xm2; XC(n - 3) = xm3;
   double p1 = xm3, p2 = xm2, p3 = xm1, p4 = x0;   // x(i+1) .. x(i+4)
-  nx = XC(n - 4);
-  for (int i = n - 4; i >= 1; i--) {
-    const double b = nx;
-    if (i > 1) nx = XC(i - 1);
-    const double v = (b - __ldg(&M9(lu, 4, i + 1)) * p1 - __ldg(&M9(lu, 3, i + 2)) * p2
-                      - __ldg(&M9(lu, 2, i + 3)) * p3 - __ldg(&M9(lu, 1, i + 4)) * p4) / __ldg(&M9(lu, 5, i));
-    XC(i) = v;
-    p4 = p3; p3 = p2; p2 = p1; p1 = v;
+  for (int i0 = n - 4; i0 >= 1; i0 -= PF) {
+    d_chunk<-1>(x, stride, n, i0 - PF, nb);
+#pragma unroll
+    for (int u = 0; u < PF; u++) {
+      const int i = i0 - u;
+      if (i >= 1) {
+        const double v = (buf[u] - __ldg(&M9(lu, 4, i + 1)) * p1 - __ldg(&M9(lu, 3, i + 2)) * p2
+                          - __ldg(&M9(lu, 2, i + 3)) * p3 - __ldg(&M9(lu, 1, i + 4)) * p4) *
+                         (1.0 / __ldg(&M9(lu, 5, i)));
+        XC(i) = v;
+        p4 = p3; p3 = p2; p2 = p1; p1 = v;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PF; u++) buf[u] = nb[u];
   }
 }
 
