@@ -259,6 +259,17 @@ __global__ void k_lu_factorise(RJArgs a, double cv, double cb, double ct, double
   if (err) atomicOr(status, 1);
 }
 
+// [l][row][entry] -> [row][entry][l]: the degrees side by side, so a warp of
+// consecutive (l, m) columns of one order reads each band factor as one run
+template <typename T>
+__global__ void k_interleave_l(const T *src, T *dst, int nl, int w, int n) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x, tot = (size_t)nl * w * n;
+  if (e >= tot) return;
+  const int l = (int)(e % nl);
+  const size_t re = e / nl;   // row * w + entry
+  dst[e] = src[(size_t)l * w * n + re];
+}
+
 int rj_lu_factorise(Ctx &c) {
   int n = c.nr, L = c.L;
   size_t per = (size_t)(18 * n + 2 * (n + 1));
@@ -278,6 +289,24 @@ int rj_lu_factorise(Ctx &c) {
       c.p.coef_imp_t * c.p.coef_d_temp * dt, work, c.d_lu_vp, c.d_pv_vp, c.d_lu_vt, c.d_pv_vt,
       c.d_lu_bs, c.d_pv_bs, c.d_lu_bt, c.d_pv_bt, c.d_lu_t, c.d_pv_t, c.d_status);
   CB2_CUDA(cudaGetLastError());
+  // degree-interleaved copies (through the work buffer, which is larger)
+  {
+    const int nl = L + 1;
+    double *lus[5] = {c.d_lu_vp, c.d_lu_vt, c.d_lu_bs, c.d_lu_bt, c.d_lu_t};
+    const int ws[5] = {9, 5, 5, 5, 5};
+    for (int q = 0; q < 5; q++) {
+      const size_t tot = (size_t)nl * ws[q] * n;
+      k_interleave_l<double><<<cdiv((long)tot, 256), 256, 0, c.stream>>>(lus[q], work, nl, ws[q], n);
+      CB2_CUDA(cudaMemcpyAsync(lus[q], work, tot * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    }
+    int *pvs[5] = {c.d_pv_vp, c.d_pv_vt, c.d_pv_bs, c.d_pv_bt, c.d_pv_t};
+    for (int q = 0; q < 5; q++) {
+      const size_t tot = (size_t)nl * n;
+      k_interleave_l<int><<<cdiv((long)tot, 256), 256, 0, c.stream>>>(pvs[q], (int *)work, nl, 1, n);
+      CB2_CUDA(cudaMemcpyAsync(pvs[q], work, tot * sizeof(int), cudaMemcpyDeviceToDevice, c.stream));
+    }
+    CB2_CUDA(cudaGetLastError());
+  }
   int st = 0;
   CB2_CUDA(cudaMemcpyAsync(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   CB2_CUDA(cudaStreamSynchronize(c.stream));
@@ -301,11 +330,16 @@ int rj_lu_factorise(Ctx &c) {
 // per row; the band factors come through the read-only path and the
 // divisions by the diagonal of U become multiplications by its reciprocal
 // (off the dependency chain).
+// band factors in the degree-interleaved layout: lu = base + l, entry b of
+// row c at lu[((c - 1) * width + b - 1) * nl]
+#define M5I(a, b, c) (a)[(size_t)(((c) - 1) * 5 + ((b) - 1)) * nl]
+#define M9I(a, b, c) (a)[(size_t)(((c) - 1) * 9 + ((b) - 1)) * nl]
+
 constexpr int PF = 8;
 
-__device__ static void d_pivots(int n, const int *piv, double *x, size_t stride) {
+__device__ static void d_pivots(int n, const int *piv, int nl, double *x, size_t stride) {
   for (int i = 1; i <= n; i++) {
-    const int ll = __ldg(piv + i - 1);
+    const int ll = __ldg(piv + (size_t)(i - 1) * nl);
     if (ll != i) { const double s = XC(ll); XC(ll) = XC(i); XC(i) = s; }
   }
 }
@@ -321,10 +355,10 @@ __device__ __forceinline__ void d_chunk(const double *x, size_t stride, int n, i
   }
 }
 
-__device__ static void d_solve_3band(int n, const double *lu, const int *piv, double *x, size_t stride) {
-  d_pivots(n, piv, x, stride);
+__device__ static void d_solve_3band(int n, const double *lu, const int *piv, int nl, double *x, size_t stride) {
+  d_pivots(n, piv, nl, x, stride);
   // forward: L y = P b
-  double ym2 = XC(1), ym1 = XC(2) - __ldg(&M5(lu, 4, 1)) * ym2;
+  double ym2 = XC(1), ym1 = XC(2) - __ldg(&M5I(lu, 4, 1)) * ym2;
   XC(2) = ym1;
   double buf[PF], nb[PF];
   d_chunk<1>(x, stride, n, 3, buf);
@@ -334,7 +368,7 @@ __device__ static void d_solve_3band(int n, const double *lu, const int *piv, do
     for (int u = 0; u < PF; u++) {
       const int i = i0 + u;
       if (i <= n) {
-        const double y = buf[u] - __ldg(&M5(lu, 5, i - 2)) * ym2 - __ldg(&M5(lu, 4, i - 1)) * ym1;
+        const double y = buf[u] - __ldg(&M5I(lu, 5, i - 2)) * ym2 - __ldg(&M5I(lu, 4, i - 1)) * ym1;
         XC(i) = y;
         ym2 = ym1; ym1 = y;
       }
@@ -343,9 +377,9 @@ __device__ static void d_solve_3band(int n, const double *lu, const int *piv, do
     for (int u = 0; u < PF; u++) buf[u] = nb[u];
   }
   // backward: U x = y
-  double xp2 = ym1 * (1.0 / __ldg(&M5(lu, 3, n)));
+  double xp2 = ym1 * (1.0 / __ldg(&M5I(lu, 3, n)));
   const double yn1 = XC(n - 1);
-  double xp1 = (yn1 - __ldg(&M5(lu, 2, n)) * xp2) * (1.0 / __ldg(&M5(lu, 3, n - 1)));
+  double xp1 = (yn1 - __ldg(&M5I(lu, 2, n)) * xp2) * (1.0 / __ldg(&M5I(lu, 3, n - 1)));
   d_chunk<-1>(x, stride, n, n - 2, buf);
   XC(n) = xp2;
   XC(n - 1) = xp1;
@@ -355,8 +389,8 @@ __device__ static void d_solve_3band(int n, const double *lu, const int *piv, do
     for (int u = 0; u < PF; u++) {
       const int i = i0 - u;
       if (i >= 1) {
-        const double v = (buf[u] - __ldg(&M5(lu, 2, i + 1)) * xp1 - __ldg(&M5(lu, 1, i + 2)) * xp2) *
-                         (1.0 / __ldg(&M5(lu, 3, i)));
+        const double v = (buf[u] - __ldg(&M5I(lu, 2, i + 1)) * xp1 - __ldg(&M5I(lu, 1, i + 2)) * xp2) *
+                         (1.0 / __ldg(&M5I(lu, 3, i)));
         XC(i) = v;
         xp2 = xp1; xp1 = v;
       }
@@ -366,13 +400,13 @@ __device__ static void d_solve_3band(int n, const double *lu, const int *piv, do
   }
 }
 
-__device__ static void d_solve_5band(int n, const double *lu, const int *piv, double *x, size_t stride) {
-  d_pivots(n, piv, x, stride);
+__device__ static void d_solve_5band(int n, const double *lu, const int *piv, int nl, double *x, size_t stride) {
+  d_pivots(n, piv, nl, x, stride);
   // forward: L y = P b
   double y1 = XC(1);
-  double y2 = XC(2) - __ldg(&M9(lu, 6, 1)) * y1;
-  double y3 = XC(3) - __ldg(&M9(lu, 7, 1)) * y1 - __ldg(&M9(lu, 6, 2)) * y2;
-  double y4 = XC(4) - __ldg(&M9(lu, 8, 1)) * y1 - __ldg(&M9(lu, 7, 2)) * y2 - __ldg(&M9(lu, 6, 3)) * y3;
+  double y2 = XC(2) - __ldg(&M9I(lu, 6, 1)) * y1;
+  double y3 = XC(3) - __ldg(&M9I(lu, 7, 1)) * y1 - __ldg(&M9I(lu, 6, 2)) * y2;
+  double y4 = XC(4) - __ldg(&M9I(lu, 8, 1)) * y1 - __ldg(&M9I(lu, 7, 2)) * y2 - __ldg(&M9I(lu, 6, 3)) * y3;
   double buf[PF], nb[PF];
   d_chunk<1>(x, stride, n, 5, buf);
   XC(2) = y2; XC(3) = y3; XC(4) = y4;
@@ -382,8 +416,8 @@ __device__ static void d_solve_5band(int n, const double *lu, const int *piv, do
     for (int u = 0; u < PF; u++) {
       const int i = i0 + u;
       if (i <= n) {
-        const double y = buf[u] - __ldg(&M9(lu, 9, i - 4)) * y1 - __ldg(&M9(lu, 8, i - 3)) * y2
-                       - __ldg(&M9(lu, 7, i - 2)) * y3 - __ldg(&M9(lu, 6, i - 1)) * y4;
+        const double y = buf[u] - __ldg(&M9I(lu, 9, i - 4)) * y1 - __ldg(&M9I(lu, 8, i - 3)) * y2
+                       - __ldg(&M9I(lu, 7, i - 2)) * y3 - __ldg(&M9I(lu, 6, i - 1)) * y4;
         XC(i) = y;
         y1 = y2; y2 = y3; y3 = y4; y4 = y;
       }
@@ -393,12 +427,12 @@ __device__ static void d_solve_5band(int n, const double *lu, const int *piv, do
   }
   // backward: U x = y (y4 = y(n))
   const double b1 = XC(n - 1), b2 = XC(n - 2), b3 = XC(n - 3);
-  const double x0 = y4 * (1.0 / __ldg(&M9(lu, 5, n)));
-  const double xm1 = (b1 - __ldg(&M9(lu, 4, n)) * x0) * (1.0 / __ldg(&M9(lu, 5, n - 1)));
-  const double xm2 = (b2 - __ldg(&M9(lu, 4, n - 1)) * xm1 - __ldg(&M9(lu, 3, n)) * x0) *
-                     (1.0 / __ldg(&M9(lu, 5, n - 2)));
-  const double xm3 = (b3 - __ldg(&M9(lu, 4, n - 2)) * xm2 - __ldg(&M9(lu, 3, n - 1)) * xm1
-                      - __ldg(&M9(lu, 2, n)) * x0) * (1.0 / __ldg(&M9(lu, 5, n - 3)));
+  const double x0 = y4 * (1.0 / __ldg(&M9I(lu, 5, n)));
+  const double xm1 = (b1 - __ldg(&M9I(lu, 4, n)) * x0) * (1.0 / __ldg(&M9I(lu, 5, n - 1)));
+  const double xm2 = (b2 - __ldg(&M9I(lu, 4, n - 1)) * xm1 - __ldg(&M9I(lu, 3, n)) * x0) *
+                     (1.0 / __ldg(&M9I(lu, 5, n - 2)));
+  const double xm3 = (b3 - __ldg(&M9I(lu, 4, n - 2)) * xm2 - __ldg(&M9I(lu, 3, n - 1)) * xm1
+                      - __ldg(&M9I(lu, 2, n)) * x0) * (1.0 / __ldg(&M9I(lu, 5, n - 3)));
   d_chunk<-1>(x, stride, n, n - 4, buf);
   XC(n) = x0; XC(n - 1) = xm1; XC(n - 2) = xm2; XC(n - 3) = xm3;
   double p1 = xm3, p2 = xm2, p3 = xm1, p4 = x0;   // x(i+1) .. x(i+4)
@@ -408,9 +442,9 @@ __device__ static void d_solve_5band(int n, const double *lu, const int *piv, do
     for (int u = 0; u < PF; u++) {
       const int i = i0 - u;
       if (i >= 1) {
-        const double v = (buf[u] - __ldg(&M9(lu, 4, i + 1)) * p1 - __ldg(&M9(lu, 3, i + 2)) * p2
-                          - __ldg(&M9(lu, 2, i + 3)) * p3 - __ldg(&M9(lu, 1, i + 4)) * p4) *
-                         (1.0 / __ldg(&M9(lu, 5, i)));
+        const double v = (buf[u] - __ldg(&M9I(lu, 4, i + 1)) * p1 - __ldg(&M9I(lu, 3, i + 2)) * p2
+                          - __ldg(&M9I(lu, 2, i + 3)) * p3 - __ldg(&M9I(lu, 1, i + 4)) * p4) *
+                         (1.0 / __ldg(&M9I(lu, 5, i)));
         XC(i) = v;
         p4 = p3; p3 = p2; p2 = p1; p1 = v;
       }
@@ -475,26 +509,38 @@ __global__ void k_implicit(RJArgs a, Fields F, const double *lu_vp, const int *p
                            const double *lu_t, const int *pv_t) {
   const int jj = blockIdx.x * blockDim.x + threadIdx.x;
   if (jj >= a.jmax) return;
-  const int n = a.nr, l = a.jl[jj], fld = blockIdx.y;
+  const int n = a.nr, l = a.jl[jj], fld = blockIdx.y, nl = a.L + 1;   // factors interleaved by degree
   const size_t st = a.jmax;
   if (fld < 2) {
     // velocity from vorticity: S <- tor(w), T <- pol(w); l = 0 removed; walls zero
     double *u = F(VELO + 2 * fld) + jj, *udS = F(VELO + 1) + jj;
     const double *w = F(VORT + 2 - 2 * fld) + jj;
-    for (int k = 0; k < n; k++) {
-      const bool wall = (k <= a.kin || k == a.kout);
-      const double v = (jj == 0 || wall) ? 0.0 : w[k * st];
-      u[k * st] = v;
-      if (fld == 0 && wall) udS[k * st] = 0.0;
+    // PF levels per pass, loads before stores (w is only read here)
+    for (int k0 = 0; k0 < n; k0 += PF) {
+      double v[PF];
+#pragma unroll
+      for (int q = 0; q < PF; q++) {
+        const int k = k0 + q;
+        const bool wall = (k <= a.kin || k == a.kout);
+        v[q] = (k < n && jj != 0 && !wall) ? __ldg(w + (size_t)k * st) : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < PF; q++) {
+        const int k = k0 + q;
+        if (k < n) {
+          u[(size_t)k * st] = v[q];
+          if (fld == 0 && (k <= a.kin || k == a.kout)) udS[(size_t)k * st] = 0.0;
+        }
+      }
     }
-    if (fld == 0) d_solve_5band(n, lu_vp + (size_t)l * 9 * n, pv_vp + (size_t)l * n, u, st);
-    else d_solve_3band(n, lu_vt + (size_t)l * 5 * n, pv_vt + (size_t)l * n, u, st);
+    if (fld == 0) d_solve_5band(n, lu_vp + l, pv_vp + l, nl, u, st);
+    else d_solve_3band(n, lu_vt + l, pv_vt + l, nl, u, st);
   } else if (fld == 2) {
     // temperature with fixed wall values
     double *T = F(TEMP) + jj;
     for (int k = a.kout; k < n; k++) T[k * st] = cmb_fld(a, jj);
     for (int k = 0; k <= a.kin; k++) T[k * st] = icb_fld(a, jj);
-    d_solve_3band(n, lu_t + (size_t)l * 5 * n, pv_t + (size_t)l * n, T, st);
+    d_solve_3band(n, lu_t + l, pv_t + l, nl, T, st);
   } else if (fld == 3) {
     // poloidal magnetic field, insulating walls, l = 0 removed
     double *bS = F(MAGNE) + jj, *bdS = F(MAGNE + 1) + jj;
@@ -502,7 +548,7 @@ __global__ void k_implicit(RJArgs a, Fields F, const double *lu_vp, const int *p
       for (int k = 0; k < n; k++) bS[k * st] = 0.0;
     bdS[a.kin * st] = (a.gl[jj] + 1.0) * a.bc.r_icb[1] * bS[a.kin * st];
     bdS[a.kout * st] = -a.gl[jj] * a.bc.r_cmb[1] * bS[a.kout * st];
-    d_solve_3band(n, lu_bs + (size_t)l * 5 * n, pv_bs + (size_t)l * n, bS, st);
+    d_solve_3band(n, lu_bs + l, pv_bs + l, nl, bS, st);
   } else {
     // toroidal magnetic field, zero at the walls
     double *bT = F(MAGNE + 2) + jj;
@@ -510,7 +556,7 @@ __global__ void k_implicit(RJArgs a, Fields F, const double *lu_vp, const int *p
       for (int k = 0; k < n; k++) bT[k * st] = 0.0;
     bT[a.kin * st] = 0.0;
     bT[a.kout * st] = 0.0;
-    d_solve_3band(n, lu_bt + (size_t)l * 5 * n, pv_bt + (size_t)l * n, bT, st);
+    d_solve_3band(n, lu_bt + l, pv_bt + l, nl, bT, st);
   }
 }
 
