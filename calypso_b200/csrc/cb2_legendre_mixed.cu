@@ -357,11 +357,12 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
   const uint32_t acc1 = accw / 2;                          // parity-1 accumulator within a set
 
   if (tid == 0) {
-    for (int q = 0; q < FRS; q++) { mbar_init(&sb->rawfull[q], 1); mbar_init(&sb->rawempty[q], FW_CONV); }
+    // consumer barriers count warps: one elected lane arrives for its warp
+    for (int q = 0; q < FRS; q++) { mbar_init(&sb->rawfull[q], 1); mbar_init(&sb->rawempty[q], FW_CONV / 32); }
     for (int q = 0; q < FAB; q++) {
-      mbar_init(&sb->afull[q], FW_CONV); mbar_init(&sb->bfull[q], 1); mbar_init(&sb->abempty[q], 1);
+      mbar_init(&sb->afull[q], FW_CONV / 32); mbar_init(&sb->bfull[q], 1); mbar_init(&sb->abempty[q], 1);
     }
-    for (int q = 0; q < 2; q++) { mbar_init(&sb->accfull[q], 1); mbar_init(&sb->accempty[q], FW_EPI); }
+    for (int q = 0; q < 2; q++) { mbar_init(&sb->accfull[q], 1); mbar_init(&sb->accempty[q], FW_EPI / 32); }
     mbar_init(&sb->fin, 1);
     sb->abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -483,16 +484,19 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
     const int r = tid & (TM - 1), h = tid >> 7;
     uint32_t nraw = 0, nab = 0;
     bool bad = false;
+    // every decision is warp-uniform: a warp arrives through one lane
     for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x) {
-      if (ws_aborted(sb)) { bad = true; break; }
+      if (__any_sync(0xffffffffu, ws_aborted(sb))) { bad = true; break; }
       const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
       const int row = q.row0 + r, q4 = row & 3;
       const float sc = fwd_row_scale(a, q, row);
       for (int b = 0; b < q.NB; b++) {
         const int tb = q.g ? (b >> 1) : b, part = q.g ? (b & 1) : 0;
         const uint32_t rs = nraw % FRS, s = nab % FAB;
-        if (part == 0 && !mbar_wait(&sb->rawfull[rs], (nraw / FRS) & 1)) { bad = true; break; }
-        if (nab >= FAB && !mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1)) { bad = true; break; }
+        bool ok = true;
+        if (part == 0) ok = mbar_wait(&sb->rawfull[rs], (nraw / FRS) & 1);
+        if (ok && nab >= FAB) ok = mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1);
+        if (!__all_sync(0xffffffffu, ok)) { bad = true; break; }
         // the two folds of this row's 16 K values; gemm P and the mP part
         // use fold p, the dP part fold 1 - p (with the signs of its rows)
         const float *rs_s = reinterpret_cast<const float *>(raw0 + rs * RAW_BYTES);
@@ -538,9 +542,13 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
           }
         }
         fence_proxy_async();
-        mbar_arrive(&sb->afull[s]);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sb->afull[s]);
         nab++;
-        if (!q.g || part == 1) { mbar_arrive(&sb->rawempty[rs]); nraw++; }
+        if (!q.g || part == 1) {
+          if (lane == 0) mbar_arrive(&sb->rawempty[rs]);
+          nraw++;
+        }
       }
     }
     if (bad) sb->abort = 1;
@@ -611,7 +619,8 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
         tmem_ld16x2(tl + (uint32_t)(c * 16), tl + acc1 + (uint32_t)(c * 16), v0, v1);
         if (c == nch - 1) {
           tc_fence_before();
-          mbar_arrive(&sb->accempty[ab]);
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sb->accempty[ab]);
         }
         const double c7 = n7 * (double)nbu, c6 = n6 * (double)nbu;
         fetch(c + 1, n7, n6, nbu);
@@ -863,9 +872,10 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
 
   if (tid == 0) {
     for (int q = 0; q < BW_ST; q++) {
-      mbar_init(&sb->full[q], 1); mbar_init(&sb->afull[q], BW_CONV); mbar_init(&sb->empty[q], 1);
+      // consumer barriers count warps: one elected lane arrives for its warp
+      mbar_init(&sb->full[q], 1); mbar_init(&sb->afull[q], BW_CONV / 32); mbar_init(&sb->empty[q], 1);
     }
-    for (int q = 0; q < 2; q++) { mbar_init(&sb->accfull[q], 1); mbar_init(&sb->accempty[q], BW_EPI); }
+    for (int q = 0; q < 2; q++) { mbar_init(&sb->accfull[q], 1); mbar_init(&sb->accempty[q], BW_EPI / 32); }
     mbar_init(&sb->fin, 1);
     sb->abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -975,8 +985,9 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
       const BwdTile q0 = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
       mx_next = bwd_row_max(a, q0, q0.row0 + r);
     }
+    // every decision is warp-uniform: a warp arrives through one lane
     for (; t < ntiles && !bad; t += gridDim.x) {
-      if (ws_aborted(sb)) { bad = true; break; }
+      if (__any_sync(0xffffffffu, ws_aborted(sb))) { bad = true; break; }
       const BwdTile q = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
       const int row = q.row0 + r, q4 = row & 3;
       const float sc = pow2_scale(mx_next);
@@ -990,7 +1001,7 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
         int p, part, ib, len;
         bwd_blk(q, b, p, part, ib, len);
         const uint32_t s = n % BW_ST;
-        if (!mbar_wait(&sb->full[s], (n / BW_ST) & 1)) { bad = true; break; }
+        if (!__all_sync(0xffffffffu, mbar_wait(&sb->full[s], (n / BW_ST) & 1))) { bad = true; break; }
         unsigned char *st = base + s * ST_BYTES;
         const float *raw = reinterpret_cast<const float *>(st);
         int src = r;
@@ -1022,7 +1033,8 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
           *reinterpret_cast<uint4 *>(alo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
         }
         fence_proxy_async();
-        mbar_arrive(&sb->afull[s]);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sb->afull[s]);
         n++;
       }
     }
@@ -1060,7 +1072,8 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
       const int c0 = hc ? ch : 0, c1 = hc ? nch : ch;
       if (c0 == c1) {
         tc_fence_before();
-        mbar_arrive(&sb->accempty[ab]);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sb->accempty[ab]);
       }
       for (int c = c0; c < c1; c++) {
         float e[32], o[32];
@@ -1073,7 +1086,8 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
         }
         if (c == c1 - 1) {
           tc_fence_before();
-          mbar_arrive(&sb->accempty[ab]);
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sb->accempty[ab]);
         }
         if (valid) {
 #pragma unroll
