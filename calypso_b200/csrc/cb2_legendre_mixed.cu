@@ -190,8 +190,14 @@ __host__ __device__ inline float pow2_scale(double mx) {
   return ldexpf(1.0f, sh);
 }
 
-__device__ inline uint32_t pack_half2(__half a, __half b) {
-  return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
+// x0, x1 -> fp16 hi and lo pairs (x = hi + lo to 22 bits), x0 in the low
+// half; the paired conversions run on the full-rate pipes
+__device__ inline void split_pair(float x0, float x1, uint32_t &hi, uint32_t &lo) {
+  const __half2 h = __floats2half2_rn(x0, x1);
+  const float2 f = __half22float2(h);
+  const __half2 l = __floats2half2_rn(x0 - f.x, x1 - f.y);
+  hi = *reinterpret_cast<const uint32_t *>(&h);
+  lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
 __device__ inline unsigned char *smem_base_1024(unsigned char *raw) {
@@ -531,10 +537,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             uint32_t hh[4], ll[4];
 #pragma unroll
             for (int e = 0; e < 8; e += 2) {
-              const float x0 = x2[p][c * 8 + e], x1 = x2[p][c * 8 + e + 1];
-              const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
-              hh[e >> 1] = pack_half2(h0, h1);
-              ll[e >> 1] = pack_half2(__float2half_rn(x0 - __half2float(h0)), __float2half_rn(x1 - __half2float(h1)));
+              split_pair(x2[p][c * 8 + e], x2[p][c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
             }
             const uint32_t off = sw64_chunk(r, 2 * h + c);
             *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
@@ -1023,10 +1026,7 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
           uint32_t hh[4], ll[4];
 #pragma unroll
           for (int e = 0; e < 8; e += 2) {
-            const float x0 = x[c * 8 + e], x1 = x[c * 8 + e + 1];
-            const __half h0 = __float2half_rn(x0), h1 = __float2half_rn(x1);
-            hh[e >> 1] = pack_half2(h0, h1);
-            ll[e >> 1] = pack_half2(__float2half_rn(x0 - __half2float(h0)), __float2half_rn(x1 - __half2float(h1)));
+            split_pair(x[c * 8 + e], x[c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
           }
           const uint32_t off = sw64_chunk(r, 2 * h + c);
           *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
