@@ -145,23 +145,6 @@ __device__ inline void fence_proxy_async() { asm volatile("fence.proxy.async.sha
 __device__ inline void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ inline void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// two 16-column loads (columns ta.. and tb..) behind one wait
-__device__ inline void tmem_ld16x2(uint32_t ta, uint32_t tb, float va[16], float vb[16]) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%32];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%33];\n\t"
-      "tcgen05.wait::ld.sync.aligned;"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(ta), "r"(tb)
-      : "memory");
-#pragma unroll
-  for (int i = 0; i < 16; i++) { va[i] = __uint_as_float(r[i]); vb[i] = __uint_as_float(r[16 + i]); }
-}
-
 // two 32-column loads (columns ta.. and tb..) behind one wait
 __device__ inline void tmem_ld32x2(uint32_t ta, uint32_t tb, float va[32], float vb[32]) {
   uint32_t r[64];
@@ -188,6 +171,22 @@ __host__ __device__ inline float pow2_scale(double mx) {
   int sh = kScaleExp - e;
   sh = sh < -120 ? -120 : (sh > 120 ? 120 : sh);
   return ldexpf(1.0f, sh);
+}
+
+// tcgen05.ld 16x256b, two loads behind one wait: thread t receives columns
+// 2 (t & 3) and 2 (t & 3) + 1 of lanes (t >> 2) and (t >> 2) + 8 of the 16
+// lanes addressed (va[0..1]: lane t >> 2, va[2..3]: lane (t >> 2) + 8)
+__device__ inline void tmem_ld_16x256b_pair(uint32_t ta, uint32_t tb, float va[4], float vb[4]) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.16x256b.x1.b32 {%0,%1,%2,%3}, [%8];\n\t"
+      "tcgen05.ld.sync.aligned.16x256b.x1.b32 {%4,%5,%6,%7}, [%9];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(ta), "r"(tb)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 4; i++) { va[i] = __uint_as_float(r[i]); vb[i] = __uint_as_float(r[4 + i]); }
 }
 
 // x0, x1 -> fp16 hi and lo pairs (x = hi + lo to 22 bits), x0 in the low
@@ -263,18 +262,22 @@ constexpr int FAB = 2;   // A/B stages
 // basis tables of a few orders in L2.  Roles:
 //   warps 0-7   converters: raw float32 rows (TMA) -> scaled, folded, split
 //               fp16 hi/lo A operands (64-byte swizzle), both parities
-//   warps 8-11  epilogue: TMEM -> per-warp shared transpose -> one row's
-//               degrees l = m .. L per store run, float64, geometric factors
-//   warp 12     TMA producer (raw rows and basis tiles)
-//   warp 13     MMA issuer (tcgen05, one elected thread)
+//   warps 8-15  epilogue: TMEM (16x256b loads, the two parities side by
+//               side) -> float64 degree runs of each row, geometric factors
+//   warp 16     TMA producer (raw rows and basis tiles)
+//   warp 17     MMA issuer (tcgen05, one elected thread)
 // Two TMEM accumulator sets (when they fit) let the epilogue of one tile
 // overlap the main loop of the next.
-constexpr int FW_CONV = 256, FW_EPI = 128, FW_THREADS = 448;
-constexpr int FW_PROD_WARP = 12, FW_MMA_WARP = 13;
-constexpr int FW_EPI_PITCH = 33;
+constexpr int FW_CONV = 256, FW_EPI = 256, FW_THREADS = FW_CONV + FW_EPI + 64;
+constexpr int FW_PROD_WARP = (FW_CONV + FW_EPI) / 32, FW_MMA_WARP = FW_PROD_WARP + 1;
+
+// epilogue staging of one warp: 16 rows x 16 degrees (+1 pad) floats, then
+// the row metadata (destination offset, scale, factor select) of its 16 rows
+constexpr int FW_STG_P = 17;
+constexpr uint32_t FW_STG_BYTES = ((16 * FW_STG_P * 4 + 16 * 8 + 16 * 8 + 16 * 4) + 15) & ~15u;
 
 struct FwdWsLayout {
-  uint32_t raw, ab, stg, moff, mc, mg, w, bar, total;   // byte offsets from the aligned base
+  uint32_t raw, ab, stg, w, bar, total;   // byte offsets from the aligned base
 };
 
 __host__ __device__ inline FwdWsLayout fwd_ws_layout(int nfb, int L, int nth) {
@@ -283,10 +286,7 @@ __host__ __device__ inline FwdWsLayout fwd_ws_layout(int nfb, int L, int nth) {
   const uint32_t bbytes = (uint32_t)nfb * FKB * 2;
   o.raw = p; p += FRS * RAW_BYTES;
   o.ab = p; p += FAB * (4 * FA_BYTES + 4 * bbytes);
-  o.stg = p; p += 4 * 32 * FW_EPI_PITCH * 4;
-  o.moff = p; p += TM * 8;
-  o.mc = p; p += TM * 8;
-  o.mg = p; p += TM * 4;
+  o.stg = p; p += (FW_EPI / 32) * FW_STG_BYTES;
   o.w = p; p += ((uint32_t)nth * 4 + 15) & ~15u;
   o.bar = p; p += 256;
   o.total = p;
@@ -556,23 +556,31 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
     }
     if (bad) sb->abort = 1;
   } else {
-    // epilogue warps 8-11: TMEM lanes 32 (warp % 4) .. + 31.  Every
-    // decision that guards a warp-collective TMEM load is made warp-uniform.
-    const int ew = warp - FW_CONV / 32, er = ew * 32 + lane;
-    float *stg = reinterpret_cast<float *>(base + lay.stg) + ew * 32 * FW_EPI_PITCH;
-    long long *moff = reinterpret_cast<long long *>(base + lay.moff);
-    double *mc = reinterpret_cast<double *>(base + lay.mc);
-    int *mg = reinterpret_cast<int *>(base + lay.mg);
+    // epilogue warps 8-15: warp 8 + h * 4 + q reads TMEM lanes 32 q + 16 h ..
+    // + 15 with 16x256b loads: thread (t0 = lane & 3, t1 = lane >> 2) gets
+    // columns 2 t0, 2 t0 + 1 of rows t1, t1 + 8, and the two parity
+    // accumulators interleave to the degrees 16 g + 4 t0 .. + 3 of a row.
+    // Through the warp's shared staging [16 rows][16 degrees], a store then
+    // writes 16 consecutive degrees of two rows (lanes 0-15, 16-31).
+    // Decisions that guard the warp-collective TMEM loads are warp-uniform.
+    const int ew = warp - FW_CONV / 32, qd = ew & 3, hf = ew >> 2;
+    const int t0 = lane & 3, t1 = lane >> 2, lc = lane & 15, lr = lane >> 4;
+    unsigned char *wst = base + lay.stg + ew * FW_STG_BYTES;
+    float *stg = reinterpret_cast<float *>(wst);                                   // [16][FW_STG_P]
+    long long *moff = reinterpret_cast<long long *>(wst + 16 * FW_STG_P * 4);     // [16]
+    double *mc = reinterpret_cast<double *>(moff + 16);                           // [16]
+    int *mg = reinterpret_cast<int *>(mc + 16);                                   // [16]
     double *__restrict__ fout = a.f;
     int i = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
       if (__any_sync(0xffffffffu, ws_aborted(sb))) break;
       const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
       const int nl = a.L + 1 - q.m;
-      // this thread's row: destination, scale and which degree factor
+      // lanes 0-15: destination, scale and degree factor of row lane
       // (sel 0: g7, 1: g6; both depend on l and m only, not on s)
-      {
-        const int rw = q.row0 + er;
+      __syncwarp();
+      if (lane < 16) {
+        const int rw = q.row0 + qd * 32 + hf * 16 + lane;
         long long off = -1;
         double cr = 0.0;
         int sel = 0;
@@ -594,21 +602,20 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             sel = (kind == 2) ? 1 : 0;
           }
         }
-        moff[er] = off; mc[er] = cr; mg[er] = sel;
+        moff[lane] = off; mc[lane] = cr; mg[lane] = sel;
       }
-      __syncwarp();
       const int ab = i % nacc;
       const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1);
       if (!__all_sync(0xffffffffu, ok)) { sb->abort = 1; break; }
       tc_fence_after();
-      const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)(ew * 32) << 16);
-      const int nch = (nl + 31) / 32, j0 = a.moff[q.m];
+      const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)(qd * 32 + hf * 16) << 16);
+      const int ng = (nl + 15) / 16, j0 = a.moff[q.m];
       const float *bun0 = a.bunscale + ((size_t)q.g * (a.L + 1) * 2 + q.m * 2) * a.NFmax, *bun1 = bun0 + a.NFmax;
-      // degree factors of chunk c (l = m + 32 c + lane), fetched one chunk ahead
-      auto fetch = [&](int c, double &g7v, double &g6v, float &buv) {
-        const int lm = c * 32 + lane;
+      // degree factors of degree 16 g + lc (this lane's column), a group ahead
+      auto fetch = [&](int g, double &g7v, double &g6v, float &buv) {
+        const int lm = g * 16 + lc;
         g7v = 0.0; g6v = 0.0; buv = 0.0f;
-        if (c < nch && lm < nl) {
+        if (g < ng && lm < nl) {
           g7v = __ldg(a.g7 + j0 + lm);
           g6v = __ldg(a.g6 + j0 + lm);
           buv = (lm & 1) ? __ldg(bun1 + (lm >> 1)) : __ldg(bun0 + (lm >> 1));
@@ -617,40 +624,29 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
       double n7, n6;
       float nbu;
       fetch(0, n7, n6, nbu);
-      for (int c = 0; c < nch; c++) {
-        float v0[16], v1[16];
-        tmem_ld16x2(tl + (uint32_t)(c * 16), tl + acc1 + (uint32_t)(c * 16), v0, v1);
-        if (c == nch - 1) {
+      for (int g = 0; g < ng; g++) {
+        float p0[4], p1[4];
+        tmem_ld_16x256b_pair(tl + (uint32_t)(g * 8), tl + acc1 + (uint32_t)(g * 8), p0, p1);
+        if (g == ng - 1) {
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(&sb->accempty[ab]);
         }
         const double c7 = n7 * (double)nbu, c6 = n6 * (double)nbu;
-        fetch(c + 1, n7, n6, nbu);
+        fetch(g + 1, n7, n6, nbu);
 #pragma unroll
-        for (int e = 0; e < 16; e++) {
-          stg[lane * FW_EPI_PITCH + 2 * e] = v0[e];
-          stg[lane * FW_EPI_PITCH + 2 * e + 1] = v1[e];
+        for (int j = 0; j < 2; j++) {
+          float *srow = stg + (t1 + 8 * j) * FW_STG_P + 4 * t0;
+          srow[0] = p0[2 * j]; srow[1] = p1[2 * j]; srow[2] = p0[2 * j + 1]; srow[3] = p1[2 * j + 1];
         }
         __syncwarp();
-        const int lm = c * 32 + lane;
+        const int lm = g * 16 + lc;
         if (lm < nl) {
-          // eight rows at a time: all loads, then all stores
-          for (int r0 = 0; r0 < 32; r0 += 8) {
-            float v[8];
-            long long o[8];
-            double cr[8];
-            int sl[8];
-#pragma unroll
-            for (int u = 0; u < 8; u++) {
-              v[u] = stg[(r0 + u) * FW_EPI_PITCH + lane];
-              o[u] = moff[ew * 32 + r0 + u];
-              cr[u] = mc[ew * 32 + r0 + u];
-              sl[u] = mg[ew * 32 + r0 + u];
-            }
-#pragma unroll
-            for (int u = 0; u < 8; u++)
-              if (o[u] >= 0) fout[o[u] + lm] = (double)v[u] * cr[u] * (sl[u] ? c6 : c7);
+#pragma unroll 4
+          for (int u = 0; u < 8; u++) {
+            const int rr = u + 8 * lr;
+            const long long o = moff[rr];
+            if (o >= 0) fout[o + lm] = (double)stg[rr * FW_STG_P + lc] * mc[rr] * (mg[rr] ? c6 : c7);
           }
         }
         __syncwarp();
