@@ -110,6 +110,10 @@ struct Ctx {
   int graph_nsteps = 0;
   // kernel variants chosen by the autotuner (cb2_autotune); defaults until tuned
   int tune[8] = {4, 2, 2, 384, 0, 0, 0, 0};
+  // persistent Legendre kernels launch min(SMs, tiles / ws_tiles_per_cta)
+  // CTAs: 1 = every SM; an ensemble raises it so small shells take a few
+  // SMs each and run side by side
+  int ws_tiles_per_cta = 1;
 
   size_t fsize() const { return (size_t)nr * jmax; }
   double *fld(int slot) { return d_f + (size_t)slot * fsize(); }

@@ -1418,6 +1418,13 @@ MLayout mlayout(const Ctx &c, void *buf, int nvec, int nscal) {
   return l;
 }
 
+// CTAs of a persistent Legendre launch over ntiles tiles
+static int ws_grid(const Ctx &c, int ntiles) {
+  const MixedTables *t = (const MixedTables *)c.mixed;
+  const int per = std::max(1, c.ws_tiles_per_cta);
+  return std::max(1, std::min(t->nsm, (ntiles + per - 1) / per));
+}
+
 int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   MixedTables *t = (MixedTables *)c.mixed;
   const int nvec = out.nvec, nscal = out.nscal, ng = nvec + nscal;
@@ -1456,7 +1463,7 @@ int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   const int rows0 = ng * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
   const int ntiles = (tiles0 + tiles1) * (c.L + 1);
-  k_leg_bwd_ws<<<std::min(ntiles, t->nsm), BW_THREADS, t->smem_bwd, c.stream>>>(
+  k_leg_bwd_ws<<<ws_grid(c, ntiles), BW_THREADS, t->smem_bwd, c.stream>>>(
       a, rows0, rows1, tiles0, tiles1, ntiles, rawP, rawD, t->tm_bb_hi, t->tm_bb_lo, t->tmem_bwd, t->nacc_bwd);
   return 0;
 }
@@ -1490,7 +1497,7 @@ int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots) {
   const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
   const int ntiles = (tiles0 + tiles1) * (c.L + 1);
-  k_leg_fwd_ws<<<std::min(ntiles, t->nsm), FW_THREADS, t->smem_fwd, c.stream>>>(
+  k_leg_fwd_ws<<<ws_grid(c, ntiles), FW_THREADS, t->smem_fwd, c.stream>>>(
       a, rows0, rows1, tiles0, tiles1, ntiles, rawP, rawD, t->tm_bfp_hi, t->tm_bfp_lo, t->tm_bfd_hi, t->tm_bfd_lo,
       t->tmem_fwd, t->nacc_fwd);
   return 0;

@@ -172,6 +172,9 @@ int cb2_ensemble_create(const cb2_params *ps, int n, int precision, int device, 
     int rc = cb2_create(&ps[i], precision, e->device, &c);
     if (rc) return fail(rc);
     e->shells.push_back(c);
+    // small shells take a few SMs each (about eight tiles per CTA of the
+    // persistent Legendre kernels), so the graph's branches run side by side
+    if (n > 1) c->ws_tiles_per_cta = 8;
     cudaEvent_t ev;
     if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
       return fail(cuda_fail(cudaGetLastError(), "ensemble event"));
