@@ -1120,9 +1120,17 @@ k_rowmax_four(MLayout in, const float *wgt, float *Mf) {
   if (e >= sP + sD) return;
   const float *x = (e < sP) ? in.P + (size_t)m * in.nth * sP + e : in.D + (size_t)m * in.nth * sD + (e - sP);
   const size_t st = (e < sP) ? sP : sD;
+  // 16 colatitudes per pass, all their loads in flight together
   float mx = 0.0f;
-#pragma unroll 8
-  for (int th = 0; th < in.nth; th++) mx = fmaxf(mx, fabsf(__ldg(x + (size_t)th * st)) * __ldg(wgt + th));
+  int th = 0;
+  for (; th + 16 <= in.nth; th += 16) {
+    float v[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) v[u] = __ldg(x + (size_t)(th + u) * st);
+#pragma unroll
+    for (int u = 0; u < 16; u++) mx = fmaxf(mx, fabsf(v[u]) * __ldg(wgt + th + u));
+  }
+  for (; th < in.nth; th++) mx = fmaxf(mx, fabsf(__ldg(x + (size_t)th * st)) * __ldg(wgt + th));
   Mf[(size_t)m * (sP + sD) + e] = 2.0f * mx;
 }
 
