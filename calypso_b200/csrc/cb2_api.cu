@@ -281,7 +281,7 @@ int cb2_destroy(cb2_ctx *c) {
   closure_free(*c);
   free_tables(*c);
   void *ptrs[] = {c->d_lu_vp, c->d_lu_vt, c->d_lu_bs, c->d_lu_bt, c->d_lu_t, c->d_pv_vp, c->d_pv_vt,
-                  c->d_pv_bs, c->d_pv_bt, c->d_pv_t, c->d_status, c->d_tw_fft, c->d_tw_fft32, c->d_twp32, c->d_twf4,
+                  c->d_pv_bs, c->d_pv_bt, c->d_pv_t, c->d_status, c->d_tw_fft, c->d_tw_fft32, c->d_twp32, c->d_twf4, c->d_imp_map,
                   c->d_f, c->d_four, c->d_four2, c->d_ene, c->d_tmp, c->d_host_state};
   for (void *q : ptrs)
     if (q) cudaFree(q);

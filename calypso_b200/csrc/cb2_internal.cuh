@@ -83,6 +83,10 @@ struct Ctx {
   double *d_sw = nullptr, *d_tw = nullptr;       // [6][jmax], [8][jmax]
   double *d_lu_vp = nullptr, *d_lu_vt = nullptr, *d_lu_bs = nullptr, *d_lu_bt = nullptr, *d_lu_t = nullptr;
   int *d_pv_vp = nullptr, *d_pv_vt = nullptr, *d_pv_bs = nullptr, *d_pv_bt = nullptr, *d_pv_t = nullptr;
+  // implicit-solve blocks: int4 (sign, m0, l0, -) tiles of consecutive
+  // degrees x orders, imp_slots of them
+  int *d_imp_map = nullptr;
+  int imp_slots = 0;
   int *d_status = nullptr;               // device error word
   double *d_tw_fft = nullptr;            // exp(-2 pi i e / nph), e = 0..nph-1
   float *d_tw_fft32 = nullptr;

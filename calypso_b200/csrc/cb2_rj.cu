@@ -270,6 +270,18 @@ __global__ void k_interleave_l(const T *src, T *dst, int nl, int w, int n) {
   dst[e] = src[(size_t)l * w * n + re];
 }
 
+// implicit solve: blocks of IMP_LD degrees x IMP_MD orders; band factors of
+// the block's degrees in shared memory
+constexpr int IMP_LD = 8, IMP_MD = 16;
+struct ImpLU {
+  const double *lu[5];   // fields 0 (5-band), 1-4 (3-band), degree-interleaved
+  const int *pv[5];
+};
+static size_t imp_smem(int n, int w) { return (size_t)n * w * IMP_LD * sizeof(double) + (size_t)n * IMP_LD * sizeof(int); }
+struct Fields;
+template <int W>
+__global__ void k_implicit(RJArgs a, Fields F, ImpLU lup, const int *moff, const int4 *tiles);
+
 int rj_lu_factorise(Ctx &c) {
   int n = c.nr, L = c.L;
   size_t per = (size_t)(18 * n + 2 * (n + 1));
@@ -307,6 +319,30 @@ int rj_lu_factorise(Ctx &c) {
     }
     CB2_CUDA(cudaGetLastError());
   }
+  // implicit-solve blocks: (sign, m0, l0) tiles of IMP_LD degrees x IMP_MD
+  // orders that hold at least one (l, m) of the sign
+  {
+    std::vector<int4> tl;
+    for (int s = 0; s < 2; s++)
+      for (int m0 = 0; m0 <= L; m0 += IMP_MD)
+        for (int l0 = 0; l0 <= L; l0 += IMP_LD) {
+          bool any = false;
+          for (int q = 0; q < IMP_LD * IMP_MD && !any; q++) {
+            const int l = l0 + q % IMP_LD, m = m0 + q / IMP_LD;
+            any = l <= L && m <= l && !(s == 1 && m == 0);
+          }
+          if (any) tl.push_back(int4{s, m0, l0, 0});
+        }
+    c.imp_slots = (int)tl.size();
+    CB2_CUDA(cudaMalloc(&c.d_imp_map, tl.size() * sizeof(int4)));
+    CB2_CUDA(cudaMemcpyAsync(c.d_imp_map, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice, c.stream));
+    CB2_CUDA(raise_smem_limit(k_implicit<9>, imp_smem(n, 9)));
+    CB2_CUDA(raise_smem_limit(k_implicit<5>, imp_smem(n, 5)));
+    if (imp_smem(n, 9) > 227 * 1024) {
+      set_error("too many radial levels for the implicit solve's shared-memory band factors");
+      return CB2_ERR_ARG;
+    }
+  }
   int st = 0;
   CB2_CUDA(cudaMemcpyAsync(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   CB2_CUDA(cudaStreamSynchronize(c.stream));
@@ -327,9 +363,9 @@ int rj_lu_factorise(Ctx &c) {
 // U x = y.  The recurrence is carried in registers and the column streamed
 // in chunks of PF rows, the loads of the next chunk issued before the stores
 // of this one, so a sweep waits on memory once per chunk rather than once
-// per row; the band factors come through the read-only path and the
-// divisions by the diagonal of U become multiplications by its reciprocal
-// (off the dependency chain).
+// per row; the band factors come from the block's shared-memory copy
+// (k_implicit stages them) and the divisions by the diagonal of U become
+// multiplications by its reciprocal (off the dependency chain).
 // band factors in the degree-interleaved layout: lu = base + l, entry b of
 // row c at lu[((c - 1) * width + b - 1) * nl]
 #define M5I(a, b, c) (a)[(size_t)(((c) - 1) * 5 + ((b) - 1)) * nl]
@@ -339,7 +375,7 @@ constexpr int PF = 8;
 
 __device__ static void d_pivots(int n, const int *piv, int nl, double *x, size_t stride) {
   for (int i = 1; i <= n; i++) {
-    const int ll = __ldg(piv + (size_t)(i - 1) * nl);
+    const int ll = piv[(size_t)(i - 1) * nl];
     if (ll != i) { const double s = XC(ll); XC(ll) = XC(i); XC(i) = s; }
   }
 }
@@ -358,7 +394,7 @@ __device__ __forceinline__ void d_chunk(const double *x, size_t stride, int n, i
 __device__ static void d_solve_3band(int n, const double *lu, const int *piv, int nl, double *x, size_t stride) {
   d_pivots(n, piv, nl, x, stride);
   // forward: L y = P b
-  double ym2 = XC(1), ym1 = XC(2) - __ldg(&M5I(lu, 4, 1)) * ym2;
+  double ym2 = XC(1), ym1 = XC(2) - (M5I(lu, 4, 1)) * ym2;
   XC(2) = ym1;
   double buf[PF], nb[PF];
   d_chunk<1>(x, stride, n, 3, buf);
@@ -368,7 +404,7 @@ __device__ static void d_solve_3band(int n, const double *lu, const int *piv, in
     for (int u = 0; u < PF; u++) {
       const int i = i0 + u;
       if (i <= n) {
-        const double y = buf[u] - __ldg(&M5I(lu, 5, i - 2)) * ym2 - __ldg(&M5I(lu, 4, i - 1)) * ym1;
+        const double y = buf[u] - (M5I(lu, 5, i - 2)) * ym2 - (M5I(lu, 4, i - 1)) * ym1;
         XC(i) = y;
         ym2 = ym1; ym1 = y;
       }
@@ -377,9 +413,9 @@ __device__ static void d_solve_3band(int n, const double *lu, const int *piv, in
     for (int u = 0; u < PF; u++) buf[u] = nb[u];
   }
   // backward: U x = y
-  double xp2 = ym1 * (1.0 / __ldg(&M5I(lu, 3, n)));
+  double xp2 = ym1 * (1.0 / (M5I(lu, 3, n)));
   const double yn1 = XC(n - 1);
-  double xp1 = (yn1 - __ldg(&M5I(lu, 2, n)) * xp2) * (1.0 / __ldg(&M5I(lu, 3, n - 1)));
+  double xp1 = (yn1 - (M5I(lu, 2, n)) * xp2) * (1.0 / (M5I(lu, 3, n - 1)));
   d_chunk<-1>(x, stride, n, n - 2, buf);
   XC(n) = xp2;
   XC(n - 1) = xp1;
@@ -389,8 +425,8 @@ __device__ static void d_solve_3band(int n, const double *lu, const int *piv, in
     for (int u = 0; u < PF; u++) {
       const int i = i0 - u;
       if (i >= 1) {
-        const double v = (buf[u] - __ldg(&M5I(lu, 2, i + 1)) * xp1 - __ldg(&M5I(lu, 1, i + 2)) * xp2) *
-                         (1.0 / __ldg(&M5I(lu, 3, i)));
+        const double v = (buf[u] - (M5I(lu, 2, i + 1)) * xp1 - (M5I(lu, 1, i + 2)) * xp2) *
+                         (1.0 / (M5I(lu, 3, i)));
         XC(i) = v;
         xp2 = xp1; xp1 = v;
       }
@@ -404,9 +440,9 @@ __device__ static void d_solve_5band(int n, const double *lu, const int *piv, in
   d_pivots(n, piv, nl, x, stride);
   // forward: L y = P b
   double y1 = XC(1);
-  double y2 = XC(2) - __ldg(&M9I(lu, 6, 1)) * y1;
-  double y3 = XC(3) - __ldg(&M9I(lu, 7, 1)) * y1 - __ldg(&M9I(lu, 6, 2)) * y2;
-  double y4 = XC(4) - __ldg(&M9I(lu, 8, 1)) * y1 - __ldg(&M9I(lu, 7, 2)) * y2 - __ldg(&M9I(lu, 6, 3)) * y3;
+  double y2 = XC(2) - (M9I(lu, 6, 1)) * y1;
+  double y3 = XC(3) - (M9I(lu, 7, 1)) * y1 - (M9I(lu, 6, 2)) * y2;
+  double y4 = XC(4) - (M9I(lu, 8, 1)) * y1 - (M9I(lu, 7, 2)) * y2 - (M9I(lu, 6, 3)) * y3;
   double buf[PF], nb[PF];
   d_chunk<1>(x, stride, n, 5, buf);
   XC(2) = y2; XC(3) = y3; XC(4) = y4;
@@ -416,8 +452,8 @@ __device__ static void d_solve_5band(int n, const double *lu, const int *piv, in
     for (int u = 0; u < PF; u++) {
       const int i = i0 + u;
       if (i <= n) {
-        const double y = buf[u] - __ldg(&M9I(lu, 9, i - 4)) * y1 - __ldg(&M9I(lu, 8, i - 3)) * y2
-                       - __ldg(&M9I(lu, 7, i - 2)) * y3 - __ldg(&M9I(lu, 6, i - 1)) * y4;
+        const double y = buf[u] - (M9I(lu, 9, i - 4)) * y1 - (M9I(lu, 8, i - 3)) * y2
+                       - (M9I(lu, 7, i - 2)) * y3 - (M9I(lu, 6, i - 1)) * y4;
         XC(i) = y;
         y1 = y2; y2 = y3; y3 = y4; y4 = y;
       }
@@ -427,12 +463,12 @@ __device__ static void d_solve_5band(int n, const double *lu, const int *piv, in
   }
   // backward: U x = y (y4 = y(n))
   const double b1 = XC(n - 1), b2 = XC(n - 2), b3 = XC(n - 3);
-  const double x0 = y4 * (1.0 / __ldg(&M9I(lu, 5, n)));
-  const double xm1 = (b1 - __ldg(&M9I(lu, 4, n)) * x0) * (1.0 / __ldg(&M9I(lu, 5, n - 1)));
-  const double xm2 = (b2 - __ldg(&M9I(lu, 4, n - 1)) * xm1 - __ldg(&M9I(lu, 3, n)) * x0) *
-                     (1.0 / __ldg(&M9I(lu, 5, n - 2)));
-  const double xm3 = (b3 - __ldg(&M9I(lu, 4, n - 2)) * xm2 - __ldg(&M9I(lu, 3, n - 1)) * xm1
-                      - __ldg(&M9I(lu, 2, n)) * x0) * (1.0 / __ldg(&M9I(lu, 5, n - 3)));
+  const double x0 = y4 * (1.0 / (M9I(lu, 5, n)));
+  const double xm1 = (b1 - (M9I(lu, 4, n)) * x0) * (1.0 / (M9I(lu, 5, n - 1)));
+  const double xm2 = (b2 - (M9I(lu, 4, n - 1)) * xm1 - (M9I(lu, 3, n)) * x0) *
+                     (1.0 / (M9I(lu, 5, n - 2)));
+  const double xm3 = (b3 - (M9I(lu, 4, n - 2)) * xm2 - (M9I(lu, 3, n - 1)) * xm1
+                      - (M9I(lu, 2, n)) * x0) * (1.0 / (M9I(lu, 5, n - 3)));
   d_chunk<-1>(x, stride, n, n - 4, buf);
   XC(n) = x0; XC(n - 1) = xm1; XC(n - 2) = xm2; XC(n - 3) = xm3;
   double p1 = xm3, p2 = xm2, p3 = xm1, p4 = x0;   // x(i+1) .. x(i+4)
@@ -442,9 +478,9 @@ __device__ static void d_solve_5band(int n, const double *lu, const int *piv, in
     for (int u = 0; u < PF; u++) {
       const int i = i0 - u;
       if (i >= 1) {
-        const double v = (buf[u] - __ldg(&M9I(lu, 4, i + 1)) * p1 - __ldg(&M9I(lu, 3, i + 2)) * p2
-                          - __ldg(&M9I(lu, 2, i + 3)) * p3 - __ldg(&M9I(lu, 1, i + 4)) * p4) *
-                         (1.0 / __ldg(&M9I(lu, 5, i)));
+        const double v = (buf[u] - (M9I(lu, 4, i + 1)) * p1 - (M9I(lu, 3, i + 2)) * p2
+                          - (M9I(lu, 2, i + 3)) * p3 - (M9I(lu, 1, i + 4)) * p4) *
+                         (1.0 / (M9I(lu, 5, i)));
         XC(i) = v;
         p4 = p3; p3 = p2; p2 = p1; p1 = v;
       }
@@ -501,15 +537,36 @@ __global__ void k_explicit(RJArgs a, Fields F, int euler) {
 __device__ inline double icb_fld(const RJArgs &a, int jj) { return jj == 0 ? a.temp_icb_fld : 0.0; }
 __device__ inline double cmb_fld(const RJArgs &a, int jj) { return jj == 0 ? a.temp_cmb_fld : 0.0; }
 
-// Crank-Nicolson solves: one thread per (field, (l, m) column); the five
-// solves of a column are independent (blockIdx.y picks the field)
-__global__ void k_implicit(RJArgs a, Fields F, const double *lu_vp, const int *pv_vp,
-                           const double *lu_vt, const int *pv_vt, const double *lu_bs,
-                           const int *pv_bs, const double *lu_bt, const int *pv_bt,
-                           const double *lu_t, const int *pv_t) {
-  const int jj = blockIdx.x * blockDim.x + threadIdx.x;
-  if (jj >= a.jmax) return;
-  const int n = a.nr, l = a.jl[jj], fld = blockIdx.y, nl = a.L + 1;   // factors interleaved by degree
+// Crank-Nicolson solves: one thread per (field, (l, m) column).  A block
+// holds IMP_LD consecutive degrees x IMP_MD orders of one sign; it first
+// stages the band factors and pivots of its IMP_LD degrees in shared memory
+// (interleaved by degree, loaded together), so every factor a thread needs in
+// its sweeps is a shared-memory read.  W = 9: the 5-band poloidal velocity
+// (field 0); W = 5: the 3-band systems (fields 1-4, blockIdx.y + 1).
+template <int W>
+__global__ void __launch_bounds__(IMP_LD * IMP_MD)
+k_implicit(RJArgs a, Fields F, ImpLU lup, const int *moff, const int4 *tiles) {
+  extern __shared__ double lus[];                                   // [n * W][IMP_LD]
+  const int n = a.nr, nl = a.L + 1, tid = threadIdx.x;
+  int *pvs = reinterpret_cast<int *>(lus + (size_t)n * W * IMP_LD);  // [n][IMP_LD]
+  const int4 tl = tiles[blockIdx.x];                                // (sign, m0, l0, -)
+  const int fld = (W == 9) ? 0 : 1 + blockIdx.y;
+  const double *lug = lup.lu[fld];
+  const int *pvg = lup.pv[fld];
+  for (int e = tid; e < n * W * IMP_LD; e += IMP_LD * IMP_MD) {
+    const int lo = e % IMP_LD, l = tl.z + lo;
+    lus[e] = (l < nl) ? __ldg(lug + (size_t)(e / IMP_LD) * nl + l) : 1.0;
+  }
+  for (int e = tid; e < n * IMP_LD; e += IMP_LD * IMP_MD) {
+    const int lo = e % IMP_LD, l = tl.z + lo, row = e / IMP_LD;
+    pvs[e] = (l < nl) ? __ldg(pvg + (size_t)row * nl + l) : row + 1;
+  }
+  __syncthreads();
+  const int lo = tid % IMP_LD, l = tl.z + lo, m = tl.y + tid / IMP_LD, sgn = tl.x;
+  if (l >= nl || m > l || (sgn == 1 && m == 0)) return;
+  const int jj = moff[m] + sgn * (nl - m) + (l - m);
+  const double *lu = lus + lo;
+  const int *pv = pvs + lo;
   const size_t st = a.jmax;
   if (fld < 2) {
     // velocity from vorticity: S <- tor(w), T <- pol(w); l = 0 removed; walls zero
@@ -533,30 +590,32 @@ __global__ void k_implicit(RJArgs a, Fields F, const double *lu_vp, const int *p
         }
       }
     }
-    if (fld == 0) d_solve_5band(n, lu_vp + l, pv_vp + l, nl, u, st);
-    else d_solve_3band(n, lu_vt + l, pv_vt + l, nl, u, st);
-  } else if (fld == 2) {
-    // temperature with fixed wall values
-    double *T = F(TEMP) + jj;
-    for (int k = a.kout; k < n; k++) T[k * st] = cmb_fld(a, jj);
-    for (int k = 0; k <= a.kin; k++) T[k * st] = icb_fld(a, jj);
-    d_solve_3band(n, lu_t + l, pv_t + l, nl, T, st);
-  } else if (fld == 3) {
-    // poloidal magnetic field, insulating walls, l = 0 removed
-    double *bS = F(MAGNE) + jj, *bdS = F(MAGNE + 1) + jj;
-    if (jj == 0)
-      for (int k = 0; k < n; k++) bS[k * st] = 0.0;
-    bdS[a.kin * st] = (a.gl[jj] + 1.0) * a.bc.r_icb[1] * bS[a.kin * st];
-    bdS[a.kout * st] = -a.gl[jj] * a.bc.r_cmb[1] * bS[a.kout * st];
-    d_solve_3band(n, lu_bs + l, pv_bs + l, nl, bS, st);
-  } else {
-    // toroidal magnetic field, zero at the walls
-    double *bT = F(MAGNE + 2) + jj;
-    if (jj == 0)
-      for (int k = 0; k < n; k++) bT[k * st] = 0.0;
-    bT[a.kin * st] = 0.0;
-    bT[a.kout * st] = 0.0;
-    d_solve_3band(n, lu_bt + l, pv_bt + l, nl, bT, st);
+    if constexpr (W == 9) d_solve_5band(n, lu, pv, IMP_LD, u, st);
+    else d_solve_3band(n, lu, pv, IMP_LD, u, st);
+  } else if constexpr (W == 5) {
+    if (fld == 2) {
+      // temperature with fixed wall values
+      double *T = F(TEMP) + jj;
+      for (int k = a.kout; k < n; k++) T[k * st] = cmb_fld(a, jj);
+      for (int k = 0; k <= a.kin; k++) T[k * st] = icb_fld(a, jj);
+      d_solve_3band(n, lu, pv, IMP_LD, T, st);
+    } else if (fld == 3) {
+      // poloidal magnetic field, insulating walls, l = 0 removed
+      double *bS = F(MAGNE) + jj, *bdS = F(MAGNE + 1) + jj;
+      if (jj == 0)
+        for (int k = 0; k < n; k++) bS[k * st] = 0.0;
+      bdS[a.kin * st] = (a.gl[jj] + 1.0) * a.bc.r_icb[1] * bS[a.kin * st];
+      bdS[a.kout * st] = -a.gl[jj] * a.bc.r_cmb[1] * bS[a.kout * st];
+      d_solve_3band(n, lu, pv, IMP_LD, bS, st);
+    } else {
+      // toroidal magnetic field, zero at the walls
+      double *bT = F(MAGNE + 2) + jj;
+      if (jj == 0)
+        for (int k = 0; k < n; k++) bT[k * st] = 0.0;
+      bT[a.kin * st] = 0.0;
+      bT[a.kout * st] = 0.0;
+      d_solve_3band(n, lu, pv, IMP_LD, bT, st);
+    }
   }
 }
 
@@ -869,9 +928,12 @@ void rj_explicit(Ctx &c, bool euler) {
 
 void rj_implicit(Ctx &c) {
   RJArgs a = c.rj_args();
-  k_implicit<<<dim3(cdiv(c.jmax, 128), 5), 128, 0, c.stream>>>(a, fields(c), c.d_lu_vp, c.d_pv_vp, c.d_lu_vt,
-                                                      c.d_pv_vt, c.d_lu_bs, c.d_pv_bs, c.d_lu_bt,
-                                                      c.d_pv_bt, c.d_lu_t, c.d_pv_t);
+  const ImpLU lup{{c.d_lu_vp, c.d_lu_vt, c.d_lu_t, c.d_lu_bs, c.d_lu_bt},
+                  {c.d_pv_vp, c.d_pv_vt, c.d_pv_t, c.d_pv_bs, c.d_pv_bt}};
+  const int4 *tiles = reinterpret_cast<const int4 *>(c.d_imp_map);
+  k_implicit<9><<<c.imp_slots, IMP_LD * IMP_MD, imp_smem(c.nr, 9), c.stream>>>(a, fields(c), lup, c.d_moff, tiles);
+  k_implicit<5><<<dim3(c.imp_slots, 4), IMP_LD * IMP_MD, imp_smem(c.nr, 5), c.stream>>>(a, fields(c), lup,
+                                                                                        c.d_moff, tiles);
   k_derived_a<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(a, fields(c));
   k_derived_b<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(a, fields(c));
 }
