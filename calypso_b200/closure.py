@@ -8,7 +8,7 @@ low-resolution solver computes from the filtered state.  The network is
 trained on the GPU by the library's own forward / backward / Adam kernels;
 torch tensors only hold the device buffers.  The plain low-resolution
 solver is the fallback (detach the closure) and, against the filtered
-high-resolution run, the judge of the closure's error.
+high-resolution run, the yardstick of the closure's error.
 """
 from __future__ import annotations
 

@@ -64,7 +64,7 @@ def run(small: bool = False, spin: int = 200, epochs: int = 4, horizon: int = 50
     r2_train = closure.explained(net, norm, xtr[-n_test:], ytr[-n_test:])
     r2_test = closure.explained(net, norm, xte, yte)
 
-    def judge_from_current(alist):
+    def errors_from_current(alist):
         """spectra errors after `horizon` steps from the current hi state:
         low-resolution rollouts from its filtered state against the filtered
         high-resolution state `horizon` steps later"""
@@ -80,10 +80,10 @@ def run(small: bool = False, spin: int = 200, epochs: int = 4, horizon: int = 50
         return out
 
     # validation rollout picks the relaxation (0 = the plain solver, the fallback)
-    val = judge_from_current((0.0,) + tuple(alphas))
+    val = errors_from_current((0.0,) + tuple(alphas))
     best = min(val, key=val.get)
     hi.step(every * 4, graph=True)
-    test = judge_from_current((0.0, best) if best > 0 else (0.0,))
+    test = errors_from_current((0.0, best) if best > 0 else (0.0,))
     return {
         "experiment": "closure_small" if small else "closure_L255_to_L63",
         "hi": {"L": p_hi["ltr"], "Nr": p_hi["nr"]}, "lo": {"L": p_lo["ltr"], "Nr": p_lo["nr"]},

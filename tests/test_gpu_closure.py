@@ -95,7 +95,7 @@ def test_closure_attach_detach():
 
 
 def test_closure_beats_plain_low_resolution_rollout():
-    # the plain low-resolution solver is the judge: from a filtered
+    # the plain low-resolution solver is the yardstick: from a filtered
     # high-resolution state, 40 steps with the closure (relaxation 0.5) end
     # with kinetic and magnetic energy spectra closer to the filtered
     # high-resolution run than 40 plain steps do (deterministic: seeded data,
