@@ -336,12 +336,12 @@ int rj_lu_factorise(Ctx &c) {
     c.imp_slots = (int)tl.size();
     CB2_CUDA(cudaMalloc(&c.d_imp_map, tl.size() * sizeof(int4)));
     CB2_CUDA(cudaMemcpyAsync(c.d_imp_map, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice, c.stream));
-    CB2_CUDA(raise_smem_limit(k_implicit<9>, imp_smem(n, 9)));
-    CB2_CUDA(raise_smem_limit(k_implicit<5>, imp_smem(n, 5)));
     if (imp_smem(n, 9) > 227 * 1024) {
       set_error("too many radial levels for the implicit solve's shared-memory band factors");
       return CB2_ERR_ARG;
     }
+    CB2_CUDA(raise_smem_limit(k_implicit<9>, imp_smem(n, 9)));
+    CB2_CUDA(raise_smem_limit(k_implicit<5>, imp_smem(n, 5)));
   }
   int st = 0;
   CB2_CUDA(cudaMemcpyAsync(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
