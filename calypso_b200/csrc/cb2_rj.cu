@@ -337,6 +337,8 @@ int rj_lu_factorise(Ctx &c) {
     CB2_CUDA(cudaMalloc(&c.d_imp_map, tl.size() * sizeof(int4)));
     CB2_CUDA(cudaMemcpyAsync(c.d_imp_map, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice, c.stream));
     if (imp_smem(n, 9) > 227 * 1024) {
+      cudaStreamSynchronize(c.stream);
+      cudaFree(work);
       set_error("too many radial levels for the implicit solve's shared-memory band factors");
       return CB2_ERR_ARG;
     }
