@@ -353,7 +353,12 @@ def main():
                        "tuning": list(tuning)},
             "roofline": roof, "stages_ms": stages, "cpu_baseline": cpu, "e2e": e2e,
             "fp64_plain": fp64,
-            "gpu_launches": (12 if prec == PREC_MIXED else 10) * args.steps, "clocks": clocks,
+            # kernels per step: explicit; implicit (5-band, 3-band) and two
+            # derived-field kernels; Coriolis; backward Legendre (pack + GEMM
+            # when mixed); FFT + products; forward Legendre (row maxima + GEMM
+            # when mixed); after-transform; reference-temperature shift
+            "gpu_launches": ((13 if prec == PREC_MIXED else 11) - (0 if params.get("use_ref_temp", 0) else 1))
+                            * args.steps, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
