@@ -123,6 +123,22 @@ def legendre_flops(L, nr, nth, nvec_b=4, nscal_b=1, nvec_f=4, nscal_f=0):
     return (5 * nvec_b + nscal_b) * U, (5 * nvec_f + nscal_f) * U
 
 
+def max_over_ranks(ms, dist, device):
+    """The job's time: the largest per-rank device time (replicas that share
+    no data still finish together only when the slowest does)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(ms, steps, world):
+    """Whole-job steps/s: every replica advances its own shell `steps` times."""
+    return world * steps / (ms / 1000.0)
+
+
 def run_reference(args, params):
     """The reference's algorithm on the host cores (oracle port), rank 0 only."""
     rank, _, world = env_rank()
@@ -146,7 +162,7 @@ def run_reference(args, params):
         "warmup": args.warmup, "ms_per_step": 1000.0 * dt / nt, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: seeded thermal perturbation (l<=8) + dipole seed field",
-        "config": {"workload": WORKLOAD, "L": p["ltr"], "Nr": p["nr"], "Ntheta": p["nth"],
+        "config": {"workload": args.workload, "L": p["ltr"], "Nr": p["nr"], "Ntheta": p["nth"],
                    "Nphi": p["nph"], "precision": "fp64 (CPU)", "parallelism": "openmp"},
         "impl": "reference",
         "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": "port",
@@ -214,12 +230,8 @@ def main():
     ms = g.time_steps(args.steps, graph=True)
     barrier()
     clocks = clock.stop()
-    if dist is not None:
-        import torch
-        t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms / 1000.0)
+    ms = max_over_ranks(ms, dist, f"cuda:{local_rank}")
+    value = job_value(ms, args.steps, world)
 
     # stage breakdown (eager steps with per-stage CUDA events, not the timed run)
     os.environ["CB2_TIMERS"] = "1"
