@@ -248,9 +248,12 @@ def main():
     L, nr, nth, nph = params["ltr"], params["nr"], params["nth"], params["nph"]
     fb, ff = legendre_flops(L, nr, nth)
     peaks, peak_kind = load_peaks()
-    stages = {"explicit": st[6], "implicit+rj_derived": st[7], "coriolis": st[13],
+    fused_cn = tuning[4] == 1
+    stages = ({"cn_step": st[6] + st[7]} if fused_cn else
+              {"explicit": st[6], "implicit+rj_derived": st[7]})
+    stages.update({"coriolis": st[13],
               "legendre_bwd": st[22], "fft_products": st[24], "legendre_fwd": st[23],
-              "rj_after_transform": st[17], "step": st[0]}
+              "rj_after_transform": st[17], "step": st[0]})
     # dominant transform stage and its roofline.  Algorithmic bytes: one read
     # of each input and one write of each output (13 spectral slots and 13
     # Fourier components backward, 12 each forward); algorithmic flops:
@@ -365,12 +368,14 @@ def main():
                        "tuning": list(tuning)},
             "roofline": roof, "stages_ms": stages, "cpu_baseline": cpu, "e2e": e2e,
             "fp64_plain": fp64,
-            # kernels per step: explicit; implicit (5-band, 3-band) and two
-            # derived-field kernels; Coriolis; backward Legendre (pack + GEMM
-            # when mixed); FFT + products; forward Legendre (row maxima + GEMM
-            # when mixed); after-transform; reference-temperature shift
-            "gpu_launches": ((13 if prec == PREC_MIXED else 11) - (0 if params.get("use_ref_temp", 0) else 1))
-                            * args.steps, "clocks": clocks,
+            # kernels per step: the Crank-Nicolson stage (one fused kernel, or
+            # explicit, implicit 5-band and 3-band, two derived-field kernels);
+            # Coriolis; backward Legendre (pack + GEMM when mixed); FFT +
+            # products; forward Legendre (row maxima + GEMM when mixed);
+            # after-transform; reference-temperature shift
+            "gpu_launches": ((13 if prec == PREC_MIXED else 11) - (4 if fused_cn else 0)
+                             - (0 if params.get("use_ref_temp", 0) else 1)) * args.steps,
+            "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

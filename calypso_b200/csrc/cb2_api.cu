@@ -158,9 +158,15 @@ static void temp_roundtrip(Ctx &c) {
 int step_once(Ctx &c) {
   c.istep += 1;
   if (c.timers) cudaEventRecord(c.ev[0], c.stream);
-  rj_explicit(c, c.istep == 1);
-  if (c.timers) cudaEventRecord(c.ev[1], c.stream);
-  rj_implicit(c);
+  if (c.cn_ready && c.tune[TUNE_CN] == 1) {
+    // explicit update, solves and derived fields in one kernel
+    if (c.timers) cudaEventRecord(c.ev[1], c.stream);
+    cn_step(c, c.istep == 1);
+  } else {
+    rj_explicit(c, c.istep == 1);
+    if (c.timers) cudaEventRecord(c.ev[1], c.stream);
+    rj_implicit(c);
+  }
   if (c.timers) cudaEventRecord(c.ev[2], c.stream);
   int rc = nonlinear(c);
   temp_roundtrip(c);
@@ -251,6 +257,7 @@ int cb2_create(const cb2_params *p, int precision, int device, cb2_ctx **out) {
   if (cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "cudaMalloc(status)"));
   if ((rc = setup_tables(*c))) return fail(rc);
   if ((rc = rj_lu_factorise(*c))) return fail(rc);
+  if ((rc = cn_setup(*c))) return fail(rc);
   if ((rc = fft_setup(*c))) return fail(rc);
   size_t fs = c->fsize();
   if (cudaMalloc(&c->d_f, (size_t)NSLOT * fs * sizeof(double)) != cudaSuccess)
@@ -279,10 +286,11 @@ int cb2_destroy(cb2_ctx *c) {
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->prec == CB2_PREC_MIXED) mixed_free(*c);
   closure_free(*c);
+  cn_free(*c);
   free_tables(*c);
   void *ptrs[] = {c->d_lu_vp, c->d_lu_vt, c->d_lu_bs, c->d_lu_bt, c->d_lu_t, c->d_pv_vp, c->d_pv_vt,
                   c->d_pv_bs, c->d_pv_bt, c->d_pv_t, c->d_status, c->d_tw_fft, c->d_tw_fft32, c->d_twp32, c->d_twf4, c->d_imp_map,
-                  c->d_f, c->d_four, c->d_four2, c->d_ene, c->d_tmp, c->d_host_state};
+                  c->d_cn_lu, c->d_cn_tiles, c->d_f, c->d_four, c->d_four2, c->d_ene, c->d_tmp, c->d_host_state};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (c->h_stage) cudaFreeHost(c->h_stage);

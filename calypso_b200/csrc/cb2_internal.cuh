@@ -87,6 +87,15 @@ struct Ctx {
   // degrees x orders, imp_slots of them
   int *d_imp_map = nullptr;
   int imp_slots = 0;
+  // fused Crank-Nicolson step (cb2_cn.cu): the factors in its forms (one
+  // allocation), int4 (field, m0, l0, -) block tiles, the kernel's view of
+  // the factors (CnPack), its shared memory; cn_ready when usable
+  double *d_cn_lu = nullptr;
+  int4 *d_cn_tiles = nullptr;
+  int cn_tiles = 0;
+  void *cn_pack = nullptr;
+  size_t cn_smem = 0;
+  bool cn_ready = false;
   int *d_status = nullptr;               // device error word
   double *d_tw_fft = nullptr;            // exp(-2 pi i e / nph), e = 0..nph-1
   float *d_tw_fft32 = nullptr;
@@ -167,6 +176,14 @@ void rj_temp_total(Ctx &c, double sign);
 int rj_energies(Ctx &c, double out[7]);
 int rj_energies_scratch(Ctx &c, double *scratch, double out[7]);
 int rj_lu_factorise(Ctx &c);
+// fused Crank-Nicolson step (cb2_cn.cu): set-up after rj_lu_factorise, and
+// the step (explicit update, solves, derived fields) when c.cn_ready
+int cn_setup(Ctx &c);
+void cn_step(Ctx &c, bool euler);
+void cn_free(Ctx &c);
+// the Crank-Nicolson stage as the tuning selects it: cn_step, or
+// rj_explicit + rj_implicit
+void cn_stage(Ctx &c, bool euler);
 // Fourier coefficients of the mixed-precision path, order-major so that one
 // Legendre GEMM row is one contiguous element.  For nvec vectors + nscal
 // scalars, at each (m, theta):
@@ -219,7 +236,10 @@ enum Tune {
   TUNE_PACK_KC = 2,      // mixed backward pack: radial levels per block (1, 2, 4)
   TUNE_FFT_THREADS = 3,  // mixed FFT + products: threads per row block; 384 = the four-step kernel
                          // (nphi = 3 (L + 1)), 128 / 256 / 512 = the Stockham kernel
-  TUNE_N = 4
+  TUNE_CN = 4,           // 1: explicit update, solves and derived fields in one kernel
+                         // (k_cn_step); 0: the separate kernels; -1: the one kernel
+                         // cannot take this context's factors (fixed)
+  TUNE_N = 5
 };
 // one time step (explicit, implicit, nonlinear); advances istep (cb2_api.cu)
 int step_once(Ctx &c);

@@ -69,6 +69,13 @@ static int stage_fft_mixed(Ctx &c) {
   return 0;
 }
 
+// the Crank-Nicolson stage of an Adams-Bashforth step, as the step runs it
+static int stage_cn(Ctx &c) {
+  cn_stage(c, false);
+  CB2_CUDA(cudaGetLastError());
+  return 0;
+}
+
 int autotune(Ctx &c) {
   struct Item {
     int which;
@@ -83,6 +90,7 @@ int autotune(Ctx &c) {
     items.push_back({TUNE_PACK_KC, {1, 2, 4}, stage_bwd_mixed});
     items.push_back({TUNE_FFT_THREADS, {384, 512, 256, 128}, stage_fft_mixed});
   }
+  if (c.cn_ready) items.push_back({TUNE_CN, {0, 1}, stage_cn});
   for (const Item &it : items) {
     int best = c.tune[it.which];
     float best_ms = 1e30f;
@@ -125,19 +133,20 @@ int cb2_autotune(cb2_ctx *c) {
   return autotune(*c);
 }
 
-int cb2_get_tuning(const cb2_ctx *c, int out[4]) {
+int cb2_get_tuning(const cb2_ctx *c, int out[TUNE_N]) {
   if (!c || !out) { set_error("cb2_get_tuning: null argument"); return CB2_ERR_ARG; }
   for (int q = 0; q < TUNE_N; q++) out[q] = c->tune[q];
   return 0;
 }
 
-int cb2_set_tuning(cb2_ctx *c, const int in[4]) {
+int cb2_set_tuning(cb2_ctx *c, const int in[TUNE_N]) {
   if (!c || !in) { set_error("cb2_set_tuning: null argument"); return CB2_ERR_ARG; }
   if (c->graph_exec) {
     set_error("cb2_set_tuning: the step graph is already captured");
     return CB2_ERR_STATE;
   }
-  for (int q = 0; q < TUNE_N; q++) c->tune[q] = in[q];
+  for (int q = 0; q < TUNE_N; q++)
+    if (q != TUNE_CN || c->cn_ready) c->tune[q] = in[q];
   return 0;
 }
 
@@ -188,7 +197,11 @@ int cb2_ensemble_create(const cb2_params *ps, int n, int precision, int device, 
       if (first_of[i] < 0) {
         if ((rc = autotune(*c))) return fail(rc);
       } else {
+        // the kernel shapes, and the fused Crank-Nicolson choice where this
+        // shell's factors allow it (same shape, possibly other operators)
+        const int cn = c->tune[TUNE_CN];
         std::memcpy(c->tune, e->shells[first_of[i]]->tune, sizeof(c->tune));
+        if (!c->cn_ready) c->tune[TUNE_CN] = cn;
       }
     }
   }

@@ -39,6 +39,12 @@ PREC_MIXED = 1
 # d_rj slots of the evolved fields
 VELO, VORT, MAGNE, CURRENT, TEMP = 0, 3, 6, 9, 12
 
+# kernel-variant tuning entries (cb2_get_tuning / cb2_set_tuning): float64
+# backward radial tile, float64 forward radial tile, mixed pack radial tile,
+# mixed FFT threads, fused Crank-Nicolson step (1) or separate kernels (0)
+TUNE_BWD_KT, TUNE_FWD_KT, TUNE_PACK_KC, TUNE_FFT_THREADS, TUNE_CN = range(5)
+TUNE_N = 5
+
 
 class CalypsoError(RuntimeError):
     pass
@@ -227,13 +233,16 @@ class SphMHD:
 
     @property
     def tuning(self) -> list:
-        out = (ctypes.c_int * 4)()
+        out = (ctypes.c_int * TUNE_N)()
         _check(load_library().cb2_get_tuning(self._h, out), "cb2_get_tuning")
         return list(out)
 
     @tuning.setter
     def tuning(self, values):
-        arr = (ctypes.c_int * 4)(*values)
+        # entries not given keep their current values
+        vals = list(values)
+        vals += self.tuning[len(vals):]
+        arr = (ctypes.c_int * TUNE_N)(*vals[:TUNE_N])
         _check(load_library().cb2_set_tuning(self._h, arr), "cb2_set_tuning")
 
     @property

@@ -164,13 +164,16 @@ int cb2_free_pinned(void *p);
  * which times its Legendre loop variants at start-up): times every
  * candidate tile / launch shape of the transform kernels on this context
  * and keeps the fastest.  Only before cb2_init_fields / cb2_start (it
- * overwrites the work fields).  tuning[4]: float64 backward radial tile,
+ * overwrites the work fields).  tuning[5]: float64 backward radial tile,
  * float64 forward radial tile, mixed pack radial tile, mixed FFT threads
  * (384: the four-step kernel, used where nphi = 3 (ltr + 1); 128, 256, 512:
- * the Stockham kernel). */
+ * the Stockham kernel), and 1 to run the explicit update, the radial solves
+ * and the derived fields of the step as one kernel, 0 (the default) as
+ * separate kernels; -1 (fixed) where the one kernel cannot take the
+ * context's radial factors (a row interchange beyond two rows). */
 int cb2_autotune(cb2_ctx *ctx);
-int cb2_get_tuning(const cb2_ctx *ctx, int tuning[4]);
-int cb2_set_tuning(cb2_ctx *ctx, const int tuning[4]);
+int cb2_get_tuning(const cb2_ctx *ctx, int tuning[5]);
+int cb2_set_tuning(cb2_ctx *ctx, const int tuning[5]);
 
 /* Ensemble of independent shells (any mix of truncations and parameters),
  * advanced together: one CUDA graph holds a time step of every shell as
