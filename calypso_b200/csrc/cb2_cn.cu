@@ -39,8 +39,8 @@
 namespace cb2 {
 
 constexpr int CN_THREADS = 256;   // a block: LD degrees x 128 / LD orders x both signs of m
-constexpr int CN_PF = 4;          // forward sweep: rows per batch of loads
-constexpr int CN_PB = 4;          // backward sweep: rows per batch of loads
+constexpr int CN_RING = 6;        // rows each thread keeps in flight (cp.async ring)
+constexpr int CN_RV = 4;          // values per ring slot (forward: X, D, F, P; backward: y)
 
 // Forms of one field's factors.  Per row i: NL multipliers L(i,i-1) ..
 // L(i,i-NL), NL superdiagonals U(i,i+1) .. U(i,i+NL), then 1 / U(i,i);
@@ -50,13 +50,18 @@ enum CnForm { CN_N5 = 0, CN_W5 = 1, CN_N3 = 2, CN_W3 = 3 };
 __host__ __device__ constexpr int cn_nl(int f) { return f == CN_N5 ? 2 : f == CN_W5 ? 4 : f == CN_N3 ? 1 : 2; }
 __host__ __device__ constexpr int cn_pd(int f) { return f == CN_W5 ? 2 : f == CN_W3 ? 1 : 0; }
 __host__ __device__ constexpr int cn_entries(int f) { return 2 * cn_nl(f) + 1; }
-// degrees per block: 4 for the widest form, so that its factors leave room
-// for 3 blocks per SM
+// degrees per block: 4 for the widest form, so that its factors and the
+// rings leave room for 2 blocks per SM
 __host__ __device__ constexpr int cn_ld(int f) { return f == CN_W5 ? 4 : 8; }
 
-static size_t cn_smem_form(int n, int f) {
+// shared memory of a block: radial coefficients, the factors of its
+// degrees, their interchange offsets, and the per-thread rings
+__host__ __device__ inline size_t cn_ring_offset(int n, int f) {
   return 9 * (size_t)n * sizeof(double) + (size_t)n * cn_entries(f) * cn_ld(f) * sizeof(double) +
          ((cn_pd(f) ? (size_t)n * cn_ld(f) : 0) + 15) / 16 * 16;
+}
+static size_t cn_smem_form(int n, int f) {
+  return cn_ring_offset(n, f) + (size_t)CN_RING * CN_RV * CN_THREADS * sizeof(double);
 }
 
 struct LuSet {
@@ -70,6 +75,14 @@ struct CnPack {
   const double *fac[5];
   const unsigned char *piv[5];
   int form[5];
+};
+
+// host side: the pack, each field's first tile (tile0[5] = all tiles) and
+// its launch's shared memory
+struct CnHost {
+  CnPack pk;
+  int tile0[6];
+  size_t smem[5];
 };
 
 // entry b (1-based) of band column c (1-based) of one degree's factors
@@ -143,23 +156,35 @@ struct RadCo {
   }
 };
 
-// one column of one slot: element k at p[k * st] (k * st < 2^31).  ldcs /
-// stcs: streamed once (evict-first); ldkeep / stkeep: the forward sweep's y,
-// read back by the backward sweep, held in L2 with an evict-last policy
+// one column of one slot: element k at p[k * st] (k * st < 2^31).  stcs:
+// written once (evict-first); stkeep: the forward sweep's y, read back by
+// the backward sweep, held in L2 with an evict-last policy
 struct Col {
   double *p;
-  __device__ double ldcs(int k, unsigned st) const { return __ldcs(p + (unsigned)k * st); }
   __device__ void stcs(int k, unsigned s, double v) const { __stcs(p + (unsigned)k * s, v); }
-  __device__ double ldkeep(int k, unsigned st, uint64_t pol) const {
-    double v;
-    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p + (unsigned)k * st), "l"(pol));
-    return v;
-  }
   __device__ void stkeep(int k, unsigned st, double v, uint64_t pol) const {
     asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p + (unsigned)k * st), "d"(v), "l"(pol)
                  : "memory");
   }
 };
+// 8-byte asynchronous copy global -> shared, and its group bookkeeping
+__device__ __forceinline__ void cp8(double *dst, const double *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// this thread's ring: slot s, value v at base[(s * CN_RV + v) * CN_THREADS]
+struct Ring {
+  double *base;
+  __device__ double *at(int s, int v) const { return base + (s * CN_RV + v) * CN_THREADS; }
+};
+
 __device__ __forceinline__ uint64_t l2_evict_last() {
   uint64_t pol;
   asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
@@ -189,10 +214,12 @@ struct CnCtx {
 // FLD: 0 poloidal velocity (from the toroidal vorticity), 1 toroidal
 // velocity (from the poloidal vorticity), 2 temperature, 3 poloidal and
 // 4 toroidal magnetic field.  fac: the column's factors in shared memory
-// (row stride NE * LD), pv: its interchange offsets (row stride LD).
+// (row stride NE * LD), pv: its interchange offsets (row stride LD).  The
+// inputs of row k + CN_RING are copied into the thread's ring while row k
+// is computed, so a thread keeps CN_RING rows of loads in flight.
 template <int FLD, int FORM>
-__device__ __forceinline__ void cn_forward(const CnCtx &q, const double *fac, const unsigned char *pv, Col X,
-                                           Col D, Col F, Col P, Col S, int euler) {
+__device__ __forceinline__ void cn_forward(const CnCtx &q, const double *fac, const unsigned char *pv, Ring ring,
+                                           Col X, Col D, Col F, Col P, Col S, int euler) {
   constexpr int NL = cn_nl(FORM), PD = cn_pd(FORM), LD = cn_ld(FORM), NE = cn_entries(FORM);
   const RJArgs &a = q.a;
   const int n = q.n;
@@ -201,117 +228,112 @@ __device__ __forceinline__ void cn_forward(const CnCtx &q, const double *fac, co
   const double ce = (FLD <= 1) ? a.cev : (FLD == 2) ? a.cet : a.ceb;
   const double fbi = (q.jj == 0) ? a.temp_icb_fld : 0.0, fbo = (q.jj == 0) ? a.temp_cmb_fld : 0.0;
   const uint64_t keep = l2_evict_last();
+  auto fetch = [&](int sl, int k) {   // inputs of row k into slot sl (none past the last row)
+    if (k < n) {
+      const unsigned o = (unsigned)k * st;
+      cp8(ring.at(sl, 0), X.p + o);
+      cp8(ring.at(sl, 1), D.p + o);
+      cp8(ring.at(sl, 2), F.p + o);
+      if (!euler) cp8(ring.at(sl, 3), P.p + o);
+    }
+    cp_commit();
+  };
+#pragma unroll
+  for (int r = 0; r < CN_RING; r++) fetch(r, r);
   double yh[NL];       // y(i - 1 - t)
   double pend[PD + 1]; // right-hand side of rows i .. i + PD, interchanges of rows < i applied
 #pragma unroll
   for (int t = 0; t < NL; t++) yh[t] = 0.0;
 #pragma unroll
   for (int t = 0; t <= PD; t++) pend[t] = 0.0;
-  for (int k0 = 0; k0 < n + PD; k0 += CN_PF) {
-    double xv[CN_PF], dv[CN_PF], fv[CN_PF], pw[CN_PF];
+  int sl = 0;
+  for (int k = 0; k < n + PD; k++) {
+    double b = 0.0;
+    if (k < n) {
+      cp_wait<CN_RING - 1>();   // row k has landed
+      const double xv = *ring.at(sl, 0), dv = *ring.at(sl, 1), fv = *ring.at(sl, 2);
+      const double pw = euler ? 0.0 : *ring.at(sl, 3);
+      // the temperature's force is minus the heat advection (pH = -H)
+      const double f = (FLD == 2) ? -fv : fv;
+      const double rhs = euler ? xv + dt * (ce * dv + f) : xv + dt * (ce * dv + adam_0 * f + adam_1 * pw);
+      P.stcs(k, st, f);
+      const bool wall = (k == 0 || k == n - 1);
+      if (FLD == 0 || FLD == 1 || FLD == 4) b = (q.jj != 0 && !wall) ? rhs : 0.0;
+      else if (FLD == 2) b = (k == 0) ? fbi : (k == n - 1) ? fbo : rhs;
+      else b = (q.jj != 0) ? rhs : 0.0;
+    }
+    pend[PD] = b;
+    const int i = k - PD;
+    if (i >= 0 && i < n) {
+      if constexpr (PD >= 1) {
+        const int d = pv[i * LD];
+        if (d == 1) { const double t = pend[0]; pend[0] = pend[1]; pend[1] = t; }
+        if constexpr (PD >= 2)
+          if (d == 2) { const double t = pend[0]; pend[0] = pend[2]; pend[2] = t; }
+      }
+      const double *fk = fac + i * NE * LD;
+      double y = pend[0];
 #pragma unroll
-    for (int u = 0; u < CN_PF; u++) {
-      const int k = k0 + u;
-      const bool in = k < n;
-      xv[u] = in ? X.ldcs(k, st) : 0.0;
-      dv[u] = in ? D.ldcs(k, st) : 0.0;
-      fv[u] = in ? F.ldcs(k, st) : 0.0;
-      pw[u] = (in && !euler) ? P.ldcs(k, st) : 0.0;
+      for (int t = NL - 1; t >= 0; t--) y = y - fk[t * LD] * yh[t];
+      S.stkeep(i, st, y, keep);
+#pragma unroll
+      for (int t = NL - 1; t > 0; t--) yh[t] = yh[t - 1];
+      yh[0] = y;
     }
 #pragma unroll
-    for (int u = 0; u < CN_PF; u++) {
-      const int k = k0 + u;
-      double b = 0.0;
-      if (k < n) {
-        // the temperature's force is minus the heat advection (pH = -H)
-        const double f = (FLD == 2) ? -fv[u] : fv[u];
-        const double rhs = euler ? xv[u] + dt * (ce * dv[u] + f)
-                                 : xv[u] + dt * (ce * dv[u] + adam_0 * f + adam_1 * pw[u]);
-        P.stcs(k, st, f);
-        const bool wall = (k == 0 || k == n - 1);
-        if (FLD == 0 || FLD == 1 || FLD == 4) b = (q.jj != 0 && !wall) ? rhs : 0.0;
-        else if (FLD == 2) b = (k == 0) ? fbi : (k == n - 1) ? fbo : rhs;
-        else b = (q.jj != 0) ? rhs : 0.0;
-      }
-      pend[PD] = b;
-      const int i = k - PD;
-      if (i >= 0 && i < n) {
-        if constexpr (PD >= 1) {
-          const int d = pv[i * LD];
-          if (d == 1) { const double t = pend[0]; pend[0] = pend[1]; pend[1] = t; }
-          if constexpr (PD >= 2)
-            if (d == 2) { const double t = pend[0]; pend[0] = pend[2]; pend[2] = t; }
-        }
-        const double *fk = fac + i * NE * LD;
-        double y = pend[0];
-#pragma unroll
-        for (int t = NL - 1; t >= 0; t--) y = y - fk[t * LD] * yh[t];
-        S.stkeep(i, st, y, keep);
-#pragma unroll
-        for (int t = NL - 1; t > 0; t--) yh[t] = yh[t - 1];
-        yh[0] = y;
-      }
-#pragma unroll
-      for (int t = 0; t < PD; t++) pend[t] = pend[t + 1];
+    for (int t = 0; t < PD; t++) pend[t] = pend[t + 1];
+    if (k < n) {
+      // refill the slot just read (its values are used above)
+      fetch(sl, k + CN_RING);
+      sl = (sl + 1 == CN_RING) ? 0 : sl + 1;
     }
   }
+  cp_wait<0>();   // the ring is free for the backward sweep
 }
 
 // backward sweep: U x = y, rows n-1 .. 0, handing each x to the emitter:
 // em.point(k, x) for the row itself, then em.top() once rows n-1 .. n-3
 // are known, em.interior(r) for rows r = n-2 .. 1 as soon as row r - 1 is
-// known, and em.bottom() at the end
+// known, and em.bottom() at the end.  y of row k - CN_RING is copied into
+// the ring while row k is computed.
 template <int FORM, class Em>
-__device__ __forceinline__ void cn_backward(const CnCtx &q, const double *fac, Col S, Em &em) {
+__device__ __forceinline__ void cn_backward(const CnCtx &q, const double *fac, Ring ring, Col S, Em &em) {
   constexpr int NL = cn_nl(FORM), LD = cn_ld(FORM), NE = cn_entries(FORM);
   const int n = q.n;
   const unsigned st = q.st;
+  auto fetch = [&](int sl, int k) {
+    if (k >= 0) cp8(ring.at(sl, 0), S.p + (unsigned)k * st);
+    cp_commit();
+  };
+#pragma unroll
+  for (int r = 0; r < CN_RING; r++) fetch(r, n - 1 - r);
   double xh[NL];   // x(k + 1 + t)
 #pragma unroll
   for (int t = 0; t < NL; t++) xh[t] = 0.0;
-  auto solve = [&](int k, double y) {
+  int sl = 0;
+  for (int k = n - 1; k >= 0; k--) {
+    cp_wait<CN_RING - 1>();
     const double *fk = fac + k * NE * LD;
-    double v = y;
+    double v = *ring.at(sl, 0);
 #pragma unroll
     for (int t = 0; t < NL; t++) v = v - fk[(NL + t) * LD] * xh[t];
     const double x = v * fk[2 * NL * LD];
 #pragma unroll
     for (int t = NL - 1; t > 0; t--) xh[t] = xh[t - 1];
     xh[0] = x;
-    return x;
-  };
-  const uint64_t keep = l2_evict_last();
-  const double y0 = S.ldkeep(n - 1, st, keep), y1 = S.ldkeep(n - 2, st, keep), y2 = S.ldkeep(n - 3, st, keep);
-  double by[CN_PB];
-#pragma unroll
-  for (int u = 0; u < CN_PB; u++) {
-    const int k = n - 4 - u;
-    by[u] = (k >= 0) ? S.ldkeep(k, st, keep) : 0.0;
-  }
-  em.point(n - 1, solve(n - 1, y0));
-  em.point(n - 2, solve(n - 2, y1));
-  em.point(n - 3, solve(n - 3, y2));
-  em.top();
-  em.interior(n - 2);
-  for (int k0 = n - 4; k0 >= 0; k0 -= CN_PB) {
-    double nb[CN_PB];
-#pragma unroll
-    for (int u = 0; u < CN_PB; u++) {
-      const int k = k0 - CN_PB - u;
-      nb[u] = (k >= 0) ? S.ldkeep(k, st, keep) : 0.0;
+    em.point(k, x);
+    // refill the slot just read (its value is stored above, through x)
+    fetch(sl, k - CN_RING);
+    sl = (sl + 1 == CN_RING) ? 0 : sl + 1;
+    if (k == n - 3) {
+      em.top();
+      em.interior(n - 2);
+    } else if (k < n - 3) {
+      em.interior(k + 1);
     }
-#pragma unroll
-    for (int u = 0; u < CN_PB; u++) {
-      const int k = k0 - u;
-      if (k >= 0) {
-        em.point(k, solve(k, by[u]));
-        em.interior(k + 1);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < CN_PB; u++) by[u] = nb[u];
   }
   em.bottom();
+  cp_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -497,30 +519,30 @@ struct EmMagTor {
 // one (field, column) thread: the sweeps with the field's slots and emitter
 template <int FLD, int FORM>
 __device__ __forceinline__ void cn_column(const CnCtx &q, double *col, size_t fs, const double *fac,
-                                          const unsigned char *pv, int euler) {
+                                          const unsigned char *pv, Ring ring, int euler) {
   auto C = [&](int slot) { return Col{col + (size_t)slot * fs}; };
   if constexpr (FLD == 0) {
-    cn_forward<0, FORM>(q, fac, pv, C(VORT + 2), C(WDIFF + 2), C(FORCES + 2), C(PREMOM + 2), C(VELO), euler);
+    cn_forward<0, FORM>(q, fac, pv, ring, C(VORT + 2), C(WDIFF + 2), C(FORCES + 2), C(PREMOM + 2), C(VELO), euler);
     EmVelPol em{q, C(VELO), C(VELO + 1), C(VORT + 2), C(WDIFF + 2)};
-    cn_backward<FORM>(q, fac, C(VELO), em);
+    cn_backward<FORM>(q, fac, ring, C(VELO), em);
   } else if constexpr (FLD == 1) {
-    cn_forward<1, FORM>(q, fac, pv, C(VORT), C(WDIFF), C(FORCES), C(PREMOM), C(VELO + 2), euler);
+    cn_forward<1, FORM>(q, fac, pv, ring, C(VORT), C(WDIFF), C(FORCES), C(PREMOM), C(VELO + 2), euler);
     EmVelTor em{q, C(VELO + 2), C(VORT), C(VORT + 1), C(WDIFF)};
-    cn_backward<FORM>(q, fac, C(VELO + 2), em);
+    cn_backward<FORM>(q, fac, ring, C(VELO + 2), em);
   } else if constexpr (FLD == 2) {
-    cn_forward<2, FORM>(q, fac, pv, C(TEMP), C(TDIFF), C(HADV), C(PREHEAT), C(TEMP), euler);
+    cn_forward<2, FORM>(q, fac, pv, ring, C(TEMP), C(TDIFF), C(HADV), C(PREHEAT), C(TEMP), euler);
     EmTemp em{q, C(TEMP), C(ROTBUO + 2), C(TDIFF), (q.jj == 0) ? q.a.temp_icb_fld : 0.0,
               (q.jj == 0) ? q.a.temp_cmb_fld : 0.0};
-    cn_backward<FORM>(q, fac, C(TEMP), em);
+    cn_backward<FORM>(q, fac, ring, C(TEMP), em);
   } else if constexpr (FLD == 3) {
-    cn_forward<3, FORM>(q, fac, pv, C(MAGNE), C(BDIFF), C(INDUCT), C(PREUXB), C(MAGNE), euler);
+    cn_forward<3, FORM>(q, fac, pv, ring, C(MAGNE), C(BDIFF), C(INDUCT), C(PREUXB), C(MAGNE), euler);
     EmMagPol em{q, C(MAGNE), C(MAGNE + 1), C(CURRENT + 2), C(BDIFF)};
-    cn_backward<FORM>(q, fac, C(MAGNE), em);
+    cn_backward<FORM>(q, fac, ring, C(MAGNE), em);
   } else {
-    cn_forward<4, FORM>(q, fac, pv, C(MAGNE + 2), C(BDIFF + 2), C(INDUCT + 2), C(PREUXB + 2), C(MAGNE + 2),
+    cn_forward<4, FORM>(q, fac, pv, ring, C(MAGNE + 2), C(BDIFF + 2), C(INDUCT + 2), C(PREUXB + 2), C(MAGNE + 2),
                         euler);
     EmMagTor em{q, C(MAGNE + 2), C(CURRENT), C(CURRENT + 1), C(BDIFF + 2)};
-    cn_backward<FORM>(q, fac, C(MAGNE + 2), em);
+    cn_backward<FORM>(q, fac, ring, C(MAGNE + 2), em);
   }
 }
 
@@ -545,7 +567,7 @@ __device__ __forceinline__ CnField cn_field(const CnPack &pk, int fld) {
 // signs of one field (the tile's x); it stages the radial coefficients and
 // the factors of its degrees in shared memory, then each thread runs its
 // column.
-__global__ void __launch_bounds__(CN_THREADS, 3)
+__global__ void __launch_bounds__(CN_THREADS, 2)
 k_cn_step(RJArgs a, double *f, size_t fs, CnPack pk, const int *moff, const int4 *tiles, int euler) {
   extern __shared__ double cn_sm[];
   const int n = a.nr, nl = a.L + 1, tid = threadIdx.x;
@@ -585,17 +607,18 @@ k_cn_step(RJArgs a, double *f, size_t fs, CnPack pk, const int *moff, const int4
   double *col = f + jj;
   const double *fac = sfac + lo;
   const unsigned char *pv = spv + lo;
+  const Ring ring{reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(cn_sm) + cn_ring_offset(n, form)) + tid};
   switch (fld * 4 + form) {
-    case 0 * 4 + CN_N5: cn_column<0, CN_N5>(q, col, fs, fac, pv, euler); break;
-    case 0 * 4 + CN_W5: cn_column<0, CN_W5>(q, col, fs, fac, pv, euler); break;
-    case 1 * 4 + CN_N3: cn_column<1, CN_N3>(q, col, fs, fac, pv, euler); break;
-    case 1 * 4 + CN_W3: cn_column<1, CN_W3>(q, col, fs, fac, pv, euler); break;
-    case 2 * 4 + CN_N3: cn_column<2, CN_N3>(q, col, fs, fac, pv, euler); break;
-    case 2 * 4 + CN_W3: cn_column<2, CN_W3>(q, col, fs, fac, pv, euler); break;
-    case 3 * 4 + CN_N3: cn_column<3, CN_N3>(q, col, fs, fac, pv, euler); break;
-    case 3 * 4 + CN_W3: cn_column<3, CN_W3>(q, col, fs, fac, pv, euler); break;
-    case 4 * 4 + CN_N3: cn_column<4, CN_N3>(q, col, fs, fac, pv, euler); break;
-    case 4 * 4 + CN_W3: cn_column<4, CN_W3>(q, col, fs, fac, pv, euler); break;
+    case 0 * 4 + CN_N5: cn_column<0, CN_N5>(q, col, fs, fac, pv, ring, euler); break;
+    case 0 * 4 + CN_W5: cn_column<0, CN_W5>(q, col, fs, fac, pv, ring, euler); break;
+    case 1 * 4 + CN_N3: cn_column<1, CN_N3>(q, col, fs, fac, pv, ring, euler); break;
+    case 1 * 4 + CN_W3: cn_column<1, CN_W3>(q, col, fs, fac, pv, ring, euler); break;
+    case 2 * 4 + CN_N3: cn_column<2, CN_N3>(q, col, fs, fac, pv, ring, euler); break;
+    case 2 * 4 + CN_W3: cn_column<2, CN_W3>(q, col, fs, fac, pv, ring, euler); break;
+    case 3 * 4 + CN_N3: cn_column<3, CN_N3>(q, col, fs, fac, pv, ring, euler); break;
+    case 3 * 4 + CN_W3: cn_column<3, CN_W3>(q, col, fs, fac, pv, ring, euler); break;
+    case 4 * 4 + CN_N3: cn_column<4, CN_N3>(q, col, fs, fac, pv, ring, euler); break;
+    case 4 * 4 + CN_W3: cn_column<4, CN_W3>(q, col, fs, fac, pv, ring, euler); break;
     default: break;
   }
 }
@@ -653,24 +676,29 @@ int cn_setup(Ctx &c) {
   CB2_CUDA(cudaGetLastError());
   // blocks: (field, m0, l0) tiles of LD degrees x 128 / LD orders
   std::vector<int4> tl;
+  CnHost h;
+  h.pk = pk;
   for (int q = 0; q < 5; q++) {
+    h.tile0[q] = (int)tl.size();
+    h.smem[q] = cn_smem_form(n, pk.form[q]);
     const int ld = cn_ld(pk.form[q]), md = CN_THREADS / (2 * ld);
     for (int l0 = 0; l0 <= c.L; l0 += ld)
       for (int m0 = 0; m0 <= std::min(l0 + ld - 1, c.L); m0 += md) tl.push_back(int4{q, m0, l0, 0});
   }
+  h.tile0[5] = (int)tl.size();
   c.cn_tiles = (int)tl.size();
   CB2_CUDA(cudaMalloc(&c.d_cn_tiles, tl.size() * sizeof(int4)));
   CB2_CUDA(cudaMemcpyAsync(c.d_cn_tiles, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice, c.stream));
   CB2_CUDA(raise_smem_limit(k_cn_step, smem));
   CB2_CUDA(cudaStreamSynchronize(c.stream));
-  c.cn_pack = new CnPack(pk);
+  c.cn_pack = new CnHost(h);
   c.cn_smem = smem;
   c.cn_ready = true;
   return 0;
 }
 
 void cn_free(Ctx &c) {
-  delete static_cast<CnPack *>(c.cn_pack);
+  delete static_cast<CnHost *>(c.cn_pack);
   c.cn_pack = nullptr;
 }
 
@@ -683,10 +711,16 @@ void cn_stage(Ctx &c, bool euler) {
   }
 }
 
+// one launch per field: each is about one wave of blocks (a block per
+// LD degrees x 128 / LD orders, two blocks per SM), so all columns of the
+// field sweep the radial levels together and the rows in use at any time,
+// and the memory pages under them, stay few
 void cn_step(Ctx &c, bool euler) {
-  k_cn_step<<<c.cn_tiles, CN_THREADS, c.cn_smem, c.stream>>>(
-      c.rj_args(), c.d_f, c.fsize(), *static_cast<const CnPack *>(c.cn_pack), c.d_moff, c.d_cn_tiles,
-      euler ? 1 : 0);
+  const CnHost &h = *static_cast<const CnHost *>(c.cn_pack);
+  const RJArgs a = c.rj_args();
+  for (int q = 0; q < 5; q++)
+    k_cn_step<<<h.tile0[q + 1] - h.tile0[q], CN_THREADS, h.smem[q], c.stream>>>(
+        a, c.d_f, c.fsize(), h.pk, c.d_moff, c.d_cn_tiles + h.tile0[q], euler ? 1 : 0);
 }
 
 }  // namespace cb2
