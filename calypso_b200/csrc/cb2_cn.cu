@@ -38,7 +38,7 @@
 
 namespace cb2 {
 
-constexpr int CN_THREADS = 256;   // a block: LD degrees x 128 / LD orders x both signs of m
+constexpr int CN_THREADS = 256;   // a block: 8 warps, each 32 consecutive degrees of one (m, sign)
 constexpr int CN_RING = 6;        // rows each thread keeps in flight (cp.async ring)
 constexpr int CN_RV = 4;          // values per ring slot (forward: X, D, F, P; backward: y)
 
@@ -50,18 +50,11 @@ enum CnForm { CN_N5 = 0, CN_W5 = 1, CN_N3 = 2, CN_W3 = 3 };
 __host__ __device__ constexpr int cn_nl(int f) { return f == CN_N5 ? 2 : f == CN_W5 ? 4 : f == CN_N3 ? 1 : 2; }
 __host__ __device__ constexpr int cn_pd(int f) { return f == CN_W5 ? 2 : f == CN_W3 ? 1 : 0; }
 __host__ __device__ constexpr int cn_entries(int f) { return 2 * cn_nl(f) + 1; }
-// degrees per block: 4 for the widest form, so that its factors and the
-// rings leave room for 2 blocks per SM
-__host__ __device__ constexpr int cn_ld(int f) { return f == CN_W5 ? 4 : 8; }
 
-// shared memory of a block: radial coefficients, the factors of its
-// degrees, their interchange offsets, and the per-thread rings
-__host__ __device__ inline size_t cn_ring_offset(int n, int f) {
-  return 9 * (size_t)n * sizeof(double) + (size_t)n * cn_entries(f) * cn_ld(f) * sizeof(double) +
-         ((cn_pd(f) ? (size_t)n * cn_ld(f) : 0) + 15) / 16 * 16;
-}
-static size_t cn_smem_form(int n, int f) {
-  return cn_ring_offset(n, f) + (size_t)CN_RING * CN_RV * CN_THREADS * sizeof(double);
+// shared memory of a block: the radial coefficients, then the per-thread rings
+__host__ __device__ inline size_t cn_ring_offset(int n) { return 9 * (size_t)n * sizeof(double); }
+static size_t cn_smem(int n) {
+  return cn_ring_offset(n) + (size_t)CN_RING * CN_RV * CN_THREADS * sizeof(double);
 }
 
 struct LuSet {
@@ -77,12 +70,10 @@ struct CnPack {
   int form[5];
 };
 
-// host side: the pack, each field's first tile (tile0[5] = all tiles) and
-// its launch's shared memory
+// host side: the pack and each field's first tile (tile0[5] = all tiles)
 struct CnHost {
   CnPack pk;
   int tile0[6];
-  size_t smem[5];
 };
 
 // entry b (1-based) of band column c (1-based) of one degree's factors
@@ -207,20 +198,31 @@ struct CnCtx {
   double g3, gl;
 };
 
+// one degree's factors in global memory (degree-interleaved, so the 32
+// lanes of a warp read 32 consecutive values; the block's 8 warps share
+// them through L1): entry e of row i at p[(i * NE + e) * nl], the
+// interchange offset of row i at pv[i * nl]
+struct FacCol {
+  const double *p;
+  const unsigned char *pv;
+  int nl;
+  __device__ double at(int i, int ne, int e) const { return __ldg(p + (i * ne + e) * nl); }
+  __device__ int piv(int i) const { return __ldg(pv + i * nl); }
+};
+
 // ---------------------------------------------------------------------------
 // forward sweep: explicit right-hand side and L y = P b.  X, D, F, P: the
 // field before the step, its diffusion term, its force and the force of the
 // step before (P receives this step's force); S: the solution slot.
 // FLD: 0 poloidal velocity (from the toroidal vorticity), 1 toroidal
 // velocity (from the poloidal vorticity), 2 temperature, 3 poloidal and
-// 4 toroidal magnetic field.  fac: the column's factors in shared memory
-// (row stride NE * LD), pv: its interchange offsets (row stride LD).  The
+// 4 toroidal magnetic field.  fac: the column's factors.  The
 // inputs of row k + CN_RING are copied into the thread's ring while row k
 // is computed, so a thread keeps CN_RING rows of loads in flight.
 template <int FLD, int FORM>
-__device__ __forceinline__ void cn_forward(const CnCtx &q, const double *fac, const unsigned char *pv, Ring ring,
+__device__ __forceinline__ void cn_forward(const CnCtx &q, FacCol fac, Ring ring,
                                            Col X, Col D, Col F, Col P, Col S, int euler) {
-  constexpr int NL = cn_nl(FORM), PD = cn_pd(FORM), LD = cn_ld(FORM), NE = cn_entries(FORM);
+  constexpr int NL = cn_nl(FORM), PD = cn_pd(FORM), NE = cn_entries(FORM);
   const RJArgs &a = q.a;
   const int n = q.n;
   const unsigned st = q.st;
@@ -266,15 +268,14 @@ __device__ __forceinline__ void cn_forward(const CnCtx &q, const double *fac, co
     const int i = k - PD;
     if (i >= 0 && i < n) {
       if constexpr (PD >= 1) {
-        const int d = pv[i * LD];
+        const int d = fac.piv(i);
         if (d == 1) { const double t = pend[0]; pend[0] = pend[1]; pend[1] = t; }
         if constexpr (PD >= 2)
           if (d == 2) { const double t = pend[0]; pend[0] = pend[2]; pend[2] = t; }
       }
-      const double *fk = fac + i * NE * LD;
       double y = pend[0];
 #pragma unroll
-      for (int t = NL - 1; t >= 0; t--) y = y - fk[t * LD] * yh[t];
+      for (int t = NL - 1; t >= 0; t--) y = y - fac.at(i, NE, t) * yh[t];
       S.stkeep(i, st, y, keep);
 #pragma unroll
       for (int t = NL - 1; t > 0; t--) yh[t] = yh[t - 1];
@@ -297,8 +298,8 @@ __device__ __forceinline__ void cn_forward(const CnCtx &q, const double *fac, co
 // known, and em.bottom() at the end.  y of row k - CN_RING is copied into
 // the ring while row k is computed.
 template <int FORM, class Em>
-__device__ __forceinline__ void cn_backward(const CnCtx &q, const double *fac, Ring ring, Col S, Em &em) {
-  constexpr int NL = cn_nl(FORM), LD = cn_ld(FORM), NE = cn_entries(FORM);
+__device__ __forceinline__ void cn_backward(const CnCtx &q, FacCol fac, Ring ring, Col S, Em &em) {
+  constexpr int NL = cn_nl(FORM), NE = cn_entries(FORM);
   const int n = q.n;
   const unsigned st = q.st;
   auto fetch = [&](int sl, int k) {
@@ -313,11 +314,10 @@ __device__ __forceinline__ void cn_backward(const CnCtx &q, const double *fac, R
   int sl = 0;
   for (int k = n - 1; k >= 0; k--) {
     cp_wait<CN_RING - 1>();
-    const double *fk = fac + k * NE * LD;
     double v = *ring.at(sl, 0);
 #pragma unroll
-    for (int t = 0; t < NL; t++) v = v - fk[(NL + t) * LD] * xh[t];
-    const double x = v * fk[2 * NL * LD];
+    for (int t = 0; t < NL; t++) v = v - fac.at(k, NE, NL + t) * xh[t];
+    const double x = v * fac.at(k, NE, 2 * NL);
 #pragma unroll
     for (int t = NL - 1; t > 0; t--) xh[t] = xh[t - 1];
     xh[0] = x;
@@ -518,28 +518,28 @@ struct EmMagTor {
 // ---------------------------------------------------------------------------
 // one (field, column) thread: the sweeps with the field's slots and emitter
 template <int FLD, int FORM>
-__device__ __forceinline__ void cn_column(const CnCtx &q, double *col, size_t fs, const double *fac,
-                                          const unsigned char *pv, Ring ring, int euler) {
+__device__ __forceinline__ void cn_column(const CnCtx &q, double *col, size_t fs, FacCol fac, Ring ring,
+                                          int euler) {
   auto C = [&](int slot) { return Col{col + (size_t)slot * fs}; };
   if constexpr (FLD == 0) {
-    cn_forward<0, FORM>(q, fac, pv, ring, C(VORT + 2), C(WDIFF + 2), C(FORCES + 2), C(PREMOM + 2), C(VELO), euler);
+    cn_forward<0, FORM>(q, fac, ring, C(VORT + 2), C(WDIFF + 2), C(FORCES + 2), C(PREMOM + 2), C(VELO), euler);
     EmVelPol em{q, C(VELO), C(VELO + 1), C(VORT + 2), C(WDIFF + 2)};
     cn_backward<FORM>(q, fac, ring, C(VELO), em);
   } else if constexpr (FLD == 1) {
-    cn_forward<1, FORM>(q, fac, pv, ring, C(VORT), C(WDIFF), C(FORCES), C(PREMOM), C(VELO + 2), euler);
+    cn_forward<1, FORM>(q, fac, ring, C(VORT), C(WDIFF), C(FORCES), C(PREMOM), C(VELO + 2), euler);
     EmVelTor em{q, C(VELO + 2), C(VORT), C(VORT + 1), C(WDIFF)};
     cn_backward<FORM>(q, fac, ring, C(VELO + 2), em);
   } else if constexpr (FLD == 2) {
-    cn_forward<2, FORM>(q, fac, pv, ring, C(TEMP), C(TDIFF), C(HADV), C(PREHEAT), C(TEMP), euler);
+    cn_forward<2, FORM>(q, fac, ring, C(TEMP), C(TDIFF), C(HADV), C(PREHEAT), C(TEMP), euler);
     EmTemp em{q, C(TEMP), C(ROTBUO + 2), C(TDIFF), (q.jj == 0) ? q.a.temp_icb_fld : 0.0,
               (q.jj == 0) ? q.a.temp_cmb_fld : 0.0};
     cn_backward<FORM>(q, fac, ring, C(TEMP), em);
   } else if constexpr (FLD == 3) {
-    cn_forward<3, FORM>(q, fac, pv, ring, C(MAGNE), C(BDIFF), C(INDUCT), C(PREUXB), C(MAGNE), euler);
+    cn_forward<3, FORM>(q, fac, ring, C(MAGNE), C(BDIFF), C(INDUCT), C(PREUXB), C(MAGNE), euler);
     EmMagPol em{q, C(MAGNE), C(MAGNE + 1), C(CURRENT + 2), C(BDIFF)};
     cn_backward<FORM>(q, fac, ring, C(MAGNE), em);
   } else {
-    cn_forward<4, FORM>(q, fac, pv, ring, C(MAGNE + 2), C(BDIFF + 2), C(INDUCT + 2), C(PREUXB + 2), C(MAGNE + 2),
+    cn_forward<4, FORM>(q, fac, ring, C(MAGNE + 2), C(BDIFF + 2), C(INDUCT + 2), C(PREUXB + 2), C(MAGNE + 2),
                         euler);
     EmMagTor em{q, C(MAGNE + 2), C(CURRENT), C(CURRENT + 1), C(BDIFF + 2)};
     cn_backward<FORM>(q, fac, ring, C(MAGNE + 2), em);
@@ -563,22 +563,20 @@ __device__ __forceinline__ CnField cn_field(const CnPack &pk, int fld) {
   }
 }
 
-// One block: LD consecutive degrees x 128 / LD consecutive orders x both
-// signs of one field (the tile's x); it stages the radial coefficients and
-// the factors of its degrees in shared memory, then each thread runs its
-// column.
-__global__ void __launch_bounds__(CN_THREADS, 2)
+// One block: 8 warps of one field (the tile's x); warp w takes the (m, sign)
+// pair p0 + w (pair 0: m = 0; pair 2m - 1: (m, +); pair 2m: (m, -)), lane
+// the degree l0 + lane, so every access of a warp to a slot row is 32
+// consecutive doubles.  The block stages the radial coefficients in shared
+// memory; each thread then runs its column.
+__global__ void __launch_bounds__(CN_THREADS, 3)
 k_cn_step(RJArgs a, double *f, size_t fs, CnPack pk, const int *moff, const int4 *tiles, int euler) {
   extern __shared__ double cn_sm[];
   const int n = a.nr, nl = a.L + 1, tid = threadIdx.x;
-  const int4 tl = tiles[blockIdx.x];   // (field, m0, l0, -)
+  const int4 tl = tiles[blockIdx.x];   // (field, p0, l0, -)
   const int fld = tl.x;
   const CnField fd = cn_field(pk, fld);
   const int form = fd.form;
-  const int NE = cn_entries(form), LD = cn_ld(form);
-  double *sco = cn_sm;                                                      // [9][n]
-  double *sfac = cn_sm + 9 * n;                                             // [n][NE][LD]
-  unsigned char *spv = reinterpret_cast<unsigned char *>(sfac + (size_t)n * NE * LD);   // [n][LD]
+  double *sco = cn_sm;                 // [9][n]
   for (int e = tid; e < 3 * n; e += CN_THREADS) {
     sco[e] = __ldg(a.d1 + e);
     sco[3 * n + e] = __ldg(a.d2 + e);
@@ -588,37 +586,26 @@ k_cn_step(RJArgs a, double *f, size_t fs, CnPack pk, const int *moff, const int4
     sco[7 * n + e] = __ldg(a.ar2 + e);
     sco[8 * n + e] = __ldg(a.r + e);
   }
-  for (int e = tid; e < n * NE * LD; e += CN_THREADS) {
-    const int lo = e % LD, l = tl.z + lo;
-    sfac[e] = (l < nl) ? __ldg(fd.fac + (size_t)(e / LD) * nl + l) : 0.0;
-  }
-  if (cn_pd(form))
-    for (int e = tid; e < n * LD; e += CN_THREADS) {
-      const int lo = e % LD, l = tl.z + lo;
-      spv[e] = (l < nl) ? fd.piv[(size_t)(e / LD) * nl + l] : 0;
-    }
   __syncthreads();
-  const int md = CN_THREADS / (2 * LD);
-  const int lo = tid % LD, mo = (tid / LD) % md, sgn = tid / (LD * md);
-  const int l = tl.z + lo, m = tl.y + mo;
-  if (l >= nl || m > l || (sgn == 1 && m == 0)) return;
+  const int p = tl.y + tid / 32, l = tl.z + tid % 32;
+  const int m = (p + 1) >> 1, sgn = (p > 0 && (p & 1) == 0) ? 1 : 0;
+  if (l >= nl || m > l) return;
   const int jj = moff[m] + sgn * (nl - m) + (l - m);
   const CnCtx q{a, RadCo{sco, n}, n, (unsigned)a.jmax, jj, __ldg(a.g3 + jj), __ldg(a.gl + jj)};
   double *col = f + jj;
-  const double *fac = sfac + lo;
-  const unsigned char *pv = spv + lo;
-  const Ring ring{reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(cn_sm) + cn_ring_offset(n, form)) + tid};
+  const FacCol fac{fd.fac + l, fd.piv ? fd.piv + l : nullptr, nl};
+  const Ring ring{reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(cn_sm) + cn_ring_offset(n)) + tid};
   switch (fld * 4 + form) {
-    case 0 * 4 + CN_N5: cn_column<0, CN_N5>(q, col, fs, fac, pv, ring, euler); break;
-    case 0 * 4 + CN_W5: cn_column<0, CN_W5>(q, col, fs, fac, pv, ring, euler); break;
-    case 1 * 4 + CN_N3: cn_column<1, CN_N3>(q, col, fs, fac, pv, ring, euler); break;
-    case 1 * 4 + CN_W3: cn_column<1, CN_W3>(q, col, fs, fac, pv, ring, euler); break;
-    case 2 * 4 + CN_N3: cn_column<2, CN_N3>(q, col, fs, fac, pv, ring, euler); break;
-    case 2 * 4 + CN_W3: cn_column<2, CN_W3>(q, col, fs, fac, pv, ring, euler); break;
-    case 3 * 4 + CN_N3: cn_column<3, CN_N3>(q, col, fs, fac, pv, ring, euler); break;
-    case 3 * 4 + CN_W3: cn_column<3, CN_W3>(q, col, fs, fac, pv, ring, euler); break;
-    case 4 * 4 + CN_N3: cn_column<4, CN_N3>(q, col, fs, fac, pv, ring, euler); break;
-    case 4 * 4 + CN_W3: cn_column<4, CN_W3>(q, col, fs, fac, pv, ring, euler); break;
+    case 0 * 4 + CN_N5: cn_column<0, CN_N5>(q, col, fs, fac, ring, euler); break;
+    case 0 * 4 + CN_W5: cn_column<0, CN_W5>(q, col, fs, fac, ring, euler); break;
+    case 1 * 4 + CN_N3: cn_column<1, CN_N3>(q, col, fs, fac, ring, euler); break;
+    case 1 * 4 + CN_W3: cn_column<1, CN_W3>(q, col, fs, fac, ring, euler); break;
+    case 2 * 4 + CN_N3: cn_column<2, CN_N3>(q, col, fs, fac, ring, euler); break;
+    case 2 * 4 + CN_W3: cn_column<2, CN_W3>(q, col, fs, fac, ring, euler); break;
+    case 3 * 4 + CN_N3: cn_column<3, CN_N3>(q, col, fs, fac, ring, euler); break;
+    case 3 * 4 + CN_W3: cn_column<3, CN_W3>(q, col, fs, fac, ring, euler); break;
+    case 4 * 4 + CN_N3: cn_column<4, CN_N3>(q, col, fs, fac, ring, euler); break;
+    case 4 * 4 + CN_W3: cn_column<4, CN_W3>(q, col, fs, fac, ring, euler); break;
     default: break;
   }
 }
@@ -656,8 +643,8 @@ int cn_setup(Ctx &c) {
     pk.form[q] = (all & 1) ? (q == 0 ? CN_N5 : CN_N3) : (q == 0 ? CN_W5 : CN_W3);
     dbl += (size_t)n * cn_entries(pk.form[q]) * nl;
     if (cn_pd(pk.form[q])) byt += (size_t)n * nl;
-    smem = std::max(smem, cn_smem_form(n, pk.form[q]));
   }
+  smem = cn_smem(n);
   if (smem > 227 * 1024) {
     c.tune[TUNE_CN] = -1;
     return 0;
@@ -674,16 +661,16 @@ int cn_setup(Ctx &c) {
   }
   k_cn_pack<<<cdiv(5 * nl, 128), 128, 0, c.stream>>>(n, nl, set, pk);
   CB2_CUDA(cudaGetLastError());
-  // blocks: (field, m0, l0) tiles of LD degrees x 128 / LD orders
+  // blocks: (field, p0, l0) tiles of 8 (m, sign) pairs x 32 degrees
   std::vector<int4> tl;
   CnHost h;
   h.pk = pk;
   for (int q = 0; q < 5; q++) {
     h.tile0[q] = (int)tl.size();
-    h.smem[q] = cn_smem_form(n, pk.form[q]);
-    const int ld = cn_ld(pk.form[q]), md = CN_THREADS / (2 * ld);
-    for (int l0 = 0; l0 <= c.L; l0 += ld)
-      for (int m0 = 0; m0 <= std::min(l0 + ld - 1, c.L); m0 += md) tl.push_back(int4{q, m0, l0, 0});
+    for (int l0 = 0; l0 <= c.L; l0 += 32) {
+      const int npair = 2 * std::min(l0 + 31, c.L) + 1;
+      for (int p0 = 0; p0 < npair; p0 += 8) tl.push_back(int4{q, p0, l0, 0});
+    }
   }
   h.tile0[5] = (int)tl.size();
   c.cn_tiles = (int)tl.size();
@@ -711,15 +698,14 @@ void cn_stage(Ctx &c, bool euler) {
   }
 }
 
-// one launch per field: each is about one wave of blocks (a block per
-// LD degrees x 128 / LD orders, two blocks per SM), so all columns of the
-// field sweep the radial levels together and the rows in use at any time,
-// and the memory pages under them, stay few
+// one launch per field: each is about one wave of blocks (3 per SM), so all
+// columns of the field sweep the radial levels together and the rows in use
+// at any time, and the memory pages under them, stay few
 void cn_step(Ctx &c, bool euler) {
   const CnHost &h = *static_cast<const CnHost *>(c.cn_pack);
   const RJArgs a = c.rj_args();
   for (int q = 0; q < 5; q++)
-    k_cn_step<<<h.tile0[q + 1] - h.tile0[q], CN_THREADS, h.smem[q], c.stream>>>(
+    k_cn_step<<<h.tile0[q + 1] - h.tile0[q], CN_THREADS, c.cn_smem, c.stream>>>(
         a, c.d_f, c.fsize(), h.pk, c.d_moff, c.d_cn_tiles + h.tile0[q], euler ? 1 : 0);
 }
 
