@@ -39,7 +39,7 @@
 namespace cb2 {
 
 constexpr int CN_THREADS = 256;   // a block: 8 warps, each 32 consecutive degrees of one (m, sign)
-constexpr int CN_RING = 6;        // rows each thread keeps in flight (cp.async ring)
+constexpr int CN_RING = 4;        // rows each thread keeps in flight (cp.async ring)
 constexpr int CN_RV = 4;          // values per ring slot (forward: X, D, F, P; backward: y)
 
 // Forms of one field's factors.  Per row i: NL multipliers L(i,i-1) ..
@@ -568,7 +568,7 @@ __device__ __forceinline__ CnField cn_field(const CnPack &pk, int fld) {
 // the degree l0 + lane, so every access of a warp to a slot row is 32
 // consecutive doubles.  The block stages the radial coefficients in shared
 // memory; each thread then runs its column.
-__global__ void __launch_bounds__(CN_THREADS, 3)
+__global__ void __launch_bounds__(CN_THREADS, 4)
 k_cn_step(RJArgs a, double *f, size_t fs, CnPack pk, const int *moff, const int4 *tiles, int euler) {
   extern __shared__ double cn_sm[];
   const int n = a.nr, nl = a.L + 1, tid = threadIdx.x;
@@ -698,15 +698,11 @@ void cn_stage(Ctx &c, bool euler) {
   }
 }
 
-// one launch per field: each is about one wave of blocks (3 per SM), so all
-// columns of the field sweep the radial levels together and the rows in use
-// at any time, and the memory pages under them, stay few
+// one launch for the five fields (the 5-band field's blocks first)
 void cn_step(Ctx &c, bool euler) {
   const CnHost &h = *static_cast<const CnHost *>(c.cn_pack);
-  const RJArgs a = c.rj_args();
-  for (int q = 0; q < 5; q++)
-    k_cn_step<<<h.tile0[q + 1] - h.tile0[q], CN_THREADS, c.cn_smem, c.stream>>>(
-        a, c.d_f, c.fsize(), h.pk, c.d_moff, c.d_cn_tiles + h.tile0[q], euler ? 1 : 0);
+  k_cn_step<<<h.tile0[5], CN_THREADS, c.cn_smem, c.stream>>>(c.rj_args(), c.d_f, c.fsize(), h.pk, c.d_moff,
+                                                             c.d_cn_tiles, euler ? 1 : 0);
 }
 
 }  // namespace cb2
