@@ -70,12 +70,6 @@ struct CnPack {
   int form[5];
 };
 
-// host side: the pack and each field's first tile (tile0[5] = all tiles)
-struct CnHost {
-  CnPack pk;
-  int tile0[6];
-};
-
 // entry b (1-based) of band column c (1-based) of one degree's factors
 struct BandCol {
   const double *lu;
@@ -663,29 +657,25 @@ int cn_setup(Ctx &c) {
   CB2_CUDA(cudaGetLastError());
   // blocks: (field, p0, l0) tiles of 8 (m, sign) pairs x 32 degrees
   std::vector<int4> tl;
-  CnHost h;
-  h.pk = pk;
   for (int q = 0; q < 5; q++) {
-    h.tile0[q] = (int)tl.size();
     for (int l0 = 0; l0 <= c.L; l0 += 32) {
       const int npair = 2 * std::min(l0 + 31, c.L) + 1;
       for (int p0 = 0; p0 < npair; p0 += 8) tl.push_back(int4{q, p0, l0, 0});
     }
   }
-  h.tile0[5] = (int)tl.size();
   c.cn_tiles = (int)tl.size();
   CB2_CUDA(cudaMalloc(&c.d_cn_tiles, tl.size() * sizeof(int4)));
   CB2_CUDA(cudaMemcpyAsync(c.d_cn_tiles, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice, c.stream));
   CB2_CUDA(raise_smem_limit(k_cn_step, smem));
   CB2_CUDA(cudaStreamSynchronize(c.stream));
-  c.cn_pack = new CnHost(h);
+  c.cn_pack = new CnPack(pk);
   c.cn_smem = smem;
   c.cn_ready = true;
   return 0;
 }
 
 void cn_free(Ctx &c) {
-  delete static_cast<CnHost *>(c.cn_pack);
+  delete static_cast<CnPack *>(c.cn_pack);
   c.cn_pack = nullptr;
 }
 
@@ -700,9 +690,9 @@ void cn_stage(Ctx &c, bool euler) {
 
 // one launch for the five fields (the 5-band field's blocks first)
 void cn_step(Ctx &c, bool euler) {
-  const CnHost &h = *static_cast<const CnHost *>(c.cn_pack);
-  k_cn_step<<<h.tile0[5], CN_THREADS, c.cn_smem, c.stream>>>(c.rj_args(), c.d_f, c.fsize(), h.pk, c.d_moff,
-                                                             c.d_cn_tiles, euler ? 1 : 0);
+  k_cn_step<<<c.cn_tiles, CN_THREADS, c.cn_smem, c.stream>>>(c.rj_args(), c.d_f, c.fsize(),
+                                                              *static_cast<const CnPack *>(c.cn_pack), c.d_moff,
+                                                              c.d_cn_tiles, euler ? 1 : 0);
 }
 
 }  // namespace cb2
