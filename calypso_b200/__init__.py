@@ -6,9 +6,9 @@ reader (:mod:`calypso_b200.control`), the named workloads
 (:mod:`calypso_b200.configs`) and the ctypes binding that mirrors the
 reference's module procedures (:mod:`calypso_b200.sph_mhd`).
 """
-from .sph_mhd import (PREC_FP64, PREC_MIXED, CalypsoError, Ensemble, SphMHD,  # noqa: F401
-                      load_library)
+from .sph_mhd import (PREC_FP64, PREC_MIXED, CalypsoError, Ensemble, SphMHD, SphTables,  # noqa: F401
+                      fft_library_known, legendre_trans_mode, load_library, sph_tables)
 from . import configs, control  # noqa: F401
 
 __all__ = ["SphMHD", "Ensemble", "CalypsoError", "PREC_FP64", "PREC_MIXED", "load_library",
-           "configs", "control"]
+           "SphTables", "sph_tables", "legendre_trans_mode", "fft_library_known", "configs", "control"]

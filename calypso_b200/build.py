@@ -14,7 +14,7 @@ LIB = os.path.join(HERE, "libcalypso_b200.so")
 OBJDIR = os.path.join(HERE, "_build")
 SOURCES = ["cb2_api.cu", "cb2_tables.cu", "cb2_rj.cu", "cb2_legendre_f64.cu",
            "cb2_fft.cu", "cb2_legendre_mixed.cu", "cb2_static_scratch.cu",
-           "cb2_tune.cu", "cb2_closure.cu", "cb2_cn.cu"]
+           "cb2_tune.cu", "cb2_closure.cu", "cb2_cn.cu", "cb2_boundary.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC,-fopenmp", "--expt-relaxed-constexpr", "-ccbin", "/usr/bin/g++"]

@@ -49,6 +49,28 @@ def sht_roundtrip() -> dict:
     return shell_params(255, 65, 384, 768, E=1e-4, Ra=300.0, dt=5e-6)
 
 
+def sht_roundtrip_spectra(L: int, nr: int, nvec: int = 3, nscal: int = 2):
+    """Seeded spectra of the SHT round-trip workload: field f (the vectors,
+    then the scalars) draws from seed f independent N(0, 1) values for every
+    real harmonic coefficient (the cos and sin parts of m are separate
+    coefficients), scaled by 1 / (l sqrt(2l+1)) so that the power of degree
+    l, summed over m, falls as l^-2 (l = 0 scaled as l = 1).  A vector's
+    three slots (S, dS/dr, T) come from the same stream; its dS/dr and T
+    have no l = 0 part.  Array (3 nvec + nscal, nr, (L+1)^2), j = l(l+1)+m."""
+    import numpy as np
+    ls = np.array([l for l in range(L + 1) for _ in range(2 * l + 1)])
+    amp = 1.0 / (np.maximum(ls, 1) * np.sqrt(2 * ls + 1.0))
+    out = []
+    for f in range(nvec + nscal):
+        rng = np.random.default_rng(f)
+        ncomp = 3 if f < nvec else 1
+        x = rng.standard_normal((ncomp, nr, (L + 1) ** 2)) * amp[None, None, :]
+        if f < nvec:
+            x[1:, :, 0] = 0.0
+        out.append(x)
+    return np.concatenate(out)
+
+
 def full_step_L255() -> dict:
     """Full time step: L255, Nr129, 384 x 768 grid, E 1e-4, Ra 300.
 

@@ -211,3 +211,14 @@ def time_control(mhd_text: str) -> dict:
         legendre_trans_loop=(tl.get("Legendre_trans_loop_ctl") or "").upper(),
         fft_library=(tl.get("FFT_library_ctl") or "").upper(),
     )
+
+
+def precision_from_control(mhd_text: str) -> int:
+    """Precision of the transforms a control_MHD selects through
+    Legendre_trans_loop_ctl (set_legendre_trans_mode_ctl,
+    legendre_transform_select.f90:181-224): 'B200_mixed' or 'B200_tcgen05'
+    -> the mixed path, any other value -> the float64 path.  FFT_library_ctl
+    names (set_fft_library_ctl) all select the library's own FFT, in that
+    precision."""
+    from .sph_mhd import legendre_trans_mode
+    return legendre_trans_mode(time_control(mhd_text)["legendre_trans_loop"])

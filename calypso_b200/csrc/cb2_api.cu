@@ -1,4 +1,5 @@
 // cb2_api.cu -- the C ABI of libcalypso_b200 (see include/calypso_b200.h).
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -244,6 +245,7 @@ int cb2_create(const cb2_params *p, int precision, int device, cb2_ctx **out) {
   c->kin = 0; c->kout = p->nr - 1;
   const char *tm = getenv("CB2_TIMERS");
   c->timers = tm && tm[0] == '1';
+  if (const char *pw = getenv("CB2_PIPE_WAIT_NS")) c->pipe_wait_ns = strtoull(pw, nullptr, 10);
   int rc;
   auto fail = [&](int code) { cb2_destroy(c); return code; };
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -274,6 +276,7 @@ int cb2_create(const cb2_params *p, int precision, int device, cb2_ctx **out) {
       cudaMalloc(&c->d_tmp, fs * sizeof(double)) != cudaSuccess)
     return fail(cuda_fail(cudaGetLastError(), "cudaMalloc(work)"));
   if (precision == CB2_PREC_MIXED && (rc = mixed_setup(*c))) return fail(rc);
+  if ((rc = static_scratch_setup(c->device))) return fail(rc);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess)
     return fail(cuda_fail(cudaGetLastError(), "set-up"));
   *out = c;
@@ -290,7 +293,8 @@ int cb2_destroy(cb2_ctx *c) {
   free_tables(*c);
   void *ptrs[] = {c->d_lu_vp, c->d_lu_vt, c->d_lu_bs, c->d_lu_bt, c->d_lu_t, c->d_pv_vp, c->d_pv_vt,
                   c->d_pv_bs, c->d_pv_bt, c->d_pv_t, c->d_status, c->d_tw_fft, c->d_tw_fft32, c->d_twp32, c->d_twf4, c->d_imp_map,
-                  c->d_cn_lu, c->d_cn_tiles, c->d_f, c->d_four, c->d_four2, c->d_ene, c->d_tmp, c->d_host_state};
+                  c->d_cn_lu, c->d_cn_tiles, c->d_f, c->d_four, c->d_four2, c->d_ene, c->d_tmp, c->d_host_state,
+                  c->d_bnd_a, c->d_bnd_b, c->d_bnd_grid, c->d_bnd_tab};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -355,7 +359,7 @@ int cb2_start(cb2_ctx *c) {
   int rc = nonlinear(*c);
   if (rc) return rc;
   CB2_CUDA(cudaGetLastError());
-  CB2_CUDA(cudaStreamSynchronize(c->stream));
+  if ((rc = check_status(*c))) return rc;
   c->istep = 0;
   c->started = true;
   return 0;
@@ -442,6 +446,12 @@ int cb2_energies(cb2_ctx *c, double out[7]) {
   if (!c || !out) return CB2_ERR_ARG;
   int rc = check_status(*c);
   return rc ? rc : rj_energies(*c, out);
+}
+
+int cb2_energy_spectra(cb2_ctx *c, double *out_l, double *out_m, double *out_lm) {
+  if (!c || !out_l || !out_m || !out_lm) return CB2_ERR_ARG;
+  int rc = check_status(*c);
+  return rc ? rc : rj_energy_spectra(*c, out_l, out_m, out_lm);
 }
 
 int cb2_get_field_device(cb2_ctx *c, int slot, double *dev) {
@@ -622,6 +632,36 @@ int cb2_alloc_pinned(size_t bytes, void **out) {
 
 int cb2_free_pinned(void *p) {
   if (p) CB2_CUDA(cudaFreeHost(p));
+  return 0;
+}
+
+static bool same_nocase(const char *a, const char *b) {
+  for (; *a && *b; a++, b++)
+    if (std::tolower((unsigned char)*a) != std::tolower((unsigned char)*b)) return false;
+  return *a == 0 && *b == 0;
+}
+
+// trailing blanks of a Fortran character value are not part of the name
+static std::string trimmed(const char *s) {
+  std::string t(s);
+  while (!t.empty() && (t.back() == ' ' || t.back() == '\t' || t.back() == '\0')) t.pop_back();
+  return t;
+}
+
+int cb2_legendre_trans_mode(const char *ctl) {
+  if (!ctl) return CB2_PREC_FP64;
+  const std::string v = trimmed(ctl);
+  if (same_nocase(v.c_str(), "B200_mixed") || same_nocase(v.c_str(), "B200_tcgen05")) return CB2_PREC_MIXED;
+  return CB2_PREC_FP64;
+}
+
+int cb2_fft_library_known(const char *ctl) {
+  if (!ctl) return 0;
+  const std::string v = trimmed(ctl);
+  static const char *known[] = {"fftpack", "ispack", "fftw", "fftw3", "fftw_single", "fftw3_single",
+                                "fftw_field", "fftw3_field", "B200"};
+  for (const char *k : known)
+    if (same_nocase(v.c_str(), k)) return 1;
   return 0;
 }
 

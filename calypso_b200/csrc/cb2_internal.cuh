@@ -97,6 +97,10 @@ struct Ctx {
   size_t cn_smem = 0;
   bool cn_ready = false;
   int *d_status = nullptr;               // device error word
+  // budget of each wait inside the tensor-core pipelines (ns): 200 ms, or
+  // CB2_PIPE_WAIT_NS from the environment at cb2_create (0: one try, so the
+  // first wait that is not already complete runs out)
+  unsigned long long pipe_wait_ns = 200ull * 1000 * 1000;
   double *d_tw_fft = nullptr;            // exp(-2 pi i e / nph), e = 0..nph-1
   float *d_tw_fft32 = nullptr;
   void *d_twp32 = nullptr;               // per-stage float2 twiddles of the compile-time FFT plans
@@ -114,6 +118,12 @@ struct Ctx {
   void *mixed = nullptr;
   // learned subgrid closure attached to the step (cb2_closure.cu), or null
   void *closure = nullptr;
+  // routine-level entry points (cb2_boundary.cu): device staging of the
+  // caller's host buffers, a grid buffer and the index tables, grown on demand
+  double *d_bnd_a = nullptr, *d_bnd_b = nullptr, *d_bnd_grid = nullptr;
+  size_t bnd_a_bytes = 0, bnd_b_bytes = 0, bnd_grid_bytes = 0;
+  int *d_bnd_tab = nullptr;
+  size_t bnd_tab_bytes = 0;
   int istep = 0;
   bool started = false;
   bool timers = false;
@@ -175,6 +185,9 @@ void rj_start_derived(Ctx &c);
 void rj_temp_total(Ctx &c, double sign);
 int rj_energies(Ctx &c, double out[7]);
 int rj_energies_scratch(Ctx &c, double *scratch, double out[7]);
+int rj_energy_spectra(Ctx &c, double *out_l, double *out_m, double *out_lm);
+// look up the static scratch of cb2_energies_static on a device (cb2_static_scratch.cu)
+int static_scratch_setup(int device);
 int rj_lu_factorise(Ctx &c);
 // fused Crank-Nicolson step (cb2_cn.cu): set-up after rj_lu_factorise, and
 // the step (explicit update, solves, derived fields) when c.cn_ready

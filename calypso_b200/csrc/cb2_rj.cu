@@ -60,7 +60,7 @@ __device__ static int d_ludcmp_3band(int n, const double *A, double *lu, int *pi
     double am = fabs(M5(lu, 3, i));
     if (i < n) am = fmax(am, fabs(M5(lu, 2, i + 1)));
     if (i > 1) am = fmax(am, fabs(M5(lu, 4, i - 1)));
-    if (am == 0.0) return 1;
+    if (!(am > 0.0) || !isfinite(am)) return 1;   // zero row, or an entry that is not finite
     vwk[i] = 1.0 / am;
     idx[i] = i;
   }
@@ -105,7 +105,7 @@ __device__ static int d_ludcmp_band5(int n, const double *A, double *lu, int *pi
     int jst = max(i - nb1, 1), jed = min(i + nb1, n);
     double am = fabs(M5(A, i - jst + nb1 + 1, jst));
     for (int j = jst + 1; j <= jed; j++) am = fmax(am, fabs(M5(A, i - j + nb1 + 1, j)));
-    if (am == 0.0) return 1;
+    if (!(am > 0.0) || !isfinite(am)) return 1;   // zero row, or an entry that is not finite
     vv[i] = 1.0 / am;
     idx[i] = i;
   }
@@ -976,6 +976,59 @@ int rj_energies(Ctx &c, double out[7]) {
     if (!std::isfinite(out[q])) {
       set_error("non-finite value in the energy diagnostics");
       return CB2_ERR_NAN;
+    }
+  return 0;
+}
+
+// per-(l,m) radial integrals ej[q][jj] grouped by degree l (kind 0), order
+// |m| (kind 1) and l - |m| (kind 2): one thread per (kind, q, group g) sums
+// its modes in a fixed order (sum_sph_rms_data.f90 set_sum_table_4_sph_spectr,
+// sum_sph_v_rms_by_degree)
+__global__ void k_energy_group(int L, int jmax, const int *moff, const double *ej, double *out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x, q = blockIdx.y, kind = blockIdx.z;
+  if (g > L) return;
+  const double *e = ej + (size_t)q * jmax;
+  double s = 0.0;
+  if (kind == 0) {
+    for (int m = 0; m <= g; m++) {
+      s += e[moff[m] + (g - m)];
+      if (m > 0) s += e[moff[m] + (L + 1 - m) + (g - m)];
+    }
+  } else if (kind == 1) {
+    for (int l = g; l <= L; l++) {
+      s += e[moff[g] + (l - g)];
+      if (g > 0) s += e[moff[g] + (L + 1 - g) + (l - g)];
+    }
+  } else {
+    for (int m = 0; m + g <= L; m++) {
+      s += e[moff[m] + g];
+      if (m > 0) s += e[moff[m] + (L + 1 - m) + g];
+    }
+  }
+  out[((size_t)kind * 7 + q) * (L + 1) + g] = s;
+}
+
+int rj_energy_spectra(Ctx &c, double *out_l, double *out_m, double *out_lm) {
+  k_energy_j<<<cdiv(c.jmax, 128), 128, 0, c.stream>>>(c.rj_args(), fields(c), c.d_g11, c.d_g12, c.d_ene);
+  // the grouped sums go to the temporary slot array (3 x 7 x (L+1) << nr jmax)
+  double *grp = c.d_tmp;
+  k_energy_group<<<dim3(cdiv(c.L + 1, 128), 7, 3), 128, 0, c.stream>>>(c.L, c.jmax, c.d_moff, c.d_ene, grp);
+  CB2_CUDA(cudaGetLastError());
+  const size_t n = 7 * (size_t)(c.L + 1);
+  std::vector<double> h(3 * n);
+  CB2_CUDA(cudaMemcpyAsync(h.data(), grp, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  CB2_CUDA(cudaStreamSynchronize(c.stream));
+  const double ri = c.h_r[c.kin], ro = c.h_r[c.kout];
+  const double avol = 3.0 / (ro * ro * ro - ri * ri * ri);
+  double *outs[3] = {out_l, out_m, out_lm};
+  for (int kind = 0; kind < 3; kind++)
+    for (size_t i = 0; i < n; i++) {
+      const double v = avol * h[kind * n + i];
+      if (!std::isfinite(v)) {
+        set_error("non-finite value in the energy spectra");
+        return CB2_ERR_NAN;
+      }
+      outs[kind][i] = v;
     }
   return 0;
 }

@@ -12,10 +12,20 @@ this module                    reference (src/Fortran_libraries/...)
                                + first ``nonlinear``
 ``SPH_analyze_MHD(n)``         ``SPH_analyze_MHD`` (SPH_analyzer_MHD.f90:115-202)
 ``energies()``                 ``cal_rms_sph_outer_core`` -> sph_pwr_volume_s.dat row
-``sel_backward_legendre_trans``  the backward SHT (legendre_transform_select.f90:309,
-                               MHD_FFT_selector.F90:219) from spectra to grid
-``sel_forward_legendre_trans``   the forward SHT (legendre_transform_select.f90:375,
-                               MHD_FFT_selector.F90:185) from grid to spectra
+``sel_backward_legendre_trans``  the backward Legendre transform alone on the
+                               reference's rlm / rtm buffers
+                               (legendre_transform_select.f90:309-317)
+``sel_forward_legendre_trans``   the forward Legendre transform alone
+                               (legendre_transform_select.f90:375-383)
+``back_MHD_FFT_sel_from_recv``   the backward FFT alone, rtm -> rtp
+                               (MHD_FFT_selector.F90:219-249)
+``fwd_MHD_FFT_sel_from_recv``    the forward FFT alone, rtp -> rtm
+                               (MHD_FFT_selector.F90:185-215)
+``sph_back_trans``             the whole backward transform, spectra (rj) to
+                               grid (the Legendre and FFT stages of
+                               sph_back_trans_4_MHD, sph_transforms_4_MHD.f90:152-172)
+``sph_forward_trans``          the whole forward transform, grid to spectra
+                               (sph_forward_trans_4_MHD, :176-195)
 =============================  ==============================================
 
 Errors come back as :class:`CalypsoError` (the reference aborts through
@@ -46,8 +56,71 @@ TUNE_BWD_KT, TUNE_FWD_KT, TUNE_PACK_KC, TUNE_FFT_THREADS, TUNE_CN = range(5)
 TUNE_N = 5
 
 
+# status codes of the C ABI (include/calypso_b200.h)
+ERR_ARG, ERR_CUDA, ERR_SINGULAR, ERR_NAN, ERR_STATE, ERR_TIMEOUT = -1, -2, -3, -4, -5, -6
+
+
 class CalypsoError(RuntimeError):
-    pass
+    """A failed library call; `code` is its CB2_ERR_* status."""
+
+    def __init__(self, msg, code=None):
+        super().__init__(msg)
+        self.code = code
+
+
+class SphTables(ctypes.Structure):
+    """cb2_sph_tables: index tables of a single-domain grid in the form the
+    reference's module m_spheric_parameter holds them (1-based values,
+    column-major index arrays).  Build one with :func:`sph_tables`."""
+    _fields_ = [
+        ("nidx_rlm", ctypes.c_int * 2), ("istep_rlm", ctypes.c_int * 2),
+        ("idx_gl_1d_rlm_j", ctypes.POINTER(ctypes.c_int)),
+        ("nidx_rtm", ctypes.c_int * 3), ("istep_rtm", ctypes.c_int * 3),
+        ("idx_gl_1d_rtm_m", ctypes.POINTER(ctypes.c_int)),
+        ("nidx_rtp", ctypes.c_int * 3), ("istep_rtp", ctypes.c_int * 3),
+    ]
+
+
+def sph_tables(L: int, nr: int, nth: int, nph: int, j_order=None, m_order=None,
+               istep_rlm=None, istep_rtm=None, istep_rtp=None) -> SphTables:
+    """Index tables of a single-domain grid.  j_order: the (l, m) pairs of
+    the rlm index j_rlm = 1.. (default: l(l+1)+m order); m_order: the orders
+    of the rtm index mp = 1.. (default -L..L, so mp and nidx_rtm(3)-mp+1
+    are the orders +-m as the reference's transforms pair them); strides
+    default to the innermost index running fastest (j, then k; k, theta, m;
+    phi, theta, k).  The arrays stay referenced by the returned object."""
+    if j_order is None:
+        j_order = [(l, m) for l in range(L + 1) for m in range(-l, l + 1)]
+    if m_order is None:
+        m_order = list(range(-L, L + 1))
+    nj, nm = len(j_order), len(m_order)
+    jt = np.zeros((3, nj), dtype=np.int32)          # column-major nj x 3
+    for q, (l, m) in enumerate(j_order):
+        jt[:, q] = (l * (l + 1) + m + 1, l, m)
+    mt = np.zeros((2, nm), dtype=np.int32)
+    for q, m in enumerate(m_order):
+        mt[:, q] = (q + 1, m)
+    t = SphTables()
+    t.nidx_rlm[:] = (nr, nj)
+    t.istep_rlm[:] = istep_rlm or (nj, 1)
+    t.nidx_rtm[:] = (nr, nth, nm)
+    t.istep_rtm[:] = istep_rtm or (1, nr, nr * nth)
+    t.nidx_rtp[:] = (nr, nth, nph)
+    t.istep_rtp[:] = istep_rtp or (nth * nph, nph, 1)
+    t._jt, t._mt = np.ascontiguousarray(jt.reshape(-1)), np.ascontiguousarray(mt.reshape(-1))
+    t.idx_gl_1d_rlm_j = t._jt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    t.idx_gl_1d_rtm_m = t._mt.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    t.j_order, t.m_order = list(j_order), list(m_order)
+    return t
+
+
+def rlm_size(t: SphTables, ncomp: int) -> int:
+    return ncomp * ((t.nidx_rlm[0] - 1) * t.istep_rlm[0] + (t.nidx_rlm[1] - 1) * t.istep_rlm[1] + 1)
+
+
+def rtm_size(t: SphTables, ncomp: int) -> int:
+    return ncomp * ((t.nidx_rtm[0] - 1) * t.istep_rtm[0] + (t.nidx_rtm[1] - 1) * t.istep_rtm[1]
+                    + (t.nidx_rtm[2] - 1) * t.istep_rtm[2] + 1)
 
 
 class Params(ctypes.Structure):
@@ -83,7 +156,8 @@ EXPORTS = [
     "cb2_energies_static", "cb2_autotune", "cb2_get_tuning", "cb2_set_tuning",
     "cb2_ensemble_create", "cb2_ensemble_destroy", "cb2_ensemble_size", "cb2_ensemble_shell",
     "cb2_ensemble_init_fields", "cb2_ensemble_step", "cb2_ensemble_sync", "cb2_ensemble_time_steps",
-    "cb2_ensemble_energies",
+    "cb2_ensemble_energies", "cb2_leg_bwd", "cb2_leg_fwd", "cb2_fft_bwd", "cb2_fft_fwd",
+    "cb2_legendre_trans_mode", "cb2_fft_library_known", "cb2_energy_spectra", "cb2_fft_products",
 ]
 
 
@@ -136,6 +210,14 @@ def load_library(path: str = LIB_PATH):
         "cb2_ensemble_sync": ([vp], i),
         "cb2_ensemble_time_steps": ([vp, i, pd], i),
         "cb2_ensemble_energies": ([vp, pd], i),
+        "cb2_leg_bwd": ([vp, P(SphTables), i, i, i, ctypes.c_size_t, ctypes.c_size_t, vp, vp], i),
+        "cb2_leg_fwd": ([vp, P(SphTables), i, i, i, ctypes.c_size_t, ctypes.c_size_t, vp, vp], i),
+        "cb2_fft_bwd": ([vp, P(SphTables), i, ctypes.c_size_t, vp, vp], i),
+        "cb2_fft_fwd": ([vp, P(SphTables), i, vp, ctypes.c_size_t, vp], i),
+        "cb2_legendre_trans_mode": ([ctypes.c_char_p], i),
+        "cb2_fft_library_known": ([ctypes.c_char_p], i),
+        "cb2_energy_spectra": ([vp, pd, pd, pd], i),
+        "cb2_fft_products": ([vp, P(SphTables), ctypes.c_size_t, vp, ctypes.c_size_t, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -154,7 +236,7 @@ def _ptr(a: np.ndarray):
 def _check(rc: int, what: str):
     if rc != 0:
         msg = load_library().cb2_last_error().decode(errors="replace")
-        raise CalypsoError(f"{what} failed ({rc}): {msg}")
+        raise CalypsoError(f"{what} failed ({rc}): {msg}", rc)
 
 
 class SphMHD:
@@ -254,6 +336,14 @@ class SphMHD:
         _check(load_library().cb2_energies(self._h, _ptr(out)), "cb2_energies")
         return out
 
+    def energy_spectra(self) -> dict:
+        """The seven energies of energies() by degree 'l', order 'm' and
+        'lm' = l - |m|: arrays (7, L+1) (sph_pwr_volume_l/_m/_lm.dat)."""
+        out = {k: np.zeros((7, self.L + 1)) for k in ("l", "m", "lm")}
+        _check(load_library().cb2_energy_spectra(self._h, _ptr(out["l"]), _ptr(out["m"]), _ptr(out["lm"])),
+               "cb2_energy_spectra")
+        return out
+
     def stage_times(self) -> np.ndarray:
         out = np.zeros(32)
         _check(load_library().cb2_stage_times(self._h, _ptr(out)), "cb2_stage_times")
@@ -277,7 +367,8 @@ class SphMHD:
         return ene
 
     # --- transforms -----------------------------------------------------
-    def sel_backward_legendre_trans(self, nvec: int, nscal: int, spec: np.ndarray) -> np.ndarray:
+    def sph_back_trans(self, nvec: int, nscal: int, spec: np.ndarray) -> np.ndarray:
+        """Spectra (nc x nr x jmax, j = l(l+1)+m) -> grid (nc x nr x nth x nph)."""
         nc = 3 * nvec + nscal
         spec = np.ascontiguousarray(spec, dtype=np.float64).reshape(nc, self.nr, self.jmax)
         grid = np.zeros((nc, self.nr, self.nth, self.nph))
@@ -285,13 +376,89 @@ class SphMHD:
                "cb2_sht_backward")
         return grid
 
-    def sel_forward_legendre_trans(self, nvec: int, nscal: int, grid: np.ndarray) -> np.ndarray:
+    def sph_forward_trans(self, nvec: int, nscal: int, grid: np.ndarray) -> np.ndarray:
+        """Grid (nc x nr x nth x nph) -> spectra (nc x nr x jmax)."""
         nc = 3 * nvec + nscal
         grid = np.ascontiguousarray(grid, dtype=np.float64).reshape(nc, self.nr, self.nth, self.nph)
         spec = np.zeros((nc, self.nr, self.jmax))
         _check(load_library().cb2_sht_forward(self._h, nvec, nscal, _ptr(grid), _ptr(spec)),
                "cb2_sht_forward")
         return spec
+
+    # the reference's routine-level entry points on its transposed buffers
+    # (host numpy arrays or device addresses as ints; see cb2_sph_tables)
+    @staticmethod
+    def _buf(a, n):
+        if isinstance(a, int):
+            return ctypes.c_void_p(a), None
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        if a.size < n:
+            raise CalypsoError(f"buffer of {a.size} values, the tables need {n}")
+        return ctypes.c_void_p(a.ctypes.data), a
+
+    def sel_backward_legendre_trans(self, ncomp: int, nvector: int, nscalar: int, WR, tables: SphTables,
+                                    WS=None):
+        """sp_rlm (WR) -> vr_rtm (WS), Legendre transform only."""
+        n_wr, n_ws = rlm_size(tables, ncomp), rtm_size(tables, ncomp)
+        pr, keep = self._buf(WR, n_wr)
+        if WS is None:
+            WS = np.zeros(n_ws)
+        pw, out = self._buf(WS, n_ws)
+        _check(load_library().cb2_leg_bwd(self._h, ctypes.byref(tables), ncomp, nvector, nscalar,
+                                          keep.size if keep is not None else n_wr,
+                                          out.size if out is not None else n_ws, pr, pw), "cb2_leg_bwd")
+        return WS
+
+    def sel_forward_legendre_trans(self, ncomp: int, nvector: int, nscalar: int, WR, tables: SphTables,
+                                   WS=None):
+        """vr_rtm (WR) -> sp_rlm (WS), Legendre transform only."""
+        n_wr, n_ws = rtm_size(tables, ncomp), rlm_size(tables, ncomp)
+        pr, keep = self._buf(WR, n_wr)
+        if WS is None:
+            WS = np.zeros(n_ws)
+        pw, out = self._buf(WS, n_ws)
+        _check(load_library().cb2_leg_fwd(self._h, ctypes.byref(tables), ncomp, nvector, nscalar,
+                                          keep.size if keep is not None else n_wr,
+                                          out.size if out is not None else n_ws, pr, pw), "cb2_leg_fwd")
+        return WS
+
+    def back_MHD_FFT_sel_from_recv(self, ncomp: int, WR, tables: SphTables, fld_rtp=None):
+        """vr_rtm (WR) -> fld_rtp (nnod_rtp x ncomp, Fortran order), FFT only."""
+        n_wr = rtm_size(tables, ncomp)
+        nnod = self.nr * self.nth * self.nph
+        pr, keep = self._buf(WR, n_wr)
+        if fld_rtp is None:
+            fld_rtp = np.zeros(nnod * ncomp)
+        pf, _ = self._buf(fld_rtp, nnod * ncomp)
+        _check(load_library().cb2_fft_bwd(self._h, ctypes.byref(tables), ncomp,
+                                          keep.size if keep is not None else n_wr, pr, pf), "cb2_fft_bwd")
+        return fld_rtp
+
+    def fft_products(self, WR, tables: SphTables, WS=None):
+        """13 Fourier components (u, w, B, J, T) in the rtm layout -> the 12
+        product components (w x u, J x B, u x B, u T with their
+        coefficients): FFT, grid products and FFT of the time step."""
+        n_wr, n_ws = rtm_size(tables, 13), rtm_size(tables, 12)
+        pr, keep = self._buf(WR, n_wr)
+        if WS is None:
+            WS = np.zeros(n_ws)
+        pw, out = self._buf(WS, n_ws)
+        _check(load_library().cb2_fft_products(self._h, ctypes.byref(tables),
+                                               keep.size if keep is not None else n_wr, pr,
+                                               out.size if out is not None else n_ws, pw), "cb2_fft_products")
+        return WS
+
+    def fwd_MHD_FFT_sel_from_recv(self, ncomp: int, frc_rtp, tables: SphTables, WS=None):
+        """frc_rtp (nnod_rtp x ncomp, Fortran order) -> vr_rtm (WS), FFT only."""
+        n_ws = rtm_size(tables, ncomp)
+        nnod = self.nr * self.nth * self.nph
+        pf, keep = self._buf(frc_rtp, nnod * ncomp)
+        if WS is None:
+            WS = np.zeros(n_ws)
+        pw, out = self._buf(WS, n_ws)
+        _check(load_library().cb2_fft_fwd(self._h, ctypes.byref(tables), ncomp, pf,
+                                          out.size if out is not None else n_ws, pw), "cb2_fft_fwd")
+        return WS
 
     def gauss(self):
         c, w = np.zeros(self.nth), np.zeros(self.nth)
@@ -302,6 +469,15 @@ class SphMHD:
         p, dp = np.zeros(self.nth), np.zeros(self.nth)
         _check(load_library().cb2_get_plm(self._h, l, m, _ptr(p), _ptr(dp)), "cb2_get_plm")
         return p, dp
+
+
+def legendre_trans_mode(legendre_trans_loop_ctl: str) -> int:
+    """Precision a Legendre_trans_loop_ctl value selects (cb2_legendre_trans_mode)."""
+    return load_library().cb2_legendre_trans_mode((legendre_trans_loop_ctl or "").encode())
+
+
+def fft_library_known(fft_library_ctl: str) -> bool:
+    return bool(load_library().cb2_fft_library_known((fft_library_ctl or "").encode()))
 
 
 class Ensemble:

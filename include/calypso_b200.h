@@ -5,9 +5,9 @@
  * The reference (hlokavarapu/calypso) is Fortran 90; its hot path is reached
  * through module procedures with module-global state.  Each entry point
  * below names the reference routine it replaces (paths relative to the
- * reference's src/Fortran_libraries).  A Fortran host binds these with
- * bind(C) interfaces (INTEGRATION.md shows the iso_c_binding module);
- * the Python host (calypso_b200/) binds them with ctypes.
+ * reference's src/Fortran_libraries).  A Fortran host binds these with the
+ * bind(C) interfaces of include/m_calypso_b200.f90; the Python host
+ * (calypso_b200/) binds them with ctypes.
  *
  * Conventions
  *   - every call returns 0 on success or a negative CB2_ERR_* code;
@@ -37,7 +37,11 @@ extern "C" {
 #define CB2_ERR_NAN -4        /* NaN/Inf found in the energy diagnostics    */
 #define CB2_ERR_STATE -5      /* call out of order (e.g. step before start) */
 #define CB2_ERR_TIMEOUT -6    /* a bounded wait inside a tensor-core kernel
-                                 ran out; the results of that step are void */
+                                 ran out; the results of that step are void
+                                 and later launches on the context do
+                                 nothing: destroy it.  Each wait's budget is
+                                 200 ms, or CB2_PIPE_WAIT_NS (nanoseconds)
+                                 from the environment at cb2_create */
 
 #define CB2_PREC_FP64 0       /* plain path: every stage in float64          */
 #define CB2_PREC_MIXED 1      /* Legendre split-fp16 tcgen05, fp32 FFT and
@@ -107,6 +111,14 @@ int cb2_istep(const cb2_ctx *ctx);
  * Synchronises.  Returns CB2_ERR_NAN if any value is not finite
  * (MHD_src/sph_MHD/cal_sol_sph_fluid_crank.f90 check_NaN_temperature). */
 int cb2_energies(cb2_ctx *ctx, double out[7]);
+/* The seven energies of cb2_energies as volume spectra (the reference's
+ * sph_pwr_volume_l.dat, _m.dat and _lm.dat columns:
+ * PARALLEL_src/SPH_SHELL_src/sum_sph_rms_data.f90:135-192 grouping,
+ * cal_rms_by_sph_spectr.f90:74-172 per mode): out_l[q (L+1) + l] over the
+ * modes of degree l, out_m[q (L+1) + m] over order |m|, out_lm[q (L+1) + d]
+ * over l - |m| = d; q in the order of cb2_energies.  Synchronises;
+ * CB2_ERR_NAN on a non-finite value. */
+int cb2_energy_spectra(cb2_ctx *ctx, double *out_l, double *out_m, double *out_lm);
 /* The same seven values as cb2_energies, computed without allocating any
  * device memory: the partial sums go to a static array in the library (one
  * per device, 3.5 MiB) instead of a buffer of the context.  This entry point
@@ -116,8 +128,9 @@ int cb2_energies(cb2_ctx *ctx, double out[7]);
  * Limits: jmax = (L+1)^2 <= 65536 (L <= 255), else CB2_ERR_ARG.  Every call
  * on a device shares the array (it keeps the last call's contents; nothing
  * in it needs to start at zero), so calls that overlap on one device race:
- * serialise them.  The first call on a device looks the array up; make it
- * before any stream capture starts on that device.  Synchronises. */
+ * serialise them.  cb2_create looks the array up on its device, so the
+ * array's memory is reserved while a context is set up, never by a call of
+ * this function.  Synchronises. */
 int cb2_energies_static(cb2_ctx *ctx, double out[7]);
 
 /* d_rj field slot access (host buffers of nr*jmax float64).  Slot numbers:
@@ -148,6 +161,77 @@ int cb2_step_host_state(cb2_ctx *ctx, double *state, double out_energies[7]);
  * context's precision selects the Legendre / FFT arithmetic. */
 int cb2_sht_backward(cb2_ctx *ctx, int nvec, int nscal, const double *spec, double *grid);
 int cb2_sht_forward(cb2_ctx *ctx, int nvec, int nscal, const double *grid, double *spec);
+
+/* Index tables of a single-domain spherical grid, as the reference's
+ * module SERIAL_src/SPH_SPECTR_src/m_spheric_parameter.f90 holds them for
+ * its Legendre and FFT routines (Fortran order, 1-based values):
+ *   rlm spectra   sp_rlm(comp + ncomp*((k-1)*istep_rlm(1) + (j-1)*istep_rlm(2)))
+ *                 idx_gl_1d_rlm_j(j, 1:3) = global j, degree l, order m
+ *   rtm Fourier   vr_rtm(comp + ncomp*((k-1)*istep_rtm(1) + (l-1)*istep_rtm(2)
+ *                                      + (mp-1)*istep_rtm(3)))
+ *                 idx_gl_1d_rtm_m(mp, 1:2) = global index, order m (m < 0:
+ *                 the sin(|m| phi) coefficient; colatitude l is the Gauss
+ *                 node l counted from the south pole)
+ *   rtp grid      fld_rtp(inod, comp), inod = (k-1)*istep_rtp(1)
+ *                 + (l-1)*istep_rtp(2) + (p-1)*istep_rtp(3) + 1
+ * The arrays are column-major (nidx x 3 and nidx x 2) int32. */
+typedef struct cb2_sph_tables {
+  int nidx_rlm[2];              /* radial points, harmonics of the rlm layout  */
+  int istep_rlm[2];
+  const int *idx_gl_1d_rlm_j;   /* nidx_rlm(2) x 3                            */
+  int nidx_rtm[3];              /* radial points, colatitudes, orders          */
+  int istep_rtm[3];
+  const int *idx_gl_1d_rtm_m;   /* nidx_rtm(3) x 2                            */
+  int nidx_rtp[3];              /* radial points, colatitudes, longitudes      */
+  int istep_rtp[3];
+} cb2_sph_tables;
+
+/* Legendre transform alone, in the context's precision, on the reference's
+ * transposed buffers (PARALLEL_src/SPH_SHELL_src/legendre_transform_select.f90:
+ * 309-317 sel_backward_legendre_trans and 375-383 sel_forward_legendre_trans,
+ * same arguments).  Backward: WR = sp_rlm (per vector S, dS/dr, T; then the
+ * scalars) -> WS = vr_rtm (per vector v_r, v_theta, v_phi; then the
+ * scalars), WS cleared first as the reference's transforms do.  Forward:
+ * WR = vr_rtm -> WS = sp_rlm.  ncomp is the component stride (>= 3 nvector
+ * + nscalar); components beyond 3 nvector + nscalar are left alone.  WR and
+ * WS may be host or device memory (device buffers are used in place). */
+int cb2_leg_bwd(cb2_ctx *ctx, const cb2_sph_tables *t, int ncomp, int nvector, int nscalar, size_t n_WR,
+                size_t n_WS, const double *WR, double *WS);
+int cb2_leg_fwd(cb2_ctx *ctx, const cb2_sph_tables *t, int ncomp, int nvector, int nscalar, size_t n_WR,
+                size_t n_WS, const double *WR, double *WS);
+/* Longitudinal transform alone (MHD_src/sph_MHD/MHD_FFT_selector.F90:219-249
+ * back_MHD_FFT_sel_from_recv and 185-215 fwd_MHD_FFT_sel_from_recv, plus
+ * the rtm <-> rtp transposes around them): Fourier coefficients in the rtm
+ * layout (a_m, b_m with f = a_0 + sum a_m cos m phi + b_m sin m phi) <->
+ * grid fld_rtp(nnod_rtp, ncomp), nnod_rtp = nr nth nph.  Host or device
+ * buffers. */
+int cb2_fft_bwd(cb2_ctx *ctx, const cb2_sph_tables *t, int ncomp, size_t n_WR, const double *WR,
+                double *fld_rtp);
+int cb2_fft_fwd(cb2_ctx *ctx, const cb2_sph_tables *t, int ncomp, const double *frc_rtp, size_t n_WS,
+                double *WS);
+
+/* The grid-space products alone, with the FFTs around them: the kernel the
+ * time step runs for MHD_src/sph_MHD/cal_nonlinear_sph_MHD.f90:35-84
+ * (s_cal_nonlinear_sph_MHD) between back_MHD_FFT_sel_from_recv and
+ * fwd_MHD_FFT_sel_from_recv.  WR: 13 Fourier components in the rtm layout
+ * (ncomp = 13: u, w, B, J as r, theta, phi, then T); WS: 12 (ncomp = 12:
+ * c_v w x u, c_L J x B, c_i u x B, c_T u T), the coefficients of the
+ * context's parameters.  Host or device buffers. */
+int cb2_fft_products(cb2_ctx *ctx, const cb2_sph_tables *t, size_t n_WR, const double *WR, size_t n_WS,
+                     double *WS);
+
+/* Precision selected by a Legendre_trans_loop_ctl value of control_MHD
+ * (set_legendre_trans_mode_ctl, legendre_transform_select.f90:181-224):
+ * "B200_mixed" or "B200_tcgen05" (any case) -> CB2_PREC_MIXED; "B200_fp64",
+ * every loop name of the reference and an unknown value (the reference then
+ * falls back to original_loop) -> CB2_PREC_FP64.  NULL -> CB2_PREC_FP64. */
+int cb2_legendre_trans_mode(const char *legendre_trans_loop_ctl);
+/* FFT_library_ctl (set_fft_library_ctl, SERIAL_src/FFT_wrapper/
+ * m_FFT_selector.f90:60-80): 1 for the names the reference knows (fftpack,
+ * ispack, fftw, fftw3 and their _single / _field forms) and "B200", 0 for
+ * others (the reference keeps its default then).  Every name selects the
+ * library's own FFT, in the precision of the Legendre mode. */
+int cb2_fft_library_known(const char *fft_library_ctl);
 
 /* Tables computed on the device, for checking: Gauss colatitudes/weights
  * (nth), Schmidt P_l^m and dP/dtheta at the nth nodes for one (l, m>=0). */

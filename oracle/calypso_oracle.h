@@ -80,6 +80,8 @@ int calo_istep(const cal_oracle *o);
 /* volume mean square of the output file sph_pwr_volume_s.dat:
  * out[0..6] = K_pol, K_tor, K, <T^2>, M_pol, M_tor, M  (total temperature) */
 int calo_energies(cal_oracle *o, double out[7]);
+/* the seven energies by degree l, order |m| and l - |m|: out_x[q (L+1) + g] */
+int calo_energy_spectra(cal_oracle *o, double *out_l, double *out_m, double *out_lm);
 /* copy one field slot (nr*jmax doubles) out / in */
 int calo_get_field(const cal_oracle *o, int slot, double *buf);
 int calo_set_field(cal_oracle *o, int slot, const double *buf);
@@ -105,6 +107,13 @@ int calo_sht_backward(cal_oracle *o, int nvec, int nscal,
                       const double *spec, double *grid);
 int calo_sht_forward(cal_oracle *o, int nvec, int nscal,
                      const double *grid, double *spec);
+/* Legendre-only and FFT-only halves of the transforms: Fourier arrays
+ * four[c][k][i][m + L] (m < 0: the sin(|m| phi) coefficient), grids
+ * grid[c][k][i][p]; spectra as for calo_sht_* */
+int calo_leg_backward(cal_oracle *o, int nvec, int nscal, const double *spec, double *four);
+int calo_leg_forward(cal_oracle *o, int nvec, int nscal, const double *four, double *spec);
+int calo_fft_backward(cal_oracle *o, int ncomp, const double *four, double *grid);
+int calo_fft_forward(cal_oracle *o, int ncomp, const double *grid, double *four);
 
 #ifdef __cplusplus
 }

@@ -81,6 +81,11 @@ def lib():
             ("calo_get_gaunt", [vp, ctypes.c_int, P(d), P(d)]),
             ("calo_sht_backward", [vp, ctypes.c_int, ctypes.c_int, P(d), P(d)]),
             ("calo_sht_forward", [vp, ctypes.c_int, ctypes.c_int, P(d), P(d)]),
+            ("calo_energy_spectra", [vp, P(d), P(d), P(d)]),
+            ("calo_leg_backward", [vp, ctypes.c_int, ctypes.c_int, P(d), P(d)]),
+            ("calo_leg_forward", [vp, ctypes.c_int, ctypes.c_int, P(d), P(d)]),
+            ("calo_fft_backward", [vp, ctypes.c_int, P(d), P(d)]),
+            ("calo_fft_forward", [vp, ctypes.c_int, P(d), P(d)]),
         ]:
             f = getattr(L, name)
             f.argtypes = args
@@ -144,6 +149,13 @@ class Oracle:
         lib().calo_energies(self._h, _ptr(out))
         return out
 
+    def energy_spectra(self) -> dict:
+        """The seven energies by degree 'l', order 'm' and 'lm' = l - |m|,
+        each an array (7, L+1)."""
+        out = {k: np.zeros((7, self.L + 1)) for k in ("l", "m", "lm")}
+        lib().calo_energy_spectra(self._h, _ptr(out["l"]), _ptr(out["m"]), _ptr(out["lm"]))
+        return out
+
     def get_field(self, slot: int) -> np.ndarray:
         out = np.zeros((self.nr, self.jmax))
         lib().calo_get_field(self._h, slot, _ptr(out))
@@ -186,6 +198,36 @@ class Oracle:
         spec = np.zeros((nc, self.nr, self.jmax))
         lib().calo_sht_forward(self._h, nvec, nscal, _ptr(grid), _ptr(spec))
         return spec
+
+
+    # Legendre-only / FFT-only halves: Fourier arrays [c][k][theta][m + L]
+    def leg_backward(self, nvec: int, nscal: int, spec: np.ndarray) -> np.ndarray:
+        nc = 3 * nvec + nscal
+        spec = np.ascontiguousarray(spec, dtype=np.float64).reshape(nc, self.nr, self.jmax)
+        four = np.zeros((nc, self.nr, self.nth, 2 * self.L + 1))
+        lib().calo_leg_backward(self._h, nvec, nscal, _ptr(spec), _ptr(four))
+        return four
+
+    def leg_forward(self, nvec: int, nscal: int, four: np.ndarray) -> np.ndarray:
+        nc = 3 * nvec + nscal
+        four = np.ascontiguousarray(four, dtype=np.float64).reshape(nc, self.nr, self.nth, 2 * self.L + 1)
+        spec = np.zeros((nc, self.nr, self.jmax))
+        lib().calo_leg_forward(self._h, nvec, nscal, _ptr(four), _ptr(spec))
+        return spec
+
+    def fft_backward(self, four: np.ndarray) -> np.ndarray:
+        four = np.ascontiguousarray(four, dtype=np.float64)
+        nc = four.shape[0]
+        grid = np.zeros((nc, self.nr, self.nth, self.nph))
+        lib().calo_fft_backward(self._h, nc, _ptr(four), _ptr(grid))
+        return grid
+
+    def fft_forward(self, grid: np.ndarray) -> np.ndarray:
+        grid = np.ascontiguousarray(grid, dtype=np.float64)
+        nc = grid.shape[0]
+        four = np.zeros((nc, self.nr, self.nth, 2 * self.L + 1))
+        lib().calo_fft_forward(self._h, nc, _ptr(grid), _ptr(four))
+        return four
 
 
 def leadki(l1, m1, l2, m2, l3, m3) -> float:

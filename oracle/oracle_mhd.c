@@ -85,8 +85,6 @@ int calo_ludcmp_3band(int n, const double *band_a, double *lu, int *ipiv) {
   return 0;
 }
 
-static int band5_oob = 0;
-
 /* general banded LU for 5 bands (nb1 = 2, nb2 = 4) */
 int calo_ludcmp_band5(int n, const double *band_a, double *lu_in, int *ipiv) {
   const double TINY = 1.0e-30;
@@ -135,7 +133,6 @@ int calo_ludcmp_band5(int n, const double *band_a, double *lu_in, int *ipiv) {
       int kst = (j - nb2 > 1) ? j - nb2 : 1, ked = (imax + nb2 < n) ? imax + nb2 : n;
       for (k = kst; k <= ked; k++) {
         int m1 = j - k + nb2 + 1, m2 = imax - k + nb2 + 1;
-        if (m1 < 1 || m2 < 1 || m1 > 9 || m2 > 9) band5_oob++;
         long i1 = (long)(k - 1) * 9 + (m1 - 1), i2 = (long)(k - 1) * 9 + (m2 - 1);
         if (i1 < 0 || i2 < 0 || i1 >= 9L * n || i2 >= 9L * n) continue;
         double t = lu[i2];
@@ -362,7 +359,6 @@ static int build_matrices(cal_oracle *o) {
     err |= calo_ludcmp_3band(n, m3, o->temp_lu[l].lu, o->temp_lu[l].piv);
     free(vt); free(wt); free(vs); free(vp); free(m3);
   }
-  if (band5_oob) fprintf(stderr, "oracle: %d out-of-band pivot swaps\n", band5_oob);
   return err;
 }
 
@@ -933,6 +929,63 @@ static void output_stage(cal_oracle *o, double ene[7]) {
   compute_energies(o, ene);
   if (o->p.use_ref_temp)
     for (int k = 0; k < o->nr; k++) FLD(o, CALO_TEMP)[AT(o, k, 0)] -= o->reft0[k];
+}
+
+/* Volume spectra of the seven energies grouped by degree l, order |m| and
+ * l - |m| (sum_sph_rms_data.f90 set_sum_table_4_sph_spectr and
+ * sum_sph_v_rms_by_degree: per-j radial integrals of rms_vector /
+ * rms_scalar added into the group of their j, times 1/volume), with the
+ * total temperature as calo_energies.  out_x[q * (L+1) + g]. */
+int calo_energy_spectra(cal_oracle *o, double *out_l, double *out_m, double *out_lm) {
+  int ki = o->kin, ko = o->kout, L = o->L;
+  size_t n = 7 * (size_t)(L + 1);
+  memset(out_l, 0, n * sizeof(double));
+  memset(out_m, 0, n * sizeof(double));
+  memset(out_lm, 0, n * sizeof(double));
+  if (o->p.use_ref_temp)
+    for (int k = 0; k < o->nr; k++) FLD(o, CALO_TEMP)[AT(o, k, 0)] += o->reft0[k];
+  double *f = malloc(o->nr * 7 * sizeof(double));
+  for (int j = 0; j < o->jmax; j++) {
+    for (int k = 0; k < o->nr; k++) {
+      size_t a = AT(o, k, j);
+      double a1 = o->ar1[k];
+      for (int v = 0; v < 2; v++) {
+        int s = v ? CALO_MAGNE : CALO_VELO, q0 = v ? 4 : 0;
+        double S = FLD(o, s)[a], dS = FLD(o, s + 1)[a], T = FLD(o, s + 2)[a], p, t;
+        if (j == 0) {
+          p = (0.5 * S) * (0.5 * S) * a1 * a1;
+          t = 0.0;
+        } else {
+          p = o->g12[j] * (o->g3[j] * a1 * a1 * S * S + dS * dS);
+          t = o->g12[j] * T * T;
+        }
+        f[7 * k + q0] = 0.5 * p;
+        f[7 * k + q0 + 1] = 0.5 * t;
+        f[7 * k + q0 + 2] = 0.5 * (p + t);
+      }
+      double tv = FLD(o, CALO_TEMP)[a];
+      f[7 * k + 3] = tv * tv * o->g11[j] * o->r[k] * o->r[k];
+    }
+    int l = o->jl[j], m = abs(o->jm[j]);
+    for (int q = 0; q < 7; q++) {
+      double fi = 0.0;
+      for (int kr = ki; kr < ko; kr++)
+        fi = fi + 0.5 * (o->r[kr + 1] - o->r[kr]) * (f[7 * kr + q] + f[7 * (kr + 1) + q]);
+      out_l[q * (L + 1) + l] += fi;
+      out_m[q * (L + 1) + m] += fi;
+      out_lm[q * (L + 1) + (l - m)] += fi;
+    }
+  }
+  free(f);
+  if (o->p.use_ref_temp)
+    for (int k = 0; k < o->nr; k++) FLD(o, CALO_TEMP)[AT(o, k, 0)] -= o->reft0[k];
+  double avol = 3.0 / (pow(o->r[ko], 3) - pow(o->r[ki], 3));
+  for (size_t i = 0; i < n; i++) {
+    out_l[i] *= avol;
+    out_m[i] *= avol;
+    out_lm[i] *= avol;
+  }
+  return 0;
 }
 
 /* energies of the current state without touching it (initial state) */

@@ -389,6 +389,96 @@ int calo_sht_forward(cal_oracle *o, int nvec, int nscal,
   return 0;
 }
 
+/* The two halves of calo_sht_backward / calo_sht_forward on their own, for
+ * the Legendre-only and FFT-only entry points (legendre_transform_select.f90:
+ * 309-439, MHD_FFT_selector.F90:185-249).  Fourier arrays are
+ * four[c][k][i][m + L], m = -L..L (m < 0: the sin(|m| phi) coefficient);
+ * grids grid[c][k][i][p]. */
+int calo_leg_backward(cal_oracle *o, int nvec, int nscal, const double *spec, double *four) {
+  int ncomp = 3 * nvec + nscal, nth = o->nth, L = o->L, nr = o->nr;
+  size_t fs = (size_t)nr * o->jmax, cs = (size_t)nth * (2 * L + 1);
+  const double **sp = malloc(ncomp * sizeof(double *));
+  for (int c = 0; c < ncomp; c++) sp[c] = spec + c * fs;
+#pragma omp parallel
+  {
+    double *f = malloc((size_t)ncomp * cs * sizeof(double));
+#pragma omp for schedule(dynamic)
+    for (int k = 0; k < nr; k++) {
+      leg_bwd_k(o, k, nvec, nscal, sp, f);
+      for (int c = 0; c < ncomp; c++)
+        memcpy(four + ((size_t)c * nr + k) * cs, f + (size_t)c * cs, cs * sizeof(double));
+    }
+    free(f);
+  }
+  free(sp);
+  return 0;
+}
+
+int calo_leg_forward(cal_oracle *o, int nvec, int nscal, const double *four, double *spec) {
+  int ncomp = 3 * nvec + nscal, nth = o->nth, L = o->L, nr = o->nr;
+  size_t fs = (size_t)nr * o->jmax, cs = (size_t)nth * (2 * L + 1);
+  double **sp = malloc(ncomp * sizeof(double *));
+  for (int c = 0; c < ncomp; c++) {
+    sp[c] = spec + c * fs;
+    memset(sp[c], 0, fs * sizeof(double));
+  }
+#pragma omp parallel
+  {
+    double *f = malloc((size_t)ncomp * cs * sizeof(double));
+#pragma omp for schedule(dynamic)
+    for (int k = 0; k < nr; k++) {
+      for (int c = 0; c < ncomp; c++)
+        memcpy(f + (size_t)c * cs, four + ((size_t)c * nr + k) * cs, cs * sizeof(double));
+      leg_fwd_k(o, k, nvec, nscal, f, sp);
+    }
+    free(f);
+  }
+  free(sp);
+  return 0;
+}
+
+int calo_fft_backward(cal_oracle *o, int ncomp, const double *four, double *grid) {
+  int nth = o->nth, nph = o->nph, L = o->L, nr = o->nr;
+  size_t cs = (size_t)nth * (2 * L + 1), gs = (size_t)nth * nph;
+#pragma omp parallel
+  {
+    double *f = malloc((size_t)ncomp * cs * sizeof(double));
+    double *g = malloc((size_t)ncomp * gs * sizeof(double));
+    double *wa = malloc(2 * (L + 1) * sizeof(double)), *wb = malloc(2 * (L + 1) * sizeof(double));
+#pragma omp for schedule(dynamic)
+    for (int k = 0; k < nr; k++) {
+      for (int c = 0; c < ncomp; c++)
+        memcpy(f + (size_t)c * cs, four + ((size_t)c * nr + k) * cs, cs * sizeof(double));
+      four_to_grid_rows(o, ncomp, f, g, wa, wb);
+      for (int c = 0; c < ncomp; c++)
+        memcpy(grid + ((size_t)c * nr + k) * gs, g + (size_t)c * gs, gs * sizeof(double));
+    }
+    free(f); free(g); free(wa); free(wb);
+  }
+  return 0;
+}
+
+int calo_fft_forward(cal_oracle *o, int ncomp, const double *grid, double *four) {
+  int nth = o->nth, nph = o->nph, L = o->L, nr = o->nr;
+  size_t cs = (size_t)nth * (2 * L + 1), gs = (size_t)nth * nph;
+#pragma omp parallel
+  {
+    double *f = malloc((size_t)ncomp * cs * sizeof(double));
+    double *g = malloc((size_t)ncomp * gs * sizeof(double));
+    double *wa = malloc(2 * (L + 1) * sizeof(double)), *wb = malloc(2 * (L + 1) * sizeof(double));
+#pragma omp for schedule(dynamic)
+    for (int k = 0; k < nr; k++) {
+      for (int c = 0; c < ncomp; c++)
+        memcpy(g + (size_t)c * gs, grid + ((size_t)c * nr + k) * gs, gs * sizeof(double));
+      grid_to_four_rows(o, ncomp, g, f, wa, wb);
+      for (int c = 0; c < ncomp; c++)
+        memcpy(four + ((size_t)c * nr + k) * cs, f + (size_t)c * cs, cs * sizeof(double));
+    }
+    free(f); free(g); free(wa); free(wb);
+  }
+  return 0;
+}
+
 /* Nonlinear terms by the pseudo-spectral method (F/MHD_src/sph_MHD/
  * cal_nonlinear.f90 nonlinear_by_pseudo_sph, sph_transforms_4_MHD.f90,
  * cal_nonlinear_sph_MHD.f90:35-84, F/SERIAL_src/BASE/cal_products_smp.f90):

@@ -69,3 +69,28 @@ def test_unsupported_boundary_rejected():
     bad = _read("control_MHD").replace("non_slip_sph  ICB", "free_slip_sph  ICB")
     with pytest.raises(ValueError):
         shell_params_from_control(bad, _read("control_sph_shell"))
+
+
+def test_legendre_trans_loop_ctl_selects_the_precision():
+    # the C ABI's mapping (no GPU work): the B200 names pick the mixed path,
+    # every name of the reference and unknown values the float64 path (the
+    # reference falls back to original_loop for an unknown value)
+    from calypso_b200 import PREC_FP64, PREC_MIXED, fft_library_known, legendre_trans_mode
+    assert legendre_trans_mode("B200_mixed") == PREC_MIXED
+    assert legendre_trans_mode("b200_TCGEN05   ") == PREC_MIXED
+    assert legendre_trans_mode("B200_fp64") == PREC_FP64
+    for name in ("original_loop", "symmetric_matmul", "symmetric_BLAS_big", "test_loop", "no_such_loop", ""):
+        assert legendre_trans_mode(name) == PREC_FP64, name
+    for name in ("fftpack", "FFTW3", "fftw_single", "ispack", "B200"):
+        assert fft_library_known(name), name
+    assert not fft_library_known("cufft")
+
+
+def test_precision_from_control_file():
+    from calypso_b200 import PREC_FP64, PREC_MIXED
+    from calypso_b200.control import precision_from_control
+    txt = _read("control_MHD")
+    assert precision_from_control(txt) == PREC_FP64          # 'SYMMETRIC_MATMUL'
+    mixed = txt.replace("'SYMMETRIC_MATMUL'", "'B200_mixed'")
+    assert mixed != txt
+    assert precision_from_control(mixed) == PREC_MIXED

@@ -59,11 +59,11 @@ def test_sht_fp64_matches_oracle(oracle_lib, case1, nvec, nscal):
     nc = 3 * nvec + nscal
     zl0 = [3 * v + 1 for v in range(nvec)] + [3 * v + 2 for v in range(nvec)]
     spec = random_spec(g.L, g.nr, nc, 7 + nc, zero_l0=zl0)
-    grid_g = g.sel_backward_legendre_trans(nvec, nscal, spec)
+    grid_g = g.sph_back_trans(nvec, nscal, spec)
     grid_o = o.sht_backward(nvec, nscal, spec)
     for c in range(nc):
         assert rel_l2(grid_g[c], grid_o[c]) < 1e-12, c
-    back_g = g.sel_forward_legendre_trans(nvec, nscal, grid_o)
+    back_g = g.sph_forward_trans(nvec, nscal, grid_o)
     back_o = o.sht_forward(nvec, nscal, grid_o)
     for c in range(nc):
         assert rel_l2(back_g[c], back_o[c]) < 1e-12, c
@@ -139,3 +139,38 @@ def test_host_state_step_matches_device_step(case1):
     b.step_host_state(state)
     for q, s in enumerate(slots):
         np.testing.assert_allclose(state[q], a.get_field(s), rtol=0, atol=1e-12 * np.abs(a.get_field(s)).max() + 1e-300)
+
+
+def test_energy_spectra_match_oracle(oracle_lib, case1):
+    """Volume spectra by l, |m| and l - |m| (sph_pwr_volume_l/_m/_lm.dat)
+    after 20 steps of case 1: 1e-10 relative to each spectrum's total; each
+    spectrum sums to the volume energies."""
+    g = SphMHD(case1, PREC_FP64)
+    o = oracle_lib.Oracle(case1)
+    g.init_fields(1)
+    o.init_fields(1)
+    g.step(20)
+    o.step(20)
+    sg, so = g.energy_spectra(), o.energy_spectra()
+    e = g.energies()
+    for kind in ("l", "m", "lm"):
+        a, b = sg[kind], so[kind]
+        for q in range(7):
+            tot = np.abs(b[q]).sum()
+            assert np.abs(a[q] - b[q]).max() <= 1e-10 * tot, (kind, q)
+            assert abs(a[q].sum() - e[q]) <= 1e-12 * abs(e[q]), (kind, q)
+
+
+def test_bench_shell_fp64_matches_oracle(oracle_lib):
+    """The bench workload itself (L255, Nr129, 384 x 768, seeded start):
+    the float64 path against the oracle after the Euler step and one
+    Adams-Bashforth step, 1e-10 relative L2 per field."""
+    p = configs.full_step_L255()
+    g = SphMHD(p, PREC_FP64)
+    o = oracle_lib.Oracle(dict(p, nthreads=os.cpu_count() or 1))
+    g.init_fields(2, seed=1)
+    o.init_fields(2, 1)
+    g.step(2)
+    o.step(2)
+    _compare_fields(g, o, 1e-10)
+    np.testing.assert_allclose(g.energies(), o.energies(), rtol=1e-10)
