@@ -78,8 +78,10 @@ __device__ inline void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
                : "memory");
 }
 
-// wait for the phase with the given parity to complete; false after kWaitNs
-__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// wait for the phase with the given parity to complete; false after
+// budget_ns (0: one try).  The pipelines' waits take the context's budget;
+// the drains after an abort (copies and MMAs still in flight) take kWaitNs.
+__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned long long budget_ns = kWaitNs) {
   const uint32_t addr = smem_u32(bar);
   unsigned long long t0 = 0;
   for (uint32_t it = 0;; ++it) {
@@ -92,9 +94,10 @@ __device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity) {
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
+    if (budget_ns == 0) return false;
     if (it == 64) t0 = globaltimer();
     if (it > 64) {
-      if (globaltimer() - t0 > kWaitNs) return false;
+      if (globaltimer() - t0 > budget_ns) return false;
       __nanosleep(32);
     }
   }
@@ -233,6 +236,7 @@ struct FwdArgs {
   const int *roff, *nlp; // B row offset and number of degrees of (m, parity)
   const float *rowmax;   // [m][element], k_rowmax_four
   int *status;
+  unsigned long long wait_ns;   // budget of each pipeline wait (Ctx::pipe_wait_ns)
 };
 
 // shared-memory descriptor, K-major, 64-byte swizzle (8-row groups 512 bytes apart)
@@ -401,7 +405,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
           const int tb = q.g ? (b >> 1) : b, part = q.g ? (b & 1) : 0;
           if (part == 0) {
             const uint32_t rs = nraw % FRS;
-            if (nraw >= FRS && !mbar_wait(&sb->rawempty[rs], ((nraw / FRS) - 1) & 1)) { bad = true; break; }
+            if (nraw >= FRS && !mbar_wait(&sb->rawempty[rs], ((nraw / FRS) - 1) & 1, a.wait_ns)) { bad = true; break; }
             unsigned char *dst = raw0 + rs * RAW_BYTES;
             mbar_expect_tx(&sb->rawfull[rs], RAW_BYTES);
             const uint64_t pf = policy_evict_first();
@@ -411,7 +415,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             nraw++;
           }
           const uint32_t s = nab % FAB;
-          if (nab >= FAB && !mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1)) { bad = true; break; }
+          if (nab >= FAB && !mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1, a.wait_ns)) { bad = true; break; }
           unsigned char *bb = ab0 + s * AB_BYTES + 4 * FA_BYTES;
           mbar_expect_tx(&sb->bfull[s], bbytes);
           const int x = part * a.nhp + tb * FKB;
@@ -449,12 +453,12 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
         if (ws_aborted(sb)) { bad = true; break; }
         const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
         const int ab = i % nacc;
-        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1)) { bad = true; break; }
+        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1, a.wait_ns)) { bad = true; break; }
         tc_fence_after();
         const uint32_t accb = tmem + (uint32_t)ab * accw;
         for (int b = 0; b < q.NB; b++) {
           const uint32_t s = nab % FAB, ph = (nab / FAB) & 1;
-          if (!mbar_wait(&sb->afull[s], ph) || !mbar_wait(&sb->bfull[s], ph)) { bad = true; break; }
+          if (!mbar_wait(&sb->afull[s], ph, a.wait_ns) || !mbar_wait(&sb->bfull[s], ph, a.wait_ns)) { bad = true; break; }
           tc_fence_after();
           unsigned char *at = ab0 + s * AB_BYTES, *bb = at + 4 * FA_BYTES;
           for (int p = 0; p < 2; p++) {
@@ -500,8 +504,8 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
         const int tb = q.g ? (b >> 1) : b, part = q.g ? (b & 1) : 0;
         const uint32_t rs = nraw % FRS, s = nab % FAB;
         bool ok = true;
-        if (part == 0) ok = mbar_wait(&sb->rawfull[rs], (nraw / FRS) & 1);
-        if (ok && nab >= FAB) ok = mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1);
+        if (part == 0) ok = mbar_wait(&sb->rawfull[rs], (nraw / FRS) & 1, a.wait_ns);
+        if (ok && nab >= FAB) ok = mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1, a.wait_ns);
         if (!__all_sync(0xffffffffu, ok)) { bad = true; break; }
         // the two folds of this row's 16 K values; gemm P and the mP part
         // use fold p, the dP part fold 1 - p (with the signs of its rows)
@@ -605,7 +609,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
         moff[lane] = off; mc[lane] = cr; mg[lane] = sel;
       }
       const int ab = i % nacc;
-      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1);
+      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1, a.wait_ns);
       if (!__all_sync(0xffffffffu, ok)) { sb->abort = 1; break; }
       tc_fence_after();
       const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)(qd * 32 + hf * 16) << 16);
@@ -780,6 +784,7 @@ struct BwdArgs {
   const float *bunscale;   // [gemm][m][nhp] 1 / column scale of B
   MLayout out;
   int *status;
+  unsigned long long wait_ns;   // budget of each pipeline wait (Ctx::pipe_wait_ns)
 };
 
 constexpr uint32_t BRAW_BYTES = FKB * TM * 4;   // raw rows of one K block
@@ -904,7 +909,7 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
           int p, part, ib, len;
           bwd_blk(q, b, p, part, ib, len);
           const uint32_t s = n % BW_ST;
-          if (n >= BW_ST && !mbar_wait(&sb->empty[s], ((n / BW_ST) - 1) & 1)) { bad = true; break; }
+          if (n >= BW_ST && !mbar_wait(&sb->empty[s], ((n / BW_ST) - 1) & 1, a.wait_ns)) { bad = true; break; }
           unsigned char *st = base + s * ST_BYTES;
           // raw rows: parity of l-m of this part
           const int par = (q.g == 0) ? p : (part == 0 ? 1 - p : p);
@@ -937,14 +942,14 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
         if (ws_aborted(sb)) { bad = true; break; }
         const BwdTile q = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
         const int ab = i % nacc;
-        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1)) { bad = true; break; }
+        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1, a.wait_ns)) { bad = true; break; }
         tc_fence_after();
         const uint32_t accb = tmem + (uint32_t)ab * accw;
         for (int b = 0; b < q.total; b++) {
           int p, part, ib, len;
           bwd_blk(q, b, p, part, ib, len);
           const uint32_t s = n % BW_ST, ph = (n / BW_ST) & 1;
-          if (!mbar_wait(&sb->afull[s], ph) || !mbar_wait(&sb->full[s], ph)) { bad = true; break; }
+          if (!mbar_wait(&sb->afull[s], ph, a.wait_ns) || !mbar_wait(&sb->full[s], ph, a.wait_ns)) { bad = true; break; }
           tc_fence_after();
           unsigned char *ahi = base + s * ST_BYTES + BRAW_BYTES, *alo = ahi + FA_BYTES;
           unsigned char *bh = alo + FA_BYTES, *bl = bh + B_BYTES;
@@ -1000,7 +1005,7 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
         int p, part, ib, len;
         bwd_blk(q, b, p, part, ib, len);
         const uint32_t s = n % BW_ST;
-        if (!__all_sync(0xffffffffu, mbar_wait(&sb->full[s], (n / BW_ST) & 1))) { bad = true; break; }
+        if (!__all_sync(0xffffffffu, mbar_wait(&sb->full[s], (n / BW_ST) & 1, a.wait_ns))) { bad = true; break; }
         unsigned char *st = base + s * ST_BYTES;
         const float *raw = reinterpret_cast<const float *>(st);
         int src = r;
@@ -1060,7 +1065,7 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
       __syncwarp();
       const bool has1 = q.nkb1 > 0;
       const int ab = i % nacc;
-      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1);
+      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1, a.wait_ns);
       if (!__all_sync(0xffffffffu, ok)) { sb->abort = 1; break; }
       tc_fence_after();
       const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)((ew & 3) * 32) << 16);
@@ -1467,7 +1472,7 @@ int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   a.L = c.L; a.nr = c.nr; a.nh = c.nh; a.nhp = t->nhp; a.nth = c.nth; a.nvec = nvec; a.nscal = nscal;
   a.pitchP = pitchP; a.pitchD = pitchD;
   a.kbase = t->kbase; a.ko = t->bb_ko; a.maxP = t->maxP; a.maxD = t->maxD;
-  a.bunscale = t->bb_unscale; a.out = out; a.status = c.d_status;
+  a.bunscale = t->bb_unscale; a.out = out; a.status = c.d_status; a.wait_ns = c.pipe_wait_ns;
   const int rows0 = ng * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
   const int ntiles = (tiles0 + tiles1) * (c.L + 1);
@@ -1490,6 +1495,7 @@ int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots) {
   a.bunscale = t->bf_unscale; a.roff = t->bf_roff; a.nlp = t->bf_nl;
   a.rowmax = t->rowmax_four;
   a.status = c.d_status;
+  a.wait_ns = c.pipe_wait_ns;
   // raw Fourier rows: float32 [(m, theta)][element], boxes of 128 elements x 32 colatitudes
   CUtensorMap rawP{}, rawD{};
   const uint64_t nthr = (uint64_t)(c.L + 1) * c.nth;

@@ -19,9 +19,12 @@
 //     later reads.  Two calls whose work overlaps on the same device (two
 //     host threads, or two contexts on different streams) race on the array
 //     and may return each other's sums: serialise them.
-//   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it; make
-//     that first call before any stream capture begins on the device.
+//   * cb2_create looks up the array's device address on its device with
+//     cudaGetSymbolAddress (with that device current) and caches it, so the
+//     module that holds the array is loaded -- and its memory reserved --
+//     while the context is set up (with lazy module loading, the CUDA
+//     default, that would otherwise happen at the first call).  No call of
+//     cb2_energies_static itself allocates.
 #include <mutex>
 
 #include "cb2_internal.cuh"
@@ -59,6 +62,12 @@ int scratch_on(int device, double **out) {
 }
 
 }  // namespace
+
+int static_scratch_setup(int device) {
+  double *p = nullptr;
+  return scratch_on(device, &p);
+}
+
 }  // namespace cb2
 
 using namespace cb2;

@@ -48,6 +48,30 @@ def test_energies_static_matches_energies_twice():
     g.close()
 
 
+def _free_device_bytes():
+    """cudaMemGetInfo's free bytes on the current device (the CUDA runtime
+    the library itself loaded)."""
+    rt = ctypes.CDLL("libcudart.so.12")
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    assert rt.cudaMemGetInfo(ctypes.byref(free), ctypes.byref(total)) == 0
+    return free.value
+
+
+def test_energies_static_allocates_nothing():
+    # the context is created (which reserves the static scratch) and warmed
+    # up first; after that, many calls leave the device's free memory as it was
+    _, f = _static_entry()
+    g = SphMHD(configs.dynamobench_case1(), PREC_FP64)
+    g.init_fields(1)
+    g.step(2)
+    _call(f, g)
+    before = _free_device_bytes()
+    for _ in range(50):
+        _call(f, g)
+    assert _free_device_bytes() == before
+    g.close()
+
+
 def test_energies_static_rejects_truncation_beyond_scratch():
     lib, f = _static_entry()
     # L = 256: jmax = 66049 > 65536 (smallest grid the library accepts)
