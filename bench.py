@@ -139,40 +139,117 @@ def job_value(ms, steps, world):
     return world * steps / (ms / 1000.0)
 
 
+# the reference arm times at most this many steps (and warm-up steps): one
+# oracle step at L255 / Nr129 takes about 5 s on 16 host cores
+REF_MAX_STEPS, REF_MAX_WARMUP = 30, 5
+DATA = "synthetic: seeded thermal perturbation (l<=8) + dipole seed field"
+
+
+def workload_config(params, workload):
+    """The workload both arms run (identical in both JSON lines)."""
+    E = 2.0 / params["coef_cor"]
+    return {"workload": workload, "L": params["ltr"], "Nr": params["nr"], "Ntheta": params["nth"],
+            "Nphi": params["nph"], "dt": params["dt"], "E": E,
+            "Ra": params["coef_buo"] * E / (1.0 - params["r_icb"] / params["r_cmb"]),
+            "Pr": 1.0 / params["coef_d_temp"], "Pm": 1.0 / params["coef_d_magne"],
+            "start": "seeded (kind 2, seed 1 + rank)",
+            "l2": "state 3.9 GB > 126 MB L2, no flush needed"}
+
+
+def oracle_steps(params, cores, n_warm, n_timed):
+    """Wall time of n_timed oracle steps after n_warm (the first is the
+    Euler step, so timed steps are Adams-Bashforth steps when n_warm >= 1)."""
+    from oracle.calypso_oracle import Oracle
+    p = dict(params)
+    p["nthreads"] = cores
+    o = Oracle(p)
+    o.init_fields(2, 1)
+    o.step(n_warm)
+    t0 = time.perf_counter()
+    o.step(n_timed)
+    dt = time.perf_counter() - t0
+    o.close()
+    return dt
+
+
 def run_reference(args, params):
     """The reference's algorithm on the host cores (oracle port), rank 0 only."""
     rank, _, world = env_rank()
     if rank != 0:
         return
-    from oracle.calypso_oracle import Oracle
     cores = os.cpu_count() or 1
-    p = dict(params)
-    p["nthreads"] = cores
-    o = Oracle(p)
-    o.init_fields(2, 1)
-    nw = min(args.warmup, 1)
-    nt = max(1, min(args.steps, 2))
-    o.step(nw)
-    t0 = time.perf_counter()
-    o.step(nt)
-    dt = time.perf_counter() - t0
+    nw = max(1, min(args.warmup, REF_MAX_WARMUP))
+    nt = max(1, min(args.steps, REF_MAX_STEPS))
+    dt = oracle_steps(params, cores, nw, nt)
     v = nt / dt
     line = {
-        "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1000.0 * dt / nt, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic: seeded thermal perturbation (l<=8) + dipole seed field",
-        "config": {"workload": args.workload, "L": p["ltr"], "Nr": p["nr"], "Ntheta": p["nth"],
-                   "Nphi": p["nph"], "precision": "fp64 (CPU)", "parallelism": "openmp"},
+        "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world, "steps": nt,
+        "warmup": nw, "ms_per_step": 1000.0 * dt / nt, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+        "config": workload_config(params, args.workload),
+        "impl_config": {"precision": "fp64 (CPU)", "parallelism": f"openmp x{cores}"},
         "impl": "reference",
         "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": "port",
-                         "sample": f"{nt} full time step(s) after {nw} warm-up, host wall clock"},
+                         "sample": f"{nt} Adams-Bashforth steps after {nw} warm-up steps "
+                                   "(the first an Euler step), host wall clock"},
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's Fortran build is unavailable in this image (no Fortran "
                 "compiler); this arm runs the oracle, its C restatement pinned to the "
                 "reference's Dynamobench golden energies",
     }
     print(json.dumps(line), flush=True)
+
+
+def stage_times(params, prec, tuning, rank, local_rank, nst=3):
+    """Per-stage CUDA-event times (ms per step) of nst eager Adams-Bashforth
+    steps on a fresh context (CB2_TIMERS), outside the timed run."""
+    from calypso_b200 import SphMHD
+    os.environ["CB2_TIMERS"] = "1"
+    try:
+        gt = SphMHD(params, prec, device=local_rank)
+        gt.tuning = tuning
+        gt.init_fields(2, seed=1 + rank)
+        gt.step(1)
+        gt.step(nst)
+        st = gt.stage_times() / nst
+        gt.close()
+    finally:
+        os.environ.pop("CB2_TIMERS", None)
+    return st
+
+
+def stage_dict(st, tuning):
+    """Stage names of cb2_stage_times ids (the reference's timer labels)."""
+    d = ({"cn_step": st[6] + st[7]} if tuning[4] == 1 else
+         {"explicit": st[6], "implicit+rj_derived": st[7]})
+    d.update({"coriolis": st[13], "legendre_bwd": st[22], "fft_products": st[24],
+              "legendre_fwd": st[23], "rj_after_transform": st[17], "step": st[0]})
+    return d
+
+
+def dgemm_peak(local_rank):
+    """Measured float64 GEMM throughput (cuBLAS through torch.matmul, 8192^3,
+    best of 5), TFLOP/s: the yardstick of the FP64 Legendre stages."""
+    try:
+        import torch
+        dev = f"cuda:{local_rank}"
+        a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+        b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+        torch.matmul(a, b)
+        best = None
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            e1.synchronize()
+            t = e0.elapsed_time(e1)
+            best = t if best is None else min(best, t)
+        del a, b
+        torch.cuda.empty_cache()
+        return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+    except Exception:
+        return None
 
 
 def main():
@@ -234,26 +311,13 @@ def main():
     value = job_value(ms, args.steps, world)
 
     # stage breakdown (eager steps with per-stage CUDA events, not the timed run)
-    os.environ["CB2_TIMERS"] = "1"
-    gt = SphMHD(params, prec, device=local_rank)
-    gt.tuning = tuning
-    gt.init_fields(2, seed=1 + rank)
-    gt.step(1)
-    nst = 3
-    gt.step(nst)
-    st = gt.stage_times() / nst
-    gt.close()
-    os.environ.pop("CB2_TIMERS", None)
+    st = stage_times(params, prec, tuning, rank, local_rank)
 
     L, nr, nth, nph = params["ltr"], params["nr"], params["nth"], params["nph"]
     fb, ff = legendre_flops(L, nr, nth)
     peaks, peak_kind = load_peaks()
     fused_cn = tuning[4] == 1
-    stages = ({"cn_step": st[6] + st[7]} if fused_cn else
-              {"explicit": st[6], "implicit+rj_derived": st[7]})
-    stages.update({"coriolis": st[13],
-              "legendre_bwd": st[22], "fft_products": st[24], "legendre_fwd": st[23],
-              "rj_after_transform": st[17], "step": st[0]})
+    stages = stage_dict(st, tuning)
     # dominant transform stage and its roofline.  Algorithmic bytes: one read
     # of each input and one write of each output (13 spectral slots and 13
     # Fourier components backward, 12 each forward); algorithmic flops:
@@ -314,14 +378,23 @@ def main():
         ms64 = g64.time_steps(args.steps, graph=True)
         g64.step(ncmp - g64.istep, graph=True)
         e64 = g64.energies()
+        tuning64 = g64.tuning
+        g64.close()
+        st64 = stage_times(params, PREC_FP64, tuning64, rank, local_rank)
         rel = np.abs(ene_mixed - e64) / np.abs(e64)
         fp64 = {"steps_per_s": args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
                 "speedup_mixed_over_fp64": (args.steps / (ms / 1000.0)) / (args.steps / (ms64 / 1000.0)),
                 "compare_steps": ncmp,
                 "energy_rel_err_max": float(rel.max()),
                 "energy_rel_err": dict(zip(["K_pol", "K_tor", "K", "T2", "M_pol", "M_tor", "M"],
-                                           [float(x) for x in rel]))}
-        g64.close()
+                                           [float(x) for x in rel])),
+                "tuning": list(tuning64), "stages_ms": stage_dict(st64, tuning64),
+                "legendre_fp64_tflops": {"legendre_bwd": fb / (st64[22] * 1e-3) / 1e12,
+                                         "legendre_fwd": ff / (st64[23] * 1e-3) / 1e12}}
+        dg = dgemm_peak(local_rank)
+        if dg:
+            fp64["fp64_dgemm_tflops_measured"] = dg
+            fp64["legendre_frac_of_dgemm"] = {k: v / dg for k, v in fp64["legendre_fp64_tflops"].items()}
 
     # end to end through the C ABI with host-resident state (pinned buffers)
     n = g.nr * g.jmax
@@ -341,18 +414,11 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle.calypso_oracle import Oracle
         cores = os.cpu_count() or 1
-        p = dict(params)
-        p["nthreads"] = cores
-        o = Oracle(p)
-        o.init_fields(2, 1)
-        t0 = time.perf_counter()
-        o.step(1)
-        tc = time.perf_counter() - t0
-        cpu = {"value": 1.0 / tc, "unit": "steps/s", "cores": cores, "kind": "port",
-               "sample": "1 full time step (the Euler first step) at L255/Nr129 after set-up, host wall clock"}
-        o.close()
+        nc = 3
+        tc = oracle_steps(params, cores, 1, nc)
+        cpu = {"value": nc / tc, "unit": "steps/s", "cores": cores, "kind": "port",
+               "sample": f"{nc} Adams-Bashforth steps at L255/Nr129 after the Euler step, host wall clock"}
 
     if rank == 0:
         line = {
@@ -360,12 +426,10 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "fp16-split tensor / f32 FFT / f64 solves" if prec == PREC_MIXED else "f64",
-            "data": "synthetic: seeded thermal perturbation (l<=8) + dipole seed field",
-            "config": {"workload": args.workload, "L": L, "Nr": nr, "Ntheta": nth,
-                       "Nphi": params["nph"], "dt": params["dt"],
-                       "precision": args.precision, "parallelism": f"replicas x{world}",
-                       "l2": "state 3.9 GB > 126 MB L2, no flush needed", "graph": True,
-                       "tuning": list(tuning)},
+            "data": DATA,
+            "config": workload_config(params, args.workload),
+            "impl_config": {"precision": args.precision, "parallelism": f"replicas x{world}",
+                            "graph": True, "tuning": list(tuning)},
             "roofline": roof, "stages_ms": stages, "cpu_baseline": cpu, "e2e": e2e,
             "fp64_plain": fp64,
             # kernels per step: the Crank-Nicolson stage (one fused kernel, or
