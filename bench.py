@@ -252,6 +252,82 @@ def dgemm_peak(local_rank):
         return None
 
 
+def sht_roundtrip_extras(local_rank, with_oracle=True):
+    """The isolated SHT round trip at L255 / 384 x 768 / Nr65, 3 vectors + 2
+    scalars, seeded spectra with power falling as l^-2: wall time of the
+    four routine-level calls (backward Legendre, backward FFT, forward FFT,
+    forward Legendre; reference layouts, device buffers, each call
+    synchronous) per precision, and the error of each field against the
+    float64 GPU path and, when with_oracle, against the oracle (whose round
+    trip is timed on the host cores too)."""
+    import torch
+    from calypso_b200 import PREC_FP64, PREC_MIXED, SphMHD, configs, sph_tables
+    from calypso_b200.sph_mhd import rlm_size, rtm_size
+    p = configs.sht_roundtrip()
+    L, nr, nth, nph = p["ltr"], p["nr"], p["nth"], p["nph"]
+    nvec, nscal = 3, 2
+    nc = 3 * nvec + nscal
+    spec = configs.sht_roundtrip_spectra(L, nr, nvec, nscal)
+    t = sph_tables(L, nr, nth, nph)
+    jg = np.array([l * (l + 1) + m for (l, m) in t.j_order])
+    WR = np.zeros(rlm_size(t, nc))
+    for c in range(nc):
+        idx = c + nc * (np.arange(nr)[:, None] * t.istep_rlm[0] + np.arange(len(jg))[None, :] * t.istep_rlm[1])
+        WR[idx] = spec[c][:, jg]
+    dev = f"cuda:{local_rank}"
+    dWR = torch.from_numpy(WR).to(dev)
+    nnod = nr * nth * nph
+    out = {"workload": "sht_roundtrip_L255_Nr65", "fields": "3 vectors + 2 scalars",
+           "timer": "host wall clock around the four synchronous calls (device buffers), best of 3"}
+    grids, backs = {}, {}
+    for prec, name in ((PREC_FP64, "fp64"), (PREC_MIXED, "mixed")):
+        g = SphMHD(p, prec, device=local_rank)
+        four = torch.zeros(rtm_size(t, nc), dtype=torch.float64, device=dev)
+        grid = torch.zeros(nnod * nc, dtype=torch.float64, device=dev)
+        four2 = torch.zeros_like(four)
+        back = torch.zeros(rlm_size(t, nc), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        best = None
+        for _ in range(3):
+            t0 = time.perf_counter()
+            g.sel_backward_legendre_trans(nc, nvec, nscal, dWR.data_ptr(), t, WS=four.data_ptr())
+            g.back_MHD_FFT_sel_from_recv(nc, four.data_ptr(), t, fld_rtp=grid.data_ptr())
+            g.fwd_MHD_FFT_sel_from_recv(nc, grid.data_ptr(), t, WS=four2.data_ptr())
+            g.sel_forward_legendre_trans(nc, nvec, nscal, four2.data_ptr(), t, WS=back.data_ptr())
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out[f"roundtrip_ms_{name}"] = 1e3 * best
+        grids[name] = grid.view(nc, nnod).cpu().numpy()
+        backs[name] = back.cpu().numpy()
+        g.close()
+        del four, grid, four2, back
+    torch.cuda.empty_cache()
+    fields = [list(range(3 * v, 3 * v + 3)) for v in range(nvec)] + [[3 * nvec + s] for s in range(nscal)]
+
+    def err(a, b):
+        return [float(np.linalg.norm(a[f] - b[f]) / np.linalg.norm(b[f])) for f in fields]
+    out["grid_err_mixed_vs_fp64"] = err(grids["mixed"], grids["fp64"])
+    rb = {k: v.reshape(-1, nc).T for k, v in backs.items()}
+    out["roundtrip_err_mixed_vs_fp64"] = err(rb["mixed"], rb["fp64"])
+    out["roundtrip_err_fp64_vs_input"] = err(rb["fp64"], WR.reshape(-1, nc).T)
+    if with_oracle:
+        from oracle.calypso_oracle import Oracle
+        cores = os.cpu_count() or 1
+        o = Oracle(dict(p, nthreads=cores))
+        t0 = time.perf_counter()
+        go = o.sht_backward(nvec, nscal, spec)
+        so = o.sht_forward(nvec, nscal, go)
+        out["cpu_roundtrip_s"] = time.perf_counter() - t0
+        out["cpu_cores"] = cores
+        o.close()
+        # the library's grid in its default rtp layout: phi fastest, then theta, k
+        gk = go.reshape(nc, -1)
+        out["grid_err_fp64_vs_oracle"] = err(grids["fp64"], gk)
+        out["grid_err_mixed_vs_oracle"] = err(grids["mixed"], gk)
+        del go, so
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -262,6 +338,7 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--no-sht", action="store_true", help="skip the SHT round-trip extra key")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variants")
     ap.add_argument("--compare-steps", type=int, default=500,
                     help="steps of the mixed and FP64 runs whose energies are compared")
@@ -412,6 +489,10 @@ def main():
            "timer": "host wall clock around cb2_step_host_state (copy in, step, copy out, energies)",
            "steps": ke}
 
+    sht = None
+    if rank == 0 and world == 1 and not args.no_sht:
+        sht = sht_roundtrip_extras(local_rank, with_oracle=not args.no_cpu_baseline)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
@@ -431,7 +512,7 @@ def main():
             "impl_config": {"precision": args.precision, "parallelism": f"replicas x{world}",
                             "graph": True, "tuning": list(tuning)},
             "roofline": roof, "stages_ms": stages, "cpu_baseline": cpu, "e2e": e2e,
-            "fp64_plain": fp64,
+            "fp64_plain": fp64, "sht_roundtrip": sht,
             # kernels per step: the Crank-Nicolson stage (one fused kernel, or
             # explicit, implicit 5-band and 3-band, two derived-field kernels);
             # Coriolis; backward Legendre (pack + GEMM when mixed); FFT +
