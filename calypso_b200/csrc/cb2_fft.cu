@@ -15,6 +15,7 @@
 // Two real rows share one complex FFT (x + i y).  The complex FFT is a
 // shared-memory Stockham autosort transform with radix 3, 4 and 2 stages,
 // N = 3^a 2^b.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -34,14 +35,20 @@ __device__ inline T2 cmul(T2 a, T2 b) {
   return r;
 }
 
-// Two real rows x, y share one complex transform z = x + i y.  The float32
-// rounding error of a transform is relative to the larger row, so a row far
-// below its partner (u x B beside u T while the field is weak, say) would
-// carry the partner's error.  The second row is therefore multiplied by
-// 2^(ex - ey), ex and ey the exponents of the two rows' largest magnitudes
-// (passed as the bit patterns of non-negative floats), which puts both rows
-// at the same size; the factor is exact and is undone after the transform.
-// 1 when either row is zero or subnormal.
+// Two real rows x, y share one complex transform z = x + i y.  The rounding
+// error of a transform is relative to the larger row, so a row far below its
+// partner would carry the partner's error.  Where the rows of a pair can be
+// of any size -- the float64 step kernel (parity with the oracle for any
+// field sizes), the generic float32 kernel and the standalone transforms of
+// caller-given components -- the second row is multiplied by 2^(ex - ey),
+// ex and ey the exponents of the two rows' largest magnitudes (passed as
+// the bit patterns of non-negative floats), which puts both rows at the
+// same size; the factor is exact and is undone after the transform (1 when
+// either row is zero or subnormal).  The float32 four-step and Stockham step
+// kernels pair rows of related size (components of one field, or a field
+// and its curl) and do without: on the L255 bench state the scaling changed
+// neither the per-term errors nor the energy drift and cost 14 % of the
+// kernel's time.
 __device__ __forceinline__ int pair_exp(unsigned mx_bits, unsigned my_bits) {
   const int ex = (int)(mx_bits >> 23), ey = (int)(my_bits >> 23);
   if (ex == 0 || ey == 0) return 0;
@@ -49,6 +56,28 @@ __device__ __forceinline__ int pair_exp(unsigned mx_bits, unsigned my_bits) {
 }
 __device__ __forceinline__ float pow2i(int e) { return __int_as_float((127 + e) << 23); }
 __device__ __forceinline__ unsigned abs_bits(float x) { return __float_as_uint(x) & 0x7FFFFFFFu; }
+
+// the same for either precision: magnitudes as ordered bit patterns and the
+// power-of-two factor of the second row (inverse when `inv`)
+template <typename T> struct PairBits;
+template <> struct PairBits<float> {
+  using U = unsigned;
+  __device__ static U abs_bits(float x) { return __float_as_uint(x) & 0x7FFFFFFFu; }
+  __device__ static float factor(U mx, U my, bool inv) {
+    const int e = pair_exp(mx, my);
+    return pow2i(inv ? -e : e);
+  }
+};
+template <> struct PairBits<double> {
+  using U = unsigned long long;
+  __device__ static U abs_bits(double x) { return (U)__double_as_longlong(x) & 0x7FFFFFFFFFFFFFFFull; }
+  __device__ static double factor(U mx, U my, bool inv) {
+    const int ex = (int)(mx >> 52), ey = (int)(my >> 52);
+    if (ex == 0 || ey == 0) return 1.0;
+    const int e = max(-1000, min(1000, ex - ey));
+    return __longlong_as_double((long long)(1023 + (inv ? -e : e)) << 52);
+  }
+};
 
 struct FFTPlan {
   int n, nst;
@@ -227,27 +256,41 @@ __global__ void __launch_bounds__(512)
 k_fft_products(FFTPlan pl, int L, int NS, const T *__restrict__ four, T *__restrict__ four2,
                const typename C2<T>::t *__restrict__ tw, ProdCoef pc) {
   using T2 = typename C2<T>::t;
+  using U = typename PairBits<T>::U;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int N = pl.n;
   T2 *A = reinterpret_cast<T2 *>(smraw);    // 7 x N
   T2 *B = A + 7 * N;                         // 7 x N
+  U *cmx = reinterpret_cast<U *>(B + 7 * N); // [13] input maxima, [13..24] product maxima (bits)
   const size_t row = blockIdx.x;
   const T *fin = four + row * 13 * NS;
   T *fout = four2 + row * 12 * NS;
   const int mmax = min(L, (N + 1) / 2 - 1);
-  // Hermitian spectra of the 7 pairs (z = x + i y)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  if (threadIdx.x < 25) cmx[threadIdx.x] = 0;
+  __syncthreads();
+  // pair scaling (pair_exp): the largest coefficient of each component
+  for (int c = warp; c < 13; c += nwarp) {
+    U mx = 0;
+    for (int q = lane; q < 2 * (mmax + 1); q += 32) mx = max(mx, PairBits<T>::abs_bits(fin[(size_t)c * NS + q]));
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, (U)__shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) cmx[c] = mx;
+  }
+  __syncthreads();
+  // Hermitian spectra of the 7 pairs (z = x + i y), the second row scaled
   for (int idx = threadIdx.x; idx < 7 * N; idx += blockDim.x) {
     int p = idx / N, n = idx - p * N;
     const T *f0 = fin + (size_t)(2 * p) * NS;
     const T *f1 = (2 * p + 1 < 13) ? fin + (size_t)(2 * p + 1) * NS : nullptr;
+    const T sy = f1 ? PairBits<T>::factor(cmx[2 * p], cmx[2 * p + 1], false) : (T)1;
     T2 z = T2{0, 0};
     if (n == 0) {
-      z = T2{f0[0], f1 ? f1[0] : (T)0};
+      z = T2{f0[0], f1 ? f1[0] * sy : (T)0};
     } else {
       int m = (n <= mmax) ? n : ((N - n <= mmax) ? N - n : -1);
       if (m > 0) {
         T a0 = f0[2 * m], b0 = f0[2 * m + 1];
-        T a1 = f1 ? f1[2 * m] : (T)0, b1 = f1 ? f1[2 * m + 1] : (T)0;
+        T a1 = f1 ? f1[2 * m] * sy : (T)0, b1 = f1 ? f1[2 * m + 1] * sy : (T)0;
         T xr = (T)0.5 * a0, xi = (T)-0.5 * b0, yr = (T)0.5 * a1, yi = (T)-0.5 * b1;
         z = (m == n) ? T2{xr - yi, xi + yr} : T2{xr + yi, -xi + yr};
       }
@@ -258,17 +301,41 @@ k_fft_products(FFTPlan pl, int L, int NS, const T *__restrict__ four, T *__restr
   T2 *g = batch_fft<T, T2>(A, B, 7, pl, tw, +1);
   T2 *h = (g == A) ? B : A;
   const T cv = (T)pc.cv, cl = (T)pc.cl, ci = (T)pc.ci, ct = (T)pc.ct;
+  T iy[6];
+#pragma unroll
+  for (int p = 0; p < 6; p++) iy[p] = PairBits<T>::factor(cmx[2 * p], cmx[2 * p + 1], true);
+  U hm[12];
+#pragma unroll
+  for (int c = 0; c < 12; c++) hm[c] = 0;
   for (int q = threadIdx.x; q < N; q += blockDim.x) {
     T2 p0 = g[0 * N + q], p1 = g[1 * N + q], p2 = g[2 * N + q], p3 = g[3 * N + q];
     T2 p4 = g[4 * N + q], p5 = g[5 * N + q], p6 = g[6 * N + q];
-    T ur = p0.x, ut = p0.y, up = p1.x, wr = p1.y, wt = p2.x, wp = p2.y;
-    T br = p3.x, bt = p3.y, bp = p4.x, jr = p4.y, jt = p5.x, jp = p5.y, tt = p6.x;
-    h[0 * N + q] = T2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv};
-    h[1 * N + q] = T2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl};
-    h[2 * N + q] = T2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl};
-    h[3 * N + q] = T2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci};
-    h[4 * N + q] = T2{(ur * bt - ut * br) * ci, ur * tt * ct};
-    h[5 * N + q] = T2{ut * tt * ct, up * tt * ct};
+    T ur = p0.x, ut = p0.y * iy[0], up = p1.x, wr = p1.y * iy[1], wt = p2.x, wp = p2.y * iy[2];
+    T br = p3.x, bt = p3.y * iy[3], bp = p4.x, jr = p4.y * iy[4], jt = p5.x, jp = p5.y * iy[5], tt = p6.x;
+    const T2 hv[6] = {T2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv},
+                      T2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl},
+                      T2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl},
+                      T2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci},
+                      T2{(ur * bt - ut * br) * ci, ur * tt * ct},
+                      T2{ut * tt * ct, up * tt * ct}};
+#pragma unroll
+    for (int p = 0; p < 6; p++) {
+      h[p * N + q] = hv[p];
+      hm[2 * p] = max(hm[2 * p], PairBits<T>::abs_bits(hv[p].x));
+      hm[2 * p + 1] = max(hm[2 * p + 1], PairBits<T>::abs_bits(hv[p].y));
+    }
+  }
+  // row maxima of the 12 product rows: every lane of every warp takes part
+#pragma unroll
+  for (int c = 0; c < 12; c++) {
+    U v = hm[c];
+    for (int o = 16; o > 0; o >>= 1) v = max(v, (U)__shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0) atomicMax(cmx + 13 + c, v);
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < 6 * N; idx += blockDim.x) {
+    const int p = idx / N;
+    h[idx].y *= PairBits<T>::factor(cmx[13 + 2 * p], cmx[14 + 2 * p], false);
   }
   __syncthreads();
   T2 *zf = batch_fft<T, T2>(h, g, 6, pl, tw, -1);
@@ -277,15 +344,16 @@ k_fft_products(FFTPlan pl, int L, int NS, const T *__restrict__ four, T *__restr
     int p = idx / (L + 1), m = idx - p * (L + 1);
     T *f0 = fout + (size_t)(2 * p) * NS, *f1 = fout + (size_t)(2 * p + 1) * NS;
     const T2 *Z = zf + p * N;
+    const T ay = an * PairBits<T>::factor(cmx[13 + 2 * p], cmx[14 + 2 * p], true);
     if (m == 0) {
       f0[0] = an * Z[0].x; f0[1] = 0;
-      f1[0] = an * Z[0].y; f1[1] = 0;
+      f1[0] = ay * Z[0].y; f1[1] = 0;
     } else {
       T2 zk = Z[m % N], zn = Z[(N - m) % N];
       T xr = (T)0.5 * (zk.x + zn.x), xi = (T)0.5 * (zk.y - zn.y);
       T yr = (T)0.5 * (zk.y + zn.y), yi = (T)-0.5 * (zk.x - zn.x);
       f0[2 * m] = (T)2 * an * xr; f0[2 * m + 1] = (T)-2 * an * xi;
-      f1[2 * m] = (T)2 * an * yr; f1[2 * m + 1] = (T)-2 * an * yi;
+      f1[2 * m] = (T)2 * ay * yr; f1[2 * m + 1] = (T)-2 * ay * yi;
     }
   }
 }
@@ -653,14 +721,11 @@ k_fft_products_t(int L, MLayout fin, MLayout fout, const float2 *__restrict__ tw
   float2 *A = reinterpret_cast<float2 *>(smraw);   // 7 x NP
   float2 *B = A + 7 * NP;                           // 7 x NP
   float2 *TW = B + 7 * NP;                          // per-stage twiddles (ntw)
-  float *SC = reinterpret_cast<float *>(TW + N);    // pair factors [7], their inverses [8..14]
-  unsigned *FMX = reinterpret_cast<unsigned *>(SC + 16);   // forward row maxima [12]
   const int M1 = L + 1, MP = M1 | 1;                // padded (odd) staging stride
   float *S = reinterpret_cast<float *>(B);          // [c * 2 + s][MP]
   const int th = blockIdx.x / fin.nr, k = blockIdx.x % fin.nr;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
   for (int e = tid; e < P::ntw(); e += blockDim.x) TW[e] = twp[e];
-  if (tid < 12) FMX[tid] = 0u;
   // input: one warp per order m, lane j < 26 reads element j of the 10 + 16 run
   {
     int cs = 0;
@@ -672,33 +737,18 @@ k_fft_products_t(int L, MLayout fin, MLayout fout, const float2 *__restrict__ tw
       for (int m = warp; m <= L; m += nwarp) S[cs * MP + m] = __ldg(src + m * mst);
   }
   __syncthreads();
-  // pair scaling (pair_exp) of the 6 full pairs; pair 6 (T alone) keeps 1
-  for (int p = warp; p < 7; p += nwarp) {
-    unsigned mx = 0u, my = 0u;
-    if (p < 6)
-      for (int m = lane; m <= L; m += 32) {
-        mx = max(mx, max(abs_bits(S[(4 * p) * MP + m]), abs_bits(S[(4 * p + 1) * MP + m])));
-        my = max(my, max(abs_bits(S[(4 * p + 2) * MP + m]), abs_bits(S[(4 * p + 3) * MP + m])));
-      }
-    mx = __reduce_max_sync(0xffffffffu, mx);
-    my = __reduce_max_sync(0xffffffffu, my);
-    const int e = pair_exp(mx, my);
-    if (lane == 0) { SC[p] = pow2i(e); SC[8 + p] = pow2i(-e); }
-  }
-  __syncthreads();
   // Hermitian rows z = x + i y of the 7 pairs: one thread per (pair, m) fills
   // n = m and n = N - m; the orders above L are zero
   for (int p = 0; p < 7; p++) {
     const int c0 = 2 * p, c1 = 2 * p + 1;
     const bool has1 = c1 < 13;
-    const float sy = SC[p];
     float2 *Z = A + p * NP;
     for (int m = tid; m <= L; m += blockDim.x) {
-      const float a0 = S[(c0 * 2) * MP + m], a1 = has1 ? S[(c1 * 2) * MP + m] * sy : 0.0f;
+      const float a0 = S[(c0 * 2) * MP + m], a1 = has1 ? S[(c1 * 2) * MP + m] : 0.0f;
       if (m == 0) {
         Z[0] = float2{a0, a1};
       } else {
-        const float b0 = S[(c0 * 2 + 1) * MP + m], b1 = has1 ? S[(c1 * 2 + 1) * MP + m] * sy : 0.0f;
+        const float b0 = S[(c0 * 2 + 1) * MP + m], b1 = has1 ? S[(c1 * 2 + 1) * MP + m] : 0.0f;
         const float xr = 0.5f * a0, xi = -0.5f * b0, yr = 0.5f * a1, yi = -0.5f * b1;
         Z[fpad(m)] = float2{xr - yi, xi + yr};
         Z[fpad(N - m)] = float2{xr + yi, -xi + yr};
@@ -710,42 +760,18 @@ k_fft_products_t(int L, MLayout fin, MLayout fout, const float2 *__restrict__ tw
   float2 *g = fft_passes<N, 7, +1, 0>(A, B, TW);
   float2 *hb = (g == A) ? B : A;
   const float cv = (float)pc.cv, cl = (float)pc.cl, ci = (float)pc.ci, ct = (float)pc.ct;
-  {
-    const float i0 = SC[8], i1 = SC[9], i2 = SC[10], i3 = SC[11], i4 = SC[12], i5 = SC[13];
-    unsigned hm[12];
-#pragma unroll
-    for (int c = 0; c < 12; c++) hm[c] = 0u;
-    for (int qq = tid; qq < N; qq += blockDim.x) {
-      const int q = fpad(qq);
-      const float2 p0 = g[0 * NP + q], p1 = g[1 * NP + q], p2 = g[2 * NP + q], p3 = g[3 * NP + q];
-      const float2 p4 = g[4 * NP + q], p5 = g[5 * NP + q], p6 = g[6 * NP + q];
-      const float ur = p0.x, ut = p0.y * i0, up = p1.x, wr = p1.y * i1, wt = p2.x, wp = p2.y * i2;
-      const float br = p3.x, bt = p3.y * i3, bp = p4.x, jr = p4.y * i4, jt = p5.x, jp = p5.y * i5, tt = p6.x;
-      const float2 h[6] = {float2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv},
-                           float2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl},
-                           float2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl},
-                           float2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci},
-                           float2{(ur * bt - ut * br) * ci, ur * tt * ct},
-                           float2{ut * tt * ct, up * tt * ct}};
-#pragma unroll
-      for (int p = 0; p < 6; p++) {
-        hb[p * NP + q] = h[p];
-        hm[2 * p] = max(hm[2 * p], abs_bits(h[p].x));
-        hm[2 * p + 1] = max(hm[2 * p + 1], abs_bits(h[p].y));
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < 12; c++) {
-      const unsigned r = __reduce_max_sync(0xffffffffu, hm[c]);
-      if (lane == 0) atomicMax(FMX + c, r);
-    }
-  }
-  __syncthreads();
-  // forward pair scaling: the second row of each product pair to the size of the first
-  for (int idx = tid; idx < 6 * N; idx += blockDim.x) {
-    const int p = idx / N, q = fpad(idx - p * N);
-    const int e = pair_exp(FMX[2 * p], FMX[2 * p + 1]);
-    if (e != 0) hb[p * NP + q].y *= pow2i(e);
+  for (int qq = tid; qq < N; qq += blockDim.x) {
+    const int q = fpad(qq);
+    const float2 p0 = g[0 * NP + q], p1 = g[1 * NP + q], p2 = g[2 * NP + q], p3 = g[3 * NP + q];
+    const float2 p4 = g[4 * NP + q], p5 = g[5 * NP + q], p6 = g[6 * NP + q];
+    const float ur = p0.x, ut = p0.y, up = p1.x, wr = p1.y, wt = p2.x, wp = p2.y;
+    const float br = p3.x, bt = p3.y, bp = p4.x, jr = p4.y, jt = p5.x, jp = p5.y, tt = p6.x;
+    hb[0 * NP + q] = float2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv};
+    hb[1 * NP + q] = float2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl};
+    hb[2 * NP + q] = float2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl};
+    hb[3 * NP + q] = float2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci};
+    hb[4 * NP + q] = float2{(ur * bt - ut * br) * ci, ur * tt * ct};
+    hb[5 * NP + q] = float2{ut * tt * ct, up * tt * ct};
   }
   __syncthreads();
   float2 *zf = fft_passes<N, 6, -1, 0>(hb, g, TW);
@@ -756,15 +782,14 @@ k_fft_products_t(int L, MLayout fin, MLayout fout, const float2 *__restrict__ tw
   for (int p = 0; p < 6; p++) {
     const float2 *Z = zf + p * NP;
     float *o0 = O + (2 * p) * 2 * MP, *o1 = O + (2 * p + 1) * 2 * MP;
-    const float ay = an * pow2i(-pair_exp(FMX[2 * p], FMX[2 * p + 1]));
     for (int m = tid; m <= L; m += blockDim.x) {
       if (m == 0) {
         const float2 z0 = Z[0];
-        o0[0] = an * z0.x; o0[MP] = 0.0f; o1[0] = ay * z0.y; o1[MP] = 0.0f;
+        o0[0] = an * z0.x; o0[MP] = 0.0f; o1[0] = an * z0.y; o1[MP] = 0.0f;
       } else {
         const float2 zk = Z[fpad(m)], zn = Z[fpad(N - m)];
         o0[m] = an * (zk.x + zn.x); o0[MP + m] = -an * (zk.y - zn.y);
-        o1[m] = ay * (zk.y + zn.y); o1[MP + m] = ay * (zk.x - zn.x);
+        o1[m] = an * (zk.y + zn.y); o1[MP + m] = an * (zk.x - zn.x);
       }
     }
   }
@@ -811,9 +836,7 @@ struct F4Plan {
   static constexpr int NTW = 3 * M + R2 * WP;  // tables: [3][M] e^{2 pi i m r/N}, [R2][WP] e^{2 pi i n2 k1/M}
   // staging: max(14 rows x MP2 complex in, 24 rows x (M | 1) floats out)
   static constexpr int SF = (28 * MP2 > 24 * (M | 1)) ? 28 * MP2 : 24 * (M | 1);
-  // pair scaling: 7 backward factors, 12 forward maxima, 6 forward factors (floats)
-  static constexpr int NSC = 32;
-  static constexpr size_t smem() { return (size_t)SF * 4 + ((size_t)X + NTW) * 8 + NSC * 4; }
+  static constexpr size_t smem() { return (size_t)SF * 4 + ((size_t)X + NTW) * 8; }
 };
 
 __device__ __forceinline__ float2 cmulc(float2 a, float2 w) {   // a * conj(w)
@@ -832,13 +855,10 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
   float2 *X = reinterpret_cast<float2 *>(smraw + (size_t)P::SF * 4);   // transposes / grid rows / F_r
   float2 *TW3 = X + P::X;                                          // [3][M]
   float2 *TWM = TW3 + 3 * M;                                       // [R2][WP]
-  float *BSC = reinterpret_cast<float *>(TW3 + P::NTW);            // [6] 1 / backward pair factor
-  unsigned *FMX = reinterpret_cast<unsigned *>(BSC + 8);           // [12] forward row maxima (bits)
   const int th = blockIdx.x / fin.nr, k = blockIdx.x % fin.nr;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = F4_THREADS / 32;
   const int grp = tid >> 4, lt = tid & 15;
   for (int e = tid; e < P::NTW; e += F4_THREADS) TW3[e] = tables[e];
-  if (tid < 12) FMX[tid] = 0u;
   for (int e = tid; e < 14; e += F4_THREADS) S2[e * MP2 + M] = float2{0.0f, 0.0f};
   for (int e = tid; e < M; e += F4_THREADS) S2[13 * MP2 + e] = float2{0.0f, 0.0f};
   // input: one warp per order m, lane j < 26 copies element j of the 10 + 16
@@ -855,27 +875,6 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + m * mst) : "memory");
       }
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-  }
-  __syncthreads();
-  // pair scaling (pair_exp): warp p < 6 brings the second row of pair p to
-  // the size of the first, in place (undone at the products); pair 6 (T and
-  // the zero row) needs none
-  if (warp < 6) {
-    float2 *x0 = S2 + (2 * warp) * MP2, *y0 = x0 + MP2;
-    unsigned mx = 0u, my = 0u;
-    for (int m = lane; m < M; m += 32) {
-      const float2 a = x0[m], b = y0[m];
-      mx = max(mx, max(abs_bits(a.x), abs_bits(a.y)));
-      my = max(my, max(abs_bits(b.x), abs_bits(b.y)));
-    }
-    mx = __reduce_max_sync(0xffffffffu, mx);
-    my = __reduce_max_sync(0xffffffffu, my);
-    const int e = pair_exp(mx, my);
-    if (e != 0) {
-      const float s = pow2i(e);
-      for (int m = lane; m < M; m += 32) y0[m] = float2{y0[m].x * s, y0[m].y * s};
-    }
-    if (lane == 0) BSC[warp] = pow2i(-e);
   }
   __syncthreads();
   const int gp = grp / 3, gr = grp - 3 * gp;   // pair, residue of this group
@@ -920,29 +919,17 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
   {
     const float cv = 0.25f * (float)pc.cv, cl = 0.25f * (float)pc.cl, ci = 0.25f * (float)pc.ci,
                 ct = 0.25f * (float)pc.ct;
-    // N is a multiple of 32, so a warp runs an iteration with all its lanes
-    // or not at all; the row maxima of the 12 product rows (pair scaling)
-    // are reduced per pass
-    static_assert(N % 32 == 0, "whole warps per products pass");
-    const float i0 = BSC[0], i1 = BSC[1], i2 = BSC[2], i3 = BSC[3], i4 = BSC[4], i5 = BSC[5];
     for (int q = tid; q < N; q += F4_THREADS) {
       const float2 p0 = X[0 * N + q], p1 = X[1 * N + q], p2 = X[2 * N + q], p3 = X[3 * N + q];
       const float2 p4 = X[4 * N + q], p5 = X[5 * N + q], p6 = X[6 * N + q];
-      const float ur = p0.x, ut = p0.y * i0, up = p1.x, wr = p1.y * i1, wt = p2.x, wp = p2.y * i2;
-      const float br = p3.x, bt = p3.y * i3, bp = p4.x, jr = p4.y * i4, jt = p5.x, jp = p5.y * i5, tt = p6.x;
-      const float2 h[6] = {float2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv},
-                           float2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl},
-                           float2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl},
-                           float2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci},
-                           float2{(ur * bt - ut * br) * ci, ur * tt * ct},
-                           float2{ut * tt * ct, up * tt * ct}};
-#pragma unroll
-      for (int p = 0; p < 6; p++) {
-        X[p * N + q] = h[p];
-        const unsigned rx = __reduce_max_sync(0xffffffffu, abs_bits(h[p].x));
-        const unsigned ry = __reduce_max_sync(0xffffffffu, abs_bits(h[p].y));
-        if (lane == 0) { atomicMax(FMX + 2 * p, rx); atomicMax(FMX + 2 * p + 1, ry); }
-      }
+      const float ur = p0.x, ut = p0.y, up = p1.x, wr = p1.y, wt = p2.x, wp = p2.y;
+      const float br = p3.x, bt = p3.y, bp = p4.x, jr = p4.y, jt = p5.x, jp = p5.y, tt = p6.x;
+      X[0 * N + q] = float2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv};
+      X[1 * N + q] = float2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl};
+      X[2 * N + q] = float2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl};
+      X[3 * N + q] = float2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci};
+      X[4 * N + q] = float2{(ur * bt - ut * br) * ci, ur * tt * ct};
+      X[5 * N + q] = float2{ut * tt * ct, up * tt * ct};
     }
   }
   __syncthreads();
@@ -950,12 +937,8 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
   float2 v[R1];
   if (grp < 18 && lt < R2) {
     const float2 *G = X + gp * N + 3 * lt + gr;
-    const float sy = pow2i(pair_exp(FMX[2 * gp], FMX[2 * gp + 1]));
 #pragma unroll
-    for (int n1 = 0; n1 < R1; n1++) {
-      const float2 g = G[3 * R2 * n1];
-      v[n1] = float2{g.x, g.y * sy};
-    }
+    for (int n1 = 0; n1 < R1; n1++) v[n1] = G[3 * R2 * n1];
     dftr<R1, -1>(v);
 #pragma unroll
     for (int k1 = 1; k1 < R1; k1++) v[k1] = cmulc(v[k1], TWM[lt * WP + k1]);
@@ -992,12 +975,11 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
       const float2 zk = cadd(F[m], cadd(cmulc(F[M + m], t1), cmulc(F[2 * M + m], t2)));
       const float2 zn = cadd(F[mm], cadd(cmulf(F[M + mm], t1), cmulf(F[2 * M + mm], t2)));
       float *o0 = Sf + (2 * p) * 2 * MPO, *o1 = Sf + (2 * p + 1) * 2 * MPO;
-      const float ay = an * pow2i(-pair_exp(FMX[2 * p], FMX[2 * p + 1]));
       if (m == 0) {
-        o0[0] = an * zk.x; o0[MPO] = 0.0f; o1[0] = ay * zk.y; o1[MPO] = 0.0f;
+        o0[0] = an * zk.x; o0[MPO] = 0.0f; o1[0] = an * zk.y; o1[MPO] = 0.0f;
       } else {
         o0[m] = an * (zk.x + zn.x); o0[MPO + m] = -an * (zk.y - zn.y);
-        o1[m] = ay * (zk.y + zn.y); o1[MPO + m] = ay * (zk.x - zn.x);
+        o1[m] = an * (zk.y + zn.y); o1[MPO + m] = an * (zk.x - zn.x);
       }
     }
   }
@@ -1140,7 +1122,7 @@ static FFTPlan make_plan(int n) {
 }
 
 template <int N>
-static size_t smem_fft_t() { return (14 * (size_t)Plan3x2<N>::NP + N) * sizeof(float2) + 32 * sizeof(float); }
+static size_t smem_fft_t() { return (14 * (size_t)Plan3x2<N>::NP + N) * sizeof(float2); }
 
 // smem attribute and the per-stage twiddle table w^(r k) of Plan3x2<N>
 template <int N>
@@ -1196,7 +1178,7 @@ int fft_setup(Ctx &c) {
   k_twiddles<<<cdiv(c.nph, 256), 256, 0, c.stream>>>(c.nph, (double2 *)c.d_tw_fft,
                                                      (float2 *)c.d_tw_fft32);
   CB2_CUDA(cudaGetLastError());
-  size_t big = 14 * (size_t)c.nph * sizeof(double2);
+  size_t big = 14 * (size_t)c.nph * sizeof(double2) + 32 * sizeof(double);
   if (big > 227 * 1024) {
     set_error("ngrid_zonal_ctl too large for the fused FFT kernel");
     return CB2_ERR_ARG;
@@ -1242,7 +1224,7 @@ template <typename T>
 void fft_products(Ctx &c, const T *four, T *four2) {
   using T2 = typename C2<T>::t;
   FFTPlan p = make_plan(c.nph);
-  size_t sm = 14 * (size_t)c.nph * sizeof(T2);
+  size_t sm = 14 * (size_t)c.nph * sizeof(T2) + 32 * sizeof(double);
   ProdCoef pc{c.p.coef_velo, c.p.coef_lor, c.p.coef_induct, c.p.coef_temp};
   k_fft_products<T><<<(unsigned)(c.nth * c.nr), 512, sm, c.stream>>>(p, c.L, c.NS, four, four2,
                                                                      twid<T>(c), pc);
