@@ -207,6 +207,7 @@ def time_control(mhd_text: str) -> dict:
         i_step_init=int(ts.get("i_step_init_ctl", "0")),
         i_step_finish=int(ts.get("i_step_finish_ctl", "0")),
         i_step_check=int(ts.get("i_step_check_ctl", "0")),
+        i_step_rst=int(ts.get("i_step_rst_ctl", "0")),
         dt=float(ts.get("dt_ctl")),
         legendre_trans_loop=(tl.get("Legendre_trans_loop_ctl") or "").upper(),
         fft_library=(tl.get("FFT_library_ctl") or "").upper(),

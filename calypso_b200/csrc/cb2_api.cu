@@ -1,4 +1,5 @@
 // cb2_api.cu -- the C ABI of libcalypso_b200 (see include/calypso_b200.h).
+#include <algorithm>
 #include <cctype>
 #include <cmath>
 #include <cstdio>
@@ -355,6 +356,7 @@ int cb2_init_fields(cb2_ctx *c, int kind, unsigned seed) {
 
 int cb2_start(cb2_ctx *c) {
   if (!c) return CB2_ERR_ARG;
+  c->terms_stale = false;
   rj_start_derived(*c);
   int rc = nonlinear(*c);
   if (rc) return rc;
@@ -365,9 +367,20 @@ int cb2_start(cb2_ctx *c) {
   return 0;
 }
 
+// the nonlinear terms of the current state, when the last call left them out
+static int fresh_terms(Ctx &c) {
+  if (!c.terms_stale) return 0;
+  int rc = nonlinear(c);
+  if (rc) return rc;
+  temp_roundtrip(c);
+  c.terms_stale = false;
+  return 0;
+}
+
 int cb2_step(cb2_ctx *c, int nsteps) {
   if (!c) return CB2_ERR_ARG;
   if (!c->started) { set_error("cb2_step before cb2_start / cb2_init_fields"); return CB2_ERR_STATE; }
+  if (int rc = fresh_terms(*c)) return rc;
   if (c->timers) for (int i = 0; i < 32; i++) c->stage_ms[i] = 0.0;
   for (int s = 0; s < nsteps; s++) {
     int rc = step_once(*c);
@@ -381,6 +394,7 @@ int cb2_step(cb2_ctx *c, int nsteps) {
 int cb2_step_graph(cb2_ctx *c, int nsteps) {
   if (!c) return CB2_ERR_ARG;
   if (!c->started) { set_error("cb2_step_graph before cb2_start"); return CB2_ERR_STATE; }
+  if (int rc = fresh_terms(*c)) return rc;
   // the first step is an Euler step and not captured
   int done = 0;
   if (c->istep == 0 && nsteps > 0) {
@@ -521,6 +535,7 @@ int cb2_step_host_state(cb2_ctx *c, double *state, double out_energies[7]) {
     k_to_device_order<<<cdiv(n, 256), 256, 0, c->stream>>>(c->nr, c->jmax, c->d_perm,
                                                              c->d_host_state + q * n, c->fld(kHostStateSlots[q]));
   if (c->istep == 0) c->istep = 1;   // the loaded history makes this an Adams-Bashforth step
+  c->terms_stale = false;            // the state carries its own nonlinear terms
   if (int rc = step_once(*c)) return rc;
   for (int q = 0; q < 20; q++)
     k_to_host_order<<<cdiv(n, 256), 256, 0, c->stream>>>(c->nr, c->jmax, c->d_perm,
@@ -530,6 +545,47 @@ int cb2_step_host_state(cb2_ctx *c, double *state, double out_energies[7]) {
   if (!pinned) memcpy(state, c->h_stage, bytes);
   if (out_energies) return cb2_energies(c, out_energies);
   return 0;
+}
+
+// The reference's restart set (MHD_src/sph_MHD/set_sph_restart_IO.f90:62-142,
+// written after trans_per_temp_to_temp_sph, so the temperature is the total
+// one): velocity (S, dS/dr, T), temperature, magnetic field (S, dS/dr, T),
+// previous_momentum (3), previous_induction (3), previous_heat (1).
+static const int kRestartSlots[14] = {VELO, VELO + 1, VELO + 2, TEMP, MAGNE, MAGNE + 1, MAGNE + 2,
+                                      PREMOM, PREMOM + 1, PREMOM + 2, PREUXB, PREUXB + 1, PREUXB + 2, PREHEAT};
+
+__global__ void k_add_l0(int nr, size_t jmax, const double *reft0, double *T, double sign) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nr) T[(size_t)k * jmax] += sign * reft0[k];   // host order: j = 0 is l = m = 0
+}
+
+// host restart state -> field slots (through the device staging d_host_state)
+static int load_restart(Ctx &c, const double *state) {
+  const size_t n = c.fsize(), bytes = 14 * n * sizeof(double);
+  if (!c.d_host_state) CB2_CUDA(cudaMalloc(&c.d_host_state, 20 * n * sizeof(double)));
+  CB2_CUDA(cudaMemcpyAsync(c.d_host_state, state, bytes, cudaMemcpyHostToDevice, c.stream));
+  // the total temperature back to the perturbation (sync_temp_by_per_temp_sph)
+  if (c.p.use_ref_temp)
+    k_add_l0<<<cdiv(c.nr, 128), 128, 0, c.stream>>>(c.nr, (size_t)c.jmax, c.d_reft0, c.d_host_state + 3 * n, -1.0);
+  for (int q = 0; q < 14; q++)
+    k_to_device_order<<<cdiv(n, 256), 256, 0, c.stream>>>(c.nr, c.jmax, c.d_perm, c.d_host_state + q * n,
+                                                          c.fld(kRestartSlots[q]));
+  CB2_CUDA(cudaGetLastError());
+  return 0;
+}
+
+static int store_restart(Ctx &c, double *state) {
+  const size_t n = c.fsize(), bytes = 14 * n * sizeof(double);
+  if (!c.d_host_state) CB2_CUDA(cudaMalloc(&c.d_host_state, 20 * n * sizeof(double)));
+  for (int q = 0; q < 14; q++)
+    k_to_host_order<<<cdiv(n, 256), 256, 0, c.stream>>>(c.nr, c.jmax, c.d_perm, c.fld(kRestartSlots[q]),
+                                                        c.d_host_state + q * n);
+  if (c.p.use_ref_temp)
+    k_add_l0<<<cdiv(c.nr, 128), 128, 0, c.stream>>>(c.nr, (size_t)c.jmax, c.d_reft0, c.d_host_state + 3 * n, 1.0);
+  CB2_CUDA(cudaGetLastError());
+  CB2_CUDA(cudaMemcpyAsync(state, c.d_host_state, bytes, cudaMemcpyDeviceToHost, c.stream));
+  CB2_CUDA(cudaStreamSynchronize(c.stream));
+  return check_status(c);
 }
 
 static int sht_common(cb2_ctx *c, int nvec, int nscal) {
@@ -598,6 +654,39 @@ int cb2_sht_forward(cb2_ctx *c, int nvec, int nscal, const double *grid, double 
   for (int q = 0; q < nc; q++)
     if ((rc = cb2_get_field(c, MADV + q, spec + q * n))) return rc;
   return 0;
+}
+
+int cb2_get_restart_state(cb2_ctx *c, double *state) {
+  if (!c || !state) return CB2_ERR_ARG;
+  if (!c->started) { set_error("cb2_get_restart_state before cb2_start"); return CB2_ERR_STATE; }
+  return store_restart(*c, state);
+}
+
+int cb2_set_restart_state(cb2_ctx *c, const double *state, int istep) {
+  if (!c || !state || istep < 0) return CB2_ERR_ARG;
+  int rc = load_restart(*c, state);
+  if (rc) return rc;
+  // set_sph_field_to_start + the first nonlinear terms
+  if ((rc = cb2_start(c))) return rc;
+  c->istep = istep;
+  c->terms_stale = false;
+  return 0;
+}
+
+int cb2_step_restart_state(cb2_ctx *c, double *state, double out_energies[7]) {
+  if (!c || !state) return CB2_ERR_ARG;
+  if (!c->started) { set_error("cb2_step_restart_state before cb2_start"); return CB2_ERR_STATE; }
+  int rc = load_restart(*c, state);
+  if (rc) return rc;
+  rj_start_derived(*c);
+  if ((rc = nonlinear(*c))) return rc;
+  c->istep = std::max(c->istep, 1) + 1;     // the loaded history makes this an Adams-Bashforth step
+  cn_stage(*c, false);
+  // the nonlinear terms of the new state are left to the next call (or to
+  // the next cb2_step, which computes them first)
+  c->terms_stale = true;
+  if ((rc = store_restart(*c, state))) return rc;
+  return out_energies ? cb2_energies(c, out_energies) : 0;
 }
 
 int cb2_get_gauss(cb2_ctx *c, double *colat, double *weight) {

@@ -126,6 +126,9 @@ struct Ctx {
   size_t bnd_tab_bytes = 0;
   int istep = 0;
   bool started = false;
+  // the nonlinear terms of the current state are not computed yet
+  // (cb2_step_restart_state leaves them to the next call)
+  bool terms_stale = false;
   bool timers = false;
   cudaEvent_t ev[64];
   double stage_ms[32] = {0};

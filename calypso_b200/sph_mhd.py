@@ -49,6 +49,12 @@ PREC_MIXED = 1
 # d_rj slots of the evolved fields
 VELO, VORT, MAGNE, CURRENT, TEMP = 0, 3, 6, 9, 12
 
+# the reference's restart file: field names and components, in the order of
+# the restart state (cb2_get_restart_state)
+RESTART_FIELDS = [("velocity", 3), ("temperature", 1), ("magnetic_field", 3),
+                  ("previous_momentum", 3), ("previous_induction", 3), ("previous_heat", 1)]
+RESTART_FIELDS_COMPS = [(n, c) for n, nc in RESTART_FIELDS for c in range(nc)]
+
 # kernel-variant tuning entries (cb2_get_tuning / cb2_set_tuning): float64
 # backward radial tile, float64 forward radial tile, mixed pack radial tile,
 # mixed FFT threads, fused Crank-Nicolson step (1) or separate kernels (0)
@@ -158,6 +164,7 @@ EXPORTS = [
     "cb2_ensemble_init_fields", "cb2_ensemble_step", "cb2_ensemble_sync", "cb2_ensemble_time_steps",
     "cb2_ensemble_energies", "cb2_leg_bwd", "cb2_leg_fwd", "cb2_fft_bwd", "cb2_fft_fwd",
     "cb2_legendre_trans_mode", "cb2_fft_library_known", "cb2_energy_spectra", "cb2_fft_products",
+    "cb2_get_restart_state", "cb2_set_restart_state", "cb2_step_restart_state",
 ]
 
 
@@ -218,6 +225,9 @@ def load_library(path: str = LIB_PATH):
         "cb2_fft_library_known": ([ctypes.c_char_p], i),
         "cb2_energy_spectra": ([vp, pd, pd, pd], i),
         "cb2_fft_products": ([vp, P(SphTables), ctypes.c_size_t, vp, ctypes.c_size_t, vp], i),
+        "cb2_get_restart_state": ([vp, pd], i),
+        "cb2_set_restart_state": ([vp, pd, i], i),
+        "cb2_step_restart_state": ([vp, pd, pd], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -364,6 +374,25 @@ class SphMHD:
         ene = np.zeros(7)
         _check(load_library().cb2_step_host_state(
             self._h, _ptr(state), _ptr(ene) if with_energies else None), "cb2_step_host_state")
+        return ene
+
+    # --- restart state (the fields of the reference's restart file) ---------
+    def get_restart_state(self) -> np.ndarray:
+        """(14, nr, jmax): velocity (3), total temperature, magnetic field
+        (3), previous_momentum (3), previous_induction (3), previous_heat."""
+        out = np.zeros((len(RESTART_FIELDS_COMPS), self.nr, self.jmax))
+        _check(load_library().cb2_get_restart_state(self._h, _ptr(out)), "cb2_get_restart_state")
+        return out
+
+    def set_restart_state(self, state: np.ndarray, istep: int):
+        state = np.ascontiguousarray(state, dtype=np.float64).reshape(len(RESTART_FIELDS_COMPS), self.nr, self.jmax)
+        _check(load_library().cb2_set_restart_state(self._h, _ptr(state), istep), "cb2_set_restart_state")
+
+    def step_restart_state(self, state: np.ndarray, with_energies: bool = True):
+        """One Adams-Bashforth step of a host-resident restart state (in place)."""
+        ene = np.zeros(7)
+        _check(load_library().cb2_step_restart_state(self._h, _ptr(state), _ptr(ene) if with_energies else None),
+               "cb2_step_restart_state")
         return ene
 
     # --- transforms -----------------------------------------------------

@@ -15,8 +15,12 @@ formats (:mod:`calypso_b200.monitor`).  The precision comes from
 ``Legendre_trans_loop_ctl`` unless ``--precision`` is given.
 
 Initial fields (``rst_ctl``): ``dynamo_benchmark_1`` (the reference's
-case-1 start) and ``B200_seeded`` (a seeded thermal perturbation on l <= 8
-plus a dipole-dominated seed field; no reference counterpart).
+case-1 start), ``start_from_rst_file`` (the restart file of step
+``i_step_init_ctl``) and ``B200_seeded`` (a seeded thermal perturbation on
+l <= 8 plus a dipole-dominated seed field; no reference counterpart).
+Every ``i_step_rst_ctl`` steps a restart file
+``<restart_file_prefix>.<step / i_step_rst_ctl>.0.fst`` is written
+(:mod:`calypso_b200.restart`).
 """
 from __future__ import annotations
 
@@ -26,9 +30,10 @@ import time
 
 from .control import parse_control, precision_from_control, shell_params_from_control, time_control
 from .monitor import MonitorFiles
+from .restart import read_restart, restart_file_name, write_restart
 from .sph_mhd import PREC_FP64, PREC_MIXED, SphMHD
 
-INIT_KINDS = {"dynamo_benchmark_1": 1, "b200_seeded": 2}
+INIT_KINDS = {"dynamo_benchmark_1": 1, "b200_seeded": 2, "start_from_rst_file": 0}
 
 
 def monitor_settings(mhd_text: str) -> dict:
@@ -65,19 +70,36 @@ def run(directory: str, precision: int | None = None, steps: int | None = None, 
                          volume_prefix=mon.get("volume_prefix", "sph_pwr_volume"), spectra=mon["spectra"],
                          degree=mon.get("degree", True), order=mon.get("order", True),
                          diff_lm=mon.get("diff_lm", True))
+    files_def = parse_control(mhd).block("MHD_control", "data_files_def")
+    rst_prefix = ((files_def.get("restart_file_prefix") if files_def else None) or "restart/rst").strip("'\"")
+    rst_prefix = os.path.join(directory, rst_prefix)
+    i_rst = tc["i_step_rst"]
     g = SphMHD(params, prec, device=device)
-    g.init_fields(INIT_KINDS[rst_ctl], 0)
     i0 = tc["i_step_init"]
+    if INIT_KINDS[rst_ctl] == 0:
+        if i_rst <= 0:
+            raise ValueError("start_from_rst_file needs i_step_rst_ctl > 0")
+        state, _, _, _ = read_restart(restart_file_name(rst_prefix, i0 // i_rst), g.nr, g.jmax)
+        g.set_restart_state(state, i0)
+    else:
+        g.init_fields(INIT_KINDS[rst_ctl], 0)
     i1 = tc["i_step_finish"] if steps is None else i0 + steps
     check = tc["i_step_check"]
     dt = params["dt"]
     t0 = time.perf_counter()
     istep = i0
     while istep < i1:
-        # advance to the next check step (or the end) in one call
-        nxt = min(i1, (istep // check + 1) * check) if check > 0 else i1
+        # advance to the next check or restart step (or the end) in one call
+        nxt = i1
+        for every in (check, i_rst):
+            if every > 0:
+                nxt = min(nxt, (istep // every + 1) * every)
         g.step(nxt - istep, graph=graph)
         istep = nxt
+        if i_rst > 0 and istep % i_rst == 0:
+            os.makedirs(os.path.dirname(rst_prefix) or ".", exist_ok=True)
+            write_restart(restart_file_name(rst_prefix, istep // i_rst), g.get_restart_state(), istep,
+                          istep * dt, dt)
         if check > 0 and istep % check == 0:
             e = g.energies()
             files.write(istep, istep * dt, e, g.energy_spectra() if mon["spectra"] else None)

@@ -152,6 +152,27 @@ int cb2_set_field_device(cb2_ctx *ctx, int slot, const double *dev);
  * previous value (negated).  out_energies may be NULL. */
 int cb2_step_host_state(cb2_ctx *ctx, double *state, double out_energies[7]);
 
+/* The reference's restart state (MHD_src/IO/sph_mhd_rst_IO_control.f90:89-145,
+ * MHD_src/sph_MHD/set_sph_restart_IO.f90:62-142: the fields of a restart
+ * file): 14 x nr*jmax float64 host array, in this order: velocity S, dS/dr,
+ * T; temperature (the total temperature, reference profile included, as
+ * the reference writes it after trans_per_temp_to_temp_sph); magnetic field
+ * S, dS/dr, T; previous_momentum (3); previous_induction (3);
+ * previous_heat (the negated heat advection of the last step).
+ * cb2_get_restart_state reads it after any step.  cb2_set_restart_state
+ * loads it and restarts the loop as the reference's start from a restart
+ * file does (set_sph_field_to_start and the first nonlinear terms); the
+ * next step is an Adams-Bashforth step numbered istep + 1. */
+int cb2_get_restart_state(cb2_ctx *ctx, double *state);
+int cb2_set_restart_state(cb2_ctx *ctx, const double *state, int istep);
+/* One Adams-Bashforth step of a host that keeps the restart state in its
+ * own memory (14 fields in and out instead of the 20 of
+ * cb2_step_host_state): loads the state, computes its derived fields and
+ * nonlinear terms, advances one step and returns the new state.  The
+ * nonlinear terms of the new state are left to the next call (or to the
+ * next cb2_step, which computes them first).  out_energies may be NULL. */
+int cb2_step_restart_state(cb2_ctx *ctx, double *state, double out_energies[7]);
+
 /* Spherical transform of nvec vectors + nscal scalars at every radius
  * (PARALLEL_src/SPH_SHELL_src/legendre_transform_select.f90:309-439
  *  sel_backward_legendre_trans / sel_forward_legendre_trans, plus

@@ -192,6 +192,30 @@ module m_calypso_b200
       integer(c_int) :: rc
     end function cb2_step_host_state
 
+    function cb2_get_restart_state(ctx, state) bind(C, name='cb2_get_restart_state') result(rc)
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(inout) :: state(*)
+      integer(c_int) :: rc
+    end function cb2_get_restart_state
+
+    function cb2_set_restart_state(ctx, state, istep) bind(C, name='cb2_set_restart_state') result(rc)
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: state(*)
+      integer(c_int), value :: istep
+      integer(c_int) :: rc
+    end function cb2_set_restart_state
+
+    function cb2_step_restart_state(ctx, state, out_energies) &
+        bind(C, name='cb2_step_restart_state') result(rc)
+      import
+      type(c_ptr), value :: ctx
+      real(c_double), intent(inout) :: state(*)
+      real(c_double), intent(out) :: out_energies(7)
+      integer(c_int) :: rc
+    end function cb2_step_restart_state
+
     function cb2_sht_backward(ctx, nvec, nscal, spec, grid) &
         bind(C, name='cb2_sht_backward') result(rc)
       import

@@ -1,0 +1,102 @@
+"""Restart state on the GPU: a run continued from the reference-format
+restart file of its step 50 reproduces the uninterrupted run's step-100
+energies (16 significant digits in the file, so 1e-12 on the float64 path),
+and the host-resident restart step (cb2_step_restart_state, the end-to-end
+entry) advances a state exactly as cb2_step does."""
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+from calypso_b200 import PREC_FP64, PREC_MIXED, SphMHD
+from calypso_b200 import configs
+from calypso_b200.control import shell_params_from_control
+from calypso_b200.sph_mhd import TEMP
+from calypso_b200.monitor import compare_mean_square, read_mean_square
+from calypso_b200.restart import read_restart, restart_file_name
+from calypso_b200.sph_mhd_program import run
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "dynamobench_case1")
+
+
+def _case(d, rst_every, start_from_file=False, i_init=0):
+    os.makedirs(d, exist_ok=True)
+    shutil.copyfile(os.path.join(GOLD, "control_sph_shell"), os.path.join(d, "control_sph_shell"))
+    txt = open(os.path.join(GOLD, "control_MHD")).read()
+    txt = txt.replace("i_step_rst_ctl         1000", f"i_step_rst_ctl         {rst_every}")
+    txt = txt.replace("i_step_init_ctl           0", f"i_step_init_ctl           {i_init}")
+    if start_from_file:
+        txt = txt.replace("rst_ctl                dynamo_benchmark_1", "rst_ctl                start_from_rst_file")
+    open(os.path.join(d, "control_MHD"), "w").write(txt)
+    return d
+
+
+@pytest.mark.parametrize("prec,tol", [(PREC_FP64, 1e-12), (PREC_MIXED, 1e-6)])
+def test_program_continues_from_restart_file(tmp_path, prec, tol):
+    a = _case(str(tmp_path / "a"), 50)
+    run(a, precision=prec, graph=True, log=lambda *x: None)
+    for k in (1, 2):
+        assert os.path.exists(restart_file_name(os.path.join(a, "rst_4/rst"), k))
+    b = _case(str(tmp_path / "b"), 50, start_from_file=True, i_init=50)
+    os.makedirs(os.path.join(b, "rst_4"))
+    shutil.copyfile(restart_file_name(os.path.join(a, "rst_4/rst"), 1), restart_file_name(os.path.join(b, "rst_4/rst"), 1))
+    r = run(b, precision=prec, graph=True, log=lambda *x: None)
+    assert r["steps"] == 50
+    rows = read_mean_square(os.path.join(b, "sph_pwr_volume_s.dat"))
+    assert [row[0] for row in rows] == [100]
+    ok, worst = compare_mean_square(os.path.join(b, "sph_pwr_volume_s.dat"), os.path.join(a, "sph_pwr_volume_s.dat"), tol)
+    assert ok, worst
+    # the restart files of step 100 agree too
+    p = shell_params_from_control(open(os.path.join(a, "control_MHD")).read(),
+                                  open(os.path.join(a, "control_sph_shell")).read())
+    nr, jmax = p["nr"], (p["ltr"] + 1) ** 2
+    sa, ia, _, _ = read_restart(restart_file_name(os.path.join(a, "rst_4/rst"), 2), nr, jmax)
+    sb, ib, _, _ = read_restart(restart_file_name(os.path.join(b, "rst_4/rst"), 2), nr, jmax)
+    assert ia == ib == 100
+    assert np.linalg.norm(sa - sb) <= tol * np.linalg.norm(sa)
+
+
+@pytest.mark.parametrize("prec,tol", [(PREC_FP64, 1e-12), (PREC_MIXED, 1e-9)])
+def test_step_restart_state_matches_step(prec, tol):
+    p = configs.small_shell()
+    g = SphMHD(p, prec)
+    g.init_fields(2, 5)
+    g.step(3)
+    state = g.get_restart_state()
+    h = SphMHD(p, prec)
+    h.init_fields(2, 5)
+    h.set_restart_state(state, 3)
+    ene = None
+    for _ in range(4):
+        ene = h.step_restart_state(state)
+    g.step(4)
+    want = g.get_restart_state()
+    for q in range(state.shape[0]):
+        nrm = np.linalg.norm(want[q])
+        assert np.linalg.norm(state[q] - want[q]) <= tol * max(nrm, 1e-300), q
+    np.testing.assert_allclose(ene, g.energies(), rtol=tol)
+    # and cb2_step continues from the host state (its nonlinear terms first)
+    h.step(2)
+    g.step(2)
+    np.testing.assert_allclose(h.energies(), g.energies(), rtol=tol)
+    g.close()
+    h.close()
+
+
+def test_restart_state_keeps_total_temperature():
+    """The restart temperature is the total one (reference profile on l = 0
+    added back, trans_per_temp_to_temp_sph), and set -> get is the identity."""
+    p = configs.shell_params(15, 17, 24, 48, E=1e-3, Ra=100.0)
+    g = SphMHD(p, PREC_FP64)
+    g.init_fields(1, 0)
+    s = g.get_restart_state()
+    T = g.get_field(TEMP)
+    assert not np.allclose(s[3][:, 0], T[:, 0])
+    np.testing.assert_allclose(s[3][:, 1:], T[:, 1:], rtol=0, atol=0)
+    g.set_restart_state(s, 7)
+    s2 = g.get_restart_state()
+    np.testing.assert_allclose(s2, s, rtol=1e-15, atol=1e-300)
+    g.close()
