@@ -368,6 +368,7 @@ def main():
     # the library's start-up autotuner picks the kernel variants (before the
     # fields exist); the stage-timer context and the FP64 context reuse it
     tuning = g.autotune() if not args.no_autotune else g.tuning
+    tuning_note = g.tuning_note
     g.init_fields(2, seed=1 + rank)
     g.step(1)                                    # Euler first step
     g.step(args.warmup, graph=True)              # warm-up (graph capture + replays)
@@ -512,7 +513,8 @@ def main():
             "data": DATA,
             "config": workload_config(params, args.workload),
             "impl_config": {"precision": args.precision, "parallelism": f"replicas x{world}",
-                            "graph": True, "tuning": list(tuning)},
+                            "graph": True, "tuning": list(tuning),
+                            **({"tuning_note": tuning_note} if tuning_note else {})},
             "roofline": roof, "stages_ms": stages, "cpu_baseline": cpu, "e2e": e2e,
             "fp64_plain": fp64, "sht_roundtrip": sht,
             # kernels per step: the Crank-Nicolson stage (one fused kernel, or

@@ -138,9 +138,9 @@ static int nonlinear(Ctx &c) {
     int rc = leg_bwd_mixed(c, bslots, fin);
     if (rc) return rc;
     if (c.timers) cudaEventRecord(c.ev[12], c.stream);
-    fft_products_m(c, fin, fout);
+    const bool maxima = fft_products_m(c, fin, fout, mixed_fwd_pmax(c));
     if (c.timers) cudaEventRecord(c.ev[13], c.stream);
-    if ((rc = leg_fwd_mixed(c, fout, fslots))) return rc;
+    if ((rc = leg_fwd_mixed(c, fout, fslots, maxima))) return rc;
   }
   if (c.timers) cudaEventRecord(c.ev[14], c.stream);
   rj_after_transform(c);
@@ -293,7 +293,7 @@ int cb2_destroy(cb2_ctx *c) {
   cn_free(*c);
   free_tables(*c);
   void *ptrs[] = {c->d_lu_vp, c->d_lu_vt, c->d_lu_bs, c->d_lu_bt, c->d_lu_t, c->d_pv_vp, c->d_pv_vt,
-                  c->d_pv_bs, c->d_pv_bt, c->d_pv_t, c->d_status, c->d_tw_fft, c->d_tw_fft32, c->d_twp32, c->d_twf4, c->d_imp_map,
+                  c->d_pv_bs, c->d_pv_bt, c->d_pv_t, c->d_status, c->d_tw_fft, c->d_tw_fft32, c->d_twp32, c->d_twf4, c->d_twf4_64, c->d_imp_map,
                   c->d_cn_lu, c->d_cn_tiles, c->d_f, c->d_four, c->d_four2, c->d_ene, c->d_tmp, c->d_host_state,
                   c->d_bnd_a, c->d_bnd_b, c->d_bnd_grid, c->d_bnd_tab};
   for (void *q : ptrs)

@@ -607,9 +607,12 @@ k_cn_step(RJArgs a, double *f, size_t fs, CnPack pk, const int *moff, const int4
 // ---------------------------------------------------------------------------
 int cn_setup(Ctx &c) {
   c.cn_ready = false;
+  c.cn_off_reason = "";
   const int n = c.nr, nl = c.L + 1;
   if (n < 6 || c.kin != 0 || c.kout != n - 1 || (size_t)n * c.jmax >= ((size_t)1 << 31)) {
     c.tune[TUNE_CN] = -1;
+    c.cn_off_reason = n < 6 ? "fewer than 6 radial points" : "the fluid shell is not the whole radial grid, or "
+                                                             "the shell has 2^31 values or more per field";
     return 0;
   }
   int *d_ok = nullptr;
@@ -632,6 +635,7 @@ int cn_setup(Ctx &c) {
     for (int l = 0; l < nl; l++) all &= ok[(size_t)q * nl + l];
     if (!all) {
       c.tune[TUNE_CN] = -1;   // an interchange beyond the form's reach
+      c.cn_off_reason = "a radial LU factor has a row interchange more than two rows away";
       return 0;
     }
     pk.form[q] = (all & 1) ? (q == 0 ? CN_N5 : CN_N3) : (q == 0 ? CN_W5 : CN_W3);
@@ -641,6 +645,7 @@ int cn_setup(Ctx &c) {
   smem = cn_smem(n);
   if (smem > 227 * 1024) {
     c.tune[TUNE_CN] = -1;
+    c.cn_off_reason = "the per-thread input rings need more than 227 KB of shared memory";
     return 0;
   }
   CB2_CUDA(cudaMalloc(&c.d_cn_lu, dbl * sizeof(double) + byt));

@@ -589,58 +589,67 @@ struct Plan3x2 {
 
 __host__ __device__ __forceinline__ int fpad(int i) { return i + (i >> 4); }
 
-__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return float2{a.x + b.x, a.y + b.y}; }
-__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return float2{a.x - b.x, a.y - b.y}; }
-__host__ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
-  return float2{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+template <typename T2> struct ScalarOf;
+template <> struct ScalarOf<float2> { using t = float; };
+template <> struct ScalarOf<double2> { using t = double; };
+
+template <typename T2>
+__host__ __device__ __forceinline__ T2 cadd(T2 a, T2 b) { return T2{a.x + b.x, a.y + b.y}; }
+template <typename T2>
+__host__ __device__ __forceinline__ T2 csub(T2 a, T2 b) { return T2{a.x - b.x, a.y - b.y}; }
+template <typename T2>
+__host__ __device__ __forceinline__ T2 cmulf(T2 a, T2 b) {
+  return T2{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
 }
 // multiply by -i (forward) or +i (inverse)
-template <int SIGN>
-__host__ __device__ __forceinline__ float2 rot90(float2 a) {
-  return (SIGN < 0) ? float2{a.y, -a.x} : float2{-a.y, a.x};
+template <int SIGN, typename T2>
+__host__ __device__ __forceinline__ T2 rot90(T2 a) {
+  return (SIGN < 0) ? T2{a.y, -a.x} : T2{-a.y, a.x};
 }
 
 // exp(SIGN 2 pi i q / 16) from exact values of the cosine at multiples of
 // pi/8: cos(pi/8) = sqrt(2 + sqrt 2)/2, cos(pi/4) = sqrt(2)/2, sin(pi/8) =
 // sqrt(2 - sqrt 2)/2
-template <int SIGN>
-__host__ __device__ __forceinline__ float2 w16(int q) {
-  constexpr float c1 = 0.92387953251128675613f, c2 = 0.70710678118654752440f, c3 = 0.38268343236508977173f;
-  const float cs[16] = {1.f, c1, c2, c3, 0.f, -c3, -c2, -c1, -1.f, -c1, -c2, -c3, 0.f, c3, c2, c1};
-  const float sn[16] = {0.f, c3, c2, c1, 1.f, c1, c2, c3, 0.f, -c3, -c2, -c1, -1.f, -c1, -c2, -c3};
-  return float2{cs[q & 15], (SIGN < 0) ? -sn[q & 15] : sn[q & 15]};
+template <int SIGN, typename T2 = float2>
+__host__ __device__ __forceinline__ T2 w16(int q) {
+  using T = typename ScalarOf<T2>::t;
+  constexpr T c1 = (T)0.92387953251128675613, c2 = (T)0.70710678118654752440, c3 = (T)0.38268343236508977173;
+  const T cs[16] = {1, c1, c2, c3, 0, -c3, -c2, -c1, -1, -c1, -c2, -c3, 0, c3, c2, c1};
+  const T sn[16] = {0, c3, c2, c1, 1, c1, c2, c3, 0, -c3, -c2, -c1, -1, -c1, -c2, -c3};
+  return T2{cs[q & 15], (SIGN < 0) ? -sn[q & 15] : sn[q & 15]};
 }
 
-template <int SIGN>
-__host__ __device__ __forceinline__ void dft4(float2 &v0, float2 &v1, float2 &v2, float2 &v3) {
-  const float2 a0 = cadd(v0, v2), a1 = csub(v0, v2), a2 = cadd(v1, v3), a3 = rot90<SIGN>(csub(v1, v3));
+template <int SIGN, typename T2>
+__host__ __device__ __forceinline__ void dft4(T2 &v0, T2 &v1, T2 &v2, T2 &v3) {
+  const T2 a0 = cadd(v0, v2), a1 = csub(v0, v2), a2 = cadd(v1, v3), a3 = rot90<SIGN>(csub(v1, v3));
   v0 = cadd(a0, a2); v1 = cadd(a1, a3); v2 = csub(a0, a2); v3 = csub(a1, a3);
 }
 
 // in-register DFT of R points, natural order in and out
-template <int R, int SIGN>
-__host__ __device__ __forceinline__ void dftr(float2 (&v)[R]) {
+template <int R, int SIGN, typename T2>
+__host__ __device__ __forceinline__ void dftr(T2 (&v)[R]) {
+  using T = typename ScalarOf<T2>::t;
   if constexpr (R == 2) {
-    const float2 a = v[0], b = v[1];
+    const T2 a = v[0], b = v[1];
     v[0] = cadd(a, b); v[1] = csub(a, b);
   } else if constexpr (R == 3) {
-    const float s32 = 0.86602540378443864676f;   // sin(pi/3) = sqrt(3)/2
-    const float2 t1 = cadd(v[1], v[2]);
-    const float2 t2 = float2{v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y};
-    const float dx = v[1].x - v[2].x, dy = v[1].y - v[2].y;
-    const float2 t3 = (SIGN < 0) ? float2{s32 * dy, -s32 * dx} : float2{-s32 * dy, s32 * dx};
+    const T s32 = (T)0.86602540378443864676;   // sin(pi/3) = sqrt(3)/2
+    const T2 t1 = cadd(v[1], v[2]);
+    const T2 t2 = T2{v[0].x - (T)0.5 * t1.x, v[0].y - (T)0.5 * t1.y};
+    const T dx = v[1].x - v[2].x, dy = v[1].y - v[2].y;
+    const T2 t3 = (SIGN < 0) ? T2{s32 * dy, -s32 * dx} : T2{-s32 * dy, s32 * dx};
     v[0] = cadd(v[0], t1); v[1] = cadd(t2, t3); v[2] = csub(t2, t3);
   } else if constexpr (R == 4) {
     dft4<SIGN>(v[0], v[1], v[2], v[3]);
   } else if constexpr (R == 8) {
     // 2 x 4: even / odd halves, then W8^k twiddles
-    float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-    float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    T2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    T2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
     dft4<SIGN>(e0, e1, e2, e3);
     dft4<SIGN>(o0, o1, o2, o3);
-    o1 = cmulf(o1, w16<SIGN>(2));
+    o1 = cmulf(o1, w16<SIGN, T2>(2));
     o2 = rot90<SIGN>(o2);
-    o3 = cmulf(o3, w16<SIGN>(6));
+    o3 = cmulf(o3, w16<SIGN, T2>(6));
     v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
     v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
     v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
@@ -648,7 +657,7 @@ __host__ __device__ __forceinline__ void dftr(float2 (&v)[R]) {
   } else {
     static_assert(R == 16, "radix");
     // 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2
-    float2 a[4][4];
+    T2 a[4][4];
 #pragma unroll
     for (int n2 = 0; n2 < 4; n2++) {
       a[n2][0] = v[n2]; a[n2][1] = v[4 + n2]; a[n2][2] = v[8 + n2]; a[n2][3] = v[12 + n2];
@@ -657,10 +666,10 @@ __host__ __device__ __forceinline__ void dftr(float2 (&v)[R]) {
 #pragma unroll
     for (int n2 = 1; n2 < 4; n2++)
 #pragma unroll
-      for (int k1 = 1; k1 < 4; k1++) a[n2][k1] = cmulf(a[n2][k1], w16<SIGN>(n2 * k1));
+      for (int k1 = 1; k1 < 4; k1++) a[n2][k1] = cmulf(a[n2][k1], w16<SIGN, T2>(n2 * k1));
 #pragma unroll
     for (int k1 = 0; k1 < 4; k1++) {
-      float2 b0 = a[0][k1], b1 = a[1][k1], b2 = a[2][k1], b3 = a[3][k1];
+      T2 b0 = a[0][k1], b1 = a[1][k1], b2 = a[2][k1], b3 = a[3][k1];
       dft4<SIGN>(b0, b1, b2, b3);                              // over n2 -> k2
       v[k1] = b0; v[k1 + 4] = b1; v[k1 + 8] = b2; v[k1 + 12] = b3;
     }
@@ -839,14 +848,20 @@ struct F4Plan {
   static constexpr size_t smem() { return (size_t)SF * 4 + ((size_t)X + NTW) * 8; }
 };
 
-__device__ __forceinline__ float2 cmulc(float2 a, float2 w) {   // a * conj(w)
-  return float2{a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y};
+template <typename T2>
+__device__ __forceinline__ T2 cmulc(T2 a, T2 w) {   // a * conj(w)
+  return T2{a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y};
 }
 
 
+// pmax (optional): the forward Legendre row scales' raw material, the
+// largest |a_m| w(theta) of each output element over each block of 16
+// orders, [theta][m / 16][element] with the elements of the output layout
+// (P block k 8 + j, then D block sP + k 16 + j).
 template <int R1, int R2>
 __global__ void __launch_bounds__(F4_THREADS, 2)
-k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, ProdCoef pc) {
+k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, ProdCoef pc,
+                  float *__restrict__ pmax, const float *__restrict__ wgt) {
   using P = F4Plan<R1, R2>;
   constexpr int M = P::M, N = P::N, TP = P::TP, TG = P::TG, MP2 = P::MP2, WP = P::WP, MPO = M | 1;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -993,6 +1008,232 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
     const size_t mst = (size_t)fout.nth * ((lane < 8) ? fout.sP() : fout.sD());
     if (lane < 24)
       for (int m = warp; m < M; m += nwarp) dst[m * mst] = Sf[cs * MPO + m];
+  }
+  if (pmax) {
+    constexpr int MB = M / 16;
+    const float wt = __ldg(wgt + th);
+    const size_t E = fout.sP() + fout.sD();
+    float *pm = pmax + (size_t)th * MB * E;
+    for (int t = tid; t < 24 * MB; t += F4_THREADS) {
+      const int j = t % 24, mb = t / 24;
+      int c, sg;
+      m_comp_of_out(j, c, sg);
+      const float *row = Sf + (c * 2 + sg) * MPO + mb * 16;
+      float mx = 0.0f;
+#pragma unroll
+      for (int u = 0; u < 16; u++) mx = fmaxf(mx, fabsf(row[u]));
+      const size_t e = (j < 8) ? (size_t)k * 8 + j : fout.sP() + (size_t)k * 16 + (j - 8);
+      pm[(size_t)mb * E + e] = mx * wt;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The float64 four-step products kernel (the plain path's step): the data
+// flow of k_fft_products_4s on the float64 Fourier rows
+// four[(theta, k)][c][2 m + s] (a_m at 2 m, b_m at 2 m + 1), with the pair
+// scaling of k_fft_products (the second row of each pair, inputs and
+// products, brought to the size of the first), so every row keeps float64
+// precision whatever the sizes of the fields.  One CTA per (theta, k), 384
+// threads, one CTA per SM (166 KB of shared memory at M = 256).
+template <int R1, int R2>
+struct F4Plan64 {
+  static constexpr int M = R1 * R2, N = 3 * M;
+  static constexpr int TP = R2 + 1;
+  static constexpr int TG = R1 * TP;
+  static constexpr int X = (21 * TG > 7 * N) ? 21 * TG : 7 * N;
+  static constexpr int MP2 = M + 1;            // staging row pitch, slot M stays zero
+  static constexpr int WP = R1 + 1;
+  static constexpr int NTW = 3 * M + R2 * WP;
+  static constexpr int SC = 14 * MP2;          // staging: 14 rows in, then 12 rows out
+  static constexpr size_t smem() { return ((size_t)SC + X + NTW) * sizeof(double2) + 32 * sizeof(double); }
+};
+
+template <int R1, int R2>
+__global__ void __launch_bounds__(F4_THREADS, 1)
+k_fft_products_4s64(const double *__restrict__ four, double *__restrict__ four2, int NS,
+                    const double2 *__restrict__ tables, ProdCoef pc) {
+  using P = F4Plan64<R1, R2>;
+  using PB = PairBits<double>;
+  using U = PB::U;
+  constexpr int M = P::M, N = P::N, TP = P::TP, TG = P::TG, MP2 = P::MP2, WP = P::WP;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2 *S2 = reinterpret_cast<double2 *>(smraw);   // [14][MP2] (a_m, b_m); later [12][MP2] out
+  double2 *X = S2 + P::SC;                             // transposes / grid rows / F_r
+  double2 *TW3 = X + P::X;                             // [3][M]
+  double2 *TWM = TW3 + 3 * M;                          // [R2][WP]
+  U *cmx = reinterpret_cast<U *>(TWM + R2 * WP);      // [0, 13) input maxima, [13, 25) products
+  const size_t row = blockIdx.x;
+  const double *fin = four + row * 13 * (size_t)NS;
+  double *fout = four2 + row * 12 * (size_t)NS;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = F4_THREADS / 32;
+  const int grp = tid >> 4, lt = tid & 15;
+  for (int e = tid; e < P::NTW; e += F4_THREADS) TW3[e] = tables[e];
+  for (int e = tid; e < 14; e += F4_THREADS) S2[e * MP2 + M] = double2{0.0, 0.0};
+  for (int e = tid; e < M; e += F4_THREADS) S2[13 * MP2 + e] = double2{0.0, 0.0};
+  for (int e = tid; e < 13 * M; e += F4_THREADS) {
+    const int c = e / M, m = e - c * M;
+    S2[c * MP2 + m] = __ldg(reinterpret_cast<const double2 *>(fin + (size_t)c * NS) + m);
+  }
+  if (tid < 12) cmx[13 + tid] = 0;
+  __syncthreads();
+  // largest magnitude of each input row (one warp per row)
+  for (int c = warp; c < 13; c += nwarp) {
+    U mx = 0;
+    for (int m = lane; m < M; m += 32) {
+      const double2 v = S2[c * MP2 + m];
+      mx = max(mx, max(PB::abs_bits(v.x), PB::abs_bits(v.y)));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, (U)__shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) cmx[c] = mx;
+  }
+  __syncthreads();
+  const int gp = grp / 3, gr = grp - 3 * gp;
+  // ---- backward, step 1: column n2 = lt, pair rows from the staging (the
+  // second row of the pair scaled by sy)
+  if (grp < 21 && lt < R2) {
+    const double2 *x0 = S2 + (2 * gp) * MP2, *y0 = S2 + (2 * gp + 1) * MP2;
+    const double sy = (2 * gp + 1 < 13) ? PB::factor(cmx[2 * gp], cmx[2 * gp + 1], false) : 1.0;
+    const double2 om = (gr == 0) ? double2{1.0, 0.0}
+                     : double2{-0.5, (gr == 1) ? -0.86602540378443864676 : 0.86602540378443864676};
+    const double2 *tw = TW3 + gr * M;
+    double2 v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; n1++) {
+      const int m = n1 * R2 + lt, mq = M - m;
+      const double2 a = x0[m], c = x0[mq];
+      const double2 b = double2{y0[m].x * sy, y0[m].y * sy}, d = double2{y0[mq].x * sy, y0[mq].y * sy};
+      double2 zm = double2{a.x + b.y, b.x - a.y};           // 2 Z[m]
+      const double2 zp = double2{c.x - d.y, c.y + d.x};     // 2 Z[N - (M - m)] (zero at m = 0)
+      if (n1 == 0 && lt == 0) zm = double2{2.0 * a.x, 2.0 * b.x};
+      v[n1] = cmulf(cadd(zm, cmulf(om, zp)), tw[m]);
+    }
+    dftr<R1, +1>(v);
+    double2 *T = X + grp * TG;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; k1++) T[k1 * TP + lt] = (k1 == 0) ? v[0] : cmulf(v[k1], TWM[lt * WP + k1]);
+  }
+  __syncthreads();
+  // ---- backward, step 2: row k1 = lt -> grid samples j = 3 (k1 + R1 k2) + r
+  {
+    double2 w[R2];
+    if (grp < 21 && lt < R1) {
+      const double2 *T = X + grp * TG + lt * TP;
+#pragma unroll
+      for (int n2 = 0; n2 < R2; n2++) w[n2] = T[n2];
+      dftr<R2, +1>(w);
+    }
+    __syncthreads();
+    if (grp < 21 && lt < R1) {
+      double2 *G = X + gp * N + 3 * lt + gr;
+#pragma unroll
+      for (int k2 = 0; k2 < R2; k2++) G[3 * R1 * k2] = w[k2];
+    }
+  }
+  __syncthreads();
+  // ---- products at every grid point (the second rows unscaled on the way
+  // in), with the largest magnitude of each product row
+  {
+    const double cv = 0.25 * pc.cv, cl = 0.25 * pc.cl, ci = 0.25 * pc.ci, ct = 0.25 * pc.ct;
+    double iy[6];
+#pragma unroll
+    for (int p = 0; p < 6; p++) iy[p] = PB::factor(cmx[2 * p], cmx[2 * p + 1], true);
+    U hm[12];
+#pragma unroll
+    for (int c = 0; c < 12; c++) hm[c] = 0;
+    for (int q = tid; q < N; q += F4_THREADS) {
+      const double2 p0 = X[0 * N + q], p1 = X[1 * N + q], p2 = X[2 * N + q], p3 = X[3 * N + q];
+      const double2 p4 = X[4 * N + q], p5 = X[5 * N + q], p6 = X[6 * N + q];
+      const double ur = p0.x, ut = p0.y * iy[0], up = p1.x, wr = p1.y * iy[1], wt = p2.x, wp = p2.y * iy[2];
+      const double br = p3.x, bt = p3.y * iy[3], bp = p4.x, jr = p4.y * iy[4], jt = p5.x, jp = p5.y * iy[5];
+      const double tt = p6.x;
+      const double2 hv[6] = {double2{(wt * up - wp * ut) * cv, (wp * ur - wr * up) * cv},
+                             double2{(wr * ut - wt * ur) * cv, (jt * bp - jp * bt) * cl},
+                             double2{(jp * br - jr * bp) * cl, (jr * bt - jt * br) * cl},
+                             double2{(ut * bp - up * bt) * ci, (up * br - ur * bp) * ci},
+                             double2{(ur * bt - ut * br) * ci, ur * tt * ct},
+                             double2{ut * tt * ct, up * tt * ct}};
+#pragma unroll
+      for (int p = 0; p < 6; p++) {
+        X[p * N + q] = hv[p];
+        hm[2 * p] = max(hm[2 * p], PB::abs_bits(hv[p].x));
+        hm[2 * p + 1] = max(hm[2 * p + 1], PB::abs_bits(hv[p].y));
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+      U v = hm[c];
+      for (int o = 16; o > 0; o >>= 1) v = max(v, (U)__shfl_xor_sync(0xffffffffu, v, o));
+      if (lane == 0) atomicMax(cmx + 13 + c, v);
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < 6 * N; idx += F4_THREADS) {
+    const int p = idx / N;
+    X[idx].y *= PB::factor(cmx[13 + 2 * p], cmx[14 + 2 * p], false);
+  }
+  __syncthreads();
+  // ---- forward, step 1: column n2 = lt of the samples j = 3 (n1 R2 + n2) + r
+  {
+    double2 v[R1];
+    if (grp < 18 && lt < R2) {
+      const double2 *G = X + gp * N + 3 * lt + gr;
+#pragma unroll
+      for (int n1 = 0; n1 < R1; n1++) v[n1] = G[3 * R2 * n1];
+      dftr<R1, -1>(v);
+#pragma unroll
+      for (int k1 = 1; k1 < R1; k1++) v[k1] = cmulc(v[k1], TWM[lt * WP + k1]);
+    }
+    __syncthreads();
+    if (grp < 18 && lt < R2) {
+      double2 *T = X + grp * TG;
+#pragma unroll
+      for (int k1 = 0; k1 < R1; k1++) T[k1 * TP + lt] = v[k1];
+    }
+  }
+  __syncthreads();
+  // ---- forward, step 2: row k1 = lt -> F_r[k1 + R1 k2]
+  {
+    double2 w[R2];
+    if (grp < 18 && lt < R1) {
+      const double2 *T = X + grp * TG + lt * TP;
+#pragma unroll
+      for (int n2 = 0; n2 < R2; n2++) w[n2] = T[n2];
+      dftr<R2, -1>(w);
+    }
+    __syncthreads();
+    if (grp < 18 && lt < R1) {
+      double2 *F = X + grp * M + lt;   // [pair][r][M]: grp = 3 p + r
+#pragma unroll
+      for (int k2 = 0; k2 < R2; k2++) F[R1 * k2] = w[k2];
+    }
+  }
+  __syncthreads();
+  // ---- combine the residues: (a_m, b_m) of both rows of each pair (the
+  // second unscaled), into the staging rows [c][MP2]
+  {
+    const double an = 1.0 / (double)N;
+    for (int idx = tid; idx < 6 * M; idx += F4_THREADS) {
+      const int p = idx / M, m = idx - p * M, mm = (M - m) & (M - 1);
+      const double2 *F = X + p * 3 * M;
+      const double2 t1 = TW3[M + m], t2 = TW3[2 * M + m];
+      const double2 zk = cadd(F[m], cadd(cmulc(F[M + m], t1), cmulc(F[2 * M + m], t2)));
+      const double2 zn = cadd(F[mm], cadd(cmulf(F[M + mm], t1), cmulf(F[2 * M + mm], t2)));
+      const double ay = an * PB::factor(cmx[13 + 2 * p], cmx[14 + 2 * p], true);
+      double2 *o0 = S2 + (2 * p) * MP2, *o1 = S2 + (2 * p + 1) * MP2;
+      if (m == 0) {
+        o0[0] = double2{an * zk.x, 0.0};
+        o1[0] = double2{ay * zk.y, 0.0};
+      } else {
+        o0[m] = double2{an * (zk.x + zn.x), -an * (zk.y - zn.y)};
+        o1[m] = double2{ay * (zk.y + zn.y), ay * (zk.x - zn.x)};
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < 12 * M; e += F4_THREADS) {
+    const int c = e / M, m = e - c * M;
+    reinterpret_cast<double2 *>(fout + (size_t)c * NS)[m] = S2[c * MP2 + m];
   }
 }
 
@@ -1167,6 +1408,27 @@ static int attr_fft_4s(Ctx &c) {
   return 0;
 }
 
+template <int R1, int R2>
+static int attr_fft_4s64(Ctx &c) {
+  using P = F4Plan64<R1, R2>;
+  CB2_CUDA(raise_smem_limit(k_fft_products_4s64<R1, R2>, (int)P::smem()));
+  std::vector<double2> t(P::NTW, double2{0.0, 0.0});
+  const double pi = 3.14159265358979323846;
+  for (int r = 0; r < 3; r++)
+    for (int m = 0; m < P::M; m++) {
+      const double ang = 2.0 * pi * (double)(m * r) / (double)P::N;
+      t[r * P::M + m] = double2{std::cos(ang), std::sin(ang)};
+    }
+  for (int n2 = 0; n2 < R2; n2++)
+    for (int k1 = 0; k1 < R1; k1++) {
+      const double ang = 2.0 * pi * (double)(n2 * k1) / (double)P::M;
+      t[3 * P::M + n2 * P::WP + k1] = double2{std::cos(ang), std::sin(ang)};
+    }
+  CB2_CUDA(cudaMalloc(&c.d_twf4_64, t.size() * sizeof(double2)));
+  CB2_CUDA(cudaMemcpy(c.d_twf4_64, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  return 0;
+}
+
 int fft_setup(Ctx &c) {
   FFTPlan p = make_plan(c.nph);
   if (p.nst < 0) {
@@ -1205,6 +1467,14 @@ int fft_setup(Ctx &c) {
         default: break;
       }
       if (rc) return rc;
+      switch (c.nph) {
+        case 768: rc = attr_fft_4s64<16, 16>(c); break;
+        case 384: rc = attr_fft_4s64<16, 8>(c); break;
+        case 192: rc = attr_fft_4s64<8, 8>(c); break;
+        case 96: rc = attr_fft_4s64<8, 4>(c); break;
+        default: break;
+      }
+      if (rc) return rc;
     }
   }
   if (26 * (size_t)(c.L + 1) * sizeof(float) > 7 * (size_t)c.nph * sizeof(float2)) {
@@ -1220,9 +1490,28 @@ static const typename C2<T>::t *twid(Ctx &c) {
   return (const typename C2<T>::t *)c.d_tw_fft32;
 }
 
+template <int R1, int R2>
+static void launch_fft_4s64(Ctx &c, const double *four, double *four2, const ProdCoef &pc) {
+  k_fft_products_4s64<R1, R2><<<(unsigned)(c.nth * c.nr), F4_THREADS, F4Plan64<R1, R2>::smem(), c.stream>>>(
+      four, four2, c.NS, (const double2 *)c.d_twf4_64, pc);
+}
+
 template <typename T>
 void fft_products(Ctx &c, const T *four, T *four2) {
   using T2 = typename C2<T>::t;
+  if constexpr (sizeof(T) == 8) {
+    // tuning value F4_THREADS selects the four-step kernel where it applies
+    if (c.d_twf4_64 && c.tune[TUNE_FFT_THREADS] == F4_THREADS) {
+      ProdCoef pc{c.p.coef_velo, c.p.coef_lor, c.p.coef_induct, c.p.coef_temp};
+      switch (c.nph) {
+        case 768: launch_fft_4s64<16, 16>(c, four, four2, pc); return;
+        case 384: launch_fft_4s64<16, 8>(c, four, four2, pc); return;
+        case 192: launch_fft_4s64<8, 8>(c, four, four2, pc); return;
+        case 96: launch_fft_4s64<8, 4>(c, four, four2, pc); return;
+        default: break;
+      }
+    }
+  }
   FFTPlan p = make_plan(c.nph);
   size_t sm = 14 * (size_t)c.nph * sizeof(T2) + 32 * sizeof(double);
   ProdCoef pc{c.p.coef_velo, c.p.coef_lor, c.p.coef_induct, c.p.coef_temp};
@@ -1258,34 +1547,36 @@ static void launch_fft_t(Ctx &c, const MLayout &in, const MLayout &out, const Pr
 }
 
 template <int R1, int R2>
-static void launch_fft_4s(Ctx &c, const MLayout &in, const MLayout &out, const ProdCoef &pc) {
+static bool launch_fft_4s(Ctx &c, const MLayout &in, const MLayout &out, const ProdCoef &pc, float *pmax) {
   k_fft_products_4s<R1, R2><<<(unsigned)(c.nth * c.nr), F4_THREADS, F4Plan<R1, R2>::smem(), c.stream>>>(
-      in, out, (const float2 *)c.d_twf4, pc);
+      in, out, (const float2 *)c.d_twf4, pc, pmax, pmax ? mixed_weights32(c) : nullptr);
+  return pmax != nullptr;
 }
 
-void fft_products_m(Ctx &c, const MLayout &in, const MLayout &out) {
+bool fft_products_m(Ctx &c, const MLayout &in, const MLayout &out, float *pmax) {
   ProdCoef pc{c.p.coef_velo, c.p.coef_lor, c.p.coef_induct, c.p.coef_temp};
   // tuning value F4_THREADS selects the four-step kernel where it applies
   if (c.d_twf4 && c.tune[TUNE_FFT_THREADS] == F4_THREADS) {
     switch (c.nph) {
-      case 768: launch_fft_4s<16, 16>(c, in, out, pc); return;
-      case 384: launch_fft_4s<16, 8>(c, in, out, pc); return;
-      case 192: launch_fft_4s<8, 8>(c, in, out, pc); return;
-      case 96: launch_fft_4s<8, 4>(c, in, out, pc); return;
+      case 768: return launch_fft_4s<16, 16>(c, in, out, pc, pmax);
+      case 384: return launch_fft_4s<16, 8>(c, in, out, pc, pmax);
+      case 192: return launch_fft_4s<8, 8>(c, in, out, pc, pmax);
+      case 96: return launch_fft_4s<8, 4>(c, in, out, pc, pmax);
       default: break;
     }
   }
   switch (c.nph) {
-    case 768: launch_fft_t<768>(c, in, out, pc); return;
-    case 384: launch_fft_t<384>(c, in, out, pc); return;
-    case 192: launch_fft_t<192>(c, in, out, pc); return;
-    case 96: launch_fft_t<96>(c, in, out, pc); return;
+    case 768: launch_fft_t<768>(c, in, out, pc); return false;
+    case 384: launch_fft_t<384>(c, in, out, pc); return false;
+    case 192: launch_fft_t<192>(c, in, out, pc); return false;
+    case 96: launch_fft_t<96>(c, in, out, pc); return false;
     default: break;
   }
   FFTPlan p = make_plan(c.nph);
   size_t sm = 14 * (size_t)c.nph * sizeof(float2) + 32 * sizeof(float);
   k_fft_products_m<<<(unsigned)(c.nth * c.nr), 512, sm, c.stream>>>(p, c.L, in, out, (const float2 *)c.d_tw_fft32,
                                                                    pc);
+  return false;
 }
 
 void fft_backward_grid_m(Ctx &c, const MLayout &in, double *grid) {

@@ -96,6 +96,7 @@ struct Ctx {
   void *cn_pack = nullptr;
   size_t cn_smem = 0;
   bool cn_ready = false;
+  const char *cn_off_reason = "";   // why the fused kernel is unavailable ("" when it is)
   int *d_status = nullptr;               // device error word
   // budget of each wait inside the tensor-core pipelines (ns): 200 ms, or
   // CB2_PIPE_WAIT_NS from the environment at cb2_create (0: one try, so the
@@ -105,6 +106,7 @@ struct Ctx {
   float *d_tw_fft32 = nullptr;
   void *d_twp32 = nullptr;               // per-stage float2 twiddles of the compile-time FFT plans
   void *d_twf4 = nullptr;                // tables of the four-step products kernel (nphi = 3 (L + 1))
+  void *d_twf4_64 = nullptr;             // the same in float64 (float64 four-step kernel)
   // state
   double *d_f = nullptr;                 // NSLOT * nr * jmax
   void *d_four = nullptr;                // F: nth*nr*13*NS (double or float)
@@ -239,9 +241,18 @@ int mixed_setup(Ctx &c);
 void mixed_free(Ctx &c);
 // slots: first rj slot of each vector, then of each scalar (out.nvec + out.nscal)
 int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out);
-int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots);
+// rowmax_ready: the FFT kernel that wrote `in` also wrote the partial row
+// maxima of mixed_fwd_pmax (fft_products_m returned true)
+int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots, bool rowmax_ready = false);
+// buffer for the partial forward row maxima of a four-step FFT kernel
+// ([theta][(L+1)/16][elements], nullptr when the shape has none) and the
+// Gauss weights in float32
+float *mixed_fwd_pmax(Ctx &c);
+const float *mixed_weights32(Ctx &c);
 // FFT and products of the mixed path (cb2_fft.cu), float32, order-major layouts
-void fft_products_m(Ctx &c, const MLayout &in, const MLayout &out);
+// returns true when it wrote the partial row maxima into pmax (the
+// four-step kernel; pmax may be nullptr)
+bool fft_products_m(Ctx &c, const MLayout &in, const MLayout &out, float *pmax = nullptr);
 void fft_backward_grid_m(Ctx &c, const MLayout &in, double *grid);
 void fft_forward_grid_m(Ctx &c, const double *grid, const MLayout &out);
 

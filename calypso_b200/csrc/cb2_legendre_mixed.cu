@@ -5,11 +5,17 @@
 // float16 halves
 //     x s = hi + lo,  hi = fp16(x s),  lo = fp16(x s - hi),
 // and a product is accumulated in float32 as hi*hi' + hi*lo' + lo*hi'
-// (three tcgen05.mma kind::f16 into one TMEM accumulator), unscaled in the
-// epilogue.  Scaling to 2^14 rather than 1 keeps lo a normal fp16 number for
-// every value within 2^17 of the row (column) maximum, so those values carry
-// 22 significant bits; smaller ones keep an absolute error of ~2^-38 of the
-// maximum.  The float32 accumulator adds ~2^-24 of the running sum per term.
+// (three tcgen05.mma kind::f16), unscaled in the epilogue.  Scaling to 2^14
+// rather than 1 keeps lo a normal fp16 number for every value within 2^17 of
+// the row (column) maximum, so those values carry 22 significant bits;
+// smaller ones keep an absolute error of ~2^-38 of the maximum.  The float32
+// accumulator is rounded after every MMA, which sets the error of these
+// transforms (dropping the lo*lo' term changes nothing measurable): the
+// backward kernel adds the three products into one TMEM accumulator, the
+// forward kernel (longer K: all colatitudes of a hemisphere, twice for the
+// theta/phi block) keeps hi*hi' and the cross terms, 2^-11 smaller, in two
+// accumulators summed in the epilogue, so the large one is rounded a third
+// as often.
 //
 // Mathematics: the per-order contractions of legendre_bwd_trans_org.f90 /
 // legendre_fwd_trans_org.f90 of the reference (the float64 version is
@@ -237,6 +243,7 @@ struct FwdArgs {
   const float *rowmax;   // [m][element], k_rowmax_four
   int *status;
   unsigned long long wait_ns;   // budget of each pipeline wait (Ctx::pipe_wait_ns)
+  int split;             // 1: hi*hi' and the cross terms in separate accumulators
 };
 
 // shared-memory descriptor, K-major, 64-byte swizzle (8-row groups 512 bytes apart)
@@ -364,7 +371,10 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
   const uint32_t AB_BYTES = 4 * FA_BYTES + 4 * B_BYTES;    // A hi/lo x 2 parities, B hi/lo x 2 parities
   unsigned char *raw0 = base + lay.raw, *ab0 = base + lay.ab;
   const uint32_t accw = tmem_cols / (uint32_t)nacc;       // columns of one accumulator set
-  const uint32_t acc1 = accw / 2;                          // parity-1 accumulator within a set
+  // a set holds the accumulator of each parity (hi*hi' + cross terms), or
+  // with a.split the hi*hi' accumulators at 0 and acc1 and the cross-term
+  // accumulators at 2 acc1 and 3 acc1
+  const uint32_t acc1 = a.split ? accw / 4 : accw / 2;
 
   if (tid == 0) {
     // consumer barriers count warps: one elected lane arrives for its warp
@@ -468,12 +478,16 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             const uint64_t dah = smem_desc_sw64(at + (2 * p) * FA_BYTES), dal = smem_desc_sw64(at + (2 * p + 1) * FA_BYTES);
             const uint64_t dbh = smem_desc_sw64(bb + (2 * p) * B_BYTES), dbl = smem_desc_sw64(bb + (2 * p + 1) * B_BYTES);
             const uint32_t acc = accb + (p ? acc1 : 0u);
+            // the cross terms are 2^-11 of hi*hi': in their own accumulator
+            // they add no rounding to the large one
+            const uint32_t accx = a.split ? acc + 2 * acc1 : acc;
 #pragma unroll
             for (int ks = 0; ks < FKB / 16; ks++) {
               const uint64_t o = (uint64_t)(ks * 2);
-              mma_f16(acc, dah + o, dbh + o, idesc, (b == 0 && ks == 0) ? 0u : 1u);
-              mma_f16(acc, dah + o, dbl + o, idesc, 1u);
-              mma_f16(acc, dal + o, dbh + o, idesc, 1u);
+              const uint32_t first = (b == 0 && ks == 0) ? 0u : 1u;
+              mma_f16(acc, dah + o, dbh + o, idesc, first);
+              mma_f16(accx, dah + o, dbl + o, idesc, a.split ? first : 1u);
+              mma_f16(accx, dal + o, dbh + o, idesc, 1u);
             }
           }
           mma_commit(&sb->abempty[s]);
@@ -631,6 +645,12 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
       for (int g = 0; g < ng; g++) {
         float p0[4], p1[4];
         tmem_ld_16x256b_pair(tl + (uint32_t)(g * 8), tl + acc1 + (uint32_t)(g * 8), p0, p1);
+        if (a.split) {
+          float x0[4], x1[4];
+          tmem_ld_16x256b_pair(tl + 2 * acc1 + (uint32_t)(g * 8), tl + 3 * acc1 + (uint32_t)(g * 8), x0, x1);
+#pragma unroll
+          for (int j = 0; j < 4; j++) { p0[j] += x0[j]; p1[j] += x1[j]; }
+        }
         if (g == ng - 1) {
           tc_fence_before();
           __syncwarp();
@@ -1139,6 +1159,30 @@ k_rowmax_four(MLayout in, const float *wgt, float *Mf) {
   Mf[(size_t)m * (sP + sD) + e] = 2.0f * mx;
 }
 
+// the same maxima from the four-step FFT kernel's partial maxima
+// pm[theta][mb][e] (largest |x| w over the 16 orders of block mb at one
+// colatitude): a row's scale then covers its block of 16 orders
+__global__ void __launch_bounds__(256)
+k_rowmax_reduce(const float *__restrict__ pm, int nth, int MB, size_t E, int L, float *__restrict__ Mf) {
+  const int mb = blockIdx.y;
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  const float *x = pm + (size_t)mb * E + e;
+  const size_t st = (size_t)MB * E;
+  float mx = 0.0f;
+  int th = 0;
+  for (; th + 16 <= nth; th += 16) {
+    float v[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) v[u] = __ldg(x + (size_t)(th + u) * st);
+#pragma unroll
+    for (int u = 0; u < 16; u++) mx = fmaxf(mx, v[u]);
+  }
+  for (; th < nth; th++) mx = fmaxf(mx, __ldg(x + (size_t)th * st));
+  const int m1 = min(L + 1, mb * 16 + 16);
+  for (int m = mb * 16; m < m1; m++) Mf[(size_t)m * E + e] = 2.0f * mx;
+}
+
 // ---------------------------------------------------------------------------
 // B operands: scaled fp16 hi/lo copies of the float64 P tables
 __device__ inline void split_store(__half *hi, __half *lo, size_t at, double v, float s) {
@@ -1229,12 +1273,14 @@ struct MixedTables {
   int *bf_roff = nullptr, *bf_nl = nullptr;
   float *wgt32 = nullptr;                         // Gauss weights in float
   float *rowmax_four = nullptr;                   // [(L+1)][26 nr + 8]
+  float *fwd_pmax = nullptr;                      // [nth][(L+1)/16][E], four-step FFT maxima
+  int pmax_mb = 0;
   int Kb_all = 0, rows_all = 0, nhp = 0, NFmax = 0;
   size_t smem_bwd = 0, smem_fwd = 0, smem_pack = 0;
   CUtensorMap tm_bb_hi, tm_bb_lo, tm_bfp_hi, tm_bfp_lo, tm_bfd_hi, tm_bfd_lo;
   int boxr = 0, nfb = 0;
   uint32_t tmem_fwd = 0;
-  int nacc_fwd = 1, nsm = 148;
+  int nacc_fwd = 1, nsm = 148, split_fwd = 0;
   uint32_t tmem_bwd = 0;
   int nacc_bwd = 1;
 };
@@ -1328,10 +1374,17 @@ int mixed_setup(Ctx &c) {
   if (c.nth % 8 != 0) { set_error("mixed precision path needs nth divisible by 8"); return CB2_ERR_ARG; }
   t->boxr = std::min(64, t->NFmax);
   t->nfb = ((t->NFmax + t->boxr - 1) / t->boxr) * t->boxr;
-  // one accumulator set = both parities; two sets when they fit in TMEM
-  t->nacc_fwd = (4 * t->NFmax <= 512) ? 2 : 1;
+  // one accumulator set = both parities, each as a hi*hi' and a cross-term
+  // accumulator where they fit in TMEM (L <= 255); two sets when they fit.
+  // Measured on the L255/Nr129 state: the separate cross-term accumulators
+  // halve the error of the forward transform (1.1e-6 -> 5.5e-7 relative on
+  // the theta/phi outputs, 3e-7 -> 6e-8 on the radial ones), because the
+  // large accumulator is rounded after 1 MMA in 3 instead of every MMA.
+  t->split_fwd = (4 * t->NFmax <= 512) ? 1 : 0;
+  const int per_set = (t->split_fwd ? 4 : 2) * t->NFmax;
+  t->nacc_fwd = (2 * per_set <= 512) ? 2 : 1;
   t->tmem_fwd = 32;
-  while ((int)t->tmem_fwd < 2 * t->nacc_fwd * t->NFmax) t->tmem_fwd *= 2;
+  while ((int)t->tmem_fwd < t->nacc_fwd * per_set) t->tmem_fwd *= 2;
   t->rows_all = R + t->NFmax;   // every NFmax-row box stays in the array
   auto up = [&](int **d, const std::vector<int> &v) -> int {
     CB2_CUDA(cudaMalloc(d, v.size() * sizeof(int)));
@@ -1365,6 +1418,14 @@ int mixed_setup(Ctx &c) {
     CB2_CUDA(cudaMemcpy(t->wgt32, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   CB2_CUDA(cudaMalloc(&t->rowmax_four, (size_t)(L + 1) * (26 * (size_t)c.nr + 8) * sizeof(float)));
+  // the four-step FFT kernel (nph = 3 (L + 1), L + 1 a multiple of 16)
+  // writes maxima over blocks of 16 orders, which replace k_rowmax_four
+  if (c.nph == 3 * (L + 1) && (L + 1) % 16 == 0) {
+    MLayout o;
+    o.nvec = 4; o.nscal = 0; o.nr = c.nr; o.nth = c.nth;
+    t->pmax_mb = (L + 1) / 16;
+    CB2_CUDA(cudaMalloc(&t->fwd_pmax, (size_t)c.nth * t->pmax_mb * (o.sP() + o.sD()) * sizeof(float)));
+  }
   k_build_bwd_b<<<dim3(cdiv(nh, 64), L + 1), 64, 0, c.stream>>>(L, nh, t->nhp, c.d_poff, c.d_Plt, c.d_dPlt,
                                                                 c.d_asin, t->bb_ko, t->Kb_all, t->bb_unscale,
                                                                 t->bb_hi, t->bb_lo);
@@ -1414,7 +1475,7 @@ void mixed_free(Ctx &c) {
   if (!t) return;
   void *ptrs[] = {t->bb_hi, t->bb_lo, t->bb_unscale, t->bb_ko, t->kbase, t->rlmP, t->rlmD, t->maxP, t->maxD,
                   t->bfp_hi, t->bfp_lo, t->bfd_hi, t->bfd_lo, t->bf_unscale, t->bf_roff, t->bf_nl, t->wgt32,
-                  t->rowmax_four};
+                  t->rowmax_four, t->fwd_pmax};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete t;
@@ -1481,7 +1542,17 @@ int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   return 0;
 }
 
-int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots) {
+float *mixed_fwd_pmax(Ctx &c) {
+  MixedTables *t = (MixedTables *)c.mixed;
+  return t ? t->fwd_pmax : nullptr;
+}
+
+const float *mixed_weights32(Ctx &c) {
+  MixedTables *t = (MixedTables *)c.mixed;
+  return t ? t->wgt32 : nullptr;
+}
+
+int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots, bool rowmax_ready) {
   MixedTables *t = (MixedTables *)c.mixed;
   const int nvec = in.nvec, nscal = in.nscal;
   FwdArgs a{};
@@ -1496,6 +1567,7 @@ int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots) {
   a.rowmax = t->rowmax_four;
   a.status = c.d_status;
   a.wait_ns = c.pipe_wait_ns;
+  a.split = t->split_fwd;
   // raw Fourier rows: float32 [(m, theta)][element], boxes of 128 elements x 32 colatitudes
   CUtensorMap rawP{}, rawD{};
   const uint64_t nthr = (uint64_t)(c.L + 1) * c.nth;
@@ -1506,8 +1578,14 @@ int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots) {
     return CB2_ERR_ARG;
   }
   if (nvec == 0) rawD = rawP;
-  k_rowmax_four<<<dim3(cdiv((long)(in.sP() + in.sD()), 256), c.L + 1), 256, 0, c.stream>>>(in, t->wgt32,
-                                                                                       t->rowmax_four);
+  if (rowmax_ready && t->fwd_pmax && nvec == 4 && nscal == 0) {
+    const size_t E = in.sP() + in.sD();
+    k_rowmax_reduce<<<dim3(cdiv((long)E, 256), t->pmax_mb), 256, 0, c.stream>>>(t->fwd_pmax, c.nth, t->pmax_mb, E,
+                                                                               c.L, t->rowmax_four);
+  } else {
+    k_rowmax_four<<<dim3(cdiv((long)(in.sP() + in.sD()), 256), c.L + 1), 256, 0, c.stream>>>(in, t->wgt32,
+                                                                                         t->rowmax_four);
+  }
   const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
   const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
   const int ntiles = (tiles0 + tiles1) * (c.L + 1);

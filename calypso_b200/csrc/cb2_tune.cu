@@ -58,6 +58,11 @@ static int stage_fwd_f64(Ctx &c) {
   CB2_CUDA(cudaGetLastError());
   return 0;
 }
+static int stage_fft_f64(Ctx &c) {
+  fft_products<double>(c, (const double *)c.d_four, (double *)c.d_four2);
+  CB2_CUDA(cudaGetLastError());
+  return 0;
+}
 static int stage_bwd_mixed(Ctx &c) {
   int rc = leg_bwd_mixed(c, kBwdSlots, mlayout(c, c.d_four, 4, 1));
   if (!rc) CB2_CUDA(cudaGetLastError());
@@ -86,6 +91,8 @@ int autotune(Ctx &c) {
   if (c.prec == CB2_PREC_FP64) {
     items.push_back({TUNE_BWD_KT, {2, 4}, stage_bwd_f64});
     items.push_back({TUNE_FWD_KT, {1, 2}, stage_fwd_f64});
+    // 384: the float64 four-step kernel (where nphi = 3 (L + 1)), 512: Stockham
+    items.push_back({TUNE_FFT_THREADS, {384, 512}, stage_fft_f64});
   } else {
     items.push_back({TUNE_PACK_KC, {1, 2, 4}, stage_bwd_mixed});
     items.push_back({TUNE_FFT_THREADS, {384, 512, 256, 128}, stage_fft_mixed});
@@ -138,6 +145,8 @@ int cb2_get_tuning(const cb2_ctx *c, int out[TUNE_N]) {
   for (int q = 0; q < TUNE_N; q++) out[q] = c->tune[q];
   return 0;
 }
+
+const char *cb2_tuning_note(const cb2_ctx *c) { return c ? c->cn_off_reason : ""; }
 
 int cb2_set_tuning(cb2_ctx *c, const int in[TUNE_N]) {
   if (!c || !in) { set_error("cb2_set_tuning: null argument"); return CB2_ERR_ARG; }

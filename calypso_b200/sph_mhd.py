@@ -57,7 +57,8 @@ RESTART_FIELDS_COMPS = [(n, c) for n, nc in RESTART_FIELDS for c in range(nc)]
 
 # kernel-variant tuning entries (cb2_get_tuning / cb2_set_tuning): float64
 # backward radial tile, float64 forward radial tile, mixed pack radial tile,
-# mixed FFT threads, fused Crank-Nicolson step (1) or separate kernels (0)
+# FFT kernel (384 four-step, else Stockham threads), fused Crank-Nicolson
+# step (1) or separate kernels (0)
 TUNE_BWD_KT, TUNE_FWD_KT, TUNE_PACK_KC, TUNE_FFT_THREADS, TUNE_CN = range(5)
 TUNE_N = 5
 
@@ -164,7 +165,7 @@ EXPORTS = [
     "cb2_ensemble_init_fields", "cb2_ensemble_step", "cb2_ensemble_sync", "cb2_ensemble_time_steps",
     "cb2_ensemble_energies", "cb2_leg_bwd", "cb2_leg_fwd", "cb2_fft_bwd", "cb2_fft_fwd",
     "cb2_legendre_trans_mode", "cb2_fft_library_known", "cb2_energy_spectra", "cb2_fft_products",
-    "cb2_get_restart_state", "cb2_set_restart_state", "cb2_step_restart_state",
+    "cb2_get_restart_state", "cb2_set_restart_state", "cb2_step_restart_state", "cb2_tuning_note",
 ]
 
 
@@ -207,6 +208,7 @@ def load_library(path: str = LIB_PATH):
         "cb2_energies_static": ([vp, pd], i),
         "cb2_autotune": ([vp], i),
         "cb2_get_tuning": ([vp, P(i)], i),
+        "cb2_tuning_note": ([vp], ctypes.c_char_p),
         "cb2_set_tuning": ([vp, P(i)], i),
         "cb2_ensemble_create": ([P(Params), i, i, i, i, P(vp)], i),
         "cb2_ensemble_destroy": ([vp], i),
@@ -328,6 +330,11 @@ class SphMHD:
         out = (ctypes.c_int * TUNE_N)()
         _check(load_library().cb2_get_tuning(self._h, out), "cb2_get_tuning")
         return list(out)
+
+    @property
+    def tuning_note(self) -> str:
+        """Why the one-kernel Crank-Nicolson step is off ('' when available)."""
+        return load_library().cb2_tuning_note(self._h).decode(errors="replace")
 
     @tuning.setter
     def tuning(self, values):

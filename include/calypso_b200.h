@@ -270,15 +270,20 @@ int cb2_free_pinned(void *p);
  * candidate tile / launch shape of the transform kernels on this context
  * and keeps the fastest.  Only before cb2_init_fields / cb2_start (it
  * overwrites the work fields).  tuning[5]: float64 backward radial tile,
- * float64 forward radial tile, mixed pack radial tile, mixed FFT threads
- * (384: the four-step kernel, used where nphi = 3 (ltr + 1); 128, 256, 512:
- * the Stockham kernel), and 1 to run the explicit update, the radial solves
- * and the derived fields of the step as one kernel, 0 (the default) as
- * separate kernels; -1 (fixed) where the one kernel cannot take the
- * context's radial factors (a row interchange beyond two rows). */
+ * float64 forward radial tile, mixed pack radial tile, FFT kernel of either
+ * precision (384: the four-step kernel, used where nphi = 3 (ltr + 1);
+ * 128, 256, 512: the Stockham kernel, float64 always with 512 threads), and
+ * 1 to run the explicit update, the radial solves and the derived fields
+ * of the step as one kernel, 0 (the default) as separate kernels; -1
+ * (fixed) where the one kernel cannot take the context (cb2_tuning_note
+ * says why). */
 int cb2_autotune(cb2_ctx *ctx);
 int cb2_get_tuning(const cb2_ctx *ctx, int tuning[5]);
 int cb2_set_tuning(cb2_ctx *ctx, const int tuning[5]);
+/* Why the one-kernel Crank-Nicolson step is unavailable on this context
+ * (tuning entry 4 = -1), e.g. a radial LU factor with a row interchange
+ * more than two rows away; "" when it is available.  Owned by the context. */
+const char *cb2_tuning_note(const cb2_ctx *ctx);
 
 /* Ensemble of independent shells (any mix of truncations and parameters),
  * advanced together: one CUDA graph holds a time step of every shell as

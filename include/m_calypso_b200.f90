@@ -359,6 +359,12 @@ module m_calypso_b200
       integer(c_int) :: rc
     end function cb2_get_tuning
 
+    function cb2_tuning_note(ctx) bind(C, name='cb2_tuning_note') result(rc)
+      import
+      type(c_ptr), value :: ctx
+      type(c_ptr) :: rc
+    end function cb2_tuning_note
+
     function cb2_set_tuning(ctx, tuning) bind(C, name='cb2_set_tuning') result(rc)
       import
       type(c_ptr), value :: ctx

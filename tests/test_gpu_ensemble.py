@@ -92,14 +92,16 @@ def test_small_shell_created_after_large_one_leaves_it_working():
         b.close()
 
 
-def test_four_step_and_stockham_fft_agree():
+@pytest.mark.parametrize("prec,tol", [(PREC_MIXED, 1e-5), (PREC_FP64, 1e-12)])
+def test_four_step_and_stockham_fft_agree(prec, tol):
     # tuning value 384 runs the four-step products kernel (nphi = 3 (L + 1)),
-    # 512 the Stockham kernel: the same float32 transform up to rounding
+    # 512 the Stockham kernel: the same transform up to rounding, in float32
+    # (mixed path) and in float64 (plain path)
     p = configs.small_shell()
     assert p["nph"] == 3 * (p["ltr"] + 1)
     out = []
     for nt in (384, 512):
-        g = SphMHD(p, PREC_MIXED, device=0)
+        g = SphMHD(p, prec, device=0)
         t = g.tuning
         t[3] = nt
         g.tuning = t
@@ -108,4 +110,4 @@ def test_four_step_and_stockham_fft_agree():
         out.append(np.stack([g.get_field(s) for s in (VELO, MAGNE, TEMP)]))
         g.close()
     for a, b in zip(out[0], out[1]):
-        assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b)
+        assert np.linalg.norm(a - b) <= tol * np.linalg.norm(b)
