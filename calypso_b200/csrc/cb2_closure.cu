@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "cb2_internal.cuh"
+#include "cb2_tc.cuh"
 
 namespace cb2 {
 namespace {
@@ -107,69 +108,163 @@ __global__ void k_add_tendency(size_t n, int nr, int jmax, const float *Y, const
 }
 
 // ---------------------------------------------------------------------------
-// GEMM: C[M][N] (+)= sum_k opA[m][k] opB[k][n];
+// GEMM on the tensor cores: C[M][N] (+)= sum_k opA[m][k] opB[k][n];
 //   opA[m][k] = TA ? A[k * lda + m] : A[m * lda + k]
 //   opB[k][n] = TB ? B[n * ldb + k] : B[k * ldb + n]
-// 64 x 64 tile per block, K in steps of 16 through shared memory, each of
-// 256 threads 4 x 4 outputs; blockIdx.z splits K into chunks of kchunk whose
-// partial products are added with float32 atomics (atomic != 0).
+// One CTA (128 threads) per tile of 128 rows x NT <= 256 columns and per
+// chunk of K (blockIdx.z, partial sums added with float32 atomics when
+// `atomic`).  K runs in blocks of 32: the threads load both operand tiles,
+// split float32 values into bfloat16 hi + lo (x = hi + lo to 16 bits;
+// bfloat16 weights are one exact term) and write them K-major, 64-byte
+// swizzled, into one of two shared-memory stages; one thread issues
+// tcgen05.mma kind::f16 with bf16 operands (hi*hi', hi*lo', lo*hi': the
+// products that reach 2^-16 of the result) into a float32 TMEM accumulator
+// and commits to the stage's mbarrier, which the loads of the stage after
+// next wait on.  Every wait is bounded; a wait that runs out sets bit 2 of
+// *status and the CTA drains its MMAs, frees its TMEM and returns.
+constexpr int GK = 32;                        // K per stage (64-byte rows)
+constexpr unsigned long long kWaitNsGemm = 200ull * 1000 * 1000;
+constexpr uint32_t GA_BYTES = 128 * GK * 2;   // one bf16 term of the A tile
+
+template <typename T> struct Terms { static constexpr int n = 2; };
+template <> struct Terms<__nv_bfloat16> { static constexpr int n = 1; };
+
+__device__ inline float to_f(float x) { return x; }
+__device__ inline float to_f(__nv_bfloat16 x) { return __bfloat162float(x); }
+
+// 8 consecutive K values of one row -> nt bf16 terms, 16 bytes each
+template <int NT_>
+__device__ inline void put_row8(unsigned char *tile, uint32_t term_bytes, int row, int chunk, const float v[8]) {
+  uint32_t hi[4], lo[4];
+#pragma unroll
+  for (int e = 0; e < 8; e += 2) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v[e], v[e + 1]);
+    const float2 f = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(v[e] - f.x, v[e + 1] - f.y);
+    hi[e >> 1] = *reinterpret_cast<const uint32_t *>(&h);
+    lo[e >> 1] = *reinterpret_cast<const uint32_t *>(&l);
+  }
+  const uint32_t off = tc::sw64_chunk(row, chunk);
+  *reinterpret_cast<uint4 *>(tile + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+  if (NT_ > 1) *reinterpret_cast<uint4 *>(tile + term_bytes + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+}
+
 template <typename TAT, typename TBT, bool TA, bool TB>
-__global__ void __launch_bounds__(256)
-k_gemm(int M, int N, int K, const TAT *__restrict__ A, int lda, const TBT *__restrict__ B, int ldb, float *C, int ldc,
-       int kchunk, int atomic, int accumulate) {
-  __shared__ float As[16][64 + 4];
-  __shared__ float Bs[16][64 + 4];
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+__global__ void __launch_bounds__(128)
+k_tc_gemm(int M, int N, int NT, int K, const TAT *__restrict__ A, int lda, const TBT *__restrict__ B, int ldb,
+          float *C, int ldc, int kchunk, int atomic, uint32_t tmem_cols, int *status, unsigned long long wait_ns) {
+  constexpr int NA = Terms<TAT>::n, NBT = Terms<TBT>::n;
+  extern __shared__ unsigned char g_smem_raw[];
+  unsigned char *base = tc::smem_base_1024(g_smem_raw);
+  const uint32_t b_bytes = (uint32_t)NT * GK * 2;               // one bf16 term of the B tile
+  const uint32_t stage_bytes = ((NA * GA_BYTES + NBT * b_bytes) + 1023u) & ~1023u;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(base + 2 * stage_bytes);   // [2] stage done, [2] final
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 3);
+  int *abort = reinterpret_cast<int *>(tslot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * 128, n0 = blockIdx.x * NT;
   const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
-  float acc[4][4] = {};
-  for (int k0 = kb; k0 < ke; k0 += 16) {
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const int idx = tid + e * 256;
-      int r, kk;
-      if (TA) { kk = idx >> 6; r = idx & 63; } else { r = idx >> 4; kk = idx & 15; }
-      const int gm = m0 + r, gk = k0 + kk;
-      float v = 0.0f;
-      if (gm < M && gk < ke) v = (float)(TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk]);
-      As[kk][r] = v;
-    }
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const int idx = tid + e * 256;
-      int c, kk;
-      if (TB) { c = idx >> 4; kk = idx & 15; } else { kk = idx >> 6; c = idx & 63; }
-      const int gn = n0 + c, gk = k0 + kk;
-      float v = 0.0f;
-      if (gn < N && gk < ke) v = (float)(TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn]);
-      Bs[kk][c] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < 16; kk++) {
-      float a[4], b[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) { a[q] = As[kk][ty * 4 + q]; b[q] = Bs[kk][tx * 4 + q]; }
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
+  if (tid == 0) {
+    tc::mbar_init(&bar[0], 1); tc::mbar_init(&bar[1], 1); tc::mbar_init(&bar[2], 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  if (warp == 0) tc::tmem_alloc(tslot, tmem_cols);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = tc::idesc_bf16_f32(128, NT);
+  const int nblk = (ke - kb + GK - 1) / GK;
+  bool bad = false;
+  for (int ib = 0; ib < nblk; ib++) {
+    const int st = ib & 1, k0 = kb + ib * GK;
+    unsigned char *ta = base + st * stage_bytes, *tbp = ta + NA * GA_BYTES;
+    // the stage's previous MMAs (block ib - 2) must have read it
+    if (ib >= 2 && !tc::mbar_wait(&bar[st], ((ib - 2) >> 1) & 1, wait_ns)) bad = true;
+    if (__syncthreads_or(bad)) { bad = true; break; }
+    // A tile: thread = row
+    {
+      const int m = m0 + tid;
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const int gm = m0 + ty * 4 + i;
-    if (gm >= M) continue;
+      for (int c = 0; c < GK / 8; c++) {
+        float v[8];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int gn = n0 + tx * 4 + j;
-      if (gn >= N) continue;
-      float *cp = C + (size_t)gm * ldc + gn;
-      if (atomic) atomicAdd(cp, acc[i][j]);
-      else *cp = accumulate ? *cp + acc[i][j] : acc[i][j];
+        for (int e = 0; e < 8; e++) {
+          const int k = k0 + c * 8 + e;
+          v[e] = (m < M && k < ke) ? to_f(TA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k]) : 0.0f;
+        }
+        put_row8<NA>(ta, GA_BYTES, tid, c, v);
+      }
+    }
+    // B tile: rows n of the column tile
+    for (int r = tid; r < NT; r += 128) {
+      const int n = n0 + r;
+#pragma unroll
+      for (int c = 0; c < GK / 8; c++) {
+        float v[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+          const int k = k0 + c * 8 + e;
+          v[e] = (n < N && k < ke) ? to_f(TB ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n]) : 0.0f;
+        }
+        put_row8<NBT>(tbp, b_bytes, r, c, v);
+      }
+    }
+    tc::fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc::tc_fence_after();
+#pragma unroll
+      for (int ks = 0; ks < GK / 16; ks++) {
+        const uint64_t o = (uint64_t)(ks * 2);
+        const uint64_t ah = tc::smem_desc_sw64(ta) + o, bh = tc::smem_desc_sw64(tbp) + o;
+        tc::mma_f16(tmem, ah, bh, idesc, (ib == 0 && ks == 0) ? 0u : 1u);
+        if (NBT > 1) tc::mma_f16(tmem, ah, tc::smem_desc_sw64(tbp + b_bytes) + o, idesc, 1u);
+        if (NA > 1) tc::mma_f16(tmem, tc::smem_desc_sw64(ta + GA_BYTES) + o, bh, idesc, 1u);
+      }
+      tc::mma_commit(&bar[st]);
     }
   }
+  // every MMA has completed before the accumulator is read and freed
+  if (tid == 0) {
+    if (nblk > 0) tc::mma_commit(&bar[2]);
+  }
+  __syncthreads();
+  const bool done = nblk == 0 || tc::mbar_wait(&bar[2], 0, tc::kWaitNs);
+  if (!done || bad) {
+    if (tid == 0) atomicOr(status, CB2_STATUS_PIPE_TIMEOUT);
+    *abort = 1;
+  }
+  __syncthreads();
+  tc::tc_fence_after();
+  if (!*abort && nblk > 0) {
+    // epilogue: warp w holds TMEM lanes 32 w .. 32 w + 31 (tile rows)
+    const int m = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < NT; c0 += 64) {
+      float va[32], vb[32];
+      const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      tc::tmem_ld32x2(ta, ta + 32, va, vb);
+      if (m < M) {
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          const int n = n0 + c0 + j;
+          if (c0 + j < NT && n < N) {
+            float *cp = C + (size_t)m * ldc + n;
+            if (atomic) atomicAdd(cp, va[j]); else *cp = va[j];
+          }
+          const int n2 = n + 32;
+          if (c0 + 32 + j < NT && n2 < N) {
+            float *cp = C + (size_t)m * ldc + n2;
+            if (atomic) atomicAdd(cp, vb[j]); else *cp = vb[j];
+          }
+        }
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, tmem_cols);
 }
 
 __device__ inline float sigm(float z) { return 1.0f / (1.0f + __expf(-z)); }
@@ -260,6 +355,7 @@ struct cb2_mlp {
   float *Z1 = nullptr, *H1 = nullptr, *Z2 = nullptr, *H2 = nullptr, *Yp = nullptr, *dY = nullptr;
   float *dH = nullptr, *dZ = nullptr;
   double *part = nullptr;       // loss partial sums
+  int *status = nullptr;        // device status word of the GEMMs (bit 2: a wait ran out)
   size_t part_cap = 0;
   cudaStream_t stream = nullptr;
 };
@@ -286,29 +382,50 @@ int mlp_reserve(cb2_mlp *n, size_t rows) {
   return 0;
 }
 
+// C = opA opB on the tensor cores (k_tc_gemm).  split_k: K is cut into
+// chunks so that the grid covers the SMs about twice, C is cleared and the
+// chunks' partial products are added with atomics.
 template <typename TAT, typename TBT, bool TA, bool TB>
-void gemm(cudaStream_t st, int M, int N, int K, const TAT *A, int lda, const TBT *B, int ldb, float *C, int ldc,
-          bool split_k) {
+void gemm(cudaStream_t st, int *status, int M, int N, int K, const TAT *A, int lda, const TBT *B, int ldb, float *C,
+          int ldc, bool split_k) {
+  constexpr int NA = Terms<TAT>::n, NBT = Terms<TBT>::n;
+  const int NT = std::min(256, ((N + 15) / 16) * 16);
+  uint32_t cols = 64;
+  while ((int)cols < NT) cols *= 2;
+  const uint32_t stage = ((NA * GA_BYTES + NBT * (uint32_t)NT * GK * 2) + 1023u) & ~1023u;
+  const size_t smem = 2 * (size_t)stage + 64 + 1024;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_tc_gemm<TAT, TBT, TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         2 * (2 * GA_BYTES + 2 * 256 * GK * 2) + 64 + 1024);
+    attr_set = true;
+  }
+  const int tiles = ((N + NT - 1) / NT) * ((M + 127) / 128);
   int kchunk = K, nz = 1;
   if (split_k) {
-    kchunk = 4096;
+    nz = std::max(1, std::min((K + 255) / 256, (2 * 148 + tiles - 1) / tiles));
+    kchunk = (((K + nz - 1) / nz) + GK - 1) / GK * GK;
     nz = (K + kchunk - 1) / kchunk;
     cudaMemsetAsync(C, 0, (size_t)M * ldc * sizeof(float), st);
   }
-  dim3 grid((N + 63) / 64, (M + 63) / 64, nz);
-  k_gemm<TAT, TBT, TA, TB><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, kchunk, split_k ? 1 : 0, 0);
+  dim3 grid((N + NT - 1) / NT, (M + 127) / 128, nz);
+  k_tc_gemm<TAT, TBT, TA, TB><<<grid, 128, smem, st>>>(M, N, NT, K, A, lda, B, ldb, C, ldc, kchunk,
+                                                        split_k ? 1 : 0, cols, status, kWaitNsGemm);
 }
 
 // forward pass of n rows of X (normalised features) into n->Yp, on stream st
-int mlp_forward(cb2_mlp *nt, const float *X, size_t n, cudaStream_t st) {
+int mlp_forward(cb2_mlp *nt, const float *X, size_t n, cudaStream_t st, int *status = nullptr) {
   int rc = mlp_reserve(nt, n);
   if (rc) return rc;
+  if (!status) status = nt->status;
   const int F = nt->F, H = nt->H, O = nt->O;
-  gemm<float, __nv_bfloat16, false, true>(st, (int)n, H, F, X, F, nt->w + nt->oW1, F, nt->Z1, H, false);
+  gemm<float, __nv_bfloat16, false, true>(st, status, (int)n, H, F, X, F, nt->w + nt->oW1, F, nt->Z1, H, false);
   k_bias_act<<<blocks(n * H), 256, 0, st>>>(n, H, nt->Z1, nt->master + nt->ob1, nt->H1, 1);
-  gemm<float, __nv_bfloat16, false, true>(st, (int)n, H, H, nt->H1, H, nt->w + nt->oW2, H, nt->Z2, H, false);
+  gemm<float, __nv_bfloat16, false, true>(st, status, (int)n, H, H, nt->H1, H, nt->w + nt->oW2, H, nt->Z2, H,
+                                          false);
   k_bias_act<<<blocks(n * H), 256, 0, st>>>(n, H, nt->Z2, nt->master + nt->ob2, nt->H2, 1);
-  gemm<float, __nv_bfloat16, false, true>(st, (int)n, O, H, nt->H2, H, nt->w + nt->oW3, H, nt->Yp, O, false);
+  gemm<float, __nv_bfloat16, false, true>(st, status, (int)n, O, H, nt->H2, H, nt->w + nt->oW3, H, nt->Yp, O,
+                                          false);
   k_bias_act<<<blocks(n * O), 256, 0, st>>>(n, O, nt->Yp, nt->master + nt->ob3, nt->Yp, 0);
   CB2_CUDA(cudaGetLastError());
   return 0;
@@ -323,17 +440,17 @@ int mlp_backward(cb2_mlp *nt, const float *X, const float *T, size_t n, double *
   const unsigned nb = blocks(n * O);
   k_mse<<<nb, 256, 0, st>>>(n, O, nt->Yp, T, nt->dY, nt->part);
   // layer 3
-  gemm<float, float, true, false>(st, O, H, (int)n, nt->dY, O, nt->H2, H, nt->grad + nt->oW3, H, true);
+  gemm<float, float, true, false>(st, nt->status, O, H, (int)n, nt->dY, O, nt->H2, H, nt->grad + nt->oW3, H, true);
   k_colsum<<<O, 256, 0, st>>>(n, O, nt->dY, nt->grad + nt->ob3);
-  gemm<float, __nv_bfloat16, false, false>(st, (int)n, H, O, nt->dY, O, nt->w + nt->oW3, H, nt->dH, H, false);
+  gemm<float, __nv_bfloat16, false, false>(st, nt->status, (int)n, H, O, nt->dY, O, nt->w + nt->oW3, H, nt->dH, H, false);
   k_act_grad<<<blocks(n * H), 256, 0, st>>>(n * H, nt->Z2, nt->dH, nt->dZ);
   // layer 2
-  gemm<float, float, true, false>(st, H, H, (int)n, nt->dZ, H, nt->H1, H, nt->grad + nt->oW2, H, true);
+  gemm<float, float, true, false>(st, nt->status, H, H, (int)n, nt->dZ, H, nt->H1, H, nt->grad + nt->oW2, H, true);
   k_colsum<<<H, 256, 0, st>>>(n, H, nt->dZ, nt->grad + nt->ob2);
-  gemm<float, __nv_bfloat16, false, false>(st, (int)n, H, H, nt->dZ, H, nt->w + nt->oW2, H, nt->dH, H, false);
+  gemm<float, __nv_bfloat16, false, false>(st, nt->status, (int)n, H, H, nt->dZ, H, nt->w + nt->oW2, H, nt->dH, H, false);
   k_act_grad<<<blocks(n * H), 256, 0, st>>>(n * H, nt->Z1, nt->dH, nt->dZ);
   // layer 1
-  gemm<float, float, true, false>(st, H, F, (int)n, nt->dZ, H, X, F, nt->grad + nt->oW1, F, true);
+  gemm<float, float, true, false>(st, nt->status, H, F, (int)n, nt->dZ, H, X, F, nt->grad + nt->oW1, F, true);
   k_colsum<<<H, 256, 0, st>>>(n, H, nt->dZ, nt->grad + nt->ob1);
   CB2_CUDA(cudaGetLastError());
   if (loss) {
@@ -368,7 +485,7 @@ int closure_apply(Ctx &c) {
                                               c.h_r[c.kout], c.d_f, c.fsize(), feat_slots(), cs->X);
   const size_t nn = (size_t)c.nr * NF;
   k_normalise<<<blocks(n * NF), 256, 0, c.stream>>>(n, c.jmax, cs->X, cs->norm, cs->norm + nn, cs->Xn);
-  int rc = mlp_forward(cs->net, cs->Xn, n, c.stream);
+  int rc = mlp_forward(cs->net, cs->Xn, n, c.stream, c.d_status);
   if (rc) return rc;
   k_add_tendency<<<blocks(n), 256, 0, c.stream>>>(n, c.nr, c.jmax, cs->net->Yp, cs->norm + 2 * nn, c.d_f, c.fsize(),
                                                   out_slots());
@@ -419,12 +536,14 @@ int cb2_mlp_create(int nin, int nhid, int nout, unsigned seed, cb2_mlp **out) {
       cudaMalloc(&n->grad, n->np * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&n->m, n->np * sizeof(float)) != cudaSuccess ||
       cudaMalloc(&n->v, n->np * sizeof(float)) != cudaSuccess ||
-      cudaMalloc(&n->w, n->np * sizeof(__nv_bfloat16)) != cudaSuccess)
+      cudaMalloc(&n->w, n->np * sizeof(__nv_bfloat16)) != cudaSuccess ||
+      cudaMalloc(&n->status, sizeof(int)) != cudaSuccess)
     return fail(cuda_fail(cudaGetLastError(), "cb2_mlp_create"));
   cudaMemcpy(n->master, p.data(), n->np * sizeof(float), cudaMemcpyHostToDevice);
   cudaMemset(n->grad, 0, n->np * sizeof(float));
   cudaMemset(n->m, 0, n->np * sizeof(float));
   cudaMemset(n->v, 0, n->np * sizeof(float));
+  cudaMemset(n->status, 0, sizeof(int));
   k_to_bf16<<<blocks(n->np), 256, 0, n->stream>>>(n->np, n->master, n->w);
   if (cudaStreamSynchronize(n->stream) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "cb2_mlp_create"));
   *out = n;
@@ -435,7 +554,7 @@ int cb2_mlp_destroy(cb2_mlp *n) {
   if (!n) return 0;
   if (n->stream) cudaStreamSynchronize(n->stream);
   void *ptrs[] = {n->master, n->grad, n->m, n->v, n->w, n->Z1, n->H1, n->Z2, n->H2, n->Yp, n->dY, n->dH, n->dZ,
-                  n->part};
+                  n->part, n->status};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (n->stream) cudaStreamDestroy(n->stream);
@@ -460,13 +579,26 @@ int cb2_mlp_set_params(cb2_mlp *n, const float *host) {
   return 0;
 }
 
+// the GEMMs' status word after the stream has drained: a pipeline wait
+// that ran out is reported (and the word cleared)
+static int mlp_status(cb2_mlp *n) {
+  int st = 0;
+  CB2_CUDA(cudaMemcpyAsync(&st, n->status, sizeof(int), cudaMemcpyDeviceToHost, n->stream));
+  CB2_CUDA(cudaStreamSynchronize(n->stream));
+  if (st) {
+    CB2_CUDA(cudaMemsetAsync(n->status, 0, sizeof(int), n->stream));
+    set_error("closure network: a tensor-core pipeline wait ran out");
+    return CB2_ERR_TIMEOUT;
+  }
+  return 0;
+}
+
 int cb2_mlp_forward(cb2_mlp *n, const float *dev_x, long long rows, float *dev_y) {
   if (!n || !dev_x || !dev_y || rows <= 0) return CB2_ERR_ARG;
   int rc = mlp_forward(n, dev_x, (size_t)rows, n->stream);
   if (rc) return rc;
   CB2_CUDA(cudaMemcpyAsync(dev_y, n->Yp, (size_t)rows * n->O * sizeof(float), cudaMemcpyDeviceToDevice, n->stream));
-  CB2_CUDA(cudaStreamSynchronize(n->stream));
-  return 0;
+  return mlp_status(n);
 }
 
 // mean squared error of rows x (normalised features) against t, and its
@@ -476,7 +608,7 @@ int cb2_mlp_loss_grad(cb2_mlp *n, const float *dev_x, const float *dev_t, long l
   if (!n || !dev_x || !dev_t || rows <= 0) return CB2_ERR_ARG;
   double l = 0.0;
   int rc = mlp_backward(n, dev_x, dev_t, (size_t)rows, &l);
-  if (rc) return rc;
+  if (rc || (rc = mlp_status(n))) return rc;
   if (loss) *loss = l;
   if (host_grad) CB2_CUDA(cudaMemcpy(host_grad, n->grad, n->np * sizeof(float), cudaMemcpyDeviceToHost));
   return 0;
@@ -494,8 +626,7 @@ int cb2_mlp_adam_step(cb2_mlp *n, float lr, float beta1, float beta2, float eps)
 
 int cb2_mlp_sync(cb2_mlp *n) {
   if (!n) return CB2_ERR_ARG;
-  CB2_CUDA(cudaStreamSynchronize(n->stream));
-  return 0;
+  return mlp_status(n);
 }
 
 // dst's 13 state fields (velocity, vorticity, magnetic field, current,

@@ -50,31 +50,41 @@ __device__ inline size_t four_at(const LegArgs &a, int th, int k, int c) {
   return (((size_t)th * a.nr + k) * a.ncomp + c) * a.NS;
 }
 
+// Each lane handles two Gauss nodes of the south half, i and i + 32, so the
+// spectral coefficients it reads from shared memory (three 16-byte loads
+// per radial level and degree) feed twice the FMAs.
 template <int BWD_KT>
 __global__ void __launch_bounds__(32 * MAXG)
 k_leg_bwd_f64(LegArgs a, double *four) {
-  const int m = blockIdx.z, k0 = blockIdx.y * BWD_KT, i0 = blockIdx.x * 32;
+  const int m = blockIdx.z, k0 = blockIdx.y * BWD_KT, i0 = blockIdx.x * 64;
   const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
   const int ngrp = a.nvec + a.nscal;
   const int nl = a.L + 1 - m;
-  const int i = i0 + lane;
-  const bool act = (g < ngrp) && (i < a.nh);
+  const int ia = i0 + lane, ib = i0 + 32 + lane;
+  const bool act = g < ngrp && ia < a.nh;
   const bool isvec = g < a.nvec;
-  __shared__ double sc[MAXG][BWD_LC][6][BWD_KT];
-  double acc[BWD_KT][6][2];
+  // [group][degree][radial level][S+ S- D+ D- T+ T-]
+  __shared__ __align__(16) double sc[MAXG][BWD_LC][BWD_KT][6];
+  double acc[2][BWD_KT][6][2];
 #pragma unroll
-  for (int q = 0; q < BWD_KT; q++)
+  for (int h = 0; h < 2; h++)
 #pragma unroll
-    for (int c = 0; c < 6; c++) acc[q][c][0] = acc[q][c][1] = 0.0;
-  const double am = (i < a.nh) ? (double)m * a.asin_t[i] : 0.0;
+    for (int q = 0; q < BWD_KT; q++)
+#pragma unroll
+      for (int c = 0; c < 6; c++) acc[h][q][c][0] = acc[h][q][c][1] = 0.0;
+  // node b may lie beyond the half grid: it reads node a's tables and is
+  // not stored
+  const int ibr = (ib < a.nh) ? ib : ia;
+  const double ama = (ia < a.nh) ? (double)m * a.asin_t[ia] : 0.0;
+  const double amb = (ia < a.nh) ? (double)m * a.asin_t[ibr] : 0.0;
   const size_t po = a.poff[m];
   for (int lc0 = 0; lc0 < nl; lc0 += BWD_LC) {
     __syncthreads();
-    int tot = ngrp * BWD_LC * 6 * BWD_KT;
+    const int tot = ngrp * BWD_LC * 6 * BWD_KT;
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
       int lc = e % BWD_LC, t = e / BWD_LC;
-      int q = t % BWD_KT; t /= BWD_KT;
-      int v = t % 6, gg = t / 6;
+      int v = t % 6; t /= 6;
+      int q = t % BWD_KT, gg = t / BWD_KT;
       int l = m + lc0 + lc, k = k0 + q;
       int s = v & 1, comp = v >> 1;  // v: 0 S+ 1 S- 2 D+ 3 D- 4 T+ 5 T-
       double val = 0.0;
@@ -88,7 +98,7 @@ k_leg_bwd_f64(LegArgs a, double *four) {
           val = a.f[(size_t)a.slot[gg] * a.fs + (size_t)k * a.jmax + jj];
         }
       }
-      sc[gg][lc][v][q] = val;
+      sc[gg][lc][q][v] = val;
     }
     __syncthreads();
     if (act) {
@@ -97,32 +107,30 @@ k_leg_bwd_f64(LegArgs a, double *four) {
       // two keeps the parity index a compile-time constant (registers)
       auto body = [&](int lc, auto SPc) {
         constexpr int sp = decltype(SPc)::value, sd = sp ^ 1;
-        int t = lc0 + lc;
-        double P = a.Plt[po + (size_t)t * a.nh + i];
-        double dP = a.dPlt[po + (size_t)t * a.nh + i];
-        double mP = P * am;
-        if (isvec) {
+        const int t = lc0 + lc;
+        const double *Pr = a.Plt + po + (size_t)t * a.nh, *dPr = a.dPlt + po + (size_t)t * a.nh;
+        const double Pa = Pr[ia], dPa = dPr[ia], Pb = Pr[ibr], dPb = dPr[ibr];
+        const double mPa = Pa * ama, mPb = Pb * amb;
 #pragma unroll
-          for (int q = 0; q < BWD_KT; q++) {
-            double Sp = sc[g][lc][0][q], Sm = sc[g][lc][1][q];
-            double Dp = sc[g][lc][2][q], Dm = sc[g][lc][3][q];
-            double Tp = sc[g][lc][4][q], Tm = sc[g][lc][5][q];
-            acc[q][0][sp] += Sp * P;        // v_r(+m)
-            acc[q][1][sp] += Sm * P;        // v_r(-m)
-            acc[q][2][sd] += Dp * dP;       // v_theta(+m)
-            acc[q][2][sp] += Tm * mP;
-            acc[q][3][sd] += Dm * dP;       // v_theta(-m)
-            acc[q][3][sp] -= Tp * mP;
-            acc[q][4][sd] -= Tp * dP;       // v_phi(+m)
-            acc[q][4][sp] += Dm * mP;
-            acc[q][5][sd] -= Tm * dP;       // v_phi(-m)
-            acc[q][5][sp] -= Dp * mP;
-          }
-        } else {
-#pragma unroll
-          for (int q = 0; q < BWD_KT; q++) {
-            acc[q][0][sp] += sc[g][lc][0][q] * P;
-            acc[q][1][sp] += sc[g][lc][1][q] * P;
+        for (int q = 0; q < BWD_KT; q++) {
+          const double2 *row = reinterpret_cast<const double2 *>(&sc[g][lc][q][0]);
+          const double2 S = row[0];
+          if (isvec) {
+            const double2 D = row[1], T = row[2];
+            // S = (S+, S-), D = (D+, D-), T = (T+, T-)
+            acc[0][q][0][sp] += S.x * Pa;          acc[1][q][0][sp] += S.x * Pb;   // v_r(+m)
+            acc[0][q][1][sp] += S.y * Pa;          acc[1][q][1][sp] += S.y * Pb;   // v_r(-m)
+            acc[0][q][2][sd] += D.x * dPa;         acc[1][q][2][sd] += D.x * dPb;  // v_theta(+m)
+            acc[0][q][2][sp] += T.y * mPa;         acc[1][q][2][sp] += T.y * mPb;
+            acc[0][q][3][sd] += D.y * dPa;         acc[1][q][3][sd] += D.y * dPb;  // v_theta(-m)
+            acc[0][q][3][sp] -= T.x * mPa;         acc[1][q][3][sp] -= T.x * mPb;
+            acc[0][q][4][sd] -= T.x * dPa;         acc[1][q][4][sd] -= T.x * dPb;  // v_phi(+m)
+            acc[0][q][4][sp] += D.y * mPa;         acc[1][q][4][sp] += D.y * mPb;
+            acc[0][q][5][sd] -= T.y * dPa;         acc[1][q][5][sd] -= T.y * dPb;  // v_phi(-m)
+            acc[0][q][5][sp] -= D.x * mPa;         acc[1][q][5][sp] -= D.x * mPb;
+          } else {
+            acc[0][q][0][sp] += S.x * Pa;          acc[1][q][0][sp] += S.x * Pb;
+            acc[0][q][1][sp] += S.y * Pa;          acc[1][q][1][sp] += S.y * Pb;
           }
         }
       };
@@ -135,54 +143,66 @@ k_leg_bwd_f64(LegArgs a, double *four) {
     }
   }
   if (!act) return;
-  const int ii = a.nth - 1 - i;
   const int ncw = isvec ? 3 : 1;
   const int c0 = a.cbase + (isvec ? 3 * g : 3 * a.nvec + (g - a.nvec));
 #pragma unroll
-  for (int q = 0; q < BWD_KT; q++) {
-    int k = k0 + q;
-    if (k >= a.nr) break;
-    for (int c = 0; c < ncw; c++) {
-      double e0 = acc[q][2 * c][0], o0 = acc[q][2 * c][1];
-      double e1 = acc[q][2 * c + 1][0], o1 = acc[q][2 * c + 1][1];
-      double2 south = make_double2(e0 + o0, m == 0 ? 0.0 : e1 + o1);
-      double2 north = make_double2(e0 - o0, m == 0 ? 0.0 : e1 - o1);
-      *reinterpret_cast<double2 *>(four + four_at(a, i, k, c0 + c) + 2 * m) = south;
-      if (ii != i)
-        *reinterpret_cast<double2 *>(four + four_at(a, ii, k, c0 + c) + 2 * m) = north;
+  for (int h = 0; h < 2; h++) {
+    const int i = h ? ib : ia;
+    if (i >= a.nh) break;
+    const int ii = a.nth - 1 - i;
+#pragma unroll
+    for (int q = 0; q < BWD_KT; q++) {
+      int k = k0 + q;
+      if (k >= a.nr) break;
+      for (int c = 0; c < ncw; c++) {
+        double e0 = acc[h][q][2 * c][0], o0 = acc[h][q][2 * c][1];
+        double e1 = acc[h][q][2 * c + 1][0], o1 = acc[h][q][2 * c + 1][1];
+        double2 south = make_double2(e0 + o0, m == 0 ? 0.0 : e1 + o1);
+        double2 north = make_double2(e0 - o0, m == 0 ? 0.0 : e1 - o1);
+        *reinterpret_cast<double2 *>(four + four_at(a, i, k, c0 + c) + 2 * m) = south;
+        if (ii != i)
+          *reinterpret_cast<double2 *>(four + four_at(a, ii, k, c0 + c) + 2 * m) = north;
+      }
     }
   }
 }
 
-// forward: block = (order m, radial tile); lane = degree l - m.  NV vectors
-// and NSC scalars starting at component c0 of the Fourier buffer (which
-// holds a.ncomp components) and at group g0 of a.slot.
+// forward: block = (order m, radial tile); thread = two consecutive
+// degrees l - m = t (even) and t + 1, one of each reflection parity, so the
+// symmetric and antisymmetric sums of a grid value, adjacent in shared
+// memory, are read as one 16-byte pair and both used.  NV vectors and NSC
+// scalars starting at component c0 of the Fourier buffer (which holds
+// a.ncomp components) and at group g0 of a.slot.
 template <int NV, int NSC, int FWD_KT>
 __global__ void __launch_bounds__(256)
 k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
   const int m = blockIdx.z, k0 = blockIdx.y * FWD_KT;
   const int nl = a.L + 1 - m;
   constexpr int C = 3 * NV + NSC;
-  extern __shared__ double hs[];   // [pair][k][c][s][sym/anti]
+  extern __shared__ __align__(16) double hs[];   // [pair][k][c][s][sym/anti]
   auto H = [&](int ip, int q, int c, int s, int par) -> double & {
     return hs[((((size_t)ip * FWD_KT + q) * C + c) * 2 + s) * 2 + par];
   };
+  auto H2 = [&](int ip, int q, int c, int s) -> double2 {   // (sym, anti) of (c, s)
+    return *reinterpret_cast<const double2 *>(&hs[((((size_t)ip * FWD_KT + q) * C + c) * 2 + s) * 2]);
+  };
   const size_t po = a.poff[m];
-  for (int lt0 = 0; lt0 < nl; lt0 += blockDim.x) {
-    const int t = lt0 + threadIdx.x;   // l - m
-    const bool act = t < nl;
-    const int par = t & 1;
-    double accv[NV > 0 ? NV : 1][FWD_KT][6];
-    double accs[NSC > 0 ? NSC : 1][FWD_KT][2];
+  for (int lt0 = 0; lt0 < nl; lt0 += 2 * blockDim.x) {
+    const int t = lt0 + 2 * threadIdx.x;   // even: parity 0; t + 1: parity 1
+    const bool act0 = t < nl, act1 = t + 1 < nl;
+    double accv[2][NV > 0 ? NV : 1][FWD_KT][6];
+    double accs[2][NSC > 0 ? NSC : 1][FWD_KT][2];
 #pragma unroll
-    for (int q = 0; q < FWD_KT; q++) {
+    for (int d = 0; d < 2; d++)
 #pragma unroll
-      for (int v = 0; v < (NV > 0 ? NV : 1); v++)
+      for (int q = 0; q < FWD_KT; q++) {
 #pragma unroll
-        for (int c = 0; c < 6; c++) accv[v][q][c] = 0.0;
+        for (int v = 0; v < (NV > 0 ? NV : 1); v++)
 #pragma unroll
-      for (int v = 0; v < (NSC > 0 ? NSC : 1); v++) accs[v][q][0] = accs[v][q][1] = 0.0;
-    }
+          for (int c = 0; c < 6; c++) accv[d][v][q][c] = 0.0;
+#pragma unroll
+        for (int v = 0; v < (NSC > 0 ? NSC : 1); v++) accs[d][v][q][0] = accs[d][v][q][1] = 0.0;
+      }
     for (int ib = 0; ib < a.nh; ib += FWD_TC) {
       __syncthreads();
       int npair = min(FWD_TC, a.nh - ib);
@@ -201,43 +221,56 @@ k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
         H(ip, q, c, s, 1) = fa - fb;
       }
       __syncthreads();
-      if (act) {
+      if (act0) {
+        const int t1 = act1 ? t + 1 : t;   // a missing odd degree reads the even one's table, not stored
         for (int ip = 0; ip < npair; ip++) {
-          int i = ib + ip;
-          double P = a.Ptl[po + (size_t)i * nl + t];
-          double dP = a.dPtl[po + (size_t)i * nl + t];
-          double pg = P * (double)m * a.asin_t[i];   // P m / sin(theta), order +m
+          const int i = ib + ip;
+          const double *Pr = a.Ptl + po + (size_t)i * nl, *dPr = a.dPtl + po + (size_t)i * nl;
+          const double P0 = Pr[t], dP0 = dPr[t], P1 = Pr[t1], dP1 = dPr[t1];
+          const double am = (double)m * a.asin_t[i];
+          const double pg0 = P0 * am, pg1 = P1 * am;   // P m / sin(theta), order +m
 #pragma unroll
           for (int v = 0; v < NV; v++) {
 #pragma unroll
             for (int q = 0; q < FWD_KT; q++) {
-              // order +m: ip slot 0, in slot 1 ; order -m: ip slot 1, in slot 0
-              double r0 = H(ip, q, 3 * v, 0, par), r1 = H(ip, q, 3 * v, 1, par);
-              double tp0 = H(ip, q, 3 * v + 1, 0, par ^ 1), tp1 = H(ip, q, 3 * v + 1, 1, par ^ 1);
-              double tn0 = H(ip, q, 3 * v + 1, 0, par), tn1 = H(ip, q, 3 * v + 1, 1, par);
-              double pp0 = H(ip, q, 3 * v + 2, 0, par ^ 1), pp1 = H(ip, q, 3 * v + 2, 1, par ^ 1);
-              double pn0 = H(ip, q, 3 * v + 2, 0, par), pn1 = H(ip, q, 3 * v + 2, 1, par);
-              accv[v][q][0] += r0 * P;
-              accv[v][q][1] += r1 * P;
-              accv[v][q][2] += tp0 * dP - pn1 * pg;
-              accv[v][q][3] += tp1 * dP + pn0 * pg;
-              accv[v][q][4] -= tn1 * pg + pp0 * dP;
-              accv[v][q][5] -= -tn0 * pg + pp1 * dP;
+              const double2 R0 = H2(ip, q, 3 * v, 0), R1 = H2(ip, q, 3 * v, 1);
+              const double2 T0 = H2(ip, q, 3 * v + 1, 0), T1 = H2(ip, q, 3 * v + 1, 1);
+              const double2 F0 = H2(ip, q, 3 * v + 2, 0), F1 = H2(ip, q, 3 * v + 2, 1);
+              // parity 0 (degree t): r, tn, pn from the symmetric sums,
+              // tp, pp from the antisymmetric ones; parity 1 the converse.
+              // Order +m: s slot 0, order -m: s slot 1.
+              accv[0][v][q][0] += R0.x * P0;
+              accv[0][v][q][1] += R1.x * P0;
+              accv[0][v][q][2] += T0.y * dP0 - F1.x * pg0;
+              accv[0][v][q][3] += T1.y * dP0 + F0.x * pg0;
+              accv[0][v][q][4] -= T1.x * pg0 + F0.y * dP0;
+              accv[0][v][q][5] -= -T0.x * pg0 + F1.y * dP0;
+              accv[1][v][q][0] += R0.y * P1;
+              accv[1][v][q][1] += R1.y * P1;
+              accv[1][v][q][2] += T0.x * dP1 - F1.y * pg1;
+              accv[1][v][q][3] += T1.x * dP1 + F0.y * pg1;
+              accv[1][v][q][4] -= T1.y * pg1 + F0.x * dP1;
+              accv[1][v][q][5] -= -T0.y * pg1 + F1.x * dP1;
             }
           }
 #pragma unroll
           for (int sc = 0; sc < NSC; sc++) {
 #pragma unroll
             for (int q = 0; q < FWD_KT; q++) {
-              accs[sc][q][0] += H(ip, q, 3 * NV + sc, 0, par) * P;
-              accs[sc][q][1] += H(ip, q, 3 * NV + sc, 1, par) * P;
+              const double2 S0 = H2(ip, q, 3 * NV + sc, 0), S1 = H2(ip, q, 3 * NV + sc, 1);
+              accs[0][sc][q][0] += S0.x * P0;
+              accs[0][sc][q][1] += S1.x * P0;
+              accs[1][sc][q][0] += S0.y * P1;
+              accs[1][sc][q][1] += S1.y * P1;
             }
           }
         }
       }
     }
-    if (act) {
-      int l = m + t;
+#pragma unroll
+    for (int d = 0; d < 2; d++) {
+      if (!(d ? act1 : act0)) continue;
+      int l = m + t + d;
       for (int s = 0; s < (m == 0 ? 1 : 2); s++) {
         int jj = jj_of(a, l, m, s);
         double g7 = a.g7[jj], g6 = a.g6[jj];
@@ -250,13 +283,13 @@ k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
 #pragma unroll
           for (int v = 0; v < NV; v++) {
             double *f0 = a.f + (size_t)a.slot[g0 + v] * a.fs;
-            f0[at] = accv[v][q][0 + s] * g7 * r * r;
-            f0[a.fs + at] = accv[v][q][2 + s] * g7 * r;
-            f0[2 * a.fs + at] = accv[v][q][4 + s] * g7 * r;
+            f0[at] = accv[d][v][q][0 + s] * g7 * r * r;
+            f0[a.fs + at] = accv[d][v][q][2 + s] * g7 * r;
+            f0[2 * a.fs + at] = accv[d][v][q][4 + s] * g7 * r;
           }
 #pragma unroll
           for (int sc = 0; sc < NSC; sc++)
-            a.f[(size_t)a.slot[g0 + NV + sc] * a.fs + at] = accs[sc][q][s] * g6;
+            a.f[(size_t)a.slot[g0 + NV + sc] * a.fs + at] = accs[d][sc][q][s] * g6;
         }
       }
     }
@@ -287,11 +320,12 @@ void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four) {
     b.nscal = nb - b.nvec;
     b.cbase = comp;
     for (int q = 0; q < nb; q++) b.slot[q] = slots[g + q];
+    // tuning value 2: two radial levels per block, 4: four
     if (c.tune[TUNE_BWD_KT] == 2) {
-      dim3 grid(cdiv(c.nh, 32), cdiv(c.nr, 2), c.L + 1);
+      dim3 grid(cdiv(c.nh, 64), cdiv(c.nr, 2), c.L + 1);
       k_leg_bwd_f64<2><<<grid, 32 * nb, 0, c.stream>>>(b, four);
     } else {
-      dim3 grid(cdiv(c.nh, 32), cdiv(c.nr, 4), c.L + 1);
+      dim3 grid(cdiv(c.nh, 64), cdiv(c.nr, 4), c.L + 1);
       k_leg_bwd_f64<4><<<grid, 32 * nb, 0, c.stream>>>(b, four);
     }
     comp += 3 * b.nvec + b.nscal;
@@ -301,7 +335,7 @@ void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four) {
 
 template <int NV, int NSC, int KT>
 static void launch_fwd_kt(Ctx &c, const LegArgs &a, const double *four, int c0) {
-  int nthr = 32 * cdiv(std::min(c.L + 1, 256), 32);
+  int nthr = 32 * cdiv(cdiv(std::min(c.L + 1, 512), 2), 32);   // two degrees per thread
   size_t sm = (size_t)FWD_TC * KT * (3 * NV + NSC) * 2 * 2 * sizeof(double);
   dim3 grid(1, cdiv(c.nr, KT), c.L + 1);
   k_leg_fwd_f64<NV, NSC, KT><<<grid, nthr, sm, c.stream>>>(a, four, c0, 0);
@@ -312,7 +346,6 @@ static void launch_fwd(Ctx &c, LegArgs a, const double *four, int c0, const int 
   for (int q = 0; q < NV + NSC; q++) a.slot[q] = slots[q];
   switch (c.tune[TUNE_FWD_KT]) {
     case 1: launch_fwd_kt<NV, NSC, 1>(c, a, four, c0); break;
-    case 4: launch_fwd_kt<NV, NSC, 4>(c, a, four, c0); break;
     default: launch_fwd_kt<NV, NSC, 2>(c, a, four, c0); break;
   }
 }

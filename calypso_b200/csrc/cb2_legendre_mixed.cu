@@ -57,116 +57,14 @@
 #include <vector>
 
 #include "cb2_internal.cuh"
+#include "cb2_tc.cuh"
 
 namespace cb2 {
 
 namespace {
 
 constexpr int TM = 128;          // GEMM rows per tile (= TMEM lanes)
-constexpr unsigned long long kWaitNs = 200ull * 1000 * 1000;   // 200 ms per wait
-
-__device__ inline uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ inline unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ inline void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ inline void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-
-// wait for the phase with the given parity to complete; false after
-// budget_ns (0: one try).  The pipelines' waits take the context's budget;
-// the drains after an abort (copies and MMAs still in flight) take kWaitNs.
-__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned long long budget_ns = kWaitNs) {
-  const uint32_t addr = smem_u32(bar);
-  unsigned long long t0 = 0;
-  for (uint32_t it = 0;; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (budget_ns == 0) return false;
-    if (it == 64) t0 = globaltimer();
-    if (it > 64) {
-      if (globaltimer() - t0 > budget_ns) return false;
-      __nanosleep(32);
-    }
-  }
-}
-
-// L2 policies: the B tables are re-read by every CTA of an order (keep
-// them), the raw operand rows are read once (let them go first)
-__device__ inline uint64_t policy_evict_last() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-__device__ inline uint64_t policy_evict_first() {
-  uint64_t p;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-  return p;
-}
-
-__device__ inline void tma_load_2d_hint(void *dst, const CUtensorMap *tm, uint64_t *bar, int c0, int c1,
-                                        uint64_t policy) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
-      " [%0], [%1, {%3, %4}], [%2], %5;"
-      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(tm)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "l"(policy)
-      : "memory");
-}
-
-
-// instruction descriptor: D f32, A and B f16, both K-major, M x N
-__device__ inline uint32_t idesc_f16_f32(int M, int N) {
-  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ inline void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-      ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc));
-}
-
-__device__ inline void mma_commit(uint64_t *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ inline void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ inline void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ inline void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// two 32-column loads (columns ta.. and tb..) behind one wait
-__device__ inline void tmem_ld32x2(uint32_t ta, uint32_t tb, float va[32], float vb[32]) {
-  uint32_t r[64];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%64];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%65];\n\t"
-      "tcgen05.wait::ld.sync.aligned;"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
-      : "r"(ta), "r"(tb)
-      : "memory");
-#pragma unroll
-  for (int i = 0; i < 32; i++) { va[i] = __uint_as_float(r[i]); vb[i] = __uint_as_float(r[32 + i]); }
-}
+using namespace tc;
 
 // largest scaled magnitude: 2^13 <= mx s < 2^14 (fp16 holds up to 65504)
 constexpr int kScaleExp = 14;
@@ -182,22 +80,6 @@ __host__ __device__ inline float pow2_scale(double mx) {
   return ldexpf(1.0f, sh);
 }
 
-// tcgen05.ld 16x256b, two loads behind one wait: thread t receives columns
-// 2 (t & 3) and 2 (t & 3) + 1 of lanes (t >> 2) and (t >> 2) + 8 of the 16
-// lanes addressed (va[0..1]: lane t >> 2, va[2..3]: lane (t >> 2) + 8)
-__device__ inline void tmem_ld_16x256b_pair(uint32_t ta, uint32_t tb, float va[4], float vb[4]) {
-  uint32_t r[8];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.16x256b.x1.b32 {%0,%1,%2,%3}, [%8];\n\t"
-      "tcgen05.ld.sync.aligned.16x256b.x1.b32 {%4,%5,%6,%7}, [%9];\n\t"
-      "tcgen05.wait::ld.sync.aligned;"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-      : "r"(ta), "r"(tb)
-      : "memory");
-#pragma unroll
-  for (int i = 0; i < 4; i++) { va[i] = __uint_as_float(r[i]); vb[i] = __uint_as_float(r[4 + i]); }
-}
-
 // x0, x1 -> fp16 hi and lo pairs (x = hi + lo to 22 bits), x0 in the low
 // half; the paired conversions run on the full-rate pipes
 __device__ inline void split_pair(float x0, float x1, uint32_t &hi, uint32_t &lo) {
@@ -208,8 +90,17 @@ __device__ inline void split_pair(float x0, float x1, uint32_t &hi, uint32_t &lo
   lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
-__device__ inline unsigned char *smem_base_1024(unsigned char *raw) {
-  return (unsigned char *)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
+// the same with hi on a fixed grid: hi = x rounded to a multiple of 16 (x
+// scaled below 2^14, so hi is an fp16 number of at most 11 bits), lo = the
+// remainder (|lo| <= 8, 11 bits of it kept, 2^-23 of the row maximum).  Every
+// product hi*hi' is then a multiple of 256 below 2^28, and an FP32
+// accumulator holds their sums exactly while they stay below 2^32.
+__device__ inline void split_pair_q(float x0, float x1, uint32_t &hi, uint32_t &lo) {
+  const float h0 = rintf(x0 * 0.0625f) * 16.0f, h1 = rintf(x1 * 0.0625f) * 16.0f;
+  const __half2 h = __floats2half2_rn(h0, h1);
+  const __half2 l = __floats2half2_rn(x0 - h0, x1 - h1);
+  hi = *reinterpret_cast<const uint32_t *>(&h);
+  lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
 // ---------------------------------------------------------------------------
@@ -245,20 +136,6 @@ struct FwdArgs {
   unsigned long long wait_ns;   // budget of each pipeline wait (Ctx::pipe_wait_ns)
   int split;             // 1: hi*hi' and the cross terms in separate accumulators
 };
-
-// shared-memory descriptor, K-major, 64-byte swizzle (8-row groups 512 bytes apart)
-__device__ inline uint64_t smem_desc_sw64(const void *p) {
-  uint64_t d = (uint64_t)((smem_u32(p) & 0x3FFFF) >> 4);
-  d |= (uint64_t)1 << 16;
-  d |= (uint64_t)(512 >> 4) << 32;
-  d |= (uint64_t)1 << 46;
-  d |= (uint64_t)4 << 61;                 // 64-byte swizzle
-  return d;
-}
-
-__device__ inline uint32_t sw64_chunk(int row, int c) {
-  return (uint32_t)row * 64u + ((uint32_t)(c ^ ((row >> 1) & 3)) << 4);
-}
 
 // Forward stages: both parities come from one raw tile (the symmetric and
 // the antisymmetric fold), so a K block has two raw halves (south + north,
@@ -346,10 +223,6 @@ __device__ inline float fwd_row_scale(const FwdArgs &a, const FwdTile &q, int ro
     else mx = fmaxf(Mf[a.sP + row], Mf[a.sP + row - q4 + 3 - q4]);
   }
   return pow2_scale(mx);
-}
-
-__device__ inline void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 template <typename Bars>
@@ -478,8 +351,9 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             const uint64_t dah = smem_desc_sw64(at + (2 * p) * FA_BYTES), dal = smem_desc_sw64(at + (2 * p + 1) * FA_BYTES);
             const uint64_t dbh = smem_desc_sw64(bb + (2 * p) * B_BYTES), dbl = smem_desc_sw64(bb + (2 * p + 1) * B_BYTES);
             const uint32_t acc = accb + (p ? acc1 : 0u);
-            // the cross terms are 2^-11 of hi*hi': in their own accumulator
-            // they add no rounding to the large one
+            // split: hi*hi' in its own accumulator (for the theta/phi gemm
+            // on the fixed grid, summed exactly), the cross terms and there
+            // lo*lo' (2^-11 and 2^-22 of it) in the second
             const uint32_t accx = a.split ? acc + 2 * acc1 : acc;
 #pragma unroll
             for (int ks = 0; ks < FKB / 16; ks++) {
@@ -488,6 +362,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
               mma_f16(acc, dah + o, dbh + o, idesc, first);
               mma_f16(accx, dah + o, dbl + o, idesc, a.split ? first : 1u);
               mma_f16(accx, dal + o, dbh + o, idesc, 1u);
+              if (a.split && q.g) mma_f16(accx, dal + o, dbl + o, idesc, 1u);
             }
           }
           mma_commit(&sb->abempty[s]);
@@ -555,7 +430,8 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             uint32_t hh[4], ll[4];
 #pragma unroll
             for (int e = 0; e < 8; e += 2) {
-              split_pair(x2[p][c * 8 + e], x2[p][c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
+              if (a.split && q.g) split_pair_q(x2[p][c * 8 + e], x2[p][c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
+              else split_pair(x2[p][c * 8 + e], x2[p][c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
             }
             const uint32_t off = sw64_chunk(r, 2 * h + c);
             *reinterpret_cast<uint4 *>(ahi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
@@ -1191,6 +1067,12 @@ __device__ inline void split_store(__half *hi, __half *lo, size_t at, double v, 
   hi[at] = h;
   lo[at] = __float2half_rn((float)(x - (double)__half2float(h)));
 }
+// hi on a fixed grid (a multiple of q = 16 or 8), as split_pair_q does
+__device__ inline void split_store_q(__half *hi, __half *lo, size_t at, double v, float s, double q) {
+  const double x = v * (double)s, h = rint(x / q) * q;
+  hi[at] = __float2half_rn((float)h);
+  lo[at] = __float2half_rn((float)(x - h));
+}
 
 // backward B[theta][K]: one thread per (m, south node i).  Column groups per
 // m: P0, P1 (P_l^m, l - m even / odd), D0 = {dP of odd l-m | mP of even l-m},
@@ -1231,9 +1113,19 @@ __global__ void k_build_bwd_b(int L, int nh, int nhp, const size_t *poff, const 
 // forward B[l][theta] (P) and B[l][dP theta | mP theta] (DM): one thread per (m, degree)
 __global__ void k_build_fwd_b(int L, int nh, int nhp, int NFmax, const size_t *poff, const double *Plt,
                               const double *dPlt, const double *asin_t, const int *roff, const int *nlp,
-                              float *bunscale, __half *php, __half *plp, __half *dhp, __half *dlp) {
+                              float *bunscale, __half *php, __half *plp, __half *dhp, __half *dlp, int quant) {
   const int m = blockIdx.y, t = blockIdx.x * blockDim.x + threadIdx.x;
   if (m > L) return;
+  // quantised (theta/phi tables only): on the grid of 16, the A operand's,
+  // so the products hi*hi' are multiples of 256 below 2^28 and sum exactly
+  // below 2^32.  The P tables keep the floating split: a fixed grid bounds
+  // the error by the column maximum, and a row dominated by one smooth
+  // component (a scalar's mean) would leave its small high-degree outputs to
+  // that bound.
+  auto put = [&](__half *hi, __half *lo, size_t at, double v, float s, double q) {
+    if (quant && q > 0.0) split_store_q(hi, lo, at, v, s, q);
+    else split_store(hi, lo, at, v, s);
+  };
   const size_t po = poff[m];
   for (int p = 0; p < 2; p++) {
     if (t >= nlp[m * 2 + p]) continue;
@@ -1250,9 +1142,9 @@ __global__ void k_build_fwd_b(int L, int nh, int nhp, int NFmax, const size_t *p
     bunscale[((size_t)(L + 1) * 2 + m * 2 + p) * NFmax + t] = 1.0f / sd;          // gemm DM
     for (int i = 0; i < nh; i++) {
       const double P = Plt[po + (size_t)(l - m) * nh + i];
-      split_store(php, plp, row * nhp + i, P, sp);
-      split_store(dhp, dlp, row * 2 * nhp + i, dPlt[po + (size_t)(l - m) * nh + i], sd);
-      split_store(dhp, dlp, row * 2 * nhp + nhp + i, P * (double)m * asin_t[i], sd);
+      put(php, plp, row * nhp + i, P, sp, 0.0);
+      put(dhp, dlp, row * 2 * nhp + i, dPlt[po + (size_t)(l - m) * nh + i], sd, 16.0);
+      put(dhp, dlp, row * 2 * nhp + nhp + i, P * (double)m * asin_t[i], sd, 16.0);
     }
   }
 }
@@ -1432,7 +1324,7 @@ int mixed_setup(Ctx &c) {
   CB2_CUDA(cudaGetLastError());
   k_build_fwd_b<<<dim3(cdiv(t->NFmax, 64), L + 1), 64, 0, c.stream>>>(
       L, nh, t->nhp, t->NFmax, c.d_poff, c.d_Plt, c.d_dPlt, c.d_asin, t->bf_roff, t->bf_nl, t->bf_unscale,
-      t->bfp_hi, t->bfp_lo, t->bfd_hi, t->bfd_lo);
+      t->bfp_hi, t->bfp_lo, t->bfd_hi, t->bfd_lo, t->split_fwd);
   CB2_CUDA(cudaGetLastError());
   CB2_CUDA(cudaStreamSynchronize(c.stream));
   if ((rc = make_map64(&t->tm_bb_hi, t->bb_hi, t->Kb_all, t->nhp, t->nhp)) ||
