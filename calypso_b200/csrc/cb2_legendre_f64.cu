@@ -24,8 +24,8 @@
 
 namespace cb2 {
 
-constexpr int BWD_LC = 32;  // degrees per staged chunk
-constexpr int FWD_TC = 16;  // Gauss node pairs per staged chunk
+constexpr int BWD_LC = 16;  // degrees per staged chunk
+constexpr int FWD_TC = 8;   // Gauss node pairs per staged chunk
 // radial levels per block (BWD_KT backward, FWD_KT forward) are template
 // parameters; the autotuner picks them per shell shape (cb2_autotune)
 constexpr int MAXG = 6;     // field groups (vectors + scalars) per launch
@@ -63,8 +63,11 @@ k_leg_bwd_f64(LegArgs a, double *four) {
   const int ia = i0 + lane, ib = i0 + 32 + lane;
   const bool act = g < ngrp && ia < a.nh;
   const bool isvec = g < a.nvec;
-  // [group][degree][radial level][S+ S- D+ D- T+ T-]
+  // [group][degree][radial level][S+ S- D+ D- T+ T-], and P_l^m, dP_l^m of
+  // the chunk's degrees at the block's 64 nodes: every global load of a
+  // chunk is issued before the FMAs start
   __shared__ __align__(16) double sc[MAXG][BWD_LC][BWD_KT][6];
+  __shared__ double Ps[BWD_LC][64], dPs[BWD_LC][64];
   double acc[2][BWD_KT][6][2];
 #pragma unroll
   for (int h = 0; h < 2; h++)
@@ -100,6 +103,12 @@ k_leg_bwd_f64(LegArgs a, double *four) {
       }
       sc[gg][lc][q][v] = val;
     }
+    for (int e = threadIdx.x; e < BWD_LC * 64; e += blockDim.x) {
+      const int lc = e >> 6, ii = i0 + (e & 63), t = lc0 + lc;
+      const bool in = t < nl && ii < a.nh;
+      Ps[lc][e & 63] = in ? a.Plt[po + (size_t)t * a.nh + ii] : 0.0;
+      dPs[lc][e & 63] = in ? a.dPlt[po + (size_t)t * a.nh + ii] : 0.0;
+    }
     __syncthreads();
     if (act) {
       int lcn = min(BWD_LC, nl - lc0);
@@ -107,9 +116,7 @@ k_leg_bwd_f64(LegArgs a, double *four) {
       // two keeps the parity index a compile-time constant (registers)
       auto body = [&](int lc, auto SPc) {
         constexpr int sp = decltype(SPc)::value, sd = sp ^ 1;
-        const int t = lc0 + lc;
-        const double *Pr = a.Plt + po + (size_t)t * a.nh, *dPr = a.dPlt + po + (size_t)t * a.nh;
-        const double Pa = Pr[ia], dPa = dPr[ia], Pb = Pr[ibr], dPb = dPr[ibr];
+        const double Pa = Ps[lc][lane], dPa = dPs[lc][lane], Pb = Ps[lc][32 + lane], dPb = dPs[lc][32 + lane];
         const double mPa = Pa * ama, mPb = Pb * amb;
 #pragma unroll
         for (int q = 0; q < BWD_KT; q++) {
@@ -179,7 +186,7 @@ k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
   const int m = blockIdx.z, k0 = blockIdx.y * FWD_KT;
   const int nl = a.L + 1 - m;
   constexpr int C = 3 * NV + NSC;
-  extern __shared__ __align__(16) double hs[];   // [pair][k][c][s][sym/anti]
+  extern __shared__ __align__(16) double hs[];   // [pair][k][c][s][sym/anti], then P and dP [pair][t]
   auto H = [&](int ip, int q, int c, int s, int par) -> double & {
     return hs[((((size_t)ip * FWD_KT + q) * C + c) * 2 + s) * 2 + par];
   };
@@ -187,6 +194,7 @@ k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
     return *reinterpret_cast<const double2 *>(&hs[((((size_t)ip * FWD_KT + q) * C + c) * 2 + s) * 2]);
   };
   const size_t po = a.poff[m];
+  double *PT = hs + (size_t)FWD_TC * FWD_KT * C * 4, *dPT = PT + (size_t)FWD_TC * nl;
   for (int lt0 = 0; lt0 < nl; lt0 += 2 * blockDim.x) {
     const int t = lt0 + 2 * threadIdx.x;   // even: parity 0; t + 1: parity 1
     const bool act0 = t < nl, act1 = t + 1 < nl;
@@ -220,12 +228,18 @@ k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
         H(ip, q, c, s, 0) = fa + fb;
         H(ip, q, c, s, 1) = fa - fb;
       }
+      // P_l^m, dP_l^m of the chunk's nodes: all global loads in flight together
+      for (int e = threadIdx.x; e < npair * nl; e += blockDim.x) {
+        const int ip = e / nl, tt = e - ip * nl;
+        PT[ip * nl + tt] = a.Ptl[po + (size_t)(ib + ip) * nl + tt];
+        dPT[ip * nl + tt] = a.dPtl[po + (size_t)(ib + ip) * nl + tt];
+      }
       __syncthreads();
       if (act0) {
         const int t1 = act1 ? t + 1 : t;   // a missing odd degree reads the even one's table, not stored
         for (int ip = 0; ip < npair; ip++) {
           const int i = ib + ip;
-          const double *Pr = a.Ptl + po + (size_t)i * nl, *dPr = a.dPtl + po + (size_t)i * nl;
+          const double *Pr = PT + ip * nl, *dPr = dPT + ip * nl;
           const double P0 = Pr[t], dP0 = dPr[t], P1 = Pr[t1], dP1 = dPr[t1];
           const double am = (double)m * a.asin_t[i];
           const double pg0 = P0 * am, pg1 = P1 * am;   // P m / sin(theta), order +m
@@ -336,7 +350,12 @@ void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four) {
 template <int NV, int NSC, int KT>
 static void launch_fwd_kt(Ctx &c, const LegArgs &a, const double *four, int c0) {
   int nthr = 32 * cdiv(cdiv(std::min(c.L + 1, 512), 2), 32);   // two degrees per thread
-  size_t sm = (size_t)FWD_TC * KT * (3 * NV + NSC) * 2 * 2 * sizeof(double);
+  size_t sm = ((size_t)FWD_TC * KT * (3 * NV + NSC) * 2 * 2 + 2 * (size_t)FWD_TC * (c.L + 1)) * sizeof(double);
+  static size_t attr = 0;   // the kernel's dynamic shared-memory limit, raised once per size
+  if (sm > 48 * 1024 && sm > attr) {
+    cudaFuncSetAttribute(k_leg_fwd_f64<NV, NSC, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    attr = sm;
+  }
   dim3 grid(1, cdiv(c.nr, KT), c.L + 1);
   k_leg_fwd_f64<NV, NSC, KT><<<grid, nthr, sm, c.stream>>>(a, four, c0, 0);
 }

@@ -162,7 +162,7 @@ constexpr int FW_PROD_WARP = (FW_CONV + FW_EPI) / 32, FW_MMA_WARP = FW_PROD_WARP
 // epilogue staging of one warp: 16 rows x 16 degrees (+1 pad) floats, then
 // the row metadata (destination offset, scale, factor select) of its 16 rows
 constexpr int FW_STG_P = 17;
-constexpr uint32_t FW_STG_BYTES = ((16 * FW_STG_P * 4 + 16 * 8 + 16 * 8 + 16 * 4) + 15) & ~15u;
+constexpr uint32_t FW_STG_BYTES = ((16 * FW_STG_P * 8 + 16 * 8 + 16 * 8 + 16 * 4) + 15) & ~15u;
 
 struct FwdWsLayout {
   uint32_t raw, ab, stg, w, bar, total;   // byte offsets from the aligned base
@@ -351,9 +351,9 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             const uint64_t dah = smem_desc_sw64(at + (2 * p) * FA_BYTES), dal = smem_desc_sw64(at + (2 * p + 1) * FA_BYTES);
             const uint64_t dbh = smem_desc_sw64(bb + (2 * p) * B_BYTES), dbl = smem_desc_sw64(bb + (2 * p + 1) * B_BYTES);
             const uint32_t acc = accb + (p ? acc1 : 0u);
-            // split: hi*hi' in its own accumulator (for the theta/phi gemm
-            // on the fixed grid, summed exactly), the cross terms and there
-            // lo*lo' (2^-11 and 2^-22 of it) in the second
+            // split: hi*hi' (on the fixed grid, summed exactly) in its own
+            // accumulator, the cross terms and lo*lo' (2^-11 and 2^-22 of
+            // it) in the second
             const uint32_t accx = a.split ? acc + 2 * acc1 : acc;
 #pragma unroll
             for (int ks = 0; ks < FKB / 16; ks++) {
@@ -362,7 +362,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
               mma_f16(acc, dah + o, dbh + o, idesc, first);
               mma_f16(accx, dah + o, dbl + o, idesc, a.split ? first : 1u);
               mma_f16(accx, dal + o, dbh + o, idesc, 1u);
-              if (a.split && q.g) mma_f16(accx, dal + o, dbl + o, idesc, 1u);
+              if (a.split) mma_f16(accx, dal + o, dbl + o, idesc, 1u);
             }
           }
           mma_commit(&sb->abempty[s]);
@@ -430,7 +430,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             uint32_t hh[4], ll[4];
 #pragma unroll
             for (int e = 0; e < 8; e += 2) {
-              if (a.split && q.g) split_pair_q(x2[p][c * 8 + e], x2[p][c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
+              if (a.split) split_pair_q(x2[p][c * 8 + e], x2[p][c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
               else split_pair(x2[p][c * 8 + e], x2[p][c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
             }
             const uint32_t off = sw64_chunk(r, 2 * h + c);
@@ -460,8 +460,8 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
     const int ew = warp - FW_CONV / 32, qd = ew & 3, hf = ew >> 2;
     const int t0 = lane & 3, t1 = lane >> 2, lc = lane & 15, lr = lane >> 4;
     unsigned char *wst = base + lay.stg + ew * FW_STG_BYTES;
-    float *stg = reinterpret_cast<float *>(wst);                                   // [16][FW_STG_P]
-    long long *moff = reinterpret_cast<long long *>(wst + 16 * FW_STG_P * 4);     // [16]
+    double *stg = reinterpret_cast<double *>(wst);                                 // [16][FW_STG_P]
+    long long *moff = reinterpret_cast<long long *>(wst + 16 * FW_STG_P * 8);     // [16]
     double *mc = reinterpret_cast<double *>(moff + 16);                           // [16]
     int *mg = reinterpret_cast<int *>(mc + 16);                                   // [16]
     double *__restrict__ fout = a.f;
@@ -519,13 +519,17 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
       float nbu;
       fetch(0, n7, n6, nbu);
       for (int g = 0; g < ng; g++) {
-        float p0[4], p1[4];
-        tmem_ld_16x256b_pair(tl + (uint32_t)(g * 8), tl + acc1 + (uint32_t)(g * 8), p0, p1);
+        float f0[4], f1[4];
+        tmem_ld_16x256b_pair(tl + (uint32_t)(g * 8), tl + acc1 + (uint32_t)(g * 8), f0, f1);
+        // the two accumulators are added in float64: no rounding of the sum
+        double p0[4], p1[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) { p0[j] = (double)f0[j]; p1[j] = (double)f1[j]; }
         if (a.split) {
           float x0[4], x1[4];
           tmem_ld_16x256b_pair(tl + 2 * acc1 + (uint32_t)(g * 8), tl + 3 * acc1 + (uint32_t)(g * 8), x0, x1);
 #pragma unroll
-          for (int j = 0; j < 4; j++) { p0[j] += x0[j]; p1[j] += x1[j]; }
+          for (int j = 0; j < 4; j++) { p0[j] += (double)x0[j]; p1[j] += (double)x1[j]; }
         }
         if (g == ng - 1) {
           tc_fence_before();
@@ -536,7 +540,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
         fetch(g + 1, n7, n6, nbu);
 #pragma unroll
         for (int j = 0; j < 2; j++) {
-          float *srow = stg + (t1 + 8 * j) * FW_STG_P + 4 * t0;
+          double *srow = stg + (t1 + 8 * j) * FW_STG_P + 4 * t0;
           srow[0] = p0[2 * j]; srow[1] = p1[2 * j]; srow[2] = p0[2 * j + 1]; srow[3] = p1[2 * j + 1];
         }
         __syncwarp();
@@ -546,7 +550,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
           for (int u = 0; u < 8; u++) {
             const int rr = u + 8 * lr;
             const long long o = moff[rr];
-            if (o >= 0) fout[o + lm] = (double)stg[rr * FW_STG_P + lc] * mc[rr] * (mg[rr] ? c6 : c7);
+            if (o >= 0) fout[o + lm] = stg[rr * FW_STG_P + lc] * mc[rr] * (mg[rr] ? c6 : c7);
           }
         }
         __syncwarp();
@@ -1116,12 +1120,16 @@ __global__ void k_build_fwd_b(int L, int nh, int nhp, int NFmax, const size_t *p
                               float *bunscale, __half *php, __half *plp, __half *dhp, __half *dlp, int quant) {
   const int m = blockIdx.y, t = blockIdx.x * blockDim.x + threadIdx.x;
   if (m > L) return;
-  // quantised (theta/phi tables only): on the grid of 16, the A operand's,
-  // so the products hi*hi' are multiples of 256 below 2^28 and sum exactly
-  // below 2^32.  The P tables keep the floating split: a fixed grid bounds
-  // the error by the column maximum, and a row dominated by one smooth
-  // component (a scalar's mean) would leave its small high-degree outputs to
-  // that bound.
+  // quantised: the theta/phi tables on the grid of 16, the A operand's, so
+  // the products hi*hi' are multiples of 256 below 2^28 and sum exactly
+  // below 2^32; the P tables on the grid of 8 (products multiples of 128,
+  // exact below 2^31), which halves their representation error.  A fixed
+  // grid bounds the error by the column maximum rather than by each value:
+  // in a row dominated by one smooth component (a scalar's mean) the small
+  // high-degree outputs carry that bound (measured: 6e-6 relative on the
+  // seeded scalars of the L255 round trip, against 1e-6 with the floating
+  // split, whose FP32 accumulation leaves the L255 step's toroidal magnetic
+  // energy 5 % above the 1e-6 target).
   auto put = [&](__half *hi, __half *lo, size_t at, double v, float s, double q) {
     if (quant && q > 0.0) split_store_q(hi, lo, at, v, s, q);
     else split_store(hi, lo, at, v, s);
@@ -1142,7 +1150,7 @@ __global__ void k_build_fwd_b(int L, int nh, int nhp, int NFmax, const size_t *p
     bunscale[((size_t)(L + 1) * 2 + m * 2 + p) * NFmax + t] = 1.0f / sd;          // gemm DM
     for (int i = 0; i < nh; i++) {
       const double P = Plt[po + (size_t)(l - m) * nh + i];
-      put(php, plp, row * nhp + i, P, sp, 0.0);
+      put(php, plp, row * nhp + i, P, sp, 8.0);
       put(dhp, dlp, row * 2 * nhp + i, dPlt[po + (size_t)(l - m) * nh + i], sd, 16.0);
       put(dhp, dlp, row * 2 * nhp + nhp + i, P * (double)m * asin_t[i], sd, 16.0);
     }
@@ -1268,10 +1276,11 @@ int mixed_setup(Ctx &c) {
   t->nfb = ((t->NFmax + t->boxr - 1) / t->boxr) * t->boxr;
   // one accumulator set = both parities, each as a hi*hi' and a cross-term
   // accumulator where they fit in TMEM (L <= 255); two sets when they fit.
-  // Measured on the L255/Nr129 state: the separate cross-term accumulators
-  // halve the error of the forward transform (1.1e-6 -> 5.5e-7 relative on
-  // the theta/phi outputs, 3e-7 -> 6e-8 on the radial ones), because the
-  // large accumulator is rounded after 1 MMA in 3 instead of every MMA.
+  // Measured on the L255/Nr129 state (relative error of the forward
+  // transform, theta/phi outputs / radial outputs): one accumulator 1.1e-6 /
+  // 3e-7; separate cross-term accumulators 5.5e-7 / 6e-8 (the large one is
+  // rounded after one MMA in three); with hi*hi' on the fixed grid, summed
+  // exactly, 2.0e-7 / 4e-8.
   t->split_fwd = (4 * t->NFmax <= 512) ? 1 : 0;
   const int per_set = (t->split_fwd ? 4 : 2) * t->NFmax;
   t->nacc_fwd = (2 * per_set <= 512) ? 2 : 1;
