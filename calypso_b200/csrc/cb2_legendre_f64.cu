@@ -30,6 +30,17 @@ constexpr int FWD_TC = 8;   // Gauss node pairs per staged chunk
 // parameters; the autotuner picks them per shell shape (cb2_autotune)
 constexpr int MAXG = 6;     // field groups (vectors + scalars) per launch
 
+// 8-byte asynchronous copy global -> shared; n = 0 fills the 8 bytes with
+// zeros and reads nothing
+__device__ inline void cp_async8(double *dst, const double *src, int n) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(n)
+               : "memory");
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// every group but the newest has landed
+__device__ inline void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 struct LegArgs {
   int L, nr, nth, nh, jmax, NS, nvec, nscal, ncomp, cbase;
   int slot[MAXG];           // first rj slot of each group of this launch
@@ -63,11 +74,12 @@ k_leg_bwd_f64(LegArgs a, double *four) {
   const int ia = i0 + lane, ib = i0 + 32 + lane;
   const bool act = g < ngrp && ia < a.nh;
   const bool isvec = g < a.nvec;
-  // [group][degree][radial level][S+ S- D+ D- T+ T-], and P_l^m, dP_l^m of
-  // the chunk's degrees at the block's 64 nodes: every global load of a
-  // chunk is issued before the FMAs start
-  __shared__ __align__(16) double sc[MAXG][BWD_LC][BWD_KT][6];
-  __shared__ double Ps[BWD_LC][64], dPs[BWD_LC][64];
+  // two shared-memory buffers, each [group][degree][radial level][S+ S- D+
+  // D- T+ T-] and P_l^m, dP_l^m of the chunk's degrees at the block's 64
+  // nodes: the copies of the next chunk (cp.async) are in flight while the
+  // FMAs of this one run
+  constexpr int SCN = MAXG * BWD_LC * BWD_KT * 6, PN = BWD_LC * 64, BUF = SCN + 2 * PN;
+  extern __shared__ __align__(16) double smb[];
   double acc[2][BWD_KT][6][2];
 #pragma unroll
   for (int h = 0; h < 2; h++)
@@ -81,35 +93,62 @@ k_leg_bwd_f64(LegArgs a, double *four) {
   const double ama = (ia < a.nh) ? (double)m * a.asin_t[ia] : 0.0;
   const double amb = (ia < a.nh) ? (double)m * a.asin_t[ibr] : 0.0;
   const size_t po = a.poff[m];
-  for (int lc0 = 0; lc0 < nl; lc0 += BWD_LC) {
-    __syncthreads();
-    const int tot = ngrp * BWD_LC * 6 * BWD_KT;
+  const int tot = ngrp * BWD_LC * 6 * BWD_KT;
+  // element e of a chunk: degree lc (fastest, coalesced), component v, level q, group gg
+  auto decomp = [&](int e, int &lc, int &v, int &q, int &gg) {
+    lc = e % BWD_LC;
+    int t = e / BWD_LC;
+    v = t % 6; t /= 6;
+    q = t % BWD_KT; gg = t / BWD_KT;
+  };
+  auto issue = [&](int lc0, int b) {
+    double *sc = smb + (size_t)b * BUF, *ps = sc + SCN, *dps = ps + PN;
     for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-      int lc = e % BWD_LC, t = e / BWD_LC;
-      int v = t % 6; t /= 6;
-      int q = t % BWD_KT, gg = t / BWD_KT;
-      int l = m + lc0 + lc, k = k0 + q;
-      int s = v & 1, comp = v >> 1;  // v: 0 S+ 1 S- 2 D+ 3 D- 4 T+ 5 T-
-      double val = 0.0;
-      if (l <= a.L && k < a.nr && !(m == 0 && s == 1)) {
-        int jj = jj_of(a, l, m, s);
-        if (gg < a.nvec) {
-          double x = a.f[(size_t)(a.slot[gg] + comp) * a.fs + (size_t)k * a.jmax + jj];
-          double ar = a.ar1[k];
-          val = (comp == 0) ? x * ar * ar * a.g3rlm[jj] : x * ar;
-        } else if (comp == 0) {
-          val = a.f[(size_t)a.slot[gg] * a.fs + (size_t)k * a.jmax + jj];
-        }
-      }
-      sc[gg][lc][q][v] = val;
+      int lc, v, q, gg;
+      decomp(e, lc, v, q, gg);
+      const int l = m + lc0 + lc, k = k0 + q, s = v & 1, comp = v >> 1;  // v: 0 S+ 1 S- 2 D+ 3 D- 4 T+ 5 T-
+      const double *src = nullptr;
+      if (l <= a.L && k < a.nr && !(m == 0 && s == 1) && (gg < a.nvec || comp == 0))
+        src = a.f + (size_t)(a.slot[gg] + (gg < a.nvec ? comp : 0)) * a.fs + (size_t)k * a.jmax + jj_of(a, l, m, s);
+      cp_async8(sc + ((gg * BWD_LC + lc) * BWD_KT + q) * 6 + v, src ? src : a.f, src ? 8 : 0);
     }
-    for (int e = threadIdx.x; e < BWD_LC * 64; e += blockDim.x) {
+    for (int e = threadIdx.x; e < PN; e += blockDim.x) {
       const int lc = e >> 6, ii = i0 + (e & 63), t = lc0 + lc;
       const bool in = t < nl && ii < a.nh;
-      Ps[lc][e & 63] = in ? a.Plt[po + (size_t)t * a.nh + ii] : 0.0;
-      dPs[lc][e & 63] = in ? a.dPlt[po + (size_t)t * a.nh + ii] : 0.0;
+      const size_t at = in ? po + (size_t)t * a.nh + ii : 0;
+      cp_async8(ps + e, a.Plt + at, in ? 8 : 0);
+      cp_async8(dps + e, a.dPlt + at, in ? 8 : 0);
     }
+    cp_async_commit();
+  };
+  // the radial and degree factors of the vector spectra, applied by the
+  // thread that copied each value once its copies have landed
+  auto convert = [&](int lc0, int b) {
+    double *sc = smb + (size_t)b * BUF;
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      int lc, v, q, gg;
+      decomp(e, lc, v, q, gg);
+      const int l = m + lc0 + lc, k = k0 + q;
+      if (gg < a.nvec && l <= a.L && k < a.nr) {
+        const double ar = a.ar1[k], l3 = (l == 0) ? 0.5 : (double)l * (double)(l + 1);
+        double &x = sc[((gg * BWD_LC + lc) * BWD_KT + q) * 6 + v];
+        x *= ((v >> 1) == 0) ? ar * ar * l3 : ar;
+      }
+    }
+  };
+  const int nch = (nl + BWD_LC - 1) / BWD_LC;
+  issue(0, 0);
+  for (int ch = 0; ch < nch; ch++) {
+    const int lc0 = ch * BWD_LC, b = ch & 1;
+    if (ch + 1 < nch) issue(lc0 + BWD_LC, b ^ 1);
+    else cp_async_commit();
+    cp_async_wait1();
+    convert(lc0, b);
     __syncthreads();
+    const double(*sc)[BWD_LC][BWD_KT][6] =
+        reinterpret_cast<const double(*)[BWD_LC][BWD_KT][6]>(smb + (size_t)b * BUF);
+    const double(*Ps)[64] = reinterpret_cast<const double(*)[64]>(smb + (size_t)b * BUF + SCN);
+    const double(*dPs)[64] = reinterpret_cast<const double(*)[64]>(smb + (size_t)b * BUF + SCN + PN);
     if (act) {
       int lcn = min(BWD_LC, nl - lc0);
       // lc0 is even, so degree t = lc0 + lc has parity lc & 1: unrolling by
@@ -148,6 +187,7 @@ k_leg_bwd_f64(LegArgs a, double *four) {
       }
       if (lc < lcn) body(lc, std::integral_constant<int, 0>());
     }
+    __syncthreads();   // buffer b is refilled by the next iteration's copies
   }
   if (!act) return;
   const int ncw = isvec ? 3 : 1;
@@ -186,15 +226,52 @@ k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
   const int m = blockIdx.z, k0 = blockIdx.y * FWD_KT;
   const int nl = a.L + 1 - m;
   constexpr int C = 3 * NV + NSC;
-  extern __shared__ __align__(16) double hs[];   // [pair][k][c][s][sym/anti], then P and dP [pair][t]
-  auto H = [&](int ip, int q, int c, int s, int par) -> double & {
-    return hs[((((size_t)ip * FWD_KT + q) * C + c) * 2 + s) * 2 + par];
-  };
+  // two buffers, each [pair][k][c][s][sym/anti] and P_l^m, dP_l^m
+  // [pair][degree] of one chunk of node pairs: the copies (cp.async) of the
+  // next chunk are in flight while the FMAs of this one run
+  extern __shared__ __align__(16) double hs0[];
+  const size_t HN = (size_t)FWD_TC * FWD_KT * C * 4, BUF = HN + 2 * (size_t)FWD_TC * nl;
+  double *hs = hs0;
   auto H2 = [&](int ip, int q, int c, int s) -> double2 {   // (sym, anti) of (c, s)
     return *reinterpret_cast<const double2 *>(&hs[((((size_t)ip * FWD_KT + q) * C + c) * 2 + s) * 2]);
   };
   const size_t po = a.poff[m];
-  double *PT = hs + (size_t)FWD_TC * FWD_KT * C * 4, *dPT = PT + (size_t)FWD_TC * nl;
+  const double *PT = nullptr, *dPT = nullptr;
+  // the raw values of pair (ip, q, c, s): this node and its mirror, into
+  // the (sym, anti) slots that convert() fills
+  auto issue = [&](int ib, int b) {
+    double *h = hs0 + b * BUF, *pt = h + HN, *dpt = pt + (size_t)FWD_TC * nl;
+    const int npair = min(FWD_TC, a.nh - ib), tot = npair * FWD_KT * C * 2;
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      int s = e & 1, tt = e >> 1;
+      int c = tt % C; tt /= C;
+      int q = tt % FWD_KT, ip = tt / FWD_KT;
+      int k = k0 + q, i = ib + ip, ii = a.nth - 1 - i;
+      const bool in = k < a.nr && !(m == 0 && s == 1);
+      double *d = h + ((((size_t)ip * FWD_KT + q) * C + c) * 2 + s) * 2;
+      cp_async8(d, in ? four + four_at(a, i, k, c0 + c) + 2 * m + s : four, in ? 8 : 0);
+      cp_async8(d + 1, in ? four + four_at(a, ii, k, c0 + c) + 2 * m + s : four, in ? 8 : 0);
+    }
+    for (int e = threadIdx.x; e < npair * nl; e += blockDim.x) {
+      const int ip = e / nl, tt = e - ip * nl;
+      cp_async8(pt + ip * nl + tt, a.Ptl + po + (size_t)(ib + ip) * nl + tt, 8);
+      cp_async8(dpt + ip * nl + tt, a.dPtl + po + (size_t)(ib + ip) * nl + tt, 8);
+    }
+    cp_async_commit();
+  };
+  auto convert = [&](int ib, int b) {
+    double *h = hs0 + b * BUF;
+    const int npair = min(FWD_TC, a.nh - ib), tot = npair * FWD_KT * C * 2;
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      int tt = e >> 1;
+      tt /= C;
+      const int ip = tt / FWD_KT, i = ib + ip, ii = a.nth - 1 - i;
+      double *d = h + (size_t)e * 2;
+      const double fa = d[0] * a.wgt[i], fb = d[1] * a.wgt[ii];
+      d[0] = fa + fb;
+      d[1] = fa - fb;
+    }
+  };
   for (int lt0 = 0; lt0 < nl; lt0 += 2 * blockDim.x) {
     const int t = lt0 + 2 * threadIdx.x;   // even: parity 0; t + 1: parity 1
     const bool act0 = t < nl, act1 = t + 1 < nl;
@@ -211,30 +288,18 @@ k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
 #pragma unroll
         for (int v = 0; v < (NSC > 0 ? NSC : 1); v++) accs[d][v][q][0] = accs[d][v][q][1] = 0.0;
       }
-    for (int ib = 0; ib < a.nh; ib += FWD_TC) {
+    __syncthreads();   // the buffers of the previous degree block are free
+    issue(0, 0);
+    for (int ib = 0, b = 0; ib < a.nh; ib += FWD_TC, b ^= 1) {
+      const int npair = min(FWD_TC, a.nh - ib);
+      if (ib + FWD_TC < a.nh) issue(ib + FWD_TC, b ^ 1);
+      else cp_async_commit();
+      cp_async_wait1();
+      convert(ib, b);
       __syncthreads();
-      int npair = min(FWD_TC, a.nh - ib);
-      int tot = npair * FWD_KT * C * 2;
-      for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-        int s = e & 1, tt = e >> 1;
-        int c = tt % C; tt /= C;
-        int q = tt % FWD_KT, ip = tt / FWD_KT;
-        int k = k0 + q, i = ib + ip, ii = a.nth - 1 - i;
-        double fa = 0.0, fb = 0.0;
-        if (k < a.nr && !(m == 0 && s == 1)) {
-          fa = four[four_at(a, i, k, c0 + c) + 2 * m + s] * a.wgt[i];
-          fb = four[four_at(a, ii, k, c0 + c) + 2 * m + s] * a.wgt[ii];
-        }
-        H(ip, q, c, s, 0) = fa + fb;
-        H(ip, q, c, s, 1) = fa - fb;
-      }
-      // P_l^m, dP_l^m of the chunk's nodes: all global loads in flight together
-      for (int e = threadIdx.x; e < npair * nl; e += blockDim.x) {
-        const int ip = e / nl, tt = e - ip * nl;
-        PT[ip * nl + tt] = a.Ptl[po + (size_t)(ib + ip) * nl + tt];
-        dPT[ip * nl + tt] = a.dPtl[po + (size_t)(ib + ip) * nl + tt];
-      }
-      __syncthreads();
+      hs = hs0 + b * BUF;
+      PT = hs + HN;
+      dPT = PT + (size_t)FWD_TC * nl;
       if (act0) {
         const int t1 = act1 ? t + 1 : t;   // a missing odd degree reads the even one's table, not stored
         for (int ip = 0; ip < npair; ip++) {
@@ -280,6 +345,7 @@ k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
           }
         }
       }
+      __syncthreads();   // buffer b is refilled by the next chunk's copies
     }
 #pragma unroll
     for (int d = 0; d < 2; d++) {
@@ -323,6 +389,18 @@ static LegArgs leg_args(Ctx &c, int nvec, int nscal, const int *slots) {
   return a;
 }
 
+template <int KT>
+static void launch_bwd(Ctx &c, const LegArgs &b, double *four, int nb) {
+  const size_t sm = 2 * ((size_t)MAXG * BWD_LC * KT * 6 + 2 * BWD_LC * 64) * sizeof(double);
+  static bool attr = false;   // the kernel's dynamic shared-memory limit, raised once
+  if (!attr) {
+    cudaFuncSetAttribute(k_leg_bwd_f64<KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    attr = true;
+  }
+  dim3 grid(cdiv(c.nh, 64), cdiv(c.nr, KT), c.L + 1);
+  k_leg_bwd_f64<KT><<<grid, 32 * nb, sm, c.stream>>>(b, four);
+}
+
 void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four) {
   LegArgs a = leg_args(c, nvec, nscal, slots);
   // launches of at most MAXG groups: vectors first, then scalars
@@ -335,13 +413,8 @@ void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four) {
     b.cbase = comp;
     for (int q = 0; q < nb; q++) b.slot[q] = slots[g + q];
     // tuning value 2: two radial levels per block, 4: four
-    if (c.tune[TUNE_BWD_KT] == 2) {
-      dim3 grid(cdiv(c.nh, 64), cdiv(c.nr, 2), c.L + 1);
-      k_leg_bwd_f64<2><<<grid, 32 * nb, 0, c.stream>>>(b, four);
-    } else {
-      dim3 grid(cdiv(c.nh, 64), cdiv(c.nr, 4), c.L + 1);
-      k_leg_bwd_f64<4><<<grid, 32 * nb, 0, c.stream>>>(b, four);
-    }
+    if (c.tune[TUNE_BWD_KT] == 2) launch_bwd<2>(c, b, four, nb);
+    else launch_bwd<4>(c, b, four, nb);
     comp += 3 * b.nvec + b.nscal;
     g += nb;
   }
@@ -350,7 +423,7 @@ void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four) {
 template <int NV, int NSC, int KT>
 static void launch_fwd_kt(Ctx &c, const LegArgs &a, const double *four, int c0) {
   int nthr = 32 * cdiv(cdiv(std::min(c.L + 1, 512), 2), 32);   // two degrees per thread
-  size_t sm = ((size_t)FWD_TC * KT * (3 * NV + NSC) * 2 * 2 + 2 * (size_t)FWD_TC * (c.L + 1)) * sizeof(double);
+  size_t sm = 2 * ((size_t)FWD_TC * KT * (3 * NV + NSC) * 2 * 2 + 2 * (size_t)FWD_TC * (c.L + 1)) * sizeof(double);
   static size_t attr = 0;   // the kernel's dynamic shared-memory limit, raised once per size
   if (sm > 48 * 1024 && sm > attr) {
     cudaFuncSetAttribute(k_leg_fwd_f64<NV, NSC, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
