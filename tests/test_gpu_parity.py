@@ -1,14 +1,15 @@
 """GPU parity of the float64 plain path against the CPU oracle and the
 reference's golden energies.  Tolerances: Gauss nodes / P_l^m 1e-13, SHT
 1e-12 relative L2, time-stepped fields 1e-10 relative L2, golden energies
-1e-9 (the reference's own regression tolerance)."""
+1e-9 (the reference's own regression tolerance); config 0's full 2000-step
+run: energies and spectra 1e-9 (float64) and 1e-6 (mixed path)."""
 import json
 import os
 
 import numpy as np
 import pytest
 
-from calypso_b200 import PREC_FP64, SphMHD, configs
+from calypso_b200 import PREC_FP64, PREC_MIXED, SphMHD, configs
 from calypso_b200.sph_mhd import CURRENT, MAGNE, TEMP, VELO, VORT
 
 pytestmark = pytest.mark.gpu
@@ -174,3 +175,29 @@ def test_bench_shell_fp64_matches_oracle(oracle_lib):
     o.step(2)
     _compare_fields(g, o, 1e-10)
     np.testing.assert_allclose(g.energies(), o.energies(), rtol=1e-10)
+
+
+def test_config0_full_run_energies_and_spectra(oracle_lib):
+    """Config 0 as stated: L31, Nr33, 48 x 96, E 1e-3, Ra 100, seeded start,
+    dt 1e-4, 2000 steps, energies and spectra against the oracle.  float64
+    path: energies 1e-9 relative, spectra 1e-9 of each spectrum's total
+    (2000 steps of differently ordered float64 sums); mixed path: energies
+    1e-6, spectra 1e-6 of each spectrum's total."""
+    import os
+    p = configs.small_shell()
+    o = oracle_lib.Oracle(dict(p, nthreads=os.cpu_count() or 1))
+    o.init_fields(2, 5)
+    o.step(2000)
+    eo, so = o.energies(), o.energy_spectra()
+    for prec, tol in ((PREC_FP64, 1e-9), (PREC_MIXED, 1e-6)):
+        g = SphMHD(p, prec)
+        g.init_fields(2, seed=5)
+        g.step(1)
+        g.step(1999, graph=True)
+        eg, sg = g.energies(), g.energy_spectra()
+        g.close()
+        np.testing.assert_allclose(eg, eo, rtol=tol)
+        for kind in ("l", "m", "lm"):
+            for q in range(7):
+                tot = np.abs(so[kind][q]).sum()
+                assert np.abs(sg[kind][q] - so[kind][q]).max() <= tol * tot, (prec, kind, q)
