@@ -18,6 +18,11 @@ Arms
                      oracle; the reference's Fortran build is unavailable in
                      this image), timed on the host cores, rank 0 only.
 
+Extra keys of the default arm (rank 0, one GPU; each can be skipped):
+fp64_plain (config 2 on the FP64 path), sht_roundtrip (config 1, per-field
+errors), ensemble (config 3, 48 shells) and closure (config 4, the network
+trained on filtered L255 runs and applied at L63).
+
 Timing: W untimed warm-up steps, then K steps captured as a CUDA graph and
 timed with CUDA events on the library's stream, bracketed by barriers and
 device synchronisation; the max over ranks is reported.  The model state
@@ -338,6 +343,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-sht", action="store_true", help="skip the SHT round-trip extra key")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-shell ensemble extra key")
+    ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure extra key")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variants")
     ap.add_argument("--compare-steps", type=int, default=500,
                     help="steps of the mixed and FP64 runs whose energies are compared")
@@ -498,6 +505,17 @@ def main():
     if rank == 0 and world == 1 and not args.no_sht:
         sht = sht_roundtrip_extras(local_rank, with_oracle=not args.no_cpu_baseline)
 
+    # config 3 (48-shell ensemble, one graph launch per ensemble step) and
+    # config 4 (closure trained on filtered L255 runs, applied at L63)
+    ens = clo = None
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        from calypso_b200 import ensemble_bench
+        ens = ensemble_bench.run(steps=10, warmup=3, device=local_rank)
+    if rank == 0 and world == 1 and not args.no_closure:
+        from calypso_b200 import closure_experiment
+        clo = closure_experiment.run()
+        clo.pop("loss_per_epoch", None)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
@@ -518,7 +536,7 @@ def main():
                             "graph": True, "tuning": list(tuning),
                             **({"tuning_note": tuning_note} if tuning_note else {})},
             "roofline": roof, "stages_ms": stages, "cpu_baseline": cpu, "e2e": e2e,
-            "fp64_plain": fp64, "sht_roundtrip": sht,
+            "fp64_plain": fp64, "sht_roundtrip": sht, "ensemble": ens, "closure": clo,
             # kernels per step: the Crank-Nicolson stage (one fused kernel, or
             # explicit, implicit 5-band and 3-band, two derived-field kernels);
             # Coriolis; backward Legendre (pack + GEMM when mixed); FFT +

@@ -239,27 +239,32 @@ k_tc_gemm(int M, int N, int NT, int K, const TAT *__restrict__ A, int lda, const
   __syncthreads();
   tc::tc_fence_after();
   if (!*abort && nblk > 0) {
-    // epilogue: warp w holds TMEM lanes 32 w .. 32 w + 31 (tile rows)
-    const int m = m0 + warp * 32 + lane;
+    // epilogue: warp w holds TMEM lanes 32 w .. 32 w + 31 (tile rows), a
+    // thread 64 columns of its row per load; through the warp's 32 x 65
+    // staging (the stage buffers are free now) a store then writes 32
+    // consecutive columns of one row
+    float *stg = reinterpret_cast<float *>(base) + warp * 32 * 65;
     for (int c0 = 0; c0 < NT; c0 += 64) {
       float va[32], vb[32];
       const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
       tc::tmem_ld32x2(ta, ta + 32, va, vb);
-      if (m < M) {
 #pragma unroll
-        for (int j = 0; j < 32; j++) {
-          const int n = n0 + c0 + j;
-          if (c0 + j < NT && n < N) {
+      for (int j = 0; j < 32; j++) { stg[lane * 65 + j] = va[j]; stg[lane * 65 + 32 + j] = vb[j]; }
+      __syncwarp();
+      for (int r = 0; r < 32; r++) {
+        const int m = m0 + warp * 32 + r;
+        if (m >= M) break;
+#pragma unroll
+        for (int hh = 0; hh < 2; hh++) {
+          const int cc = c0 + 32 * hh + lane, n = n0 + cc;
+          if (cc < NT && n < N) {
             float *cp = C + (size_t)m * ldc + n;
-            if (atomic) atomicAdd(cp, va[j]); else *cp = va[j];
-          }
-          const int n2 = n + 32;
-          if (c0 + 32 + j < NT && n2 < N) {
-            float *cp = C + (size_t)m * ldc + n2;
-            if (atomic) atomicAdd(cp, vb[j]); else *cp = vb[j];
+            const float v = stg[r * 65 + 32 * hh + lane];
+            if (atomic) atomicAdd(cp, v); else *cp = v;
           }
         }
       }
+      __syncwarp();
     }
   }
   tc::tc_fence_before();

@@ -16,6 +16,36 @@ from . import configs
 from .sph_mhd import PREC_FP64, PREC_MIXED, Ensemble, SphMHD
 
 
+def run(steps: int = 20, warmup: int = 3, per_shape: int = 16, precision: str = "mixed", device: int = 0) -> dict:
+    prec = PREC_MIXED if precision == "mixed" else PREC_FP64
+    params = configs.ensemble(per_shape)
+    ens = Ensemble(params, prec, device=device, autotune=True)
+    ens.init_fields(2, 1)
+    ens.step(1 + warmup)
+    ms = ens.time_steps(steps)
+    tuning = {f"L{p['ltr']}": s.tuning for p, s in zip(params, ens.shells)}
+    ens.close()
+    # the same shells one after another (each its own captured graph)
+    seq_ms = 0.0
+    for q, p in enumerate(params):
+        g = SphMHD(p, prec, device=device)
+        g.tuning = tuning[f"L{p['ltr']}"]
+        g.init_fields(2, 1 + q)
+        g.step(1)
+        g.step(warmup, graph=True)
+        seq_ms += g.time_steps(steps, graph=True)
+        g.close()
+    n = len(params)
+    return {
+        "workload": f"ensemble_{n}_shells", "precision": precision, "steps": steps,
+        "shell_steps_per_s": n * steps / (ms / 1000.0),
+        "ms_per_ensemble_step": ms / steps,
+        "sequential_shell_steps_per_s": n * steps / (seq_ms / 1000.0),
+        "speedup_over_sequential": seq_ms / ms,
+        "tuning": tuning,
+    }
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=20)
@@ -23,33 +53,7 @@ def main(argv=None):
     ap.add_argument("--per-shape", type=int, default=16)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args(argv)
-    prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
-    params = configs.ensemble(args.per_shape)
-    ens = Ensemble(params, prec, device=0, autotune=True)
-    ens.init_fields(2, 1)
-    ens.step(1 + args.warmup)
-    ms = ens.time_steps(args.steps)
-    tuning = {f"L{p['ltr']}": s.tuning for p, s in zip(params, ens.shells)}
-    ens.close()
-    # the same shells one after another (each its own captured graph)
-    seq_ms = 0.0
-    for q, p in enumerate(params):
-        g = SphMHD(p, prec, device=0)
-        g.tuning = tuning[f"L{p['ltr']}"]
-        g.init_fields(2, 1 + q)
-        g.step(1)
-        g.step(args.warmup, graph=True)
-        seq_ms += g.time_steps(args.steps, graph=True)
-        g.close()
-    n = len(params)
-    print(json.dumps({
-        "workload": f"ensemble_{n}_shells", "precision": args.precision, "steps": args.steps,
-        "shell_steps_per_s": n * args.steps / (ms / 1000.0),
-        "ms_per_ensemble_step": ms / args.steps,
-        "sequential_shell_steps_per_s": n * args.steps / (seq_ms / 1000.0),
-        "speedup_over_sequential": seq_ms / ms,
-        "tuning": tuning,
-    }), flush=True)
+    print(json.dumps(run(args.steps, args.warmup, args.per_shape, args.precision)), flush=True)
 
 
 if __name__ == "__main__":
