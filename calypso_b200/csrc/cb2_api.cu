@@ -121,27 +121,34 @@ static int jj_of(const Ctx &c, int l, int m) {
   return c.h_moff[am] + ((m < 0) ? (c.L + 1 - am) : 0) + (l - am);
 }
 
-static int nonlinear(Ctx &c) {
-  const int bslots[5] = {VELO, VORT, MAGNE, CURRENT, TEMP};
-  const int fslots[4] = {MADV, LOR, VPIND, HFLUX};
+static const int kBwdSlots[5] = {VELO, VORT, MAGNE, CURRENT, TEMP};
+static const int kFwdSlots[4] = {MADV, LOR, VPIND, HFLUX};
+
+// The nonlinear terms in three parts around the mixed path's two
+// tensor-core Legendre GEMMs:
+//   head: Coriolis; mixed: the spectra packed for the backward GEMM
+//   grid: mixed: FFT + grid products, the forward GEMM's row scales
+//   tail: rj operators after the forward transform, closure
+// nonlinear() launches this shell's GEMMs between them; an ensemble
+// launches each GEMM once for all its shells (step_phase).
+static int nl_head(Ctx &c) {
   if (c.timers) cudaEventRecord(c.ev[10], c.stream);
   rj_coriolis(c);
   if (c.timers) cudaEventRecord(c.ev[11], c.stream);
-  if (c.prec == CB2_PREC_FP64) {
-    leg_bwd_f64(c, 4, 1, bslots, (double *)c.d_four);
-    if (c.timers) cudaEventRecord(c.ev[12], c.stream);
-    fft_products<double>(c, (const double *)c.d_four, (double *)c.d_four2);
-    if (c.timers) cudaEventRecord(c.ev[13], c.stream);
-    leg_fwd_f64(c, 4, 0, (const double *)c.d_four2, fslots);
-  } else {
-    const MLayout fin = mlayout(c, c.d_four, 4, 1), fout = mlayout(c, c.d_four2, 4, 0);
-    int rc = leg_bwd_mixed(c, bslots, fin);
-    if (rc) return rc;
-    if (c.timers) cudaEventRecord(c.ev[12], c.stream);
-    const bool maxima = fft_products_m(c, fin, fout, mixed_fwd_pmax(c));
-    if (c.timers) cudaEventRecord(c.ev[13], c.stream);
-    if ((rc = leg_fwd_mixed(c, fout, fslots, maxima))) return rc;
-  }
+  if (c.prec == CB2_PREC_MIXED) return leg_bwd_pack(c, kBwdSlots, mlayout(c, c.d_four, 4, 1));
+  return 0;
+}
+
+static int nl_grid(Ctx &c) {
+  if (c.timers) cudaEventRecord(c.ev[12], c.stream);
+  const MLayout fin = mlayout(c, c.d_four, 4, 1), fout = mlayout(c, c.d_four2, 4, 0);
+  const bool maxima = fft_products_m(c, fin, fout, mixed_fwd_pmax(c));
+  if (c.timers) cudaEventRecord(c.ev[13], c.stream);
+  leg_fwd_rowmax(c, fout, maxima);
+  return 0;
+}
+
+static int nl_tail(Ctx &c) {
   if (c.timers) cudaEventRecord(c.ev[14], c.stream);
   rj_after_transform(c);
   if (c.closure) {
@@ -152,12 +159,30 @@ static int nonlinear(Ctx &c) {
   return 0;
 }
 
+static int nonlinear(Ctx &c) {
+  int rc = nl_head(c);
+  if (rc) return rc;
+  if (c.prec == CB2_PREC_FP64) {
+    leg_bwd_f64(c, 4, 1, kBwdSlots, (double *)c.d_four);
+    if (c.timers) cudaEventRecord(c.ev[12], c.stream);
+    fft_products<double>(c, (const double *)c.d_four, (double *)c.d_four2);
+    if (c.timers) cudaEventRecord(c.ev[13], c.stream);
+    leg_fwd_f64(c, 4, 0, (const double *)c.d_four2, kFwdSlots);
+  } else {
+    if ((rc = leg_bwd_gemm(c, mlayout(c, c.d_four, 4, 1)))) return rc;
+    if ((rc = nl_grid(c))) return rc;
+    if ((rc = leg_fwd_gemm(c, mlayout(c, c.d_four2, 4, 0), kFwdSlots))) return rc;
+  }
+  return nl_tail(c);
+}
+
 static void temp_roundtrip(Ctx &c) {
   if (!c.p.use_ref_temp) return;
   k_temp_roundtrip<<<cdiv(c.nr, 128), 128, 0, c.stream>>>(c.nr, (size_t)c.jmax, c.d_reft0, c.fld(TEMP));
 }
 
-int step_once(Ctx &c) {
+// explicit update and radial solves of a step
+static void solve(Ctx &c) {
   c.istep += 1;
   if (c.timers) cudaEventRecord(c.ev[0], c.stream);
   if (c.cn_ready && c.tune[TUNE_CN] == 1) {
@@ -170,10 +195,34 @@ int step_once(Ctx &c) {
     rj_implicit(c);
   }
   if (c.timers) cudaEventRecord(c.ev[2], c.stream);
+}
+
+int step_once(Ctx &c) {
+  solve(c);
   int rc = nonlinear(c);
   temp_roundtrip(c);
   if (c.timers) cudaEventRecord(c.ev[3], c.stream);
   return rc;
+}
+
+int step_phase(Ctx &c, int phase) {
+  if (c.prec != CB2_PREC_MIXED) {
+    set_error("step_phase: mixed-precision contexts only");
+    return CB2_ERR_ARG;
+  }
+  if (phase == 0) {
+    solve(c);
+    return nl_head(c);
+  }
+  if (phase == 1) return nl_grid(c);
+  const int rc = nl_tail(c);
+  temp_roundtrip(c);
+  if (c.timers) cudaEventRecord(c.ev[3], c.stream);
+  return rc;
+}
+
+int step_gemms_setup(const std::vector<Ctx *> &shells, MultiLeg **out) {
+  return multi_leg_setup(shells, 4, 1, kFwdSlots, 4, 0, out);
 }
 
 static void accumulate_timers(Ctx &c) {

@@ -597,6 +597,23 @@ template <typename T2>
 __host__ __device__ __forceinline__ T2 cadd(T2 a, T2 b) { return T2{a.x + b.x, a.y + b.y}; }
 template <typename T2>
 __host__ __device__ __forceinline__ T2 csub(T2 a, T2 b) { return T2{a.x - b.x, a.y - b.y}; }
+// float32 pairs on sm_100: one packed float32x2 instruction for both lanes,
+// each lane rounded as the scalar add (b (-1) + a is a - b exactly), so the
+// results are those of the scalar forms
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __fadd2_rn(a, b);
+#else
+  return float2{a.x + b.x, a.y + b.y};
+#endif
+}
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+  return __ffma2_rn(b, float2{-1.0f, -1.0f}, a);
+#else
+  return float2{a.x - b.x, a.y - b.y};
+#endif
+}
 template <typename T2>
 __host__ __device__ __forceinline__ T2 cmulf(T2 a, T2 b) {
   return T2{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
@@ -843,8 +860,8 @@ struct F4Plan {
   static constexpr int MP2 = M + 1;            // staging row pitch (complex), slot M stays zero
   static constexpr int WP = R1 + 1;            // twiddle row pitch (complex)
   static constexpr int NTW = 3 * M + R2 * WP;  // tables: [3][M] e^{2 pi i m r/N}, [R2][WP] e^{2 pi i n2 k1/M}
-  // staging: max(14 rows x MP2 complex in, 24 rows x (M | 1) floats out)
-  static constexpr int SF = (28 * MP2 > 24 * (M | 1)) ? 28 * MP2 : 24 * (M | 1);
+  // staging (floats): 14 rows x MP2 complex in, later 12 rows x MP2 complex out
+  static constexpr int SF = 28 * MP2;
   static constexpr size_t smem() { return (size_t)SF * 4 + ((size_t)X + NTW) * 8; }
 };
 
@@ -863,9 +880,8 @@ __global__ void __launch_bounds__(F4_THREADS, 2)
 k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, ProdCoef pc,
                   float *__restrict__ pmax, const float *__restrict__ wgt) {
   using P = F4Plan<R1, R2>;
-  constexpr int M = P::M, N = P::N, TP = P::TP, TG = P::TG, MP2 = P::MP2, WP = P::WP, MPO = M | 1;
+  constexpr int M = P::M, N = P::N, TP = P::TP, TG = P::TG, MP2 = P::MP2, WP = P::WP;
   extern __shared__ __align__(16) unsigned char smraw[];
-  float *Sf = reinterpret_cast<float *>(smraw);                    // staging
   float2 *S2 = reinterpret_cast<float2 *>(smraw);                  // [14][MP2] (a_m, b_m), row 13 zero
   float2 *X = reinterpret_cast<float2 *>(smraw + (size_t)P::SF * 4);   // transposes / grid rows / F_r
   float2 *TW3 = X + P::X;                                          // [3][M]
@@ -873,21 +889,36 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
   const int th = blockIdx.x / fin.nr, k = blockIdx.x % fin.nr;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = F4_THREADS / 32;
   const int grp = tid >> 4, lt = tid & 15;
-  for (int e = tid; e < P::NTW; e += F4_THREADS) TW3[e] = tables[e];
   for (int e = tid; e < 14; e += F4_THREADS) S2[e * MP2 + M] = float2{0.0f, 0.0f};
   for (int e = tid; e < M; e += F4_THREADS) S2[13 * MP2 + e] = float2{0.0f, 0.0f};
-  // input: one warp per order m, lane j < 26 copies element j of the 10 + 16
-  // run; asynchronous copies, so every load of the CTA is in flight at once
+  // input and tables by asynchronous 8-byte copies, all in flight at once.
+  // At one (theta, k) an order m has 13 (cos, sin) pairs: a run of 5 in the
+  // P block and one of 8 in the D block; half-warp h of warp w copies the
+  // orders 2 (w + nwarp i) + h, lane j < 13 of the half pair j into the
+  // staging row of its component
+  for (int e = tid; e < P::NTW; e += F4_THREADS) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(TW3 + e);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(tables + e) : "memory");
+  }
   {
-    int off = 0;
-    if (lane < 26) { int c, sg; m_comp_of_in(lane, c, sg); off = c * 2 * MP2 + sg; }
-    const float *src = (lane < 10) ? fin.P + (size_t)th * fin.sP() + (size_t)k * 10 + lane
-                                   : fin.D + (size_t)th * fin.sD() + (size_t)k * 16 + (lane - 10);
-    const size_t mst = (size_t)fin.nth * ((lane < 10) ? fin.sP() : fin.sD());
-    if (lane < 26)
-      for (int m = warp; m < M; m += nwarp) {
-        const uint32_t d = (uint32_t)__cvta_generic_to_shared(Sf + off + 2 * m);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src + m * mst) : "memory");
+    const int j = lane & 15, hw = lane >> 4;
+    int c = 0;
+    const float *src = fin.P;
+    size_t mst = 0;
+    if (j < 5) {
+      c = (j < 4) ? 3 * j : 12;
+      src = fin.P + (size_t)th * fin.sP() + (size_t)k * 10 + 2 * j;
+      mst = (size_t)fin.nth * fin.sP();
+    } else if (j < 13) {
+      const int jd = j - 5;
+      c = 3 * (jd >> 1) + 1 + (jd & 1);
+      src = fin.D + (size_t)th * fin.sD() + (size_t)k * 16 + 2 * jd;
+      mst = (size_t)fin.nth * fin.sD();
+    }
+    if (j < 13)
+      for (int m = 2 * warp + hw; m < M; m += 2 * nwarp) {
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(S2 + c * MP2 + m);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src + m * mst) : "memory");
       }
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
   }
@@ -914,7 +945,9 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
 #pragma unroll
     for (int k1 = 0; k1 < R1; k1++) T[k1 * TP + lt] = (k1 == 0) ? v[0] : cmulf(v[k1], TWM[lt * WP + k1]);
   }
-  __syncthreads();
+  // the transpose block T of a group is written and read by the group's own
+  // 16 threads, half of one warp
+  __syncwarp();
   // ---- backward, step 2: row k1 = lt -> grid samples j = 3 (k1 + R1 k2) + r
   float2 w[R2];
   if (grp < 21 && lt < R1) {
@@ -964,7 +997,7 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
 #pragma unroll
     for (int k1 = 0; k1 < R1; k1++) T[k1 * TP + lt] = v[k1];
   }
-  __syncthreads();
+  __syncwarp();   // the group's own transpose block, as in the backward steps
   // ---- forward, step 2: row k1 = lt -> F_r[k1 + R1 k2]
   if (grp < 18 && lt < R1) {
     const float2 *T = X + grp * TG + lt * TP;
@@ -980,7 +1013,9 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
   }
   __syncthreads();
   // ---- combine the residues: Z[m], Z[N - m] -> (a_m, b_m) of both
-  // components of each pair, into the output staging rows [c * 2 + s][M | 1]
+  // components of each pair, into the output staging rows [c][MP2] of
+  // (a_m, b_m) pairs
+  float2 *O2 = S2;
   {
     const float an = 1.0f / (float)N;
     for (int idx = tid; idx < 6 * M; idx += F4_THREADS) {
@@ -989,25 +1024,37 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
       const float2 t1 = TW3[M + m], t2 = TW3[2 * M + m];
       const float2 zk = cadd(F[m], cadd(cmulc(F[M + m], t1), cmulc(F[2 * M + m], t2)));
       const float2 zn = cadd(F[mm], cadd(cmulf(F[M + mm], t1), cmulf(F[2 * M + mm], t2)));
-      float *o0 = Sf + (2 * p) * 2 * MPO, *o1 = Sf + (2 * p + 1) * 2 * MPO;
+      float2 *o0 = O2 + (2 * p) * MP2, *o1 = o0 + MP2;
       if (m == 0) {
-        o0[0] = an * zk.x; o0[MPO] = 0.0f; o1[0] = an * zk.y; o1[MPO] = 0.0f;
+        o0[0] = float2{an * zk.x, 0.0f}; o1[0] = float2{an * zk.y, 0.0f};
       } else {
-        o0[m] = an * (zk.x + zn.x); o0[MPO + m] = -an * (zk.y - zn.y);
-        o1[m] = an * (zk.y + zn.y); o1[MPO + m] = an * (zk.x - zn.x);
+        o0[m] = float2{an * (zk.x + zn.x), -an * (zk.y - zn.y)};
+        o1[m] = float2{an * (zk.y + zn.y), an * (zk.x - zn.x)};
       }
     }
   }
   __syncthreads();
-  // output: one warp per m, lane j < 24 writes element j of the 8 + 16 run
+  // output: 12 (cos, sin) pairs per order, a run of 4 in the P block and one
+  // of 8 in the D block; half-warp h of warp w writes the orders
+  // 2 (w + nwarp i) + h, lane j < 12 of the half pair j (8-byte stores)
   {
-    int cs = 0;
-    if (lane < 24) { int c, sg; m_comp_of_out(lane, c, sg); cs = c * 2 + sg; }
-    float *dst = (lane < 8) ? fout.P + (size_t)th * fout.sP() + (size_t)k * 8 + lane
-                            : fout.D + (size_t)th * fout.sD() + (size_t)k * 16 + (lane - 8);
-    const size_t mst = (size_t)fout.nth * ((lane < 8) ? fout.sP() : fout.sD());
-    if (lane < 24)
-      for (int m = warp; m < M; m += nwarp) dst[m * mst] = Sf[cs * MPO + m];
+    const int j = lane & 15, hw = lane >> 4;
+    int c = 0;
+    float *dst = fout.P;
+    size_t mst = 0;
+    if (j < 4) {
+      c = 3 * j;
+      dst = fout.P + (size_t)th * fout.sP() + (size_t)k * 8 + 2 * j;
+      mst = (size_t)fout.nth * fout.sP();
+    } else if (j < 12) {
+      const int jd = j - 4;
+      c = 3 * (jd >> 1) + 1 + (jd & 1);
+      dst = fout.D + (size_t)th * fout.sD() + (size_t)k * 16 + 2 * jd;
+      mst = (size_t)fout.nth * fout.sD();
+    }
+    if (j < 12)
+      for (int m = 2 * warp + hw; m < M; m += 2 * nwarp)
+        *reinterpret_cast<float2 *>(dst + m * mst) = O2[c * MP2 + m];
   }
   if (pmax) {
     constexpr int MB = M / 16;
@@ -1018,10 +1065,10 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
       const int j = t % 24, mb = t / 24;
       int c, sg;
       m_comp_of_out(j, c, sg);
-      const float *row = Sf + (c * 2 + sg) * MPO + mb * 16;
+      const float *row = reinterpret_cast<const float *>(O2 + c * MP2 + mb * 16) + sg;
       float mx = 0.0f;
 #pragma unroll
-      for (int u = 0; u < 16; u++) mx = fmaxf(mx, fabsf(row[u]));
+      for (int u = 0; u < 16; u++) mx = fmaxf(mx, fabsf(row[2 * u]));
       const size_t e = (j < 8) ? (size_t)k * 8 + j : fout.sP() + (size_t)k * 16 + (j - 8);
       pm[(size_t)mb * E + e] = mx * wt;
     }

@@ -244,6 +244,22 @@ int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out);
 // rowmax_ready: the FFT kernel that wrote `in` also wrote the partial row
 // maxima of mixed_fwd_pmax (fft_products_m returned true)
 int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots, bool rowmax_ready = false);
+// the two halves of each: the kernels before the GEMM (spectra packing; row
+// scales) and the tensor-core GEMM itself
+int leg_bwd_pack(Ctx &c, const int *slots, const MLayout &out);
+int leg_bwd_gemm(Ctx &c, const MLayout &out);
+void leg_fwd_rowmax(Ctx &c, const MLayout &in, bool rowmax_ready);
+int leg_fwd_gemm(Ctx &c, const MLayout &in, const int *slots);
+// one persistent GEMM launch per transform over the tiles of several
+// mixed-precision shells (an ensemble): the backward transform of each
+// shell's d_four (bnvec vectors, bnscal scalars) and the forward transform
+// of its d_four2 into fslots; the buffers and slots are fixed at set-up
+struct MultiLeg;
+int multi_leg_setup(const std::vector<Ctx *> &shells, int bnvec, int bnscal, const int *fslots, int fnvec, int fnscal,
+                    MultiLeg **out);
+void multi_leg_bwd(const MultiLeg *m, cudaStream_t st);
+void multi_leg_fwd(const MultiLeg *m, cudaStream_t st);
+void multi_leg_free(MultiLeg *m);
 // buffer for the partial forward row maxima of a four-step FFT kernel
 // ([theta][(L+1)/16][elements], nullptr when the shape has none) and the
 // Gauss weights in float32
@@ -270,6 +286,13 @@ enum Tune {
 };
 // one time step (explicit, implicit, nonlinear); advances istep (cb2_api.cu)
 int step_once(Ctx &c);
+// the same step of a mixed-precision context without its two Legendre
+// GEMMs, in three phases: 0 (solves, Coriolis, backward packing), then the
+// backward GEMM, 1 (FFT + products, forward row scales), then the forward
+// GEMM, 2 (after the transform); phase 0 advances istep
+int step_phase(Ctx &c, int phase);
+// the multi-shell Legendre GEMM launches of step_phase's shells
+int step_gemms_setup(const std::vector<Ctx *> &shells, MultiLeg **out);
 // learned closure (cb2_closure.cu): adds its tendency to the nonlinear terms
 int closure_apply(Ctx &c);
 void closure_free(Ctx &c);

@@ -54,6 +54,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "cb2_internal.cuh"
@@ -185,7 +186,7 @@ struct FwdWsBars {
   uint64_t rawfull[FRS], rawempty[FRS], afull[FAB], bfull[FAB], abempty[FAB];
   uint64_t accfull[2], accempty[2], fin;
   uint32_t tmem_base;
-  int abort;
+  int abort, skip;
 };
 
 struct FwdTile {
@@ -228,26 +229,61 @@ __device__ inline float fwd_row_scale(const FwdArgs &a, const FwdTile &q, int ro
 template <typename Bars>
 __device__ inline bool ws_aborted(const Bars *sb) { return *(volatile const int *)&sb->abort != 0; }
 
+// One shell of a forward launch: its tensor maps (raw Fourier rows of both
+// gemms, B tables hi / lo of both gemms), arguments and tile counts.  A
+// single-shell launch takes it as a kernel parameter; an ensemble launch
+// reads a table of them from device memory, shell s owning the tiles
+// tile0(s) .. tile0(s + 1) - 1 of the launch.
+struct FwdShell {
+  CUtensorMap rawP, rawD, phi, plo, dhi, dlo;   // 64-byte aligned
+  FwdArgs a;
+  int rows_g0, rows_g1, tiles_g0, tiles_g1, tile0;
+};
+
+// the shell that owns tile t (tile0 ascending, tab[0].tile0 == 0)
+template <typename S>
+__device__ inline const S &shell_of(const S *tab, int nsh, int t) {
+  int lo = 0, hi = nsh - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&tab[mid].tile0) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return tab[lo];
+}
+
+// a tensor map written to device memory by the host: order that write
+// before the tensor-map proxy reads it
+__device__ inline void tensormap_acquire(const CUtensorMap *tm) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tm) : "memory");
+}
+
+// MULTI: the tiles of the shells in `tab` (nsh of them, ntiles in all) in
+// one launch, every shell with the same accumulator split; otherwise the
+// tiles of `one`.  Shared memory holds B tiles of nfb_max rows (the largest
+// shell) and, for one shell, its nth_w Gauss weights (an ensemble launch
+// reads the weights of each tile's shell through the cache instead).
+template <bool MULTI>
 __global__ void __launch_bounds__(FW_THREADS, 1)
-k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int tiles_g0, int tiles_g1, int ntiles,
-             const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
-             const __grid_constant__ CUtensorMap tmp_hi, const __grid_constant__ CUtensorMap tmp_lo,
-             const __grid_constant__ CUtensorMap tmd_hi, const __grid_constant__ CUtensorMap tmd_lo,
-             uint32_t tmem_cols, int nacc) {
+k_leg_fwd_ws(const __grid_constant__ FwdShell one, const FwdShell *__restrict__ tab, int nsh, int ntiles,
+             int nfb_max, int nth_w, uint32_t tmem_cols, int nacc) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char *base = smem_base_1024(smem_raw);
-  const FwdWsLayout lay = fwd_ws_layout(a.nfb, a.L, a.nth);
+  const FwdWsLayout lay = fwd_ws_layout(nfb_max, one.a.L, nth_w);
   FwdWsBars *sb = reinterpret_cast<FwdWsBars *>(base + lay.bar);
   float *w = reinterpret_cast<float *>(base + lay.w);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t B_BYTES = (uint32_t)a.nfb * FKB * 2;      // one of hi / lo, one parity
+  const uint32_t B_BYTES = (uint32_t)nfb_max * FKB * 2;    // one of hi / lo, one parity
   const uint32_t AB_BYTES = 4 * FA_BYTES + 4 * B_BYTES;    // A hi/lo x 2 parities, B hi/lo x 2 parities
   unsigned char *raw0 = base + lay.raw, *ab0 = base + lay.ab;
   const uint32_t accw = tmem_cols / (uint32_t)nacc;       // columns of one accumulator set
   // a set holds the accumulator of each parity (hi*hi' + cross terms), or
-  // with a.split the hi*hi' accumulators at 0 and acc1 and the cross-term
+  // with split the hi*hi' accumulators at 0 and acc1 and the cross-term
   // accumulators at 2 acc1 and 3 acc1
-  const uint32_t acc1 = a.split ? accw / 4 : accw / 2;
+  const int split = one.a.split;
+  const uint32_t acc1 = split ? accw / 4 : accw / 2;
+  const unsigned long long wait_ns = one.a.wait_ns;
+  auto shell = [&](int t) -> const FwdShell & { return MULTI ? shell_of(tab, nsh, t) : one; };
 
   if (tid == 0) {
     // consumer barriers count warps: one elected lane arrives for its warp
@@ -258,9 +294,14 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
     for (int q = 0; q < 2; q++) { mbar_init(&sb->accfull[q], 1); mbar_init(&sb->accempty[q], FW_EPI / 32); }
     mbar_init(&sb->fin, 1);
     sb->abort = 0;
+    // an earlier launch on any of the shells timed out: this one does nothing
+    int st = *(volatile int *)one.a.status;
+    if (MULTI)
+      for (int s = 0; s < nsh; s++) st |= *(volatile int *)tab[s].a.status;
+    sb->skip = (st & CB2_STATUS_PIPE_TIMEOUT) != 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int q = tid; q < a.nth; q += FW_THREADS) w[q] = a.wgt[q];
+  for (int q = tid; q < nth_w; q += FW_THREADS) w[q] = one.a.wgt[q];
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sb->tmem_base)),
                  "r"(tmem_cols));
@@ -270,7 +311,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sb->tmem_base;
-  const bool skip = (*(volatile int *)a.status & CB2_STATUS_PIPE_TIMEOUT) != 0;
+  const bool skip = sb->skip != 0;
 
   if (skip) {
     // an earlier launch timed out: do nothing
@@ -278,17 +319,25 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
     if (lane == 0) {
       uint32_t nraw = 0, nab = 0;
       bool bad = false;
+      const FwdShell *last = nullptr;
       for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x) {
         if (ws_aborted(sb)) { bad = true; break; }
-        const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
-        const CUtensorMap *traw = q.g ? &tm_rawD : &tm_rawP;
-        const CUtensorMap *tbh = q.g ? &tmd_hi : &tmp_hi, *tbl = q.g ? &tmd_lo : &tmp_lo;
+        const FwdShell &sh = shell(t);
+        const FwdArgs &a = sh.a;
+        const FwdTile q = fwd_tile(a, t - sh.tile0, sh.rows_g0, sh.rows_g1, sh.tiles_g0, sh.tiles_g1);
+        const CUtensorMap *traw = q.g ? &sh.rawD : &sh.rawP;
+        const CUtensorMap *tbh = q.g ? &sh.dhi : &sh.phi, *tbl = q.g ? &sh.dlo : &sh.plo;
+        if (MULTI && &sh != last) {   // the first tile of this CTA from this shell
+          const CUtensorMap *maps[6] = {&sh.rawP, &sh.rawD, &sh.phi, &sh.plo, &sh.dhi, &sh.dlo};
+          for (int u = 0; u < 6; u++) tensormap_acquire(maps[u]);
+          last = &sh;
+        }
         const uint32_t bbytes = 2u * (uint32_t)(q.nbox0 + q.nbox1) * a.boxr * FKB * 2;
         for (int b = 0; b < q.NB; b++) {
           const int tb = q.g ? (b >> 1) : b, part = q.g ? (b & 1) : 0;
           if (part == 0) {
             const uint32_t rs = nraw % FRS;
-            if (nraw >= FRS && !mbar_wait(&sb->rawempty[rs], ((nraw / FRS) - 1) & 1, a.wait_ns)) { bad = true; break; }
+            if (nraw >= FRS && !mbar_wait(&sb->rawempty[rs], ((nraw / FRS) - 1) & 1, wait_ns)) { bad = true; break; }
             unsigned char *dst = raw0 + rs * RAW_BYTES;
             mbar_expect_tx(&sb->rawfull[rs], RAW_BYTES);
             const uint64_t pf = policy_evict_first();
@@ -298,7 +347,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             nraw++;
           }
           const uint32_t s = nab % FAB;
-          if (nab >= FAB && !mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1, a.wait_ns)) { bad = true; break; }
+          if (nab >= FAB && !mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1, wait_ns)) { bad = true; break; }
           unsigned char *bb = ab0 + s * AB_BYTES + 4 * FA_BYTES;
           mbar_expect_tx(&sb->bfull[s], bbytes);
           const int x = part * a.nhp + tb * FKB;
@@ -334,14 +383,15 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
       int i = 0;
       for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x, i++) {
         if (ws_aborted(sb)) { bad = true; break; }
-        const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+        const FwdShell &sh = shell(t);
+        const FwdTile q = fwd_tile(sh.a, t - sh.tile0, sh.rows_g0, sh.rows_g1, sh.tiles_g0, sh.tiles_g1);
         const int ab = i % nacc;
-        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1, a.wait_ns)) { bad = true; break; }
+        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1, wait_ns)) { bad = true; break; }
         tc_fence_after();
         const uint32_t accb = tmem + (uint32_t)ab * accw;
         for (int b = 0; b < q.NB; b++) {
           const uint32_t s = nab % FAB, ph = (nab / FAB) & 1;
-          if (!mbar_wait(&sb->afull[s], ph, a.wait_ns) || !mbar_wait(&sb->bfull[s], ph, a.wait_ns)) { bad = true; break; }
+          if (!mbar_wait(&sb->afull[s], ph, wait_ns) || !mbar_wait(&sb->bfull[s], ph, wait_ns)) { bad = true; break; }
           tc_fence_after();
           unsigned char *at = ab0 + s * AB_BYTES, *bb = at + 4 * FA_BYTES;
           for (int p = 0; p < 2; p++) {
@@ -354,15 +404,15 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             // split: hi*hi' (on the fixed grid, summed exactly) in its own
             // accumulator, the cross terms and lo*lo' (2^-11 and 2^-22 of
             // it) in the second
-            const uint32_t accx = a.split ? acc + 2 * acc1 : acc;
+            const uint32_t accx = split ? acc + 2 * acc1 : acc;
 #pragma unroll
             for (int ks = 0; ks < FKB / 16; ks++) {
               const uint64_t o = (uint64_t)(ks * 2);
               const uint32_t first = (b == 0 && ks == 0) ? 0u : 1u;
               mma_f16(acc, dah + o, dbh + o, idesc, first);
-              mma_f16(accx, dah + o, dbl + o, idesc, a.split ? first : 1u);
+              mma_f16(accx, dah + o, dbl + o, idesc, split ? first : 1u);
               mma_f16(accx, dal + o, dbh + o, idesc, 1u);
-              if (a.split) mma_f16(accx, dal + o, dbl + o, idesc, 1u);
+              if (split) mma_f16(accx, dal + o, dbl + o, idesc, 1u);
             }
           }
           mma_commit(&sb->abempty[s]);
@@ -386,15 +436,19 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
     // every decision is warp-uniform: a warp arrives through one lane
     for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x) {
       if (__any_sync(0xffffffffu, ws_aborted(sb))) { bad = true; break; }
-      const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+      const FwdShell &sh = shell(t);
+      const FwdArgs &a = sh.a;
+      const FwdTile q = fwd_tile(a, t - sh.tile0, sh.rows_g0, sh.rows_g1, sh.tiles_g0, sh.tiles_g1);
       const int row = q.row0 + r, q4 = row & 3;
       const float sc = fwd_row_scale(a, q, row);
+      // Gauss weight of node i: staged in shared memory for one shell
+      auto wt = [&](int i) { return MULTI ? __ldg(a.wgt + i) : w[i]; };
       for (int b = 0; b < q.NB; b++) {
         const int tb = q.g ? (b >> 1) : b, part = q.g ? (b & 1) : 0;
         const uint32_t rs = nraw % FRS, s = nab % FAB;
         bool ok = true;
-        if (part == 0) ok = mbar_wait(&sb->rawfull[rs], (nraw / FRS) & 1, a.wait_ns);
-        if (ok && nab >= FAB) ok = mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1, a.wait_ns);
+        if (part == 0) ok = mbar_wait(&sb->rawfull[rs], (nraw / FRS) & 1, wait_ns);
+        if (ok && nab >= FAB) ok = mbar_wait(&sb->abempty[s], ((nab / FAB) - 1) & 1, wait_ns);
         if (!__all_sync(0xffffffffu, ok)) { bad = true; break; }
         // the two folds of this row's 16 K values; gemm P and the mP part
         // use fold p, the dP part fold 1 - p (with the signs of its rows)
@@ -413,8 +467,8 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
           const int kk = h * 16 + e, i = tb * FKB + kk;
           float vs = 0.0f, va = 0.0f;
           if (i < a.nh) {
-            const float fa = rs_s[kk * TM + src] * w[i];
-            const float fb = rs_n[(FKB - 1 - kk) * TM + src] * w[a.nth - 1 - i];
+            const float fa = rs_s[kk * TM + src] * wt(i);
+            const float fb = rs_n[(FKB - 1 - kk) * TM + src] * wt(a.nth - 1 - i);
             vs = (fa + fb) * sg;
             va = (fa - fb) * sg;
           }
@@ -430,7 +484,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
             uint32_t hh[4], ll[4];
 #pragma unroll
             for (int e = 0; e < 8; e += 2) {
-              if (a.split) split_pair_q(x2[p][c * 8 + e], x2[p][c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
+              if (split) split_pair_q(x2[p][c * 8 + e], x2[p][c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
               else split_pair(x2[p][c * 8 + e], x2[p][c * 8 + e + 1], hh[e >> 1], ll[e >> 1]);
             }
             const uint32_t off = sw64_chunk(r, 2 * h + c);
@@ -464,11 +518,13 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
     long long *moff = reinterpret_cast<long long *>(wst + 16 * FW_STG_P * 8);     // [16]
     double *mc = reinterpret_cast<double *>(moff + 16);                           // [16]
     int *mg = reinterpret_cast<int *>(mc + 16);                                   // [16]
-    double *__restrict__ fout = a.f;
     int i = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
       if (__any_sync(0xffffffffu, ws_aborted(sb))) break;
-      const FwdTile q = fwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+      const FwdShell &sh = shell(t);
+      const FwdArgs &a = sh.a;
+      double *__restrict__ fout = a.f;
+      const FwdTile q = fwd_tile(a, t - sh.tile0, sh.rows_g0, sh.rows_g1, sh.tiles_g0, sh.tiles_g1);
       const int nl = a.L + 1 - q.m;
       // lanes 0-15: destination, scale and degree factor of row lane
       // (sel 0: g7, 1: g6; both depend on l and m only, not on s)
@@ -499,7 +555,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
         moff[lane] = off; mc[lane] = cr; mg[lane] = sel;
       }
       const int ab = i % nacc;
-      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1, a.wait_ns);
+      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1, wait_ns);
       if (!__all_sync(0xffffffffu, ok)) { sb->abort = 1; break; }
       tc_fence_after();
       const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)(qd * 32 + hf * 16) << 16);
@@ -525,7 +581,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
         double p0[4], p1[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) { p0[j] = (double)f0[j]; p1[j] = (double)f1[j]; }
-        if (a.split) {
+        if (split) {
           float x0[4], x1[4];
           tmem_ld_16x256b_pair(tl + 2 * acc1 + (uint32_t)(g * 8), tl + 3 * acc1 + (uint32_t)(g * 8), x0, x1);
 #pragma unroll
@@ -559,7 +615,12 @@ k_leg_fwd_ws(const __grid_constant__ FwdArgs a, int rows_g0, int rows_g1, int ti
   }
   tc_fence_before();
   __syncthreads();
-  if (tid == 0 && sb->abort) atomicOr(a.status, CB2_STATUS_PIPE_TIMEOUT);
+  if (tid == 0 && sb->abort) {
+    // a multi-shell launch voids the state of every shell in it
+    atomicOr(one.a.status, CB2_STATUS_PIPE_TIMEOUT);
+    if (MULTI)
+      for (int s = 0; s < nsh; s++) atomicOr(tab[s].a.status, CB2_STATUS_PIPE_TIMEOUT);
+  }
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
 }
@@ -689,6 +750,16 @@ struct BwdArgs {
 
 constexpr uint32_t BRAW_BYTES = FKB * TM * 4;   // raw rows of one K block
 
+// One shell of a backward launch: its tensor maps, arguments and tile
+// counts.  A single-shell launch takes it as a kernel parameter; an
+// ensemble launch reads a table of them from device memory, shell s owning
+// the tiles tile0(s) .. tile0(s + 1) - 1 of the launch.
+struct BwdShell {
+  CUtensorMap rawP, rawD, bhi, blo;   // 64-byte aligned
+  BwdArgs a;
+  int rows_g0, rows_g1, tiles_g0, tiles_g1, tile0;
+};
+
 // ---------------------------------------------------------------------------
 // backward, warp-specialised and persistent: the roles of the forward kernel
 // (converters, epilogue warps, TMA producer, MMA issuer), one CTA per SM over
@@ -707,7 +778,7 @@ struct BwdWsBars {
   uint64_t full[BW_ST], afull[BW_ST], empty[BW_ST];
   uint64_t accfull[2], accempty[2], fin;
   uint32_t tmem_base;
-  int abort;
+  int abort, skip;
 };
 
 struct BwdTile {
@@ -759,20 +830,23 @@ __device__ inline float bwd_row_max(const BwdArgs &a, const BwdTile &q, int row)
   return fmaxf(a.maxD[(size_t)q.m * a.pitchD + row], a.maxD[(size_t)q.m * a.pitchD + row - q4 + 3 - q4]);
 }
 
+// MULTI: the tiles of the shells in `tab` (nsh of them, ntiles in all) in
+// one launch; otherwise the tiles of `one`.  Shared memory and tensor memory
+// are laid out for nhp_max colatitudes (the largest shell); the parity-1
+// accumulator of a tile sits at its own shell's nhp.
+template <bool MULTI>
 __global__ void __launch_bounds__(BW_THREADS, 1)
-k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int tiles_g0, int tiles_g1, int ntiles,
-             const __grid_constant__ CUtensorMap tm_rawP, const __grid_constant__ CUtensorMap tm_rawD,
-             const __grid_constant__ CUtensorMap tb_hi, const __grid_constant__ CUtensorMap tb_lo,
-             uint32_t tmem_cols, int nacc) {
+k_leg_bwd_ws(const __grid_constant__ BwdShell one, const BwdShell *__restrict__ tab, int nsh, int ntiles,
+             int nhp_max, uint32_t tmem_cols, int nacc) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char *base = smem_base_1024(smem_raw);
-  const uint32_t B_BYTES = (uint32_t)a.nhp * FKB * 2;       // one of hi / lo
+  const uint32_t B_BYTES = (uint32_t)nhp_max * FKB * 2;     // one of hi / lo
   const uint32_t ST_BYTES = BRAW_BYTES + 2 * FA_BYTES + 2 * B_BYTES;
   BwdWsBars *sb = reinterpret_cast<BwdWsBars *>(base + BW_ST * ST_BYTES);
-  float *buntab = reinterpret_cast<float *>(base + BW_ST * ST_BYTES + 256);   // [8 epilogue warps][nhp]
+  float *buntab = reinterpret_cast<float *>(base + BW_ST * ST_BYTES + 256);   // [8 epilogue warps][nhp_max]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t accw = tmem_cols / (uint32_t)nacc;         // columns of one accumulator set
-  const uint32_t acc1 = (uint32_t)a.nhp;                    // parity-1 accumulator within a set
+  auto shell = [&](int t) -> const BwdShell & { return MULTI ? shell_of(tab, nsh, t) : one; };
 
   if (tid == 0) {
     for (int q = 0; q < BW_ST; q++) {
@@ -782,6 +856,11 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
     for (int q = 0; q < 2; q++) { mbar_init(&sb->accfull[q], 1); mbar_init(&sb->accempty[q], BW_EPI / 32); }
     mbar_init(&sb->fin, 1);
     sb->abort = 0;
+    // an earlier launch on any of the shells timed out: this one does nothing
+    int st = *(volatile int *)one.a.status;
+    if (MULTI)
+      for (int s = 0; s < nsh; s++) st |= *(volatile int *)tab[s].a.status;
+    sb->skip = (st & CB2_STATUS_PIPE_TIMEOUT) != 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -793,7 +872,8 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sb->tmem_base;
-  const bool skip = (*(volatile int *)a.status & CB2_STATUS_PIPE_TIMEOUT) != 0;
+  const bool skip = sb->skip != 0;
+  const unsigned long long wait_ns = one.a.wait_ns;
 
   if (skip) {
     // an earlier launch timed out: do nothing
@@ -801,25 +881,35 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
     if (lane == 0) {
       uint32_t n = 0;
       bool bad = false;
+      const BwdShell *last = nullptr;
       for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x) {
         if (ws_aborted(sb)) { bad = true; break; }
-        const BwdTile q = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
-        const CUtensorMap *traw = q.g ? &tm_rawD : &tm_rawP;
+        const BwdShell &sh = shell(t);
+        const BwdArgs &a = sh.a;
+        const BwdTile q = bwd_tile(a, t - sh.tile0, sh.rows_g0, sh.rows_g1, sh.tiles_g0, sh.tiles_g1);
+        const CUtensorMap *traw = q.g ? &sh.rawD : &sh.rawP;
+        if (MULTI && &sh != last) {   // the first tile of this CTA from this shell
+          tensormap_acquire(&sh.rawP); tensormap_acquire(&sh.rawD);
+          tensormap_acquire(&sh.bhi); tensormap_acquire(&sh.blo);
+          last = &sh;
+        }
         for (int b = 0; b < q.total; b++) {
           int p, part, ib, len;
           bwd_blk(q, b, p, part, ib, len);
           const uint32_t s = n % BW_ST;
-          if (n >= BW_ST && !mbar_wait(&sb->empty[s], ((n / BW_ST) - 1) & 1, a.wait_ns)) { bad = true; break; }
+          if (n >= BW_ST && !mbar_wait(&sb->empty[s], ((n / BW_ST) - 1) & 1, wait_ns)) { bad = true; break; }
           unsigned char *st = base + s * ST_BYTES;
           // raw rows: parity of l-m of this part
           const int par = (q.g == 0) ? p : (part == 0 ? 1 - p : p);
           const int ky = a.kbase[q.m * 2 + par] + ib * FKB;
           const int bx = a.ko[(q.m * 4 + q.g * 2 + p) * 2 + part] + ib * FKB;
-          mbar_expect_tx(&sb->full[s], BRAW_BYTES + 2 * B_BYTES);
+          // the B tile of this shell: nhp rows of 64 bytes
+          const uint32_t bbytes = (uint32_t)a.nhp * FKB * 2;
+          mbar_expect_tx(&sb->full[s], BRAW_BYTES + 2 * bbytes);
           const uint64_t pf = policy_evict_first(), pl = policy_evict_last();
           tma_load_2d_hint(st, traw, &sb->full[s], q.row0, ky, pf);
-          tma_load_2d_hint(st + BRAW_BYTES + 2 * FA_BYTES, &tb_hi, &sb->full[s], bx, 0, pl);
-          tma_load_2d_hint(st + BRAW_BYTES + 2 * FA_BYTES + B_BYTES, &tb_lo, &sb->full[s], bx, 0, pl);
+          tma_load_2d_hint(st + BRAW_BYTES + 2 * FA_BYTES, &sh.bhi, &sb->full[s], bx, 0, pl);
+          tma_load_2d_hint(st + BRAW_BYTES + 2 * FA_BYTES + B_BYTES, &sh.blo, &sb->full[s], bx, 0, pl);
           n++;
         }
       }
@@ -837,19 +927,22 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
       uint32_t n = 0;
       bool bad = false, any = false;
       int i = 0;
-      const uint32_t idesc = idesc_f16_f32(TM, a.nhp);
       for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x, i++) {
         if (ws_aborted(sb)) { bad = true; break; }
-        const BwdTile q = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+        const BwdShell &sh = shell(t);
+        const BwdArgs &a = sh.a;
+        const BwdTile q = bwd_tile(a, t - sh.tile0, sh.rows_g0, sh.rows_g1, sh.tiles_g0, sh.tiles_g1);
+        const uint32_t idesc = idesc_f16_f32(TM, a.nhp);
+        const uint32_t acc1 = (uint32_t)a.nhp;                  // parity-1 accumulator within a set
         const int ab = i % nacc;
-        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1, a.wait_ns)) { bad = true; break; }
+        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1, wait_ns)) { bad = true; break; }
         tc_fence_after();
         const uint32_t accb = tmem + (uint32_t)ab * accw;
         for (int b = 0; b < q.total; b++) {
           int p, part, ib, len;
           bwd_blk(q, b, p, part, ib, len);
           const uint32_t s = n % BW_ST, ph = (n / BW_ST) & 1;
-          if (!mbar_wait(&sb->afull[s], ph, a.wait_ns) || !mbar_wait(&sb->full[s], ph, a.wait_ns)) { bad = true; break; }
+          if (!mbar_wait(&sb->afull[s], ph, wait_ns) || !mbar_wait(&sb->full[s], ph, wait_ns)) { bad = true; break; }
           tc_fence_after();
           unsigned char *ahi = base + s * ST_BYTES + BRAW_BYTES, *alo = ahi + FA_BYTES;
           unsigned char *bh = alo + FA_BYTES, *bl = bh + B_BYTES;
@@ -885,27 +978,28 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
     bool bad = false;
     int t = blockIdx.x;
     float mx_next = 0.0f;
-    if (t < ntiles) {
-      const BwdTile q0 = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
-      mx_next = bwd_row_max(a, q0, q0.row0 + r);
-    }
+    // the row maximum of tile t (row r)
+    auto tile_max = [&](int tt) {
+      const BwdShell &sn = shell(tt);
+      const BwdTile qn = bwd_tile(sn.a, tt - sn.tile0, sn.rows_g0, sn.rows_g1, sn.tiles_g0, sn.tiles_g1);
+      return bwd_row_max(sn.a, qn, qn.row0 + r);
+    };
+    if (t < ntiles) mx_next = tile_max(t);
     // every decision is warp-uniform: a warp arrives through one lane
     for (; t < ntiles && !bad; t += gridDim.x) {
       if (__any_sync(0xffffffffu, ws_aborted(sb))) { bad = true; break; }
-      const BwdTile q = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+      const BwdShell &sh = shell(t);
+      const BwdTile q = bwd_tile(sh.a, t - sh.tile0, sh.rows_g0, sh.rows_g1, sh.tiles_g0, sh.tiles_g1);
       const int row = q.row0 + r, q4 = row & 3;
       const float sc = pow2_scale(mx_next);
       // the next tile's row maximum is fetched now and used a tile later
       const int tn = t + gridDim.x;
-      if (tn < ntiles) {
-        const BwdTile qn = bwd_tile(a, tn, rows_g0, rows_g1, tiles_g0, tiles_g1);
-        mx_next = bwd_row_max(a, qn, qn.row0 + r);
-      }
+      if (tn < ntiles) mx_next = tile_max(tn);
       for (int b = 0; b < q.total; b++) {
         int p, part, ib, len;
         bwd_blk(q, b, p, part, ib, len);
         const uint32_t s = n % BW_ST;
-        if (!__all_sync(0xffffffffu, mbar_wait(&sb->full[s], (n / BW_ST) & 1, a.wait_ns))) { bad = true; break; }
+        if (!__all_sync(0xffffffffu, mbar_wait(&sb->full[s], (n / BW_ST) & 1, wait_ns))) { bad = true; break; }
         unsigned char *st = base + s * ST_BYTES;
         const float *raw = reinterpret_cast<const float *>(st);
         int src = r;
@@ -948,11 +1042,14 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
     // tile's column unscale (no barrier between the epilogue warps).
     // Decisions that guard the warp-collective TMEM loads are warp-uniform.
     const int ew = warp - BW_CONV / 32, er = (ew & 3) * 32 + lane, hc = ew >> 2;
-    float *bw = buntab + ew * a.nhp;
+    float *bw = buntab + ew * nhp_max;
     int i = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
       if (__any_sync(0xffffffffu, ws_aborted(sb))) break;
-      const BwdTile q = bwd_tile(a, t, rows_g0, rows_g1, tiles_g0, tiles_g1);
+      const BwdShell &sh = shell(t);
+      const BwdArgs &a = sh.a;
+      const BwdTile q = bwd_tile(a, t - sh.tile0, sh.rows_g0, sh.rows_g1, sh.tiles_g0, sh.tiles_g1);
+      const uint32_t acc1 = (uint32_t)a.nhp;
       const int row = q.row0 + er;
       const bool valid = row < q.nrows;
       const float ua = 1.0f / pow2_scale(bwd_row_max(a, q, row));
@@ -965,7 +1062,7 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
       __syncwarp();
       const bool has1 = q.nkb1 > 0;
       const int ab = i % nacc;
-      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1, a.wait_ns);
+      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1, wait_ns);
       if (!__all_sync(0xffffffffu, ok)) { sb->abort = 1; break; }
       tc_fence_after();
       const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)((ew & 3) * 32) << 16);
@@ -1006,7 +1103,12 @@ k_leg_bwd_ws(const __grid_constant__ BwdArgs a, int rows_g0, int rows_g1, int ti
   }
   tc_fence_before();
   __syncthreads();
-  if (tid == 0 && sb->abort) atomicOr(a.status, CB2_STATUS_PIPE_TIMEOUT);
+  if (tid == 0 && sb->abort) {
+    // a multi-shell launch voids the state of every shell in it
+    atomicOr(one.a.status, CB2_STATUS_PIPE_TIMEOUT);
+    if (MULTI)
+      for (int s = 0; s < nsh; s++) atomicOr(tab[s].a.status, CB2_STATUS_PIPE_TIMEOUT);
+  }
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
 }
@@ -1359,9 +1461,9 @@ int mixed_setup(Ctx &c) {
     set_error("mixed precision tiles exceed shared memory");
     return CB2_ERR_ARG;
   }
-  CB2_CUDA(raise_smem_limit(k_leg_bwd_ws, (int)t->smem_bwd));
+  CB2_CUDA(raise_smem_limit(k_leg_bwd_ws<false>, (int)t->smem_bwd));
   CB2_CUDA(raise_smem_limit(k_pack_bwd, (int)t->smem_pack));
-  CB2_CUDA(raise_smem_limit(k_leg_fwd_ws, (int)t->smem_fwd));
+  CB2_CUDA(raise_smem_limit(k_leg_fwd_ws<false>, (int)t->smem_fwd));
   {
     int dev = 0, nsm = 0;
     CB2_CUDA(cudaGetDevice(&dev));
@@ -1400,15 +1502,25 @@ static int ws_grid(const Ctx &c, int ntiles) {
   return std::max(1, std::min(t->nsm, (ntiles + per - 1) / per));
 }
 
-int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
-  MixedTables *t = (MixedTables *)c.mixed;
-  const int nvec = out.nvec, nscal = out.nscal, ng = nvec + nscal;
-  const int pitchP = ((2 * ng * c.nr + 3) / 4) * 4, pitchD = ((4 * nvec * c.nr + 3) / 4) * 4;
+// the backward transform's pack kernel (float32 order-major spectra and
+// their row maxima), and the GEMM's shell descriptor (no launch)
+static int bwd_check(const Ctx &c, const MLayout &out, int &pitchP, int &pitchD) {
+  const MixedTables *t = (const MixedTables *)c.mixed;
+  const int nvec = out.nvec, ng = out.nvec + out.nscal;
+  pitchP = ((2 * ng * c.nr + 3) / 4) * 4;
+  pitchD = ((4 * nvec * c.nr + 3) / 4) * 4;
   if (ng > 8 || nvec > 4 || pitchP > t->pitch_max || pitchD > t->pitch_max) {
     set_error("mixed backward transform: at most 8 fields and 4 vectors");
     return CB2_ERR_ARG;
   }
-  // step 1: order-major float32 spectra and their row maxima
+  return 0;
+}
+
+int leg_bwd_pack(Ctx &c, const int *slots, const MLayout &out) {
+  MixedTables *t = (MixedTables *)c.mixed;
+  int pitchP, pitchD, rc;
+  if ((rc = bwd_check(c, out, pitchP, pitchD))) return rc;
+  const int nvec = out.nvec, ng = out.nvec + out.nscal;
   PackArgs pk{};
   pk.L = c.L; pk.nr = c.nr; pk.jmax = c.jmax; pk.nvec = nvec; pk.ng = ng;
   pk.kc = (c.tune[TUNE_PACK_KC] == 1 || c.tune[TUNE_PACK_KC] == 4) ? c.tune[TUNE_PACK_KC] : 2;
@@ -1418,29 +1530,54 @@ int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
   pk.kbase = t->kbase; pk.maxP = t->maxP; pk.maxD = t->maxD;
   const size_t smp = (size_t)pk.kc * (2 * ng + 4 * nvec) * ((c.L + 1) | 1) * sizeof(float);
   k_pack_bwd<<<dim3(c.L + 1, cdiv(c.nr, pk.kc)), 256, smp, c.stream>>>(pk);
-  // step 2: the tensor-core transform
-  CUtensorMap rawP{}, rawD{};
-  if (make_map_any(&rawP, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, t->rlmP, pitchP, t->Ktot, TM, FKB,
+  return 0;
+}
+
+static int bwd_desc(Ctx &c, const MLayout &out, BwdShell &d, int &ntiles) {
+  MixedTables *t = (MixedTables *)c.mixed;
+  int pitchP, pitchD, rc;
+  if ((rc = bwd_check(c, out, pitchP, pitchD))) return rc;
+  const int nvec = out.nvec, nscal = out.nscal, ng = nvec + nscal;
+  std::memset(&d, 0, sizeof(d));
+  if (make_map_any(&d.rawP, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, t->rlmP, pitchP, t->Ktot, TM, FKB,
                    CU_TENSOR_MAP_SWIZZLE_NONE))
     return CB2_ERR_ARG;
   if (nvec > 0) {
-    if (make_map_any(&rawD, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, t->rlmD, pitchD, t->Ktot, TM, FKB,
+    if (make_map_any(&d.rawD, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, t->rlmD, pitchD, t->Ktot, TM, FKB,
                      CU_TENSOR_MAP_SWIZZLE_NONE))
       return CB2_ERR_ARG;
   } else {
-    rawD = rawP;
+    d.rawD = d.rawP;
   }
-  BwdArgs a{};
+  d.bhi = t->tm_bb_hi;
+  d.blo = t->tm_bb_lo;
+  BwdArgs &a = d.a;
   a.L = c.L; a.nr = c.nr; a.nh = c.nh; a.nhp = t->nhp; a.nth = c.nth; a.nvec = nvec; a.nscal = nscal;
   a.pitchP = pitchP; a.pitchD = pitchD;
   a.kbase = t->kbase; a.ko = t->bb_ko; a.maxP = t->maxP; a.maxD = t->maxD;
   a.bunscale = t->bb_unscale; a.out = out; a.status = c.d_status; a.wait_ns = c.pipe_wait_ns;
-  const int rows0 = ng * 2 * c.nr, rows1 = nvec * 4 * c.nr;
-  const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
-  const int ntiles = (tiles0 + tiles1) * (c.L + 1);
-  k_leg_bwd_ws<<<ws_grid(c, ntiles), BW_THREADS, t->smem_bwd, c.stream>>>(
-      a, rows0, rows1, tiles0, tiles1, ntiles, rawP, rawD, t->tm_bb_hi, t->tm_bb_lo, t->tmem_bwd, t->nacc_bwd);
+  d.rows_g0 = ng * 2 * c.nr;
+  d.rows_g1 = nvec * 4 * c.nr;
+  d.tiles_g0 = cdiv(d.rows_g0, TM);
+  d.tiles_g1 = (nvec > 0) ? cdiv(d.rows_g1, TM) : 0;
+  d.tile0 = 0;
+  ntiles = (d.tiles_g0 + d.tiles_g1) * (c.L + 1);
   return 0;
+}
+
+int leg_bwd_gemm(Ctx &c, const MLayout &out) {
+  MixedTables *t = (MixedTables *)c.mixed;
+  BwdShell d;
+  int ntiles, rc;
+  if ((rc = bwd_desc(c, out, d, ntiles))) return rc;
+  k_leg_bwd_ws<false><<<ws_grid(c, ntiles), BW_THREADS, t->smem_bwd, c.stream>>>(d, nullptr, 1, ntiles, t->nhp,
+                                                                                 t->tmem_bwd, t->nacc_bwd);
+  return 0;
+}
+
+int leg_bwd_mixed(Ctx &c, const int *slots, const MLayout &out) {
+  int rc = leg_bwd_pack(c, slots, out);
+  return rc ? rc : leg_bwd_gemm(c, out);
 }
 
 float *mixed_fwd_pmax(Ctx &c) {
@@ -1453,10 +1590,25 @@ const float *mixed_weights32(Ctx &c) {
   return t ? t->wgt32 : nullptr;
 }
 
-int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots, bool rowmax_ready) {
+// the forward transform's row scales: from the four-step FFT kernel's
+// partial maxima when it wrote them, else one pass over the Fourier rows
+void leg_fwd_rowmax(Ctx &c, const MLayout &in, bool rowmax_ready) {
+  MixedTables *t = (MixedTables *)c.mixed;
+  if (rowmax_ready && t->fwd_pmax && in.nvec == 4 && in.nscal == 0) {
+    const size_t E = in.sP() + in.sD();
+    k_rowmax_reduce<<<dim3(cdiv((long)E, 256), t->pmax_mb), 256, 0, c.stream>>>(t->fwd_pmax, c.nth, t->pmax_mb, E,
+                                                                               c.L, t->rowmax_four);
+  } else {
+    k_rowmax_four<<<dim3(cdiv((long)(in.sP() + in.sD()), 256), c.L + 1), 256, 0, c.stream>>>(in, t->wgt32,
+                                                                                         t->rowmax_four);
+  }
+}
+
+static int fwd_desc(Ctx &c, const MLayout &in, const int *slots, FwdShell &d, int &ntiles) {
   MixedTables *t = (MixedTables *)c.mixed;
   const int nvec = in.nvec, nscal = in.nscal;
-  FwdArgs a{};
+  std::memset(&d, 0, sizeof(d));
+  FwdArgs &a = d.a;
   a.L = c.L; a.nr = c.nr; a.jmax = c.jmax; a.nh = c.nh; a.nhp = t->nhp; a.nth = c.nth; a.NFmax = t->NFmax;
   a.boxr = t->boxr; a.nfb = t->nfb;
   a.nvec = nvec; a.nscal = nscal;
@@ -1470,30 +1622,133 @@ int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots, bool rowmax_ready
   a.wait_ns = c.pipe_wait_ns;
   a.split = t->split_fwd;
   // raw Fourier rows: float32 [(m, theta)][element], boxes of 128 elements x 32 colatitudes
-  CUtensorMap rawP{}, rawD{};
   const uint64_t nthr = (uint64_t)(c.L + 1) * c.nth;
-  if (make_map_any(&rawP, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, in.P, in.sP(), nthr, TM, FKB,
+  if (make_map_any(&d.rawP, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, in.P, in.sP(), nthr, TM, FKB,
                    CU_TENSOR_MAP_SWIZZLE_NONE) ||
-      (nvec > 0 && make_map_any(&rawD, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, in.D, in.sD(), nthr, TM, FKB,
-                                CU_TENSOR_MAP_SWIZZLE_NONE))) {
+      (nvec > 0 && make_map_any(&d.rawD, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, in.D, in.sD(), nthr, TM, FKB,
+                                CU_TENSOR_MAP_SWIZZLE_NONE)))
     return CB2_ERR_ARG;
-  }
-  if (nvec == 0) rawD = rawP;
-  if (rowmax_ready && t->fwd_pmax && nvec == 4 && nscal == 0) {
-    const size_t E = in.sP() + in.sD();
-    k_rowmax_reduce<<<dim3(cdiv((long)E, 256), t->pmax_mb), 256, 0, c.stream>>>(t->fwd_pmax, c.nth, t->pmax_mb, E,
-                                                                               c.L, t->rowmax_four);
-  } else {
-    k_rowmax_four<<<dim3(cdiv((long)(in.sP() + in.sD()), 256), c.L + 1), 256, 0, c.stream>>>(in, t->wgt32,
-                                                                                         t->rowmax_four);
-  }
-  const int rows0 = (nvec + nscal) * 2 * c.nr, rows1 = nvec * 4 * c.nr;
-  const int tiles0 = cdiv(rows0, TM), tiles1 = (nvec > 0) ? cdiv(rows1, TM) : 0;
-  const int ntiles = (tiles0 + tiles1) * (c.L + 1);
-  k_leg_fwd_ws<<<ws_grid(c, ntiles), FW_THREADS, t->smem_fwd, c.stream>>>(
-      a, rows0, rows1, tiles0, tiles1, ntiles, rawP, rawD, t->tm_bfp_hi, t->tm_bfp_lo, t->tm_bfd_hi, t->tm_bfd_lo,
-      t->tmem_fwd, t->nacc_fwd);
+  if (nvec == 0) d.rawD = d.rawP;
+  d.phi = t->tm_bfp_hi; d.plo = t->tm_bfp_lo; d.dhi = t->tm_bfd_hi; d.dlo = t->tm_bfd_lo;
+  d.rows_g0 = (nvec + nscal) * 2 * c.nr;
+  d.rows_g1 = nvec * 4 * c.nr;
+  d.tiles_g0 = cdiv(d.rows_g0, TM);
+  d.tiles_g1 = (nvec > 0) ? cdiv(d.rows_g1, TM) : 0;
+  d.tile0 = 0;
+  ntiles = (d.tiles_g0 + d.tiles_g1) * (c.L + 1);
   return 0;
 }
 
+int leg_fwd_gemm(Ctx &c, const MLayout &in, const int *slots) {
+  MixedTables *t = (MixedTables *)c.mixed;
+  FwdShell d;
+  int ntiles, rc;
+  if ((rc = fwd_desc(c, in, slots, d, ntiles))) return rc;
+  k_leg_fwd_ws<false><<<ws_grid(c, ntiles), FW_THREADS, t->smem_fwd, c.stream>>>(d, nullptr, 1, ntiles, t->nfb,
+                                                                                 c.nth, t->tmem_fwd, t->nacc_fwd);
+  return 0;
+}
+
+int leg_fwd_mixed(Ctx &c, const MLayout &in, const int *slots, bool rowmax_ready) {
+  leg_fwd_rowmax(c, in, rowmax_ready);
+  return leg_fwd_gemm(c, in, slots);
+}
+
+// ---------------------------------------------------------------------------
+// Ensemble launches: one persistent launch per Legendre GEMM over the
+// tiles of every shell (the shells' tables laid end to end, the largest
+// first so the long tiles start early).
+struct MultiLeg {
+  BwdShell *d_bwd = nullptr;
+  FwdShell *d_fwd = nullptr;
+  BwdShell one_bwd;
+  FwdShell one_fwd;
+  int nsh = 0, ntiles_bwd = 0, ntiles_fwd = 0, grid = 1;
+  int nhp_max = 0, nfb_max = 0;
+  uint32_t tmem_bwd = 0, tmem_fwd = 0;
+  int nacc_bwd = 1, nacc_fwd = 1;
+  size_t smem_bwd = 0, smem_fwd = 0;
+};
+
+void multi_leg_free(MultiLeg *m) {
+  if (!m) return;
+  if (m->d_bwd) cudaFree(m->d_bwd);
+  if (m->d_fwd) cudaFree(m->d_fwd);
+  delete m;
+}
+
+int multi_leg_setup(const std::vector<Ctx *> &shells, int bnvec, int bnscal, const int *fslots, int fnvec, int fnscal,
+                    MultiLeg **out) {
+  *out = nullptr;
+  const int n = (int)shells.size();
+  if (n == 0) { set_error("multi-shell Legendre: no shells"); return CB2_ERR_ARG; }
+  std::vector<int> order(n);
+  for (int i = 0; i < n; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return (long long)shells[x]->L * shells[x]->nr > (long long)shells[y]->L * shells[y]->nr;
+  });
+  MultiLeg *m = new MultiLeg();
+  std::vector<BwdShell> hb(n);
+  std::vector<FwdShell> hf(n);
+  int split = -1, rc = 0;
+  for (int j = 0; j < n && !rc; j++) {
+    Ctx &c = *shells[order[j]];
+    const MixedTables *t = (const MixedTables *)c.mixed;
+    if (!t || c.prec != CB2_PREC_MIXED) { set_error("multi-shell Legendre: mixed-precision shells only"); rc = CB2_ERR_ARG; break; }
+    if (split >= 0 && split != t->split_fwd) {
+      set_error("multi-shell Legendre: shells with and without the split forward accumulators");
+      rc = CB2_ERR_ARG;
+      break;
+    }
+    split = t->split_fwd;
+    int nb, nf;
+    if ((rc = bwd_desc(c, mlayout(c, c.d_four, bnvec, bnscal), hb[j], nb)) ||
+        (rc = fwd_desc(c, mlayout(c, c.d_four2, fnvec, fnscal), fslots, hf[j], nf)))
+      break;
+    hb[j].tile0 = m->ntiles_bwd;
+    hf[j].tile0 = m->ntiles_fwd;
+    m->ntiles_bwd += nb;
+    m->ntiles_fwd += nf;
+    // shared and tensor memory of the largest shell hold every shell's tiles
+    if (t->nhp > m->nhp_max) {
+      m->nhp_max = t->nhp;
+      m->tmem_bwd = t->tmem_bwd; m->nacc_bwd = t->nacc_bwd; m->smem_bwd = t->smem_bwd;
+    }
+    if (t->nfb > m->nfb_max || (t->nfb == m->nfb_max && t->tmem_fwd > m->tmem_fwd)) {
+      m->nfb_max = t->nfb;
+      m->tmem_fwd = t->tmem_fwd; m->nacc_fwd = t->nacc_fwd;
+    }
+    m->grid = std::max(m->grid, t->nsm);
+  }
+  if (!rc) {
+    m->nsh = n;
+    m->one_bwd = hb[0];
+    m->one_fwd = hf[0];
+    // the forward stages without the staged Gauss weights
+    m->smem_fwd = 1024 + fwd_ws_layout(m->nfb_max, 0, 0).total;
+    m->grid = std::min(m->grid, std::max(m->ntiles_bwd, m->ntiles_fwd));
+    cudaError_t e = cudaMalloc(&m->d_bwd, n * sizeof(BwdShell));
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_fwd, n * sizeof(FwdShell));
+    if (e == cudaSuccess) e = cudaMemcpy(m->d_bwd, hb.data(), n * sizeof(BwdShell), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(m->d_fwd, hf.data(), n * sizeof(FwdShell), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = raise_smem_limit(k_leg_bwd_ws<true>, (int)m->smem_bwd);
+    if (e == cudaSuccess) e = raise_smem_limit(k_leg_fwd_ws<true>, (int)m->smem_fwd);
+    if (e != cudaSuccess) rc = cuda_fail(e, "multi-shell Legendre tables");
+  }
+  if (rc) { multi_leg_free(m); return rc; }
+  *out = m;
+  return 0;
+}
+
+void multi_leg_bwd(const MultiLeg *m, cudaStream_t st) {
+  k_leg_bwd_ws<true><<<m->grid, BW_THREADS, m->smem_bwd, st>>>(m->one_bwd, m->d_bwd, m->nsh, m->ntiles_bwd,
+                                                               m->nhp_max, m->tmem_bwd, m->nacc_bwd);
+}
+
+void multi_leg_fwd(const MultiLeg *m, cudaStream_t st) {
+  k_leg_fwd_ws<true><<<m->grid, FW_THREADS, m->smem_fwd, st>>>(m->one_fwd, m->d_fwd, m->nsh, m->ntiles_fwd,
+                                                               m->nfb_max, 0, m->tmem_fwd, m->nacc_fwd);
+}
+
 }  // namespace cb2
+

@@ -123,10 +123,14 @@ using namespace cb2;
 struct cb2_ensemble {
   std::vector<cb2_ctx *> shells;
   cudaStream_t stream = nullptr;         // fork / join stream of the graph
-  cudaEvent_t fork = nullptr;
-  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork[3] = {nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> join[3];      // per phase and shell
   cudaGraphExec_t graph = nullptr;
   int device = 0;
+  // mixed-precision shells: each Legendre GEMM launched once for all shells
+  // (between the shells' step phases) instead of once per shell
+  int batched = 1;
+  MultiLeg *ml = nullptr;
 };
 
 extern "C" {
@@ -163,10 +167,13 @@ int cb2_ensemble_destroy(cb2_ensemble *e) {
   if (!e) return 0;
   if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->graph) cudaGraphExecDestroy(e->graph);
+  multi_leg_free(e->ml);
   for (cb2_ctx *c : e->shells) cb2_destroy(c);
-  for (cudaEvent_t ev : e->join)
-    if (ev) cudaEventDestroy(ev);
-  if (e->fork) cudaEventDestroy(e->fork);
+  for (int ph = 0; ph < 3; ph++) {
+    for (cudaEvent_t ev : e->join[ph])
+      if (ev) cudaEventDestroy(ev);
+    if (e->fork[ph]) cudaEventDestroy(e->fork[ph]);
+  }
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return 0;
@@ -180,9 +187,11 @@ int cb2_ensemble_create(const cb2_params *ps, int n, int precision, int device, 
   auto fail = [&](int rc) { cb2_ensemble_destroy(e); return rc; };
   if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "cudaSetDevice"));
   cudaGetDevice(&e->device);
-  if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(cuda_fail(cudaGetLastError(), "ensemble stream"));
+  for (int ph = 0; ph < 3; ph++)
+    if (cudaEventCreateWithFlags(&e->fork[ph], cudaEventDisableTiming) != cudaSuccess)
+      return fail(cuda_fail(cudaGetLastError(), "ensemble event"));
   // shells of one shape (L, nr, nth, nph) share the first one's autotuning
   std::vector<int> first_of(n, -1);
   for (int i = 0; i < n; i++) {
@@ -193,10 +202,12 @@ int cb2_ensemble_create(const cb2_params *ps, int n, int precision, int device, 
     // small shells take a few SMs each (about eight tiles per CTA of the
     // persistent Legendre kernels), so the graph's branches run side by side
     if (n > 1) c->ws_tiles_per_cta = 8;
-    cudaEvent_t ev;
-    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
-      return fail(cuda_fail(cudaGetLastError(), "ensemble event"));
-    e->join.push_back(ev);
+    for (int ph = 0; ph < 3; ph++) {
+      cudaEvent_t ev;
+      if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+        return fail(cuda_fail(cudaGetLastError(), "ensemble event"));
+      e->join[ph].push_back(ev);
+    }
     for (int j = 0; j < i; j++)
       if (ps[j].ltr == ps[i].ltr && ps[j].nr == ps[i].nr && ps[j].nth == ps[i].nth && ps[j].nph == ps[i].nph) {
         first_of[i] = j;
@@ -215,6 +226,18 @@ int cb2_ensemble_create(const cb2_params *ps, int n, int precision, int device, 
     }
   }
   *out = e;
+  return 0;
+}
+
+int cb2_ensemble_set_batched(cb2_ensemble *e, int on) {
+  if (!e) { set_error("cb2_ensemble_set_batched: null ensemble"); return CB2_ERR_ARG; }
+  if ((on != 0) != (e->batched != 0) && e->graph) {
+    // the step graph is captured again at the next cb2_ensemble_step
+    CB2_CUDA(cudaStreamSynchronize(e->stream));
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  e->batched = on ? 1 : 0;
   return 0;
 }
 
@@ -255,21 +278,42 @@ int cb2_ensemble_step(cb2_ensemble *e, int nsteps) {
   }
   if (done == nsteps) return 0;
   if (!e->graph) {
+    bool batched = e->batched != 0;
+    for (cb2_ctx *c : e->shells) batched &= (c->prec == CB2_PREC_MIXED);
+    if (batched && !e->ml) {
+      std::vector<Ctx *> v(e->shells.begin(), e->shells.end());
+      int rc = step_gemms_setup(v, &e->ml);
+      if (rc) return rc;
+    }
     cudaGraph_t g;
     CB2_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     int rc = 0;
-    cudaEventRecord(e->fork, e->stream);
-    for (size_t i = 0; i < e->shells.size() && !rc; i++) {
-      cb2_ctx *c = e->shells[i];
-      cudaStreamWaitEvent(c->stream, e->fork, 0);
-      const bool tm = c->timers;
-      c->timers = false;
-      const int save = c->istep;
-      rc = step_once(*c);
-      c->istep = save;
-      c->timers = tm;
-      cudaEventRecord(e->join[i], c->stream);
-      cudaStreamWaitEvent(e->stream, e->join[i], 0);
+    std::vector<int> save(e->shells.size());
+    std::vector<bool> tm(e->shells.size());
+    for (size_t i = 0; i < e->shells.size(); i++) {
+      save[i] = e->shells[i]->istep;
+      tm[i] = e->shells[i]->timers;
+      e->shells[i]->timers = false;
+    }
+    // batched: phase 0 of every shell, the backward GEMM of all, phase 1 of
+    // every shell, the forward GEMM of all, phase 2 of every shell; else one
+    // branch per shell holding its whole step
+    const int nph = batched ? 3 : 1;
+    for (int ph = 0; ph < nph && !rc; ph++) {
+      cudaEventRecord(e->fork[ph], e->stream);
+      for (size_t i = 0; i < e->shells.size() && !rc; i++) {
+        cb2_ctx *c = e->shells[i];
+        cudaStreamWaitEvent(c->stream, e->fork[ph], 0);
+        rc = batched ? step_phase(*c, ph) : step_once(*c);
+        cudaEventRecord(e->join[ph][i], c->stream);
+        cudaStreamWaitEvent(e->stream, e->join[ph][i], 0);
+      }
+      if (batched && ph == 0) multi_leg_bwd(e->ml, e->stream);
+      if (batched && ph == 1) multi_leg_fwd(e->ml, e->stream);
+    }
+    for (size_t i = 0; i < e->shells.size(); i++) {
+      e->shells[i]->istep = save[i];
+      e->shells[i]->timers = tm[i];
     }
     cudaError_t ec = cudaStreamEndCapture(e->stream, &g);
     if (rc) {

@@ -162,7 +162,7 @@ EXPORTS = [
     "cb2_get_plm", "cb2_stage_times", "cb2_time_steps", "cb2_alloc_pinned", "cb2_free_pinned",
     "cb2_energies_static", "cb2_autotune", "cb2_get_tuning", "cb2_set_tuning",
     "cb2_ensemble_create", "cb2_ensemble_destroy", "cb2_ensemble_size", "cb2_ensemble_shell",
-    "cb2_ensemble_init_fields", "cb2_ensemble_step", "cb2_ensemble_sync", "cb2_ensemble_time_steps",
+    "cb2_ensemble_init_fields", "cb2_ensemble_step", "cb2_ensemble_set_batched", "cb2_ensemble_sync", "cb2_ensemble_time_steps",
     "cb2_ensemble_energies", "cb2_leg_bwd", "cb2_leg_fwd", "cb2_fft_bwd", "cb2_fft_fwd",
     "cb2_legendre_trans_mode", "cb2_fft_library_known", "cb2_energy_spectra", "cb2_fft_products",
     "cb2_get_restart_state", "cb2_set_restart_state", "cb2_step_restart_state", "cb2_tuning_note",
@@ -216,6 +216,7 @@ def load_library(path: str = LIB_PATH):
         "cb2_ensemble_shell": ([vp, i], vp),
         "cb2_ensemble_init_fields": ([vp, i, ctypes.c_uint], i),
         "cb2_ensemble_step": ([vp, i], i),
+        "cb2_ensemble_set_batched": ([vp, i], i),
         "cb2_ensemble_sync": ([vp], i),
         "cb2_ensemble_time_steps": ([vp, i, pd], i),
         "cb2_ensemble_energies": ([vp, pd], i),
@@ -518,7 +519,9 @@ def fft_library_known(fft_library_ctl: str) -> bool:
 
 class Ensemble:
     """Independent shells advanced together, one CUDA graph launch per step
-    (cb2_ensemble_*).  `shells[i]` is a view of shell i (do not close it)."""
+    (cb2_ensemble_*); mixed-precision shells share one launch of each
+    Legendre GEMM (set_batched).  `shells[i]` is a view of shell i (do not
+    close it)."""
 
     def __init__(self, params_list, precision: int = PREC_MIXED, device: int = -1, autotune: bool = True):
         lib = load_library()
@@ -554,6 +557,11 @@ class Ensemble:
 
     def step(self, nsteps: int = 1):
         _check(load_library().cb2_ensemble_step(self._h, nsteps), "cb2_ensemble_step")
+
+    def set_batched(self, on: bool):
+        """Mixed-precision shells: each Legendre GEMM as one launch over all
+        shells (True, the default) or one launch per shell."""
+        _check(load_library().cb2_ensemble_set_batched(self._h, 1 if on else 0), "cb2_ensemble_set_batched")
 
     def sync(self):
         _check(load_library().cb2_ensemble_sync(self._h), "cb2_ensemble_sync")

@@ -419,6 +419,13 @@ module m_calypso_b200
       integer(c_int) :: rc
     end function cb2_ensemble_step
 
+    function cb2_ensemble_set_batched(e, on) bind(C, name='cb2_ensemble_set_batched') result(rc)
+      import
+      type(c_ptr), value :: e
+      integer(c_int), value :: on
+      integer(c_int) :: rc
+    end function cb2_ensemble_set_batched
+
     function cb2_ensemble_sync(e) bind(C, name='cb2_ensemble_sync') result(rc)
       import
       type(c_ptr), value :: e

@@ -1,7 +1,9 @@
 """Batched ensemble and kernel-variant autotuner on the GPU.
 
   - every shell of an ensemble (mixed truncations, one CUDA graph launch per
-    step) ends bit-for-bit where the same shell stepped alone ends;
+    step) ends bit-for-bit where the same shell stepped alone ends, with the
+    mixed path's Legendre GEMMs as one launch over all shells or one per
+    shell;
   - the autotuner picks from its candidate sets, refuses to run once the
     fields exist, and no kernel variant changes a result (bitwise)."""
 import numpy as np
@@ -23,10 +25,11 @@ def small_ensemble():
     return out
 
 
-@pytest.mark.parametrize("prec", [PREC_MIXED, PREC_FP64])
-def test_ensemble_matches_shells_stepped_alone(prec):
+@pytest.mark.parametrize("prec,batched", [(PREC_MIXED, True), (PREC_MIXED, False), (PREC_FP64, True)])
+def test_ensemble_matches_shells_stepped_alone(prec, batched):
     params = small_ensemble()
     ens = Ensemble(params, prec, device=0, autotune=True)
+    ens.set_batched(batched)
     ens.init_fields(2, 11)
     ens.step(12)
     e_ens = ens.energies()
@@ -42,6 +45,37 @@ def test_ensemble_matches_shells_stepped_alone(prec):
         for a, slot in zip(fields[q], (VELO, MAGNE + 2, TEMP)):
             assert np.array_equal(a, g.get_field(slot)), (q, slot)
         g.close()
+
+
+def test_batched_legendre_launches_three_truncations():
+    """Mixed shells of three truncations in an unsorted order (L31, L127,
+    L63, L31: different colatitude counts, B-table heights and tensor-memory
+    widths in one launch) and four radial sizes: the ensemble whose two
+    Legendre GEMMs are one launch over every shell's tiles ends bitwise where
+    the ensemble with one launch per shell ends, and switching between the
+    two forms in the middle of a run changes nothing."""
+    params = [configs.shell_params(31, 9, 48, 96, E=1e-3, Ra=150.0, dt=1e-4),
+              configs.shell_params(127, 9, 192, 384, E=1e-4, Ra=300.0, dt=5e-6),
+              configs.shell_params(63, 13, 96, 192, E=1e-3, Ra=250.0, dt=5e-5),
+              configs.shell_params(31, 17, 48, 96, E=1e-3, Ra=350.0, dt=1e-4)]
+    runs = []
+    for mode in ("batched", "branches", "switch"):
+        ens = Ensemble(params, PREC_MIXED, device=0, autotune=False)
+        ens.set_batched(mode != "branches")
+        ens.init_fields(2, 5)
+        ens.step(4)
+        if mode == "switch":
+            ens.set_batched(False)
+        ens.step(4)
+        runs.append((ens.energies(), [[s.get_field(slot) for slot in (VELO, MAGNE + 2, TEMP)]
+                                      for s in ens.shells]))
+        ens.close()
+    for e, f in runs[1:]:
+        assert np.array_equal(e, runs[0][0])
+        for q in range(len(params)):
+            for a, b in zip(f[q], runs[0][1][q]):
+                assert np.array_equal(a, b), q
+    assert np.isfinite(runs[0][0]).all()
 
 
 @pytest.mark.parametrize("prec", [PREC_MIXED, PREC_FP64])
