@@ -128,8 +128,11 @@ struct cb2_ensemble {
   cudaGraphExec_t graph = nullptr;
   int device = 0;
   // mixed-precision shells: each Legendre GEMM launched once for all shells
-  // (between the shells' step phases) instead of once per shell
-  int batched = 1;
+  // (between the shells' step phases) instead of once per shell.  Off by
+  // default: on the 48-shell and 64-shell ensembles measured the joins
+  // around the two launches cost more (3-4 % of the step) than the single
+  // launches save in GEMM time (6 %)
+  int batched = 0;
   MultiLeg *ml = nullptr;
 };
 
@@ -299,9 +302,19 @@ int cb2_ensemble_step(cb2_ensemble *e, int nsteps) {
     // every shell, the forward GEMM of all, phase 2 of every shell; else one
     // branch per shell holding its whole step
     const int nph = batched ? 3 : 1;
+    // branches in order of decreasing work per step (L^3 nr), so the longest
+    // chains start first and the joins wait less on a late start
+    std::vector<size_t> order(e->shells.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = i;
+    auto work = [&](size_t i) {
+      const double l1 = e->shells[i]->L + 1.0;
+      return l1 * l1 * l1 * e->shells[i]->nr;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return work(x) > work(y); });
     for (int ph = 0; ph < nph && !rc; ph++) {
       cudaEventRecord(e->fork[ph], e->stream);
-      for (size_t i = 0; i < e->shells.size() && !rc; i++) {
+      for (size_t i : order) {
+        if (rc) break;
         cb2_ctx *c = e->shells[i];
         cudaStreamWaitEvent(c->stream, e->fork[ph], 0);
         rc = batched ? step_phase(*c, ph) : step_once(*c);

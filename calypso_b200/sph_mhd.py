@@ -519,9 +519,9 @@ def fft_library_known(fft_library_ctl: str) -> bool:
 
 class Ensemble:
     """Independent shells advanced together, one CUDA graph launch per step
-    (cb2_ensemble_*); mixed-precision shells share one launch of each
-    Legendre GEMM (set_batched).  `shells[i]` is a view of shell i (do not
-    close it)."""
+    (cb2_ensemble_*); set_batched(True) makes mixed-precision shells share
+    one launch of each Legendre GEMM.  `shells[i]` is a view of shell i (do
+    not close it)."""
 
     def __init__(self, params_list, precision: int = PREC_MIXED, device: int = -1, autotune: bool = True):
         lib = load_library()
@@ -560,7 +560,7 @@ class Ensemble:
 
     def set_batched(self, on: bool):
         """Mixed-precision shells: each Legendre GEMM as one launch over all
-        shells (True, the default) or one launch per shell."""
+        shells (True) or one launch per shell (False, the default)."""
         _check(load_library().cb2_ensemble_set_batched(self._h, 1 if on else 0), "cb2_ensemble_set_batched")
 
     def sync(self):

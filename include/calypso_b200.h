@@ -287,11 +287,11 @@ const char *cb2_tuning_note(const cb2_ctx *ctx);
 
 /* Ensemble of independent shells (any mix of truncations and parameters),
  * advanced together: one CUDA graph holds a time step of every shell, so one
- * graph launch advances all of them.  For mixed-precision shells (batched,
- * the default) each of the two tensor-core Legendre GEMMs is one persistent
- * launch over the tiles of every shell, and the other kernels of the step
- * run as parallel per-shell branches between them; otherwise (FP64 shells,
- * or cb2_ensemble_set_batched(e, 0)) each shell's whole step is one branch.
+ * graph launch advances all of them.  By default each shell's whole step is
+ * one branch of the graph.  Batched (cb2_ensemble_set_batched(e, 1),
+ * mixed-precision shells): each of the two tensor-core Legendre GEMMs is one
+ * persistent launch over the tiles of every shell, and the other kernels of
+ * the step run as parallel per-shell branches between them.
  * No counterpart in the reference (it runs one shell per job).  Shells of
  * one shape (ltr, nr, nth, nph) share one autotuning when
  * autotune_shapes != 0.  Shell i is an ordinary context
@@ -306,7 +306,7 @@ cb2_ctx *cb2_ensemble_shell(cb2_ensemble *e, int i);
 /* shell i gets cb2_init_fields(kind, seed0 + i) */
 int cb2_ensemble_init_fields(cb2_ensemble *e, int kind, unsigned seed0);
 int cb2_ensemble_step(cb2_ensemble *e, int nsteps);
-/* on != 0: batched Legendre GEMM launches (the default); takes effect at the
+/* on != 0: batched Legendre GEMM launches (default off); takes effect at the
  * next cb2_ensemble_step, with identical results either way */
 int cb2_ensemble_set_batched(cb2_ensemble *e, int on);
 int cb2_ensemble_sync(cb2_ensemble *e);
