@@ -274,8 +274,8 @@ void fft_forward_grid_m(Ctx &c, const double *grid, const MLayout &out);
 
 // autotuned kernel variants (Ctx::tune)
 enum Tune {
-  TUNE_BWD_KT = 0,       // float64 backward Legendre: radial levels per block (2, 4)
-  TUNE_FWD_KT = 1,       // float64 forward Legendre: radial levels per block (1, 2, 4)
+  TUNE_BWD_KT = 0,       // float64 backward Legendre: 1 tensor cores (mma f64); CUDA cores with 2 or 4 radial levels per block
+  TUNE_FWD_KT = 1,       // float64 forward Legendre: CUDA cores with 1 or 2 radial levels per block; 3 tensor cores (mma f64)
   TUNE_PACK_KC = 2,      // mixed backward pack: radial levels per block (1, 2, 4)
   TUNE_FFT_THREADS = 3,  // mixed FFT + products: threads per row block; 384 = the four-step kernel
                          // (nphi = 3 (L + 1)), 128 / 256 / 512 = the Stockham kernel

@@ -37,6 +37,12 @@ __device__ inline void cp_async8(double *dst, const double *src, int n) {
                "l"(src), "r"(n)
                : "memory");
 }
+// 16-byte form (both addresses 16-byte aligned); n = 0 fills zeros
+__device__ inline void cp_async16(double *dst, const double *src, int n) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(n)
+               : "memory");
+}
 __device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 // every group but the newest has landed
 __device__ inline void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
@@ -214,6 +220,235 @@ k_leg_bwd_f64(LegArgs a, double *four) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Backward on the float64 tensor cores (mma.sync m16n8k4, f64 in and out).
+//
+// For one order m and the degrees l of one parity p = (l - m) & 1 the sums
+// of k_leg_bwd_f64 are three products whose terms land in the
+// reflection-parity accumulators (south node = sigma 0 + sigma 1, mirror
+// node = sigma 0 - sigma 1):
+//   R  (A = P_l^m):        columns (k, group, s) of X_s, X = S l(l+1)/r^2
+//                          (vector) or the scalar          -> sigma = p
+//   TP (A = dP_l^m):       columns (k, vector, q) of
+//                          [D+, D-, -T+, -T-] (D = dS/dr / r, T = T / r)
+//                                                          -> sigma = 1 - p
+//   TM (A = m P_l^m / sin): the same columns of [T-, -T+, D-, -D+]
+//                                                          -> sigma = p
+// with q = 0 v_theta(+m), 1 v_theta(-m), 2 v_phi(+m), 3 v_phi(-m).
+// A block takes 64 south nodes (four row tiles of 16) and TKT radial
+// levels; per node row tile, TW warps share the column tiles (8 columns
+// each; R and TP/TM tiles round-robin).  A chunk of 16 degrees (8 of each
+// parity) is staged by cp.async (P, dP by parity [j][node]; the spectra as
+// copied), converted into the three B matrices [parity][j][column], and
+// consumed by two k4 steps per parity; the next chunk's copies are in flight
+// meanwhile.
+constexpr int TKT = 2;                      // radial levels per block
+constexpr int TW = 2;                       // warps per 16-node row tile
+constexpr int TLC = 16;                     // degrees per chunk
+constexpr int TMAXG = 6;                    // groups per launch
+constexpr int TAP = 68;                     // A row pitch (nodes, 68 = 4 mod 16: no bank conflicts)
+constexpr int TRP = ((2 * TMAXG * TKT + 15) / 16) * 16 + 4;   // 36: R pitch, 4 mod 16
+constexpr int TTP = ((4 * TMAXG * TKT + 15) / 16) * 16 + 4;   // 52: TP / TM pitch, 4 mod 16
+constexpr int TRAW = TKT * TMAXG * 6;       // raw spectral columns of a chunk
+constexpr int TMAXT = ((2 * TMAXG * TKT + 7) / 8 + (4 * TMAXG * TKT) / 8 + TW - 1) / TW;   // tiles per warp
+constexpr int TBUF = 2 * 2 * (TLC / 2) * TAP + TLC * TRAW;   // one stage: P, dP by parity + raw spectra
+constexpr int TBM = 2 * (TLC / 2) * (TRP + 2 * TTP);          // the built B matrices
+constexpr int TBST = 2;                                       // staging buffers (cp.async pipeline depth)
+// + the column tables (raw offsets, R and T factors, R and T descriptors)
+constexpr size_t tc_bwd_smem() {
+  return (TBST * (size_t)TBUF + TBM) * sizeof(double) + TRAW * 8 + 6 * TMAXG * TKT * 8 + 6 * TMAXG * TKT * 4;
+}
+
+__device__ __forceinline__ void dmma16n8k4(double (&d)[4], double a0, double a1, double b0) {
+  asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+               : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+               : "d"(a0), "d"(a1), "d"(b0));
+}
+
+__global__ void __launch_bounds__(4 * TW * 32, 2)
+k_leg_bwd_f64tc(LegArgs a, double *four) {
+  const int m = blockIdx.z, k0 = blockIdx.y * TKT, i0 = blockIdx.x * 64;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int rt = warp / TW, wc = warp - rt * TW;        // row tile (16 nodes), column warp
+  const int gq = lane >> 2, tq = lane & 3;              // fragment row / k index
+  const int G = a.nvec + a.nscal, nl = a.L + 1 - m;
+  const int ncr = 2 * G * TKT, nct = 4 * a.nvec * TKT;  // R and TP/TM columns
+  const int nraw = 6 * G * TKT;                         // raw columns ((kq G + g) 3 + comp) 2 + s
+  const int ntr = (ncr + 7) / 8, ntt = nct / 8, ntiles = ntr + ntt;
+  extern __shared__ __align__(16) double smt[];
+  double *BR = smt + TBST * TBUF, *BTP = BR + 2 * (TLC / 2) * TRP, *BTM = BTP + 2 * (TLC / 2) * TTP;
+  // per-block column tables, so the staging of a chunk does no index
+  // division: raw column -> offset of its degree-m spectral value (-1: a
+  // zero column); R column -> raw column (+ 1 << 16 for a vector) and its
+  // radial factor; T column -> raw column of its vector's S+ and 1 / r
+  long long *rawsrc = reinterpret_cast<long long *>(BTM + 2 * (TLC / 2) * TTP);
+  double *rsc = reinterpret_cast<double *>(rawsrc + TRAW), *tsc = rsc + 2 * TMAXG * TKT;
+  int *rdesc = reinterpret_cast<int *>(tsc + 4 * TMAXG * TKT), *tdesc = rdesc + 2 * TMAXG * TKT;
+  for (int col = tid; col < nraw; col += blockDim.x) {
+    const int s = col & 1, comp = (col >> 1) % 3, kg = col / 6, g = kg % G, kq = kg / G, k = k0 + kq;
+    long long off = -1;
+    if (k < a.nr && !(m == 0 && s == 1) && (g < a.nvec || comp == 0))
+      off = (long long)(a.slot[g] + (g < a.nvec ? comp : 0)) * (long long)a.fs + (long long)k * a.jmax +
+            a.moff[m] + s * nl;
+    rawsrc[col] = off;
+  }
+  for (int c = tid; c < ncr; c += blockDim.x) {
+    const int kg = c >> 1, g = kg % G, k = k0 + kg / G;
+    const bool vec = g < a.nvec && k < a.nr;
+    const double ar = vec ? a.ar1[k] : 1.0;
+    rdesc[c] = kg * 6 + (c & 1) + (vec ? (1 << 16) : 0);
+    rsc[c] = ar * ar;
+  }
+  for (int c = tid; c < nct; c += blockDim.x) {
+    const int kv = c >> 2, v = kv % a.nvec, kq = kv / a.nvec, k = k0 + kq;
+    tdesc[c] = (kq * G + v) * 6;
+    tsc[c] = (k < a.nr) ? a.ar1[k] : 0.0;
+  }
+  __syncthreads();
+  const size_t po = a.poff[m];
+  const bool pair16 = (a.nh & 1) == 0;
+  // staging of chunk lc0 into stage b: P and dP of the block's 64 nodes by
+  // parity [p][j][node], and the raw spectra [raw column][lc]
+  auto issue = [&](int lc0, int b) {
+    double *st = smt + (size_t)b * TBUF;
+    double *Ps = st, *dPs = st + 2 * (TLC / 2) * TAP, *raw = st + 4 * (TLC / 2) * TAP;
+    if (pair16) {
+      // two nodes per 16-byte copy (nh even: every row starts 16-byte aligned)
+      for (int e = tid; e < TLC * 32; e += blockDim.x) {
+        const int lc = e >> 5, nd = (e & 31) * 2, ii = i0 + nd, t = lc0 + lc;
+        const bool in = t < nl && ii < a.nh;
+        const size_t at = in ? po + (size_t)t * a.nh + ii : 0;
+        const int o = ((lc & 1) * (TLC / 2) + (lc >> 1)) * TAP + nd;
+        cp_async16(Ps + o, a.Plt + at, in ? 16 : 0);
+        cp_async16(dPs + o, a.dPlt + at, in ? 16 : 0);
+      }
+    } else {
+      for (int e = tid; e < TLC * 64; e += blockDim.x) {
+        const int lc = e >> 6, nd = e & 63, ii = i0 + nd, t = lc0 + lc;
+        const bool in = t < nl && ii < a.nh;
+        const size_t at = in ? po + (size_t)t * a.nh + ii : 0;
+        const int o = ((lc & 1) * (TLC / 2) + (lc >> 1)) * TAP + nd;
+        cp_async8(Ps + o, a.Plt + at, in ? 8 : 0);
+        cp_async8(dPs + o, a.dPlt + at, in ? 8 : 0);
+      }
+    }
+    for (int e = tid; e < TLC * nraw; e += blockDim.x) {
+      const int lc = e & (TLC - 1), col = e >> 4;
+      const long long so = rawsrc[col];
+      const bool in = so >= 0 && lc0 + lc < nl;
+      cp_async8(raw + col * TLC + lc, in ? a.f + so + lc0 + lc : a.f, in ? 8 : 0);
+    }
+    cp_async_commit();
+  };
+  // raw spectra of stage b -> B matrices (radial and degree factors, signs)
+  auto build = [&](int lc0, int b) {
+    const double *raw = smt + (size_t)b * TBUF + 4 * (TLC / 2) * TAP;
+    // lanes along the degrees of a column: consecutive raw addresses
+    for (int e = tid; e < TLC * 32; e += blockDim.x) {
+      const int c = e >> 4, lc = e & (TLC - 1);
+      if (c >= ncr) continue;
+      const int rd = rdesc[c], l = m + lc0 + lc;
+      double x = raw[(rd & 0xffff) * TLC + lc];
+      if (rd >> 16) x *= rsc[c] * ((l == 0) ? 0.5 : (double)l * (double)(l + 1));
+      BR[((lc & 1) * (TLC / 2) + (lc >> 1)) * TRP + c] = x;
+    }
+    for (int e = tid; e < TLC * 64; e += blockDim.x) {
+      const int c = e >> 4, lc = e & (TLC - 1);
+      if (c >= nct) continue;
+      const int q = c & 3;
+      const double ar = tsc[c];
+      const double *rw = raw + tdesc[c] * TLC + lc;   // S+ S- D+ D- T+ T-, TLC apart
+      const double Dp = rw[2 * TLC] * ar, Dm = rw[3 * TLC] * ar, Tp = rw[4 * TLC] * ar, Tm = rw[5 * TLC] * ar;
+      const int o = ((lc & 1) * (TLC / 2) + (lc >> 1));
+      BTP[o * TTP + c] = (q == 0) ? Dp : (q == 1) ? Dm : (q == 2) ? -Tp : -Tm;
+      BTM[o * TTP + c] = (q == 0) ? Tm : (q == 1) ? -Tp : (q == 2) ? Dm : -Dp;
+    }
+    // padding columns of the last R tile stay zero
+    for (int e = tid; e < TLC * 8; e += blockDim.x) {
+      const int lc = e >> 3, c = ncr + (e & 7);
+      if (c < ntr * 8) BR[((lc & 1) * (TLC / 2) + (lc >> 1)) * TRP + c] = 0.0;
+    }
+  };
+  double acc[TMAXT][2][4];
+#pragma unroll
+  for (int i = 0; i < TMAXT; i++)
+#pragma unroll
+    for (int p = 0; p < 2; p++)
+#pragma unroll
+      for (int u = 0; u < 4; u++) acc[i][p][u] = 0.0;
+  // m / sin(theta) of this thread's two fragment rows
+  const int na = i0 + 16 * rt + gq, nb = na + 8;
+  const double ama = (na < a.nh) ? (double)m * a.asin_t[na] : 0.0;
+  const double amb = (nb < a.nh) ? (double)m * a.asin_t[nb] : 0.0;
+  const int nch = (nl + TLC - 1) / TLC;
+  issue(0, 0);
+  for (int ch = 0; ch < nch; ch++) {
+    const int lc0 = ch * TLC, b = ch & 1;
+    if (ch + 1 < nch) issue(lc0 + TLC, b ^ 1);
+    else cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    build(lc0, b);
+    __syncthreads();
+    const double *Ps = smt + (size_t)b * TBUF, *dPs = Ps + 2 * (TLC / 2) * TAP;
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+#pragma unroll
+      for (int ks = 0; ks < TLC / 8; ks++) {
+        const int j = ks * 4 + tq, o = (p * (TLC / 2) + j);
+        const double pa = Ps[o * TAP + 16 * rt + gq], pb = Ps[o * TAP + 16 * rt + gq + 8];
+        const double da = dPs[o * TAP + 16 * rt + gq], db = dPs[o * TAP + 16 * rt + gq + 8];
+        const double ma = pa * ama, mb = pb * amb;
+#pragma unroll
+        for (int i = 0; i < TMAXT; i++) {
+          const int jt = wc + TW * i;
+          if (jt < ntt) {
+            const double btp = BTP[o * TTP + 8 * jt + gq], btm = BTM[o * TTP + 8 * jt + gq];
+            dmma16n8k4(acc[i][p ^ 1], da, db, btp);
+            dmma16n8k4(acc[i][p], ma, mb, btm);
+          } else if (jt < ntiles) {
+            const double br = BR[o * TRP + 8 * (jt - ntt) + gq];
+            dmma16n8k4(acc[i][p], pa, pb, br);
+          }
+        }
+      }
+    }
+    __syncthreads();   // stage b and the B matrices are refilled next
+  }
+  // south / mirror values of each fragment: rows na, nb; columns 2 tq, 2 tq + 1
+  // are the orders +m and -m of one component
+#pragma unroll
+  for (int i = 0; i < TMAXT; i++) {
+    const int jt = wc + TW * i;
+    if (jt >= ntiles) continue;
+    int kq, c;
+    if (jt < ntt) {
+      const int cc = 8 * jt + 2 * tq, kv = cc >> 2, v = kv % a.nvec;
+      kq = kv / a.nvec;
+      c = a.cbase + 3 * v + 1 + ((cc & 3) >> 1);
+    } else {
+      const int cc = 8 * (jt - ntt) + 2 * tq;
+      if (cc >= ncr) continue;
+      const int kg = cc >> 1, g = kg % G;
+      kq = kg / G;
+      c = a.cbase + (g < a.nvec ? 3 * g : 3 * a.nvec + (g - a.nvec));
+    }
+    const int k = k0 + kq;
+    if (k >= a.nr) continue;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int n = h ? nb : na;
+      if (n >= a.nh) continue;
+      const double e0 = acc[i][0][2 * h], e1 = acc[i][0][2 * h + 1];
+      const double o0 = acc[i][1][2 * h], o1 = acc[i][1][2 * h + 1];
+      const double2 south = make_double2(e0 + o0, m == 0 ? 0.0 : e1 + o1);
+      const double2 north = make_double2(e0 - o0, m == 0 ? 0.0 : e1 - o1);
+      *reinterpret_cast<double2 *>(four + four_at(a, n, k, c) + 2 * m) = south;
+      *reinterpret_cast<double2 *>(four + four_at(a, a.nth - 1 - n, k, c) + 2 * m) = north;
+    }
+  }
+}
+
 // forward: block = (order m, radial tile); thread = two consecutive
 // degrees l - m = t (even) and t + 1, one of each reflection parity, so the
 // symmetric and antisymmetric sums of a grid value, adjacent in shared
@@ -376,6 +611,227 @@ k_leg_fwd_f64(LegArgs a, const double *four, int c0, int g0) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Forward on the float64 tensor cores (mma.sync m16n8k4).  For one order m
+// and the degrees of one parity p the sums of k_leg_fwd_f64 are products
+// over the south nodes i (K) of the tables (rows: degrees) with the
+// Gauss-weighted symmetric / antisymmetric grid sums H (same = the sums of
+// the parity of P, other = the converse):
+//   R  (A = P):   columns (k, group, s): R_same(s) or the scalar's S_same(s)
+//   TP (A = dP):  columns (k, vector, q): [T_other(+), T_other(-),
+//                 -F_other(+), -F_other(-)]
+//   TM (A = P, rows of B times m / sin theta_i): the same columns of
+//                 [-F_same(-), F_same(+), -T_same(-), T_same(+)]
+// with q = 0, 1 the dS/dr coefficient of orders +m, -m and q = 2, 3 the
+// toroidal one.  A block takes 64 degrees (two 16-row tiles of each parity)
+// and TKT radial levels and walks the nodes in chunks of 16 (four k4
+// steps): the P and dP rows of its degrees and the raw grid values of the
+// chunk's nodes and mirrors by cp.async (the next chunk in flight), then
+// the weighted sums built into the B matrices of both parities.
+constexpr int TFC = 16;                     // nodes per chunk
+constexpr int TFAP = TFC + 4;               // A row pitch (20 = 4 mod 16)
+constexpr int TFRAW = TKT * (3 * TMAXG) * 2 * 2;   // raw values of a node: (k, comp, s, node / mirror)
+constexpr int TFBUF = 2 * 64 * TFAP + TFC * TFRAW; // one stage: P, dP rows, raw values
+constexpr int TFBM = 2 * TFC * (TRP + 2 * TTP);   // the B matrices of both parities
+// + the column tables (raw offsets, R and T descriptors)
+constexpr size_t tc_fwd_smem() {
+  return (2 * (size_t)TFBUF + TFBM) * sizeof(double) + (TFRAW / 2) * 8 + 6 * TMAXG * TKT * 4;
+}
+
+__global__ void __launch_bounds__(4 * TW * 32, 2)
+k_leg_fwd_f64tc(LegArgs a, const double *four) {
+  const int m = blockIdx.z, k0 = blockIdx.y * TKT, t0 = blockIdx.x * 64;   // degree offset l - m
+  const int nl = a.L + 1 - m;
+  if (t0 >= nl) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int rt = warp / TW, wc = warp - rt * TW;         // row tile: parity rt & 1, half rt >> 1
+  const int gq = lane >> 2, tq = lane & 3;
+  const int G = a.nvec + a.nscal, C = 3 * a.nvec + a.nscal;
+  const int ncr = 2 * G * TKT, nct = 4 * a.nvec * TKT, nrw = 4 * C * TKT;
+  const int ntr = (ncr + 7) / 8, ntt = nct / 8, ntiles = ntr + ntt;
+  extern __shared__ __align__(16) double smf[];
+  double *BR = smf + 2 * TFBUF, *BTP = BR + 2 * TFC * TRP, *BTM = BTP + 2 * TFC * TTP;
+  // per-block column tables, so the staging of a chunk does no index
+  // division: raw value x = ((kq C + c) 2 + s) 2 + h -> offset of its
+  // (k, component, order) in a Fourier row (-1: a zero value); R column ->
+  // raw value of its node (h = 0); T column -> raw value of its vector's
+  // theta component (s = 0, h = 0)
+  long long *rawsrc = reinterpret_cast<long long *>(BTM + 2 * TFC * TTP);
+  int *rdesc = reinterpret_cast<int *>(rawsrc + TFRAW / 2), *tdesc = rdesc + 2 * TMAXG * TKT;
+  for (int x2 = tid; x2 < nrw / 2; x2 += blockDim.x) {   // x2 = (kq C + c) 2 + s
+    const int s = x2 & 1, kc = x2 >> 1, c = kc % C, k = k0 + kc / C;
+    rawsrc[x2] = (k < a.nr && !(m == 0 && s == 1))
+                     ? (long long)(((size_t)k * a.ncomp + a.cbase + c) * a.NS + 2 * m + s) : -1;
+  }
+  for (int cc = tid; cc < ncr; cc += blockDim.x) {   // cc = (kq G + g) 2 + s
+    const int s = cc & 1, kg = cc >> 1, g = kg % G, kq = kg / G;
+    const int c = (g < a.nvec) ? 3 * g : 3 * a.nvec + (g - a.nvec);
+    rdesc[cc] = ((kq * C + c) * 2 + s) * 2;
+  }
+  for (int cc = tid; cc < nct; cc += blockDim.x) {   // cc = (kq nvec + v) 4 + q
+    const int kv = cc >> 2, v = kv % a.nvec, kq = kv / a.nvec;
+    tdesc[cc] = ((kq * C + 3 * v + 1) * 2) * 2;
+  }
+  __syncthreads();
+  const size_t po = a.poff[m];
+  const bool pair16 = (a.nh & 1) == 0;
+  const size_t rowst = (size_t)a.nr * a.ncomp * a.NS;   // one colatitude of the Fourier buffer
+  // stage b: P, dP of the block's degrees (row r = 32 p + j, degree
+  // t0 + 2 j + p) at the chunk's nodes [r][node]; raw grid values
+  // [node][x], h = 0 the node, 1 its mirror
+  auto issue = [&](int ib, int b) {
+    double *st = smf + (size_t)b * TFBUF, *Ps = st, *dPs = st + 64 * TFAP, *raw = st + 2 * 64 * TFAP;
+    if (pair16) {
+      // two nodes per 16-byte copy (nh even: every row starts 16-byte aligned)
+      for (int e = tid; e < 64 * TFC / 2; e += blockDim.x) {
+        const int r = e >> 3, nd = (e & 7) * 2, t = t0 + 2 * (r & 31) + (r >> 5), i = ib + nd;
+        const bool in = t < nl && i < a.nh;
+        const size_t at = in ? po + (size_t)t * a.nh + i : 0;
+        cp_async16(Ps + r * TFAP + nd, a.Plt + at, in ? 16 : 0);
+        cp_async16(dPs + r * TFAP + nd, a.dPlt + at, in ? 16 : 0);
+      }
+    } else {
+      for (int e = tid; e < 64 * TFC; e += blockDim.x) {
+        const int r = e >> 4, nd = e & (TFC - 1), t = t0 + 2 * (r & 31) + (r >> 5), i = ib + nd;
+        const bool in = t < nl && i < a.nh;
+        const size_t at = in ? po + (size_t)t * a.nh + i : 0;
+        cp_async8(Ps + r * TFAP + nd, a.Plt + at, in ? 8 : 0);
+        cp_async8(dPs + r * TFAP + nd, a.dPlt + at, in ? 8 : 0);
+      }
+    }
+    for (int e = tid; e < TFC * 128; e += blockDim.x) {
+      const int nd = e >> 7, x = e & 127, i = ib + nd;
+      if (x >= nrw) continue;
+      const long long so = rawsrc[x >> 1];
+      const bool in = so >= 0 && i < a.nh;
+      const size_t th = (x & 1) ? (size_t)(a.nth - 1 - i) : (size_t)i;
+      cp_async8(raw + nd * TFRAW + x, in ? four + th * rowst + so : four, in ? 8 : 0);
+    }
+    cp_async_commit();
+  };
+  // weighted sums of stage b -> B matrices of both parities [p][node][col]
+  auto build = [&](int ib, int b) {
+    const double *raw = smf + (size_t)b * TFBUF + 2 * 64 * TFAP;
+    for (int e = tid; e < TFC * 32; e += blockDim.x) {
+      const int nd = e >> 5, cc = e & 31, i = ib + nd;
+      if (cc >= ncr) continue;
+      double sym = 0.0, anti = 0.0;
+      if (i < a.nh) {
+        const double *rv = raw + nd * TFRAW + rdesc[cc];
+        const double fa = rv[0] * a.wgt[i], fb = rv[1] * a.wgt[a.nth - 1 - i];
+        sym = fa + fb; anti = fa - fb;
+      }
+      BR[(0 * TFC + nd) * TRP + cc] = sym;
+      BR[(1 * TFC + nd) * TRP + cc] = anti;
+    }
+    for (int e = tid; e < TFC * 64; e += blockDim.x) {
+      const int nd = e >> 6, cc = e & 63, i = ib + nd;
+      if (cc >= nct) continue;
+      const int q = cc & 3;
+      double Ts[2] = {0, 0}, Ta[2] = {0, 0}, Fs[2] = {0, 0}, Fa[2] = {0, 0}, ams = 0.0;
+      if (i < a.nh) {
+        const double wa = a.wgt[i], wb = a.wgt[a.nth - 1 - i];
+        const double *rt_ = raw + nd * TFRAW + tdesc[cc];   // theta (s 0, 1; node, mirror)
+        const double *rf_ = rt_ + 4;                          // phi
+        for (int s = 0; s < 2; s++) {
+          const double ta = rt_[2 * s] * wa, tb = rt_[2 * s + 1] * wb;
+          const double fa = rf_[2 * s] * wa, fb = rf_[2 * s + 1] * wb;
+          Ts[s] = ta + tb; Ta[s] = ta - tb; Fs[s] = fa + fb; Fa[s] = fa - fb;
+        }
+        ams = (double)m * a.asin_t[i];
+      }
+      // parity 0: same = symmetric, other = antisymmetric; parity 1 the converse
+      for (int p = 0; p < 2; p++) {
+        const double *Tsm = p ? Ta : Ts, *Tot = p ? Ts : Ta, *Fsm = p ? Fa : Fs, *Fot = p ? Fs : Fa;
+        const double tp = (q == 0) ? Tot[0] : (q == 1) ? Tot[1] : (q == 2) ? -Fot[0] : -Fot[1];
+        const double tm = (q == 0) ? -Fsm[1] : (q == 1) ? Fsm[0] : (q == 2) ? -Tsm[1] : Tsm[0];
+        BTP[(p * TFC + nd) * TTP + cc] = tp;
+        BTM[(p * TFC + nd) * TTP + cc] = tm * ams;
+      }
+    }
+    for (int e = tid; e < TFC * 8; e += blockDim.x) {
+      const int nd = e >> 3, cc = ncr + (e & 7);
+      if (cc < ntr * 8) {
+        BR[nd * TRP + cc] = 0.0;
+        BR[(TFC + nd) * TRP + cc] = 0.0;
+      }
+    }
+  };
+  double acc[TMAXT][4];
+#pragma unroll
+  for (int i = 0; i < TMAXT; i++)
+#pragma unroll
+    for (int u = 0; u < 4; u++) acc[i][u] = 0.0;
+  const int p = rt & 1, ar0 = 32 * p + 16 * (rt >> 1);   // this warp's A rows
+  const int nchk = (a.nh + TFC - 1) / TFC;
+  issue(0, 0);
+  for (int ch = 0; ch < nchk; ch++) {
+    const int ib = ch * TFC, b = ch & 1;
+    if (ch + 1 < nchk) issue(ib + TFC, b ^ 1);
+    else cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    build(ib, b);
+    __syncthreads();
+    const double *Ps = smf + (size_t)b * TFBUF, *dPs = Ps + 64 * TFAP;
+#pragma unroll
+    for (int ks = 0; ks < TFC / 4; ks++) {
+      const int kk = 4 * ks + tq;
+      const double pa = Ps[(ar0 + gq) * TFAP + kk], pb = Ps[(ar0 + gq + 8) * TFAP + kk];
+      const double da = dPs[(ar0 + gq) * TFAP + kk], db = dPs[(ar0 + gq + 8) * TFAP + kk];
+      const int bo = p * TFC + kk;
+#pragma unroll
+      for (int i = 0; i < TMAXT; i++) {
+        const int jt = wc + TW * i;
+        if (jt < ntt) {
+          dmma16n8k4(acc[i], da, db, BTP[bo * TTP + 8 * jt + gq]);
+          dmma16n8k4(acc[i], pa, pb, BTM[bo * TTP + 8 * jt + gq]);
+        } else if (jt < ntiles) {
+          dmma16n8k4(acc[i], pa, pb, BR[bo * TRP + 8 * (jt - ntt) + gq]);
+        }
+      }
+    }
+    __syncthreads();   // stage b and the B matrices are refilled next
+  }
+  // rows: degrees t0 + 2 (16 (rt >> 1) + gq (+ 8)) + p; columns 2 tq, 2 tq + 1
+  // are the orders +m and -m
+#pragma unroll
+  for (int i = 0; i < TMAXT; i++) {
+    const int jt = wc + TW * i;
+    if (jt >= ntiles) continue;
+    int kq, slot, kind;   // kind 0: r^2 g7 (poloidal), 1: r g7, 2: g6 (scalar)
+    if (jt < ntt) {
+      const int cc = 8 * jt + 2 * tq, kv = cc >> 2, v = kv % a.nvec;
+      kq = kv / a.nvec;
+      slot = a.slot[v] + 1 + ((cc & 3) >> 1);
+      kind = 1;
+    } else {
+      const int cc = 8 * (jt - ntt) + 2 * tq;
+      if (cc >= ncr) continue;
+      const int kg = cc >> 1, g = kg % G;
+      kq = kg / G;
+      slot = a.slot[g];
+      kind = (g < a.nvec) ? 0 : 2;
+    }
+    const int k = k0 + kq;
+    if (k >= a.nr) continue;
+    const double r = a.r[k];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int t = t0 + 2 * (16 * (rt >> 1) + gq + 8 * h) + p;
+      if (t >= nl) continue;
+      const int l = m + t;
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        if (s == 1 && m == 0) break;   // order -m exists for m > 0 only
+        const int jj = jj_of(a, l, m, s);
+        const double fac = (kind == 0) ? a.g7[jj] * r * r : (kind == 1) ? a.g7[jj] * r : a.g6[jj];
+        a.f[(size_t)slot * a.fs + (size_t)k * a.jmax + jj] = acc[i][2 * h + s] * fac;
+      }
+    }
+  }
+}
+
 static LegArgs leg_args(Ctx &c, int nvec, int nscal, const int *slots) {
   LegArgs a;
   a.L = c.L; a.nr = c.nr; a.nth = c.nth; a.nh = c.nh; a.jmax = c.jmax; a.NS = c.NS;
@@ -401,6 +857,16 @@ static void launch_bwd(Ctx &c, const LegArgs &b, double *four, int nb) {
   k_leg_bwd_f64<KT><<<grid, 32 * nb, sm, c.stream>>>(b, four);
 }
 
+static void launch_bwd_tc(Ctx &c, const LegArgs &b, double *four) {
+  static bool attr = false;   // the kernel's dynamic shared-memory limit, raised once
+  if (!attr) {
+    cudaFuncSetAttribute(k_leg_bwd_f64tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_bwd_smem());
+    attr = true;
+  }
+  dim3 grid(cdiv(c.nh, 64), cdiv(c.nr, TKT), c.L + 1);
+  k_leg_bwd_f64tc<<<grid, 4 * TW * 32, tc_bwd_smem(), c.stream>>>(b, four);
+}
+
 void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four) {
   LegArgs a = leg_args(c, nvec, nscal, slots);
   // launches of at most MAXG groups: vectors first, then scalars
@@ -412,8 +878,10 @@ void leg_bwd_f64(Ctx &c, int nvec, int nscal, const int *slots, double *four) {
     b.nscal = nb - b.nvec;
     b.cbase = comp;
     for (int q = 0; q < nb; q++) b.slot[q] = slots[g + q];
-    // tuning value 2: two radial levels per block, 4: four
-    if (c.tune[TUNE_BWD_KT] == 2) launch_bwd<2>(c, b, four, nb);
+    // tuning value 1: the tensor-core kernel; 2 or 4: the CUDA-core kernel
+    // with two or four radial levels per block
+    if (c.tune[TUNE_BWD_KT] == 1) launch_bwd_tc(c, b, four);
+    else if (c.tune[TUNE_BWD_KT] == 2) launch_bwd<2>(c, b, four, nb);
     else launch_bwd<4>(c, b, four, nb);
     comp += 3 * b.nvec + b.nscal;
     g += nb;
@@ -442,8 +910,37 @@ static void launch_fwd(Ctx &c, LegArgs a, const double *four, int c0, const int 
   }
 }
 
+static void launch_fwd_tc(Ctx &c, const LegArgs &b, const double *four) {
+  static bool attr = false;   // the kernel's dynamic shared-memory limit, raised once
+  if (!attr) {
+    cudaFuncSetAttribute(k_leg_fwd_f64tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_fwd_smem());
+    attr = true;
+  }
+  dim3 grid(cdiv(c.L + 1, 64), cdiv(c.nr, TKT), c.L + 1);
+  k_leg_fwd_f64tc<<<grid, 4 * TW * 32, tc_fwd_smem(), c.stream>>>(b, four);
+}
+
 void leg_fwd_f64(Ctx &c, int nvec, int nscal, const double *four, const int *slots) {
   LegArgs a = leg_args(c, nvec, nscal, slots);
+  if (c.tune[TUNE_FWD_KT] == 3 && nvec <= 5) {
+    // the tensor-core kernel: launches of at most TMAXG groups, vectors
+    // first (at most 16 components in a launch: its staging maps the raw
+    // values of a node with a stride of 128 = 4 x 16 x TKT)
+    int g = 0, comp = 0;
+    const int ngrp = nvec + nscal;
+    while (g < ngrp) {
+      const int nb = std::min(TMAXG, ngrp - g);
+      LegArgs b = a;
+      b.nvec = std::max(0, std::min(nvec - g, nb));
+      b.nscal = nb - b.nvec;
+      b.cbase = comp;
+      for (int q = 0; q < nb; q++) b.slot[q] = slots[g + q];
+      launch_fwd_tc(c, b, four);
+      comp += 3 * b.nvec + b.nscal;
+      g += nb;
+    }
+    return;
+  }
   int g = 0, comp = 0;
   // vectors in batches of up to 4, scalars in batches of up to 4
   while (g < nvec) {

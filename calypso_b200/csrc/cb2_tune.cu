@@ -89,8 +89,8 @@ int autotune(Ctx &c) {
   };
   std::vector<Item> items;
   if (c.prec == CB2_PREC_FP64) {
-    items.push_back({TUNE_BWD_KT, {2, 4}, stage_bwd_f64});
-    items.push_back({TUNE_FWD_KT, {1, 2}, stage_fwd_f64});
+    items.push_back({TUNE_BWD_KT, {1, 2, 4}, stage_bwd_f64});
+    items.push_back({TUNE_FWD_KT, {1, 2, 3}, stage_fwd_f64});
     // 384: the float64 four-step kernel (where nphi = 3 (L + 1)), 512: Stockham
     items.push_back({TUNE_FFT_THREADS, {384, 512}, stage_fft_f64});
   } else {

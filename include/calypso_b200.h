@@ -269,8 +269,10 @@ int cb2_free_pinned(void *p);
  * which times its Legendre loop variants at start-up): times every
  * candidate tile / launch shape of the transform kernels on this context
  * and keeps the fastest.  Only before cb2_init_fields / cb2_start (it
- * overwrites the work fields).  tuning[5]: float64 backward radial tile,
- * float64 forward radial tile, mixed pack radial tile, FFT kernel of either
+ * overwrites the work fields).  tuning[5]: float64 backward kernel (1: on
+ * the float64 tensor cores; 2, 4: on the CUDA cores with that radial tile),
+ * float64 forward kernel (1, 2: on the CUDA cores with that radial tile; 3:
+ * on the float64 tensor cores), mixed pack radial tile, FFT kernel of either
  * precision (384: the four-step kernel, used where nphi = 3 (ltr + 1);
  * 128, 256, 512: the Stockham kernel, float64 always with 512 threads), and
  * 1 to run the explicit update, the radial solves and the derived fields

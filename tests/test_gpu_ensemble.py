@@ -14,7 +14,7 @@ from calypso_b200.sph_mhd import MAGNE, TEMP, VELO
 
 pytestmark = pytest.mark.gpu
 
-CANDIDATES = [(2, 4), (1, 2), (1, 2, 4), (384, 512, 256, 128)]
+CANDIDATES = [(1, 2, 4), (1, 2, 3), (1, 2, 4), (384, 512, 256, 128)]
 
 
 def small_ensemble():

@@ -53,9 +53,16 @@ def test_tables_match_oracle(oracle_lib, case1):
         assert np.abs(d1 - d2).max() / sd < 1e-12, (l, m)
 
 
-@pytest.mark.parametrize("nvec,nscal", [(3, 2), (4, 1), (1, 0), (0, 1)])
-def test_sht_fp64_matches_oracle(oracle_lib, case1, nvec, nscal):
+# float64 Legendre kernels (tuning entries 0 and 1): on the CUDA cores
+# (backward 4, forward 2) and on the float64 tensor cores (1, 3)
+KERNELS = {"cuda_cores": [4, 2], "tensor_cores": [1, 3]}
+
+
+@pytest.mark.parametrize("kern", sorted(KERNELS))
+@pytest.mark.parametrize("nvec,nscal", [(3, 2), (4, 1), (1, 0), (0, 1), (2, 6)])
+def test_sht_fp64_matches_oracle(oracle_lib, case1, nvec, nscal, kern):
     g = SphMHD(case1, PREC_FP64)
+    g.tuning = KERNELS[kern]
     o = oracle_lib.Oracle(case1)
     nc = 3 * nvec + nscal
     zl0 = [3 * v + 1 for v in range(nvec)] + [3 * v + 2 for v in range(nvec)]
@@ -85,6 +92,31 @@ def test_dynamobench_case1_golden_energies(case1):
         assert rel.max() <= gold["rel_tol"], (row["step"], rel)
 
 
+def test_fp64_kernels_L127_match_oracle(oracle_lib):
+    """L127, 192 Gauss nodes (96 per hemisphere: one full and one partial
+    64-node tile of the tensor-core backward kernel; two 64-degree blocks,
+    the second partial, of the forward one), Nr 9 (a partial radial tile),
+    4 vectors + 1 scalar: both pairs of float64 Legendre kernels against the
+    oracle, backward and forward, 1e-12 relative L2 per component."""
+    p = configs.shell_params(127, 9, 192, 384, E=1e-4, Ra=300.0, dt=5e-6)
+    o = oracle_lib.Oracle(dict(p, nthreads=os.cpu_count() or 1))
+    nvec, nscal = 4, 1
+    nc = 3 * nvec + nscal
+    zl0 = [3 * v + 1 for v in range(nvec)] + [3 * v + 2 for v in range(nvec)]
+    spec = random_spec(127, 9, nc, 21, zero_l0=zl0)
+    grid_o = o.sht_backward(nvec, nscal, spec)
+    back_o = o.sht_forward(nvec, nscal, grid_o)
+    for kern in sorted(KERNELS):
+        g = SphMHD(p, PREC_FP64)
+        g.tuning = KERNELS[kern]
+        grid_g = g.sph_back_trans(nvec, nscal, spec)
+        back_g = g.sph_forward_trans(nvec, nscal, grid_o)
+        g.close()
+        for c in range(nc):
+            assert rel_l2(grid_g[c], grid_o[c]) < 1e-12, (kern, c, rel_l2(grid_g[c], grid_o[c]))
+            assert rel_l2(back_g[c], back_o[c]) < 1e-12, (kern, c, rel_l2(back_g[c], back_o[c]))
+
+
 def _compare_fields(g, o, tol):
     for slot in (VELO, VELO + 1, VELO + 2, VORT, VORT + 2, MAGNE, MAGNE + 1, MAGNE + 2,
                  CURRENT, CURRENT + 2, TEMP):
@@ -92,8 +124,10 @@ def _compare_fields(g, o, tol):
         assert rel_l2(a, b) < tol, (slot, rel_l2(a, b))
 
 
-def test_case1_fields_match_oracle(oracle_lib, case1):
+@pytest.mark.parametrize("kern", sorted(KERNELS))
+def test_case1_fields_match_oracle(oracle_lib, case1, kern):
     g = SphMHD(case1, PREC_FP64)
+    g.tuning = KERNELS[kern]
     o = oracle_lib.Oracle(case1)
     g.init_fields(1)
     o.init_fields(1)
