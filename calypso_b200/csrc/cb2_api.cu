@@ -350,6 +350,9 @@ int cb2_destroy(cb2_ctx *c) {
   if (c->h_stage) cudaFreeHost(c->h_stage);
   for (int i = 0; i < 64; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  for (cudaEvent_t e : c->copy_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -608,19 +611,50 @@ __global__ void k_add_l0(int nr, size_t jmax, const double *reft0, double *T, do
   if (k < nr) T[(size_t)k * jmax] += sign * reft0[k];   // host order: j = 0 is l = m = 0
 }
 
-// host restart state -> field slots (through the device staging d_host_state)
-static int load_restart(Ctx &c, const double *state) {
-  const size_t n = c.fsize(), bytes = 14 * n * sizeof(double);
+// host restart state -> field slots (through the device staging
+// d_host_state).  The first 7 entries are the state (velocity, temperature,
+// magnetic field), the last 7 the Adams-Bashforth history.  Two halves: the
+// state on the compute stream, and the history, which only the explicit
+// update reads, on the copy stream after it (started by
+// load_restart_state, placed in its slots by load_restart_history), so the
+// history crosses PCIe while the nonlinear terms of the state are computed.
+static int load_restart_state(Ctx &c, const double *state) {
+  const size_t n = c.fsize(), half = 7 * n * sizeof(double);
   if (!c.d_host_state) CB2_CUDA(cudaMalloc(&c.d_host_state, 20 * n * sizeof(double)));
-  CB2_CUDA(cudaMemcpyAsync(c.d_host_state, state, bytes, cudaMemcpyHostToDevice, c.stream));
+  if (!c.copy_stream) {
+    CB2_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : c.copy_ev) CB2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  CB2_CUDA(cudaMemcpyAsync(c.d_host_state, state, half, cudaMemcpyHostToDevice, c.stream));
+  // the history after the state (so the two do not share the link), and
+  // after this context's earlier work on the staging buffer
+  CB2_CUDA(cudaEventRecord(c.copy_ev[0], c.stream));
+  CB2_CUDA(cudaStreamWaitEvent(c.copy_stream, c.copy_ev[0], 0));
+  CB2_CUDA(cudaMemcpyAsync(c.d_host_state + 7 * n, state + 7 * n, half, cudaMemcpyHostToDevice, c.copy_stream));
+  CB2_CUDA(cudaEventRecord(c.copy_ev[1], c.copy_stream));
   // the total temperature back to the perturbation (sync_temp_by_per_temp_sph)
   if (c.p.use_ref_temp)
     k_add_l0<<<cdiv(c.nr, 128), 128, 0, c.stream>>>(c.nr, (size_t)c.jmax, c.d_reft0, c.d_host_state + 3 * n, -1.0);
-  for (int q = 0; q < 14; q++)
+  for (int q = 0; q < 7; q++)
     k_to_device_order<<<cdiv(n, 256), 256, 0, c.stream>>>(c.nr, c.jmax, c.d_perm, c.d_host_state + q * n,
                                                           c.fld(kRestartSlots[q]));
   CB2_CUDA(cudaGetLastError());
   return 0;
+}
+
+static int load_restart_history(Ctx &c) {
+  const size_t n = c.fsize();
+  CB2_CUDA(cudaStreamWaitEvent(c.stream, c.copy_ev[1], 0));
+  for (int q = 7; q < 14; q++)
+    k_to_device_order<<<cdiv(n, 256), 256, 0, c.stream>>>(c.nr, c.jmax, c.d_perm, c.d_host_state + q * n,
+                                                          c.fld(kRestartSlots[q]));
+  CB2_CUDA(cudaGetLastError());
+  return 0;
+}
+
+static int load_restart(Ctx &c, const double *state) {
+  int rc = load_restart_state(c, state);
+  return rc ? rc : load_restart_history(c);
 }
 
 static int store_restart(Ctx &c, double *state) {
@@ -725,10 +759,11 @@ int cb2_set_restart_state(cb2_ctx *c, const double *state, int istep) {
 int cb2_step_restart_state(cb2_ctx *c, double *state, double out_energies[7]) {
   if (!c || !state) return CB2_ERR_ARG;
   if (!c->started) { set_error("cb2_step_restart_state before cb2_start"); return CB2_ERR_STATE; }
-  int rc = load_restart(*c, state);
+  int rc = load_restart_state(*c, state);
   if (rc) return rc;
   rj_start_derived(*c);
   if ((rc = nonlinear(*c))) return rc;
+  if ((rc = load_restart_history(*c))) return rc;   // the history has crossed meanwhile
   c->istep = std::max(c->istep, 1) + 1;     // the loaded history makes this an Adams-Bashforth step
   cn_stage(*c, false);
   // the nonlinear terms of the new state are left to the next call (or to

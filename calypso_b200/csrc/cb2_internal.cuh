@@ -116,6 +116,10 @@ struct Ctx {
   size_t h_stage_bytes = 0;
   double *d_tmp = nullptr;               // nr*jmax scratch for host transfers
   double *d_host_state = nullptr;        // 20 slots for cb2_step_host_state
+  // copy stream of cb2_step_restart_state (the restart history uploads
+  // while the nonlinear terms of the state are computed) and its events
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_ev[2] = {nullptr, nullptr};
   // mixed-precision Legendre operands (split fp16) -- owned by cb2_legendre_mixed.cu
   void *mixed = nullptr;
   // learned subgrid closure attached to the step (cb2_closure.cu), or null
