@@ -420,9 +420,9 @@ def main():
     t_s = stages[top] * 1e-3
     achieved = traffic[top] / t_s / 1e9
     # DRAM bytes (read + write) of the dominant kernel from one ncu capture of
-    # the same kernel at L255 / Nr33 (614.6 MB per launch), scaled by the
+    # the same kernel at L255 / Nr33 (632.0 MB per launch), scaled by the
     # (theta, k) rows processed; other shapes have no capture
-    dram_per_row = {("fft_products", 255, 384, 768): 614_629_376 / (384 * 33)}
+    dram_per_row = {("fft_products", 255, 384, 768): (338_202_368 + 293_795_072) / (384 * 33)}
     dkey = (top, L, nth, nph)
     measured = dram_per_row[dkey] * nth * nr if (prec == PREC_MIXED and dkey in dram_per_row) else None
     roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
