@@ -576,16 +576,22 @@ k_leg_fwd_ws(const __grid_constant__ FwdShell one, const FwdShell *__restrict__ 
       fetch(0, n7, n6, nbu);
       for (int g = 0; g < ng; g++) {
         float f0[4], f1[4];
-        tmem_ld_16x256b_pair(tl + (uint32_t)(g * 8), tl + acc1 + (uint32_t)(g * 8), f0, f1);
-        // the two accumulators are added in float64: no rounding of the sum
         double p0[4], p1[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) { p0[j] = (double)f0[j]; p1[j] = (double)f1[j]; }
         if (split) {
+          // hi*hi' and cross-term accumulators of both parities, one wait;
+          // the two accumulators are added in float64: no rounding of the sum
           float x0[4], x1[4];
-          tmem_ld_16x256b_pair(tl + 2 * acc1 + (uint32_t)(g * 8), tl + 3 * acc1 + (uint32_t)(g * 8), x0, x1);
+          const uint32_t o = (uint32_t)(g * 8);
+          tmem_ld_16x256b_quad(tl + o, tl + acc1 + o, tl + 2 * acc1 + o, tl + 3 * acc1 + o, f0, f1, x0, x1);
 #pragma unroll
-          for (int j = 0; j < 4; j++) { p0[j] += (double)x0[j]; p1[j] += (double)x1[j]; }
+          for (int j = 0; j < 4; j++) {
+            p0[j] = (double)f0[j] + (double)x0[j];
+            p1[j] = (double)f1[j] + (double)x1[j];
+          }
+        } else {
+          tmem_ld_16x256b_pair(tl + (uint32_t)(g * 8), tl + acc1 + (uint32_t)(g * 8), f0, f1);
+#pragma unroll
+          for (int j = 0; j < 4; j++) { p0[j] = (double)f0[j]; p1[j] = (double)f1[j]; }
         }
         if (g == ng - 1) {
           tc_fence_before();

@@ -130,6 +130,27 @@ __device__ inline void tmem_ld_16x256b_pair(uint32_t ta, uint32_t tb, float va[4
   for (int i = 0; i < 4; i++) { va[i] = __uint_as_float(r[i]); vb[i] = __uint_as_float(r[4 + i]); }
 }
 
+// four 16x256b loads (layout as above) behind one wait
+__device__ inline void tmem_ld_16x256b_quad(uint32_t ta, uint32_t tb, uint32_t tc, uint32_t td, float va[4],
+                                            float vb[4], float vc[4], float vd[4]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.16x256b.x1.b32 {%0,%1,%2,%3}, [%16];\n\t"
+      "tcgen05.ld.sync.aligned.16x256b.x1.b32 {%4,%5,%6,%7}, [%17];\n\t"
+      "tcgen05.ld.sync.aligned.16x256b.x1.b32 {%8,%9,%10,%11}, [%18];\n\t"
+      "tcgen05.ld.sync.aligned.16x256b.x1.b32 {%12,%13,%14,%15}, [%19];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(ta), "r"(tb), "r"(tc), "r"(td)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    va[i] = __uint_as_float(r[i]); vb[i] = __uint_as_float(r[4 + i]);
+    vc[i] = __uint_as_float(r[8 + i]); vd[i] = __uint_as_float(r[12 + i]);
+  }
+}
+
 __device__ inline unsigned char *smem_base_1024(unsigned char *raw) {
   return (unsigned char *)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
 }
