@@ -96,10 +96,15 @@ __device__ inline void split_pair(float x0, float x1, uint32_t &hi, uint32_t &lo
 // remainder (|lo| <= 8, 11 bits of it kept, 2^-23 of the row maximum).  Every
 // product hi*hi' is then a multiple of 256 below 2^28, and an FP32
 // accumulator holds their sums exactly while they stay below 2^32.
+// The scalings by 2^-4 and 2^4 and the difference x - hi are exact, so the
+// packed float32x2 forms of sm_100 give the scalar results bit for bit.
 __device__ inline void split_pair_q(float x0, float x1, uint32_t &hi, uint32_t &lo) {
-  const float h0 = rintf(x0 * 0.0625f) * 16.0f, h1 = rintf(x1 * 0.0625f) * 16.0f;
-  const __half2 h = __floats2half2_rn(h0, h1);
-  const __half2 l = __floats2half2_rn(x0 - h0, x1 - h1);
+  const float2 x = make_float2(x0, x1);
+  const float2 s = __fmul2_rn(x, make_float2(0.0625f, 0.0625f));
+  const float2 hq = __fmul2_rn(make_float2(rintf(s.x), rintf(s.y)), make_float2(16.0f, 16.0f));
+  const float2 r = __ffma2_rn(hq, make_float2(-1.0f, -1.0f), x);
+  const __half2 h = __floats2half2_rn(hq.x, hq.y);
+  const __half2 l = __floats2half2_rn(r.x, r.y);
   hi = *reinterpret_cast<const uint32_t *>(&h);
   lo = *reinterpret_cast<const uint32_t *>(&l);
 }
@@ -664,10 +669,15 @@ struct PackArgs {
 __global__ void __launch_bounds__(256)
 k_pack_bwd(const __grid_constant__ PackArgs a) {
   extern __shared__ float T[];   // [kc * RK][NLP]
-  const int m = blockIdx.x, k0 = blockIdx.y * a.kc, nk = min(a.kc, a.nr - k0);
-  const int nl = a.L + 1 - m, NLP = nl | 1;
+  const int k0 = blockIdx.y * a.kc, nk = min(a.kc, a.nr - k0);
   const int RP = 2 * a.ng, RD = 4 * a.nvec, RK = RP + RD;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  // orders m and L - m in one block: L + 2 degrees of work in every block
+  for (int pass = 0; pass < 2; pass++) {
+  const int m = pass ? a.L - (int)blockIdx.x : (int)blockIdx.x;
+  if (pass && m <= (int)blockIdx.x) break;
+  if (pass) __syncthreads();   // the first order's rows are read out of T
+  const int nl = a.L + 1 - m, NLP = nl | 1;
   const int jm = a.moff[m];
   // rows in: one warp per (radial level, row), lanes along l (coalesced
   // float64 reads, 256 degrees per pass with all loads in flight together),
@@ -739,6 +749,7 @@ k_pack_bwd(const __grid_constant__ PackArgs a) {
       float *dst = a.rlmD + base * a.pitchD + (size_t)k0 * RD + rr;
       for (int kk = warp; kk < cnt; kk += nw) dst[(size_t)kk * a.pitchD] = tr[2 * kk];
     }
+  }
   }
 }
 
@@ -1535,7 +1546,7 @@ int leg_bwd_pack(Ctx &c, const int *slots, const MLayout &out) {
   pk.rlmP = t->rlmP; pk.rlmD = t->rlmD; pk.pitchP = pitchP; pk.pitchD = pitchD;
   pk.kbase = t->kbase; pk.maxP = t->maxP; pk.maxD = t->maxD;
   const size_t smp = (size_t)pk.kc * (2 * ng + 4 * nvec) * ((c.L + 1) | 1) * sizeof(float);
-  k_pack_bwd<<<dim3(c.L + 1, cdiv(c.nr, pk.kc)), 256, smp, c.stream>>>(pk);
+  k_pack_bwd<<<dim3((c.L + 2) / 2, cdiv(c.nr, pk.kc)), 256, smp, c.stream>>>(pk);
   return 0;
 }
 
