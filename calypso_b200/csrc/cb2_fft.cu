@@ -882,15 +882,17 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
   using P = F4Plan<R1, R2>;
   constexpr int M = P::M, N = P::N, TP = P::TP, TG = P::TG, MP2 = P::MP2, WP = P::WP;
   extern __shared__ __align__(16) unsigned char smraw[];
-  float2 *S2 = reinterpret_cast<float2 *>(smraw);                  // [14][MP2] (a_m, b_m), row 13 zero
+  // input staging [7 pairs][MP2][2]: the (a_m, b_m) of components 2p and
+  // 2p + 1 side by side (component 13 zero), so one 16-byte load reads both
+  float2 *S2 = reinterpret_cast<float2 *>(smraw);
   float2 *X = reinterpret_cast<float2 *>(smraw + (size_t)P::SF * 4);   // transposes / grid rows / F_r
   float2 *TW3 = X + P::X;                                          // [3][M]
   float2 *TWM = TW3 + 3 * M;                                       // [R2][WP]
   const int th = blockIdx.x / fin.nr, k = blockIdx.x % fin.nr;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = F4_THREADS / 32;
   const int grp = tid >> 4, lt = tid & 15;
-  for (int e = tid; e < 14; e += F4_THREADS) S2[e * MP2 + M] = float2{0.0f, 0.0f};
-  for (int e = tid; e < M; e += F4_THREADS) S2[13 * MP2 + e] = float2{0.0f, 0.0f};
+  for (int e = tid; e < 14; e += F4_THREADS) S2[((e >> 1) * MP2 + M) * 2 + (e & 1)] = float2{0.0f, 0.0f};
+  for (int e = tid; e < M; e += F4_THREADS) S2[(6 * MP2 + e) * 2 + 1] = float2{0.0f, 0.0f};
   // input and tables by asynchronous 8-byte copies, all in flight at once.
   // At one (theta, k) an order m has 13 (cos, sin) pairs: a run of 5 in the
   // P block and one of 8 in the D block; half-warp h of warp w copies the
@@ -917,7 +919,7 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
     }
     if (j < 13)
       for (int m = 2 * warp + hw; m < M; m += 2 * nwarp) {
-        const uint32_t d = (uint32_t)__cvta_generic_to_shared(S2 + c * MP2 + m);
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(S2 + ((c >> 1) * MP2 + m) * 2 + (c & 1));
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src + m * mst) : "memory");
       }
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
@@ -926,7 +928,7 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
   const int gp = grp / 3, gr = grp - 3 * gp;   // pair, residue of this group
   // ---- backward, step 1: column n2 = lt, pair rows built from the staging
   if (grp < 21 && lt < R2) {
-    const float2 *x0 = S2 + (2 * gp) * MP2, *y0 = S2 + (2 * gp + 1) * MP2;
+    const float4 *xy = reinterpret_cast<const float4 *>(S2) + gp * MP2;   // (x_m, y_m) of the pair
     const float2 om = (gr == 0) ? float2{1.0f, 0.0f}
                     : float2{-0.5f, (gr == 1) ? -0.86602540378443864676f : 0.86602540378443864676f};
     const float2 *tw = TW3 + gr * M;
@@ -934,7 +936,8 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
 #pragma unroll
     for (int n1 = 0; n1 < R1; n1++) {
       const int m = n1 * R2 + lt, mq = M - m;
-      const float2 a = x0[m], b = y0[m], c = x0[mq], d = y0[mq];
+      const float4 ab = xy[m], cd = xy[mq];
+      const float2 a = float2{ab.x, ab.y}, b = float2{ab.z, ab.w}, c = float2{cd.x, cd.y}, d = float2{cd.z, cd.w};
       float2 zm = float2{a.x + b.y, b.x - a.y};           // 2 Z[m]
       const float2 zp = float2{c.x - d.y, c.y + d.x};     // 2 Z[N - (M - m)] (zero at m = 0)
       if (n1 == 0 && lt == 0) zm = float2{2.0f * a.x, 2.0f * b.x};   // 2 Z[0] = 2 (a_0, a'_0)
@@ -1014,22 +1017,37 @@ k_fft_products_4s(MLayout fin, MLayout fout, const float2 *__restrict__ tables, 
   __syncthreads();
   // ---- combine the residues: Z[m], Z[N - m] -> (a_m, b_m) of both
   // components of each pair, into the output staging rows [c][MP2] of
-  // (a_m, b_m) pairs
+  // (a_m, b_m) pairs.  A thread takes the orders m and M - m together: both
+  // read the same six F values.
   float2 *O2 = S2;
   {
     const float an = 1.0f / (float)N;
-    for (int idx = tid; idx < 6 * M; idx += F4_THREADS) {
-      const int p = idx / M, m = idx - p * M, mm = (M - m) & (M - 1);
-      const float2 *F = X + p * 3 * M;
-      const float2 t1 = TW3[M + m], t2 = TW3[2 * M + m];
-      const float2 zk = cadd(F[m], cadd(cmulc(F[M + m], t1), cmulc(F[2 * M + m], t2)));
-      const float2 zn = cadd(F[mm], cadd(cmulf(F[M + mm], t1), cmulf(F[2 * M + mm], t2)));
-      float2 *o0 = O2 + (2 * p) * MP2, *o1 = o0 + MP2;
+    constexpr int MH = M / 2 + 1;
+    auto out = [&](float2 *o0, float2 *o1, int m, float2 zk, float2 zn) {
       if (m == 0) {
         o0[0] = float2{an * zk.x, 0.0f}; o1[0] = float2{an * zk.y, 0.0f};
       } else {
         o0[m] = float2{an * (zk.x + zn.x), -an * (zk.y - zn.y)};
         o1[m] = float2{an * (zk.y + zn.y), an * (zk.x - zn.x)};
+      }
+    };
+    for (int idx = tid; idx < 6 * MH; idx += F4_THREADS) {
+      const int p = idx / MH, m = idx - p * MH, mm = (M - m) & (M - 1);
+      const float2 *F = X + p * 3 * M;
+      float2 *o0 = O2 + (2 * p) * MP2, *o1 = o0 + MP2;
+      const float2 f0 = F[m], f1 = F[M + m], f2 = F[2 * M + m];
+      const float2 g0 = F[mm], g1 = F[M + mm], g2 = F[2 * M + mm];
+      {
+        const float2 t1 = TW3[M + m], t2 = TW3[2 * M + m];
+        const float2 zk = cadd(f0, cadd(cmulc(f1, t1), cmulc(f2, t2)));
+        const float2 zn = cadd(g0, cadd(cmulf(g1, t1), cmulf(g2, t2)));
+        out(o0, o1, m, zk, zn);
+      }
+      if (m > 0 && mm != m) {   // the partner order M - m
+        const float2 t1 = TW3[M + mm], t2 = TW3[2 * M + mm];
+        const float2 zk = cadd(g0, cadd(cmulc(g1, t1), cmulc(g2, t2)));
+        const float2 zn = cadd(f0, cadd(cmulf(f1, t1), cmulf(f2, t2)));
+        out(o0, o1, mm, zk, zn);
       }
     }
   }

@@ -669,15 +669,10 @@ struct PackArgs {
 __global__ void __launch_bounds__(256)
 k_pack_bwd(const __grid_constant__ PackArgs a) {
   extern __shared__ float T[];   // [kc * RK][NLP]
-  const int k0 = blockIdx.y * a.kc, nk = min(a.kc, a.nr - k0);
+  const int m = blockIdx.x, k0 = blockIdx.y * a.kc, nk = min(a.kc, a.nr - k0);
+  const int nl = a.L + 1 - m, NLP = nl | 1;
   const int RP = 2 * a.ng, RD = 4 * a.nvec, RK = RP + RD;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  // orders m and L - m in one block: L + 2 degrees of work in every block
-  for (int pass = 0; pass < 2; pass++) {
-  const int m = pass ? a.L - (int)blockIdx.x : (int)blockIdx.x;
-  if (pass && m <= (int)blockIdx.x) break;
-  if (pass) __syncthreads();   // the first order's rows are read out of T
-  const int nl = a.L + 1 - m, NLP = nl | 1;
   const int jm = a.moff[m];
   // rows in: one warp per (radial level, row), lanes along l (coalesced
   // float64 reads, 256 degrees per pass with all loads in flight together),
@@ -749,7 +744,6 @@ k_pack_bwd(const __grid_constant__ PackArgs a) {
       float *dst = a.rlmD + base * a.pitchD + (size_t)k0 * RD + rr;
       for (int kk = warp; kk < cnt; kk += nw) dst[(size_t)kk * a.pitchD] = tr[2 * kk];
     }
-  }
   }
 }
 
@@ -1546,7 +1540,7 @@ int leg_bwd_pack(Ctx &c, const int *slots, const MLayout &out) {
   pk.rlmP = t->rlmP; pk.rlmD = t->rlmD; pk.pitchP = pitchP; pk.pitchD = pitchD;
   pk.kbase = t->kbase; pk.maxP = t->maxP; pk.maxD = t->maxD;
   const size_t smp = (size_t)pk.kc * (2 * ng + 4 * nvec) * ((c.L + 1) | 1) * sizeof(float);
-  k_pack_bwd<<<dim3((c.L + 2) / 2, cdiv(c.nr, pk.kc)), 256, smp, c.stream>>>(pk);
+  k_pack_bwd<<<dim3(c.L + 1, cdiv(c.nr, pk.kc)), 256, smp, c.stream>>>(pk);
   return 0;
 }
 
