@@ -226,7 +226,8 @@ def stage_dict(st, tuning):
     """Stage names of cb2_stage_times ids (the reference's timer labels)."""
     d = ({"cn_step": st[6] + st[7]} if tuning[4] == 1 else
          {"explicit": st[6], "implicit+rj_derived": st[7]})
-    d.update({"coriolis": st[13], "legendre_bwd": st[22], "fft_products": st[24],
+    # (the Coriolis term is evaluated inside rj_after_transform)
+    d.update({"legendre_bwd": st[22], "fft_products": st[24],
               "legendre_fwd": st[23], "rj_after_transform": st[17], "step": st[0]})
     return d
 

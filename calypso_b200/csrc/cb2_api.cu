@@ -126,14 +126,14 @@ static const int kFwdSlots[4] = {MADV, LOR, VPIND, HFLUX};
 
 // The nonlinear terms in three parts around the mixed path's two
 // tensor-core Legendre GEMMs:
-//   head: Coriolis; mixed: the spectra packed for the backward GEMM
+//   head: mixed: the spectra packed for the backward GEMM
 //   grid: mixed: FFT + grid products, the forward GEMM's row scales
-//   tail: rj operators after the forward transform, closure
+//   tail: rj operators after the forward transform (with the Coriolis
+//         term), closure
 // nonlinear() launches this shell's GEMMs between them; an ensemble
 // launches each GEMM once for all its shells (step_phase).
 static int nl_head(Ctx &c) {
   if (c.timers) cudaEventRecord(c.ev[10], c.stream);
-  rj_coriolis(c);
   if (c.timers) cudaEventRecord(c.ev[11], c.stream);
   if (c.prec == CB2_PREC_MIXED) return leg_bwd_pack(c, kBwdSlots, mlayout(c, c.d_four, 4, 1));
   return 0;

@@ -188,7 +188,6 @@ template <typename T> void fft_forward_grid(Ctx &c, int ncomp, const double *gri
 // rj operators and solves (cb2_rj.cu)
 void rj_explicit(Ctx &c, bool euler);
 void rj_implicit(Ctx &c);
-void rj_coriolis(Ctx &c);
 void rj_after_transform(Ctx &c);
 void rj_start_derived(Ctx &c);
 void rj_temp_total(Ctx &c, double sign);

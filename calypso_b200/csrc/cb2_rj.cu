@@ -772,15 +772,22 @@ __global__ void k_derived_b(RJArgs a, Fields F) {
 }
 
 // Coriolis term (sum_rot_coriolis_rlm_10): one thread per (k, jj)
-__global__ void k_coriolis(RJArgs a, Fields F, const int *jgi1, const int *jgi2, const int *jei1,
-                           const double *sw, const double *tw) {
-  // grid (jj blocks, radial level k): no division to find k and jj
-  const int jj = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
-  if (jj >= a.jmax) return;
-  const size_t idx = (size_t)k * a.jmax + jj;
+// The Coriolis term at (k, jj) in spectral space, rotation form
+// (sum_rot_coriolis_rlm_10): Gaunt / Elsasser couplings of the velocity and
+// vorticity at l +- 1; the poloidal (rc0) and toroidal (rc2) parts.  It is
+// evaluated where the force sum consumes it (k_after_transform); nothing
+// changes the state between the solve and that kernel.
+struct CorTables {
+  const int *jgi1, *jgi2, *jei1;
+  const double *sw, *tw;   // [6][jmax], [8][jmax]
+};
+
+__device__ inline void coriolis_terms(const RJArgs &a, const Fields &F, const CorTables &ct, int jj, int k,
+                                      double &rc0, double &rc2) {
   size_t base = (size_t)k * a.jmax, J = a.jmax;
   const double *vS = F(VELO), *vdS = F(VELO + 1), *wS = F(VORT), *wdS = F(VORT + 1), *wT = F(VORT + 2);
-  size_t i11 = base + jgi1[jj], i21 = base + jgi2[jj], i12 = base + jei1[jj];
+  const double *sw = ct.sw, *tw = ct.tw;
+  size_t i11 = base + ct.jgi1[jj], i21 = base + ct.jgi2[jj], i12 = base + ct.jei1[jj];
   double a1 = a.ar1[k], o0 = a.om[k], o1 = a.om[a.nr + k], o2 = a.om[2 * a.nr + k];
   double d2vp_l1 = a1 * a1 * a.g3rlm[jj] * vS[i12] - wT[i12];
   double dwp1 = wdS[i11] - 2.0 * a1 * wS[i11];
@@ -791,15 +798,14 @@ __global__ void k_coriolis(RJArgs a, Fields F, const int *jgi1, const int *jgi2,
   double t = tw[0 * J + jj] * o0 * d2vp_l1 - tw[2 * J + jj] * o2 * vS[i12]
            + tw[4 * J + jj] * o1 * wS[i11] + tw[5 * J + jj] * o1 * wS[i21]
            + tw[6 * J + jj] * o0 * dwp1 + tw[7 * J + jj] * o0 * dwp2;
-  F(ROTCOR)[idx] = -a.coef_cor * p * a1 * a1;
-  F(ROTCOR + 1)[idx] = 0.0;
-  F(ROTCOR + 2)[idx] = -a.coef_cor * t * a1 * a1;
+  rc0 = -a.coef_cor * p * a1 * a1;
+  rc2 = -a.coef_cor * t * a1 * a1;
 }
 
 // curl / divergence of the transformed forces and the force sum
 // (const_sph_force_rot2, const_sph_rotation_uxb, const_sph_scalar_advect,
 //  add_reftemp_advect_sph_MHD, set_MHD_terms_to_force)
-__global__ void k_after_transform(RJArgs a, Fields F) {
+__global__ void k_after_transform(RJArgs a, Fields F, CorTables ct) {
   // grid (jj blocks, radial level k): no division to find k and jj
   const int jj = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
   if (jj >= a.jmax) return;
@@ -864,8 +870,10 @@ __global__ void k_after_transform(RJArgs a, Fields F) {
       h = h + a.coef_temp * g3 * a.ar2[k] * a.reft1[k] * F(VELO)[idx];
     F(HADV)[idx] = h;
   }
-  F(FORCES)[idx] = -rot[0][0] + F(ROTCOR)[idx] + rot[1][0];
-  F(FORCES + 2)[idx] = -rot[0][2] + F(ROTCOR + 2)[idx] + rot[1][2] + F(ROTBUO + 2)[idx];
+  double rc0, rc2;
+  coriolis_terms(a, F, ct, jj, k, rc0, rc2);
+  F(FORCES)[idx] = -rot[0][0] + rc0 + rot[1][0];
+  F(FORCES + 2)[idx] = -rot[0][2] + rc2 + rot[1][2] + F(ROTBUO + 2)[idx];
 }
 
 __global__ void k_temp_total(RJArgs a, Fields F, double sign) {
@@ -946,13 +954,9 @@ void rj_start_derived(Ctx &c) {
   k_derived_b<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(a, fields(c));
 }
 
-void rj_coriolis(Ctx &c) {
-  k_coriolis<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(c.rj_args(), fields(c), c.d_jgi1, c.d_jgi2,
-                                                           c.d_jei1, c.d_sw, c.d_tw);
-}
-
 void rj_after_transform(Ctx &c) {
-  k_after_transform<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(c.rj_args(), fields(c));
+  const CorTables ct{c.d_jgi1, c.d_jgi2, c.d_jei1, c.d_sw, c.d_tw};
+  k_after_transform<<<dim3(cdiv(c.jmax, kThreads), c.nr), kThreads, 0, c.stream>>>(c.rj_args(), fields(c), ct);
 }
 
 void rj_temp_total(Ctx &c, double sign) {
