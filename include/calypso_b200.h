@@ -362,8 +362,10 @@ int cb2_closure_attach(cb2_ctx *ctx, cb2_mlp *net, const float *norm);
 /* CUDA-event time of the last cb2_step/cb2_step_graph call, per stage
  * (stage ids follow the reference's elapsed-time labels of
  * MHD_src/IO/init_sph_MHD_elapsed_label.f90: 6 explicit, 7 implicit,
- * 22 Legendre backward, 23 Legendre forward, 24 FFT+products, 13 Coriolis,
- * 17 rj operators).  ms[0..31]; only filled when CB2_TIMERS=1 in the env. */
+ * 22 Legendre backward, 23 Legendre forward, 24 FFT+products, 17 rj
+ * operators with the Coriolis term; 13, the reference's Coriolis label,
+ * stays zero since the term is computed inside 17).  ms[0..31]; only
+ * filled when CB2_TIMERS=1 in the env. */
 int cb2_stage_times(cb2_ctx *ctx, double ms[32]);
 
 #ifdef __cplusplus
