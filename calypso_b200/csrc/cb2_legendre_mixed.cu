@@ -257,6 +257,54 @@ __device__ inline const S &shell_of(const S *tab, int nsh, int t) {
   return tab[lo];
 }
 
+// Accumulator schedule of a forward CTA, stepped tile by tile in the same
+// way by the MMA thread and by the epilogue warps.  With two accumulator
+// sets the tiles alternate between them.  With one set of four 128-column
+// accumulators (the split layout at L255: 512 columns), a tile whose
+// accumulators fit in 64 columns takes one half of tensor memory, the halves
+// alternating, so its epilogue overlaps the next such tile's MMAs; a wider
+// tile takes both halves.  Per half: how often it has been taken (the MMA
+// waits for the previous release); per full barrier: how often committed.
+struct AccSched {
+  int dyn, next;
+  uint32_t acq0, acq1, full0, full1;
+};
+struct AccUse {
+  int nh, h0, sfull, wait0, wait1;   // halves h0 (and 1 when nh = 2)
+  uint32_t par0, par1, full_par, base, acc1;
+};
+__device__ inline AccUse acc_take(AccSched &st, int nacc, bool narrow, uint32_t accw, uint32_t acc1) {
+  AccUse u;
+  if (nacc == 2 || (st.dyn && narrow)) {
+    const int s = st.next;
+    st.next ^= 1;
+    u.nh = 1; u.h0 = s;
+    u.base = (uint32_t)s * (nacc == 2 ? accw : 256u);
+    u.acc1 = (nacc == 2) ? acc1 : 64u;
+  } else {
+    u.nh = st.dyn ? 2 : 1; u.h0 = 0;
+    u.base = 0; u.acc1 = acc1;
+  }
+  const uint32_t a0 = u.h0 ? st.acq1 : st.acq0;
+  u.wait0 = a0 > 0;
+  u.par0 = (a0 - 1) & 1;
+  if (u.h0) st.acq1++;
+  else st.acq0++;
+  u.wait1 = 0;
+  u.par1 = 0;
+  if (u.nh == 2) {   // a wide tile also takes half 1
+    u.wait1 = st.acq1 > 0;
+    u.par1 = (st.acq1 - 1) & 1;
+    st.acq1++;
+  }
+  u.sfull = u.h0;
+  const uint32_t f = u.h0 ? st.full1 : st.full0;
+  u.full_par = f & 1;
+  if (u.h0) st.full1++;
+  else st.full0++;
+  return u;
+}
+
 // a tensor map written to device memory by the host: order that write
 // before the tensor-map proxy reads it
 __device__ inline void tensormap_acquire(const CUtensorMap *tm) {
@@ -287,6 +335,9 @@ k_leg_fwd_ws(const __grid_constant__ FwdShell one, const FwdShell *__restrict__ 
   // accumulators at 2 acc1 and 3 acc1
   const int split = one.a.split;
   const uint32_t acc1 = split ? accw / 4 : accw / 2;
+  // one set of four 128-column accumulators over all of tensor memory: tiles
+  // whose accumulators fit in 64 columns take alternate halves (AccSched)
+  const int dyn = (nacc == 1 && split && tmem_cols >= 512 && acc1 >= 128) ? 1 : 0;
   const unsigned long long wait_ns = one.a.wait_ns;
   auto shell = [&](int t) -> const FwdShell & { return MULTI ? shell_of(tab, nsh, t) : one; };
 
@@ -386,14 +437,17 @@ k_leg_fwd_ws(const __grid_constant__ FwdShell one, const FwdShell *__restrict__ 
       uint32_t nab = 0;
       bool bad = false, any = false;
       int i = 0;
+      AccSched sched{dyn, 0, 0, 0, 0, 0};
       for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x, i++) {
         if (ws_aborted(sb)) { bad = true; break; }
         const FwdShell &sh = shell(t);
         const FwdTile q = fwd_tile(sh.a, t - sh.tile0, sh.rows_g0, sh.rows_g1, sh.tiles_g0, sh.tiles_g1);
-        const int ab = i % nacc;
-        if (i >= nacc && !mbar_wait(&sb->accempty[ab], ((i / nacc) - 1) & 1, wait_ns)) { bad = true; break; }
+        const AccUse u = acc_take(sched, nacc, max(q.npad0, q.npad1) <= 64, accw, acc1);
+        if (u.wait0 && !mbar_wait(&sb->accempty[u.h0], u.par0, wait_ns)) bad = true;
+        if (!bad && u.wait1 && !mbar_wait(&sb->accempty[1], u.par1, wait_ns)) bad = true;
+        if (bad) break;
         tc_fence_after();
-        const uint32_t accb = tmem + (uint32_t)ab * accw;
+        const uint32_t accb = tmem + u.base;
         for (int b = 0; b < q.NB; b++) {
           const uint32_t s = nab % FAB, ph = (nab / FAB) & 1;
           if (!mbar_wait(&sb->afull[s], ph, wait_ns) || !mbar_wait(&sb->bfull[s], ph, wait_ns)) { bad = true; break; }
@@ -405,11 +459,11 @@ k_leg_fwd_ws(const __grid_constant__ FwdShell one, const FwdShell *__restrict__ 
             const uint32_t idesc = idesc_f16_f32(TM, npad);
             const uint64_t dah = smem_desc_sw64(at + (2 * p) * FA_BYTES), dal = smem_desc_sw64(at + (2 * p + 1) * FA_BYTES);
             const uint64_t dbh = smem_desc_sw64(bb + (2 * p) * B_BYTES), dbl = smem_desc_sw64(bb + (2 * p + 1) * B_BYTES);
-            const uint32_t acc = accb + (p ? acc1 : 0u);
+            const uint32_t acc = accb + (p ? u.acc1 : 0u);
             // split: hi*hi' (on the fixed grid, summed exactly) in its own
             // accumulator, the cross terms and lo*lo' (2^-11 and 2^-22 of
             // it) in the second
-            const uint32_t accx = split ? acc + 2 * acc1 : acc;
+            const uint32_t accx = split ? acc + 2 * u.acc1 : acc;
 #pragma unroll
             for (int ks = 0; ks < FKB / 16; ks++) {
               const uint64_t o = (uint64_t)(ks * 2);
@@ -425,7 +479,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdShell one, const FwdShell *__restrict__ 
           nab++;
         }
         if (bad) break;
-        mma_commit(&sb->accfull[ab]);
+        mma_commit(&sb->accfull[u.sfull]);
       }
       // no MMA may still run when the CTA releases its tensor memory
       if (any) {
@@ -524,6 +578,7 @@ k_leg_fwd_ws(const __grid_constant__ FwdShell one, const FwdShell *__restrict__ 
     double *mc = reinterpret_cast<double *>(moff + 16);                           // [16]
     int *mg = reinterpret_cast<int *>(mc + 16);                                   // [16]
     int i = 0;
+    AccSched sched{dyn, 0, 0, 0, 0, 0};
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
       if (__any_sync(0xffffffffu, ws_aborted(sb))) break;
       const FwdShell &sh = shell(t);
@@ -559,11 +614,12 @@ k_leg_fwd_ws(const __grid_constant__ FwdShell one, const FwdShell *__restrict__ 
         }
         moff[lane] = off; mc[lane] = cr; mg[lane] = sel;
       }
-      const int ab = i % nacc;
-      const bool ok = mbar_wait(&sb->accfull[ab], (i / nacc) & 1, wait_ns);
+      const AccUse u = acc_take(sched, nacc, max(q.npad0, q.npad1) <= 64, accw, acc1);
+      const uint32_t acc1 = u.acc1;
+      const bool ok = mbar_wait(&sb->accfull[u.sfull], u.full_par, wait_ns);
       if (!__all_sync(0xffffffffu, ok)) { sb->abort = 1; break; }
       tc_fence_after();
-      const uint32_t tl = tmem + (uint32_t)ab * accw + ((uint32_t)(qd * 32 + hf * 16) << 16);
+      const uint32_t tl = tmem + u.base + ((uint32_t)(qd * 32 + hf * 16) << 16);
       const int ng = (nl + 15) / 16, j0 = a.moff[q.m];
       const float *bun0 = a.bunscale + ((size_t)q.g * (a.L + 1) * 2 + q.m * 2) * a.NFmax, *bun1 = bun0 + a.NFmax;
       // degree factors of degree 16 g + lc (this lane's column), a group ahead
@@ -601,7 +657,10 @@ k_leg_fwd_ws(const __grid_constant__ FwdShell one, const FwdShell *__restrict__ 
         if (g == ng - 1) {
           tc_fence_before();
           __syncwarp();
-          if (lane == 0) mbar_arrive(&sb->accempty[ab]);
+          if (lane == 0) {
+            mbar_arrive(&sb->accempty[u.h0]);
+            if (u.nh == 2) mbar_arrive(&sb->accempty[1]);
+          }
         }
         const double c7 = n7 * (double)nbu, c6 = n6 * (double)nbu;
         fetch(g + 1, n7, n6, nbu);
