@@ -161,7 +161,8 @@ constexpr int FAB = 2;   // A/B stages
 //   warp 16     TMA producer (raw rows and basis tiles)
 //   warp 17     MMA issuer (tcgen05, one elected thread)
 // Two TMEM accumulator sets (when they fit) let the epilogue of one tile
-// overlap the main loop of the next.
+// overlap the main loop of the next; with one set, the tiles narrow enough
+// for half of tensor memory alternate between the halves (AccSched).
 constexpr int FW_CONV = 256, FW_EPI = 256, FW_THREADS = FW_CONV + FW_EPI + 64;
 constexpr int FW_PROD_WARP = (FW_CONV + FW_EPI) / 32, FW_MMA_WARP = FW_PROD_WARP + 1;
 
