@@ -611,6 +611,28 @@ __global__ void k_add_l0(int nr, size_t jmax, const double *reft0, double *T, do
   if (k < nr) T[(size_t)k * jmax] += sign * reft0[k];   // host order: j = 0 is l = m = 0
 }
 
+// Restart entries a step never writes: the dS/dr components of
+// previous_momentum and previous_induction (entries 8 and 11; the explicit
+// update keeps only the poloidal and toroidal history).  A host that keeps
+// the restart set already holds their values after the step.
+static bool restart_entry_kept(int q) { return q == 8 || q == 11; }
+
+// consecutive runs [run[i][0], run[i][1]) of restart entries in [lo, hi)
+// that a step reads (kept = false) or keeps (kept = true), for one copy per
+// run; returns the number of runs
+static int restart_runs(int lo, int hi, bool kept, int (&run)[14][2]) {
+  int nrun = 0;
+  for (int q = lo; q < hi;) {
+    if (restart_entry_kept(q) != kept) { q++; continue; }
+    int q1 = q;
+    while (q1 < hi && restart_entry_kept(q1) == kept) q1++;
+    run[nrun][0] = q;
+    run[nrun++][1] = q1;
+    q = q1;
+  }
+  return nrun;
+}
+
 // host restart state -> field slots (through the device staging
 // d_host_state).  The first 7 entries are the state (velocity, temperature,
 // magnetic field), the last 7 the Adams-Bashforth history.  Two halves: the
@@ -618,6 +640,8 @@ __global__ void k_add_l0(int nr, size_t jmax, const double *reft0, double *T, do
 // update reads, on the copy stream after it (started by
 // load_restart_state, placed in its slots by load_restart_history), so the
 // history crosses PCIe while the nonlinear terms of the state are computed.
+// Within the history the five entries the step reads go first (copy_ev[1]),
+// the two it keeps after them (copy_ev[2]).
 static int load_restart_state(Ctx &c, const double *state) {
   const size_t n = c.fsize(), half = 7 * n * sizeof(double);
   if (!c.d_host_state) CB2_CUDA(cudaMalloc(&c.d_host_state, 20 * n * sizeof(double)));
@@ -630,8 +654,14 @@ static int load_restart_state(Ctx &c, const double *state) {
   // after this context's earlier work on the staging buffer
   CB2_CUDA(cudaEventRecord(c.copy_ev[0], c.stream));
   CB2_CUDA(cudaStreamWaitEvent(c.copy_stream, c.copy_ev[0], 0));
-  CB2_CUDA(cudaMemcpyAsync(c.d_host_state + 7 * n, state + 7 * n, half, cudaMemcpyHostToDevice, c.copy_stream));
-  CB2_CUDA(cudaEventRecord(c.copy_ev[1], c.copy_stream));
+  int run[14][2];
+  for (int kept = 0; kept < 2; kept++) {
+    for (int i = 0, nrun = restart_runs(7, 14, kept, run); i < nrun; i++)
+      CB2_CUDA(cudaMemcpyAsync(c.d_host_state + run[i][0] * n, state + run[i][0] * n,
+                               (run[i][1] - run[i][0]) * n * sizeof(double), cudaMemcpyHostToDevice,
+                               c.copy_stream));
+    CB2_CUDA(cudaEventRecord(c.copy_ev[1 + kept], c.copy_stream));
+  }
   // the total temperature back to the perturbation (sync_temp_by_per_temp_sph)
   if (c.p.use_ref_temp)
     k_add_l0<<<cdiv(c.nr, 128), 128, 0, c.stream>>>(c.nr, (size_t)c.jmax, c.d_reft0, c.d_host_state + 3 * n, -1.0);
@@ -642,31 +672,46 @@ static int load_restart_state(Ctx &c, const double *state) {
   return 0;
 }
 
-static int load_restart_history(Ctx &c) {
+// the history entries the step reads (kept = false, after copy_ev[1]) or
+// keeps (kept = true, after copy_ev[2]) into their slots
+static int load_restart_history(Ctx &c, bool kept) {
   const size_t n = c.fsize();
-  CB2_CUDA(cudaStreamWaitEvent(c.stream, c.copy_ev[1], 0));
+  CB2_CUDA(cudaStreamWaitEvent(c.stream, c.copy_ev[kept ? 2 : 1], 0));
   for (int q = 7; q < 14; q++)
-    k_to_device_order<<<cdiv(n, 256), 256, 0, c.stream>>>(c.nr, c.jmax, c.d_perm, c.d_host_state + q * n,
-                                                          c.fld(kRestartSlots[q]));
+    if (restart_entry_kept(q) == kept)
+      k_to_device_order<<<cdiv(n, 256), 256, 0, c.stream>>>(c.nr, c.jmax, c.d_perm, c.d_host_state + q * n,
+                                                            c.fld(kRestartSlots[q]));
   CB2_CUDA(cudaGetLastError());
   return 0;
 }
 
 static int load_restart(Ctx &c, const double *state) {
   int rc = load_restart_state(c, state);
-  return rc ? rc : load_restart_history(c);
+  if (!rc) rc = load_restart_history(c, false);
+  return rc ? rc : load_restart_history(c, true);
 }
 
-static int store_restart(Ctx &c, double *state) {
-  const size_t n = c.fsize(), bytes = 14 * n * sizeof(double);
+// field slots -> host restart state.  After a cb2_step_restart_state step
+// (after_step) the two entries the step keeps are not copied back (the host
+// holds them already); their upload, which trails the rest of the history,
+// is placed in its slots while the other twelve come down.
+static int store_restart(Ctx &c, double *state, bool after_step = false) {
+  const size_t n = c.fsize();
   if (!c.d_host_state) CB2_CUDA(cudaMalloc(&c.d_host_state, 20 * n * sizeof(double)));
   for (int q = 0; q < 14; q++)
-    k_to_host_order<<<cdiv(n, 256), 256, 0, c.stream>>>(c.nr, c.jmax, c.d_perm, c.fld(kRestartSlots[q]),
-                                                        c.d_host_state + q * n);
+    if (!after_step || !restart_entry_kept(q))
+      k_to_host_order<<<cdiv(n, 256), 256, 0, c.stream>>>(c.nr, c.jmax, c.d_perm, c.fld(kRestartSlots[q]),
+                                                          c.d_host_state + q * n);
   if (c.p.use_ref_temp)
     k_add_l0<<<cdiv(c.nr, 128), 128, 0, c.stream>>>(c.nr, (size_t)c.jmax, c.d_reft0, c.d_host_state + 3 * n, 1.0);
   CB2_CUDA(cudaGetLastError());
-  CB2_CUDA(cudaMemcpyAsync(state, c.d_host_state, bytes, cudaMemcpyDeviceToHost, c.stream));
+  int run[14][2] = {{0, 14}};
+  const int nrun = after_step ? restart_runs(0, 14, false, run) : 1;
+  for (int i = 0; i < nrun; i++)
+    CB2_CUDA(cudaMemcpyAsync(state + run[i][0] * n, c.d_host_state + run[i][0] * n,
+                             (run[i][1] - run[i][0]) * n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  if (after_step)
+    if (int rc = load_restart_history(c, true)) return rc;
   CB2_CUDA(cudaStreamSynchronize(c.stream));
   return check_status(c);
 }
@@ -763,13 +808,13 @@ int cb2_step_restart_state(cb2_ctx *c, double *state, double out_energies[7]) {
   if (rc) return rc;
   rj_start_derived(*c);
   if ((rc = nonlinear(*c))) return rc;
-  if ((rc = load_restart_history(*c))) return rc;   // the history has crossed meanwhile
+  if ((rc = load_restart_history(*c, false))) return rc;   // the history has crossed meanwhile
   c->istep = std::max(c->istep, 1) + 1;     // the loaded history makes this an Adams-Bashforth step
   cn_stage(*c, false);
   // the nonlinear terms of the new state are left to the next call (or to
   // the next cb2_step, which computes them first)
   c->terms_stale = true;
-  if ((rc = store_restart(*c, state))) return rc;
+  if ((rc = store_restart(*c, state, true))) return rc;
   return out_energies ? cb2_energies(c, out_energies) : 0;
 }
 

@@ -117,9 +117,10 @@ struct Ctx {
   double *d_tmp = nullptr;               // nr*jmax scratch for host transfers
   double *d_host_state = nullptr;        // 20 slots for cb2_step_host_state
   // copy stream of cb2_step_restart_state (the restart history uploads
-  // while the nonlinear terms of the state are computed) and its events
+  // while the nonlinear terms of the state are computed) and its events:
+  // state staged, history read by the step staged, all history staged
   cudaStream_t copy_stream = nullptr;
-  cudaEvent_t copy_ev[2] = {nullptr, nullptr};
+  cudaEvent_t copy_ev[3] = {nullptr, nullptr, nullptr};
   // mixed-precision Legendre operands (split fp16) -- owned by cb2_legendre_mixed.cu
   void *mixed = nullptr;
   // learned subgrid closure attached to the step (cb2_closure.cu), or null

@@ -170,7 +170,10 @@ int cb2_set_restart_state(cb2_ctx *ctx, const double *state, int istep);
  * cb2_step_host_state): loads the state, computes its derived fields and
  * nonlinear terms, advances one step and returns the new state.  The
  * nonlinear terms of the new state are left to the next call (or to the
- * next cb2_step, which computes them first).  out_energies may be NULL. */
+ * next cb2_step, which computes them first).  out_energies may be NULL.
+ * A step does not write the dS/dr entries of previous_momentum and
+ * previous_induction (entries 8 and 11), so the call leaves them as they are
+ * in `state` and copies 12 entries back instead of 14. */
 int cb2_step_restart_state(cb2_ctx *ctx, double *state, double out_energies[7]);
 
 /* Spherical transform of nvec vectors + nscal scalars at every radius
